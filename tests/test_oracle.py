@@ -1,0 +1,120 @@
+"""The oracle pinned against the reference's golden J-V curves (SimSS 5.36 runs committed in the
+reference's tests/data) at the reference's own tolerances, and its invariants.
+
+Tolerances and solvers follow the reference's tests (jaxdd tests/test_solver.py): 194-204
+(thin_l1_light 1e-5), 254-273 (held 1e-9, both solvers), 275-299 (regions 1e-6 / 2e-5), 302-321
+(two regions 2e-6), 878-888 (ions 2e-5), 890-906 (interface traps), 1318-1345 (resistances),
+1348-1358 (uniform generation), 408-420 (logarithmic scan), 1556-1575 (dark, batch, invariants),
+277-290 of the differential current (1e-9 single, 1e-8 batch)."""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from jaxdd_b200.device import build_device
+from jaxdd_b200.simss_input import read_setup, simss_voltages
+from oracle import dd
+
+#: case -> (tolerance of solve_jv, tolerance of solve_batch or None)
+GOLDENS = {
+    "thin_l1_light": (1e-5, None),
+    "frozen_1e17_x1_thin_light": (2e-5, None),
+    "steady_1e17_thin_light": (2e-5, None),
+    "held_thin_light": (1e-9, 1e-9),
+    "iface_charged_light": (1e-5, 1e-5),
+    "iface_ions_light": (2e-5, None),
+    "pin_iface_light": (1e-5, None),
+    "region_etl_light": (1e-6, 1e-6),
+    "region_htl_frozen_light": (2e-5, 2e-5),
+    "two_regions_light": (2e-6, 2e-6),
+    "frozen_thick_htl_dark": (None, 2e-5),
+    "diff_iface_light": (1e-9, 1e-8),
+    "none_light": (1e-5, None),
+    "resist_light": (1e-5, 1e-5),
+    "logv_light": (1e-5, None),
+}
+
+
+def _case(case):
+    setup = read_setup(GOLDEN / "inputs" / case / "simulation_setup.txt")
+    ref = np.genfromtxt(GOLDEN / "inputs" / case / "JV.dat", names=True)
+    V = simss_voltages(setup) if case == "logv_light" else ref["Vint"]
+    return build_device(setup, grid="simss"), V, ref
+
+
+@pytest.mark.parametrize("case", list(GOLDENS))
+def test_oracle_reproduces_simss(case):
+    dev, V, ref = _case(case)
+    scale = np.max(np.abs(ref["Jext"]))
+    tol_jv, tol_batch = GOLDENS[case]
+    if tol_jv is not None:
+        J, ok, _ = dd.solve_jv(dev, V, bernoulli_name="simss")
+        assert ok.all()
+        assert np.max(np.abs(J - ref["Jext"])) < tol_jv * scale
+    if tol_batch is not None:
+        J, ok, _ = dd.solve_batch(dd.prepare([dev]), V, bernoulli_name="simss")
+        assert ok.all()
+        assert np.max(np.abs(J[0] - ref["Jext"])) < tol_batch * scale
+        if case == "resist_light":  # V_ext = V_int + J·R_series against SimSS's
+            assert np.max(np.abs(V + J[0] * dev.R_series - ref["Vext"])) < 1e-4
+        if case == "frozen_thick_htl_dark":  # dark: monotone, zero at 0 V
+            b = dd.prepare([dev])
+            js = float(b["J_scale"][0])
+            assert np.all(np.diff(J[0]) > -dd.CURRENT_TOL * js)
+            assert abs(J[0][np.argmin(np.abs(V))]) < dd.CURRENT_TOL * js
+
+
+def test_batch_equals_single_and_mixed_batches():
+    """A batch of different devices (one with four ion slots, one with two, one without ions)
+    gives each device the curve it has alone (tests/test_solver.py:1479-1533)."""
+    names = ["two_regions_light", "pin_iface_light", "thin_l1_light"]
+    devs = [_case(c)[0] for c in names]
+    V = np.round(np.arange(-0.1, 1.25 + 1e-9, 0.05), 6)
+    J, ok, _ = dd.solve_batch(dd.prepare(devs), V)
+    assert ok.all()
+    for k, dev in enumerate(devs):
+        Js, oks, _ = dd.solve_batch(dd.prepare([dev]), V)
+        scale = float(dd.prepare([dev])["J_scale"][0])
+        assert np.max(np.abs(J[k] - Js[0])) < 1e-9 * scale
+
+
+@pytest.mark.parametrize("x", [-30.0, -1.0, -1e-3, 1e-3, 0.3, 2.0, 30.0])
+def test_bernoulli_identity(x):
+    """B(−x) = B(x) + x (tests/test_solver.py:56-59), and B' by central differences."""
+    for bern in (dd.bern_exact,):
+        assert float(bern(-x)[0]) == pytest.approx(float(bern(x)[0]) + x, rel=1e-12, abs=1e-14)
+        h = 1e-6 * max(1.0, abs(x))
+        fd = (bern(x + h)[0] - bern(x - h)[0]) / (2 * h)
+        assert float(bern(x)[1]) == pytest.approx(float(fd), rel=1e-6, abs=1e-9)
+
+
+def test_block_sweep_equals_a_dense_solve():
+    """The block Thomas sweep against a dense solve (tests/test_solver.py:1753-1773)."""
+    rng = np.random.default_rng(0)
+    nb, NP, m = 3, 12, 3
+    A = rng.normal(size=(nb, NP, 3, 3))
+    C = rng.normal(size=(nb, NP, 3, 3))
+    Bb = rng.normal(size=(nb, NP, 3, 3)) + 8 * np.eye(3)
+    A[:, 0] = 0
+    C[:, -1] = 0
+    d = rng.normal(size=(nb, NP, 3, m))
+    x = dd.block_thomas(A, Bb, C, d)
+    for b in range(nb):
+        M = np.zeros((3 * NP, 3 * NP))
+        for i in range(NP):
+            M[3 * i:3 * i + 3, 3 * i:3 * i + 3] = Bb[b, i]
+            if i:
+                M[3 * i:3 * i + 3, 3 * i - 3:3 * i] = A[b, i]
+            if i < NP - 1:
+                M[3 * i:3 * i + 3, 3 * i + 3:3 * i + 6] = C[b, i]
+        ref = np.linalg.solve(M, d[b].reshape(3 * NP, m))
+        assert np.allclose(x[b].reshape(3 * NP, m), ref, rtol=1e-10, atol=1e-12)
+
+
+def test_short_circuit_current_never_exceeds_the_generation():
+    """|J_sc| ≤ the generation's current (tests/test_solver.py:207-215)."""
+    dev, _, _ = _case("thin_l1_light")
+    J, ok, _ = dd.solve_jv(dev, np.array([0.0]))
+    from jaxdd_b200.constants import Q
+    generated = Q * np.sum(dev.h[:-1] * dev.G[:-1]) / np.sum(dev.h[:-1]) * dev.L
+    assert ok.all() and -J[0] <= generated * (1 + 1e-9)
