@@ -1,0 +1,386 @@
+"""Benchmark: J-V curves per second of the batched steady-state solve on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference] [--precision fp64]
+    python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N ...
+
+Workload: BASELINE's configuration 2 — 16384 devices per GPU drawn from seed 20261203 (grid
+NP = 400, 61 voltages from -0.2 to 1.3 V; half pre-biased at 1.0 V with their ions frozen, half
+with free ions; interface and bulk traps, doping and ion densities drawn), synthetic SIMsalabim
+inputs built by `jaxdd_b200.workloads`. One step = one `solve_batch` of the whole batch (every
+device's full J-V curve). Devices are independent: with N GPUs every rank solves its own 16384
+(weak scaling, no collective on the data path; the barrier and max-over-ranks timing only).
+
+Reports (one JSON line, rank 0): `value` (curves/s, inputs resident on the GPU, CUDA events),
+`e2e` (the same through the C ABI from pinned host buffers, copies in the timed region),
+`roofline` (the kernel's algorithmic bytes per launch over its event time, against the measured
+HBM copy bandwidth), `cpu_baseline` (the FP64 CPU oracle on one core, a bounded sample of the
+same workload), clocks sampled during the timed region.
+
+`--impl reference`: jaxdd itself needs JAX, which is not installed; its CPU path is stood in for
+by the FP64 oracle (a CPU restatement of its arithmetic), one single-threaded process per host
+core, each solving a small batch of the same workload (jaxdd benchmarks/run.py's protocol).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "J-V curves/s on 1 B200, mixed vs FP64 at 1e-6 of J scale; adjoint grads/s"
+DEVICES_PER_GPU = 16384
+NP = 400
+CHUNK = 512  # devices per build task (a multiple of 32)
+
+
+def _peaks() -> tuple[float, str]:
+    try:
+        data = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def _build_chunk(args):
+    """Build and pack devices [start, start + n) of the drawn workload (a pool worker)."""
+    start, n = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from jaxdd_b200.batch import prepare
+    from jaxdd_b200.workloads import drawn_devices
+    return prepare(drawn_devices(n, NP=NP, start=start))
+
+
+def build_workload(n: int, start: int, procs: int):
+    """The packed batch of devices [start, start + n), built in `procs` spawned processes (before
+    any CUDA call in this one)."""
+    from jaxdd_b200.batch import concat
+    tasks = [(start + k, min(CHUNK, n - k)) for k in range(0, n, CHUNK)]
+    if procs <= 1:
+        parts = [_build_chunk(t) for t in tasks]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            parts = pool.map(_build_chunk, tasks)
+    return concat(parts)
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = [r.split(", ") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        sm, mx, reasons = [], 0.0, set()
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, flag in zip(names, r[5:9]):
+                if flag.strip() == "Active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def step_bytes(NPk: int, border: bool, frozen: bool, w: int = 8) -> int:
+    """Algorithmic HBM bytes of one Newton step of one lane: c' and d' written and read back
+    (9 + 3 (1 + K') words per node, K' = 2 with the ions' border, else 0), the state read and
+    written (6 words), the static words a node needs (h, and the frozen ions' two)."""
+    kp = 2 if border else 0
+    n_stat = 1 + (2 if frozen else 0)
+    return NPk * (2 * (9 + 3 * (1 + kp)) * w + 48 + 8 * n_stat)
+
+
+def poisson_bytes(NPk: int, w: int = 8) -> int:
+    return NPk * (2 * 2 * w + 16)
+
+
+def algorithmic_bytes(batch, steps) -> float:
+    """Bytes of one launch from the steps each lane took (`lane_steps`)."""
+    total = 0.0
+    lanes = batch["lane_of"]
+    for k, dev in enumerate(batch["devices"]):
+        lane = lanes[k]
+        NPk = len(dev.x) - 2
+        frozen = bool(dev.pre_cond and dev.fix_ions)
+        total += steps[0, lane] * step_bytes(NPk, True, False)
+        total += steps[1, lane] * step_bytes(NPk, False, frozen)
+        total += steps[2, lane] * poisson_bytes(NPk)
+    return total
+
+
+def cpu_sample(n: int = 8):
+    """The oracle on one core over `n` devices of the workload (a bounded sample)."""
+    from jaxdd_b200.workloads import V_SCAN, drawn_devices
+    from oracle import dd
+    devs = drawn_devices(n, NP=NP, start=10 ** 6)
+    t0 = time.perf_counter()
+    dd.solve_batch(dd.prepare(devs), V_SCAN)
+    dt = time.perf_counter() - t0
+    return n / dt, dt
+
+
+def _ref_worker(args):
+    """One single-threaded process of the reference arm: solve `n` devices, `reps` times."""
+    core, start, n, reps = args
+    try:
+        os.sched_setaffinity(0, {core})
+    except (AttributeError, OSError):
+        pass
+    from jaxdd_b200.workloads import V_SCAN, drawn_devices
+    from oracle import dd
+    b = dd.prepare(drawn_devices(n, NP=NP, start=start))
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        dd.solve_batch(b, V_SCAN)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    per = 2  # batch 2 per process (jaxdd benchmarks/run.py's CPU protocol)
+    reps = args.warmup + args.steps
+    tasks = [(c % (os.cpu_count() or 1), 10 ** 6 + per * c, per, reps) for c in range(cores)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_ref_worker, tasks)
+    wall = time.perf_counter() - t0
+    timed = [sum(r[args.warmup:]) for r in res]
+    # all processes run together: the rate is the curves of the timed steps over their time
+    rate = sum(per * args.steps / t for t in timed)
+    step_ms = 1e3 * max(timed) / args.steps
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "curves/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "drawn p-i-n stacks (seed 20261203), NP 400, 61 V, "
+                               "batch 2 per process", "processes": cores},
+        "cpu_baseline": {"value": rate, "unit": "curves/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores} processes x {per} devices x {args.steps} timed "
+                                   f"steps (+{args.warmup} warm-up), wall {wall:.0f} s; "
+                                   "jaxdd needs JAX (absent): the FP64 oracle stands in"},
+        "e2e": {"value": rate, "unit": "curves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--precision", default="fp64", choices=("fp64",))
+    ap.add_argument("--devices", type=int, default=DEVICES_PER_GPU)
+    ap.add_argument("--build-procs", type=int, default=0)
+    ap.add_argument("--cpu-sample", type=int, default=8)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    if args.devices % 32:
+        raise SystemExit("--devices must be a multiple of 32")
+    cores = os.cpu_count() or 1
+    procs = args.build_procs or max(1, min(32, cores // max(1, world)))
+    t0 = time.perf_counter()
+    batch = build_workload(args.devices, rank * args.devices, procs)
+    build_s = time.perf_counter() - t0
+    cpu = cpu_sample(args.cpu_sample) if rank == 0 and world == 1 else None
+
+    import ctypes
+
+    import torch
+    from jaxdd_b200 import _lib
+    from jaxdd_b200.batch import _gpu, descriptor, initial_state
+    from jaxdd_b200.workloads import V_SCAN
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    g = _gpu(batch)
+    Bp, npmax = batch["Bp"], batch["np_max"]
+    nv = len(V_SCAN)
+    lanes = batch["lane_of"]
+    y0 = np.zeros((npmax + 2, 3, Bp))
+    for k, d in enumerate(batch["devices"]):
+        first = d.V_pre if d.pre_cond else V_SCAN[0]
+        y0[:len(d.x), :, lanes[k]] = initial_state(d, first)
+    flat = np.tile(V_SCAN, Bp)
+    offsets = (np.arange(Bp) * nv).astype(np.int32)
+    counts = np.full(Bp, nv, dtype=np.int32)
+    t_y0 = torch.from_numpy(y0).to(dev)
+    t_v = torch.from_numpy(flat).to(dev)
+    t_off = torch.from_numpy(offsets).to(dev)
+    t_cnt = torch.from_numpy(counts).to(dev)
+    J = torch.empty(Bp * nv, dtype=torch.float64, device=dev)
+    ok = torch.empty(Bp * nv, dtype=torch.uint8, device=dev)
+    its = torch.empty(Bp * nv, dtype=torch.int32, device=dev)
+    status = torch.empty(Bp, dtype=torch.int32, device=dev)
+    steps = torch.zeros((3, Bp), dtype=torch.int32, device=dev)
+    desc = descriptor(batch, g, t_y0)
+    volts = _lib.DdVoltages(t_v.data_ptr(), t_off.data_ptr(), t_cnt.data_ptr())
+    opts = _lib.DdOpts(1e-10, 60, 60, 0, 0, _lib.DD_MODE_BATCH, _lib.DD_PRECISION[args.precision], 0)
+    ws = g.workspace(desc)
+    so = _lib.lib()
+    stream = torch.cuda.current_stream(dev)
+
+    def launch(d=desc, v=volts):
+        _lib.check(so.dd_solve(ctypes.byref(d), ctypes.byref(v), ctypes.byref(opts),
+                               J.data_ptr(), ok.data_ptr(), its.data_ptr(), status.data_ptr(),
+                               steps.data_ptr(), ws.data_ptr(), ws.numel(), stream.cuda_stream),
+                   "dd_solve")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        launch()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            launch()
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    curves = args.devices * world
+    value = curves / (ms_max / 1e3)
+    ok_frac = float(ok.view(Bp, nv)[:batch["n"]].float().mean().item())
+    lane_steps = steps.cpu().numpy()
+
+    # e2e: the C ABI from pinned host buffers, the copies inside the timed region
+    host = {name: torch.from_numpy(arr).pin_memory() for name, arr in
+            (("stat", batch["stat"]), ("scal", batch["scal"]), ("iface", batch["iface"]),
+             ("y0", y0), ("v", flat), ("off", offsets), ("cnt", counts))}
+    dev_in = {k: torch.empty_like(v, device=dev) for k, v in host.items()}
+    J_h = torch.empty(Bp * nv, dtype=torch.float64).pin_memory()
+    ok_h = torch.empty(Bp * nv, dtype=torch.uint8).pin_memory()
+    its_h = torch.empty(Bp * nv, dtype=torch.int32).pin_memory()
+    desc2 = _lib.DdBatch(batch["n"], Bp, npmax, batch["ka"], batch["kc"],
+                         dev_in["stat"].data_ptr(), dev_in["scal"].data_ptr(),
+                         dev_in["iface"].data_ptr(), dev_in["y0"].data_ptr())
+    volts2 = _lib.DdVoltages(dev_in["v"].data_ptr(), dev_in["off"].data_ptr(),
+                             dev_in["cnt"].data_ptr())
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    d2h = J_h.numel() * 8 + ok_h.numel() + its_h.numel() * 4
+
+    def e2e_step():
+        for k in host:
+            dev_in[k].copy_(host[k], non_blocking=True)
+        launch(desc2, volts2)
+        J_h.copy_(J, non_blocking=True)
+        ok_h.copy_(ok, non_blocking=True)
+        its_h.copy_(its, non_blocking=True)
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    barrier()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    ev3.record(stream)
+    barrier()
+    e2e_ms = ev2.elapsed_time(ev3) / e2e_steps
+    t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = curves / (float(t.item()) / 1e3)
+
+    peak, peak_kind = _peaks()
+    alg = algorithmic_bytes(batch, lane_steps)
+    achieved = alg / (ms / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "curves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "BASELINE config 2: drawn p-i-n stacks (seed 20261203), "
+                                   f"{args.devices} devices/GPU, NP {NP}, {nv} voltages -0.2..1.3 V,"
+                                   " half frozen after a 1.0 V pre-bias, half free ions",
+                       "precision": args.precision, "devices_per_gpu": args.devices,
+                       "l2": f"inputs larger than L2 ({batch['stat'].nbytes / 1e9:.2f} GB of "
+                             "statics per launch)",
+                       "converged_fraction": ok_frac, "build_s": round(build_s, 1)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": alg},
+            "cpu_baseline": None if cpu is None else {
+                "value": cpu[0], "unit": "curves/s", "cores": 1, "kind": "port",
+                "sample": f"{args.cpu_sample} devices of the same workload, one batch, "
+                          f"{cpu[1]:.1f} s on one core (FP64 NumPy oracle; jaxdd needs JAX)"},
+            "e2e": {"value": e2e_value, "unit": "curves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

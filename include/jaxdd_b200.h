@@ -1,0 +1,118 @@
+/* jaxdd_b200 — C ABI of the batched steady-state drift-diffusion solve on sm_100a.
+ *
+ * The drop-in boundary for jaxdd's batched J-V path. jaxdd itself has no native layer: its
+ * solve is one jitted JAX program (`_solve_batch`, jaxdd src/jaxdd/batch.py:1033-1047) whose
+ * only hand-written kernel is the Pallas block sweep (`block_sweep`, src/jaxdd/sweep.py:313-330).
+ * These entry points are what an XLA FFI custom call (or ctypes / a torch extension) binds in
+ * its place: plain pointers and sizes, caller-owned device buffers, stream-ordered, no host
+ * synchronisation, no allocation (scratch comes from `dd_workspace_bytes`).
+ *
+ * Layout: every array is lane-interleaved (one lane = one device; lane fastest), see
+ * jaxdd_b200/csrc/dd_layout.h for the field indices. The host packer that writes it is
+ * jaxdd_b200/batch.py (`prepare`).
+ *
+ * Errors: a nonzero status for invalid arguments or a failed launch. Non-convergence is never
+ * an error: it is reported per (device, voltage) in `converged`, as jaxdd reports it
+ * (docs/solver.md "Convergence"; batch.py:1006).
+ */
+#ifndef JAXDD_B200_H
+#define JAXDD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define DD_OK 0
+#define DD_ERR_ARGS 1       /* a size, pointer or option out of range */
+#define DD_ERR_WORKSPACE 2  /* workspace smaller than dd_workspace_bytes */
+#define DD_ERR_LAUNCH 3     /* the CUDA launch failed (cudaGetLastError) */
+#define DD_ERR_DEVICE 4     /* no sm_100 device current */
+
+/* Per-lane status written by dd_solve (lane_status). */
+#define DD_LANE_OK 0
+#define DD_LANE_PREBIAS_FAILED 1 /* solve_jv mode: the pre-bias did not converge
+                                    (jaxdd solver.py:2228-2229 raises RuntimeError) */
+
+/* A packed batch (device pointers). Mirrors the pytree `prepare` returns
+ * (jaxdd batch.py:151-223), in the layout of dd_layout.h. */
+typedef struct dd_batch {
+  int32_t n_lanes;     /* devices in the batch */
+  int32_t lane_stride; /* >= n_lanes, a multiple of 32 */
+  int32_t np_max;      /* the largest grid size NP of any lane (interior points) */
+  int32_t k_anion;     /* anion slots (mobile regions), >= 1 */
+  int32_t k_cation;    /* cation slots, >= 1; k_anion + k_cation <= 4 */
+  const double* stat;  /* [(np_max + 2)][DD_NF][lane_stride] */
+  const double* scal;  /* [DD_NS_BASE + k_anion + k_cation][lane_stride] */
+  const double* iface; /* [DD_MAXIF][DD_NIF][lane_stride] */
+  const double* y0;    /* [(np_max + 2)][3][lane_stride]: (V, ln n, ln p) start at the first voltage */
+} dd_batch;
+
+/* Each lane's voltages (internal, V), flat: lane l's are v[offset[l] ... offset[l]+count[l]).
+ * Ascending in DD_MODE_BATCH (solve_batch sorts them, batch.py:1043-1045); in the caller's
+ * order in DD_MODE_JV. Outputs J/converged/iterations use the same flat positions. */
+typedef struct dd_voltages {
+  const double* v;
+  const int32_t* offset;
+  const int32_t* count;
+} dd_voltages;
+
+#define DD_MODE_BATCH 0 /* jaxdd batch.solve_batch: outward scan, extrapolated starts */
+#define DD_MODE_JV 1    /* jaxdd solver.solve_jv: caller's order, each from the last solution */
+
+#define DD_BERNOULLI_EXACT 0 /* solver.bernoulli (solver.py:95-105) */
+#define DD_BERNOULLI_SIMSS 1 /* solver.bernoulli_simss (solver.py:108-121) */
+
+#define DD_PRECISION_FP64 0  /* everything in FP64 */
+#define DD_PRECISION_MIXED 1 /* FP32 Jacobian and block sweep, FP64 residual, update, current */
+
+typedef struct dd_opts {
+  double tol;         /* Newton's step tolerance (solve_batch tol, default 1e-10) */
+  int32_t max_iter;   /* Newton steps per voltage (60 batch, 200 jv) */
+  int32_t start_iter; /* Poisson / start / pre-bias cap (= max_iter in jaxdd) */
+  int32_t strict;     /* 1: only tol or the round-off floor stop Newton (batch.py:815-816) */
+  int32_t bernoulli;  /* DD_BERNOULLI_* */
+  int32_t mode;       /* DD_MODE_* */
+  int32_t precision;  /* DD_PRECISION_* */
+  int32_t reserved;
+} dd_opts;
+
+/* Scratch bytes dd_solve needs for this batch (four state buffers, the frozen-ion profile,
+ * the sweep's c'/d' per node, per-lane records). */
+int dd_workspace_bytes(const dd_batch* batch, size_t* bytes);
+
+/* The J-V curves of a batch: jaxdd's solve_batch (DD_MODE_BATCH; batch.py:1136-1162, one pass
+ * at max_iter, which gives what its two passes give) or solve_jv (DD_MODE_JV; solver.py:2041-2060)
+ * for every lane. J (A/m^2, SIMsalabim's sign, the shunt's current added), converged (0/1) and
+ * iterations at each flat voltage position; lane_status per lane; lane_steps (may be NULL)
+ * [3][lane_stride] the steps each lane took in all: Newton steps with the ions' border (mobile
+ * ions), Newton steps without it, Poisson steps. Asynchronous on `stream` (a cudaStream_t,
+ * NULL the legacy default stream). */
+int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts, double* J,
+             uint8_t* converged, int32_t* iterations, int32_t* lane_status, int32_t* lane_steps,
+             void* workspace, size_t workspace_bytes, void* stream);
+
+/* One damped Newton step per lane from the state y (`[(np_max+2)][3][lane_stride]`, interior
+ * nodes used) and the ion normalisations logs (`[K][lane_stride]`) at the voltage Vint
+ * (`[lane_stride]`), ions scaled by `share`: jaxdd's `_newton_step` (solver.py:1563-1608),
+ * batch.py:759-785. Writes the new state in place, the new logs, the step's size and the
+ * current at the new state (integral or differential form, without the shunt). For checking a
+ * single step against a CPU restatement; dd_solve does not call it. */
+int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double* vint,
+                   double share, const dd_opts* opts, double* size, double* J, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
+/* A human-readable name of a status code. */
+const char* dd_status_string(int status);
+
+/* ABI version: (major << 16) | minor. */
+int dd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JAXDD_B200_H */

@@ -1,0 +1,82 @@
+"""ctypes binding of the C ABI in include/jaxdd_b200.h (the library built by jaxdd_b200.build).
+
+Loading fails loudly when the library is missing: the package has no other compute path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from functools import lru_cache
+
+from .build import LIB
+
+#: field counts of jaxdd_b200/csrc/dd_layout.h
+DD_NF = 26
+DD_NS_BASE = 19
+DD_NIF = 10
+DD_MAXIF = 4
+DD_MAXK = 4
+DD_NBUF = 4
+
+S = {name: k for k, name in enumerate((
+    "OFFN", "OFFP", "MUN", "MUP", "H", "DX", "FACL", "FACM", "FACU", "FAC", "SP", "SC", "DOP",
+    "KD", "NI2", "NT", "CNT", "CPT", "NT0", "PT0", "G", "ASLOT", "CSLOT", "AFIX", "CFIX", "IFK"))}
+C = {name: k for k, name in enumerate((
+    "VT", "L", "V0", "VL", "LEFT", "LNNL", "LNPL", "LNNR", "LNPR", "JSCALE", "GSHUNT",
+    "PRECOND", "VPRE", "FIXIONS", "GFRAC", "NFLOOR", "NP", "CURRDIFF", "HSUM"))}
+I = {name: k for k, name in enumerate((
+    "NT", "CN", "CP", "NT0LO", "PT0LO", "NT0HI", "PT0HI", "IW", "CHARGE", "CWE"))}
+assert len(S) == DD_NF and len(C) == DD_NS_BASE and len(I) == DD_NIF
+
+DD_MODE_BATCH, DD_MODE_JV = 0, 1
+DD_BERNOULLI = {"exact": 0, "simss": 1}
+DD_PRECISION = {"fp64": 0, "mixed": 1}
+DD_LANE_PREBIAS_FAILED = 1
+
+#: every symbol include/jaxdd_b200.h declares
+EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve",
+           "dd_newton_step")
+
+
+class DdBatch(ctypes.Structure):
+    _fields_ = [("n_lanes", ctypes.c_int32), ("lane_stride", ctypes.c_int32),
+                ("np_max", ctypes.c_int32), ("k_anion", ctypes.c_int32),
+                ("k_cation", ctypes.c_int32), ("stat", ctypes.c_void_p),
+                ("scal", ctypes.c_void_p), ("iface", ctypes.c_void_p), ("y0", ctypes.c_void_p)]
+
+
+class DdVoltages(ctypes.Structure):
+    _fields_ = [("v", ctypes.c_void_p), ("offset", ctypes.c_void_p), ("count", ctypes.c_void_p)]
+
+
+class DdOpts(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("max_iter", ctypes.c_int32),
+                ("start_iter", ctypes.c_int32), ("strict", ctypes.c_int32),
+                ("bernoulli", ctypes.c_int32), ("mode", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+@lru_cache(maxsize=1)
+def lib() -> ctypes.CDLL:
+    if not LIB.exists():
+        raise RuntimeError(f"the jaxdd_b200 CUDA library is not built ({LIB}); run "
+                           "`python -m jaxdd_b200.build` (or __graft_entry__.build())")
+    so = ctypes.CDLL(str(LIB))
+    p = ctypes.c_void_p
+    so.dd_abi_version.restype = ctypes.c_int
+    so.dd_status_string.restype = ctypes.c_char_p
+    so.dd_status_string.argtypes = [ctypes.c_int]
+    so.dd_workspace_bytes.restype = ctypes.c_int
+    so.dd_workspace_bytes.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(ctypes.c_size_t)]
+    so.dd_solve.restype = ctypes.c_int
+    so.dd_solve.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
+                            ctypes.POINTER(DdOpts), p, p, p, p, p, p, ctypes.c_size_t, p]
+    so.dd_newton_step.restype = ctypes.c_int
+    so.dd_newton_step.argtypes = [ctypes.POINTER(DdBatch), p, p, p, ctypes.c_double,
+                                  ctypes.POINTER(DdOpts), p, p, p, ctypes.c_size_t, p]
+    return so
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise RuntimeError(f"{what}: {lib().dd_status_string(status).decode()} ({status})")

@@ -1,0 +1,70 @@
+"""The C ABI without a GPU: the library builds for sm_100a, loads, and exports every symbol the
+header declares; the packer writes the layout the kernel reads."""
+
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+from jaxdd_b200 import _lib
+from jaxdd_b200.batch import prepare
+from jaxdd_b200.device import build_device
+from jaxdd_b200.simss_input import read_setup
+
+
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / "include" / "jaxdd_b200.h").read_text()
+    declared = set(re.findall(r"^\s*(?:int|const char\*)\s+(dd_\w+)\(", header, re.M))
+    assert declared == set(_lib.EXPORTS)
+    so = _lib.lib()
+    for name in declared:
+        assert hasattr(so, name), name
+    assert so.dd_abi_version() >> 16 == 1
+    assert so.dd_status_string(0).decode() == "ok"
+
+
+def test_layout_constants_match_the_header():
+    text = (ROOT / "jaxdd_b200" / "csrc" / "dd_layout.h").read_text()
+    start = text.index("enum StaticField")
+    body = text[start:text.index("DD_NF", start)]
+    names = re.findall(r"\bS_(\w+)", body)
+    assert names == list(_lib.S)
+    assert f"DD_MAXIF = {_lib.DD_MAXIF}" in text and f"DD_MAXK = {_lib.DD_MAXK}" in text
+
+
+def test_workspace_query_and_argument_checks():
+    dev = build_device(read_setup(GOLDEN / "inputs" / "thin_l1_light" / "simulation_setup.txt"))
+    b = prepare([dev])
+    desc = _lib.DdBatch(b["n"], b["Bp"], b["np_max"], b["ka"], b["kc"], 1, 1, 1, 1)
+    import ctypes
+    size = ctypes.c_size_t(0)
+    assert _lib.lib().dd_workspace_bytes(ctypes.byref(desc), ctypes.byref(size)) == 0
+    nodes = b["np_max"] + 2
+    assert size.value == 8 * nodes * b["Bp"] * (4 * 3 + 2 + 12 + 3 * 2)
+    bad = _lib.DdBatch(b["n"], 31, b["np_max"], 1, 1, 1, 1, 1, 1)
+    assert _lib.lib().dd_workspace_bytes(ctypes.byref(bad), ctypes.byref(size)) == 1
+
+
+def test_packer_writes_the_stencils():
+    dev = build_device(read_setup(GOLDEN / "inputs" / "two_regions_light" / "simulation_setup.txt"))
+    b = prepare([dev])
+    S = _lib.S
+    col = b["stat"][:, :, 0]
+    NP = len(dev.x) - 2
+    assert np.array_equal(col[:NP + 2, S["OFFN"]], dev.offset_n)
+    assert b["ka"] == 2 and b["kc"] == 2
+    assert set(np.unique(col[:NP + 2, S["ASLOT"]])) == {-1.0, 0.0, 1.0}
+    assert np.sum(col[:, S["IFK"]] >= 0) == 2  # two trapped interfaces
+    assert b["scal"][_lib.DD_NS_BASE:_lib.DD_NS_BASE + 4, 0].min() > 0
+
+
+def test_mixed_grid_sizes_are_refused_unless_ragged():
+    a = build_device(read_setup(GOLDEN / "inputs" / "thin_l1_light" / "simulation_setup.txt"))
+    from jaxdd_b200.workloads import pin_stack
+    c = pin_stack(NP=120)
+    with pytest.raises(ValueError, match="one grid size"):
+        prepare([a, c])
+    b = prepare([a, c], ragged=True)
+    assert b["np_max"] == 400 and list(b["NP"]) == [400, 120]
