@@ -44,6 +44,8 @@ METRIC = "J-V curves/s on 1 B200, mixed vs FP64 at 1e-6 of J scale; adjoint grad
 DEVICES_PER_GPU = 16384
 NP = 400
 CHUNK = 512  # devices per build task (a multiple of 32)
+#: which kernel build profiles/traffic.json must describe for its traffic to be reported
+KERNEL_TAG = "two-pass fused Newton, 26-word static record"
 
 
 def _peaks() -> tuple[float, str]:
@@ -349,6 +351,14 @@ def main() -> None:
     e2e_value = curves / (float(t.item()) / 1e3)
 
     peak, peak_kind = _peaks()
+    traffic = None
+    try:  # the ncu capture of the same kernel and workload (profiles/), per launch
+        rec = json.loads((ROOT / "profiles" / "traffic.json").read_text())
+        entry = rec.get(f"solve_kernel_{args.precision}_config2")
+        if entry and entry["devices"] == args.devices and KERNEL_TAG in entry["kernel"]:
+            traffic = entry["dram_bytes_per_launch"]
+    except (OSError, ValueError, KeyError):
+        traffic = None
     alg = algorithmic_bytes(batch, lane_steps)
     achieved = alg / (ms / 1e3) / 1e9
     if rank == 0:
@@ -365,7 +375,7 @@ def main() -> None:
                              "statics per launch)",
                        "converged_fraction": ok_frac, "build_s": round(build_s, 1)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": None if cpu is None else {
