@@ -12,7 +12,7 @@ from .build import LIB
 
 #: field counts of jaxdd_b200/csrc/dd_layout.h
 DD_NF = 26
-DD_NS_BASE = 19
+DD_NS_BASE = 20
 DD_NIF = 10
 DD_MAXIF = 4
 DD_MAXK = 4
@@ -23,7 +23,7 @@ S = {name: k for k, name in enumerate((
     "KD", "NI2", "NT", "CNT", "CPT", "NT0", "PT0", "G", "ASLOT", "CSLOT", "AFIX", "CFIX", "IFK"))}
 C = {name: k for k, name in enumerate((
     "VT", "L", "V0", "VL", "LEFT", "LNNL", "LNPL", "LNNR", "LNPR", "JSCALE", "GSHUNT",
-    "PRECOND", "VPRE", "FIXIONS", "GFRAC", "NFLOOR", "NP", "CURRDIFF", "HSUM"))}
+    "PRECOND", "VPRE", "FIXIONS", "GFRAC", "NFLOOR", "NP", "CURRDIFF", "HSUM", "MID"))}
 I = {name: k for k, name in enumerate((
     "NT", "CN", "CP", "NT0LO", "PT0LO", "NT0HI", "PT0HI", "IW", "CHARGE", "CWE"))}
 assert len(S) == DD_NF and len(C) == DD_NS_BASE and len(I) == DD_NIF

@@ -123,12 +123,25 @@ def _pack_one(dev, stat, scal, iface, lane, ka_all, kc_all):
     sc[C["NP"]] = NP
     sc[C["CURRDIFF"]] = float(dev.curr_diff)
     sc[C["HSUM"]] = np.sum(h[:NP + 1])
+    sc[C["MID"]] = split_row(NP, ifk)
     ta = _totals(dev.anion_total, dev.anion_totals)
     tc = _totals(dev.cation_total, dev.cation_totals)
     sc[_lib.DD_NS_BASE:_lib.DD_NS_BASE + len(ta)] = ta
     sc[_lib.DD_NS_BASE + ka_all:_lib.DD_NS_BASE + ka_all + len(tc)] = tc
     # cation slot indices count from 0 within the cations; the kernel adds k_anion
     return max(generated, 1.0)
+
+
+def split_row(NP: int, ifk: np.ndarray) -> int:
+    """The row where the two halves of the kernel's twisted sweep meet: near the middle, with
+    no layer interface on the three intervals around it (so that no interface term straddles
+    the two halves)."""
+    m0 = NP // 2
+    for d in range(NP):
+        for m in (m0 - d, m0 + d):
+            if 2 <= m <= NP - 2 and all(ifk[e] == -2 for e in (m - 1, m, m + 1)):
+                return m
+    raise NotImplementedError(f"no row to split a grid of {NP} points between its interfaces")
 
 
 def prepare(devices, ragged: bool = False) -> Batch:

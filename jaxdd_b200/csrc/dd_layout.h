@@ -45,6 +45,8 @@ enum ScalarField {
   C_VT = 0, C_L, C_V0, C_VL, C_LEFT, C_LNNL, C_LNPL, C_LNNR, C_LNPR,
   C_JSCALE, C_GSHUNT, C_PRECOND, C_VPRE, C_FIXIONS, C_GFRAC, C_NFLOOR, C_NP, C_CURRDIFF,
   C_HSUM,       // sum of h over the NP + 1 intervals
+  C_MID,        // the row where the two halves of the twisted sweep meet (no interface within
+                // one interval of it)
   C_TOT0,       // slot totals follow: C_TOT0 + k, k < K (anion slots first)
   DD_NS_BASE = C_TOT0
 };

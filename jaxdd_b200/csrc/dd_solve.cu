@@ -1,5 +1,5 @@
-// Batched steady-state drift-diffusion J-V solve for sm_100a: one persistent launch, one thread
-// per device ("lane"), every array lane-interleaved (dd_layout.h).
+// Batched steady-state drift-diffusion J-V solve for sm_100a: one persistent launch, two
+// threads per device (a "pair" of adjacent lanes), every array lane-interleaved (dd_layout.h).
 //
 // What it computes is jaxdd's solve_batch / solve_jv (src/jaxdd/batch.py, src/jaxdd/solver.py):
 // Newton on (V, ln n, ln p) at every interior point, the residual and 3x3 Jacobian blocks of
@@ -10,20 +10,24 @@
 // (`_start`, batch.py:875-934) and the outward voltage scan (`_solve_one`, batch.py:937-1006).
 //
 // How it computes it is this file's own:
-//  * A Newton step is two passes over the grid. The forward pass assembles row i in registers
-//    (each interval's fluxes once, carried to the next row), eliminates it at once
-//    (M = B - A c', c' = M^-1 C, d' = M^-1 (r - A d')), and writes only c' and d'. It also
-//    carries w' = U^-T W (U the unit upper factor of the sweep, W the constraints' border), so
-//    that W^T T^-1 [r | U] = sum w'^T d' is known when the forward pass ends: the K x K Schur
-//    complement is solved before the backward pass, and one back substitution with the right
-//    side d'_F - d'_U z gives the bordered step directly.
-//  * The backward pass back-substitutes, damps (`density_steps`), updates the state in place,
-//    measures the step, and accumulates the terminal current right to left (the integral form's
-//    prefix sums rewritten as suffix sums), so the current needs no pass of its own.
-//  * Each lane runs its own program (start, pre-bias, scan) as a state machine; every loop
-//    iteration takes one Newton (or Poisson) step in every lane, at that lane's own voltage.
-//    Lanes never wait for another lane's voltage, so jaxdd's two passes (first_max_iter, then
+//  * The block tridiagonal system is solved by a twisted (two-sided) factorisation: half 0 of a
+//    pair eliminates rows 1..mid-1 downwards while half 1 eliminates rows NP..mid+1 upwards;
+//    they meet at row mid (one 3x3 solve with the "twisted pivot" B - A c' - C a''), then each
+//    back-substitutes its own half. The serial chain per thread is half the grid and twice the
+//    threads are in flight. Each row is assembled in registers as it is eliminated (each
+//    interval's fluxes once); only c' (or a'') and d' go to memory.
+//  * The ions' border is carried along both eliminations (w = U^-T W and the sums w^T d'), so
+//    its K x K Schur complement is solved at the meeting row and one back substitution with the
+//    right-hand side d'_F - d'_U z gives the bordered step directly.
+//  * The back substitution damps (`density_steps`), updates the state in place, measures the
+//    step, and accumulates the terminal current: half 0 right to left with suffix sums, half 1
+//    left to right with prefix sums, combined exactly at the end (no pass of its own).
+//  * Each device runs its own program (start, pre-bias, scan) as a state machine; every loop
+//    iteration takes one Newton (or Poisson) step at that device's own voltage. Devices never
+//    wait for another device's voltages, so jaxdd's two passes (first_max_iter, then
 //    stragglers, batch.py:1194-1208) collapse into one pass at max_iter with the same results.
+//    The pair takes every decision on half 0's values (broadcast by warp shuffles), so the two
+//    threads never part ways; they exchange data only through shuffles.
 //  * Every loop is bounded (caps on Poisson and Newton steps, voltages, stages): the kernel
 //    always terminates.
 #include <cuda_runtime.h>
@@ -115,6 +119,11 @@ struct Lane {
   size_t ybuf;  // elements per state buffer
   bool frozen;
   double share;
+  // the pair of threads that share this device: half 0 eliminates rows 1..mid-1 downwards
+  // and owns points 1..mid, half 1 eliminates rows NP..mid+1 upwards and owns mid+1..NP
+  int half, mid;
+  unsigned mask;  // the pair's two lanes in the warp
+  int base;       // warp lane of half 0
 
   __device__ __forceinline__ double st(int k, int f) const {
     return __ldg(S + ((size_t)k * DD_NF + f) * Bp + l);
@@ -328,8 +337,23 @@ __device__ void small_solve(double (&M)[K][K], double (&r)[K], double (&z)[K]) {
 // ------------------------------------------------------------------------------------ advance
 
 // How the first forward pass of a voltage makes its start from the carried solutions
+
+// ------------------------------------------------------------------------------------ pair
+
+__device__ __forceinline__ double xchg(const Lane& L, double v) {
+  return __shfl_xor_sync(L.mask, v, 1);
+}
+__device__ __forceinline__ int xchgi(const Lane& L, int v) { return __shfl_xor_sync(L.mask, v, 1); }
+__device__ __forceinline__ double bcast(const Lane& L, double v) {
+  return __shfl_sync(L.mask, v, L.base);
+}
+__device__ __forceinline__ int bcasti(const Lane& L, int v) { return __shfl_sync(L.mask, v, L.base); }
+
+// ------------------------------------------------------------------------------------ advance
+
+// How the first forward pass of a voltage makes its start from the carried solutions
 // (`_solve_one`'s scan body, batch.py:964-1004): buffers 0 iterate, 1 carry, 2 previous carry,
-// 3 the pre-bias solution.
+// 3 the pre-bias solution. Only the thread that owns node k calls this for k.
 enum Adv { ADV_NONE = 0, ADV_KEEP, ADV_NOKEEP, ADV_TURN };
 
 __device__ __forceinline__ void load_state(const Lane& L, int k, int adv, double ratio, Pt& P) {
@@ -356,25 +380,303 @@ __device__ __forceinline__ void load_state(const Lane& L, int k, int adv, double
         *L.y(1, k, c) = base;
         *L.y(2, k, c) = base;
       }
-      s[c] = base + clipd(ratio * (base - prev), -cap[c], cap[c]);
+      s[c] = ratio != 0.0 ? base + clipd(ratio * (base - prev), -cap[c], cap[c]) : base;
       *L.y(0, k, c) = s[c];
     }
   }
   P.V = s[0]; P.lnn = s[1]; P.lnp = s[2];
 }
 
+// ------------------------------------------------------------------------------------ rows
+
+// Row i's residual and blocks (`_assemble`, solver.py:1021-1187, the supported scope) from its
+// points (i-1, i, i+1) and intervals (left el, right er): A, B, C in (V, ln n, ln p), the
+// right-hand side -F (or, with `noise`, each row's round-off eps sum |dF/dy| |y|, `_noise_step`),
+// the ion columns U (Poisson row only) and the constraints' border W (potential only).
+//
+// In the mirrored frame of half 1 (nodes taken from NP down, `mirror`) "behind" (pm) is the
+// physical right neighbour and "ahead" (pn) the left one: the fluxes are evaluated in that order
+// (which turns their sign, as the mirrored equations want), the Poisson stencil's two sides swap
+// (fL, fU), and A couples to the point behind, C to the one ahead, as in the unmirrored frame.
+// Only the interface traps, which know their physical left and right, read `mirror`.
+template <int K>
+__device__ __forceinline__ void assemble_row(const Lane& L, int i, const Pt& pm, const Pt& pc,
+                                             const Pt& pn, const Flux& el, const Flux& er,
+                                             double hm, double hp, int ifk_m, int ifk_i,
+                                             bool noise, bool mirror, double (&A)[3][3],
+                                             double (&Bm)[3][3], double (&Cm)[3][3],
+                                             double (&rhs)[3], double (&U0)[K], double (&W)[K]) {
+  const double iVt = L.iVt;
+  const double facl = L.st(i, mirror ? S_FACU : S_FACL), facm = L.st(i, S_FACM);
+  const double facu = L.st(i, mirror ? S_FACL : S_FACU);
+  const double fac = L.st(i, S_FAC), sP = L.st(i, S_SP), sC = L.st(i, S_SC);
+  double R, dRn, dRp;
+  recomb(L, i, pc.n, pc.p, R, dRn, dRp);
+  const double gen = L.st(i, S_G) * L.gfrac;
+  double elec = hm * er.Fn - hp * el.Fn + fac * (gen - R);
+  double hole = hp * el.Fp - hm * er.Fp + fac * (gen - R);
+  double pois = facl * pm.V + facm * pc.V + facu * pn.V -
+                Q * (pc.n - pc.p + L.st(i, S_DOP) + L.afix(i) + pc.da - L.cfix(i) - pc.dc);
+  A[0][0] = facl * sP; A[0][1] = 0.0; A[0][2] = 0.0;
+  A[1][0] = -hp * el.n0V * sC; A[1][1] = -hp * el.n0n * sC; A[1][2] = 0.0;
+  A[2][0] = hp * el.p0V * sC;  A[2][1] = 0.0;               A[2][2] = hp * el.p0p * sC;
+  Bm[0][0] = (facm - Q * (pc.da + pc.dc) * iVt) * sP;
+  Bm[0][1] = -Q * pc.n * sP;
+  Bm[0][2] = Q * pc.p * sP;
+  Bm[1][0] = (-hp * el.n1V + hm * er.n0V) * sC;
+  Bm[1][1] = (-hp * el.n1n + hm * er.n0n - fac * dRn) * sC;
+  Bm[1][2] = (-fac * dRp) * sC;
+  Bm[2][0] = (hp * el.p1V - hm * er.p0V) * sC;
+  Bm[2][1] = (-fac * dRn) * sC;
+  Bm[2][2] = (hp * el.p1p - hm * er.p0p - fac * dRp) * sC;
+  Cm[0][0] = facu * sP; Cm[0][1] = 0.0; Cm[0][2] = 0.0;
+  Cm[1][0] = hm * er.n1V * sC; Cm[1][1] = hm * er.n1n * sC; Cm[1][2] = 0.0;
+  Cm[2][0] = -hm * er.p1V * sC; Cm[2][1] = 0.0; Cm[2][2] = -hm * er.p1p * sC;
+  if (ifk_m >= 0 || ifk_i >= 0) {
+    const double sc3[3] = {Q * sP, -fac * sC, -fac * sC};
+    double X[3] = {0.0, 0.0, 0.0};
+    Iface t;
+    // (value, derivative in this point's own ln n / ln p, in the other end's) of an interval
+    // whose physical left end is `left_is_me ? pc : other`
+    auto add = [&](int ifk, const Pt& other, bool left_is_me, double (&Oth)[3][3]) {
+      if (left_is_me) iface_edge(L, ifk, pc.n, other.n, pc.p, other.p, t, true);
+      else iface_edge(L, ifk, other.n, pc.n, other.p, pc.p, t, true);
+      const int lo[3] = {4, 0, 2}, hi[3] = {4, 1, 3};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int q = left_is_me ? lo[r] : hi[r];
+        const int dn_me = left_is_me ? 0 : 1, dp_me = left_is_me ? 2 : 3;
+        X[r] += t.v[q];
+        Bm[r][1] += sc3[r] * t.d[dn_me][q];
+        Bm[r][2] += sc3[r] * t.d[dp_me][q];
+        Oth[r][1] += sc3[r] * t.d[1 - dn_me][q];
+        Oth[r][2] += sc3[r] * t.d[5 - dp_me][q];
+      }
+    };
+    if (ifk_m >= 0) add(ifk_m, pm, mirror, A);    // the interval behind this point
+    if (ifk_i >= 0) add(ifk_i, pn, !mirror, Cm);  // the interval ahead of it
+    pois += Q * X[0];
+    elec -= fac * X[1];
+    hole -= fac * X[2];
+  }
+  if (!noise) {
+    rhs[0] = -pois * sP; rhs[1] = -elec * sC; rhs[2] = -hole * sC;
+#pragma unroll
+    for (int k = 0; k < K; ++k) U0[k] = 0.0;
+    if (pc.sl.a >= 0) U0[pc.sl.a] = -Q * pc.da * sP;
+    if (pc.sl.c >= 0) U0[L.ka + pc.sl.c] = Q * pc.dc * sP;
+    ion_w<K>(L, pm, pc, pn, hm * L.L, hp * L.L, W);
+  } else {
+    const double ym[3] = {fabs(pm.V), fabs(pm.lnn), fabs(pm.lnp)};
+    const double yc[3] = {fabs(pc.V), fabs(pc.lnn), fabs(pc.lnp)};
+    const double yn[3] = {fabs(pn.V), fabs(pn.lnn), fabs(pn.lnp)};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        s += fabs(A[r][c]) * ym[c] + fabs(Bm[r][c]) * yc[c] + fabs(Cm[r][c]) * yn[c];
+      rhs[r] = EPS64 * s;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) { U0[k] = 0.0; W[k] = 0.0; }
+  }
+}
+
+// The inverse of a 3x3 block by its adjugate (jaxdd's choice, `_inverse3`, solver.py:1481-1495).
+__device__ __forceinline__ void inv3(const double (&M)[3][3], double (&Mi)[3][3]) {
+  const double co00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+  const double co01 = M[0][2] * M[2][1] - M[0][1] * M[2][2];
+  const double co02 = M[0][1] * M[1][2] - M[0][2] * M[1][1];
+  const double co10 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+  const double co11 = M[0][0] * M[2][2] - M[0][2] * M[2][0];
+  const double co12 = M[0][2] * M[1][0] - M[0][0] * M[1][2];
+  const double co20 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+  const double co21 = M[0][1] * M[2][0] - M[0][0] * M[2][1];
+  const double co22 = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+  const double idet = 1.0 / (M[0][0] * co00 + M[0][1] * co10 + M[0][2] * co20);
+  Mi[0][0] = co00 * idet; Mi[0][1] = co01 * idet; Mi[0][2] = co02 * idet;
+  Mi[1][0] = co10 * idet; Mi[1][1] = co11 * idet; Mi[1][2] = co12 * idet;
+  Mi[2][0] = co20 * idet; Mi[2][1] = co21 * idet; Mi[2][2] = co22 * idet;
+}
+
+// The elimination carried along one direction of the twisted sweep. Going down (half 0) a row
+// reads A x_{i-1} + B x_i + C x_{i+1} = r with x_{i-1} = d' - c' x_i already known in terms of
+// x_i: X = A couples to the eliminated side, Y = C to the rest, and c'_i = M^-1 C,
+// d'_i = M^-1 (r - A d'), M = B - A c'. Going up (half 1) the same with X = C, Y = A (x_i =
+// d'' - a'' x_{i-1}). Beside them w (the border W carried through the sweep, w_i = W_i - c'^T
+// w_{i-1}) and the sums w^T d', so that W^T x over this half is known without x.
+template <int K>
+struct Carry {
+  double c[9];         // c' (or a'')
+  double dF[3];        // d' of the residual column
+  double dU[3][K];     // d' of the ion columns
+  double w[3][K];      // w
+  double S[K][K];      // sum w^T d'_U
+  double s[K];         // sum w^T d'_F
+  double num[K];       // the slots' ion numbers over this half's intervals
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) c[j] = 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      dF[r] = 0.0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) { dU[r][k] = 0.0; w[r][k] = 0.0; }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      s[k] = 0.0; num[k] = 0.0;
+#pragma unroll
+      for (int j = 0; j < K; ++j) S[k][j] = 0.0;
+    }
+  }
+
+  __device__ __forceinline__ void eliminate(const double (&X)[3][3], const double (&B)[3][3],
+                                            const double (&Y)[3][3], const double (&rhs)[3],
+                                            const double (&U0)[K], const double (&W)[K]) {
+    double M[3][3], Mi[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        M[r][q] = B[r][q] - (X[r][0] * c[q] + X[r][1] * c[3 + q] + X[r][2] * c[6 + q]);
+    inv3(M, Mi);
+    double wn[3][K];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        wn[r][k] = (r == 0 ? W[k] : 0.0) - (c[0 + r] * w[0][k] + c[3 + r] * w[1][k] + c[6 + r] * w[2][k]);
+    double tF[3], tU[3][K];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      tF[r] = rhs[r] - (X[r][0] * dF[0] + X[r][1] * dF[1] + X[r][2] * dF[2]);
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        tU[r][k] = (r == 0 ? U0[k] : 0.0) - (X[r][0] * dU[0][k] + X[r][1] * dU[1][k] + X[r][2] * dU[2][k]);
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      dF[r] = Mi[r][0] * tF[0] + Mi[r][1] * tF[1] + Mi[r][2] * tF[2];
+#pragma unroll
+      for (int k = 0; k < K; ++k) dU[r][k] = Mi[r][0] * tU[0][k] + Mi[r][1] * tU[1][k] + Mi[r][2] * tU[2][k];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        c[r * 3 + q] = Mi[r][0] * Y[0][q] + Mi[r][1] * Y[1][q] + Mi[r][2] * Y[2][q];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int k = 0; k < K; ++k) w[r][k] = wn[r][k];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      s[k] += w[0][k] * dF[0] + w[1][k] * dF[1] + w[2][k] * dF[2];
+#pragma unroll
+      for (int j = 0; j < K; ++j) S[k][j] += w[0][k] * dU[0][j] + w[1][k] * dU[1][j] + w[2][k] * dU[2][j];
+    }
+  }
+
+  __device__ __forceinline__ void store(const Lane& L, int i) const {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) *L.cd(i, j) = c[j];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) *L.cd(i, 9 + r) = dF[r];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int k = 0; k < K; ++k) *L.cd(i, 12 + r * K + k) = dU[r][k];
+  }
+
+  // half 1 hands its carry to half 0 at the meeting row
+  __device__ __forceinline__ void exchange(const Lane& L) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) c[j] = xchg(L, c[j]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      dF[r] = xchg(L, dF[r]);
+#pragma unroll
+      for (int k = 0; k < K; ++k) { dU[r][k] = xchg(L, dU[r][k]); w[r][k] = xchg(L, w[r][k]); }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      s[k] = xchg(L, s[k]); num[k] = xchg(L, num[k]);
+#pragma unroll
+      for (int j = 0; j < K; ++j) S[k][j] = xchg(L, S[k][j]);
+    }
+  }
+};
+
+// Newton's damping of one point (the caps and `density_steps`, solver.py:74-88), its new state
+// and its contribution to the step's size.
+__device__ __forceinline__ void damp(const Lane& L, const double (&x)[3], const Pt& old, Pt& nw,
+                                     double& size, bool& finite) {
+  const double sV = clipd(x[0], -CAP_V * L.Vt, CAP_V * L.Vt);
+  double sd[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const double yy = s == 0 ? old.lnn : old.lnp;
+    const double d = x[1 + s];
+    const bool below = yy < L.lognf;
+    const bool pos = d > -1.0;
+    double in_n = pos ? log1p(below ? d : 0.0) : -CAP_LN;
+    in_n = clipd(in_n, -FLOOR_DROP_CAP, CAP_LN);
+    sd[s] = below ? in_n : clipd(d, -CAP_LN, CAP_LN);
+  }
+  nw.V = old.V + sV; nw.lnn = old.lnn + sd[0]; nw.lnp = old.lnp + sd[1];
+  nw.n = exp(nw.lnn); nw.p = exp(nw.lnp);
+  size = nanmax(size, fabs(sV) * L.iVt);
+  size = nanmax(size, fabs(sd[0]) * (nw.n / (nw.n + L.nfloor)));
+  size = nanmax(size, fabs(sd[1]) * (nw.p / (nw.p + L.nfloor)));
+  finite = finite && isfinite(nw.V) && isfinite(nw.lnn) && isfinite(nw.lnp);
+}
+
 // ------------------------------------------------------------------------------------ current
 //
-// The terminal current (`_current_parts`, batch.py:316-403, steady state) is accumulated right
-// to left in the backward pass, over the new state. For each carrier (electrons sn = -1, holes
+// The terminal current (`_current_parts`, batch.py:316-403, steady state), accumulated over the
+// new state in the back substitution, half 0 right to left over its points 0..mid and intervals
+// 0..mid, half 1 left to right over mid+1..NP. For each carrier (electrons sn = -1, holes
 // sn = +1), with U_k = R_k + R_int,k - G_k g (0 on the contacts), q_k = exp(sn Vg_k / V_T)/mu_k,
-// c_k = (dx_{k-1} + dx_k)/2 and the trapezoids a_k = dx_k (U_k + U_{k+1})/2:
-//   single = sum_k c_k q_k,  double = sum_k c_k q_k int_u_k = A single - sum_k c_k q_k T_k,
-// T_k = sum_{e>=k} a_e the suffix sums (A = T_0), so no prefix sum is needed; and
-//   sum_e h_e J_e = qK H + sum_k b_k Hs_k - sum_{interfaces e} h_e (b_e - t_e),
-// b_k = sn q L h_k U_k, Hs_k = sum_{e>=k} h_e, t_e the current through interval e's traps
-// (an interface's J is the one before it plus t_e). The differential form sums each interval's
-// Scharfetter-Gummel flux, an interface again taking the interval before it plus t_e.
+// c_k = (dx_{k-1} + dx_k)/2 and the trapezoids a_k = dx_k (U_k + U_{k+1})/2, jaxdd's
+//   single = sum_k c_k q_k,   double = sum_k c_k q_k int_u_k,  int_u_k = sum_{e<k} a_e,
+//   sum_e h_e J_e = qK H + sum_{k>=1} b_k Hs_k - sum_{interfaces e} h_e (b_e - t_e),
+// with b_k = sn q L h_k U_k, Hs_k = sum_{e>=k} h_e and t_e the current through interval e's
+// traps (an interface's J is the one before it plus t_e), are rewritten with suffix sums
+// (double = A single - sum c q T, T_k = sum_{e>=k} a_e, A = T_0), so that each half needs only
+// its own partial sums and the other half's totals. The differential form sums the intervals'
+// Scharfetter-Gummel fluxes, an interface again taking the interval before it plus t_e.
+struct CurPart {
+  double single[2], cq[2], A[2], bH[2], Bs[2], corr[2];
+  double H, dtot;
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) { single[s] = cq[s] = A[s] = bH[s] = Bs[s] = corr[s] = 0.0; }
+    H = 0.0; dtot = 0.0;
+  }
+  __device__ __forceinline__ void exchange(const Lane& L) {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      single[s] = xchg(L, single[s]); cq[s] = xchg(L, cq[s]); A[s] = xchg(L, A[s]);
+      bH[s] = xchg(L, bH[s]); Bs[s] = xchg(L, Bs[s]); corr[s] = xchg(L, corr[s]);
+    }
+    H = xchg(L, H); dtot = xchg(L, dtot);
+  }
+};
+
+__device__ __forceinline__ double sg_flux(const Lane& L, int s, const Pt& a, const Pt& b,
+                                          double mu, double h) {
+  const double sn = s == 0 ? -1.0 : 1.0;
+  const double Vga = a.V + (s == 0 ? a.offn : a.offp);
+  const double Vgb = b.V + (s == 0 ? b.offn : b.offp);
+  double Bf, Bb, d1, d2;
+  bern_pair(sn * (Vgb - Vga) * L.iVt, L.simss, Bf, Bb, d1, d2);
+  const double da = s == 0 ? a.n : a.p, db = s == 0 ? b.n : b.p;
+  return sn * Q * mu * L.Vt * (db * Bb - da * Bf) / (L.L * h);
+}
 
 // ------------------------------------------------------------------------------------ Newton step
 
@@ -384,239 +686,153 @@ struct StepOut {
   bool finite;
 };
 
-// One Newton step of lane L at Vint (or, with `noise`, the round-off step of
-// `_noise_step`, solver.py:1728-1751, which leaves the state as it is).
+// One Newton step of a device, both threads of its pair (or, with `noise`, the round-off step
+// of `_noise_step`, solver.py:1728-1751, which leaves the state as it is). Returns the same
+// size, current and finiteness in both threads.
+//
+// Both halves run the same instructions in a mirrored frame: position p = 1 .. nown of a half
+// is node p (half 0) or node NP + 1 - p (half 1), p = 0 its contact, p = nown its boundary
+// point (mid, or mid + 1) and p = nown + 1 the other half's. Half 0 assembles the meeting row
+// mid at p = nown instead of eliminating it.
 template <int K>
 __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, double ratio,
                                bool noise) {
-  const int NP = L.NP;
-  const double Vt = L.Vt, iVt = L.iVt;
-  const double gfrac = L.gfrac;
-  // ---------------------------------------------------------------- forward
-  Pt pm, pc, pn;
-  contact(L, 0, Vint, pm);
-  pt_fill(L, pm, 0, logs);
-  load_state(L, 1, adv, ratio, pc);
-  pt_fill(L, pc, 1, logs);
-  Flux el;
-  double h_m = L.st(0, S_H);
-  flux(L, pm, pc, L.st(0, S_MUN), L.st(0, S_MUP), el);
-  double num[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) num[k] = 0.0;
-  ion_edge<K>(L, pm, pc, h_m * L.L, num);
-  int ifk_m = (int)L.st(0, S_IFK);
+  const int NP = L.NP, m = L.mid;
+  const bool top = L.half == 0;
+  const bool mir = !top;
+  const int nown = top ? m : NP - m;
+  // position -> node; the interval between positions p and p + 1 -> its physical index
+#define NODE(p) (top ? (p) : NP + 1 - (p))
+#define EDGE(p) (top ? (p) : NP - (p))
+  // the boundary points: each half loads its own (and makes its start there) and hands the
+  // state to the other
+  Pt pb, px;
+  load_state(L, NODE(nown), adv, ratio, pb);
+  px.V = xchg(L, pb.V); px.lnn = xchg(L, pb.lnn); px.lnp = xchg(L, pb.lnp);
+  pt_fill(L, pb, NODE(nown), logs);
+  pt_fill(L, px, NODE(nown + 1), logs);
 
-  double cp[9];
-  double dF[3], dU[3][K], wp[3][K];
-  double Sm[K][K], sv[K];
-#pragma unroll
-  for (int j = 0; j < 9; ++j) cp[j] = 0.0;
-#pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    dF[r] = 0.0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) { dU[r][k] = 0.0; wp[r][k] = 0.0; }
-  }
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    sv[k] = 0.0;
-#pragma unroll
-    for (int j = 0; j < K; ++j) Sm[k][j] = 0.0;
-  }
-
-  for (int i = 1; i <= NP; ++i) {
-    // the next point
-    if (i < NP) load_state(L, i + 1, adv, ratio, pn);
-    else contact(L, 1, Vint, pn);
-    pt_fill(L, pn, i + 1, logs);
-    const double h_i = L.st(i, S_H);
-    const int ifk_i = (int)L.st(i, S_IFK);
-    Flux er;
-    flux(L, pc, pn, L.st(i, S_MUN), L.st(i, S_MUP), er);
-    ion_edge<K>(L, pc, pn, h_i * L.L, num);
-
-    // row i
-    const double facl = L.st(i, S_FACL), facm = L.st(i, S_FACM), facu = L.st(i, S_FACU);
-    const double fac = L.st(i, S_FAC), sP = L.st(i, S_SP), sC = L.st(i, S_SC);
-    const double hm = h_m, hp = h_i;
-    double R, dRn, dRp;
-    recomb(L, i, pc.n, pc.p, R, dRn, dRp);
-    const double gen = L.st(i, S_G) * gfrac;
-    double elec = hm * er.Fn - hp * el.Fn + fac * (gen - R);
-    double hole = hp * el.Fp - hm * er.Fp + fac * (gen - R);
-    double pois = facl * pm.V + facm * pc.V + facu * pn.V -
-                  Q * (pc.n - pc.p + L.st(i, S_DOP) + L.afix(i) + pc.da - L.cfix(i) - pc.dc);
-    double A[3][3], Bm[3][3], Cm[3][3];
-    A[0][0] = facl * sP; A[0][1] = 0.0; A[0][2] = 0.0;
-    A[1][0] = -hp * el.n0V * sC; A[1][1] = -hp * el.n0n * sC; A[1][2] = 0.0;
-    A[2][0] = hp * el.p0V * sC;  A[2][1] = 0.0;               A[2][2] = hp * el.p0p * sC;
-    Bm[0][0] = (facm - Q * (pc.da + pc.dc) * iVt) * sP;
-    Bm[0][1] = -Q * pc.n * sP;
-    Bm[0][2] = Q * pc.p * sP;
-    Bm[1][0] = (-hp * el.n1V + hm * er.n0V) * sC;
-    Bm[1][1] = (-hp * el.n1n + hm * er.n0n - fac * dRn) * sC;
-    Bm[1][2] = (-fac * dRp) * sC;
-    Bm[2][0] = (hp * el.p1V - hm * er.p0V) * sC;
-    Bm[2][1] = (-fac * dRn) * sC;
-    Bm[2][2] = (hp * el.p1p - hm * er.p0p - fac * dRp) * sC;
-    Cm[0][0] = facu * sP; Cm[0][1] = 0.0; Cm[0][2] = 0.0;
-    Cm[1][0] = hm * er.n1V * sC; Cm[1][1] = hm * er.n1n * sC; Cm[1][2] = 0.0;
-    Cm[2][0] = -hm * er.p1V * sC; Cm[2][1] = 0.0; Cm[2][2] = -hm * er.p1p * sC;
-    if (ifk_m >= 0 || ifk_i >= 0) {
-      // interface traps on the left interval (this point its right end) and/or the right one
-      const double sc3[3] = {Q * sP, -fac * sC, -fac * sC};
-      double X[3] = {0.0, 0.0, 0.0};
-      Iface t;
-      if (ifk_m >= 0) {
-        iface_edge(L, ifk_m, pm.n, pc.n, pm.p, pc.p, t, true);
-        const int hi[3] = {4, 1, 3};
+  Carry<K> cr;
+  cr.zero();
+  double Am[3][3], Bmm[3][3], Cmm[3][3], rm[3], Um[K], Wm[K];
+  {
+    Pt pm, pc, pn;
+    contact(L, top ? 0 : 1, Vint, pm);
+    pt_fill(L, pm, NODE(0), logs);
+    if (nown == 1) pc = pb;
+    else { load_state(L, NODE(1), adv, ratio, pc); pt_fill(L, pc, NODE(1), logs); }
+    Flux el;
+    int e = EDGE(0);
+    double h_m = L.st(e, S_H);
+    flux(L, pm, pc, L.st(e, S_MUN), L.st(e, S_MUP), el);
+    ion_edge<K>(L, pm, pc, h_m * L.L, cr.num);
+    int ifk_m = (int)L.st(e, S_IFK);
+    for (int p = 1; p <= nown; ++p) {
+      if (p + 1 == nown) pn = pb;
+      else if (p == nown) pn = px;
+      else { load_state(L, NODE(p + 1), adv, ratio, pn); pt_fill(L, pn, NODE(p + 1), logs); }
+      e = EDGE(p);
+      const double h_i = L.st(e, S_H);
+      const int ifk_i = (int)L.st(e, S_IFK);
+      Flux er;
+      flux(L, pc, pn, L.st(e, S_MUN), L.st(e, S_MUP), er);
+      if (p < nown || top) ion_edge<K>(L, pc, pn, h_i * L.L, cr.num);  // interval mid is half 0's
+      double A[3][3], Bm[3][3], Cm[3][3], rhs[3], U0[K], W[K];
+      assemble_row<K>(L, NODE(p), pm, pc, pn, el, er, h_m, h_i, ifk_m, ifk_i, noise, mir, A, Bm,
+                      Cm, rhs, U0, W);
+      if (p < nown || !top) {
+        cr.eliminate(A, Bm, Cm, rhs, U0, W);
+        cr.store(L, NODE(p));
+      } else {
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
-          X[r] += t.v[hi[r]];
-          Bm[r][1] += sc3[r] * t.d[1][hi[r]];
-          Bm[r][2] += sc3[r] * t.d[3][hi[r]];
-          A[r][1] += sc3[r] * t.d[0][hi[r]];
-          A[r][2] += sc3[r] * t.d[2][hi[r]];
+          rm[r] = rhs[r];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) { Am[r][q] = A[r][q]; Bmm[r][q] = Bm[r][q]; Cmm[r][q] = Cm[r][q]; }
         }
+#pragma unroll
+        for (int k = 0; k < K; ++k) { Um[k] = U0[k]; Wm[k] = W[k]; }
       }
-      if (ifk_i >= 0) {
-        iface_edge(L, ifk_i, pc.n, pn.n, pc.p, pn.p, t, true);
-        const int lo[3] = {4, 0, 2};
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-          X[r] += t.v[lo[r]];
-          Bm[r][1] += sc3[r] * t.d[0][lo[r]];
-          Bm[r][2] += sc3[r] * t.d[2][lo[r]];
-          Cm[r][1] += sc3[r] * t.d[1][lo[r]];
-          Cm[r][2] += sc3[r] * t.d[3][lo[r]];
-        }
-      }
-      pois += Q * X[0];
-      elec -= fac * X[1];
-      hole -= fac * X[2];
+      pm = pc; pc = pn; el = er; h_m = h_i; ifk_m = ifk_i;
     }
-    double rhs[3];
-    double U0[K];
-    double W[K];
-    if (!noise) {
-      rhs[0] = -pois * sP; rhs[1] = -elec * sC; rhs[2] = -hole * sC;
-#pragma unroll
-      for (int k = 0; k < K; ++k) U0[k] = 0.0;
-      if (pc.sl.a >= 0) U0[pc.sl.a] = -Q * pc.da * sP;
-      if (pc.sl.c >= 0) U0[L.ka + pc.sl.c] = Q * pc.dc * sP;
-      ion_w<K>(L, pm, pc, pn, h_m * L.L, h_i * L.L, W);
-    } else {
-      // each row's round-off: eps sum |d row / d y| |y| over its three points
-      const double ym[3] = {fabs(pm.V), fabs(pm.lnn), fabs(pm.lnp)};
-      const double yc[3] = {fabs(pc.V), fabs(pc.lnn), fabs(pc.lnp)};
-      const double yn[3] = {fabs(pn.V), fabs(pn.lnn), fabs(pn.lnp)};
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        double s = 0.0;
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          s += fabs(A[r][c]) * ym[c] + fabs(Bm[r][c]) * yc[c] + fabs(Cm[r][c]) * yn[c];
-        rhs[r] = EPS64 * s;
-      }
-#pragma unroll
-      for (int k = 0; k < K; ++k) { U0[k] = 0.0; W[k] = 0.0; }
-    }
-    // elimination: M = B - A c'
-    double M[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        M[r][c] = Bm[r][c] - (A[r][0] * cp[c] + A[r][1] * cp[3 + c] + A[r][2] * cp[6 + c]);
-    const double co00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
-    const double co01 = M[0][2] * M[2][1] - M[0][1] * M[2][2];
-    const double co02 = M[0][1] * M[1][2] - M[0][2] * M[1][1];
-    const double co10 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
-    const double co11 = M[0][0] * M[2][2] - M[0][2] * M[2][0];
-    const double co12 = M[0][2] * M[1][0] - M[0][0] * M[1][2];
-    const double co20 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
-    const double co21 = M[0][1] * M[2][0] - M[0][0] * M[2][1];
-    const double co22 = M[0][0] * M[1][1] - M[0][1] * M[1][0];
-    const double idet = 1.0 / (M[0][0] * co00 + M[0][1] * co10 + M[0][2] * co20);
-    const double Mi[3][3] = {{co00 * idet, co01 * idet, co02 * idet},
-                             {co10 * idet, co11 * idet, co12 * idet},
-                             {co20 * idet, co21 * idet, co22 * idet}};
-    // w' = W e_0 - c'^T w'  (the previous c')
-    double wn[3][K];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-        wn[r][k] = (r == 0 ? W[k] : 0.0) -
-                   (cp[0 + r] * wp[0][k] + cp[3 + r] * wp[1][k] + cp[6 + r] * wp[2][k]);
-    // d' = M^-1 (rhs - A d')
-    double tF[3], tU[3][K];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      tF[r] = rhs[r] - (A[r][0] * dF[0] + A[r][1] * dF[1] + A[r][2] * dF[2]);
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-        tU[r][k] = (r == 0 ? U0[k] : 0.0) -
-                   (A[r][0] * dU[0][k] + A[r][1] * dU[1][k] + A[r][2] * dU[2][k]);
-    }
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      dF[r] = Mi[r][0] * tF[0] + Mi[r][1] * tF[1] + Mi[r][2] * tF[2];
-#pragma unroll
-      for (int k = 0; k < K; ++k) dU[r][k] = Mi[r][0] * tU[0][k] + Mi[r][1] * tU[1][k] + Mi[r][2] * tU[2][k];
-    }
-    // c' = M^-1 C
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        cp[r * 3 + c] = Mi[r][0] * Cm[0][c] + Mi[r][1] * Cm[1][c] + Mi[r][2] * Cm[2][c];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int k = 0; k < K; ++k) wp[r][k] = wn[r][k];
-    // the border's sums: sum w'^T d'
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      sv[k] += wp[0][k] * dF[0] + wp[1][k] * dF[1] + wp[2][k] * dF[2];
-#pragma unroll
-      for (int j = 0; j < K; ++j)
-        Sm[k][j] += wp[0][k] * dU[0][j] + wp[1][k] * dU[1][j] + wp[2][k] * dU[2][j];
-    }
-    // store c', d'
-#pragma unroll
-    for (int j = 0; j < 9; ++j) *L.cd(i, j) = cp[j];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) *L.cd(i, 9 + r) = dF[r];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int k = 0; k < K; ++k) *L.cd(i, 12 + r * K + k) = dU[r][k];
-    // shift
-    pm = pc; pc = pn; el = er; h_m = h_i; ifk_m = ifk_i;
   }
-
-  // ---------------------------------------------------------------- border (Schur)
-  double z[K];
+  // ---------------------------------------------------------------- the meeting row mid
+  Carry<K> other = cr;
+  other.exchange(L);  // half 0 now holds half 1's carry (a''_{mid+1}, d''_{mid+1}, ...)
+  double z[K], xm[3];
 #pragma unroll
   for (int k = 0; k < K; ++k) z[k] = 0.0;
-  if (!noise) {
-    double Msch[K][K], rr[K];
+  if (top) {
+    // gamma x_mid = [r | U]_mid - A d'_{mid-1} - C d''_{mid+1}, gamma = B - A c' - C a''
+    double G[3][3], Gi[3][3];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const double tk = L.total(k);
-      const bool has = tk > 0.0;
-      const double g = has ? num[k] / tk - 1.0 : 0.0;
-      const double Dk = has ? num[k] / tk : 1.0;  // d g / d log, or the held identity
+    for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int j = 0; j < K; ++j) Msch[k][j] = (j == k ? Dk : 0.0) - Sm[k][j];
-      rr[k] = -g - sv[k];
+      for (int q = 0; q < 3; ++q)
+        G[r][q] = Bmm[r][q] - (Am[r][0] * cr.c[q] + Am[r][1] * cr.c[3 + q] + Am[r][2] * cr.c[6 + q]) -
+                  (Cmm[r][0] * other.c[q] + Cmm[r][1] * other.c[3 + q] + Cmm[r][2] * other.c[6 + q]);
+    inv3(G, Gi);
+    double RF[3], RU[3][K];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      RF[r] = rm[r] - (Am[r][0] * cr.dF[0] + Am[r][1] * cr.dF[1] + Am[r][2] * cr.dF[2]) -
+              (Cmm[r][0] * other.dF[0] + Cmm[r][1] * other.dF[1] + Cmm[r][2] * other.dF[2]);
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        RU[r][k] = (r == 0 ? Um[k] : 0.0) -
+                   (Am[r][0] * cr.dU[0][k] + Am[r][1] * cr.dU[1][k] + Am[r][2] * cr.dU[2][k]) -
+                   (Cmm[r][0] * other.dU[0][k] + Cmm[r][1] * other.dU[1][k] + Cmm[r][2] * other.dU[2][k]);
     }
-    small_solve<K>(Msch, rr, z);
+    double XF[3], XU[3][K];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      XF[r] = Gi[r][0] * RF[0] + Gi[r][1] * RF[1] + Gi[r][2] * RF[2];
+#pragma unroll
+      for (int k = 0; k < K; ++k) XU[r][k] = Gi[r][0] * RU[0][k] + Gi[r][1] * RU[1][k] + Gi[r][2] * RU[2][k];
+    }
+    if (!noise) {
+      // W^T x = both halves' sums + (W_mid - c'^T w' - a''^T w'')^T x_mid
+      double wh[3][K];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          wh[r][k] = (r == 0 ? Wm[k] : 0.0) -
+                     (cr.c[0 + r] * cr.w[0][k] + cr.c[3 + r] * cr.w[1][k] + cr.c[6 + r] * cr.w[2][k]) -
+                     (other.c[0 + r] * other.w[0][k] + other.c[3 + r] * other.w[1][k] + other.c[6 + r] * other.w[2][k]);
+      double Msch[K][K], rr[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const double tk = L.total(k);
+        const bool has = tk > 0.0;
+        const double num = cr.num[k] + other.num[k];
+        const double g = has ? num / tk - 1.0 : 0.0;
+        const double Dk = has ? num / tk : 1.0;  // d g / d log, or the held identity
+        const double sF = cr.s[k] + other.s[k] + wh[0][k] * XF[0] + wh[1][k] * XF[1] + wh[2][k] * XF[2];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+          const double SU = cr.S[k][j] + other.S[k][j] +
+                            wh[0][k] * XU[0][j] + wh[1][k] * XU[1][j] + wh[2][k] * XU[2][j];
+          Msch[k][j] = (j == k ? Dk : 0.0) - SU;
+        }
+        rr[k] = -g - sF;
+      }
+      small_solve<K>(Msch, rr, z);
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double v = XF[r];
+#pragma unroll
+      for (int k = 0; k < K; ++k) v -= XU[r][k] * z[k];
+      xm[r] = v;
+    }
   }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) xm[r] = bcast(L, xm[r]);
+#pragma unroll
+  for (int k = 0; k < K; ++k) z[k] = bcast(L, z[k]);
 
-  // ---------------------------------------------------------------- backward
+  // ---------------------------------------------------------------- back substitution
   StepOut out;
   out.size = 0.0;
   out.finite = true;
@@ -625,176 +841,210 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       dlogs[k] = clipd(z[k], -ION_LOG_CAP, ION_LOG_CAP);
-      out.size = nanmax(out.size, fabs(dlogs[k]));
+      if (top) out.size = nanmax(out.size, fabs(dlogs[k]));
     }
   }
-  double xn[3] = {0.0, 0.0, 0.0};
-  const double capV = CAP_V * Vt;
-  const bool want_J = !noise;
   const double QL = Q * L.L;
-  // right-to-left current accumulators (see `Current` above), per carrier s (0 n, 1 p)
-  double single[2] = {0.0, 0.0}, cqT[2] = {0.0, 0.0}, Tsum[2] = {0.0, 0.0};
-  double bH[2] = {0.0, 0.0}, corr[2] = {0.0, 0.0};
-  double Hs = 0.0, dtot = 0.0;
-  // what the last iteration left for point i+1 (initially the right contact, point NP+1)
-  Pt pr;
-  contact(L, 1, Vint, pr);
-  pr.n = exp(pr.lnn); pr.p = exp(pr.lnp);
-  pr.offn = L.st(NP + 1, S_OFFN); pr.offp = L.st(NP + 1, S_OFFP);
-  double R_r = 0.0;                 // bulk recombination of point i+1
-  double Ri_r[2] = {0.0, 0.0};      // interface recombination of point i+1 (partial, then final)
-  double q_r[2] = {0.0, 0.0};       // exp(sn Vg / V_T) / mu of point i+1
-  double h_r = 0.0, dx_r = 0.0;     // interval i+1's h and dx
-  int ifk_r = -2;                   // interval i+1's S_IFK
-  double U_rr[2] = {0.0, 0.0};      // U of point i+2 (final)
-  double Ri_rr[2] = {0.0, 0.0};     // interface recombination of point i+2 (final)
-
-  for (int i = NP; i >= 0; --i) {
+  const double gfrac = L.gfrac;
+  CurPart cp;
+  cp.zero();
+  // Outward from the split: "q" is the point one position further in (new state). Half 0
+  // starts with point mid + 1 as half 1 finds it (the current on interval mid is half 0's);
+  // half 1 starts with none (interval mid is not its own).
+  Pt pq;
+  double R_q = 0.0, Ri_q[2] = {0.0, 0.0}, qv_q[2] = {0.0, 0.0}, h_q = 0.0, dx_q = 0.0;
+  int ifk_q = -2;
+  double U_qq[2] = {0.0, 0.0}, Ri_qq[2] = {0.0, 0.0}, b_q[2] = {0.0, 0.0};
+  double Jd1[2] = {0.0, 0.0}, Jd2[2] = {0.0, 0.0};  // half 1: J of the last two inner intervals
+  double A_run[2] = {0.0, 0.0}, H_run = 0.0;
+  double xn[3] = {xm[0], xm[1], xm[2]};
+  if (top && !noise) {
+    double x1[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double v = other.dF[r];
+#pragma unroll
+      for (int k = 0; k < K; ++k) v -= other.dU[r][k] * z[k];
+      x1[r] = v - (other.c[r * 3 + 0] * xm[0] + other.c[r * 3 + 1] * xm[1] + other.c[r * 3 + 2] * xm[2]);
+    }
+    double sz_dummy = 0.0;
+    bool fin_dummy = true;
+    damp(L, x1, px, pq, sz_dummy, fin_dummy);
+    pq.offn = px.offn; pq.offp = px.offp;
+    double R, d1, d2;
+    recomb(L, m + 1, pq.n, pq.p, R, d1, d2);
+    const double Ug = L.st(m + 1, S_G) * gfrac;
+    U_qq[0] = R - Ug; U_qq[1] = R - Ug;  // intervals mid, mid+1 hold no traps (the split's choice)
+  }
+  for (int p = nown; p >= 0; --p) {
+    const int i = NODE(p);
     Pt pi;
-    if (i >= 1) {
+    if (p >= 1) {
       double x[3];
+      if (p == nown && top) {
+        x[0] = xm[0]; x[1] = xm[1]; x[2] = xm[2];
+      } else {
 #pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        double v = *L.cd(i, 9 + r);
-        if (!noise) {
+        for (int r = 0; r < 3; ++r) {
+          double v = *L.cd(i, 9 + r);
+          if (!noise) {
 #pragma unroll
-          for (int k = 0; k < K; ++k) v -= *L.cd(i, 12 + r * K + k) * z[k];
+            for (int k = 0; k < K; ++k) v -= *L.cd(i, 12 + r * K + k) * z[k];
+          }
+          x[r] = v - (*L.cd(i, r * 3 + 0) * xn[0] + *L.cd(i, r * 3 + 1) * xn[1] + *L.cd(i, r * 3 + 2) * xn[2]);
         }
-        x[r] = v - (*L.cd(i, r * 3 + 0) * xn[0] + *L.cd(i, r * 3 + 1) * xn[1] +
-                    *L.cd(i, r * 3 + 2) * xn[2]);
       }
       xn[0] = x[0]; xn[1] = x[1]; xn[2] = x[2];
-      const double yV = *L.y(0, i, 0), yN = *L.y(0, i, 1), yP = *L.y(0, i, 2);
+      Pt old;
+      if (p == nown) old = pb;
+      else { old.V = *L.y(0, i, 0); old.lnn = *L.y(0, i, 1); old.lnp = *L.y(0, i, 2); }
       if (noise) {
-        const double en = exp(yN), ep = exp(yP);
-        out.size = nanmax(out.size, fabs(x[0]) * iVt);
+        const double en = exp(old.lnn), ep = exp(old.lnp);
+        out.size = nanmax(out.size, fabs(x[0]) * L.iVt);
         out.size = nanmax(out.size, fabs(x[1]) * (en / (en + L.nfloor)));
         out.size = nanmax(out.size, fabs(x[2]) * (ep / (ep + L.nfloor)));
         continue;
       }
-      // damping: the caps, and densities below n_floor stepped in n (`density_steps`)
-      const double sV = clipd(x[0], -capV, capV);
-      double sd[2];
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const double yy = s == 0 ? yN : yP;
-        const double d = x[1 + s];
-        const bool below = yy < L.lognf;
-        const bool pos = d > -1.0;
-        double in_n = pos ? log1p(below ? d : 0.0) : -CAP_LN;
-        in_n = clipd(in_n, -FLOOR_DROP_CAP, CAP_LN);
-        sd[s] = below ? in_n : clipd(d, -CAP_LN, CAP_LN);
-      }
-      pi.V = yV + sV; pi.lnn = yN + sd[0]; pi.lnp = yP + sd[1];
+      damp(L, x, old, pi, out.size, out.finite);
       *L.y(0, i, 0) = pi.V; *L.y(0, i, 1) = pi.lnn; *L.y(0, i, 2) = pi.lnp;
-      pi.n = exp(pi.lnn); pi.p = exp(pi.lnp);
-      out.size = nanmax(out.size, fabs(sV) * iVt);
-      out.size = nanmax(out.size, fabs(sd[0]) * (pi.n / (pi.n + L.nfloor)));
-      out.size = nanmax(out.size, fabs(sd[1]) * (pi.p / (pi.p + L.nfloor)));
-      out.finite = out.finite && isfinite(pi.V) && isfinite(pi.lnn) && isfinite(pi.lnp);
     } else {
       if (noise) break;
-      contact(L, 0, Vint, pi);
+      contact(L, top ? 0 : 1, Vint, pi);
       pi.n = exp(pi.lnn); pi.p = exp(pi.lnp);
     }
     pi.offn = L.st(i, S_OFFN); pi.offp = L.st(i, S_OFFP);
-    // interval i (points i, i+1, both new): its traps' recombination at either end
-    const double h_i = L.st(i, S_H), dx_i = L.st(i, S_DX);
-    const int ifk_i = (int)L.st(i, S_IFK);
+    // the interval between this point and the one further in (not half 1's at its boundary)
+    const bool own_in = top || p < nown;
+    const int ein = EDGE(p);
+    const double h_in = L.st(ein, S_H), dx_in = L.st(ein, S_DX);
+    const int ifk_in = (int)L.st(ein, S_IFK);
     double Ri_i[2] = {0.0, 0.0};
-    if (ifk_i >= 0) {
+    if (own_in && ifk_in >= 0) {
       Iface t;
-      iface_edge(L, ifk_i, pi.n, pr.n, pi.p, pr.p, t, false);
-      Ri_i[0] = t.v[0]; Ri_i[1] = t.v[2];
-      Ri_r[0] += t.v[1]; Ri_r[1] += t.v[3];
+      if (top) iface_edge(L, ifk_in, pi.n, pq.n, pi.p, pq.p, t, false);
+      else iface_edge(L, ifk_in, pq.n, pi.n, pq.p, pi.p, t, false);
+      const double in_n = top ? t.v[1] : t.v[0], in_p = top ? t.v[3] : t.v[2];
+      const double me_n = top ? t.v[0] : t.v[1], me_p = top ? t.v[2] : t.v[3];
+      Ri_i[0] = me_n; Ri_i[1] = me_p;
+      Ri_q[0] += in_n; Ri_q[1] += in_p;
     }
-    // the differential form: interval i's flux; an interface takes the interval before it
     double Jd[2] = {0.0, 0.0};
-    if (L.currdiff) {
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const double sn = s == 0 ? -1.0 : 1.0;
-        const double Vga = pi.V + (s == 0 ? pi.offn : pi.offp);
-        const double Vgb = pr.V + (s == 0 ? pr.offn : pr.offp);
-        double Bf, Bb, d1, d2;
-        bern_pair(sn * (Vgb - Vga) * iVt, L.simss, Bf, Bb, d1, d2);
-        const double da = s == 0 ? pi.n : pi.p, db = s == 0 ? pr.n : pr.p;
-        const double mu = L.st(i, s == 0 ? S_MUN : S_MUP);
-        Jd[s] = sn * Q * mu * Vt * (db * Bb - da * Bf) / (L.L * h_i);
-      }
-      if (ifk_i < -1) dtot += h_i * (Jd[0] + Jd[1]);
+    if (L.currdiff && own_in) {
+      const Pt& a = top ? pi : pq;
+      const Pt& b = top ? pq : pi;
+      Jd[0] = sg_flux(L, 0, a, b, L.st(ein, S_MUN), h_in);
+      Jd[1] = sg_flux(L, 1, a, b, L.st(ein, S_MUP), h_in);
+      if (ifk_in < -1) cp.dtot += h_in * (Jd[0] + Jd[1]);
     }
-    // point i+1 is final: finalise it (left interval i, right interval i+1)
-    if (i + 1 <= NP) {
-      const double Ug = L.st(i + 1, S_G) * gfrac;
-      const double ck = 0.5 * (dx_i + dx_r);
-      Hs += h_r;
+    // the point further in is final now: its U, the trapezoid of its inner interval, its sums
+    if (p < nown) {
+      const int k = NODE(p + 1);
+      const double Ug = L.st(k, S_G) * gfrac;
+      const double ck = 0.5 * (dx_in + dx_q);
+      const bool inner_own = top || p + 1 < nown;  // half 1's boundary point: its inner interval is mid
+      if (inner_own) H_run += h_q;
+      const double hk = L.st(k, S_H);  // b_k takes the width of interval k
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         const double sn = s == 0 ? -1.0 : 1.0;
-        const double Uk = R_r + Ri_r[s] - Ug;
-        Tsum[s] += 0.5 * dx_r * (Uk + U_rr[s]);
-        single[s] += ck * q_r[s];
-        cqT[s] += ck * q_r[s] * Tsum[s];
-        const double bk = sn * QL * h_r * Uk;
-        bH[s] += bk * Hs;
-        if (ifk_r >= -1) {
-          const double tk = sn * 0.5 * QL * h_r * (Ri_r[s] + Ri_rr[s]);
-          corr[s] += h_r * (bk - tk);
-          if (L.currdiff) dtot += h_r * (Jd[s] + tk);
+        const double Uk = R_q + Ri_q[s] - Ug;
+        if (inner_own) A_run[s] += 0.5 * dx_q * (Uk + U_qq[s]);
+        cp.single[s] += ck * qv_q[s];
+        cp.cq[s] += ck * qv_q[s] * A_run[s];
+        const double bk = sn * QL * hk * Uk;
+        cp.bH[s] += bk * H_run;
+        cp.Bs[s] += bk;
+        if (inner_own && ifk_q >= -1) {
+          // the inner interval is a layer interface: the current through its traps, the
+          // interval's physical left point's b (this point in half 0, the inner one in half 1)
+          const double tk = sn * 0.5 * QL * h_q * (Ri_q[s] + Ri_qq[s]);
+          cp.corr[s] += h_q * ((top ? bk : b_q[s]) - tk);
+          if (L.currdiff) cp.dtot += h_q * ((top ? Jd[s] : Jd2[s]) + tk);
         }
-        U_rr[s] = Uk;
-        Ri_rr[s] = Ri_r[s];
+        U_qq[s] = Uk;
+        b_q[s] = bk;
       }
+      Ri_qq[0] = Ri_q[0]; Ri_qq[1] = Ri_q[1];
     }
-    // point i becomes "point i+1" of the next iteration
-    if (i >= 1) {
+    if (!top && L.currdiff) {  // half 1 keeps the J of the intervals inside this point's
+      Jd2[0] = Jd1[0]; Jd2[1] = Jd1[1];
+      Jd1[0] = Jd[0]; Jd1[1] = Jd[1];
+    }
+    if (p >= 1) {
       double R, d1, d2;
       recomb(L, i, pi.n, pi.p, R, d1, d2);
-      R_r = R;
+      R_q = R;
     } else {
-      R_r = 0.0;
+      R_q = 0.0;
     }
-    q_r[0] = exp(-(pi.V + pi.offn) * iVt) / L.st(i, S_MUN);
-    q_r[1] = exp((pi.V + pi.offp) * iVt) / L.st(i, S_MUP);
-    Ri_r[0] = Ri_i[0]; Ri_r[1] = Ri_i[1];
-    h_r = h_i; dx_r = dx_i; ifk_r = ifk_i;
-    pr = pi;
+    qv_q[0] = exp(-(pi.V + pi.offn) * L.iVt) / L.st(i, S_MUN);
+    qv_q[1] = exp((pi.V + pi.offp) * L.iVt) / L.st(i, S_MUP);
+    Ri_q[0] = Ri_i[0]; Ri_q[1] = Ri_i[1];
+    h_q = h_in; dx_q = dx_in; ifk_q = ifk_in;
+    pq = pi;
   }
-  if (want_J) {
-    // point 0, the left contact: U = 0, no width term
-    const double ck = 0.5 * dx_r;
+  if (!noise) {
+    // the contact: its inner interval (half 0: interval 0; half 1: interval NP, dx = 0); the
+    // left contact counts in the current's sums, the right one does not (q_k for k <= NP)
+    const double ck = 0.5 * dx_q;
+    H_run += h_q;
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-      Tsum[s] += 0.5 * dx_r * (0.0 + U_rr[s]);
-      single[s] += ck * q_r[s];
-      cqT[s] += ck * q_r[s] * Tsum[s];
-    }
-    const double H = L.Hsum;
-    double tot = 0.0;
-    if (!L.currdiff) {
-      Pt c0, cN;
-      contact(L, 0, Vint, c0);
-      contact(L, 1, Vint, cN);
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const double sn = s == 0 ? -1.0 : 1.0;
-        const double dbl = Tsum[s] * single[s] - cqT[s];
-        const double off0 = L.st(0, s == 0 ? S_OFFN : S_OFFP);
-        const double offN = L.st(NP + 1, s == 0 ? S_OFFN : S_OFFP);
-        const double d0 = exp(s == 0 ? c0.lnn : c0.lnp), dN = exp(s == 0 ? cN.lnn : cN.lnp);
-        const double Kc = (Vt * (sn * dN * exp(sn * (cN.V + offN) * iVt) -
-                                 sn * d0 * exp(sn * (c0.V + off0) * iVt)) -
-                           sn * dbl) / single[s];
-        tot += Q * Kc * H + bH[s] - corr[s];
+      A_run[s] += 0.5 * dx_q * (0.0 + U_qq[s]);
+      if (top) {
+        cp.single[s] += ck * qv_q[s];
+        cp.cq[s] += ck * qv_q[s] * A_run[s];
       }
-    } else {
-      tot = dtot;
+      cp.A[s] = A_run[s];
     }
-    out.J = -L.left * tot / H;
-  } else {
-    out.J = 0.0;
+    cp.H = H_run;
   }
+#undef NODE
+#undef EDGE
+  // ---------------------------------------------------------------- combine the halves
+  const double osize = xchg(L, out.size);
+  const int ofin = xchgi(L, out.finite ? 1 : 0);
+  CurPart ot = cp;
+  ot.exchange(L);
+  if (top) {
+    out.size = nanmax(out.size, osize);
+    out.finite = out.finite && ofin;
+    if (!noise) {
+      const double H = L.Hsum;
+      double tot = 0.0;
+      if (!L.currdiff) {
+        // half 0's suffix sums lack half 1's totals A_B and H_B; half 1's prefix sums are
+        // subtracted from its totals
+        Pt c0, cN;
+        contact(L, 0, Vint, c0);
+        contact(L, 1, Vint, cN);
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+          const double sn = s == 0 ? -1.0 : 1.0;
+          const double single = cp.single[s] + ot.single[s];
+          const double A = cp.A[s] + ot.A[s];
+          const double cqT = cp.cq[s] + cp.single[s] * ot.A[s] + (ot.A[s] * ot.single[s] - ot.cq[s]);
+          const double bH = cp.bH[s] + cp.Bs[s] * ot.H + (ot.H * ot.Bs[s] - ot.bH[s]);
+          const double dbl = A * single - cqT;
+          const double off0 = L.st(0, s == 0 ? S_OFFN : S_OFFP);
+          const double offN = L.st(NP + 1, s == 0 ? S_OFFN : S_OFFP);
+          const double d0 = exp(s == 0 ? c0.lnn : c0.lnp), dN = exp(s == 0 ? cN.lnn : cN.lnp);
+          const double Kc = (L.Vt * (sn * dN * exp(sn * (cN.V + offN) * L.iVt) -
+                                     sn * d0 * exp(sn * (c0.V + off0) * L.iVt)) -
+                             sn * dbl) / single;
+          tot += Q * Kc * H + bH - (cp.corr[s] + ot.corr[s]);
+        }
+      } else {
+        tot = cp.dtot + ot.dtot;
+      }
+      out.J = -L.left * tot / H;
+    } else {
+      out.J = 0.0;
+    }
+  }
+  out.size = bcast(L, out.size);
+  out.J = bcast(L, out.J);
+  out.finite = bcasti(L, out.finite ? 1 : 0) != 0;
   if (!noise) {
 #pragma unroll
     for (int k = 0; k < K; ++k) logs[k] += dlogs[k];
@@ -812,152 +1062,258 @@ __device__ __forceinline__ void pt_ions(const Lane& L, Pt& P, int k, const doubl
   P.dc = P.sl.c >= 0 ? exp(logs[L.ka + P.sl.c] - P.V * L.iVt) : 0.0;
 }
 
-// The normalisations that put each slot's ions into its region at the potential of the
-// iterate (`_ion_logs`, solver.py:1695-1725, Boltzmann ions: closed form).
+__device__ __forceinline__ void own_range(const Lane& L, int& lo, int& hi) {
+  if (L.half == 0) { lo = 1; hi = L.mid; }
+  else { lo = L.mid + 1; hi = L.NP; }
+}
+
+// The normalisations that put each slot's ions into its region at the iterate's potential
+// (`_ion_logs`, solver.py:1695-1725, Boltzmann ions: closed form). Each half sums its own
+// intervals (half 0: 0..mid, half 1: mid+1..NP); both end with half 0's result.
 template <int K>
 __device__ void ion_logs(const Lane& L, double Vint, double* logs) {
   double zero[K], num[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) { zero[k] = 0.0; num[k] = 0.0; }
+  const int m = L.mid;
+  const double vb = *L.y(0, L.half == 0 ? m : m + 1, 0);
+  const double vx = xchg(L, vb);
   Pt a, b;
-  contact(L, 0, Vint, a);
-  pt_ions(L, a, 0, zero);
-  for (int e = 0; e <= L.NP; ++e) {
-    if (e + 1 <= L.NP) b.V = *L.y(0, e + 1, 0);
-    else contact(L, 1, Vint, b);
+  int e0, e1;
+  if (L.half == 0) { e0 = 0; e1 = m; contact(L, 0, Vint, a); }
+  else { e0 = m + 1; e1 = L.NP; a.V = vb; }
+  pt_ions(L, a, e0, zero);
+  for (int e = e0; e <= e1; ++e) {
+    if (e + 1 == L.NP + 1) contact(L, 1, Vint, b);
+    else if (e + 1 == m + 1 && L.half == 0) b.V = vx;
+    else b.V = *L.y(0, e + 1, 0);
     pt_ions(L, b, e + 1, zero);
     ion_edge<K>(L, a, b, L.st(e, S_H) * L.L, num);
     a = b;
   }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
+    const double tot = num[k] + xchg(L, num[k]);
     const double tk = L.total(k);
-    logs[k] = tk > 0.0 ? log(tk / num[k]) : 0.0;
+    logs[k] = bcast(L, tk > 0.0 ? log(tk / tot) : 0.0);
   }
 }
 
 // One Newton step of Poisson's equation alone, the densities following the potential and the
 // ions re-fitted to it (`_poisson_delta`, solver.py:1757-1800; `_poisson_solve`,
-// batch.py:486-503): a scalar tridiagonal system bordered by the slots, solved with the same
-// forward-carried border as the Newton step. Without mobile ions each point's step is clipped
-// to 10 V_T; with them the step is scaled as a whole (its largest entry m to V_T ln(1 + m/V_T)).
-// Returns max |dV| / V_T of the step taken.
+// batch.py:486-503): a scalar tridiagonal system bordered by the slots, solved as the Newton
+// step is (twisted, the border carried along both halves). Without mobile ions each point's step
+// is clipped to 10 V_T; with them the step is scaled as a whole (its largest entry m to
+// V_T ln(1 + m/V_T)). Returns max |dV| / V_T of the step taken (the same in both threads).
 template <int K>
 __device__ double poisson_step(Lane& L, double Vint, bool coupled, double* logs) {
-  const int NP = L.NP;
+  const int NP = L.NP, m = L.mid;
   const double iVt = L.iVt;
+  const bool top = L.half == 0;
   ion_logs<K>(L, Vint, logs);
   bool mobile = false;
 #pragma unroll
   for (int k = 0; k < K; ++k) mobile = mobile || L.total(k) > 0.0;
   mobile = mobile && coupled;
-  Pt pm, pc, pn;
-  contact(L, 0, Vint, pm);
-  pt_ions(L, pm, 0, logs);
-  pc.V = *L.y(0, 1, 0); pc.lnn = *L.y(0, 1, 1); pc.lnp = *L.y(0, 1, 2);
-  pt_ions(L, pc, 1, logs);
-  double num[K], wp[K], dU[K], Sm[K][K], sv[K];
+  Pt pb, px;
+  const int kb = top ? m : m + 1, kx = top ? m + 1 : m;
+  pb.V = *L.y(0, kb, 0); pb.lnn = *L.y(0, kb, 1); pb.lnp = *L.y(0, kb, 2);
+  px.V = xchg(L, pb.V); px.lnn = xchg(L, pb.lnn); px.lnp = xchg(L, pb.lnp);
+  pt_ions(L, pb, kb, logs);
+  pt_ions(L, px, kx, logs);
+  double num[K], w[K], dU[K], Sm[K][K], sv[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    num[k] = 0.0; wp[k] = 0.0; dU[k] = 0.0; sv[k] = 0.0;
+    num[k] = 0.0; w[k] = 0.0; dU[k] = 0.0; sv[k] = 0.0;
 #pragma unroll
     for (int j = 0; j < K; ++j) Sm[k][j] = 0.0;
   }
-  double h_m = L.st(0, S_H);
-  ion_edge<K>(L, pm, pc, h_m * L.L, num);
-  double cprev = 0.0, dF = 0.0;
-  for (int i = 1; i <= NP; ++i) {
-    if (i < NP) { pn.V = *L.y(0, i + 1, 0); pn.lnn = *L.y(0, i + 1, 1); pn.lnp = *L.y(0, i + 1, 2); }
-    else contact(L, 1, Vint, pn);
-    pt_ions(L, pn, i + 1, logs);
-    const double h_i = L.st(i, S_H);
-    ion_edge<K>(L, pc, pn, h_i * L.L, num);
+  double c = 0.0, dF = 0.0;
+  // row m (half 0 assembles it, the meeting row)
+  double lo_m = 0.0, mid_m = 1.0, up_m = 0.0, F_m = 0.0, U_m[K], W_m[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) { U_m[k] = 0.0; W_m[k] = 0.0; }
+  // one row: its coefficients and right-hand sides
+  auto row = [&](int i, const Pt& pm, const Pt& pc, const Pt& pn, double hm, double hp,
+                 double& lo, double& mid, double& up, double& F, double (&U)[K], double (&W)[K]) {
     const double facl = L.st(i, S_FACL), facm = L.st(i, S_FACM), facu = L.st(i, S_FACU);
     const double sP = L.st(i, S_SP);
     const double n = exp(pc.lnn), p = exp(pc.lnp);
-    const double F = (facl * pm.V + facm * pc.V + facu * pn.V -
-                      Q * (n - p + L.st(i, S_DOP) + L.afix(i) + pc.da - L.cfix(i) - pc.dc)) * sP;
-    const double mid = (facm - Q * (n + p) * iVt - Q * (pc.da + pc.dc) * iVt) * sP;
-    const double lo = i > 1 ? facl * sP : 0.0;
-    const double up = i < NP ? facu * sP : 0.0;
-    double U[K], W[K];
+    F = (facl * pm.V + facm * pc.V + facu * pn.V -
+         Q * (n - p + L.st(i, S_DOP) + L.afix(i) + pc.da - L.cfix(i) - pc.dc)) * sP;
+    mid = (facm - Q * (n + p) * iVt - Q * (pc.da + pc.dc) * iVt) * sP;
+    lo = i > 1 ? facl * sP : 0.0;
+    up = i < NP ? facu * sP : 0.0;
 #pragma unroll
     for (int k = 0; k < K; ++k) U[k] = 0.0;
     if (pc.sl.a >= 0) U[pc.sl.a] = -Q * pc.da * sP;
     if (pc.sl.c >= 0) U[L.ka + pc.sl.c] = Q * pc.dc * sP;
-    ion_w<K>(L, pm, pc, pn, h_m * L.L, h_i * L.L, W);
-    const double im = 1.0 / (mid - lo * cprev);
+    ion_w<K>(L, pm, pc, pn, hm * L.L, hp * L.L, W);
+  };
+  // X couples to the eliminated side, Y to the rest
+  auto eliminate = [&](double X, double mid, double Y, double F, const double (&U)[K],
+                       const double (&W)[K]) {
+    const double im = 1.0 / (mid - X * c);
 #pragma unroll
-    for (int k = 0; k < K; ++k) wp[k] = W[k] - cprev * wp[k];
-    dF = (-F - lo * dF) * im;
+    for (int k = 0; k < K; ++k) w[k] = W[k] - c * w[k];
+    dF = (-F - X * dF) * im;
 #pragma unroll
-    for (int k = 0; k < K; ++k) dU[k] = (U[k] - lo * dU[k]) * im;
-    cprev = up * im;
+    for (int k = 0; k < K; ++k) dU[k] = (U[k] - X * dU[k]) * im;
+    c = Y * im;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      sv[k] += wp[k] * dF;
+      sv[k] += w[k] * dF;
 #pragma unroll
-      for (int j = 0; j < K; ++j) Sm[k][j] += wp[k] * dU[j];
+      for (int j = 0; j < K; ++j) Sm[k][j] += w[k] * dU[j];
     }
-    *L.cd(i, 0) = cprev;
+  };
+  auto store = [&](int i) {
+    *L.cd(i, 0) = c;
     *L.cd(i, 1) = dF;
 #pragma unroll
     for (int k = 0; k < K; ++k) *L.cd(i, 2 + k) = dU[k];
-    pm = pc; pc = pn; h_m = h_i;
+  };
+  if (top) {
+    Pt pm, pc, pn;
+    contact(L, 0, Vint, pm);
+    pt_ions(L, pm, 0, logs);
+    if (m == 1) pc = pb;
+    else { pc.V = *L.y(0, 1, 0); pc.lnn = *L.y(0, 1, 1); pc.lnp = *L.y(0, 1, 2); pt_ions(L, pc, 1, logs); }
+    double h_m = L.st(0, S_H);
+    ion_edge<K>(L, pm, pc, h_m * L.L, num);
+    for (int i = 1; i <= m; ++i) {
+      if (i + 1 == m) pn = pb;
+      else if (i == m) pn = px;
+      else { pn.V = *L.y(0, i + 1, 0); pn.lnn = *L.y(0, i + 1, 1); pn.lnp = *L.y(0, i + 1, 2); pt_ions(L, pn, i + 1, logs); }
+      const double h_i = L.st(i, S_H);
+      ion_edge<K>(L, pc, pn, h_i * L.L, num);
+      double lo, mid, up, F, U[K], W[K];
+      row(i, pm, pc, pn, h_m, h_i, lo, mid, up, F, U, W);
+      if (i < m) { eliminate(lo, mid, up, F, U, W); store(i); }
+      else {
+        lo_m = lo; mid_m = mid; up_m = up; F_m = F;
+#pragma unroll
+        for (int k = 0; k < K; ++k) { U_m[k] = U[k]; W_m[k] = W[k]; }
+      }
+      pm = pc; pc = pn; h_m = h_i;
+    }
+  } else {
+    Pt pl, pc, pn;
+    contact(L, 1, Vint, pn);
+    pt_ions(L, pn, NP + 1, logs);
+    if (NP == m + 1) pc = pb;
+    else { pc.V = *L.y(0, NP, 0); pc.lnn = *L.y(0, NP, 1); pc.lnp = *L.y(0, NP, 2); pt_ions(L, pc, NP, logs); }
+    double h_i = L.st(NP, S_H);
+    ion_edge<K>(L, pc, pn, h_i * L.L, num);
+    for (int i = NP; i >= m + 1; --i) {
+      if (i - 1 == m) pl = px;
+      else if (i - 1 == m + 1) pl = pb;
+      else { pl.V = *L.y(0, i - 1, 0); pl.lnn = *L.y(0, i - 1, 1); pl.lnp = *L.y(0, i - 1, 2); pt_ions(L, pl, i - 1, logs); }
+      const double h_m = L.st(i - 1, S_H);
+      if (i - 1 >= m + 1) ion_edge<K>(L, pl, pc, h_m * L.L, num);
+      double lo, mid, up, F, U[K], W[K];
+      row(i, pl, pc, pn, h_m, h_i, lo, mid, up, F, U, W);
+      eliminate(up, mid, lo, F, U, W);
+      store(i);
+      pn = pc; pc = pl; h_i = h_m;
+    }
   }
-  double z[K];
+  // the meeting row
+  const double c2 = xchg(L, c), dF2 = xchg(L, dF);
+  double dU2[K], w2[K], S2[K][K], s2[K], num2[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    dU2[k] = xchg(L, dU[k]); w2[k] = xchg(L, w[k]); s2[k] = xchg(L, sv[k]); num2[k] = xchg(L, num[k]);
+#pragma unroll
+    for (int j = 0; j < K; ++j) S2[k][j] = xchg(L, Sm[k][j]);
+  }
+  double z[K], xm = 0.0;
 #pragma unroll
   for (int k = 0; k < K; ++k) z[k] = 0.0;
-  if (mobile) {
-    double Msch[K][K], rr[K];
+  if (top) {
+    const double ig = 1.0 / (mid_m - lo_m * c - up_m * c2);
+    const double XF = (-F_m - lo_m * dF - up_m * dF2) * ig;
+    double XU[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const double tk = L.total(k);
-      const bool has = tk > 0.0;
-      const double g = has ? num[k] / tk - 1.0 : 0.0;
-      const double Dk = has ? num[k] / tk : 1.0;
+    for (int k = 0; k < K; ++k) XU[k] = (U_m[k] - lo_m * dU[k] - up_m * dU2[k]) * ig;
+    if (mobile) {
+      double Msch[K][K], rr[K];
 #pragma unroll
-      for (int j = 0; j < K; ++j) Msch[k][j] = (j == k ? Dk : 0.0) - Sm[k][j];
-      rr[k] = -g - sv[k];
+      for (int k = 0; k < K; ++k) {
+        const double wh = W_m[k] - c * w[k] - c2 * w2[k];
+        const double tk = L.total(k);
+        const bool has = tk > 0.0;
+        const double nm = num[k] + num2[k];
+        const double g = has ? nm / tk - 1.0 : 0.0;
+        const double Dk = has ? nm / tk : 1.0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) Msch[k][j] = (j == k ? Dk : 0.0) - (Sm[k][j] + S2[k][j] + wh * XU[j]);
+        rr[k] = -g - (sv[k] + s2[k] + wh * XF);
+      }
+      small_solve<K>(Msch, rr, z);
     }
-    small_solve<K>(Msch, rr, z);
-  }
-  const double capV = CAP_V * L.Vt;
-  double x = 0.0, m = 0.0, size = 0.0;
-  for (int i = NP; i >= 1; --i) {
-    double v = *L.cd(i, 1);
+    xm = XF;
 #pragma unroll
-    for (int k = 0; k < K; ++k) v -= *L.cd(i, 2 + k) * z[k];
-    x = v - *L.cd(i, 0) * x;
+    for (int k = 0; k < K; ++k) xm -= XU[k] * z[k];
+  }
+  xm = bcast(L, xm);
+#pragma unroll
+  for (int k = 0; k < K; ++k) z[k] = bcast(L, z[k]);
+  const double capV = CAP_V * L.Vt;
+  double mx = 0.0, size = 0.0;
+  auto apply = [&](int i, double dV) {
+    *L.y(0, i, 0) += dV;
+    *L.y(0, i, 1) += dV * iVt;
+    *L.y(0, i, 2) -= dV * iVt;
+    size = nanmax(size, fabs(dV * iVt));
+  };
+  auto visit = [&](int i, double x) {
     if (mobile) {
       *L.cd(i, 1) = x;
-      m = nanmax(m, fabs(x) * iVt);
+      mx = nanmax(mx, fabs(x) * iVt);
     } else {
-      const double dV = clipd(x, -capV, capV);
-      *L.y(0, i, 0) += dV;
-      *L.y(0, i, 1) += dV * iVt;
-      *L.y(0, i, 2) -= dV * iVt;
-      size = nanmax(size, fabs(dV * iVt));
+      apply(i, clipd(x, -capV, capV));
+    }
+  };
+  if (top) {
+    double x = xm;
+    visit(m, x);
+    for (int i = m - 1; i >= 1; --i) {
+      double v = *L.cd(i, 1);
+#pragma unroll
+      for (int k = 0; k < K; ++k) v -= *L.cd(i, 2 + k) * z[k];
+      x = v - *L.cd(i, 0) * x;
+      visit(i, x);
+    }
+  } else {
+    double x = xm;
+    for (int i = m + 1; i <= NP; ++i) {
+      double v = *L.cd(i, 1);
+#pragma unroll
+      for (int k = 0; k < K; ++k) v -= *L.cd(i, 2 + k) * z[k];
+      x = v - *L.cd(i, 0) * x;
+      visit(i, x);
     }
   }
   if (mobile) {
-    const double f = m > 0.0 ? fmin(log1p(m), CAP_V) / m : 1.0;
-    for (int i = 1; i <= NP; ++i) {
-      const double dV = *L.cd(i, 1) * f;
-      *L.y(0, i, 0) += dV;
-      *L.y(0, i, 1) += dV * iVt;
-      *L.y(0, i, 2) -= dV * iVt;
-      size = nanmax(size, fabs(dV * iVt));
-    }
+    mx = nanmax(mx, xchg(L, mx));
+    mx = bcast(L, mx);
+    const double f = mx > 0.0 ? fmin(log1p(mx), CAP_V) / mx : 1.0;
+    int lo, hi;
+    own_range(L, lo, hi);
+    for (int i = lo; i <= hi; ++i) apply(i, *L.cd(i, 1) * f);
   }
-  return size;
+  size = nanmax(size, xchg(L, size));
+  return bcast(L, size);
 }
 
 // The mobile ions of the iterate as fixed densities, no longer solved for (`_freeze`,
-// batch.py:859-872).
+// batch.py:859-872). Each half its own points.
 template <int K>
 __device__ void freeze(Lane& L, const double* logs) {
-  for (int i = 1; i <= L.NP; ++i) {
+  int lo, hi;
+  own_range(L, lo, hi);
+  for (int i = lo; i <= hi; ++i) {
     Pt P;
     P.V = *L.y(0, i, 0);
     pt_ions(L, P, i, logs);
@@ -968,7 +1324,9 @@ __device__ void freeze(Lane& L, const double* logs) {
 }
 
 __device__ void copy_state(const Lane& L, int dst, int src) {
-  for (int i = 1; i <= L.NP; ++i)
+  int lo, hi;
+  own_range(L, lo, hi);
+  for (int i = lo; i <= hi; ++i)
 #pragma unroll
     for (int c = 0; c < 3; ++c) *L.y(dst, i, c) = *L.y(src, i, c);
 }
@@ -1018,7 +1376,7 @@ struct Args {
 };
 
 template <int K>
-__device__ void lane_init(Lane& L, const Args& a, int l) {
+__device__ void lane_init(Lane& L, const Args& a, int l, int half) {
   L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l;
   L.ka = a.ka; L.K = K;
   L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L);
@@ -1027,6 +1385,7 @@ __device__ void lane_init(Lane& L, const Args& a, int l) {
   L.Jscale = L.sc(C_JSCALE); L.Gshunt = L.sc(C_GSHUNT); L.gfrac = L.sc(C_GFRAC);
   L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor); L.Hsum = L.sc(C_HSUM);
   L.NP = (int)L.sc(C_NP);
+  L.mid = (int)L.sc(C_MID);
   L.currdiff = L.sc(C_CURRDIFF) > 0.0; L.simss = a.simss;
 #pragma unroll
   for (int k = 0; k < K; ++k) L.tot[k] = L.sc(C_TOT0 + k);
@@ -1034,6 +1393,10 @@ __device__ void lane_init(Lane& L, const Args& a, int l) {
   L.ybuf = (size_t)(a.npmax + 2) * 3 * a.Bp;
   L.frozen = false;
   L.share = 1.0;
+  L.half = half;
+  const int wl = threadIdx.x & 31;
+  L.base = wl & ~1;
+  L.mask = 3u << L.base;
 }
 
 enum Phase { PH_POISSON = 0, PH_NEWTON, PH_DONE };
@@ -1042,21 +1405,29 @@ enum Ctx {
   X_JV_START, X_JV_STAGE, X_JV_PRE, X_JV_SCAN     // solve_jv (solver.py:2105-2245)
 };
 
+// The whole J-V program of one device, run by both threads of its pair: every decision is
+// taken on values both hold bit for bit (half 0's, broadcast), so the two never part ways.
 template <int K>
-__global__ void __launch_bounds__(32) solve_kernel(Args a) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(64) solve_kernel(Args a) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = tid >> 1, half = tid & 1;
   if (l >= a.B) return;
   Lane L;
-  lane_init<K>(L, a, l);
+  lane_init<K>(L, a, l, half);
+  const bool top = half == 0;
   const bool jv = a.mode == DD_MODE_JV;
   const int voff = a.voff[l], nv = a.vcnt[l];
+  if (nv <= 0) return;
   const double* Vl = a.V + voff;
-  const double pre_cond = L.sc(C_PRECOND) > 0.0, fix_ions = L.sc(C_FIXIONS) > 0.0;
+  const bool pre_cond = L.sc(C_PRECOND) > 0.0, fix_ions = L.sc(C_FIXIONS) > 0.0;
   const double first = pre_cond ? L.sc(C_VPRE) : Vl[0];
-  // the start: the initial guess into the iterate
-  for (int i = 1; i <= L.NP; ++i)
+  {
+    int lo, hi;
+    own_range(L, lo, hi);
+    for (int i = lo; i <= hi; ++i)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) *L.y(0, i, c) = __ldg(a.Y0 + ((size_t)i * 3 + c) * a.Bp + l);
+      for (int c = 0; c < 3; ++c) *L.y(0, i, c) = __ldg(a.Y0 + ((size_t)i * 3 + c) * a.Bp + l);
+  }
   bool mobile = false;
 #pragma unroll
   for (int k = 0; k < K; ++k) mobile = mobile || L.tot[k] > 0.0;
@@ -1066,14 +1437,12 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
   for (int k = 0; k < K; ++k) { logs[k] = 0.0; lgA[k] = 0.0; lgB[k] = 0.0; lgC[k] = 0.0; }
   int phase = PH_POISSON, pit = 0;
   const int pcap = jv ? a.max_iter : a.start_iter;
-  // the Newton solve in progress
   int ctx = 0, it = 0, cap = 0, adv = ADV_NONE;
   double Vint = first, ratio = 0.0;
   double hs[4], hJ[4];
   int nsz = 0;
   bool floor_known = false, pending_noise = false;
   double noise_floor = 0.0;
-  // the program's flags
   bool ok_f = false, kept_f = false, solved = false, pre_ok = true, ok_c = false;
   int stage = 0;
   double before = 1.0;
@@ -1083,7 +1452,7 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
   if (!jv) {
     while (below < nv && Vl[below] < first) ++below;  // searchsorted, left
   }
-  a.status[l] = DD_LANE_OK;
+  if (top) a.status[l] = DD_LANE_OK;
 
   auto begin = [&](int c, double v, double share, int cp_, int ad, double ra) {
     ctx = c; Vint = v; L.share = share; cap = cp_; adv = ad; ratio = ra;
@@ -1092,7 +1461,6 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
     for (int q = 0; q < 4; ++q) { hs[q] = INFINITY; hJ[q] = INFINITY; }
     phase = PH_NEWTON;
   };
-  // the scan's next voltage (batch: outward from the pre-bias; jv: the caller's order)
   auto scan_begin = [&]() {
     if (k >= nv) { phase = PH_DONE; return; }
     if (!jv) {
@@ -1172,7 +1540,6 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
       }
       continue;
     }
-    // ------------------------------------------------------------ one Newton step
     bool end = false, conv = false, fin = true;
     double Jv = 0.0;
     if (pending_noise) {
@@ -1184,7 +1551,6 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
       if (mx < noise_floor) { end = true; conv = true; }
       else if (it >= cap) { end = true; conv = false; }
       Jv = hJ[3];
-      fin = isfinite(Jv) || true;
       if (!end) continue;
     } else {
       const StepOut o = newton_step<K>(L, Vint, logs, adv, ratio, false);
@@ -1236,7 +1602,6 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
       }
       if (!end) continue;
     }
-    // ------------------------------------------------------------ a solve ended
     switch (ctx) {
       case X_START_F: {
         ok_f = conv; kept_f = fin;
@@ -1274,9 +1639,11 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
       }
       case X_SCAN: {
         const int pos = voff + jcur;
-        a.J[pos] = Jv + L.Gshunt * Vint;
-        a.ok[pos] = (conv && pre_ok) ? 1 : 0;
-        a.its[pos] = it;
+        if (top) {
+          a.J[pos] = Jv + L.Gshunt * Vint;
+          a.ok[pos] = (conv && pre_ok) ? 1 : 0;
+          a.its[pos] = it;
+        }
         const bool keep = conv && fin;
         if (keep) {
           copyv<K>(lgB, lgA); copyv<K>(lgA, logs);
@@ -1305,8 +1672,10 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
       }
       case X_JV_PRE: {
         if (!conv) {
-          a.status[l] = DD_LANE_PREBIAS_FAILED;
-          for (int q = 0; q < nv; ++q) { a.J[voff + q] = NAN; a.ok[voff + q] = 0; a.its[voff + q] = 0; }
+          if (top) {
+            a.status[l] = DD_LANE_PREBIAS_FAILED;
+            for (int q = 0; q < nv; ++q) { a.J[voff + q] = NAN; a.ok[voff + q] = 0; a.its[voff + q] = 0; }
+          }
           phase = PH_DONE;
           break;
         }
@@ -1315,9 +1684,11 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
       }
       case X_JV_SCAN: {
         const int pos = voff + jcur;
-        a.J[pos] = Jv + L.Gshunt * Vint;
-        a.ok[pos] = conv ? 1 : 0;
-        a.its[pos] = it;
+        if (top) {
+          a.J[pos] = Jv + L.Gshunt * Vint;
+          a.ok[pos] = conv ? 1 : 0;
+          a.its[pos] = it;
+        }
         const bool keep = conv && fin;
         if (keep) { copyv<K>(lgA, logs); last_keep = 1; }
         else last_keep = 0;
@@ -1327,7 +1698,7 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
       }
     }
   }
-  if (a.steps) {
+  if (a.steps && top) {
     a.steps[l] = n_border;
     a.steps[a.Bp + l] = n_plain;
     a.steps[2 * a.Bp + l] = pit;
@@ -1336,20 +1707,23 @@ __global__ void __launch_bounds__(32) solve_kernel(Args a) {
 
 // One Newton step per lane from a given state (dd_newton_step).
 template <int K>
-__global__ void __launch_bounds__(32) step_kernel(Args a) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(64) step_kernel(Args a) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = tid >> 1, half = tid & 1;
   if (l >= a.B) return;
   Lane L;
-  lane_init<K>(L, a, l);
+  lane_init<K>(L, a, l, half);
   L.share = a.share;
   double logs[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) logs[k] = a.logs_io[(size_t)k * a.Bp + l];
   const StepOut o = newton_step<K>(L, a.vint[l], logs, ADV_NONE, 0.0, false);
+  if (half == 0) {
 #pragma unroll
-  for (int k = 0; k < K; ++k) a.logs_io[(size_t)k * a.Bp + l] = logs[k];
-  a.size_out[l] = o.size;
-  a.J_out[l] = o.J;
+    for (int k = 0; k < K; ++k) a.logs_io[(size_t)k * a.Bp + l] = logs[k];
+    a.size_out[l] = o.size;
+    a.J_out[l] = o.J;
+  }
 }
 
 }  // namespace dd
@@ -1436,7 +1810,7 @@ int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opt
   a.J = J; a.ok = converged; a.its = iterations; a.status = lane_status; a.steps = lane_steps;
   a.tol = opts->tol; a.max_iter = opts->max_iter; a.start_iter = opts->start_iter;
   a.strict = opts->strict; a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS; a.mode = opts->mode;
-  const dim3 grid((batch->lane_stride + 31) / 32), block(32);
+  const dim3 grid((2 * batch->lane_stride + 63) / 64), block(64);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (slots_k(batch) == 2) dd::solve_kernel<2><<<grid, block, 0, s>>>(a);
   else dd::solve_kernel<4><<<grid, block, 0, s>>>(a);
@@ -1456,7 +1830,7 @@ int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double*
   a.Y = y;  // the caller's state is the iterate buffer
   a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS;
   a.logs_io = logs; a.vint = vint; a.share = share; a.size_out = size; a.J_out = J;
-  const dim3 grid((batch->lane_stride + 31) / 32), block(32);
+  const dim3 grid((2 * batch->lane_stride + 63) / 64), block(64);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (slots_k(batch) == 2) dd::step_kernel<2><<<grid, block, 0, s>>>(a);
   else dd::step_kernel<4><<<grid, block, 0, s>>>(a);
