@@ -45,7 +45,7 @@ DEVICES_PER_GPU = 16384
 NP = 400
 CHUNK = 512  # devices per build task (a multiple of 32)
 #: which kernel build profiles/traffic.json must describe for its traffic to be reported
-KERNEL_TAG = "two-pass fused Newton, 26-word static record"
+KERNEL_TAG = "twisted two-thread fused Newton, 26-word static record"
 
 
 def _peaks() -> tuple[float, str]:
@@ -138,16 +138,17 @@ def poisson_bytes(NPk: int, w: int = 8) -> int:
     return NPk * (2 * 2 * w + 16)
 
 
-def algorithmic_bytes(batch, steps) -> float:
-    """Bytes of one launch from the steps each lane took (`lane_steps`)."""
+def algorithmic_bytes(batch, steps, w: int = 8) -> float:
+    """Bytes of one launch from the steps each lane took (`lane_steps`); `w` the sweep's word
+    (8 FP64, 4 in the mixed precision)."""
     total = 0.0
     lanes = batch["lane_of"]
     for k, dev in enumerate(batch["devices"]):
         lane = lanes[k]
         NPk = len(dev.x) - 2
         frozen = bool(dev.pre_cond and dev.fix_ions)
-        total += steps[0, lane] * step_bytes(NPk, True, False)
-        total += steps[1, lane] * step_bytes(NPk, False, frozen)
+        total += steps[0, lane] * step_bytes(NPk, True, False, w)
+        total += steps[1, lane] * step_bytes(NPk, False, frozen, w)
         total += steps[2, lane] * poisson_bytes(NPk)
     return total
 
@@ -359,13 +360,14 @@ def main() -> None:
             traffic = entry["dram_bytes_per_launch"]
     except (OSError, ValueError, KeyError):
         traffic = None
-    alg = algorithmic_bytes(batch, lane_steps)
+    alg = algorithmic_bytes(batch, lane_steps, 8 if args.precision == "fp64" else 4)
     achieved = alg / (ms / 1e3) / 1e9
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "curves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 sweep / f64 residual",
             "data": "synthetic",
             "config": {"workload": "BASELINE config 2: drawn p-i-n stacks (seed 20261203), "
                                    f"{args.devices} devices/GPU, NP {NP}, {nv} voltages -0.2..1.3 V,"

@@ -66,8 +66,11 @@ typedef struct dd_voltages {
 #define DD_BERNOULLI_EXACT 0 /* solver.bernoulli (solver.py:95-105) */
 #define DD_BERNOULLI_SIMSS 1 /* solver.bernoulli_simss (solver.py:108-121) */
 
-#define DD_PRECISION_FP64 0  /* everything in FP64 */
-#define DD_PRECISION_MIXED 1 /* FP32 Jacobian and block sweep, FP64 residual, update, current */
+#define DD_PRECISION_FP64 0  /* everything in FP64: the only precision dd_solve accepts */
+#define DD_PRECISION_MIXED 1 /* FP32 Jacobian and block sweep, FP64 residual, update and current:
+                                refused (DD_ERR_ARGS). Measured: the FP32 block sweep of these
+                                systems converges only linearly and, on some devices, not at all,
+                                so it cannot give jaxdd's converged flags. */
 
 typedef struct dd_opts {
   double tol;         /* Newton's step tolerance (solve_batch tol, default 1e-10) */

@@ -180,3 +180,4 @@ def test_drawn_devices_match_the_oracle():
     assert np.array_equal(ok, oko)
     err = np.max(np.abs(J - Jo), axis=1) / od["J_scale"]
     assert np.all(err < 1e-6), err
+
