@@ -31,6 +31,11 @@ extern "C" {
 #define DD_ERR_WORKSPACE 2  /* workspace smaller than dd_workspace_bytes */
 #define DD_ERR_LAUNCH 3     /* the CUDA launch failed (cudaGetLastError) */
 #define DD_ERR_DEVICE 4     /* no sm_100 device current */
+#define DD_ERR_SCRATCH 5    /* dd_solve_noalloc: the batch needs more scratch than
+                               DD_NOALLOC_SCRATCH_BYTES */
+
+/* Size of dd_solve_noalloc's fixed scratch array (64 MiB per device). */
+#define DD_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 /* Per-lane status written by dd_solve (lane_status). */
 #define DD_LANE_OK 0
@@ -107,6 +112,26 @@ int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opt
 int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double* vint,
                    double share, const dd_opts* opts, double* size, double* J, void* workspace,
                    size_t workspace_bytes, void* stream);
+
+/* dd_solve without a workspace argument, for callers that cannot allocate device memory for
+ * scratch: a plain C or foreign-function caller that holds the batch's buffers but has no device
+ * allocator of its own, or a caller that must not call cudaMalloc/cudaFree between solves
+ * (cudaFree waits for the whole device). It has no counterpart in the reference, whose solve
+ * gets its scratch from XLA.
+ *
+ * The scratch is one fixed array of DD_NOALLOC_SCRATCH_BYTES in the library's own device memory
+ * (reserved when the library's module loads on a device); nothing is allocated per call. A batch
+ * whose dd_workspace_bytes exceeds it is refused with DD_ERR_SCRATCH (at 400 nodes a lane
+ * stride of at most 640 with two ion slots, 544 with four); use dd_solve with a workspace for larger batches.
+ * The first call on each device, with that device current, looks the array's address up
+ * (cudaGetSymbolAddress) and keeps it; make that first call before any stream capture.
+ * DD_ERR_DEVICE if the lookup fails. All calls on a device share the one array and it keeps what
+ * the last call left (the kernel writes every word before reading it, so nothing needs
+ * clearing): calls whose work overlaps on the device race and give wrong results, so order them
+ * on one stream or one at a time. Results are those of dd_solve on the same inputs. */
+int dd_solve_noalloc(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts,
+                     double* J, uint8_t* converged, int32_t* iterations, int32_t* lane_status,
+                     int32_t* lane_steps, void* stream);
 
 /* A human-readable name of a status code. */
 const char* dd_status_string(int status);

@@ -33,6 +33,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "dd_layout.h"
 #include "../../include/jaxdd_b200.h"
 
@@ -1778,6 +1780,7 @@ const char* dd_status_string(int status) {
     case DD_ERR_WORKSPACE: return "workspace too small";
     case DD_ERR_LAUNCH: return "kernel launch failed";
     case DD_ERR_DEVICE: return "no sm_100 device";
+    case DD_ERR_SCRATCH: return "batch needs more scratch than dd_solve_noalloc's fixed array";
     default: return "unknown status";
   }
 }
@@ -1838,3 +1841,52 @@ int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double*
 }
 
 }  // extern "C"
+
+// ===================================================== allocation-free solve (dd_solve_noalloc)
+//
+// The scratch lives in one fixed array in the library's own device memory, reserved when the
+// module loads on a device. Every call on a device uses the same array: whatever the last call
+// left there stays, and two calls whose launches overlap (two streams, two host threads) race on
+// it. The solve kernel writes each word of its scratch before it reads it (the starting state
+// from y0, the sweep's records node by node, the extrapolation buffers before any
+// extrapolation uses them), so nothing has to be cleared between calls.
+
+namespace {
+
+static __device__ __align__(256) double noalloc_scratch[DD_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+constexpr int kMaxDevices = 64;
+std::mutex noalloc_mutex;
+void* noalloc_ptr[kMaxDevices] = {};
+
+// The array's address on the current device, looked up once per device (with that device
+// current) and kept. nullptr if there is no usable device or the lookup failed.
+void* noalloc_scratch_ptr() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  std::lock_guard<std::mutex> guard(noalloc_mutex);
+  if (!noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();  // so that the caller's next cudaGetLastError does not report it
+      return nullptr;
+    }
+    noalloc_ptr[dev] = p;
+  }
+  return noalloc_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" int dd_solve_noalloc(const dd_batch* batch, const dd_voltages* volts,
+                                const dd_opts* opts, double* J, uint8_t* converged,
+                                int32_t* iterations, int32_t* lane_status, int32_t* lane_steps,
+                                void* stream) {
+  size_t need = 0;
+  if (dd_workspace_bytes(batch, &need) != DD_OK) return DD_ERR_ARGS;
+  if (need > (size_t)DD_NOALLOC_SCRATCH_BYTES) return DD_ERR_SCRATCH;
+  void* scratch = noalloc_scratch_ptr();
+  if (!scratch) return DD_ERR_DEVICE;
+  return dd_solve(batch, volts, opts, J, converged, iterations, lane_status, lane_steps, scratch,
+                  (size_t)DD_NOALLOC_SCRATCH_BYTES, stream);
+}

@@ -47,6 +47,29 @@ def test_workspace_query_and_argument_checks():
     assert _lib.lib().dd_workspace_bytes(ctypes.byref(bad), ctypes.byref(size)) == 1
 
 
+def test_the_fixed_scratch_solve_refuses_a_batch_larger_than_its_array():
+    """dd_solve_noalloc checks the batch's scratch against its fixed array before any CUDA call:
+    at 400 nodes and two ion slots a lane stride of 640 fits, 672 does not."""
+    import ctypes
+    size = ctypes.c_size_t(0)
+    fits = _lib.DdBatch(640, 640, 400, 1, 1, 1, 1, 1, 1)
+    over = _lib.DdBatch(672, 672, 400, 1, 1, 1, 1, 1, 1)
+    so = _lib.lib()
+    assert so.dd_workspace_bytes(ctypes.byref(fits), ctypes.byref(size)) == 0
+    assert size.value <= _lib.DD_NOALLOC_SCRATCH_BYTES
+    assert so.dd_workspace_bytes(ctypes.byref(over), ctypes.byref(size)) == 0
+    assert size.value > _lib.DD_NOALLOC_SCRATCH_BYTES
+    v = _lib.DdVoltages(1, 1, 1)
+    opts = _lib.DdOpts(1e-10, 60, 60, 0, 0, 0, 0, 0)
+    st = so.dd_solve_noalloc(ctypes.byref(over), ctypes.byref(v), ctypes.byref(opts),
+                             1, 1, 1, 1, None, None)
+    assert st == _lib.DD_ERR_SCRATCH
+    assert "scratch" in so.dd_status_string(st).decode()
+    text = (ROOT / "include" / "jaxdd_b200.h").read_text()
+    assert f"DD_ERR_SCRATCH {_lib.DD_ERR_SCRATCH}" in text
+    assert "DD_NOALLOC_SCRATCH_BYTES (64u << 20)" in text
+
+
 def test_packer_writes_the_stencils():
     dev = build_device(read_setup(GOLDEN / "inputs" / "two_regions_light" / "simulation_setup.txt"))
     b = prepare([dev])
