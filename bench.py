@@ -1,6 +1,7 @@
 """Benchmark: J-V curves per second of the batched steady-state solve on B200.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference] [--precision fp64]
+                    [--workload config2|uneven]
     python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N ...
 
 Workload: BASELINE's configuration 2 — 16384 devices per GPU drawn from seed 20261203 (grid
@@ -15,6 +16,10 @@ Reports (one JSON line, rank 0): `value` (curves/s, inputs resident on the GPU, 
 `roofline` (the kernel's algorithmic bytes per launch over its event time, against the measured
 HBM copy bandwidth), `cpu_baseline` (the FP64 CPU oracle on one core, a bounded sample of the
 same workload), clocks sampled during the timed region.
+
+`--workload uneven`: BASELINE's configuration 3 in FP64 — 32768 devices per GPU in one launch,
+each with its own grid size NP ~ U{150..900} and voltage count Nv ~ U{21..121} over -0.2..1.3 V
+(otherwise the same draws).
 
 `--impl reference`: jaxdd itself needs JAX, which is not installed; its CPU path is stood in for
 by the FP64 oracle (a CPU restatement of its arithmetic), one single-threaded process per host
@@ -57,25 +62,36 @@ def _peaks() -> tuple[float, str]:
 
 
 def _build_chunk(args):
-    """Build and pack devices [start, start + n) of the drawn workload (a pool worker)."""
-    start, n = args
+    """Build and pack the drawn workload's devices `indices` (a pool worker); `uneven`: each
+    device its own grid size."""
+    indices, uneven = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from jaxdd_b200.batch import prepare
-    from jaxdd_b200.workloads import drawn_devices
-    return prepare(drawn_devices(n, NP=NP, start=start))
+    from jaxdd_b200.workloads import RAGGED_NP, drawn_device
+    devs = [drawn_device(int(k), NP=RAGGED_NP if uneven else NP) for k in indices]
+    return prepare(devs, ragged=uneven)
 
 
-def build_workload(n: int, start: int, procs: int):
+def build_workload(n: int, start: int, procs: int, uneven: bool = False):
     """The packed batch of devices [start, start + n), built in `procs` spawned processes (before
-    any CUDA call in this one)."""
+    any CUDA call in this one). `uneven` (the uneven workload): devices ordered by grid size,
+    then voltage count, so that a warp's lanes do alike work; returns the batch and each
+    device's voltage count (None for the fixed-size workload)."""
     from jaxdd_b200.batch import concat
-    tasks = [(start + k, min(CHUNK, n - k)) for k in range(0, n, CHUNK)]
+    indices = np.arange(start, start + n)
+    nv = None
+    if uneven:
+        from jaxdd_b200.workloads import ragged_plan
+        NPs, nv = ragged_plan(indices)
+        order = np.lexsort((nv, -NPs))
+        indices, nv = indices[order], nv[order]
+    tasks = [(indices[k:k + CHUNK], uneven) for k in range(0, n, CHUNK)]
     if procs <= 1:
         parts = [_build_chunk(t) for t in tasks]
     else:
         with mp.get_context("spawn").Pool(procs) as pool:
             parts = pool.map(_build_chunk, tasks)
-    return concat(parts)
+    return concat(parts, ragged=uneven), nv
 
 
 class Clocks:
@@ -153,10 +169,22 @@ def algorithmic_bytes(batch, steps, w: int = 8) -> float:
     return total
 
 
-def cpu_sample(n: int = 8):
-    """The oracle on one core over `n` devices of the workload (a bounded sample)."""
-    from jaxdd_b200.workloads import V_SCAN, drawn_devices
+def cpu_sample(n: int = 8, uneven: bool = False):
+    """The oracle on one core over `n` devices of the workload (a bounded sample); the uneven
+    workload's one device at a time (the oracle, like jaxdd, takes one grid size and one
+    voltage list per batch)."""
+    from jaxdd_b200.workloads import (RAGGED_NP, V_SCAN, drawn_device, drawn_devices,
+                                      ragged_plan, ragged_voltages)
     from oracle import dd
+    if uneven:
+        idx = np.arange(10 ** 6, 10 ** 6 + n)
+        _, nv = ragged_plan(idx)
+        devs = [drawn_device(int(k), NP=RAGGED_NP) for k in idx]
+        t0 = time.perf_counter()
+        for d, m in zip(devs, nv):
+            dd.solve_batch(dd.prepare([d]), ragged_voltages(m))
+        dt = time.perf_counter() - t0
+        return n / dt, dt
     devs = drawn_devices(n, NP=NP, start=10 ** 6)
     t0 = time.perf_counter()
     dd.solve_batch(dd.prepare(devs), V_SCAN)
@@ -165,19 +193,29 @@ def cpu_sample(n: int = 8):
 
 
 def _ref_worker(args):
-    """One single-threaded process of the reference arm: solve `n` devices, `reps` times."""
-    core, start, n, reps = args
+    """One single-threaded process of the reference arm: solve `n` devices, `reps` times (the
+    uneven workload's one device per batch, as jaxdd needs one grid size and voltage list per
+    batch)."""
+    core, start, n, reps, uneven = args
     try:
         os.sched_setaffinity(0, {core})
     except (AttributeError, OSError):
         pass
-    from jaxdd_b200.workloads import V_SCAN, drawn_devices
+    from jaxdd_b200.workloads import (RAGGED_NP, V_SCAN, drawn_device, drawn_devices,
+                                      ragged_plan, ragged_voltages)
     from oracle import dd
-    b = dd.prepare(drawn_devices(n, NP=NP, start=start))
+    if uneven:
+        idx = np.arange(start, start + n)
+        _, nv = ragged_plan(idx)
+        jobs = [(dd.prepare([drawn_device(int(k), NP=RAGGED_NP)]), ragged_voltages(m))
+                for k, m in zip(idx, nv)]
+    else:
+        jobs = [(dd.prepare(drawn_devices(n, NP=NP, start=start)), V_SCAN)]
     times = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        dd.solve_batch(b, V_SCAN)
+        for b, V in jobs:
+            dd.solve_batch(b, V)
         times.append(time.perf_counter() - t0)
     return times
 
@@ -188,7 +226,9 @@ def reference_arm(args, rank: int) -> None:
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     per = 2  # batch 2 per process (jaxdd benchmarks/run.py's CPU protocol)
     reps = args.warmup + args.steps
-    tasks = [(c % (os.cpu_count() or 1), 10 ** 6 + per * c, per, reps) for c in range(cores)]
+    uneven = args.workload == "uneven"
+    tasks = [(c % (os.cpu_count() or 1), 10 ** 6 + per * c, per, reps, uneven)
+             for c in range(cores)]
     t0 = time.perf_counter()
     with mp.get_context("spawn").Pool(cores) as pool:
         res = pool.map(_ref_worker, tasks)
@@ -202,8 +242,10 @@ def reference_arm(args, rank: int) -> None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "drawn p-i-n stacks (seed 20261203), NP 400, 61 V, "
-                               "batch 2 per process", "processes": cores},
+        "config": {"workload": ("uneven drawn p-i-n stacks (seed 20261203), NP U{150..900}, "
+                                "Nv U{21..121}, 2 devices per process, one per batch")
+                   if uneven else "drawn p-i-n stacks (seed 20261203), NP 400, 61 V, "
+                                  "batch 2 per process", "processes": cores},
         "cpu_baseline": {"value": rate, "unit": "curves/s", "cores": cores, "kind": "port",
                          "sample": f"{cores} processes x {per} devices x {args.steps} timed "
                                    f"steps (+{args.warmup} warm-up), wall {wall:.0f} s; "
@@ -214,6 +256,115 @@ def reference_arm(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _fit_texts(args):
+    start, n = args
+    from jaxdd_b200.fitting import fit_texts
+    return [fit_texts(k, NP=NP) for k in range(start, start + n)]
+
+
+def adjoint_bench(args, rank: int, world: int, local: int) -> None:
+    """The adjoint workload: the gradient of a J-V misfit (against curves of the same devices at
+    log-normally perturbed parameters) in 14 log-parameters per device. One step = parameters ->
+    packed record (torch) -> checkpointed solve -> misfit -> backward (adjoint kernel, then the
+    record's chain to the parameters). Reported as gradients (devices) per second, next to the
+    plain forward solve of the same devices."""
+    import torch
+    from jaxdd_b200 import adjoint as adj
+    from jaxdd_b200 import fitting
+    from jaxdd_b200.workloads import V_SCAN
+    n = args.devices
+    procs = args.build_procs or max(1, min(32, (os.cpu_count() or 1) // max(1, world)))
+    t0 = time.perf_counter()
+    tasks = [(rank * n + k, min(CHUNK, n - k)) for k in range(0, n, CHUNK)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        texts = [t for part in pool.map(_fit_texts, tasks) for t in part]
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    st = fitting.Structure(texts)
+    build_s = time.perf_counter() - t0
+    dev = st.device
+    p = adj.plan(st.batch, V_SCAN)
+    th0 = torch.tensor(st.theta0, dtype=torch.float64, device=dev)
+    with torch.no_grad():
+        Jt, okt, _ = adj.curves(*fitting.records(torch.tensor(
+            fitting.target_theta(st.theta0, start=rank * n), dtype=torch.float64, device=dev),
+            st), p)
+    target = (adj.per_device(p, Jt), adj.per_device(p, okt))
+    scale = torch.tensor(st.batch["J_scale"], device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def grad_step():
+        th = th0.clone().requires_grad_(True)
+        J, ok, _ = adj.curves(*fitting.records(th, st), p)
+        both = adj.per_device(p, ok) * target[1]
+        loss = fitting.misfit(adj.per_device(p, J), both, target[0], scale)
+        loss.backward()
+        return loss, th.grad
+
+    rec = [t.contiguous() for t in fitting.records(th0, st)]
+
+    def fwd_step():
+        return adj.solve_states(p, *rec)
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item()), out
+
+    with Clocks(local) as clocks:
+        ms_grad, (loss, g) = timed(grad_step, args.steps)
+    ms_fwd, _ = timed(fwd_step, args.steps)
+    value = n * world / (ms_grad / 1e3)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "gradients/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_grad,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"BASELINE config 4: {n} devices/GPU (drawn p-i-n stacks, "
+                                   f"seed 20261203, explicit work functions), NP {NP}, "
+                                   f"{len(V_SCAN)} voltages; loss sum of squared J misfits to "
+                                   "curves at parameters perturbed log-normally (sigma 0.2, "
+                                   "seed 20261204); gradient in 14 log-parameters per device",
+                       "build_s": round(build_s, 1), "loss": float(loss),
+                       "grad_norm": float(g.norm()), "forward_ms": ms_fwd,
+                       "adjoint_over_forward": ms_grad / ms_fwd,
+                       "converged_fraction": float(target[1].float().mean())},
+            "gpu_launches": args.steps * 5,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def workload_name(args, batch, nflat: int) -> str:
+    if args.workload == "uneven":
+        NPs = batch["NP"]
+        return (f"BASELINE config 3 in FP64: drawn p-i-n stacks (seed 20261203), {args.devices} "
+                f"devices/GPU in one launch, NP U{{150..900}} (mean {NPs.mean():.0f}), voltage "
+                f"counts U{{21..121}} (mean {nflat / batch['n']:.1f}) over -0.2..1.3 V, half "
+                "frozen after a 1.0 V pre-bias, half free ions")
+    return (f"BASELINE config 2: drawn p-i-n stacks (seed 20261203), {args.devices} devices/GPU, "
+            f"NP {NP}, {nflat // batch['n']} voltages -0.2..1.3 V, half frozen after a 1.0 V "
+            "pre-bias, half free ions")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -221,31 +372,42 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--precision", default="fp64", choices=("fp64",))
-    ap.add_argument("--devices", type=int, default=DEVICES_PER_GPU)
+    ap.add_argument("--workload", default="config2", choices=("config2", "uneven", "adjoint"),
+                    help="config2: 16384 devices, NP 400, 61 V (the default); uneven: 32768 "
+                         "devices, NP ~ U{150..900}, Nv ~ U{21..121}, one launch; adjoint: "
+                         "gradients of a J-V misfit in 14 parameters, 4096 devices")
+    ap.add_argument("--devices", type=int, default=0)
     ap.add_argument("--build-procs", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=8)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    uneven = args.workload == "uneven"
+    if not args.devices:
+        args.devices = {"uneven": 2 * DEVICES_PER_GPU, "adjoint": 4096}.get(args.workload,
+                                                                           DEVICES_PER_GPU)
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.workload == "adjoint":
+        adjoint_bench(args, rank, world, local)
         return
     if args.devices % 32:
         raise SystemExit("--devices must be a multiple of 32")
     cores = os.cpu_count() or 1
     procs = args.build_procs or max(1, min(32, cores // max(1, world)))
     t0 = time.perf_counter()
-    batch = build_workload(args.devices, rank * args.devices, procs)
+    batch, nv_dev = build_workload(args.devices, rank * args.devices, procs, uneven)
     build_s = time.perf_counter() - t0
-    cpu = cpu_sample(args.cpu_sample) if rank == 0 and world == 1 else None
+    cpu = cpu_sample(args.cpu_sample, uneven) if rank == 0 and world == 1 else None
 
     import ctypes
 
     import torch
     from jaxdd_b200 import _lib
     from jaxdd_b200.batch import _gpu, descriptor, initial_state
-    from jaxdd_b200.workloads import V_SCAN
+    from jaxdd_b200.workloads import V_SCAN, ragged_voltages
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -256,22 +418,27 @@ def main() -> None:
     dev = torch.device("cuda", local)
     g = _gpu(batch)
     Bp, npmax = batch["Bp"], batch["np_max"]
-    nv = len(V_SCAN)
     lanes = batch["lane_of"]
+    lists = [ragged_voltages(m) for m in nv_dev] if uneven else [V_SCAN] * batch["n"]
     y0 = np.zeros((npmax + 2, 3, Bp))
+    counts = np.zeros(Bp, dtype=np.int32)
     for k, d in enumerate(batch["devices"]):
-        first = d.V_pre if d.pre_cond else V_SCAN[0]
+        first = d.V_pre if d.pre_cond else lists[k][0]
         y0[:len(d.x), :, lanes[k]] = initial_state(d, first)
-    flat = np.tile(V_SCAN, Bp)
-    offsets = (np.arange(Bp) * nv).astype(np.int32)
-    counts = np.full(Bp, nv, dtype=np.int32)
+        counts[lanes[k]] = len(lists[k])
+    offsets = np.zeros(Bp, dtype=np.int32)
+    offsets[1:] = np.cumsum(counts)[:-1]
+    nflat = int(counts.sum())
+    flat = np.zeros(nflat)
+    for k in range(batch["n"]):
+        flat[offsets[lanes[k]]:offsets[lanes[k]] + counts[lanes[k]]] = lists[k]
     t_y0 = torch.from_numpy(y0).to(dev)
     t_v = torch.from_numpy(flat).to(dev)
     t_off = torch.from_numpy(offsets).to(dev)
     t_cnt = torch.from_numpy(counts).to(dev)
-    J = torch.empty(Bp * nv, dtype=torch.float64, device=dev)
-    ok = torch.empty(Bp * nv, dtype=torch.uint8, device=dev)
-    its = torch.empty(Bp * nv, dtype=torch.int32, device=dev)
+    J = torch.empty(nflat, dtype=torch.float64, device=dev)
+    ok = torch.empty(nflat, dtype=torch.uint8, device=dev)
+    its = torch.empty(nflat, dtype=torch.int32, device=dev)
     status = torch.empty(Bp, dtype=torch.int32, device=dev)
     steps = torch.zeros((3, Bp), dtype=torch.int32, device=dev)
     desc = descriptor(batch, g, t_y0)
@@ -309,7 +476,7 @@ def main() -> None:
     ms_max = float(t.item())
     curves = args.devices * world
     value = curves / (ms_max / 1e3)
-    ok_frac = float(ok.view(Bp, nv)[:batch["n"]].float().mean().item())
+    ok_frac = float(ok.float().mean().item())
     lane_steps = steps.cpu().numpy()
 
     # e2e: the C ABI from pinned host buffers, the copies inside the timed region
@@ -317,9 +484,9 @@ def main() -> None:
             (("stat", batch["stat"]), ("scal", batch["scal"]), ("iface", batch["iface"]),
              ("y0", y0), ("v", flat), ("off", offsets), ("cnt", counts))}
     dev_in = {k: torch.empty_like(v, device=dev) for k, v in host.items()}
-    J_h = torch.empty(Bp * nv, dtype=torch.float64).pin_memory()
-    ok_h = torch.empty(Bp * nv, dtype=torch.uint8).pin_memory()
-    its_h = torch.empty(Bp * nv, dtype=torch.int32).pin_memory()
+    J_h = torch.empty(nflat, dtype=torch.float64).pin_memory()
+    ok_h = torch.empty(nflat, dtype=torch.uint8).pin_memory()
+    its_h = torch.empty(nflat, dtype=torch.int32).pin_memory()
     desc2 = _lib.DdBatch(batch["n"], Bp, npmax, batch["ka"], batch["kc"],
                          dev_in["stat"].data_ptr(), dev_in["scal"].data_ptr(),
                          dev_in["iface"].data_ptr(), dev_in["y0"].data_ptr())
@@ -355,7 +522,7 @@ def main() -> None:
     traffic = None
     try:  # the ncu capture of the same kernel and workload (profiles/), per launch
         rec = json.loads((ROOT / "profiles" / "traffic.json").read_text())
-        entry = rec.get(f"solve_kernel_{args.precision}_config2")
+        entry = rec.get(f"solve_kernel_{args.precision}_{args.workload}")
         if entry and entry["devices"] == args.devices and KERNEL_TAG in entry["kernel"]:
             traffic = entry["dram_bytes_per_launch"]
     except (OSError, ValueError, KeyError):
@@ -369,9 +536,7 @@ def main() -> None:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 sweep / f64 residual",
             "data": "synthetic",
-            "config": {"workload": "BASELINE config 2: drawn p-i-n stacks (seed 20261203), "
-                                   f"{args.devices} devices/GPU, NP {NP}, {nv} voltages -0.2..1.3 V,"
-                                   " half frozen after a 1.0 V pre-bias, half free ions",
+            "config": {"workload": workload_name(args, batch, nflat),
                        "precision": args.precision, "devices_per_gpu": args.devices,
                        "l2": f"inputs larger than L2 ({batch['stat'].nbytes / 1e9:.2f} GB of "
                              "statics per launch)",

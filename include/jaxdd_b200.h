@@ -103,6 +103,44 @@ int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opt
              uint8_t* converged, int32_t* iterations, int32_t* lane_status, int32_t* lane_steps,
              void* workspace, size_t workspace_bytes, void* stream);
 
+/* dd_solve that also keeps what differentiating the curves needs (jaxdd keeps the same under
+ * `jax.checkpoint`: the converged solution per voltage, `_tangent`, batch.py:676-680): for each
+ * lane's voltage j (its j-th in `volts`, j < nv_max) the final iterate `states`
+ * [nv_max][np_max+2][3][lane_stride] (interior nodes written) and its ion normalisations
+ * `state_logs` [nv_max][DD_MAXK][lane_stride]; and the solution at the pre-bias (or first)
+ * voltage, before any freeze, `prebias` [np_max+2][3][lane_stride], `prebias_logs`
+ * [DD_MAXK][lane_stride]. Results otherwise those of dd_solve. */
+int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts,
+                    double* J, uint8_t* converged, int32_t* iterations, int32_t* lane_status,
+                    int32_t* lane_steps, double* states, double* state_logs, double* prebias,
+                    double* prebias_logs, int nv_max, void* workspace, size_t workspace_bytes,
+                    void* stream);
+
+/* Scratch bytes dd_adjoint needs for this batch. */
+int dd_adjoint_workspace_bytes(const dd_batch* batch, size_t* bytes);
+
+/* The adjoint of dd_solve_states: given J_bar (dL/dJ at every flat voltage position), the
+ * gradient of L with respect to the packed inputs — stat_bar [np_max+2][DD_NF][lane_stride],
+ * scal_bar [DD_NS_BASE+DD_MAXK][lane_stride], iface_bar [DD_MAXIF][DD_NIF][lane_stride], each
+ * laid out as its input — by implicit differentiation at the checkpointed solutions: jaxdd's
+ * `_converged_jvp` / `_tangent` in reverse mode (batch.py:661-737), one transposed bordered solve
+ * per converged voltage, plus one at the pre-bias for devices whose ions are frozen after it.
+ * `converged`, `states`, `state_logs`, `prebias`, `prebias_logs`, `nv_max` as dd_solve_states
+ * wrote them for the same batch and voltages; not-converged voltages contribute nothing.
+ * Derivatives are given for every continuous input the residual, the ions' constraints and the
+ * integral current read (stencils, mobilities, spacings, offsets, doping, recombination
+ * parameters, generation, fixed ions; length, contacts, ion totals, shunt, generation factor,
+ * pre-bias voltage; interface trap density and width); the thermal voltage, the row scales' own
+ * inputs beyond SP/SC, the interface capture coefficients and trap levels, and the
+ * integer fields (slots, interface index) get none (zero). A device with the differential
+ * current (`currDiffInt = 1`) gets NaN in scal_bar[C_VT] and nothing else. The outputs are
+ * zeroed and written on `stream`. */
+int dd_adjoint(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts,
+               const uint8_t* converged, const double* J_bar, const double* states,
+               const double* state_logs, const double* prebias, const double* prebias_logs,
+               int nv_max, double* stat_bar, double* scal_bar, double* iface_bar,
+               void* workspace, size_t workspace_bytes, void* stream);
+
 /* One damped Newton step per lane from the state y (`[(np_max+2)][3][lane_stride]`, interior
  * nodes used) and the ion normalisations logs (`[K][lane_stride]`) at the voltage Vint
  * (`[lane_stride]`), ions scaled by `share`: jaxdd's `_newton_step` (solver.py:1563-1608),

@@ -35,7 +35,8 @@ DD_LANE_PREBIAS_FAILED = 1
 
 #: every symbol include/jaxdd_b200.h declares
 EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve",
-           "dd_newton_step", "dd_solve_noalloc")
+           "dd_newton_step", "dd_solve_noalloc", "dd_solve_states", "dd_adjoint_workspace_bytes",
+           "dd_adjoint")
 
 #: dd_solve_noalloc's fixed scratch (include/jaxdd_b200.h DD_NOALLOC_SCRATCH_BYTES)
 DD_NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -78,6 +79,17 @@ def lib() -> ctypes.CDLL:
     so.dd_newton_step.restype = ctypes.c_int
     so.dd_newton_step.argtypes = [ctypes.POINTER(DdBatch), p, p, p, ctypes.c_double,
                                   ctypes.POINTER(DdOpts), p, p, p, ctypes.c_size_t, p]
+    so.dd_solve_states.restype = ctypes.c_int
+    so.dd_solve_states.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
+                                   ctypes.POINTER(DdOpts), p, p, p, p, p, p, p, p, p,
+                                   ctypes.c_int, p, ctypes.c_size_t, p]
+    so.dd_adjoint_workspace_bytes.restype = ctypes.c_int
+    so.dd_adjoint_workspace_bytes.argtypes = [ctypes.POINTER(DdBatch),
+                                              ctypes.POINTER(ctypes.c_size_t)]
+    so.dd_adjoint.restype = ctypes.c_int
+    so.dd_adjoint.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
+                              ctypes.POINTER(DdOpts), p, p, p, p, p, p, ctypes.c_int, p, p, p, p,
+                              ctypes.c_size_t, p]
     so.dd_solve_noalloc.restype = ctypes.c_int
     so.dd_solve_noalloc.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
                                     ctypes.POINTER(DdOpts), p, p, p, p, p, p]

@@ -144,6 +144,18 @@ def split_row(NP: int, ifk: np.ndarray) -> int:
     raise NotImplementedError(f"no row to split a grid of {NP} points between its interfaces")
 
 
+def _empty_stat(nodes: int, Bp: int) -> np.ndarray:
+    """Static records of nodes no device has: outside every ion slot and interface, unit row
+    scales."""
+    stat = np.zeros((nodes, _lib.DD_NF, Bp))
+    stat[:, _lib.S["ASLOT"], :] = -1.0
+    stat[:, _lib.S["CSLOT"], :] = -1.0
+    stat[:, _lib.S["IFK"], :] = -2.0
+    stat[:, _lib.S["SP"], :] = 1.0
+    stat[:, _lib.S["SC"], :] = 1.0
+    return stat
+
+
 def prepare(devices, ragged: bool = False) -> Batch:
     """A batch of devices for `solve_batch` (jaxdd batch.py:151-223). Like jaxdd's, every device
     must have one grid size (`ValueError` otherwise) unless `ragged` is true: then devices of
@@ -167,12 +179,7 @@ def prepare(devices, ragged: bool = False) -> Batch:
     lane_order = sorted(range(B), key=lambda k: key[k])
     lane_of = np.empty(B, dtype=np.int64)
     lane_of[lane_order] = np.arange(B)
-    stat = np.zeros((npmax + 2, _lib.DD_NF, Bp))
-    stat[:, _lib.S["ASLOT"], :] = -1.0
-    stat[:, _lib.S["CSLOT"], :] = -1.0
-    stat[:, _lib.S["IFK"], :] = -2.0
-    stat[:, _lib.S["SP"], :] = 1.0
-    stat[:, _lib.S["SC"], :] = 1.0
+    stat = _empty_stat(npmax + 2, Bp)
     scal = np.zeros((_lib.DD_NS_BASE + _lib.DD_MAXK, Bp))
     iface = np.zeros((_lib.DD_MAXIF, _lib.DD_NIF, Bp))
     J_scale = np.zeros(B)
@@ -189,26 +196,37 @@ def prepare(devices, ragged: bool = False) -> Batch:
     return out
 
 
-def concat(parts: list[Batch]) -> Batch:
+def concat(parts: list[Batch], ragged: bool = False) -> Batch:
     """One batch of several packed ones (each packed by `prepare` with the same grid size and
     slot counts), their devices in order; each part's lane order is kept, so a part packed in
-    its own process needs no repacking."""
+    its own process needs no repacking. With `ragged`, parts of different grid sizes too (the
+    smaller ones padded with empty nodes)."""
     first = parts[0]
+    npmax = max(p["np_max"] for p in parts)
     for p in parts:
-        if (p["np_max"], p["ka"], p["kc"]) != (first["np_max"], first["ka"], first["kc"]):
+        if (p["ka"], p["kc"]) != (first["ka"], first["kc"]) or (
+                p["np_max"] != npmax and not ragged):
             raise ValueError("concat needs parts of one grid size and slot counts")
         if p["n"] != p["Bp"]:
             raise ValueError("concat needs parts whose device count is a multiple of 32")
+
+    def padded(p):
+        if p["np_max"] == npmax:
+            return p["stat"]
+        out = _empty_stat(npmax + 2, p["Bp"])
+        out[:p["np_max"] + 2] = p["stat"]
+        return out
+
     lane_of, base, devs = [], 0, []
     for p in parts:
         lane_of.append(p["lane_of"] + base)
         base += p["Bp"]
         devs += p["devices"]
     out = Batch(
-        stat=np.concatenate([p["stat"] for p in parts], axis=2),
+        stat=np.concatenate([padded(p) for p in parts], axis=2),
         scal=np.concatenate([p["scal"] for p in parts], axis=1),
         iface=np.concatenate([p["iface"] for p in parts], axis=2),
-        lane_of=np.concatenate(lane_of), Bp=base, np_max=first["np_max"], ka=first["ka"],
+        lane_of=np.concatenate(lane_of), Bp=base, np_max=npmax, ka=first["ka"],
         kc=first["kc"], devices=devs)
     out["n"] = base
     for key in ("J_scale", "R_series", "G_shunt", "Vt", "NP"):
@@ -340,6 +358,34 @@ def solve_batch(batch: Batch, voltages, tol: float = 1e-10, max_iter: int = 60,
         strict=strict, bernoulli_name=bernoulli_name, mode=_lib.DD_MODE_BATCH,
         precision=precision)
     return _gather(batch, J, ok, its, offsets, len(vs), inv)
+
+
+def solve_uneven(batch: Batch, voltages: list, tol: float = 1e-10, max_iter: int = 60,
+                 bernoulli_name: str = "exact", strict: bool = False):
+    """`solve_batch` with a voltage list of its own for every device (`voltages[k]`, any
+    length), in one launch; with `prepare(..., ragged=True)` the devices' grid sizes may differ
+    too. jaxdd needs one `prepare` and one `solve_batch` per (grid size, voltage list)
+    (batch.py:151-155, 1136-1162) and gets the same curves that way. Returns one
+    `(J, converged, iterations)` per device, each in the order of its voltages."""
+    devs = batch["devices"]
+    if len(voltages) != len(devs):
+        raise ValueError(f"{len(voltages)} voltage lists for {len(devs)} devices")
+    lists = [np.asarray(v, dtype=float).reshape(-1) for v in voltages]
+    if any(v.size == 0 for v in lists):
+        raise ValueError("every device needs at least one voltage")
+    orders = [np.argsort(v, kind="stable") for v in lists]
+    firsts = np.array([d.V_pre if d.pre_cond else v[o[0]]
+                       for d, v, o in zip(devs, lists, orders)])
+    J, ok, its, status, offsets, counts = run(
+        batch, [v[o] for v, o in zip(lists, orders)], firsts, tol=tol, max_iter=max_iter,
+        start_iter=max_iter, strict=strict, bernoulli_name=bernoulli_name,
+        mode=_lib.DD_MODE_BATCH)
+    J, ok, its = J.cpu().numpy(), ok.cpu().numpy().astype(bool), its.cpu().numpy()
+    out = []
+    for k, (v, o) in enumerate(zip(lists, orders)):
+        at = offsets[batch["lane_of"][k]] + np.argsort(o, kind="stable")
+        out.append((J[at], ok[at], its[at]))
+    return out
 
 
 def _gather(batch, J, ok, its, offsets, nv, inv):

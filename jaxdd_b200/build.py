@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB_DIR = HERE / "lib"
 LIB = LIB_DIR / "libjaxdd_b200.so"
-SOURCES = ["dd_solve.cu"]
+SOURCES = ["dd_solve.cu", "dd_adjoint.cu"]
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
     "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-shared",
@@ -36,7 +36,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     """Compile the library if any source is newer than it; returns its path."""
     LIB_DIR.mkdir(exist_ok=True)
     srcs = [CSRC / s for s in SOURCES]
-    deps = srcs + list(CSRC.glob("*.h")) + list((HERE.parent / "include").glob("*.h"))
+    deps = (srcs + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh"))
+            + list((HERE.parent / "include").glob("*.h")))
     if not force and LIB.exists() and all(LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")

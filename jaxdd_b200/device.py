@@ -322,13 +322,29 @@ def _profile(table, x, lid, layer_gen, total):
     return np.where((j < len(a) - 1) & layer_gen[lid], g, 0.0)
 
 
+def grid_layout(setup: Setup, grid: str = "graded", grid_split: str = "exact") -> _Layout:
+    """The grid's structure for a setup: each layer's points and unscaled spacings (jaxdd's
+    `Structure` holds the same, device.py:386-575). The thicknesses only scale it: a device built
+    with this layout and other thicknesses keeps its points per layer (as jaxdd's
+    `device_arrays(structure, params)` does, device.py:877-885)."""
+    if grid not in GRIDS:
+        raise ValueError(f"grid {grid!r}: one of {GRIDS}")
+    thick = [ly.raw["L"] for ly in setup.layers]
+    NP = setup.i("NP")
+    if grid == "graded":
+        return _graded_layout(thick, NP)
+    return _simss_layout(thick, NP, setup.f("grad"), grid_split)
+
+
 def build_device(setup: Setup, grid_split: str = "exact", surface: str = "extraction",
                  langevin: str = "layer", braun: str = "exact", grid: str = "graded",
-                 statistics: str = "boltzmann") -> Device:
+                 statistics: str = "boltzmann", layout: _Layout | None = None) -> Device:
     """The device of a SIMsalabim input (jaxdd device.py:1066-1079, same arguments). `grid`
     "graded" (jaxdd's default) or "simss" (`Make_Grid`); `grid_split` as `layer_points`.
     `surface`, `langevin` and `braun` choose among models this build does not carry and are
-    accepted only at their defaults; `statistics` only "boltzmann"."""
+    accepted only at their defaults; `statistics` only "boltzmann". `layout` (`grid_layout` of
+    another setup of the same stack) fixes the grid's structure instead of laying it out for
+    this setup's thicknesses."""
     if grid not in GRIDS:
         raise ValueError(f"grid {grid!r}: one of {GRIDS}")
     if statistics != "boltzmann":
@@ -346,11 +362,9 @@ def build_device(setup: Setup, grid_split: str = "exact", surface: str = "extrac
 
     layers = setup.layers
     NP = setup.i("NP")
-    thick = [ly.raw["L"] for ly in layers]
-    if grid == "graded":
-        lay = _graded_layout(thick, NP)
-    else:
-        lay = _simss_layout(thick, NP, setup.f("grad"), grid_split)
+    lay = layout if layout is not None else grid_layout(setup, grid, grid_split)
+    if len(lay.lid) != NP + 2 or len(lay.norm) != len(layers):
+        raise ValueError("the layout is of another grid size or stack")
     lid = lay.lid
     per = {name: np.array([float(ly.raw[name]) for ly in layers])
            for name in ("L", "eps_r", "E_c", "E_v", "N_c", "N_D", "N_A", "mu_n", "mu_p",

@@ -14,6 +14,8 @@ fixed seeds and written as SIMsalabim setups (the reference's own input format),
   eV, both interfaces' traps logU(1e12, 1e15) m^-2 (neutral, mid-gap), HTL N_A and ETL N_D
   logU(1e20, 1e23), absorber anions = cations logU(1e22, 1e24) with mobility 1e-12; devices of
   even index pre-biased at 1.0 V with their ions frozen, odd ones with free ions.
+* the uneven workload — the same draws with a grid size NP ~ U{150..900} and a voltage count
+  Nv ~ U{21..121} per device (`ragged_plan`), Nv voltages evenly over -0.2..1.3 V.
 """
 
 from __future__ import annotations
@@ -23,12 +25,16 @@ import numpy as np
 from .device import build_device
 from .simss_input import setup_from_texts
 
-__all__ = ["pin_stack", "drawn_stack", "drawn_devices", "SEED_DRAWN", "V_SCAN"]
+__all__ = ["pin_stack", "drawn_stack", "drawn_devices", "SEED_DRAWN", "V_SCAN", "ragged_plan",
+           "ragged_voltages", "drawn_device"]
 
 #: Seed of the per-device draws (workloads 2 and 3).
 SEED_DRAWN = 20261203
 #: 61 voltages from -0.2 to 1.3 V.
 V_SCAN = np.round(np.linspace(-0.2, 1.3, 61), 10)
+#: The uneven workload's grid sizes and voltage counts: NP ~ U{150..900}, Nv ~ U{21..121}.
+RAGGED_NP = (150, 900)
+RAGGED_NV = (21, 121)
 
 
 def _layer(**kv) -> str:
@@ -104,13 +110,35 @@ def drawn_stack(k: int, rng: np.random.Generator, NP: int = 400):
     return build_device(setup_from_texts(drawn_texts(k, rng, NP)))
 
 
+def drawn_device(k: int, seed: int = SEED_DRAWN, NP: int | tuple[int, int] = 400):
+    """Device `k` of the drawn workload (its draws depend only on the seed and `k`)."""
+    rng = np.random.default_rng([seed, k])
+    npk = NP if isinstance(NP, int) else int(rng.integers(NP[0], NP[1] + 1))
+    return drawn_stack(k, rng, npk)
+
+
+def ragged_plan(indices, seed: int = SEED_DRAWN) -> tuple[np.ndarray, np.ndarray]:
+    """`(NP, Nv)` of the uneven workload's devices `indices`: the grid size is the first draw
+    of the device's own stream (as `drawn_device` with `NP=RAGGED_NP` draws it), the voltage
+    count a draw of a separate stream, so the device draws stay those of the fixed-size
+    workload."""
+    idx = np.asarray(indices, dtype=np.int64)
+    NP = np.array([int(np.random.default_rng([seed, int(k)]).integers(RAGGED_NP[0],
+                                                                      RAGGED_NP[1] + 1))
+                   for k in idx])
+    Nv = np.array([int(np.random.default_rng([seed, int(k), 3]).integers(RAGGED_NV[0],
+                                                                         RAGGED_NV[1] + 1))
+                   for k in idx])
+    return NP, Nv
+
+
+def ragged_voltages(Nv: int) -> np.ndarray:
+    """`Nv` voltages evenly from -0.2 to 1.3 V."""
+    return np.round(np.linspace(-0.2, 1.3, int(Nv)), 10)
+
+
 def drawn_devices(n: int, seed: int = SEED_DRAWN, NP: int | tuple[int, int] = 400,
                   start: int = 0):
     """Devices `start .. start + n` of the drawn workload (each device's draws depend only on
     the seed and its index). `NP` an int, or `(lo, hi)` for a grid size drawn U{lo..hi}."""
-    out = []
-    for k in range(start, start + n):
-        rng = np.random.default_rng([seed, k])
-        npk = NP if isinstance(NP, int) else int(rng.integers(NP[0], NP[1] + 1))
-        out.append(drawn_stack(k, rng, npk))
-    return out
+    return [drawn_device(k, seed, NP) for k in range(start, start + n)]

@@ -91,3 +91,33 @@ def test_mixed_grid_sizes_are_refused_unless_ragged():
         prepare([a, c])
     b = prepare([a, c], ragged=True)
     assert b["np_max"] == 400 and list(b["NP"]) == [400, 120]
+
+
+def test_uneven_plan_and_padded_concat():
+    """The uneven workload's grid sizes and voltage counts stay in range and repeat; parts of
+    different grid sizes concatenate with the smaller ones padded by empty nodes, their own
+    records unchanged."""
+    from jaxdd_b200.batch import concat, solve_uneven
+    from jaxdd_b200.workloads import RAGGED_NP, drawn_device, ragged_plan, ragged_voltages
+    NPs, nv = ragged_plan(range(200))
+    assert NPs.min() >= 150 and NPs.max() <= 900 and nv.min() >= 21 and nv.max() <= 121
+    assert np.array_equal(ragged_plan([7, 3])[0], NPs[[7, 3]])
+    assert len(drawn_device(7, NP=RAGGED_NP).x) == NPs[7] + 2
+    V = ragged_voltages(21)
+    assert len(V) == 21 and V[0] == -0.2 and V[-1] == 1.3
+    small = prepare([drawn_device(k, NP=(150, 160)) for k in range(32)], ragged=True)
+    large = prepare([drawn_device(k, NP=(300, 310)) for k in range(32, 64)], ragged=True)
+    with pytest.raises(ValueError):
+        concat([small, large])
+    both = concat([small, large], ragged=True)
+    assert both["np_max"] == large["np_max"] and both["Bp"] == 64
+    n = small["np_max"] + 2
+    assert np.array_equal(both["stat"][:n, :, :32], small["stat"])
+    assert np.all(both["stat"][n:, _lib.S["IFK"], :32] == -2.0)
+    assert np.all(both["stat"][n:, _lib.S["SP"], :32] == 1.0)
+    assert np.array_equal(both["stat"][:, :, 32:], large["stat"])
+    assert np.array_equal(both["lane_of"][32:], large["lane_of"] + 32)
+    with pytest.raises(ValueError):
+        solve_uneven(small, [V] * 31)
+    with pytest.raises(ValueError):
+        solve_uneven(small, [V] * 31 + [[]])
