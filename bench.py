@@ -64,15 +64,15 @@ def _peaks() -> tuple[float, str]:
 def _build_chunk(args):
     """Build and pack the drawn workload's devices `indices` (a pool worker); `uneven`: each
     device its own grid size."""
-    indices, uneven = args
+    indices, uneven, npts = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from jaxdd_b200.batch import prepare
     from jaxdd_b200.workloads import RAGGED_NP, drawn_device
-    devs = [drawn_device(int(k), NP=RAGGED_NP if uneven else NP) for k in indices]
+    devs = [drawn_device(int(k), NP=RAGGED_NP if uneven else npts) for k in indices]
     return prepare(devs, ragged=uneven)
 
 
-def build_workload(n: int, start: int, procs: int, uneven: bool = False):
+def build_workload(n: int, start: int, procs: int, uneven: bool = False, npts: int = NP):
     """The packed batch of devices [start, start + n), built in `procs` spawned processes (before
     any CUDA call in this one). `uneven` (the uneven workload): devices ordered by grid size,
     then voltage count, so that a warp's lanes do alike work; returns the batch and each
@@ -85,7 +85,7 @@ def build_workload(n: int, start: int, procs: int, uneven: bool = False):
         NPs, nv = ragged_plan(indices)
         order = np.lexsort((nv, -NPs))
         indices, nv = indices[order], nv[order]
-    tasks = [(indices[k:k + CHUNK], uneven) for k in range(0, n, CHUNK)]
+    tasks = [(indices[k:k + CHUNK], uneven, npts) for k in range(0, n, CHUNK)]
     if procs <= 1:
         parts = [_build_chunk(t) for t in tasks]
     else:
@@ -361,7 +361,7 @@ def workload_name(args, batch, nflat: int) -> str:
                 f"counts U{{21..121}} (mean {nflat / batch['n']:.1f}) over -0.2..1.3 V, half "
                 "frozen after a 1.0 V pre-bias, half free ions")
     return (f"BASELINE config 2: drawn p-i-n stacks (seed 20261203), {args.devices} devices/GPU, "
-            f"NP {NP}, {nflat // batch['n']} voltages -0.2..1.3 V, half frozen after a 1.0 V "
+            f"NP {args.np}, {nflat // batch['n']} voltages -0.2..1.3 V, half frozen after a 1.0 V "
             "pre-bias, half free ions")
 
 
@@ -377,6 +377,9 @@ def main() -> None:
                          "devices, NP ~ U{150..900}, Nv ~ U{21..121}, one launch; adjoint: "
                          "gradients of a J-V misfit in 14 parameters, 4096 devices")
     ap.add_argument("--devices", type=int, default=0)
+    ap.add_argument("--np", type=int, default=NP,
+                    help="grid points of the fixed-size workload (400; smaller only for "
+                         "profiling the same occupancy on less memory)")
     ap.add_argument("--build-procs", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=8)
     args = ap.parse_args()
@@ -398,7 +401,7 @@ def main() -> None:
     cores = os.cpu_count() or 1
     procs = args.build_procs or max(1, min(32, cores // max(1, world)))
     t0 = time.perf_counter()
-    batch, nv_dev = build_workload(args.devices, rank * args.devices, procs, uneven)
+    batch, nv_dev = build_workload(args.devices, rank * args.devices, procs, uneven, args.np)
     build_s = time.perf_counter() - t0
     cpu = cpu_sample(args.cpu_sample, uneven) if rank == 0 and world == 1 else None
 
@@ -523,7 +526,8 @@ def main() -> None:
     try:  # the ncu capture of the same kernel and workload (profiles/), per launch
         rec = json.loads((ROOT / "profiles" / "traffic.json").read_text())
         entry = rec.get(f"solve_kernel_{args.precision}_{args.workload}")
-        if entry and entry["devices"] == args.devices and KERNEL_TAG in entry["kernel"]:
+        if (entry and entry["devices"] == args.devices and entry["NP"] == args.np
+                and KERNEL_TAG in entry["kernel"]):
             traffic = entry["dram_bytes_per_launch"]
     except (OSError, ValueError, KeyError):
         traffic = None
