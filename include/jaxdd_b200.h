@@ -141,6 +141,17 @@ int dd_adjoint(const dd_batch* batch, const dd_voltages* volts, const dd_opts* o
                int nv_max, double* stat_bar, double* scal_bar, double* iface_bar,
                void* workspace, size_t workspace_bytes, void* stream);
 
+/* What jaxdd's `solve_states` reports (batch.py:1009-1030, 1165-1191) of the checkpoints
+ * dd_solve_states wrote: per lane and voltage j < min(count, nv_max) the profiles on all
+ * np_max + 2 points — V, n, p, qfls = V_T ln(n p / n_i^2), anion, cation (frozen ions as the
+ * pre-bias left them; the ions' boundary points their neighbours') — each laid out
+ * [nv_max][np_max+2][lane_stride], and the implied V_oc and PLQY of direct recombination
+ * [nv_max][lane_stride] (NaN where the device has none, or no generation). */
+int dd_observables(const dd_batch* batch, const dd_voltages* volts, const double* states,
+                   const double* state_logs, const double* prebias, const double* prebias_logs,
+                   int nv_max, double* V, double* n, double* p, double* qfls, double* anion,
+                   double* cation, double* implied_voc, double* plqy, void* stream);
+
 /* One damped Newton step per lane from the state y (`[(np_max+2)][3][lane_stride]`, interior
  * nodes used) and the ion normalisations logs (`[K][lane_stride]`) at the voltage Vint
  * (`[lane_stride]`), ions scaled by `share`: jaxdd's `_newton_step` (solver.py:1563-1608),

@@ -1,13 +1,14 @@
 """jaxdd_b200: jaxdd's batched steady-state drift-diffusion J-V solve, B200-native.
 
 The drop-in API of jaxdd (`build_device`, `prepare`, `solve_jv`, `solve_batch`, jaxdd
-src/jaxdd/__init__.py:14-29), plus `solve_uneven` (every device its own grid size and voltage
+src/jaxdd/__init__.py:14-29) and `solve_states`, plus `solve_uneven` (every device its own grid size and voltage
 list, in one launch), over a hand-written sm_100a CUDA kernel behind a C ABI
 (include/jaxdd_b200.h). Device building is host NumPy, as in jaxdd; the solve runs only on the
 GPU (no CPU fallback: without the built library the solvers raise).
 """
 
-from .batch import Batch, external_voltages, prepare, solve_batch, solve_uneven
+from .batch import (Batch, external_voltages, prepare, solve_batch, solve_states,
+                    solve_uneven)
 from .device import Device, build_device, layer_points, make_grid
 from .simss_input import (Layer, Setup, check_supported, read_setup, setup_from_texts,
                           simss_voltages)
@@ -18,5 +19,6 @@ __version__ = "0.1.0"
 __all__ = [
     "Batch", "Device", "JVResult", "Layer", "Setup", "build_device", "check_supported",
     "external_voltages", "layer_points", "make_grid", "prepare", "read_setup",
-    "setup_from_texts", "simss_voltages", "solve_batch", "solve_jv", "solve_uneven",
+    "setup_from_texts", "simss_voltages", "solve_batch", "solve_jv", "solve_states",
+    "solve_uneven",
 ]

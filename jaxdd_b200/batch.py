@@ -388,6 +388,56 @@ def solve_uneven(batch: Batch, voltages: list, tol: float = 1e-10, max_iter: int
     return out
 
 
+def solve_states(batch: Batch, voltages=0.0, tol: float = 1e-10, max_iter: int = 60,
+                 first_max_iter: int | None = 6, bernoulli_name: str = "exact",
+                 strict: bool = False, devices=None) -> dict:
+    """The steady states of a batch at `voltages` (one or several, internal) and what
+    photoluminescence measures of them (jaxdd batch.py:1165-1191): a dict of `V`, `n`, `p`,
+    `qfls`, `anion`, `cation` (devices x voltages x NP + 2), `implied_voc`, `plqy`, `J`,
+    `converged`, `iterations` (devices x voltages), in the order of `voltages`. Solved as
+    `solve_batch` (one pass at `max_iter`, which gives jaxdd's two passes' results); the
+    states are the checkpoints of `dd_solve_states`, the profiles and measures those of
+    `dd_observables`. One grid size per batch, as jaxdd's `prepare` has it."""
+    import torch
+    from .adjoint import plan as _plan
+    from .adjoint import solve_states as _solve_states
+    del first_max_iter, devices
+    if len(set(int(n) for n in batch["NP"])) != 1:
+        raise ValueError("solve_states needs one grid size (prepare without ragged)")
+    voltages = np.atleast_1d(np.asarray(voltages, dtype=float)).reshape(-1)
+    order = np.argsort(voltages, kind="stable")
+    inv = np.argsort(order, kind="stable")
+    vs = voltages[order]
+    p = _plan(batch, vs, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
+              strict=strict)
+    g = _gpu(batch)
+    rec = (g.stat, g.scal, g.iface)
+    J, ok, its, ckpt = _solve_states(p, *rec)
+    nv, nodes, Bp = p.nv_max, batch["np_max"] + 2, batch["Bp"]
+    cuda = J.device
+    prof = {k: torch.empty((nv, nodes, Bp), dtype=torch.float64, device=cuda)
+            for k in ("V", "n", "p", "qfls", "anion", "cation")}
+    meas = {k: torch.empty((nv, Bp), dtype=torch.float64, device=cuda)
+            for k in ("implied_voc", "plqy")}
+    desc = descriptor(batch, g, p.y0)
+    volts = _lib.DdVoltages(p.v.data_ptr(), p.offsets.data_ptr(), p.counts.data_ptr())
+    _lib.check(_lib.lib().dd_observables(
+        ctypes.byref(desc), ctypes.byref(volts), ckpt["states"].data_ptr(),
+        ckpt["logs"].data_ptr(), ckpt["pre"].data_ptr(), ckpt["pre_logs"].data_ptr(), nv,
+        *[prof[k].data_ptr() for k in ("V", "n", "p", "qfls", "anion", "cation")],
+        meas["implied_voc"].data_ptr(), meas["plqy"].data_ptr(),
+        torch.cuda.current_stream(cuda).cuda_stream), "dd_observables")
+    torch.cuda.synchronize()
+    lanes = batch["lane_of"]
+    offsets = p.offsets.cpu().numpy()
+    Jd, okd, itd = _gather(batch, J, ok, its, offsets, nv, inv)
+    out = {k: np.transpose(v.cpu().numpy()[:, :, lanes], (2, 0, 1))[:, inv]
+           for k, v in prof.items()}
+    out.update({k: v.cpu().numpy()[:, lanes].T[:, inv] for k, v in meas.items()})
+    out.update({"J": Jd, "converged": okd, "iterations": itd})
+    return out
+
+
 def _gather(batch, J, ok, its, offsets, nv, inv):
     J, ok, its = J.cpu().numpy(), ok.cpu().numpy().astype(bool), its.cpu().numpy()
     lanes = batch["lane_of"]

@@ -763,7 +763,7 @@ def freeze(s, ion, y, logs, Vt, flag):
     return s, ion
 
 
-def solve_one(d, voltages, bern, tol, max_iter, start_iter, strict=False):
+def solve_one(d, voltages, bern, tol, max_iter, start_iter, strict=False, states=False):
     """batch._solve_one (batch.py:937-1006) for every lane at once: start, pre-bias (ions
     frozen after it where `fixIons`), then the scan outwards from the pre-bias — up, then down
     from the pre-bias solution again — each voltage from the last two converged solutions
@@ -789,6 +789,9 @@ def solve_one(d, voltages, bern, tol, max_iter, start_iter, strict=False):
     J_out = np.zeros((nb, nv))
     ok_out = np.zeros((nb, nv), bool)
     it_out = np.zeros((nb, nv), int)
+    if states:
+        y_out = np.zeros((nb, nv) + y.shape[1:])
+        l_out = np.zeros((nb, nv, logs.shape[1]))
     for k in range(nv):
         t = turn[:, k]
         carry = tuple(np.where(t.reshape((-1,) + (1,) * (a.ndim - 1)), a0, a)
@@ -809,6 +812,11 @@ def solve_one(d, voltages, bern, tol, max_iter, start_iter, strict=False):
         J_out[rows, order[:, k]] = J
         ok_out[rows, order[:, k]] = ok
         it_out[rows, order[:, k]] = its
+        if states:
+            y_out[rows, order[:, k]] = y_new
+            l_out[rows, order[:, k]] = logs_new
+    if states:
+        return J_out, ok_out & pre_ok[:, None], it_out, (y_out, l_out, dz)
     return J_out, ok_out & pre_ok[:, None], it_out
 
 
@@ -837,6 +845,60 @@ def solve_batch(batch, voltages, tol=1e-10, max_iter=60, first_max_iter=6,
             J2, ok2, its2 = run(take(batch, idx), max_iter)
             J[idx], ok[idx], its[idx] = J2, ok2, its2
     return J + batch["G_shunt"][:, None] * voltages[None, :], ok, its
+
+
+def observed(d, y, logs, Vint):
+    """batch._observed (batch.py:1009-1030) in this scope (contacts of infinite surface
+    recombination, no free ends, no field-dependent rates): the solution on all NP + 2 points,
+    its implied V_oc and PLQY of direct recombination (`solver.solve_state`,
+    solver.py:2079-2089) and the ions on the grid (`_ions_on_grid`, solver.py:2096-2102). `d` the
+    tree after any freeze; one voltage per lane."""
+    s, ion = d["s"], d["ion"]
+    full = full_of(bounds(d, Vint), y)
+    n, p = np.exp(full[:, 1:-1, 1]), np.exp(full[:, 1:-1, 2])
+    vol = s["fac"] / (_col(d["L"]) * s["hm"] * s["hp"])  # solver._volumes (1952-1954)
+    k = d["rec"]["kd"][:, 1:-1]
+    rad = np.sum(vol * k * n * p, 1)
+    rad0 = np.sum(vol * k * d["rec"]["ni2"][:, 1:-1], 1)
+    gen = d["g_frac"] * np.sum(vol * d["G"][:, 1:-1], 1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        voc = np.where(rad0 > 0, d["Vt"] * np.log(rad / np.where(rad0 > 0, rad0, 1.0)), np.nan)
+        plqy = np.where(gen > 0, (rad - rad0) / np.where(gen > 0, gen, 1.0), np.nan)
+    la, lc = point_logs(logs, ion)
+    V = y[..., 0]
+    anion = s["a_fix"] + s["a_mask"] * np.exp(la + V / _col(d["Vt"]))
+    cation = s["c_fix"] + s["c_mask"] * np.exp(lc - V / _col(d["Vt"]))
+    pad = lambda a: np.concatenate([a[:, :1], a, a[:, -1:]], 1)  # noqa: E731
+    return full, voc, plqy, np.stack([pad(anion), pad(cation)], -1)
+
+
+def solve_states(batch, voltages=0.0, tol=1e-10, max_iter=60, bernoulli_name="exact",
+                 strict=False):
+    """batch.solve_states (batch.py:1165-1191): the steady states at `voltages` and what
+    photoluminescence measures of them; a dict of `V, n, p, qfls, anion, cation`
+    (batch × voltages × NP + 2), `implied_voc, plqy, J, converged, iterations`
+    (batch × voltages). One pass at `max_iter` (what jaxdd's two passes give)."""
+    bern = BERNOULLI[bernoulli_name]
+    voltages = np.atleast_1d(np.asarray(voltages, dtype=float))
+    order = np.argsort(voltages, kind="stable")
+    inv = np.argsort(order, kind="stable")
+    vs = voltages[order]
+    J, ok, its, (ys, ls, dz) = solve_one(batch, vs, bern, tol, max_iter, max_iter, strict,
+                                         states=True)
+    nb, nv = J.shape
+    full = np.zeros((nb, nv) + (ys.shape[2] + 2, 3))
+    voc, plqy = np.zeros((nb, nv)), np.zeros((nb, nv))
+    ions = np.zeros((nb, nv, ys.shape[2] + 2, 2))
+    for k in range(nv):
+        full[:, k], voc[:, k], plqy[:, k], ions[:, k] = observed(
+            dz, ys[:, k], ls[:, k], np.full(nb, vs[k]))
+    n, p = np.exp(full[..., 1]), np.exp(full[..., 2])
+    qfls = batch["Vt"][:, None, None] * np.log(n * p / batch["rec"]["ni2"][:, None, :])
+    J = J + batch["G_shunt"][:, None] * vs[None, :]
+    out = {"V": full[..., 0], "n": n, "p": p, "qfls": qfls, "implied_voc": voc, "plqy": plqy,
+           "J": J, "converged": ok, "iterations": its, "anion": ions[..., 0],
+           "cation": ions[..., 1]}
+    return {k: v[:, inv] for k, v in out.items()}
 
 
 # ----------------------------------------------------------------------------- solve_jv

@@ -145,14 +145,15 @@ def test_parameter_gradients_match_central_differences(fit_case):
             name, total[j], fd[j])
 
 
-def test_one_device_against_the_oracle(fit_case):
-    """Device 1 (free ions): the GPU's gradient of one curve's weighted sum against the oracle's
-    curves differenced in two parameters."""
+@pytest.mark.parametrize("k", [0, 1])
+def test_one_device_against_the_oracle(fit_case, k):
+    """Device 0 (ions frozen after its pre-bias) and device 1 (free ions): the GPU's gradient of
+    one curve's weighted sum in all 14 parameters against the oracle's curves differenced in each
+    (central, step 1e-6 and 5e-7, Richardson-extrapolated)."""
     from jaxdd_b200.device import build_device
     from jaxdd_b200.simss_input import setup_from_texts
     from oracle import dd
     st, p, th0, target, scale = fit_case
-    k = 1
     Vs = p.v.cpu().numpy()[:9]
     w = np.random.default_rng(11).uniform(-1, 1, 9) / st.batch["J_scale"][k]
     th = th0.clone().requires_grad_(True)
@@ -168,9 +169,12 @@ def test_one_device_against_the_oracle(fit_case):
         assert oko.all()
         return float(np.sum(w * Jo[0]))
 
-    for name in ("mu_n_absorber", "L_absorber"):
-        j = fitting.NAMES.index(name)
+    def central(j, h):
         e = np.zeros(14)
-        e[j] = 1e-6
-        fd = (oracle(st.theta0[k] + e) - oracle(st.theta0[k] - e)) / 2e-6
-        assert abs(g[j] - fd) <= 2e-4 * abs(fd) + 1e-9, (name, g[j], fd)
+        e[j] = h
+        return (oracle(st.theta0[k] + e) - oracle(st.theta0[k] - e)) / (2 * h)
+
+    fds = np.array([(4 * central(j, 5e-7) - central(j, 1e-6)) / 3 for j in range(14)])
+    top = np.abs(fds).max()
+    for j, name in enumerate(fitting.NAMES):
+        assert abs(g[j] - fds[j]) <= 1e-4 * abs(fds[j]) + 1e-7 * top, (name, g[j], fds[j])

@@ -118,3 +118,25 @@ def test_short_circuit_current_never_exceeds_the_generation():
     from jaxdd_b200.constants import Q
     generated = Q * np.sum(dev.h[:-1] * dev.G[:-1]) / np.sum(dev.h[:-1]) * dev.L
     assert ok.all() and -J[0] <= generated * (1 + 1e-9)
+
+
+def test_states_restatement_is_consistent_with_the_curves():
+    """`solve_states` (batch.py:1165-1191) restated: its J and flags are `solve_batch`'s, the
+    contacts' states are their boundary values, the splitting is V_T ln(n p / n_i^2), and the
+    radiative measures are finite with PLQY below one (radiative recombination is a part of the
+    generation at most)."""
+    from jaxdd_b200.workloads import drawn_devices
+    devs = drawn_devices(2, NP=60)
+    b = dd.prepare(devs)
+    V = [0.9, 0.0, 0.5]
+    st = dd.solve_states(b, V)
+    J, ok, _ = dd.solve_batch(b, V)
+    assert np.array_equal(st["J"], J) and np.array_equal(st["converged"], ok)
+    assert st["V"].shape == (2, 3, 62) and st["implied_voc"].shape == (2, 3)
+    bnd = dd.bounds(b, np.full(2, 0.5))
+    assert np.allclose(st["V"][:, 2, 0], bnd[:, 0, 0]) and np.allclose(st["V"][:, 2, -1], bnd[:, 1, 0])
+    ni2 = b["rec"]["ni2"][:, None, :]
+    assert np.allclose(st["qfls"], b["Vt"][:, None, None] * np.log(st["n"] * st["p"] / ni2))
+    assert np.all(np.isfinite(st["implied_voc"])) and np.all((st["plqy"] > 0) & (st["plqy"] < 1))
+    # the ions at the boundary points are their neighbours'
+    assert np.array_equal(st["anion"][..., 0], st["anion"][..., 1])
