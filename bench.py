@@ -353,6 +353,90 @@ def adjoint_bench(args, rank: int, world: int, local: int) -> None:
         torch.distributed.destroy_process_group()
 
 
+def _noion_chunk(args):
+    """Devices `indices` of the drawn workload without their mobile ions (a pool worker)."""
+    indices, npts = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from jaxdd_b200.batch import prepare
+    from jaxdd_b200.device import build_device
+    from jaxdd_b200.simss_input import setup_from_texts
+    from jaxdd_b200.workloads import SEED_DRAWN, drawn_texts
+    devs = []
+    for k in indices:
+        t = drawn_texts(int(k), np.random.default_rng([SEED_DRAWN, int(k)]), npts)
+        lines = []
+        for line in t["L2.txt"].splitlines():
+            key = line.split("=")[0].strip()
+            if key in ("N_anion", "N_cation", "mu_anion", "mu_cation", "ionsMayEnter"):
+                line = f"{key} = 0"
+            lines.append(line)
+        t["L2.txt"] = "\n".join(lines) + "\n"
+        devs.append(build_device(setup_from_texts(t)))
+    return prepare(devs)
+
+
+def impedance_bench(args, rank: int, world: int, local: int) -> None:
+    """Config 5's small-signal half: each device's admittance at 41 log-spaced frequencies from
+    1 Hz to 1 MHz about 0.8 V, devices of the drawn workload without their mobile ions (the
+    impedance with mobile ions is not built). One step = the steady solve at 0.8 V
+    (`dd_solve_states`) and `dd_admittance`, inputs resident on the GPU."""
+    import torch
+    from jaxdd_b200.batch import concat
+    from jaxdd_b200.impedance import Work
+    n = args.devices
+    procs = args.build_procs or max(1, min(32, (os.cpu_count() or 1) // max(1, world)))
+    t0 = time.perf_counter()
+    tasks = [(np.arange(rank * n + k, rank * n + min(n, k + CHUNK)), args.np)
+             for k in range(0, n, CHUNK)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        batch = concat(pool.map(_noion_chunk, tasks))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    build_s = time.perf_counter() - t0
+    freqs = np.logspace(0, 6, 41)
+    work = Work(batch, freqs, 0.8)
+    dev = work.eps.device
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        J, ok, Y = work.run()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            J, ok, Y = work.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(t.item())
+    finite = float(torch.isfinite(Y[:, :, :batch["n"]]).all(dim=1).float().mean())
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": n * world / (ms / 1e3), "unit": "spectra/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": f"BASELINE config 5, small-signal half: {n} devices/GPU "
+                                   "(drawn p-i-n stacks, seed 20261203, without mobile ions), "
+                                   f"NP {args.np}, 41 frequencies 1 Hz..1 MHz at 0.8 V",
+                       "build_s": round(build_s, 1),
+                       "converged_fraction": float(ok[:batch["n"]].float().mean()),
+                       "finite_fraction": finite},
+            "gpu_launches": args.steps * 3,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def workload_name(args, batch, nflat: int) -> str:
     if args.workload == "uneven":
         NPs = batch["NP"]
@@ -372,10 +456,12 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--precision", default="fp64", choices=("fp64",))
-    ap.add_argument("--workload", default="config2", choices=("config2", "uneven", "adjoint"),
+    ap.add_argument("--workload", default="config2",
+                    choices=("config2", "uneven", "adjoint", "impedance"),
                     help="config2: 16384 devices, NP 400, 61 V (the default); uneven: 32768 "
                          "devices, NP ~ U{150..900}, Nv ~ U{21..121}, one launch; adjoint: "
-                         "gradients of a J-V misfit in 14 parameters, 4096 devices")
+                         "gradients of a J-V misfit in 14 parameters, 4096 devices; "
+                         "impedance: 8192 devices without mobile ions, 41 frequencies")
     ap.add_argument("--devices", type=int, default=0)
     ap.add_argument("--np", type=int, default=NP,
                     help="grid points of the fixed-size workload (400; smaller only for "
@@ -388,13 +474,16 @@ def main() -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     uneven = args.workload == "uneven"
     if not args.devices:
-        args.devices = {"uneven": 2 * DEVICES_PER_GPU, "adjoint": 4096}.get(args.workload,
-                                                                           DEVICES_PER_GPU)
+        args.devices = {"uneven": 2 * DEVICES_PER_GPU, "adjoint": 4096,
+                        "impedance": 8192}.get(args.workload, DEVICES_PER_GPU)
     if args.impl == "reference":
         reference_arm(args, rank)
         return
     if args.workload == "adjoint":
         adjoint_bench(args, rank, world, local)
+        return
+    if args.workload == "impedance":
+        impedance_bench(args, rank, world, local)
         return
     if args.devices % 32:
         raise SystemExit("--devices must be a multiple of 32")

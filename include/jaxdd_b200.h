@@ -152,6 +152,22 @@ int dd_observables(const dd_batch* batch, const dd_voltages* volts, const double
                    int nv_max, double* V, double* n, double* p, double* qfls, double* anion,
                    double* cation, double* implied_voc, double* plqy, void* stream);
 
+/* Scratch bytes dd_admittance needs for this batch and n_freq frequencies. */
+int dd_admittance_workspace_bytes(const dd_batch* batch, int n_freq, size_t* bytes);
+
+/* The small-signal admittance Y = dJ/dV_int (S/m^2, SIMsalabim's sign) of every lane at each of
+ * n_freq angular frequencies `laps` ([n_freq][2]: i omega as re, im), about the steady state
+ * `state` ([np_max+2][3][lane_stride], e.g. dd_solve_states' checkpoint at the voltage `vint`
+ * [lane_stride]): jaxdd's `_admittance` for devices without mobile ions (impedance.py:230-353):
+ * one complex block-tridiagonal solve of (J + i omega M + the traps' occupations' own dynamics)
+ * dy = -dF/dV per (lane, frequency) and the linearised current of a time step (control-volume
+ * widths, each density's change, the displacement current; `eps` [np_max+2][lane_stride] the
+ * permittivity at every point). Y [n_freq][2][lane_stride] (re, im). Lanes with mobile ions are
+ * not supported (the host refuses them): k_anion and k_cation must be 1. */
+int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
+                  const double* vint, const double* laps, int n_freq, int bernoulli, double* Y,
+                  void* workspace, size_t workspace_bytes, void* stream);
+
 /* One damped Newton step per lane from the state y (`[(np_max+2)][3][lane_stride]`, interior
  * nodes used) and the ion normalisations logs (`[K][lane_stride]`) at the voltage Vint
  * (`[lane_stride]`), ions scaled by `share`: jaxdd's `_newton_step` (solver.py:1563-1608),

@@ -36,7 +36,7 @@ DD_LANE_PREBIAS_FAILED = 1
 #: every symbol include/jaxdd_b200.h declares
 EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve",
            "dd_newton_step", "dd_solve_noalloc", "dd_solve_states", "dd_adjoint_workspace_bytes",
-           "dd_adjoint", "dd_observables")
+           "dd_adjoint", "dd_observables", "dd_admittance_workspace_bytes", "dd_admittance")
 
 #: dd_solve_noalloc's fixed scratch (include/jaxdd_b200.h DD_NOALLOC_SCRATCH_BYTES)
 DD_NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -93,6 +93,12 @@ def lib() -> ctypes.CDLL:
     so.dd_observables.restype = ctypes.c_int
     so.dd_observables.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages), p, p, p,
                                   p, ctypes.c_int, p, p, p, p, p, p, p, p, p]
+    so.dd_admittance_workspace_bytes.restype = ctypes.c_int
+    so.dd_admittance_workspace_bytes.argtypes = [ctypes.POINTER(DdBatch), ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_size_t)]
+    so.dd_admittance.restype = ctypes.c_int
+    so.dd_admittance.argtypes = [ctypes.POINTER(DdBatch), p, p, p, p, ctypes.c_int, ctypes.c_int,
+                                 p, p, ctypes.c_size_t, p]
     so.dd_solve_noalloc.restype = ctypes.c_int
     so.dd_solve_noalloc.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
                                     ctypes.POINTER(DdOpts), p, p, p, p, p, p]

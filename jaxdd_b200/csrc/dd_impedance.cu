@@ -1,0 +1,597 @@
+// The small-signal admittance of a batch about its steady states on sm_100a: jaxdd's
+// `solve_impedance` for devices without mobile ions (src/jaxdd/impedance.py:230-409).
+//
+// At a steady state y0 a small voltage dV e^{iwt} drives (J + iw M) dy = -dF/dV dV: J the steady
+// Jacobian (the solve's own blocks), M the time terms of implicit Euler (-fac n sC and -fac p sC
+// on each continuity row's own ln n, ln p), and the traps' occupations as states with their own
+// rates (`_trap_blocks`, `_interface_blocks`: the occupation beyond its instantaneous response,
+// -iw/(iw + a) of it, in the rates and the charge). One complex block-tridiagonal solve per
+// (device, frequency), then the current of a time step (SIMsalabim's integral form over each
+// point's control volume, each density's change and the displacement current, `_current_parts`
+// with `tr`, batch.py:316-403) linearised in dy, the voltage and the traps' extra rates:
+// Y = dJ/dV = J'(0) + iw (J'(1) - J'(0)) + J_u (`_admittance`'s `current`, impedance.py:338-350).
+//
+// How: a first kernel takes one device and keeps, per node, the steady blocks A, B, C, the mass
+// terms, the bulk traps' rate, drive and capture terms, and the current's steady integrands; a
+// second takes one (device, frequency) pair per thread (a grid-stride loop over all pairs): the
+// complex elimination forward, the back substitution, then one left-to-right pass that carries
+// the current's tangent (its dt-free and its per-dt parts at once) to the admittance. jaxdd
+// differentiates its current with jax.jvp; the tangent here is written out.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dd_layout.h"
+#include "dd_physics.cuh"
+#include "../../include/jaxdd_b200.h"
+
+namespace dd {
+namespace imp {
+
+struct cplx {
+  double re, im;
+};
+__device__ __forceinline__ cplx mk(double r, double i = 0.0) { return cplx{r, i}; }
+__device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ cplx operator*(cplx a, cplx b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__device__ __forceinline__ cplx operator*(double s, cplx a) { return {s * a.re, s * a.im}; }
+__device__ __forceinline__ cplx operator/(cplx a, cplx b) {
+  // Smith's division
+  if (fabs(b.re) >= fabs(b.im)) {
+    const double r = b.im / b.re, den = b.re + b.im * r;
+    return {(a.re + a.im * r) / den, (a.im - a.re * r) / den};
+  }
+  const double r = b.re / b.im, den = b.re * r + b.im;
+  return {(a.re * r + a.im) / den, (a.im * r - a.re) / den};
+}
+
+// Per node of the steady-state record (first kernel's output), [node][word][lane].
+enum {
+  P_A = 0, P_B = 9, P_C = 18,      // the steady blocks
+  P_MN = 27, P_MP,                 // the mass terms -fac n sC, -fac p sC
+  P_TA, P_TDN, P_TDP, P_TRN, P_TRP, // bulk traps: rate a, drive in ln n / ln p, dR_n, dR_p
+  P_EVN, P_EVP, P_IUN, P_IUP,      // exp(-+Vg/V_T), the integrated recombination
+  P_DRN, P_DRP,                    // n dR/dn, p dR/dp
+  P_N, P_P,                        // the densities
+  P_WORDS
+};
+// Per lane scalars: single_n, single_p, K_n, K_p.
+enum { L_SN = 0, L_SP, L_KN, L_KP, L_WORDS };
+// Per node of a (device, frequency) thread: c' (9 complex) and d' (3 complex; then dy).
+enum { W_C = 0, W_D = 18, W_WORDS = 24 };
+
+struct Args {
+  int B, Bp, npmax, ka, simss, nf;
+  const double* S;
+  const double* C;
+  const double* IFt;
+  const double* state;   // [np+2][3][Bp]
+  const double* eps;     // [np+2][Bp]
+  const double* vint;    // [Bp]
+  const double* laps;    // [nf][2]: i omega
+  double* rec;           // [np+2][P_WORDS][Bp]
+  double* lsc;           // [L_WORDS][Bp]
+  double* scr;           // [np+2][W_WORDS][T]
+  double* Y;             // [nf][2][Bp]
+  long T;
+};
+
+__device__ void lane_init(Lane& L, const Args& a, int l) {
+  L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l; L.ka = a.ka; L.K = 2;
+  L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L);
+  L.V0 = L.sc(C_V0); L.VL = L.sc(C_VL); L.left = L.sc(C_LEFT);
+  L.lnnL = L.sc(C_LNNL); L.lnpL = L.sc(C_LNPL); L.lnnR = L.sc(C_LNNR); L.lnpR = L.sc(C_LNPR);
+  L.Jscale = L.sc(C_JSCALE); L.Gshunt = L.sc(C_GSHUNT); L.gfrac = L.sc(C_GFRAC);
+  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor); L.Hsum = L.sc(C_HSUM);
+  L.NP = (int)L.sc(C_NP);
+  L.mid = 0; L.currdiff = 0; L.simss = a.simss;
+  L.tot[0] = 0.0; L.tot[1] = 0.0;
+  L.FX = nullptr; L.CD = nullptr; L.ncd = 0; L.ybuf = 0;
+  L.frozen = false;  // the devices have no mobile ions (the host refuses others): fixed ions
+  L.share = 1.0;     // and slots come from the record
+  L.half = 0; L.base = 0; L.mask = 0;
+  L.Y = const_cast<double*>(a.state);
+}
+
+__device__ __forceinline__ void point(const Lane& L, int k, double Vint, Pt& P) {
+  const double zero[2] = {0.0, 0.0};
+  if (k == 0) contact(L, 0, Vint, P);
+  else if (k == L.NP + 1) contact(L, 1, Vint, P);
+  else { P.V = *L.y(0, k, 0); P.lnn = *L.y(0, k, 1); P.lnp = *L.y(0, k, 2); }
+  pt_fill(L, P, k, zero);
+}
+
+// The steady state's blocks, mass and trap terms and the current's integrands, per node.
+__global__ void __launch_bounds__(64) prepare_kernel(Args a) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= a.B) return;
+  Lane L;
+  lane_init(L, a, l);
+  const int NP = L.NP;
+  const double Vint = a.vint[l];
+  auto rec = [&](int k, int f) -> double& { return a.rec[((size_t)k * P_WORDS + f) * a.Bp + l]; };
+  Pt pm, pc, pn;
+  point(L, 0, Vint, pm);
+  point(L, 1, Vint, pc);
+  Flux el, er;
+  flux(L, pm, pc, L.st(0, S_MUN), L.st(0, S_MUP), el);
+  for (int i = 1; i <= NP; ++i) {
+    point(L, i + 1, Vint, pn);
+    flux(L, pc, pn, L.st(i, S_MUN), L.st(i, S_MUP), er);
+    double A[3][3], Bm[3][3], Cm[3][3], rhs[3], U0[2], W[2];
+    assemble_row<2>(L, i, pm, pc, pn, el, er, L.st(i - 1, S_H), L.st(i, S_H),
+                    (int)L.st(i - 1, S_IFK), (int)L.st(i, S_IFK), false, false, A, Bm, Cm, rhs,
+                    U0, W);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        rec(i, P_A + 3 * r + c) = A[r][c];
+        rec(i, P_B + 3 * r + c) = Bm[r][c];
+        rec(i, P_C + 3 * r + c) = Cm[r][c];
+      }
+    const double fac = L.st(i, S_FAC), sC = L.st(i, S_SC);
+    rec(i, P_MN) = -fac * pc.n * sC;
+    rec(i, P_MP) = -fac * pc.p * sC;
+    // bulk traps (`_trap_terms`, one neutral level)
+    const double Nt = L.st(i, S_NT);
+    double ta = 1.0, tdn = 0.0, tdp = 0.0, trn = 0.0, trp = 0.0;
+    if (Nt > 0.0) {
+      const double Cn = L.st(i, S_CNT), Cp = L.st(i, S_CPT), nt0 = L.st(i, S_NT0), pt0 = L.st(i, S_PT0);
+      ta = Cn * (pc.n + nt0) + Cp * (pc.p + pt0);
+      const double f = (Cn * pc.n + Cp * pt0) / ta;
+      tdn = Cn * pc.n * (1.0 - f);
+      tdp = -f * Cp * pc.p;
+      trn = -Nt * Cn * (pc.n + nt0);
+      trp = Nt * Cp * (pc.p + pt0);
+    }
+    rec(i, P_TA) = ta; rec(i, P_TDN) = tdn; rec(i, P_TDP) = tdp; rec(i, P_TRN) = trn; rec(i, P_TRP) = trp;
+    pm = pc; pc = pn; el = er;
+  }
+  // the current's integrands (steady values) on the points 0..NP+1
+  double iu[2] = {0.0, 0.0}, uc_prev[2] = {0.0, 0.0}, dx_prev = 0.0;
+  double sgl[2] = {0.0, 0.0}, dbl[2] = {0.0, 0.0};
+  // interface point recombination of point k: edges k-1 (right end) and k (left end)
+  auto ri_at = [&](int k, double& rn, double& rp) {
+    rn = 0.0; rp = 0.0;
+    for (int e = k - 1; e <= k; ++e) {
+      if (e < 0 || e > NP) continue;
+      const int t = (int)L.st(e, S_IFK);
+      if (t < 0) continue;
+      Pt p0, p1;
+      point(L, e, Vint, p0);
+      point(L, e + 1, Vint, p1);
+      Iface f;
+      iface_edge(L, t, p0.n, p1.n, p0.p, p1.p, f, false);
+      if (e == k) { rn += f.v[0]; rp += f.v[2]; } else { rn += f.v[1]; rp += f.v[3]; }
+    }
+  };
+  for (int k = 0; k <= NP + 1; ++k) {
+    Pt P;
+    point(L, k, Vint, P);
+    const double ev[2] = {exp(-(P.V + P.offn) * L.iVt), exp((P.V + P.offp) * L.iVt)};
+    double uc[2] = {0.0, 0.0};
+    double R = 0.0, dRn = 0.0, dRp = 0.0;
+    if (k >= 1 && k <= NP) {
+      recomb(L, k, P.n, P.p, R, dRn, dRp);
+      double rn, rp;
+      ri_at(k, rn, rp);
+      const double g = L.st(k, S_G) * L.gfrac;
+      uc[0] = R + rn - g;
+      uc[1] = R + rp - g;
+    }
+    rec(k, P_EVN) = ev[0]; rec(k, P_EVP) = ev[1];
+    rec(k, P_DRN) = dRn; rec(k, P_DRP) = dRp;
+    rec(k, P_N) = P.n; rec(k, P_P) = P.p;
+    if (k <= NP) {
+      const double dx = k < NP ? L.st(k, S_DX) : 0.0;
+      const double wk = 0.5 * (dx_prev + dx);
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        if (k >= 1) iu[c] += 0.5 * dx_prev * (uc_prev[c] + uc[c]);
+        const double mu = L.st(k, c == 0 ? S_MUN : S_MUP);
+        sgl[c] += wk * ev[c] / mu;
+        dbl[c] += wk * ev[c] * iu[c] / mu;
+        uc_prev[c] = uc[c];
+      }
+      rec(k, P_IUN) = iu[0]; rec(k, P_IUP) = iu[1];
+      dx_prev = dx;
+    }
+  }
+  Pt P0, PR;
+  point(L, 0, Vint, P0);
+  point(L, NP + 1, Vint, PR);
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const double sn = c == 0 ? -1.0 : 1.0;
+    const double d0 = c == 0 ? P0.n : P0.p, dR = c == 0 ? PR.n : PR.p;
+    const double e0 = exp(sn * ((c == 0 ? P0.offn : P0.offp) + P0.V) * L.iVt);
+    const double eR = exp(sn * ((c == 0 ? PR.offn : PR.offp) + PR.V) * L.iVt);
+    const double Bc = L.Vt * sn * (dR * eR - d0 * e0);
+    a.lsc[(size_t)(L_SN + c) * a.Bp + l] = sgl[c];
+    a.lsc[(size_t)(L_KN + c) * a.Bp + l] = (Bc - sn * dbl[c]) / sgl[c];
+  }
+}
+
+// The interface traps of one edge beyond their steady occupation (`_interface_beyond`): per unit
+// of (ln n_L, ln n_R, ln p_L, ln p_R) in the rates (`rate`), and the occupation's part in the
+// four point rates and the charge (`dR`).
+__device__ void iface_beyond(const Lane& L, int t, double nL, double nR, double pL, double pR,
+                             cplx lap, cplx (&rate)[4], double (&dR)[5]) {
+  const double Nt = L.itab(t, I_NT), Cn = L.itab(t, I_CN), Cp = L.itab(t, I_CP);
+  const double nlo = L.itab(t, I_NT0LO), nhi = L.itab(t, I_NT0HI);
+  const double plo = L.itab(t, I_PT0LO), phi = L.itab(t, I_PT0HI);
+  const double iw = L.itab(t, I_IW), charge = L.itab(t, I_CHARGE);
+  const double an = Cn * Nt, bp = Cp * Nt;
+  double a = Cn * (nL + nR + nlo + nhi) + Cp * (pL + pR + plo + phi);
+  const double b = Cn * (nL + nR) + Cp * (plo + phi);
+  const double f = b / (a > 0.0 ? a : 1.0);
+  dR[0] = -iw * an * (nL + nlo); dR[1] = -iw * an * (nR + nhi);
+  dR[2] = iw * bp * (pL + plo);  dR[3] = iw * bp * (pR + phi);
+  dR[4] = -charge * 0.5 * Nt * iw;
+  const double da[4] = {Cn * nL, Cn * nR, Cp * pL, Cp * pR};
+  const double db[4] = {Cn * nL, Cn * nR, 0.0, 0.0};
+  if (!(Nt > 0.0)) a = 1.0;
+  const cplx h = mk(0.0) - lap / (lap + mk(a));
+#pragma unroll
+  for (int w = 0; w < 4; ++w) rate[w] = ((db[w] - f * da[w]) / a) * h;
+  if (!(Nt > 0.0))
+#pragma unroll
+    for (int q = 0; q < 5; ++q) dR[q] = 0.0;
+}
+
+// The interface correction of row i's blocks: edges i-1 (this point its right end) and i (left).
+__device__ void iface_rows(const Lane& L, int i, double Vint, cplx lap, const double* rs,
+                           cplx (&dA)[3][3], cplx (&dB)[3][3], cplx (&dC)[3][3]) {
+  for (int side = 0; side < 2; ++side) {
+    const int e = side == 0 ? i - 1 : i;  // the edge; this point is its right (0) or left (1) end
+    if (e < 1 || e > L.NP - 1) continue;  // edges with both points interior
+    const int t = (int)L.st(e, S_IFK);
+    if (t < 0) continue;
+    Pt p0, p1;
+    point(L, e, Vint, p0);
+    point(L, e + 1, Vint, p1);
+    cplx rate[4];
+    double dR[5];
+    iface_beyond(L, t, p0.n, p1.n, p0.p, p1.p, lap, rate, dR);
+    const bool left_end = side == 1;
+    const double rows[3] = {dR[4], left_end ? dR[0] : dR[1], left_end ? dR[2] : dR[3]};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      // own logarithms: this point's; other: the edge's other point's
+      const cplx own_n = rate[left_end ? 0 : 1], own_p = rate[left_end ? 2 : 3];
+      const cplx oth_n = rate[left_end ? 1 : 0], oth_p = rate[left_end ? 3 : 2];
+      dB[r][1] = dB[r][1] + (rows[r] * rs[r]) * own_n;
+      dB[r][2] = dB[r][2] + (rows[r] * rs[r]) * own_p;
+      if (left_end) {  // coupling to the point after: C
+        dC[r][1] = dC[r][1] + (rows[r] * rs[r]) * oth_n;
+        dC[r][2] = dC[r][2] + (rows[r] * rs[r]) * oth_p;
+      } else {  // to the point before: A
+        dA[r][1] = dA[r][1] + (rows[r] * rs[r]) * oth_n;
+        dA[r][2] = dA[r][2] + (rows[r] * rs[r]) * oth_p;
+      }
+    }
+  }
+}
+
+__device__ void inv3c(const cplx (&M)[3][3], cplx (&Mi)[3][3]) {
+  const cplx c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+  const cplx c01 = M[0][2] * M[2][1] - M[0][1] * M[2][2];
+  const cplx c02 = M[0][1] * M[1][2] - M[0][2] * M[1][1];
+  const cplx c10 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+  const cplx c11 = M[0][0] * M[2][2] - M[0][2] * M[2][0];
+  const cplx c12 = M[0][2] * M[1][0] - M[0][0] * M[1][2];
+  const cplx c20 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+  const cplx c21 = M[0][1] * M[2][0] - M[0][0] * M[2][1];
+  const cplx c22 = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+  const cplx idet = mk(1.0) / (M[0][0] * c00 + M[0][1] * c10 + M[0][2] * c20);
+  Mi[0][0] = c00 * idet; Mi[0][1] = c01 * idet; Mi[0][2] = c02 * idet;
+  Mi[1][0] = c10 * idet; Mi[1][1] = c11 * idet; Mi[1][2] = c12 * idet;
+  Mi[2][0] = c20 * idet; Mi[2][1] = c21 * idet; Mi[2][2] = c22 * idet;
+}
+
+// The interface recombination's tangent of point k (edges k-1 and k): the steady occupation's
+// derivatives in the points' logarithms and the traps' extra rates (`_interface_rates`).
+__device__ void iface_tangent(const Lane& L, int k, double Vint, cplx lap,
+                              const cplx (&dlnn)[3], const cplx (&dlnp)[3], cplx& tn, cplx& tp) {
+  tn = mk(0.0); tp = mk(0.0);
+  for (int e = k - 1; e <= k; ++e) {
+    if (e < 0 || e > L.NP) continue;
+    const int t = (int)L.st(e, S_IFK);
+    if (t < 0) continue;
+    Pt p0, p1;
+    point(L, e, Vint, p0);
+    point(L, e + 1, Vint, p1);
+    Iface f;
+    iface_edge(L, t, p0.n, p1.n, p0.p, p1.p, f, true);
+    // this edge's two points in dlnn/dlnp's frame: index 0 is k-1, 1 is k, 2 is k+1
+    const int j0 = e - (k - 1), j1 = j0 + 1;
+    const cplx v[4] = {dlnn[j0], dlnn[j1], dlnp[j0], dlnp[j1]};
+    const int qn = e == k ? 0 : 1, qp = e == k ? 2 : 3;  // this point's left or right rates
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      tn = tn + f.d[w][qn] * v[w];
+      tp = tp + f.d[w][qp] * v[w];
+    }
+    // beyond the steady occupation (only edges with both points interior move, as jaxdd's)
+    cplx rate[4];
+    double dR[5];
+    iface_beyond(L, t, p0.n, p1.n, p0.p, p1.p, lap, rate, dR);
+    cplx df = mk(0.0);
+#pragma unroll
+    for (int w = 0; w < 4; ++w) df = df + rate[w] * v[w];
+    tn = tn + dR[qn] * df;
+    tp = tp + dR[qp] * df;
+  }
+}
+
+__global__ void __launch_bounds__(64) admittance_kernel(Args a) {
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < (long)a.Bp * a.nf;
+       t += (long)gridDim.x * blockDim.x) {
+    const int l = (int)(t % a.Bp), q = (int)(t / a.Bp);
+    if (l >= a.B) continue;
+    Lane L;
+    lane_init(L, a, l);
+    const int NP = L.NP;
+    const double Vint = a.vint[l];
+    const cplx lap = mk(a.laps[2 * q], a.laps[2 * q + 1]);
+    const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    auto rec = [&](int k, int f) { return a.rec[((size_t)k * P_WORDS + f) * a.Bp + l]; };
+    auto scr = [&](int k, int f) -> double& { return a.scr[((size_t)k * W_WORDS + f) * a.T + slot]; };
+    const double e = L.left;
+    // ---- forward elimination of (J + iw M + traps) dy = -dF/dV
+    cplx cp[3][3], dp[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) { dp[r] = mk(0.0); for (int c = 0; c < 3; ++c) cp[r][c] = mk(0.0); }
+    for (int i = 1; i <= NP; ++i) {
+      cplx A[3][3], Bm[3][3], Cm[3][3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          A[r][c] = mk(rec(i, P_A + 3 * r + c));
+          Bm[r][c] = mk(rec(i, P_B + 3 * r + c));
+          Cm[r][c] = mk(rec(i, P_C + 3 * r + c));
+        }
+      Bm[1][1] = Bm[1][1] + rec(i, P_MN) * lap;
+      Bm[2][2] = Bm[2][2] + rec(i, P_MP) * lap;
+      // bulk traps beyond their instantaneous occupation
+      const double ta = rec(i, P_TA);
+      const cplx h = mk(0.0) - lap / (lap + mk(ta));
+      const double fsc = L.st(i, S_FAC) * L.st(i, S_SC);
+      const cplx rn = (rec(i, P_TDN) / ta) * h, rp = (rec(i, P_TDP) / ta) * h;
+      Bm[1][1] = Bm[1][1] - (fsc * rec(i, P_TRN)) * rn;
+      Bm[1][2] = Bm[1][2] - (fsc * rec(i, P_TRN)) * rp;
+      Bm[2][1] = Bm[2][1] - (fsc * rec(i, P_TRP)) * rn;
+      Bm[2][2] = Bm[2][2] - (fsc * rec(i, P_TRP)) * rp;
+      if ((int)L.st(i - 1, S_IFK) >= 0 || (int)L.st(i, S_IFK) >= 0) {
+        const double rs[3] = {Q * L.st(i, S_SP), -L.st(i, S_FAC) * L.st(i, S_SC),
+                              -L.st(i, S_FAC) * L.st(i, S_SC)};
+        iface_rows(L, i, Vint, lap, rs, A, Bm, Cm);
+      }
+      // the drive: the residual's derivative in V_int (the contacts' potentials)
+      cplx r[3] = {mk(0.0), mk(0.0), mk(0.0)};
+      if (i == 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r[c] = r[c] - mk(rec(1, P_A + 3 * c) * 0.5 * e);
+      if (i == NP)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r[c] = r[c] - mk(rec(NP, P_C + 3 * c) * (-0.5 * e));
+      cplx M[3][3], Mi[3][3];
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          M[rr][c] = Bm[rr][c] - (A[rr][0] * cp[0][c] + A[rr][1] * cp[1][c] + A[rr][2] * cp[2][c]);
+      inv3c(M, Mi);
+      cplx t3[3];
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr)
+        t3[rr] = r[rr] - (A[rr][0] * dp[0] + A[rr][1] * dp[1] + A[rr][2] * dp[2]);
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr) {
+        dp[rr] = Mi[rr][0] * t3[0] + Mi[rr][1] * t3[1] + Mi[rr][2] * t3[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          cp[rr][c] = Mi[rr][0] * Cm[0][c] + Mi[rr][1] * Cm[1][c] + Mi[rr][2] * Cm[2][c];
+      }
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr) {
+        scr(i, W_D + 2 * rr) = dp[rr].re; scr(i, W_D + 2 * rr + 1) = dp[rr].im;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          scr(i, W_C + 2 * (3 * rr + c)) = cp[rr][c].re;
+          scr(i, W_C + 2 * (3 * rr + c) + 1) = cp[rr][c].im;
+        }
+      }
+    }
+    // ---- back substitution: dy_i = d'_i - c'_i dy_{i+1}
+    cplx x[3] = {mk(0.0), mk(0.0), mk(0.0)};
+    for (int i = NP; i >= 1; --i) {
+      cplx nx[3];
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr) {
+        cplx v = mk(scr(i, W_D + 2 * rr), scr(i, W_D + 2 * rr + 1));
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          v = v - mk(scr(i, W_C + 2 * (3 * rr + c)), scr(i, W_C + 2 * (3 * rr + c) + 1)) * x[c];
+        nx[rr] = v;
+      }
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr) {
+        x[rr] = nx[rr];
+        scr(i, W_D + 2 * rr) = nx[rr].re; scr(i, W_D + 2 * rr + 1) = nx[rr].im;
+      }
+    }
+    // ---- the current's tangent, left to right: base (dt-free, the traps' extra rates in it)
+    // and per-dt parts for both carriers, and the displacement current
+    auto dyv = [&](int k, int c) -> cplx {
+      if (k < 1 || k > NP) return mk(0.0);
+      return mk(scr(k, W_D + 2 * c), scr(k, W_D + 2 * c + 1));
+    };
+    auto dV = [&](int k) -> cplx {
+      if (k == 0) return mk(0.5 * e);
+      if (k == NP + 1) return mk(-0.5 * e);
+      return dyv(k, 0);
+    };
+    const double sign = -L.left;
+    const double Vt = L.Vt;
+    cplx dsgl[2] = {mk(0.0), mk(0.0)}, ddb_b[2] = {mk(0.0), mk(0.0)}, ddb_t[2] = {mk(0.0), mk(0.0)};
+    cplx diu_b[2] = {mk(0.0), mk(0.0)}, diu_t[2] = {mk(0.0), mk(0.0)};
+    cplx dS_b[2] = {mk(0.0), mk(0.0)}, dS_t[2] = {mk(0.0), mk(0.0)};
+    cplx sumJ_b[2] = {mk(0.0), mk(0.0)}, sumJ_t[2] = {mk(0.0), mk(0.0)};
+    cplx duc_prev_b[2] = {mk(0.0), mk(0.0)}, duc_prev_t[2] = {mk(0.0), mk(0.0)};
+    cplx dJD = mk(0.0);
+    double hsum = 0.0, dx_prev = 0.0, h_prev = 0.0;
+    for (int k = 0; k <= NP; ++k) {
+      const double hk = L.st(k, S_H);
+      const double dx = k < NP ? L.st(k, S_DX) : 0.0;
+      const double wk = 0.5 * (dx_prev + dx);
+      const double width = k == 0 ? hk : 0.5 * (h_prev + hk);
+      hsum += hk;
+      // the interface recombination's tangent at k and k+1 (through term)
+      cplx dRi_k[2] = {mk(0.0), mk(0.0)}, dRi_k1[2] = {mk(0.0), mk(0.0)};
+      // points k and k + 1 touch edges k - 1 .. k + 1
+      bool trapped = false;
+      for (int ee = k - 1; ee <= k + 1; ++ee)
+        if (ee >= 0 && ee <= NP && (int)L.st(ee, S_IFK) >= 0) trapped = true;
+      if (trapped) {
+        const cplx ln[3] = {dyv(k - 1, 1), dyv(k, 1), dyv(k + 1, 1)};
+        const cplx lp[3] = {dyv(k - 1, 2), dyv(k, 2), dyv(k + 1, 2)};
+        iface_tangent(L, k, Vint, lap, ln, lp, dRi_k[0], dRi_k[1]);
+        if (k + 1 <= NP + 1) {
+          const cplx ln1[3] = {dyv(k, 1), dyv(k + 1, 1), dyv(k + 2, 1)};
+          const cplx lp1[3] = {dyv(k, 2), dyv(k + 1, 2), dyv(k + 2, 2)};
+          iface_tangent(L, k + 1, Vint, lap, ln1, lp1, dRi_k1[0], dRi_k1[1]);
+        }
+      }
+      // the bulk traps' extra rates at k
+      cplx dU[2] = {mk(0.0), mk(0.0)};
+      if (k >= 1) {
+        const double ta = rec(k, P_TA);
+        const cplx h = mk(0.0) - lap / (lap + mk(ta));
+        const cplx df = ((rec(k, P_TDN) / ta) * h) * dyv(k, 1) + ((rec(k, P_TDP) / ta) * h) * dyv(k, 2);
+        dU[0] = rec(k, P_TRN) * df;
+        dU[1] = rec(k, P_TRP) * df;
+      }
+      const bool iface_k = L.st(k, S_IFK) > -1.5;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const double sn = c == 0 ? -1.0 : 1.0;
+        const double ev = rec(k, c == 0 ? P_EVN : P_EVP), iu = rec(k, c == 0 ? P_IUN : P_IUP);
+        const double mu = L.st(k, c == 0 ? S_MUN : S_MUP);
+        const cplx dev = (ev * sn / Vt) * dV(k);
+        cplx duc_b = mk(0.0), duc_t = mk(0.0);
+        if (k >= 1) {
+          duc_b = rec(k, P_DRN) * dyv(k, 1) + rec(k, P_DRP) * dyv(k, 2) + dRi_k[c] + dU[c];
+          duc_t = rec(k, c == 0 ? P_N : P_P) * dyv(k, 1 + c);
+          diu_b[c] = diu_b[c] + (0.5 * dx_prev) * (duc_prev_b[c] + duc_b);
+          diu_t[c] = diu_t[c] + (0.5 * dx_prev) * (duc_prev_t[c] + duc_t);
+        }
+        dsgl[c] = dsgl[c] + (wk / mu) * dev;
+        ddb_b[c] = ddb_b[c] + (wk * iu / mu) * dev + (wk * ev / mu) * diu_b[c];
+        ddb_t[c] = ddb_t[c] + (wk * ev / mu) * diu_t[c];
+        const cplx dS_prev_b = dS_b[c], dS_prev_t = dS_t[c];
+        if (k >= 1) {
+          dS_b[c] = dS_b[c] + (sn * Q * L.L * width) * duc_b;
+          dS_t[c] = dS_t[c] + (sn * Q * L.L * width) * duc_t;
+        }
+        if (iface_k) {
+          const cplx thr = (sn * 0.5 * Q * L.L * hk) * (dRi_k[c] + dRi_k1[c]);
+          sumJ_b[c] = sumJ_b[c] + hk * (dS_prev_b + thr);
+          sumJ_t[c] = sumJ_t[c] + hk * dS_prev_t;
+        } else {
+          sumJ_b[c] = sumJ_b[c] + hk * dS_b[c];
+          sumJ_t[c] = sumJ_t[c] + hk * dS_t[c];
+        }
+        duc_prev_b[c] = duc_b;
+        duc_prev_t[c] = duc_t;
+      }
+      // the displacement current on interval k (its per-dt part)
+      const double epsk = a.eps[(size_t)k * a.Bp + l];
+      dJD = dJD + (hk * sign * epsk / (L.L * hk)) * (dV(k + 1) - dV(k));
+      dx_prev = dx;
+      h_prev = hk;
+    }
+    // K's tangent and the total
+    cplx Yb = mk(0.0), Yt = mk(0.0);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const double sn = c == 0 ? -1.0 : 1.0;
+      const double sgl = a.lsc[(size_t)(L_SN + c) * a.Bp + l], K = a.lsc[(size_t)(L_KN + c) * a.Bp + l];
+      // the contacts' densities are fixed; their exp(sn Vg / V_T) move with the voltage
+      Pt P0, PR;
+      point(L, 0, Vint, P0);
+      point(L, NP + 1, Vint, PR);
+      const double d0 = c == 0 ? P0.n : P0.p, dR = c == 0 ? PR.n : PR.p;
+      const double e0 = exp(sn * ((c == 0 ? P0.offn : P0.offp) + P0.V) / Vt);
+      const double eR = exp(sn * ((c == 0 ? PR.offn : PR.offp) + PR.V) / Vt);
+      const cplx dBc = (Vt * sn) * ((dR * eR * sn / Vt) * dV(NP + 1) - (d0 * e0 * sn / Vt) * dV(0));
+      const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (K / sgl) * dsgl[c];
+      const cplx dK_t = (-sn / sgl) * ddb_t[c];
+      Yb = Yb + sign * (Q * hsum) * dK_b + sign * sumJ_b[c];
+      Yt = Yt + sign * (Q * hsum) * dK_t + sign * sumJ_t[c];
+    }
+    Yt = Yt + dJD;
+    const cplx Y = (1.0 / hsum) * (Yb + lap * Yt);
+    a.Y[((size_t)q * 2) * a.Bp + l] = Y.re;
+    a.Y[((size_t)q * 2 + 1) * a.Bp + l] = Y.im;
+  }
+}
+
+}  // namespace imp
+}  // namespace dd
+
+namespace {
+long imp_threads() { return 148L * 256; }
+}
+
+extern "C" {
+
+int dd_admittance_workspace_bytes(const dd_batch* batch, int n_freq, size_t* bytes) {
+  if (!batch || !bytes || n_freq < 1 || batch->n_lanes < 1 || batch->lane_stride % 32 != 0 ||
+      batch->np_max < 3)
+    return DD_ERR_ARGS;
+  const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
+  long T = (long)Bp * n_freq;
+  if (T > imp_threads()) T = imp_threads();
+  *bytes = (nodes * dd::imp::P_WORDS * Bp + dd::imp::L_WORDS * Bp +
+            nodes * dd::imp::W_WORDS * (size_t)T) * sizeof(double);
+  return DD_OK;
+}
+
+int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
+                  const double* vint, const double* laps, int n_freq, int bernoulli, double* Y,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+  if (!batch || !batch->stat || !batch->scal || !batch->iface || !state || !eps || !vint ||
+      !laps || n_freq < 1 || !Y || !workspace)
+    return DD_ERR_ARGS;
+  if (batch->n_lanes < 1 || batch->lane_stride < batch->n_lanes || batch->lane_stride % 32 != 0 ||
+      batch->np_max < 3 || batch->k_anion != 1 || batch->k_cation != 1)
+    return DD_ERR_ARGS;
+  if (bernoulli != DD_BERNOULLI_EXACT && bernoulli != DD_BERNOULLI_SIMSS) return DD_ERR_ARGS;
+  size_t need;
+  dd_admittance_workspace_bytes(batch, n_freq, &need);
+  if (workspace_bytes < need) return DD_ERR_WORKSPACE;
+  const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
+  dd::imp::Args a{};
+  a.B = batch->n_lanes; a.Bp = batch->lane_stride; a.npmax = batch->np_max; a.ka = batch->k_anion;
+  a.simss = bernoulli == DD_BERNOULLI_SIMSS; a.nf = n_freq;
+  a.S = batch->stat; a.C = batch->scal; a.IFt = batch->iface;
+  a.state = state; a.eps = eps; a.vint = vint; a.laps = laps; a.Y = Y;
+  double* ws = static_cast<double*>(workspace);
+  a.rec = ws;
+  a.lsc = ws + nodes * dd::imp::P_WORDS * Bp;
+  a.scr = a.lsc + dd::imp::L_WORDS * Bp;
+  long T = (long)Bp * n_freq;
+  if (T > imp_threads()) T = imp_threads();
+  a.T = T;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  dd::imp::prepare_kernel<<<(unsigned)((Bp + 63) / 64), 64, 0, s>>>(a);
+  dd::imp::admittance_kernel<<<(unsigned)((T + 63) / 64), 64, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+"""Impedance in the frequency domain from the steady state's Jacobian: jaxdd's
+`solve_impedance` (src/jaxdd/impedance.py:365-409) for devices without mobile ions.
+
+At the steady state of each device at `voltage` (the solve's own, `dd_solve_states`) a small
+voltage drives `(J + iωM)·δy = −(∂F/∂V)·δV`, the traps' occupations following at their own rates;
+`dd_admittance` solves it for every (device, frequency) on the GPU and linearises the current of
+a time step (`Y = δJ/δV`). With a series resistance and a shunt the external
+`Z = 1/(Y + G_shunt) + R_series`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .batch import Batch, _gpu, descriptor
+
+
+@dataclass(frozen=True)
+class ImpedanceResult:
+    """Per device and frequency (devices x frequencies): `Z` the external impedance (Ω·m²),
+    `Y` the internal admittance δJ/δV_int (S/m², SIMsalabim's sign); per device the steady
+    state's `J` (A/m²) and `converged` (jaxdd impedance.py:46-64)."""
+
+    frequencies: np.ndarray
+    Z: np.ndarray
+    Y: np.ndarray
+    J: np.ndarray
+    converged: np.ndarray
+
+    @property
+    def capacitance(self) -> np.ndarray:
+        return self.Y.imag / (2 * np.pi * self.frequencies)
+
+
+class Work:
+    """The device-side inputs of one impedance run, packed once: the plan of the steady solve at
+    `voltage`, the permittivities, the frequencies, the output and the workspace. `run()` solves
+    the steady states and the admittances on the current stream and returns the device tensors
+    `(J, converged, Y)` (J, converged flat in lane order; Y [frequency][re, im][lane])."""
+
+    def __init__(self, batch: Batch, frequencies, voltage: float, tol: float = 1e-10,
+                 max_iter: int = 60, bernoulli_name: str = "exact"):
+        import torch
+        from .adjoint import plan as _plan
+        self.batch = batch
+        self.plan = _plan(batch, [float(voltage)], tol=tol, max_iter=max_iter,
+                          bernoulli_name=bernoulli_name)
+        self.g = _gpu(batch)
+        self.bern = _lib.DD_BERNOULLI[bernoulli_name]
+        Bp, nodes, lanes = batch["Bp"], batch["np_max"] + 2, batch["lane_of"]
+        cuda = self.g.stat.device
+        eps = np.zeros((nodes, Bp))
+        for k, d in enumerate(batch["devices"]):
+            eps[:len(d.x), lanes[k]] = d.eps
+        self.eps = torch.from_numpy(eps).to(cuda)
+        self.vint = torch.full((Bp,), float(voltage), dtype=torch.float64, device=cuda)
+        laps = np.zeros((len(frequencies), 2))
+        laps[:, 1] = 2 * np.pi * np.asarray(frequencies, dtype=float)
+        self.laps = torch.from_numpy(laps).to(cuda)
+        self.nf = len(frequencies)
+        self.Y = torch.empty((self.nf, 2, Bp), dtype=torch.float64, device=cuda)
+        size = ctypes.c_size_t(0)
+        desc = descriptor(batch, self.g, self.plan.y0)
+        _lib.check(_lib.lib().dd_admittance_workspace_bytes(ctypes.byref(desc), self.nf,
+                                                           ctypes.byref(size)),
+                   "dd_admittance_workspace_bytes")
+        self.ws = torch.empty(size.value, dtype=torch.uint8, device=cuda)
+
+    def run(self):
+        import torch
+        from .adjoint import solve_states as _solve_states
+        g = self.g
+        J, ok, _, ckpt = _solve_states(self.plan, g.stat, g.scal, g.iface)
+        state = ckpt["states"][0]
+        desc = descriptor(self.batch, g, state)
+        _lib.check(_lib.lib().dd_admittance(
+            ctypes.byref(desc), state.data_ptr(), self.eps.data_ptr(), self.vint.data_ptr(),
+            self.laps.data_ptr(), self.nf, self.bern, self.Y.data_ptr(), self.ws.data_ptr(),
+            self.ws.numel(), torch.cuda.current_stream(g.stat.device).cuda_stream),
+            "dd_admittance")
+        return J, ok, self.Y
+
+
+def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float = 1e-10,
+                    max_iter: int = 60, bernoulli_name: str = "exact") -> ImpedanceResult:
+    """The impedance of a batch at the internal voltage `voltage` (V) at each of `frequencies`
+    (Hz), from the steady state there by one complex linear solve per frequency (jaxdd
+    impedance.py:365-409). Devices with mobile ions are refused (`NotImplementedError`): their
+    small-signal response needs the ions as unknowns of their own, which this build does not
+    carry."""
+    devs = batch["devices"]
+    if any(d.anion_total > 0 or d.cation_total > 0 for d in devs):
+        raise NotImplementedError("impedance with mobile ions: not built (the ions' own "
+                                  "equations in the small-signal system)")
+    if batch["ka"] != 1 or batch["kc"] != 1:
+        raise NotImplementedError("impedance with ion regions")
+    frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
+    work = Work(batch, frequencies, voltage, tol=tol, max_iter=max_iter,
+                bernoulli_name=bernoulli_name)
+    J, ok, Y = work.run()
+    lanes = batch["lane_of"]
+    p = work.plan
+    Yc = Y.cpu().numpy()
+    Yd = (Yc[:, 0, :] + 1j * Yc[:, 1, :])[:, lanes].T
+    offsets = p.offsets.cpu().numpy()[lanes]
+    Jd = J.cpu().numpy()[offsets]
+    okd = ok.cpu().numpy()[offsets].astype(bool)
+    Z = 1.0 / (Yd + batch["G_shunt"][:, None]) + batch["R_series"][:, None]
+    return ImpedanceResult(frequencies=frequencies, Z=Z, Y=Yd, J=Jd, converged=okd)

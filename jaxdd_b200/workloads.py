@@ -25,7 +25,7 @@ import numpy as np
 from .device import build_device
 from .simss_input import setup_from_texts
 
-__all__ = ["pin_stack", "drawn_stack", "drawn_devices", "SEED_DRAWN", "V_SCAN", "ragged_plan",
+__all__ = ["pin_stack", "pin_texts", "drawn_stack", "drawn_devices", "SEED_DRAWN", "V_SCAN", "ragged_plan",
            "ragged_voltages", "drawn_device"]
 
 #: Seed of the per-device draws (workloads 2 and 3).
@@ -64,7 +64,12 @@ def _setup(NP: int, pre: tuple[int, float, int] = (0, 0.0, 0)) -> str:
 
 def pin_stack(NP: int = 300):
     """The p-i-n cell of workload 1, built (jaxdd's graded grid)."""
-    texts = {
+    return build_device(setup_from_texts(pin_texts(NP)))
+
+
+def pin_texts(NP: int = 300) -> dict[str, str]:
+    """The SIMsalabim input texts of workload 1's p-i-n cell."""
+    return {
         "simulation_setup.txt": _setup(NP),
         "L1.txt": _layer(L="20e-9", eps_r="3.5", E_c="2.6", E_v="5.6", mu_n="1e-6", mu_p="1e-6",
                          N_A="1e22"),
@@ -74,7 +79,6 @@ def pin_stack(NP: int = 300):
         "L3.txt": _layer(L="30e-9", eps_r="10", E_c="4.0", E_v="7.2", mu_n="1e-5", mu_p="1e-5",
                          N_D="1e22"),
     }
-    return build_device(setup_from_texts(texts))
 
 
 def _logu(rng, lo, hi):

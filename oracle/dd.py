@@ -132,7 +132,7 @@ def _one(dev) -> dict:
         "s": _stencils(dev), "ti": {k: np.asarray(ti[k], dtype=float) for k in _TI_KEYS},
         "ion": {"hL": dev.h[:-1] * dev.L, "a_slots": a_slots, "a_totals": a_totals,
                 "c_slots": c_slots, "c_totals": c_totals},
-        "Vt": dev.Vt, "g_frac": dev.G_frac, "L": dev.L, "x": dev.x, "h": dev.h,
+        "Vt": dev.Vt, "g_frac": dev.G_frac, "L": dev.L, "x": dev.x, "h": dev.h, "eps": dev.eps,
         "N_c": dev.N_c, "ni": dev.ni, "E_c": dev.E_c, "V0": dev.V0, "VL": dev.VL,
         "W_L": dev.W_L, "W_R": dev.W_R,
         "ln_n_left": np.log(dev.n_left), "ln_n_right": np.log(dev.n_right),

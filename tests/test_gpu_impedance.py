@@ -1,0 +1,67 @@
+"""`solve_impedance` on the GPU (`dd_admittance`) against the oracle's restatement of jaxdd's
+`_admittance` (with bulk and interface traps following at their own rates), and the reference's
+known answers on the GPU's own results: the steady slope at a very low frequency (against the
+GPU's `solve_states` differenced), the geometric capacitance far above every relaxation."""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from jaxdd_b200 import prepare, solve_states  # noqa: E402
+from jaxdd_b200.device import build_device  # noqa: E402
+from jaxdd_b200.impedance import solve_impedance  # noqa: E402
+from jaxdd_b200.simss_input import setup_from_texts  # noqa: E402
+from jaxdd_b200.workloads import drawn_texts, pin_texts  # noqa: E402
+from oracle import impedance as imp  # noqa: E402
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
+
+F = np.array([1.0, 1e3, 1e5, 1e6, 1e9])
+
+
+def _devices(NP=100):
+    """The p-i-n cell, with interface traps, and two of the drawn stacks without their ions."""
+    out = [build_device(setup_from_texts(pin_texts(NP)))]
+    t = pin_texts(NP)
+    for name in ("L1.txt", "L2.txt"):
+        t[name] = t[name].replace("N_t_int = 0", "N_t_int = 1e15")
+    out.append(build_device(setup_from_texts(t)))
+    for k in (1, 3):
+        t = drawn_texts(k, np.random.default_rng([20261203, k]), NP)
+        for key in ("N_anion", "N_cation", "mu_anion", "mu_cation"):
+            t["L2.txt"] = "\n".join(f"{key} = 0" if line.split("=")[0].strip() == key else line
+                                    for line in t["L2.txt"].splitlines()) + "\n"
+        t["L2.txt"] = t["L2.txt"].replace("ionsMayEnter = 1", "ionsMayEnter = 0")
+        out.append(build_device(setup_from_texts(t)))
+    return out
+
+
+def test_admittance_matches_the_oracle():
+    devs = _devices()
+    r = solve_impedance(prepare(devs), F, voltage=0.7)
+    Yo, Zo, Jo, oko = imp.solve_impedance(devs, F, voltage=0.7)
+    assert np.array_equal(r.converged, oko) and r.converged.all()
+    rel = np.abs(r.Y - Yo) / np.abs(Yo)
+    assert np.max(rel) < 1e-6, rel
+    np.testing.assert_allclose(r.Z, Zo, rtol=1e-6)
+
+
+def test_the_limits_on_the_gpu():
+    devs = _devices()[:2]
+    V0, dV = 0.6, 1e-5
+    r = solve_impedance(prepare(devs), [1e-7, 1e14], voltage=V0, tol=1e-12, max_iter=200)
+    st = solve_states(prepare(devs), [V0 - dV, V0 + dV], tol=1e-12, max_iter=200)
+    slope = (st["J"][:, 1] - st["J"][:, 0]) / (2 * dV)
+    np.testing.assert_allclose(r.Y[:, 0].real, slope, rtol=1e-6)
+    for k, d in enumerate(devs):
+        x, eps = np.asarray(d.x), np.asarray(d.eps)
+        geometric = 1.0 / np.sum(np.diff(x) * 0.5 * (1 / eps[:-1] + 1 / eps[1:]))
+        assert r.capacitance[k, 1] == pytest.approx(geometric, rel=1e-4)
+
+
+def test_mobile_ions_are_refused():
+    from jaxdd_b200.workloads import drawn_devices
+    with pytest.raises(NotImplementedError, match="mobile ions"):
+        solve_impedance(prepare(drawn_devices(2, NP=50)), [1e3])

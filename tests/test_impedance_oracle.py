@@ -1,0 +1,55 @@
+"""The impedance oracle (`oracle/impedance.py`) against the reference's own known answers
+(jaxdd tests/test_impedance.py): at a very low frequency the admittance is the steady J-V
+curve's slope, far above every relaxation the capacitance is the layers' geometric one,
+1/∫dx/ε; `Z = 1/(Y + G_shunt) + R_series`. On workload 1's p-i-n cell, with and without
+interface traps."""
+
+import numpy as np
+import pytest
+
+from jaxdd_b200.device import build_device
+from jaxdd_b200.simss_input import setup_from_texts
+from jaxdd_b200.workloads import pin_texts
+from oracle import dd
+from oracle import impedance as imp
+
+
+def _cell(NP=60, interface=False):
+    texts = pin_texts(NP)
+    if interface:
+        for name in ("L1.txt", "L2.txt"):
+            texts[name] = texts[name].replace("N_t_int = 0", "N_t_int = 1e15")
+    return build_device(setup_from_texts(texts))
+
+
+@pytest.mark.parametrize("interface", [False, True])
+def test_low_frequency_is_the_steady_slope(interface):
+    dev = _cell(interface=interface)
+    V0, dV = 0.6, 1e-5
+    Y, _, _, ok = imp.solve_impedance([dev], [1e-7], voltage=V0, tol=1e-12, max_iter=200)
+    st = dd.solve_states(dd.prepare([dev]), [V0 - dV, V0 + dV], tol=1e-12, max_iter=200)
+    slope = (st["J"][0, 1] - st["J"][0, 0]) / (2 * dV)
+    assert ok.all()
+    assert Y[0, 0].real == pytest.approx(slope, rel=1e-6)
+    assert abs(Y[0, 0].imag) < 1e-4 * abs(slope)
+
+
+def test_high_frequency_is_the_geometric_capacitance():
+    dev = _cell()
+    x, eps = np.asarray(dev.x), np.asarray(dev.eps)
+    geometric = 1.0 / np.sum(np.diff(x) * 0.5 * (1 / eps[:-1] + 1 / eps[1:]))
+    f = np.array([1e6, 1e14])
+    Y, _, _, _ = imp.solve_impedance([dev], f, voltage=0.6)
+    C = Y.imag / (2 * np.pi * f)
+    assert C[0, 1] == pytest.approx(geometric, rel=1e-4)
+    assert C[0, 0] > C[0, 1]
+
+
+def test_the_series_resistance_and_the_shunt():
+    texts = pin_texts(60)
+    texts["simulation_setup.txt"] = (texts["simulation_setup.txt"]
+                                     .replace("R_shunt = -1", "R_shunt = 0.1")
+                                     .replace("R_series = 0", "R_series = 1e-4"))
+    dev = build_device(setup_from_texts(texts))
+    Y, Z, _, _ = imp.solve_impedance([dev], [1e3, 1e6], voltage=0.3)
+    np.testing.assert_allclose(Z, 1.0 / (Y + 10.0) + 1e-4, rtol=1e-12)
