@@ -437,6 +437,60 @@ def impedance_bench(args, rank: int, world: int, local: int) -> None:
         torch.distributed.destroy_process_group()
 
 
+def build_bench(args, rank: int, world: int, local: int) -> None:
+    """Device building on the GPU (`dd_build`): the packed records of 16384 devices of one
+    structure (the drawn stacks pre-biased at 1.0 V, NP 400) from their parameter tables, against
+    the host builder and packer of one device on one core."""
+    import torch
+    from jaxdd_b200.batch import prepare
+    from jaxdd_b200.building import SweepStructure, build, parameters
+    from jaxdd_b200.device import build_device
+    from jaxdd_b200.simss_input import setup_from_texts
+    from jaxdd_b200.workloads import SEED_DRAWN, drawn_texts
+    n = args.devices
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    ks = [2 * i for i in range(n)]
+    setups = [setup_from_texts(drawn_texts(k, np.random.default_rng([SEED_DRAWN, k]), args.np))
+              for k in ks]
+    st = SweepStructure(setups[0])
+    P, D = parameters(st, setups)
+    read_s = time.perf_counter() - t0
+    # the host's rate: build and pack a bounded sample on one core
+    sample = setups[:64]
+    t1 = time.perf_counter()
+    for s in sample:
+        prepare([build_device(s, layout=st.layout)])
+    host_rate = len(sample) / (time.perf_counter() - t1)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        out = build(st, P, D)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        out = build(st, P, D)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if rank == 0:
+        nbytes = sum(t.numel() * 8 for t in out[:4])
+        print(json.dumps({
+            "metric": METRIC, "value": n / (ms / 1e3), "unit": "devices built/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{n} drawn p-i-n stacks (seed 20261203) of one structure, "
+                                   f"NP {args.np}: packed record and start state from parameter "
+                                   "tables (parameter upload, the record's allocation and "
+                                   "defaults, dd_build)",
+                       "record_bytes": nbytes, "parse_s": round(read_s, 1)},
+            "cpu_baseline": {"value": host_rate, "unit": "devices built/s", "cores": 1,
+                             "kind": "port",
+                             "sample": f"{len(sample)} devices through build_device + prepare"},
+        }), flush=True)
+
+
 def workload_name(args, batch, nflat: int) -> str:
     if args.workload == "uneven":
         NPs = batch["NP"]
@@ -457,7 +511,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--precision", default="fp64", choices=("fp64",))
     ap.add_argument("--workload", default="config2",
-                    choices=("config2", "uneven", "adjoint", "impedance"),
+                    choices=("config2", "uneven", "adjoint", "impedance", "build"),
                     help="config2: 16384 devices, NP 400, 61 V (the default); uneven: 32768 "
                          "devices, NP ~ U{150..900}, Nv ~ U{21..121}, one launch; adjoint: "
                          "gradients of a J-V misfit in 14 parameters, 4096 devices; "
@@ -484,6 +538,9 @@ def main() -> None:
         return
     if args.workload == "impedance":
         impedance_bench(args, rank, world, local)
+        return
+    if args.workload == "build":
+        build_bench(args, rank, world, local)
         return
     if args.devices % 32:
         raise SystemExit("--devices must be a multiple of 32")

@@ -168,6 +168,55 @@ int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
                   const double* vint, const double* laps, int n_freq, int bernoulli, double* Y,
                   void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- Device building on the GPU (parameter sweeps) ------------------------------------------
+ * The packed record of n devices of one stack structure from their parameters, as jaxdd's
+ * `device_tree(structure, params)` (batch.py:142-148, device.py:877-1063) builds them for sweeps:
+ * the points per layer fixed, the spacings scaled by the thicknesses. */
+#define DD_MAXLAYERS 16
+
+/* Per-layer parameters, layer_params[layer][DD_LF][n] (SI units, energies in eV). */
+enum dd_layer_field {
+  DD_L_L = 0, DD_L_EPS, DD_L_EC, DD_L_EV, DD_L_NC, DD_L_ND, DD_L_NA, DD_L_MUN, DD_L_MUP,
+  DD_L_KD, DD_L_NTB, DD_L_ETB, DD_L_CNB, DD_L_CPB, DD_L_NUN, DD_L_NUP, DD_L_NTI, DD_L_ETI,
+  DD_L_CNI, DD_L_CPI, DD_L_G, DD_L_NAN, DD_L_NCA, DD_LF
+};
+/* Per-device parameters, device_params[DD_DF][n]: temperature, work functions (unused where the
+ * structure's contact is flat-band), generation factor, shunt resistance, pre-bias voltage, and
+ * the first voltage the start state y0 is made for. */
+enum dd_device_field {
+  DD_D_T = 0, DD_D_WL, DD_D_WR, DD_D_GFRAC, DD_D_RSHUNT, DD_D_VPRE, DD_D_FIRST, DD_DF
+};
+
+/* What the devices of a sweep share (device pointers): the grid's layout (jaxdd's `Structure`,
+ * device.py:386-575) and the flags the layers' parameters do not change. */
+typedef struct dd_structure {
+  int32_t np, n_layers;
+  const int32_t* lid;        /* [np+2] each point's layer */
+  const double* raw;         /* [np+2] unscaled spacings */
+  const double* norm;        /* [n_layers] each layer's sum of raw spacings */
+  const int32_t* i0;         /* [n_layers] each layer's first point */
+  const int32_t* i1;         /* [n_layers] each layer's last point */
+  const uint8_t* at_iface;   /* [np+2] a layer's last point before the next layer */
+  const double* ifk;         /* [np+2] the interface index field of the record (dd_layout.h) */
+  const double* aslot;       /* [n_layers] the layer's mobile anion slot, -1 none */
+  const double* cslot;       /* [n_layers] cation slot, -1 none */
+  const uint8_t* afixed;     /* [n_layers] the layer's anions are fixed */
+  const uint8_t* cfixed;     /* [n_layers] */
+  const int32_t* iface_row;  /* [n_layers] row of the trapped join after the layer, -1 none */
+  const double* iface_kind;  /* [n_layers] that join's trap type (-1, 0, 1) */
+  int32_t sfb_left, sfb_right;  /* the contact's work function is its layer's flat-band one */
+  double left_elec, pre_cond, fix_ions, curr_diff, mid;
+} dd_structure;
+
+/* Build the packed record (stat, scal, iface; and y0 at each device's DD_D_FIRST voltage unless
+ * NULL) of n_devices devices in lanes 0..n_devices-1 of arrays of `lane_stride` lanes. Workspace:
+ * (np+2) * n_devices doubles. The record equals jaxdd_b200's host packer's for the same devices
+ * but for the pairwise sums of the spacings and of the current scale (a few ulp). */
+int dd_build(const dd_structure* structure, const double* layer_params,
+             const double* device_params, int n_devices, int lane_stride, int k_anion,
+             int k_cation, double* stat, double* scal, double* iface, double* y0,
+             void* workspace, size_t workspace_bytes, void* stream);
+
 /* One damped Newton step per lane from the state y (`[(np_max+2)][3][lane_stride]`, interior
  * nodes used) and the ion normalisations logs (`[K][lane_stride]`) at the voltage Vint
  * (`[lane_stride]`), ions scaled by `share`: jaxdd's `_newton_step` (solver.py:1563-1608),

@@ -36,7 +36,15 @@ DD_LANE_PREBIAS_FAILED = 1
 #: every symbol include/jaxdd_b200.h declares
 EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve",
            "dd_newton_step", "dd_solve_noalloc", "dd_solve_states", "dd_adjoint_workspace_bytes",
-           "dd_adjoint", "dd_observables", "dd_admittance_workspace_bytes", "dd_admittance")
+           "dd_adjoint", "dd_observables", "dd_admittance_workspace_bytes", "dd_admittance",
+           "dd_build")
+
+#: include/jaxdd_b200.h's per-layer and per-device parameter fields of dd_build
+LAYER_FIELDS = ("L", "eps_r", "E_c", "E_v", "N_c", "N_D", "N_A", "mu_n", "mu_p", "k_direct",
+                "N_t_bulk", "E_t_bulk", "C_n_bulk", "C_p_bulk", "nu_int_n", "nu_int_p",
+                "N_t_int", "E_t_int", "C_n_int", "C_p_int", "G_ehp", "N_anion", "N_cation")
+DEVICE_FIELDS = ("T", "W_L", "W_R", "G_frac", "R_shunt", "Vpre", "first")
+DD_MAXLAYERS = 16
 
 #: dd_solve_noalloc's fixed scratch (include/jaxdd_b200.h DD_NOALLOC_SCRATCH_BYTES)
 DD_NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -52,6 +60,16 @@ class DdBatch(ctypes.Structure):
 
 class DdVoltages(ctypes.Structure):
     _fields_ = [("v", ctypes.c_void_p), ("offset", ctypes.c_void_p), ("count", ctypes.c_void_p)]
+
+
+class DdStructure(ctypes.Structure):
+    _fields_ = [("np", ctypes.c_int32), ("n_layers", ctypes.c_int32)] + [
+        (name, ctypes.c_void_p) for name in ("lid", "raw", "norm", "i0", "i1", "at_iface", "ifk",
+                                             "aslot", "cslot", "afixed", "cfixed", "iface_row",
+                                             "iface_kind")] + [
+        ("sfb_left", ctypes.c_int32), ("sfb_right", ctypes.c_int32),
+        ("left_elec", ctypes.c_double), ("pre_cond", ctypes.c_double),
+        ("fix_ions", ctypes.c_double), ("curr_diff", ctypes.c_double), ("mid", ctypes.c_double)]
 
 
 class DdOpts(ctypes.Structure):
@@ -99,6 +117,9 @@ def lib() -> ctypes.CDLL:
     so.dd_admittance.restype = ctypes.c_int
     so.dd_admittance.argtypes = [ctypes.POINTER(DdBatch), p, p, p, p, ctypes.c_int, ctypes.c_int,
                                  p, p, ctypes.c_size_t, p]
+    so.dd_build.restype = ctypes.c_int
+    so.dd_build.argtypes = [ctypes.POINTER(DdStructure), p, p, ctypes.c_int, ctypes.c_int,
+                            ctypes.c_int, ctypes.c_int, p, p, p, p, p, ctypes.c_size_t, p]
     so.dd_solve_noalloc.restype = ctypes.c_int
     so.dd_solve_noalloc.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
                                     ctypes.POINTER(DdOpts), p, p, p, p, p, p]
