@@ -121,3 +121,15 @@ def test_uneven_plan_and_padded_concat():
         solve_uneven(small, [V] * 31)
     with pytest.raises(ValueError):
         solve_uneven(small, [V] * 31 + [[]])
+
+
+def test_the_header_compiles_as_c():
+    """The C ABI's header is plain C99: a C, cgo or FFI caller can include it."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    r = subprocess.run([gcc, "-x", "c", "-std=c99", "-Wall", "-Werror", "-fsyntax-only",
+                        str(ROOT / "include" / "jaxdd_b200.h")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
