@@ -19,10 +19,12 @@ import numpy as np
 __all__ = [
     "Layer",
     "Setup",
+    "TVG",
     "check_supported",
     "ion_regions",
     "parse_parameters",
     "read_setup",
+    "read_tvg",
     "setup_from_texts",
     "simss_voltages",
 ]
@@ -145,6 +147,117 @@ def simss_voltages(setup: Setup) -> np.ndarray:
         d = acc - vmax
         v = acc - d * np.exp((1 - np.arange(count) / (count - 1)) * np.log((acc - vmin) / d))
     return v[::-1].copy() if vscan == -1 else v
+
+
+#: ln of the largest real SIMsalabim's Pascal code handles (extended precision): the voltage's
+#: bound in `read_tvg`, |V/V_T| < 1.95 of it.
+LN_MAX_EXTENDED = 11356.523406294143
+
+
+@dataclass(frozen=True)
+class TVG:
+    """ZimT's time steps (`tVGFile`, jaxdd simss_input.py:155-175): at each time `t` (s) the
+    voltage `Vext` (V; NaN where `oc`, the open circuit), `G_frac` and `track` (0–3, ZimT's
+    automatic stop); `dti` 1/Δt from the step before, 0 at `t = 0` (a steady state). With
+    them the setup's `failureMode` (0 stop at a failed step, 1 keep it, 2 skip it), `convVar`
+    and the tolerances that compare two states (`tolPois` V, `tolDens`, `tolCurr` A/m²)."""
+
+    t: np.ndarray
+    Vext: np.ndarray
+    oc: np.ndarray
+    G_frac: np.ndarray
+    track: np.ndarray
+    dti: np.ndarray
+    failure_mode: int = 1
+    conv_var: int = 1
+    tol_pois: float = 1e-6
+    tol_dens: float = 1e-6
+    tol_curr: float = 1e-3
+
+    @classmethod
+    def steps(cls, t, Vext, G_frac=1.0, track=0, failure_mode: int = 1) -> "TVG":
+        """Time steps from arrays (the first at `t = 0`), as `read_tvg` would read them."""
+        t = np.asarray(t, dtype=float)
+        n = t.shape[0]
+        Vext, G_frac, track = (np.broadcast_to(np.asarray(a), (n,)).copy()
+                               for a in (Vext, G_frac, track))
+        if n == 0 or t[0] != 0:
+            raise ValueError("tVGFile did not specify steady-state (t=0)")
+        dti, previous = np.zeros(n), 0.0
+        for k, tk in enumerate(t):
+            if tk > previous:
+                dti[k] = 1.0 / (tk - previous)
+            elif tk != 0:
+                raise ValueError("Time steps must either be positive, or you should go back to "
+                                 f"t=0 (steady-state); at t = {tk}")
+            previous = tk
+        return cls(t=t, Vext=Vext.astype(float), oc=np.zeros(n, bool),
+                   G_frac=G_frac.astype(float), track=track.astype(int), dti=dti,
+                   failure_mode=int(failure_mode))
+
+
+def read_tvg(setup: Setup) -> TVG:
+    """ZimT 5.36's `tVGFile` (jaxdd simss_input.py:178-237): lines up to the header
+    `t Vext G_frac Track` skipped, then one step per line up to the end or an empty line,
+    columns past the fourth ignored. ZimT's checks raise `ValueError`: the header, a first step
+    at `t = 0`, times that go forward or back to 0, a voltage within range, `Track` 0–3 with a
+    1 (not on the first line, which ZimT forgets) before any 2 or 3."""
+    name = setup.raw["tVGFile"]
+    lines = iter(setup.text("tVGFile").splitlines())
+    for line in lines:
+        if "".join(line.lower().split()).startswith("tvextg_fractrack"):
+            break
+    else:
+        raise ValueError(f"Could not find correct header 't Vext G_frac Track' in {name}.")
+    from jaxdd_b200.constants import K_B, Q
+
+    vti = Q / (K_B * setup.f("T"))
+    rows: list[tuple] = []
+    previous, seen_one = 0.0, False
+    for line in lines:
+        words = line.split()
+        if not words:
+            break
+        t_s, v_s, g_s, track_s = (words + [""] * 4)[:4]
+        try:
+            t, g = float(t_s), float(g_s)
+            oc = v_s.lower() == "oc"
+            v = np.nan if oc else float(v_s)
+            if track_s not in ("0", "1", "2", "3"):
+                raise ValueError
+        except ValueError:
+            raise ValueError(f"Error while reading from file {name}; offending line: {line!r}") \
+                from None
+        if t > previous:
+            dti = 1.0 / (t - previous)
+        elif t == 0:
+            dti = 0.0
+        else:
+            raise ValueError("Time steps must either be positive, or you should go back to t=0 "
+                             f"(steady-state); at t = {t}")
+        if not oc and abs(v * vti) > 1.95 * LN_MAX_EXTENDED:
+            raise ValueError(f"V is too {'small' if v < 0 else 'large'}; at t = {t}")
+        if rows and track_s == "1":
+            seen_one = True
+        if track_s in ("2", "3") and not seen_one:
+            raise ValueError("Error in tVGFile: before setting Track=2 or 3, you need to have at "
+                             "least one Track=1")
+        rows.append((t, v, oc, g, int(track_s), dti))
+        previous = t
+    if not rows or rows[0][0] != 0:
+        raise ValueError("tVGFile did not specify steady-state (t=0)")
+    t, v, oc, g, track, dti = (np.array(c) for c in zip(*rows))
+    failure_mode, conv_var = int(setup.raw.get("failureMode", 1)), int(setup.raw.get("convVar", 1))
+    if failure_mode not in (0, 1, 2):
+        raise ValueError("Invalid failureMode selected.")
+    if conv_var not in (1, 2, 3, 4):
+        raise ValueError("Invalid convVar selected.")
+    return TVG(t=t.astype(float), Vext=v.astype(float), oc=oc.astype(bool),
+               G_frac=g.astype(float), track=track.astype(int), dti=dti.astype(float),
+               failure_mode=failure_mode, conv_var=conv_var,
+               tol_pois=float(setup.raw.get("tolPois", 1e-6)),
+               tol_dens=float(setup.raw.get("tolDens", 1e-6)),
+               tol_curr=float(setup.raw.get("tolCurr", 1e-3)))
 
 
 def ion_regions(setup: Setup, species: str) -> list[tuple[int, int, bool]]:

@@ -138,6 +138,8 @@ def _one(dev) -> dict:
         "ln_n_left": np.log(dev.n_left), "ln_n_right": np.log(dev.n_right),
         "ln_p_left": np.log(dev.p_left), "ln_p_right": np.log(dev.p_right),
         "offset_n": dev.offset_n, "offset_p": dev.offset_p, "mu_n": dev.mu_n, "mu_p": dev.mu_p,
+        "mu_a": np.zeros(NP + 2) if dev.mu_anion is None else np.asarray(dev.mu_anion, float),
+        "mu_c": np.zeros(NP + 2) if dev.mu_cation is None else np.asarray(dev.mu_cation, float),
         "G": dev.G,
         "rec": {"kd": dev.k_direct, "ni2": dev.ni ** 2, "Nt": dev.srh_Nt, "Cn": dev.srh_Cn,
                 "Cp": dev.srh_Cp, "nt0": dev.srh_nt0, "pt0": dev.srh_pt0},

@@ -25,13 +25,16 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 
-#: The reference's SimSS test cases inside this build's scope (steady state, Boltzmann, no
-#: surface recombination, no field dependence, no trap files, no charged bulk traps).
+#: The reference's SimSS and ZimT test cases inside this build's scope (Boltzmann, no surface
+#: recombination, no field dependence, no trap files, no charged bulk traps).
 CASES = (
     "thin_l1_light", "frozen_1e17_x1_thin_light", "steady_1e17_thin_light", "held_thin_light",
     "iface_charged_light", "iface_ions_light", "pin_iface_light", "region_etl_light",
     "region_htl_frozen_light", "two_regions_light", "frozen_thick_htl_dark", "diff_iface_light",
     "none_light", "resist_light", "logv_light",
+    # ZimT 5.36 transients (with their tVG.txt and ZimT's tj.dat): electrons and holes, the
+    # absorber's traps, and mobile ions over 2 x 50 ms and 2 x 5 s
+    "zimt_photo_light", "zimt_traps_photo_light", "zimt_ions_fast_light", "zimt_ions_slow_light",
 )
 
 

@@ -1,0 +1,125 @@
+"""The transient oracle pinned on ZimT 5.36's own transients (the reference's tests/data, copied
+to tests/golden/inputs): `Jext` through 241 steps to the reference's tolerances
+(test_solver.py:544-581: 1e-9 of the scale for electrons and holes and for the traps, 1e-7 with
+mobile ions), ZimT's Bernoulli function and sums (`zimt_current`). Also: the tVG reader's checks,
+the traps' step against its closed form and its derivatives, the ions' number kept in every step,
+and the refusals of what is out of scope."""
+
+import numpy as np
+import pytest
+
+from jaxdd_b200.device import build_device
+from jaxdd_b200.simss_input import TVG, read_setup, read_tvg, setup_from_texts
+from oracle import dd, transient
+
+INPUTS = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "inputs"
+
+ZIMT = {"zimt_photo_light": 1e-9, "zimt_traps_photo_light": 1e-9,
+        "zimt_ions_fast_light": 1e-7, "zimt_ions_slow_light": 1e-7}
+
+
+def zimt_case(case):
+    setup = read_setup(INPUTS / case / "simulation_setup.txt")
+    return setup, read_tvg(setup), np.genfromtxt(INPUTS / case / "tj.dat", names=True)
+
+
+def zimt_transient(batch, tvg, steps=None):
+    S = len(tvg.t) if steps is None else steps
+    return transient.solve_transient(batch, tvg.t[:S], tvg.Vext[:S], tvg.G_frac[:S],
+                                     tvg.track[:S], tvg.failure_mode, bernoulli_name="simss",
+                                     zimt_current=True)
+
+
+@pytest.mark.parametrize("case", sorted(ZIMT))
+def test_the_oracle_reproduces_zimt(case):
+    setup, tvg, ref = zimt_case(case)
+    r = zimt_transient(dd.prepare([build_device(setup, grid="simss")]), tvg)
+    assert r["converged"].all() and r["accepted"].all() and r["stop"][0] == 0
+    scale = np.max(np.abs(ref["Jext"]))
+    assert np.max(np.abs(r["J_ext"][0] - ref["Jext"])) < ZIMT[case] * scale
+
+
+def test_the_ions_keep_their_number_in_every_step():
+    """Each region's rescaling is a slot of the bordered system: after every kept step the
+    anions' and cations' numbers are their totals (to Newton's tolerance)."""
+    setup, tvg, _ = zimt_case("zimt_ions_fast_light")
+    b = dd.prepare([build_device(setup, grid="simss")])
+    r = zimt_transient(b, tvg, steps=12)
+    full = transient.full_of(b, r["y"], np.array([tvg.Vext[11]]))
+    g, _, _ = transient.constraints(full, r["logs"], b["ion"])
+    masks, totals = dd._masks(b["ion"])
+    assert np.any(totals > 0)
+    assert np.max(np.abs(g)) < 1e-9
+
+
+def test_the_traps_step_is_the_closed_form_and_its_derivatives():
+    rng = np.random.default_rng(7)
+    Cn, Cp = 10 ** rng.uniform(-15, -13, 50), 10 ** rng.uniform(-15, -13, 50)
+    nt0, pt0 = 10 ** rng.uniform(10, 16, 50), 10 ** rng.uniform(10, 16, 50)
+    n, p = 10 ** rng.uniform(14, 22, 50), 10 ** rng.uniform(14, 22, 50)
+    f_old = rng.uniform(0, 1, 50)
+    # a steady state: both the steady occupation
+    (mean, end, vac), _, _ = transient.trap_step(Cn, Cp, nt0, pt0, n, p, f_old, 0.0)
+    a = Cn * (n + nt0) + Cp * (p + pt0)
+    np.testing.assert_allclose(mean, (Cn * n + Cp * pt0) / a, rtol=1e-15)
+    np.testing.assert_allclose(end, mean, rtol=0)
+    np.testing.assert_allclose(vac, (Cn * nt0 + Cp * p) / a, rtol=1e-15)
+    # over a step: f(t) = s + (f_old − s)·exp(−a t), its mean over the step
+    dti = 10 ** rng.uniform(2, 9, 50)
+    (mean, end, vac), d_n, d_p = transient.trap_step(Cn, Cp, nt0, pt0, n, p, f_old, dti)
+    s = (Cn * n + Cp * pt0) / a
+    np.testing.assert_allclose(end, s + (f_old - s) * np.exp(-a / dti), rtol=1e-12)
+    x = a / dti
+    # (1 − e^−x)/x as written loses digits at small x (the oracle takes expm1)
+    np.testing.assert_allclose(mean, s + (f_old - s) * (1 - np.exp(-x)) / x, rtol=1e-9)
+    np.testing.assert_allclose(mean + vac, 1.0, rtol=1e-12)
+    # the derivatives are ~1e-8 of values near 1: a central difference at h = 1e-4 (round-off
+    # 1e-12/h, truncation h²)
+    for k, deriv in ((0, d_n), (1, d_p)):
+        for j in range(3):
+            h = 1e-4
+            up = [n * (1 + h), p] if k == 0 else [n, p * (1 + h)]
+            dn = [n * (1 - h), p] if k == 0 else [n, p * (1 - h)]
+            fu = transient.trap_step(Cn, Cp, nt0, pt0, *up, f_old, dti)[0][j]
+            fd = transient.trap_step(Cn, Cp, nt0, pt0, *dn, f_old, dti)[0][j]
+            base = n if k == 0 else p
+            fdiff = (fu - fd) / (2 * h * base)
+            np.testing.assert_allclose(deriv[j], fdiff, rtol=1e-4,
+                                       atol=1e-12 * np.max(abs(fdiff)))
+
+
+def test_tvg_as_zimt_reads_it():
+    _, tvg, ref = zimt_case("zimt_ions_fast_light")
+    assert len(tvg.t) == 241 == len(ref) and tvg.t[0] == 0 and tvg.failure_mode == 0
+    np.testing.assert_allclose(tvg.t, ref["t"], rtol=1e-9)
+    assert tvg.dti[0] == 0 and np.allclose(tvg.dti[1:], 1 / np.diff(tvg.t))
+    base = (INPUTS / "zimt_photo_light" / "simulation_setup.txt").read_text()
+    files = {f.name: f.read_text() for f in (INPUTS / "zimt_photo_light").glob("*.txt")}
+
+    def tvg_of(text):
+        return read_tvg(setup_from_texts(dict(files, **{"simulation_setup.txt": base,
+                                                          "tVG.txt": text})))
+
+    assert len(tvg_of("t Vext G_frac Track\n0 0 1 0\n1e-6 0.5 1 1\n\n2 0 0 0\n").t) == 2
+    assert tvg_of("t Vext G_frac Track\n0 oc 1 0\n").oc[0]
+    for text, match in (("x y\n0 0 1 0\n", "header"),
+                        ("t Vext G_frac Track\n1 0 1 0\n", "steady-state"),
+                        ("t Vext G_frac Track\n0 0 1 0\n2 0 1 0\n1 0 1 0\n", "Time steps"),
+                        ("t Vext G_frac Track\n0 0 1 0\n1 0 1 4\n", "offending"),
+                        ("t Vext G_frac Track\n0 0 1 1\n1 0 1 2\n", "Track=1")):
+        with pytest.raises(ValueError, match=match):
+            tvg_of(text)
+    steps = TVG.steps([0, 1e-9, 1e-8], [0, 0.9, 0.9])
+    assert steps.dti[0] == 0 and np.isclose(steps.dti[2], 1 / 9e-9)
+    with pytest.raises(ValueError):
+        TVG.steps([1e-9, 1e-8], 0.9)
+
+
+def test_what_the_transient_refuses():
+    setup, tvg, _ = zimt_case("zimt_photo_light")
+    b = dd.prepare([build_device(setup, grid="simss")])
+    with pytest.raises(NotImplementedError, match="Track"):
+        transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3], [0, 1, 2])
+    b["R_series"] = np.array([1e-4])
+    with pytest.raises(NotImplementedError, match="series resistance"):
+        transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3])
