@@ -217,6 +217,64 @@ int dd_build(const dd_structure* structure, const double* layer_params,
              int k_cation, double* stat, double* scal, double* iface, double* y0,
              void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- Transients with mobile ions (jaxdd transient.py:270-465, 537-637) -------------------- */
+#define DD_NT 3 /* per-point transient record fields: permittivity, anion and cation mobility */
+
+/* ZimT's time steps (jaxdd `TVG`, simss_input.py:155-237). Lane l's step k is at
+ * [k * stride + (stride ? l : 0)]: one list for every lane (stride 0) or one per lane (stride =
+ * lane_stride). The first step is at t = 0 (a steady state); a later t = 0 returns to one. */
+typedef struct dd_steps {
+  int32_t n_steps;
+  int32_t stride;
+  const double* t;             /* s */
+  const double* v;             /* internal voltage, V */
+  const double* g_frac;        /* generation factor */
+  const int32_t* track;        /* ZimT's Track: 0 or 1 (2 and 3, the automatic stop, not built) */
+  const int32_t* failure_mode; /* [lane_stride]: 0 stop at a failed step, 1 keep it, 2 skip it */
+  int32_t zimt_sums;           /* 1: ZimT's sums in the integral current (each point's change over
+                                  the interval after it); 0: over its control volume (jaxdd's) */
+} dd_steps;
+
+/* Outputs of dd_transient (device pointers). Per step and lane [n_steps][lane_stride]: J (A/m^2,
+ * internal, SIMsalabim's sign), J_ext (with the shunt), converged, iterations, accepted (the
+ * step is kept: ZimT's tJFile rows); per lane stop (0 through every step, 2 at a failed step:
+ * failureMode 0, or 2 with Track 1). The last kept state: state [np_max+2][5][lane_stride]
+ * (V, ln n, ln p, ln a, ln c; the ions' 0 outside their regions), logs [DD_MAXK][lane_stride]
+ * (the slots' scales), f_bulk and f_iface [np_max+2][lane_stride] (the traps' occupations at
+ * the points and on the intervals; either may be NULL). */
+typedef struct dd_transient_out {
+  double* J;
+  double* J_ext;
+  uint8_t* converged;
+  int32_t* iterations;
+  uint8_t* accepted;
+  int32_t* stop;
+  double* state;
+  double* logs;
+  double* f_bulk;
+  double* f_iface;
+} dd_transient_out;
+
+/* Scratch bytes dd_transient needs for this batch. */
+int dd_transient_workspace_bytes(const dd_batch* batch, size_t* bytes);
+
+/* Every lane through its time steps: jaxdd's `solve_transient` (transient.py:537) with the
+ * voltage given at every step. Each step is a Newton solve of implicit Euler with the mobile ions
+ * as unknowns (5x5 blocks bordered by the ion slots, solver.py:1364-1475), the traps' occupations
+ * carried from step to step (solver.py:594-614), the current with each density's change, the
+ * ions' currents and the displacement current (batch.py:302-483), and ZimT's main loop
+ * (transient.py:419-445: which steps are kept, dt from the last kept one). `tstat`
+ * [np_max+2][DD_NT][lane_stride] the permittivity and the ions' mobilities at each point;
+ * `start` [np_max+2][3][lane_stride] and `start_logs` [DD_MAXK][lane_stride] the steady state
+ * at the first step (dd_solve_states at steps->v[0] with the generation factor
+ * steps->g_frac[0] and no pre-bias). opts: tol, max_iter (Newton per step), bernoulli. Not
+ * supported (the host refuses them): an open circuit, a series resistance, Track 2 or 3, ion
+ * regions that reach a contact. */
+int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* steps,
+                 const double* start, const double* start_logs, const dd_opts* opts,
+                 const dd_transient_out* out, void* workspace, size_t workspace_bytes,
+                 void* stream);
+
 /* One damped Newton step per lane from the state y (`[(np_max+2)][3][lane_stride]`, interior
  * nodes used) and the ion normalisations logs (`[K][lane_stride]`) at the voltage Vint
  * (`[lane_stride]`), ions scaled by `share`: jaxdd's `_newton_step` (solver.py:1563-1608),

@@ -37,7 +37,10 @@ DD_LANE_PREBIAS_FAILED = 1
 EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve",
            "dd_newton_step", "dd_solve_noalloc", "dd_solve_states", "dd_adjoint_workspace_bytes",
            "dd_adjoint", "dd_observables", "dd_admittance_workspace_bytes", "dd_admittance",
-           "dd_build")
+           "dd_build", "dd_transient_workspace_bytes", "dd_transient")
+
+#: the transient's per-point record fields (include/jaxdd_b200.h DD_NT)
+DD_NT = 3
 
 #: include/jaxdd_b200.h's per-layer and per-device parameter fields of dd_build
 LAYER_FIELDS = ("L", "eps_r", "E_c", "E_v", "N_c", "N_D", "N_A", "mu_n", "mu_p", "k_direct",
@@ -70,6 +73,18 @@ class DdStructure(ctypes.Structure):
         ("sfb_left", ctypes.c_int32), ("sfb_right", ctypes.c_int32),
         ("left_elec", ctypes.c_double), ("pre_cond", ctypes.c_double),
         ("fix_ions", ctypes.c_double), ("curr_diff", ctypes.c_double), ("mid", ctypes.c_double)]
+
+
+class DdSteps(ctypes.Structure):
+    _fields_ = [("n_steps", ctypes.c_int32), ("stride", ctypes.c_int32), ("t", ctypes.c_void_p),
+                ("v", ctypes.c_void_p), ("g_frac", ctypes.c_void_p), ("track", ctypes.c_void_p),
+                ("failure_mode", ctypes.c_void_p), ("zimt_sums", ctypes.c_int32)]
+
+
+class DdTransientOut(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in (
+        "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs", "f_bulk",
+        "f_iface")]
 
 
 class DdOpts(ctypes.Structure):
@@ -120,6 +135,13 @@ def lib() -> ctypes.CDLL:
     so.dd_build.restype = ctypes.c_int
     so.dd_build.argtypes = [ctypes.POINTER(DdStructure), p, p, ctypes.c_int, ctypes.c_int,
                             ctypes.c_int, ctypes.c_int, p, p, p, p, p, ctypes.c_size_t, p]
+    so.dd_transient_workspace_bytes.restype = ctypes.c_int
+    so.dd_transient_workspace_bytes.argtypes = [ctypes.POINTER(DdBatch),
+                                                ctypes.POINTER(ctypes.c_size_t)]
+    so.dd_transient.restype = ctypes.c_int
+    so.dd_transient.argtypes = [ctypes.POINTER(DdBatch), p, ctypes.POINTER(DdSteps), p, p,
+                                ctypes.POINTER(DdOpts), ctypes.POINTER(DdTransientOut), p,
+                                ctypes.c_size_t, p]
     so.dd_solve_noalloc.restype = ctypes.c_int
     so.dd_solve_noalloc.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
                                     ctypes.POINTER(DdOpts), p, p, p, p, p, p]

@@ -18,7 +18,8 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB_DIR = HERE / "lib"
 LIB = LIB_DIR / "libjaxdd_b200.so"
-SOURCES = ["dd_solve.cu", "dd_adjoint.cu", "dd_states.cu", "dd_impedance.cu", "dd_build.cu"]
+SOURCES = ["dd_solve.cu", "dd_adjoint.cu", "dd_states.cu", "dd_impedance.cu", "dd_build.cu",
+           "dd_transient.cu"]
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
     "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-shared",

@@ -112,8 +112,9 @@ __device__ void lane_init(Lane& L, const Args& a, int l) {
   L.NP = (int)L.sc(C_NP);
   L.mid = (int)L.sc(C_MID);
   L.currdiff = L.sc(C_CURRDIFF) > 0.0; L.simss = a.simss;
+  // the slots' totals: rows past k_anion + k_cation need not exist in scal
 #pragma unroll
-  for (int k = 0; k < K; ++k) L.tot[k] = L.sc(C_TOT0 + k);
+  for (int k = 0; k < K; ++k) L.tot[k] = k < a.ka + a.kc ? L.sc(C_TOT0 + k) : 0.0;
   L.FX = a.FX; L.CD = nullptr; L.ncd = 0;
   L.ybuf = 0;
   L.frozen = false;

@@ -1,0 +1,1080 @@
+// Transients with mobile ions on the GPU: jaxdd's `solve_transient` (src/jaxdd/transient.py:
+// 270-465, 537-637) for the product's scope, every device through all its time steps in one
+// launch.
+//
+// What: each step is one Newton solve of implicit Euler with the ions as unknowns of their own,
+// (V, ln n, ln p, ln a, ln c) per point (`solver._assemble_ions`, solver.py:1364-1475): 5x5
+// block-tridiagonal rows bordered by the ion slots, whose rows are each region's number of ions
+// over its total (`_ion_constraints_time`, solver.py:1349-1361). The bulk and interface traps'
+// occupations are carried from step to step and solved exactly over each step
+// (`_trap_step`, solver.py:594-614); each carrier is captured by the occupation's mean over the
+// step. The current adds each density's change to the integral form's integrand, the ions'
+// currents region by region and the displacement current (batch.py:302-483). ZimT's main loop
+// decides which steps are kept (`failureMode`), and each step's dt is from the last kept one.
+//
+// How: one thread per device (lane), its state in three lane-interleaved buffers
+// [node][5][lane] (kept, the one kept before it, the Newton iterate) whose roles rotate when a
+// step is kept. A Newton iteration is four passes over the device's points: assembly and forward
+// elimination (each 5x5 block solved by its partition as the reference's `_inverse5`: the
+// carriers' 3x3 block by its adjugate, then the ions' 2x2 Schur complement), back substitution
+// with the slots' K x K Schur complement, the damped update, and the current at the new iterate.
+// The static record is the steady solve's (dd_layout.h); the permittivity and the ions'
+// mobilities come as a second per-point record.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dd_layout.h"
+#include "dd_physics.cuh"
+#include "../../include/jaxdd_b200.h"
+
+namespace dd {
+namespace tr {
+
+enum TField { T_EPS = 0, T_MUA, T_MUC };
+
+struct Args {
+  const double* S;
+  const double* C;
+  const double* IFt;
+  const double* X;  // [np+2][DD_NT][Bp]
+  int n, Bp, npmax, ka, kc;
+  // steps
+  int steps, tstride;
+  const double* t;
+  const double* V;
+  const double* G;
+  const int32_t* track;
+  const int32_t* fmode;
+  // start: the steady state at the first step
+  const double* y0;     // [np+2][3][Bp]
+  const double* logs0;  // [DD_MAXK][Bp]
+  double tol;
+  int max_iter, simss, zimt;
+  // workspace
+  double* Yb;  // [3][np+2][5][Bp]
+  double* FB;  // [np+2][Bp]
+  double* FI;  // [np+2][Bp]
+  double* CD;  // [np+2][ncd][Bp]
+  int ncd;
+  // outputs
+  double* J;
+  double* Jext;
+  uint8_t* conv;
+  int32_t* iters;
+  uint8_t* acc;
+  int32_t* stop;
+  double* state_out;  // [np+2][5][Bp]
+  double* logs_out;   // [DD_MAXK][Bp]
+  double* fb_out;     // [np+2][Bp] or nullptr
+  double* fi_out;     // [np+2][Bp] or nullptr
+};
+
+// A point of the 5-unknown state and what the rows need of it.
+struct TP {
+  Pt c;           // V, ln n, ln p, n, p, offsets, slots (dd_physics.cuh)
+  double la, lc;  // ln a, ln c (0 outside their regions)
+  double a, c2;   // exp(la), exp(lc)
+};
+
+struct View {
+  Lane L;
+  const double* X;
+  double* Yb;
+  size_t ybuf;
+  int simss, zimt;
+  __device__ __forceinline__ double x(int k, int f) const {
+    return __ldg(X + ((size_t)k * DD_NT + f) * L.Bp + L.l);
+  }
+  __device__ __forceinline__ double* y(int buf, int k, int c) const {
+    return Yb + buf * ybuf + ((size_t)k * 5 + c) * L.Bp + L.l;
+  }
+};
+
+// A point of buffer `buf` (interior) or a contact at internal voltage `Vint`.
+__device__ __forceinline__ void load_point(const View& W, int buf, int k, double Vint, TP& P) {
+  const Lane& L = W.L;
+  if (k == 0 || k == L.NP + 1) {
+    contact(L, k != 0, Vint, P.c);
+    P.la = 0.0; P.lc = 0.0;
+  } else {
+    P.c.V = *W.y(buf, k, 0); P.c.lnn = *W.y(buf, k, 1); P.c.lnp = *W.y(buf, k, 2);
+    P.la = *W.y(buf, k, 3); P.lc = *W.y(buf, k, 4);
+  }
+  P.c.n = exp(P.c.lnn);
+  P.c.p = exp(P.c.lnp);
+  P.c.offn = L.st(k, S_OFFN);
+  P.c.offp = L.st(k, S_OFFP);
+  P.c.sl = slots_at(L, k);
+  P.a = exp(P.la);
+  P.c2 = exp(P.lc);
+  P.c.da = P.c.sl.a >= 0 ? P.a : 0.0;
+  P.c.dc = P.c.sl.c >= 0 ? P.c2 : 0.0;
+}
+
+// ------------------------------------------------------------------------------------ traps
+
+// A level's occupation over a step of 1/dti from f_old (`_trap_step` with `empty`): its mean,
+// its value at the step's end and the mean of the empty share, with their derivatives in n and
+// in p (not in their logarithms). dti = 0: the steady occupation.
+struct TrapStep {
+  double mean, end, vac;
+  double mn, en, vn, mp, ep, vp;
+};
+
+__device__ __forceinline__ void trap_step(double Cn, double Cp, double nt0, double pt0, double n,
+                                          double p, double f_old, double dti, TrapStep& o) {
+  double a = Cn * (n + nt0) + Cp * (p + pt0);
+  const bool pos = a > 0.0;
+  if (!pos) a = 1.0;
+  const double da_n = pos ? Cn : 0.0, da_p = pos ? Cp : 0.0;
+  const double steady = (Cn * n + Cp * pt0) / a, vac_s = (Cn * nt0 + Cp * p) / a;
+  const double ds_n = (Cn - steady * da_n) / a, ds_p = -steady * da_p / a;
+  const double dv_n = -vac_s * da_n / a, dv_p = (Cp - vac_s * da_p) / a;
+  double E = 0.0, m = 0.0, dm = 0.0, dx_n = 0.0, dx_p = 0.0;
+  if (dti > 0.0) {
+    const double x = a / dti;
+    E = exp(-x);
+    m = -expm1(-x) / x;
+    dm = (E - m) / x;
+    dx_n = da_n / dti;
+    dx_p = da_p / dti;
+  }
+  const double gap = f_old - steady, vgap = (1.0 - f_old) - vac_s;
+  o.mean = steady + gap * m;
+  o.end = steady + gap * E;
+  o.vac = vac_s + vgap * m;
+  o.mn = ds_n * (1.0 - m) + gap * dm * dx_n;
+  o.en = ds_n * (1.0 - E) - gap * E * dx_n;
+  o.vn = dv_n * (1.0 - m) + vgap * dm * dx_n;
+  o.mp = ds_p * (1.0 - m) + gap * dm * dx_p;
+  o.ep = ds_p * (1.0 - E) - gap * E * dx_p;
+  o.vp = dv_p * (1.0 - m) + vgap * dm * dx_p;
+}
+
+// Each carrier's recombination over the step at point k (`_bulk_rates` with the traps'
+// occupation `fb`, solver.py:680-700) and their derivatives in ln n, ln p.
+__device__ __forceinline__ void bulk_rates(const Lane& L, int k, double n, double p, double fb,
+                                           double dti, double& Rn, double& Rp, double& dRn_n,
+                                           double& dRn_p, double& dRp_n, double& dRp_p) {
+  const double kd = L.st(k, S_KD), ni2 = L.st(k, S_NI2), Nt = L.st(k, S_NT);
+  const double direct = kd * (n * p - ni2);
+  Rn = direct; Rp = direct;
+  double an = kd * p, ap = kd * n, bn = kd * p, bp = kd * n;  // d/dn, d/dp of Rn; of Rp
+  if (Nt > 0.0) {
+    const double Cn = L.st(k, S_CNT), Cp = L.st(k, S_CPT);
+    const double nt0 = L.st(k, S_NT0), pt0 = L.st(k, S_PT0);
+    TrapStep o;
+    trap_step(Cn, Cp, nt0, pt0, n, p, fb, dti, o);
+    Rn += Nt * Cn * (n * o.vac - nt0 * o.mean);
+    Rp += Nt * Cp * (p * o.mean - pt0 * o.vac);
+    an += Nt * Cn * (o.vac + n * o.vn - nt0 * o.mn);
+    ap += Nt * Cn * (n * o.vp - nt0 * o.mp);
+    bn += Nt * Cp * (p * o.mn - pt0 * o.vn);
+    bp += Nt * Cp * (o.mean + p * o.mp - pt0 * o.vp);
+  }
+  dRn_n = n * an; dRn_p = p * ap;
+  dRp_n = n * bn; dRp_p = p * bp;
+}
+
+__device__ __forceinline__ double bulk_end(const Lane& L, int k, double n, double p, double fb,
+                                           double dti) {
+  TrapStep o;
+  trap_step(L.st(k, S_CNT), L.st(k, S_CPT), L.st(k, S_NT0), L.st(k, S_PT0), n, p, fb, dti, o);
+  return o.end;
+}
+
+// Interface traps of one interval (table row t) over the step (`_interface_edges` with `f_old`,
+// solver.py:814-850): v = (Rn_L, Rn_R, Rp_L, Rp_R, Q) and their derivatives in
+// ln nL, ln nR, ln pL, ln pR; `end` the occupation at the step's end.
+__device__ void iface_edge_t(const Lane& L, int t, double nL, double nR, double pL, double pR,
+                             double f_old, double dti, Iface& o, bool derivs, double* end) {
+  const double Nt = L.itab(t, I_NT), Cn = L.itab(t, I_CN), Cp = L.itab(t, I_CP);
+  const double nlo = L.itab(t, I_NT0LO), nhi = L.itab(t, I_NT0HI);
+  const double plo = L.itab(t, I_PT0LO), phi = L.itab(t, I_PT0HI);
+  const double iw = L.itab(t, I_IW);
+  const double hq = L.itab(t, I_CHARGE) * 0.5 * Nt * iw, cwe = L.itab(t, I_CWE);
+  const double an = Cn * Nt, bp = Cp * Nt;
+  TrapStep s;
+  trap_step(Cn, Cp, nlo + nhi, plo + phi, nL + nR, pL + pR, f_old, dti, s);
+  const bool traps = Nt > 0.0;
+  const double full = traps ? s.mean : 0.0, fend = traps ? s.end : 0.0;
+  const double empty = traps ? s.vac : 0.0;
+  if (end) *end = fend;
+  o.v[0] = iw * an * (nL * empty - nlo * full);
+  o.v[1] = iw * an * (nR * empty - nhi * full);
+  o.v[2] = iw * bp * (pL * full - plo * empty);
+  o.v[3] = iw * bp * (pR * full - phi * empty);
+  o.v[4] = hq * (cwe - fend);
+  if (!derivs) return;
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const double dens = w == 0 ? nL : (w == 1 ? nR : (w == 2 ? pL : pR));
+    double dF, dE, dEnd;
+    if (w < 2) { dF = s.mn * dens; dE = s.vn * dens; dEnd = s.en * dens; }
+    else { dF = s.mp * dens; dE = s.vp * dens; dEnd = s.ep * dens; }
+    if (!traps) { dF = 0.0; dE = 0.0; dEnd = 0.0; }
+    o.d[w][0] = iw * an * ((w == 0 ? nL * empty : 0.0) + nL * dE - nlo * dF);
+    o.d[w][1] = iw * an * ((w == 1 ? nR * empty : 0.0) + nR * dE - nhi * dF);
+    o.d[w][2] = iw * bp * ((w == 2 ? pL * full : 0.0) + pL * dF - plo * dE);
+    o.d[w][3] = iw * bp * ((w == 3 ? pR * full : 0.0) + pR * dF - phi * dE);
+    o.d[w][4] = -hq * dEnd;
+  }
+}
+
+// ------------------------------------------------------------------------------------ ions
+
+// One interval's Scharfetter-Gummel flux of a species between points a (left) and b (right) at
+// mobility c/V_T, and its derivatives in x = (V_b - V_a)/V_T and in ln n_a, ln n_b: anions as
+// electrons F = c (B(x) n_b - B(-x) n_a), cations as holes F = c (B(x) n_a - B(-x) n_b).
+struct IonIv {
+  double F, gx, da, db;
+};
+
+__device__ __forceinline__ void ion_iv(double sn, double x, double na, double nb, double c,
+                                       int simss, IonIv& o) {
+  double Bf, Bb, dBf, dBb;
+  bern_pair(x, simss, Bf, Bb, dBf, dBb);
+  if (sn < 0) {
+    o.F = c * (Bf * nb - Bb * na);
+    o.gx = c * (dBf * nb + dBb * na);
+    o.da = -c * Bb * na;
+    o.db = c * Bf * nb;
+  } else {
+    o.F = c * (Bf * na - Bb * nb);
+    o.gx = c * (dBf * na + dBb * nb);
+    o.da = c * Bf * na;
+    o.db = -c * Bb * nb;
+  }
+}
+
+// ------------------------------------------------------------------------------------ rows
+
+// Row i's residual (as -F in r), blocks A, B, C (5x5) and slot columns U (5xK) over the step
+// (`_assemble_ions` with `_assemble`'s carriers' rows and their time terms). `bn`, `bpd`, `ba`,
+// `bc`: the point's densities before the step; `fb` its bulk traps' occupation, `fim`, `fii`
+// those of its two intervals' interface traps.
+template <int K>
+__device__ __forceinline__ void row5(const View& W, int i, const TP& pm, const TP& pc,
+                                     const TP& pn, const Flux& el, const Flux& er, double hm,
+                                     double hp, int ifk_m, int ifk_i, double dti, double fb,
+                                     double fim, double fii, double bn, double bpd, double ba,
+                                     double bc, const double* logs, double (&A)[5][5],
+                                     double (&B)[5][5], double (&Cm)[5][5], double (&r)[5],
+                                     double (&U)[5][K]) {
+  const Lane& L = W.L;
+  const double iVt = L.iVt;
+  const double facl = L.st(i, S_FACL), facm = L.st(i, S_FACM), facu = L.st(i, S_FACU);
+  const double fac = L.st(i, S_FAC), sP = L.st(i, S_SP), sC = L.st(i, S_SC);
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+#pragma unroll
+    for (int b = 0; b < 5; ++b) { A[a][b] = 0.0; B[a][b] = 0.0; Cm[a][b] = 0.0; }
+#pragma unroll
+    for (int k = 0; k < K; ++k) U[a][k] = 0.0;
+  }
+  double Rn, Rp, dRn_n, dRn_p, dRp_n, dRp_p;
+  bulk_rates(L, i, pc.c.n, pc.c.p, fb, dti, Rn, Rp, dRn_n, dRn_p, dRp_n, dRp_p);
+  const double gen = L.st(i, S_G) * L.gfrac;
+  double elec = hm * er.Fn - hp * el.Fn + fac * (gen - Rn);
+  double hole = hp * el.Fp - hm * er.Fp + fac * (gen - Rp);
+  const double anion = pc.c.da, cation = pc.c.dc;
+  double pois = facl * pm.c.V + facm * pc.c.V + facu * pn.c.V -
+                Q * (pc.c.n - pc.c.p + L.st(i, S_DOP) + L.afix(i) + anion - L.cfix(i) - cation);
+  // Poisson's row: the ions' densities are unknowns of their own, none follows V
+  A[0][0] = facl * sP;
+  Cm[0][0] = facu * sP;
+  B[0][0] = facm * sP;
+  B[0][1] = -Q * pc.c.n * sP;
+  B[0][2] = Q * pc.c.p * sP;
+  B[0][3] = -Q * anion * sP;
+  B[0][4] = Q * cation * sP;
+  A[1][0] = -hp * el.n0V * sC; A[1][1] = -hp * el.n0n * sC;
+  A[2][0] = hp * el.p0V * sC;  A[2][2] = hp * el.p0p * sC;
+  B[1][0] = (-hp * el.n1V + hm * er.n0V) * sC;
+  B[1][1] = (-hp * el.n1n + hm * er.n0n - fac * dRn_n) * sC;
+  B[1][2] = (-fac * dRn_p) * sC;
+  B[2][0] = (hp * el.p1V - hm * er.p0V) * sC;
+  B[2][1] = (-fac * dRp_n) * sC;
+  B[2][2] = (hp * el.p1p - hm * er.p0p - fac * dRp_p) * sC;
+  Cm[1][0] = hm * er.n1V * sC; Cm[1][1] = hm * er.n1n * sC;
+  Cm[2][0] = -hm * er.p1V * sC; Cm[2][2] = -hm * er.p1p * sC;
+  if (ifk_m >= 0 || ifk_i >= 0) {
+    const double sc3[3] = {Q * sP, -fac * sC, -fac * sC};
+    double Xs[3] = {0.0, 0.0, 0.0};
+    Iface t;
+    const int lo[3] = {4, 0, 2}, hi[3] = {4, 1, 3};
+    if (ifk_m >= 0) {  // the interval behind: its right point is this one
+      iface_edge_t(L, ifk_m, pm.c.n, pc.c.n, pm.c.p, pc.c.p, fim, dti, t, true, nullptr);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int e = hi[q];
+        Xs[q] += t.v[e];
+        B[q][1] += sc3[q] * t.d[1][e]; B[q][2] += sc3[q] * t.d[3][e];
+        A[q][1] += sc3[q] * t.d[0][e]; A[q][2] += sc3[q] * t.d[2][e];
+      }
+    }
+    if (ifk_i >= 0) {  // the interval ahead: its left point is this one
+      iface_edge_t(L, ifk_i, pc.c.n, pn.c.n, pc.c.p, pn.c.p, fii, dti, t, true, nullptr);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int e = lo[q];
+        Xs[q] += t.v[e];
+        B[q][1] += sc3[q] * t.d[0][e]; B[q][2] += sc3[q] * t.d[2][e];
+        Cm[q][1] += sc3[q] * t.d[1][e]; Cm[q][2] += sc3[q] * t.d[3][e];
+      }
+    }
+    pois += Q * Xs[0];
+    elec -= fac * Xs[1];
+    hole -= fac * Xs[2];
+  }
+  // implicit Euler in the control volume (ZimT's Cont_Eq_Elec/Holes)
+  elec -= fac * dti * (pc.c.n - bn);
+  hole -= fac * dti * (pc.c.p - bpd);
+  B[1][1] += -fac * dti * pc.c.n * sC;
+  B[2][2] += -fac * dti * pc.c.p * sC;
+  r[0] = -pois * sP; r[1] = -elec * sC; r[2] = -hole * sC;
+  // the ions' rows (ZimT's Solve_Neg_Ions / Solve_Pos_Ions)
+#pragma unroll
+  for (int sp = 0; sp < 2; ++sp) {
+    const int col = 3 + sp;
+    const double sn = sp == 0 ? -1.0 : 1.0;
+    const int slot = sp == 0 ? pc.c.sl.a : pc.c.sl.c;
+    const double lcv = sp == 0 ? pc.la : pc.lc;
+    if (slot < 0) {  // held at its value (0)
+      r[col] = -lcv;
+      B[col][col] = 1.0;
+      continue;
+    }
+    const int k = sp == 0 ? slot : L.ka + slot;
+    const double ls = logs[k];
+    if (!(dti > 0.0)) {  // the steady state: Boltzmann's with the slot's normalisation
+      r[col] = -(lcv - ls + sn * pc.c.V * iVt);
+      B[col][0] = sn * iVt;
+      B[col][col] = 1.0;
+      U[col][k] = -1.0;
+      continue;
+    }
+    const double before = sp == 0 ? ba : bc;
+    const double prev = before > 0.0 ? before : 1.0;
+    const int tf = sp == 0 ? T_MUA : T_MUC;
+    const double cl = L.Vt * W.x(i - 1, tf), cr = L.Vt * W.x(i, tf);
+    // an interval counts inside the species' regions, never a contact's
+    const bool inl = (sp == 0 ? pm.c.sl.a : pm.c.sl.c) >= 0 && i > 1;
+    const bool inr = (sp == 0 ? pn.c.sl.a : pn.c.sl.c) >= 0 && i < L.NP;
+    const double scl = 1.0 / (prev * (fac * dti + hm * cr + hp * cl));
+    const double nl = sp == 0 ? pm.a : pm.c2, nc = sp == 0 ? pc.a : pc.c2;
+    const double nr = sp == 0 ? pn.a : pn.c2;
+    double flux = 0.0, dVl = 0.0, dVc = 0.0, dVr = 0.0, dll = 0.0, dlc = 0.0, dlr = 0.0;
+    if (inl) {
+      IonIv f;
+      ion_iv(sn, (pc.c.V - pm.c.V) * iVt, nl, nc, cl, W.simss, f);
+      // anions take -hp F_l, cations +hp F_l
+      const double w = sp == 0 ? -hp : hp;
+      flux += w * f.F;
+      dVl -= w * f.gx * iVt; dVc += w * f.gx * iVt;
+      dll += w * f.da; dlc += w * f.db;
+    }
+    if (inr) {
+      IonIv f;
+      ion_iv(sn, (pn.c.V - pc.c.V) * iVt, nc, nr, cr, W.simss, f);
+      // anions take +hm F_r, cations -hm F_r
+      const double w = sp == 0 ? hm : -hm;
+      flux += w * f.F;
+      dVc -= w * f.gx * iVt; dVr += w * f.gx * iVt;
+      dlc += w * f.da; dlr += w * f.db;
+    }
+    const double els = exp(ls);
+    const double value = (flux + fac * dti * (els * before - nc)) * scl;
+    r[col] = -value;
+    A[col][0] = dVl * scl; B[col][0] = dVc * scl; Cm[col][0] = dVr * scl;
+    A[col][col] = dll * scl; Cm[col][col] = dlr * scl;
+    B[col][col] = (dlc - fac * dti * nc) * scl;
+    U[col][k] = fac * dti * els * before * scl;
+  }
+}
+
+// M^-1 applied in place to v, M = [[P, Q], [R, S]] by its partition (`_inverse5`): Pi the
+// carriers' block's inverse, PiQ = Pi Q, R, Si the inverse of S - R Pi Q.
+struct Part {
+  double Pi[3][3], PiQ[3][2], R[2][3], Si[2][2];
+};
+
+__device__ __forceinline__ void partition(const double (&M)[5][5], Part& f) {
+  double P[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) P[a][b] = M[a][b];
+  inv3(P, f.Pi);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+      f.PiQ[a][b] = f.Pi[a][0] * M[0][3 + b] + f.Pi[a][1] * M[1][3 + b] + f.Pi[a][2] * M[2][3 + b];
+  double S[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+#pragma unroll
+    for (int b = 0; b < 3; ++b) f.R[a][b] = M[3 + a][b];
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+      S[a][b] = M[3 + a][3 + b] -
+                (M[3 + a][0] * f.PiQ[0][b] + M[3 + a][1] * f.PiQ[1][b] + M[3 + a][2] * f.PiQ[2][b]);
+  }
+  const double idet = 1.0 / (S[0][0] * S[1][1] - S[0][1] * S[1][0]);
+  f.Si[0][0] = S[1][1] * idet; f.Si[0][1] = -S[0][1] * idet;
+  f.Si[1][0] = -S[1][0] * idet; f.Si[1][1] = S[0][0] * idet;
+}
+
+__device__ __forceinline__ void apply(const Part& f, double (&v)[5]) {
+  double yt[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) yt[a] = f.Pi[a][0] * v[0] + f.Pi[a][1] * v[1] + f.Pi[a][2] * v[2];
+  double w[2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+    w[a] = v[3 + a] - (f.R[a][0] * yt[0] + f.R[a][1] * yt[1] + f.R[a][2] * yt[2]);
+  const double z0 = f.Si[0][0] * w[0] + f.Si[0][1] * w[1];
+  const double z1 = f.Si[1][0] * w[0] + f.Si[1][1] * w[1];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) v[a] = yt[a] - (f.PiQ[a][0] * z0 + f.PiQ[a][1] * z1);
+  v[3] = z0;
+  v[4] = z1;
+}
+
+// ------------------------------------------------------------------------------------ current
+
+// The current over the step at the iterate (buffer `cur`, contacts at Vint) from the state
+// before it (buffer `bef`, contacts at Vbef): `_current_parts` with `tr` (batch.py:316-403) and
+// `_ion_currents` (421-483), summed over the intervals as `_current` (302-313). One pass left to
+// right: each carrier's integral form by prefix sums (sum_e h_e J_e = q K H + sum_e h_e P_e,
+// P_e the prefix of q L w_k U_k; an interface's J the one before it plus its traps'), each ion
+// region's the same over its own intervals, and the displacement current.
+template <int K>
+__device__ double current_t(const View& W, int cur, double Vint, int bef, double Vbef, double dti,
+                            const double* FB, const double* FI) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = L.Bp, l = L.l;
+  const double QL = Q * L.L;
+  double single[2] = {0, 0}, dbl[2] = {0, 0}, iu[2] = {0, 0}, P[2] = {0, 0}, bH[2] = {0, 0};
+  double corr[2] = {0, 0}, dtot = 0.0, disp = 0.0;
+  double Uprev[2] = {0, 0}, qprev[2] = {0, 0}, Jd_prev[2] = {0, 0};
+  double is[K], idb[K], iiu[K], iP[K], iH[K], isum[K], first_v[K], last_v[K], Jion_prev[K];
+  int first_k[K];
+  bool have[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    is[k] = idb[k] = iiu[k] = iP[k] = iH[k] = isum[k] = first_v[k] = last_v[k] = 0.0;
+    Jion_prev[k] = 0.0;
+    first_k[k] = -1;
+    have[k] = false;
+  }
+  TP pa, pb, qa, qb;  // pa, pb: the iterate at points e, e+1; qa, qb the state before
+  load_point(W, cur, 0, Vint, pa);
+  load_point(W, bef, 0, Vbef, qa);
+  double Ri_next[2] = {0, 0};  // interface capture at point e from the interval before it
+  for (int e = 0; e <= NP; ++e) {
+    const int kb = e + 1;
+    load_point(W, cur, kb, Vint, pb);
+    load_point(W, bef, kb, Vbef, qb);
+    const double h = L.st(e, S_H), dx = L.st(e, S_DX);
+    const int ifk = (int)L.st(e, S_IFK);
+    double tRL[2] = {0, 0}, tRR[2] = {0, 0};
+    if (ifk >= 0) {
+      Iface t;
+      iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, FI[(size_t)e * Bp + l], dti, t, false,
+                   nullptr);
+      tRL[0] = t.v[0]; tRR[0] = t.v[1]; tRL[1] = t.v[2]; tRR[1] = t.v[3];
+    }
+    // interface capture at points e and e+1 (point e+1's share of interval e+1 is 0: no two
+    // trapped interfaces are neighbours)
+    const double Ri_a[2] = {Ri_next[0] + tRL[0], Ri_next[1] + tRL[1]};
+    const double Ri_b[2] = {tRR[0], tRR[1]};
+    double Ue[2] = {0, 0};  // point e's U (0 on the contacts)
+    if (e >= 1) {
+      double Rn, Rp, d0, d1, d2, d3;
+      bulk_rates(L, e, pa.c.n, pa.c.p, FB[(size_t)e * Bp + l], dti, Rn, Rp, d0, d1, d2, d3);
+      const double G = L.st(e, S_G) * L.gfrac;
+      Ue[0] = Rn + Ri_a[0] - G + dti * (pa.c.n - qa.c.n);
+      Ue[1] = Rp + Ri_a[1] - G + dti * (pa.c.p - qa.c.p);
+    }
+    Ri_next[0] = Ri_b[0]; Ri_next[1] = Ri_b[1];
+    const double width = W.zimt ? h : (e == 0 ? h : 0.5 * (L.st(e - 1, S_H) + h));
+    double Jd[2] = {0, 0};
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const double sn = s == 0 ? -1.0 : 1.0;
+      const double q = exp(sn * (pa.c.V + (s == 0 ? pa.c.offn : pa.c.offp)) * L.iVt) /
+                       L.st(e, s == 0 ? S_MUN : S_MUP);
+      if (e >= 1) {
+        // interval e-1 (points e-1, e; e-1 <= NP-1): its trapezoid and the two sums
+        const double dxm = L.st(e - 1, S_DX);
+        const double iu_e = iu[s] + 0.5 * dxm * (Uprev[s] + Ue[s]);
+        single[s] += 0.5 * dxm * (qprev[s] + q);
+        dbl[s] += 0.5 * dxm * (qprev[s] * iu[s] + q * iu_e);
+        iu[s] = iu_e;
+        P[s] += sn * QL * width * Ue[s];
+      }
+      bH[s] += h * P[s];
+      const double through = sn * 0.5 * QL * h * (Ri_a[s] + Ri_b[s]);
+      if (ifk >= -1)  // a layer interface: the current before it plus through its traps
+        corr[s] += h * (through - (e >= 1 ? sn * QL * width * Ue[s] : 0.0));
+      if (L.currdiff) {
+        const double Vga = pa.c.V + (s == 0 ? pa.c.offn : pa.c.offp);
+        const double Vgb = pb.c.V + (s == 0 ? pb.c.offn : pb.c.offp);
+        double Bf, Bb, t1, t2;
+        bern_pair(sn * (Vgb - Vga) * L.iVt, L.simss, Bf, Bb, t1, t2);
+        const double da = s == 0 ? pa.c.n : pa.c.p, db = s == 0 ? pb.c.n : pb.c.p;
+        Jd[s] = sn * Q * L.st(e, s == 0 ? S_MUN : S_MUP) * L.Vt * (db * Bb - da * Bf) / (L.L * h);
+        dtot += h * (ifk >= -1 ? Jd_prev[s] + through : Jd[s]);
+      }
+      Uprev[s] = Ue[s];
+      qprev[s] = q;
+    }
+    Jd_prev[0] = Jd[0]; Jd_prev[1] = Jd[1];
+    // the displacement current of interval e
+    disp += W.x(e, T_EPS) * ((pb.c.V - pa.c.V) - (qb.c.V - qa.c.V));
+    // the ions, region by region
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!(L.tot[k] > 0.0)) continue;
+      const bool an = k < L.ka;
+      const int sk = an ? k : k - L.ka;
+      const double sn = an ? -1.0 : 1.0;
+      const bool ina = (an ? pa.c.sl.a : pa.c.sl.c) == sk;
+      const bool inb = (an ? pb.c.sl.a : pb.c.sl.c) == sk;
+      const double da = an ? pa.a : pa.c2, db = an ? pb.a : pb.c2;
+      const double qa_ = an ? qa.a : qa.c2, qb_ = an ? qb.a : qb.c2;
+      const double eva = exp(sn * pa.c.V * L.iVt), evb = exp(sn * pb.c.V * L.iVt);
+      if (ina && !have[k]) {
+        have[k] = true;
+        first_k[k] = e;
+        first_v[k] = da * eva;
+      }
+      if (inb) last_v[k] = db * evb;
+      if (L.currdiff) {
+        // each interval's flux (an interface takes the interval's before it), counted inside
+        double Bf, Bb, t1, t2;
+        bern_pair(sn * (pb.c.V - pa.c.V) * L.iVt, L.simss, Bf, Bb, t1, t2);
+        const double Jf = sn * Q * W.x(e, an ? T_MUA : T_MUC) * L.Vt * (db * Bb - da * Bf) /
+                          (L.L * h);
+        if (ina && inb) isum[k] += h * (ifk >= -1 ? Jion_prev[k] : Jf);
+        Jion_prev[k] = Jf;
+      } else if (ina && inb) {
+        const double mua = W.x(e, an ? T_MUA : T_MUC), mub = W.x(kb, an ? T_MUA : T_MUC);
+        const double qa2 = eva / (mua > 0.0 ? mua : 1.0);
+        const double qb2 = evb / (mub > 0.0 ? mub : 1.0);
+        const double Ua = dti * (da - qa_), Ub = dti * (db - qb_);
+        const double iu_b = iiu[k] + 0.5 * dx * (Ua + Ub);
+        is[k] += 0.5 * dx * (qa2 + qb2);
+        idb[k] += 0.5 * dx * (qa2 * iiu[k] + qb2 * iu_b);
+        iiu[k] = iu_b;
+        // J_e = qK + the prefix of the steps; at an interface the interval's before it
+        const double stp = e > first_k[k] ? sn * QL * width * Ua : 0.0;
+        iP[k] += stp;
+        iH[k] += h;
+        isum[k] += h * (iP[k] - (ifk >= -1 ? stp : 0.0));
+      }
+    }
+    pa = pb;
+    qa = qb;
+  }
+  const double H = L.Hsum;
+  double tot = 0.0;
+  if (!L.currdiff) {
+    Pt c0, cN;
+    contact(L, 0, Vint, c0);
+    contact(L, 1, Vint, cN);
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const double sn = s == 0 ? -1.0 : 1.0;
+      const double off0 = L.st(0, s == 0 ? S_OFFN : S_OFFP);
+      const double offN = L.st(NP + 1, s == 0 ? S_OFFN : S_OFFP);
+      const double d0 = exp(s == 0 ? c0.lnn : c0.lnp), dN = exp(s == 0 ? cN.lnn : cN.lnp);
+      const double Kc = (L.Vt * (sn * dN * exp(sn * (cN.V + offN) * L.iVt) -
+                                 sn * d0 * exp(sn * (c0.V + off0) * L.iVt)) - sn * dbl[s]) /
+                        single[s];
+      tot += Q * Kc * H + bH[s] + corr[s];
+    }
+  } else {
+    tot = dtot;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(L.tot[k] > 0.0) || !have[k]) continue;
+    const double sn = k < L.ka ? -1.0 : 1.0;
+    if (!L.currdiff) {
+      const double sgl = is[k] > 0.0 ? is[k] : 1.0;
+      const double Kc = (L.Vt * sn * (last_v[k] - first_v[k]) - sn * idb[k]) / sgl;
+      tot += Q * Kc * iH[k] + isum[k];
+    } else {
+      tot += isum[k];
+    }
+  }
+  tot += dti * disp / L.L;
+  return -L.left * tot / H;
+}
+
+// ------------------------------------------------------------------------------------ kernel
+
+template <int K>
+__global__ void __launch_bounds__(32) transient_kernel(Args a) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= a.n) return;
+  View W;
+  Lane& L = W.L;
+  L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l;
+  L.NP = (int)L.sc(C_NP);
+  L.ka = a.ka; L.K = K;
+  L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L); L.V0 = L.sc(C_V0); L.VL = L.sc(C_VL);
+  L.left = L.sc(C_LEFT); L.lnnL = L.sc(C_LNNL); L.lnpL = L.sc(C_LNPL); L.lnnR = L.sc(C_LNNR);
+  L.lnpR = L.sc(C_LNPR); L.Jscale = L.sc(C_JSCALE); L.Gshunt = L.sc(C_GSHUNT);
+  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor); L.Hsum = L.sc(C_HSUM);
+  L.currdiff = L.sc(C_CURRDIFF) > 0.0; L.simss = a.simss;
+  L.frozen = false; L.share = 1.0;
+  // the slots' totals: rows past k_anion + k_cation need not exist in scal
+#pragma unroll
+  for (int k = 0; k < K; ++k) L.tot[k] = k < a.ka + a.kc ? L.sc(C_TOT0 + k) : 0.0;
+  W.X = a.X; W.Yb = a.Yb; W.ybuf = (size_t)(a.npmax + 2) * 5 * a.Bp; W.simss = a.simss;
+  W.zimt = a.zimt;
+  const int NP = L.NP, Bp = a.Bp;
+  const int ts = a.tstride;
+  double* FB = a.FB;
+  double* FI = a.FI;
+  auto cd = [&](int k, int f) -> double* { return a.CD + ((size_t)k * a.ncd + f) * Bp + l; };
+  constexpr int NC = 1 + K;  // right-hand sides: -F and the K slot columns
+
+  // ---- the start: the steady state at the first step, with the ions' densities as unknowns
+  int bk = 0, bp = 1, bn = 2;  // kept, kept before it, iterate
+  double logs[K], logs_p[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) { logs[k] = a.logs0[(size_t)k * Bp + l]; logs_p[k] = logs[k]; }
+  for (int i = 1; i <= NP; ++i) {
+    const double V = a.y0[((size_t)i * 3 + 0) * Bp + l];
+    const Slots sl = slots_at(L, i);
+    const double v5[5] = {V, a.y0[((size_t)i * 3 + 1) * Bp + l],
+                          a.y0[((size_t)i * 3 + 2) * Bp + l],
+                          sl.a >= 0 ? logs[sl.a] + V * L.iVt : 0.0,
+                          sl.c >= 0 ? logs[L.ka + sl.c] - V * L.iVt : 0.0};
+#pragma unroll
+    for (int c = 0; c < 5; ++c) { *W.y(bk, i, c) = v5[c]; *W.y(bp, i, c) = v5[c]; }
+    FB[(size_t)i * Bp + l] = 0.0;
+  }
+  for (int e = 0; e <= NP; ++e) FI[(size_t)e * Bp + l] = 0.0;
+  const int fm = a.fmode[l];
+  double V_now = a.V[ts ? l : 0], dti_now = 0.0, t_last = 0.0;
+  int track_curr = 0, stop = 0;
+  bool first = true;
+  const double capV = CAP_V * L.Vt;
+
+  for (int k = 0; k < a.steps; ++k) {
+    const size_t so = (size_t)k * ts + (ts ? l : 0);
+    const double t_k = a.t[so], V_k = a.V[so];
+    L.gfrac = a.G[so];
+    const double dti = t_k == 0.0 ? 0.0 : 1.0 / (t_k > t_last ? t_k - t_last : 1.0);
+    const bool moving = dti > 0.0 && dti_now > 0.0 && !first;
+    const double rt = moving ? dti_now / dti : 0.0;
+    // ---- the step's start: the last two kept states extrapolated, held to one step's caps;
+    // into a steady state the slots' Boltzmann normalisations of it
+    double num[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) num[q] = 0.0;
+    {
+      double Vprev = L.V0 + 0.5 * L.left * V_k;
+      Slots slp = slots_at(L, 0);
+      for (int i = 1; i <= NP + 1; ++i) {
+        double V;
+        if (i <= NP) {
+#pragma unroll
+          for (int c = 0; c < 5; ++c) {
+            const double y = *W.y(bk, i, c), yp = *W.y(bp, i, c);
+            const double cap = c == 0 ? capV : CAP_LN;
+            *W.y(bn, i, c) = y + clipd(rt * (y - yp), -cap, cap);
+          }
+          V = *W.y(bn, i, 0);
+        } else {
+          V = L.VL - 0.5 * L.left * V_k;
+        }
+        if (!(dti > 0.0)) {
+          const Slots sl = slots_at(L, i);
+          const double hL = L.st(i - 1, S_H) * L.L;
+          // anions exp(+V/V_T), cations exp(-V/V_T) (their steady rows, `_ion_logs`)
+          if (sl.a >= 0 && sl.a == slp.a)
+            num[sl.a] += 0.5 * (exp(Vprev * L.iVt) + exp(V * L.iVt)) * hL;
+          if (sl.c >= 0 && sl.c == slp.c)
+            num[L.ka + sl.c] += 0.5 * (exp(-Vprev * L.iVt) + exp(-V * L.iVt)) * hL;
+          slp = sl;
+        }
+        Vprev = V;
+      }
+    }
+    double lg[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      if (dti > 0.0) {
+        lg[q] = moving ? logs[q] + clipd(rt * (logs[q] - logs_p[q]), -ION_LOG_CAP, ION_LOG_CAP)
+                       : 0.0;
+      } else {
+        lg[q] = L.tot[q] > 0.0 ? log(L.tot[q] / num[q]) : 0.0;
+      }
+    }
+    // ---- Newton (batch._newton_loop, batch.py:740-848)
+    double sh[STALL_STEPS + 1], jh[STALL_STEPS + 1];
+#pragma unroll
+    for (int q = 0; q <= STALL_STEPS; ++q) { sh[q] = INFINITY; jh[q] = INFINITY; }
+    int it = 0;
+    bool done = false, finite = true;
+    while (!done && it < a.max_iter && !isnan(sh[STALL_STEPS])) {
+      finite = true;  // of this iteration's new iterate
+      // -------- assembly and forward elimination
+      double cpv[5][5], dpv[5][NC];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) cpv[r][c] = 0.0;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) dpv[r][c] = 0.0;
+      }
+      double gnum[K];
+#pragma unroll
+      for (int q = 0; q < K; ++q) gnum[q] = 0.0;
+      TP pm, pc, pn;
+      load_point(W, bn, 0, V_k, pm);
+      load_point(W, bn, 1, V_k, pc);
+      Flux el, er;
+      flux(L, pm.c, pc.c, L.st(0, S_MUN), L.st(0, S_MUP), el);
+      for (int i = 1; i <= NP; ++i) {
+        load_point(W, bn, i + 1, V_k, pn);
+        flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
+        const double hm = L.st(i - 1, S_H), hp = L.st(i, S_H);
+        const int ifm = (int)L.st(i - 1, S_IFK), ifi = (int)L.st(i, S_IFK);
+        const double fb = FB[(size_t)i * Bp + l];
+        const double fim = ifm >= 0 ? FI[(size_t)(i - 1) * Bp + l] : 0.0;
+        const double fii = ifi >= 0 ? FI[(size_t)i * Bp + l] : 0.0;
+        const double bnv = exp(*W.y(bk, i, 1)), bpv = exp(*W.y(bk, i, 2));
+        const double bav = pc.c.sl.a >= 0 ? exp(*W.y(bk, i, 3)) : 0.0;
+        const double bcv = pc.c.sl.c >= 0 ? exp(*W.y(bk, i, 4)) : 0.0;
+        double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][K];
+        row5<K>(W, i, pm, pc, pn, el, er, hm, hp, ifm, ifi, dti, fb, fim, fii, bnv, bpv, bav, bcv,
+                lg, A, Bm, Cm, r, U);
+        // the ions' numbers over interval i-1 (between points i-1 and i)
+        {
+          const double hL = hm * L.L;
+          if (pc.c.sl.a >= 0 && pc.c.sl.a == pm.c.sl.a)
+            gnum[pc.c.sl.a] += 0.5 * (pm.a + pc.a) * hL;
+          if (pc.c.sl.c >= 0 && pc.c.sl.c == pm.c.sl.c)
+            gnum[L.ka + pc.c.sl.c] += 0.5 * (pm.c2 + pc.c2) * hL;
+        }
+        // M = B - A c'_{i-1}; right-hand sides [C | -F | U] - A [0 | d'_{i-1}]
+        double M[5][5];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+          for (int c = 0; c < 5; ++c) {
+            double s = Bm[rr][c];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) s -= A[rr][q] * cpv[q][c];
+            M[rr][c] = s;
+          }
+        double rhs[5][NC];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            double s = c == 0 ? r[rr] : U[rr][c - 1];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) s -= A[rr][q] * dpv[q][c];
+            rhs[rr][c] = s;
+          }
+        }
+        Part f;
+        partition(M, f);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          double v[5] = {Cm[0][c], Cm[1][c], Cm[2][c], Cm[3][c], Cm[4][c]};
+          apply(f, v);
+#pragma unroll
+          for (int rr = 0; rr < 5; ++rr) { cpv[rr][c] = v[rr]; *cd(i, rr * 5 + c) = v[rr]; }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          double v[5] = {rhs[0][c], rhs[1][c], rhs[2][c], rhs[3][c], rhs[4][c]};
+          apply(f, v);
+#pragma unroll
+          for (int rr = 0; rr < 5; ++rr) { dpv[rr][c] = v[rr]; *cd(i, 25 + rr * NC + c) = v[rr]; }
+        }
+        pm = pc;
+        pc = pn;
+        el = er;
+      }
+      // -------- back substitution with the slots' Schur complement
+      double SM[K][K], sr[K];
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        const bool has = L.tot[q] > 0.0;
+#pragma unroll
+        for (int q2 = 0; q2 < K; ++q2) SM[q][q2] = (q == q2 && !has) ? 1.0 : 0.0;
+        sr[q] = -(has ? gnum[q] / L.tot[q] - 1.0 : lg[q]);
+      }
+      {
+        double xn[5][NC];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) xn[rr][c] = 0.0;
+        Slots s_next = slots_at(L, NP + 1), s_here = slots_at(L, NP);
+        for (int i = NP; i >= 1; --i) {
+          double xi[5][NC];
+#pragma unroll
+          for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              double s = *cd(i, 25 + rr * NC + c);
+#pragma unroll
+              for (int q = 0; q < 5; ++q) s -= *cd(i, rr * 5 + q) * xn[q][c];
+              xi[rr][c] = s;
+            }
+#pragma unroll
+          for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              *cd(i, 25 + rr * NC + c) = xi[rr][c];
+              xn[rr][c] = xi[rr][c];
+            }
+          // the constraints' border: W = d g / d (ln a_i or ln c_i)
+          const Slots s_prev = slots_at(L, i - 1);
+          const double hLm = L.st(i - 1, S_H) * L.L, hLp = L.st(i, S_H) * L.L;
+#pragma unroll
+          for (int sp = 0; sp < 2; ++sp) {
+            const int sl = sp == 0 ? s_here.a : s_here.c;
+            if (sl < 0) continue;
+            const int q = sp == 0 ? sl : L.ka + sl;
+            if (!(L.tot[q] > 0.0)) continue;
+            const int slm = sp == 0 ? s_prev.a : s_prev.c, sln = sp == 0 ? s_next.a : s_next.c;
+            const double wpt = 0.5 * ((slm == sl ? hLm : 0.0) + (sln == sl ? hLp : 0.0));
+            const double w = wpt * exp(*W.y(bn, i, 3 + sp)) / L.tot[q];
+            sr[q] -= w * xi[3 + sp][0];
+#pragma unroll
+            for (int q2 = 0; q2 < K; ++q2) SM[q][q2] -= w * xi[3 + sp][1 + q2];
+          }
+          s_next = s_here;
+          s_here = s_prev;
+        }
+      }
+      double z[K];
+      small_solve<K>(SM, sr, z);
+      // -------- the damped update (batch.py:759-785)
+      double size = 0.0, dl_max = 0.0;
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        const double dlq = clipd(z[q], -ION_LOG_CAP, ION_LOG_CAP);
+        dl_max = nanmax(dl_max, fabs(dlq));
+        lg[q] += dlq;
+      }
+      for (int i = 1; i <= NP; ++i) {
+        double d5[5];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) {
+          double s = *cd(i, 25 + rr * NC);
+#pragma unroll
+          for (int q = 0; q < K; ++q) s -= *cd(i, 25 + rr * NC + 1 + q) * z[q];
+          d5[rr] = s;
+        }
+        double y5[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) y5[c] = *W.y(bn, i, c);
+        double st5[5];
+        st5[0] = clipd(d5[0], -capV, capV);
+#pragma unroll
+        for (int c = 1; c < 5; ++c) st5[c] = clipd(d5[c], -CAP_LN, CAP_LN);
+#pragma unroll
+        for (int c = 1; c < 3; ++c) {  // a density below the floor steps in the density
+          if (y5[c] < L.lognf) {
+            const double dd = d5[c];
+            const double in_n = dd > -1.0 ? log1p(dd) : -CAP_LN;
+            st5[c] = clipd(in_n, -FLOOR_DROP_CAP, CAP_LN);
+          }
+        }
+        size = nanmax(size, fabs(st5[0]) * L.iVt);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          const double nw = y5[c] + st5[c];
+          *W.y(bn, i, c) = nw;
+          finite = finite && isfinite(nw);
+          if (c >= 1) {
+            const double dens = exp(nw);
+            size = nanmax(size, fabs(st5[c]) * (dens / (dens + L.nfloor)));
+          }
+        }
+      }
+      size = nanmax(size, dl_max);
+#pragma unroll
+      for (int q = 0; q < K; ++q) finite = finite && isfinite(lg[q]);
+      // -------- the current at the new iterate and the stops
+      const double J = current_t<K>(W, bn, V_k, bk, V_now, dti, FB, FI);
+#pragma unroll
+      for (int q = 0; q < STALL_STEPS; ++q) { sh[q] = sh[q + 1]; jh[q] = jh[q + 1]; }
+      sh[STALL_STEPS] = size;
+      jh[STALL_STEPS] = J;
+      ++it;
+      double smax = sh[0], smin1 = sh[1], jdev = 0.0;
+#pragma unroll
+      for (int q = 1; q <= STALL_STEPS; ++q) smax = nanmax(smax, sh[q]);
+#pragma unroll
+      for (int q = 2; q <= STALL_STEPS; ++q) smin1 = fmin(smin1, sh[q]);
+#pragma unroll
+      for (int q = 0; q <= STALL_STEPS; ++q) jdev = nanmax(jdev, fabs(jh[q] - J));
+      const bool stalled = it > STALL_STEPS && smax < ROUND_OFF_FLOOR && smin1 >= 0.1 * sh[0];
+      const bool settled = it > STALL_STEPS && size < CURRENT_STEP_CAP &&
+                           jdev < CURRENT_TOL * (L.Jscale + fabs(J));
+      const bool quad = it > 1 && size < QUADRATIC_TOL &&
+                        size < QUADRATIC_RATIO * sh[STALL_STEPS - 1];
+      done = size < a.tol || stalled || settled || quad;
+    }
+    const bool ok = done;
+    const double J = jh[STALL_STEPS];
+    const double J_ext = J + L.Gshunt * V_k;
+    // ---- ZimT's main loop (transient.py:419-445)
+    const bool running = stop == 0;
+    const bool failed = running && !ok && (fm == 0 || (fm == 2 && track_curr == 1));
+    const bool keep = running && !failed && finite && (ok || fm == 1 || (fm == 2 && dti == 0.0));
+    if (keep) {
+      // the traps' occupations at the step's end, from its solution
+      TP pa, pb;
+      load_point(W, bn, 0, V_k, pa);
+      for (int e = 0; e <= NP; ++e) {
+        load_point(W, bn, e + 1, V_k, pb);
+        const int ifk = (int)L.st(e, S_IFK);
+        if (ifk >= 0) {
+          Iface t;
+          double end;
+          iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, FI[(size_t)e * Bp + l], dti, t,
+                       false, &end);
+          FI[(size_t)e * Bp + l] = end;
+        }
+        if (e + 1 <= NP && L.st(e + 1, S_NT) > 0.0) {
+          const size_t o = (size_t)(e + 1) * Bp + l;
+          FB[o] = bulk_end(L, e + 1, pb.c.n, pb.c.p, FB[o], dti);
+        }
+        pa = pb;
+      }
+      const int old_p = bp;
+      bp = bk; bk = bn; bn = old_p;
+#pragma unroll
+      for (int q = 0; q < K; ++q) { logs_p[q] = logs[q]; logs[q] = lg[q]; }
+      V_now = V_k;
+      dti_now = dti;
+      track_curr = a.track[so];
+      t_last = t_k;
+    }
+    if (failed) stop = 2;
+    first = false;
+    const size_t o = (size_t)k * Bp + l;
+    a.J[o] = J;
+    a.Jext[o] = J_ext;
+    a.conv[o] = ok ? 1 : 0;
+    a.iters[o] = it;
+    a.acc[o] = keep ? 1 : 0;
+  }
+  a.stop[l] = stop;
+  for (int i = 0; i <= NP + 1; ++i) {
+    TP p;
+    load_point(W, bk, i, V_now, p);
+    const double v5[5] = {p.c.V, p.c.lnn, p.c.lnp, p.la, p.lc};
+#pragma unroll
+    for (int c = 0; c < 5; ++c) a.state_out[((size_t)i * 5 + c) * Bp + l] = v5[c];
+  }
+#pragma unroll
+  for (int q = 0; q < K; ++q) a.logs_out[(size_t)q * Bp + l] = logs[q];
+  for (int i = 0; i <= NP + 1; ++i) {
+    const size_t o = (size_t)i * Bp + l;
+    if (a.fb_out) a.fb_out[o] = (i >= 1 && i <= NP) ? FB[o] : 0.0;
+    if (a.fi_out) a.fi_out[o] = i <= NP ? FI[o] : 0.0;
+  }
+}
+
+}  // namespace tr
+}  // namespace dd
+
+// ------------------------------------------------------------------------------------ C ABI
+
+namespace {
+
+int slots_k_t(const dd_batch* b) { return b->k_anion + b->k_cation <= 2 ? 2 : 4; }
+
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+void ws_parts(const dd_batch* b, size_t* y, size_t* fb, size_t* fi, size_t* cd, int* ncd) {
+  const int K = slots_k_t(b);
+  const size_t nodes = (size_t)b->np_max + 2, Bp = (size_t)b->lane_stride;
+  *ncd = 25 + 5 * (1 + K);
+  *y = align_up(3 * nodes * 5 * Bp * sizeof(double));
+  *fb = align_up(nodes * Bp * sizeof(double));
+  *fi = align_up(nodes * Bp * sizeof(double));
+  *cd = align_up(nodes * (size_t)(*ncd) * Bp * sizeof(double));
+}
+
+bool batch_ok(const dd_batch* b) {
+  return b && b->n_lanes >= 1 && b->lane_stride >= b->n_lanes && b->np_max >= 1 &&
+         b->k_anion >= 1 && b->k_cation >= 1 && b->k_anion + b->k_cation <= dd::DD_MAXK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dd_transient_workspace_bytes(const dd_batch* batch, size_t* bytes) {
+  if (!batch_ok(batch) || !bytes) return DD_ERR_ARGS;
+  size_t y, fb, fi, cd;
+  int ncd;
+  ws_parts(batch, &y, &fb, &fi, &cd, &ncd);
+  *bytes = y + fb + fi + cd;
+  return DD_OK;
+}
+
+int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* steps,
+                 const double* start, const double* start_logs, const dd_opts* opts,
+                 const dd_transient_out* out, void* workspace, size_t workspace_bytes,
+                 void* stream) {
+  if (!batch_ok(batch) || !batch->stat || !batch->scal || !batch->iface || !tstat || !steps ||
+      !start || !start_logs || !opts || !out || !workspace)
+    return DD_ERR_ARGS;
+  if (steps->n_steps < 1 || !steps->t || !steps->v || !steps->g_frac || !steps->track ||
+      !steps->failure_mode || (steps->stride != 0 && steps->stride != batch->lane_stride))
+    return DD_ERR_ARGS;
+  if (!out->J || !out->J_ext || !out->converged || !out->iterations || !out->accepted ||
+      !out->stop || !out->state || !out->logs)
+    return DD_ERR_ARGS;
+  if (opts->max_iter < 1 || !(opts->tol > 0.0)) return DD_ERR_ARGS;
+  size_t y, fb, fi, cd;
+  int ncd;
+  ws_parts(batch, &y, &fb, &fi, &cd, &ncd);
+  if (workspace_bytes < y + fb + fi + cd) return DD_ERR_WORKSPACE;
+  char* w = static_cast<char*>(workspace);
+  dd::tr::Args a;
+  a.S = batch->stat; a.C = batch->scal; a.IFt = batch->iface; a.X = tstat;
+  a.n = batch->n_lanes; a.Bp = batch->lane_stride; a.npmax = batch->np_max;
+  a.ka = batch->k_anion; a.kc = batch->k_cation;
+  a.steps = steps->n_steps; a.tstride = steps->stride;
+  a.t = steps->t; a.V = steps->v; a.G = steps->g_frac; a.track = steps->track;
+  a.fmode = steps->failure_mode;
+  a.y0 = start; a.logs0 = start_logs;
+  a.tol = opts->tol; a.max_iter = opts->max_iter;
+  a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS;
+  a.zimt = steps->zimt_sums != 0;
+  a.Yb = reinterpret_cast<double*>(w);
+  a.FB = reinterpret_cast<double*>(w + y);
+  a.FI = reinterpret_cast<double*>(w + y + fb);
+  a.CD = reinterpret_cast<double*>(w + y + fb + fi);
+  a.ncd = ncd;
+  a.J = out->J; a.Jext = out->J_ext; a.conv = out->converged; a.iters = out->iterations;
+  a.acc = out->accepted; a.stop = out->stop; a.state_out = out->state; a.logs_out = out->logs;
+  a.fb_out = out->f_bulk; a.fi_out = out->f_iface;
+  const dim3 grid((batch->n_lanes + 31) / 32), block(32);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (slots_k_t(batch) == 2) dd::tr::transient_kernel<2><<<grid, block, 0, s>>>(a);
+  else dd::tr::transient_kernel<4><<<grid, block, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+}
+
+}  // extern "C"

@@ -1,0 +1,306 @@
+"""Transients of a batch: jaxdd's `solve_transient` (src/jaxdd/transient.py:537-637) on the GPU.
+
+Each device starts from its steady state at the first step (`t = 0`; `dd_solve_states` at the
+first voltage and generation factor, no pre-bias), then `dd_transient` takes every device
+through all its steps in one launch: per step one Newton solve of implicit Euler with the mobile
+ions as unknowns of their own (5×5 blocks bordered by the ion slots), the traps' occupations
+carried from step to step, the current with each density's change, the ions' currents and the
+displacement current, and ZimT's main loop (which steps are kept, each step's Δt from the last
+one kept).
+
+The voltage is given at every step. Refused (`NotImplementedError`), not approximated: an open
+circuit or a series resistance (the internal voltage an unknown), `Track` 2 or 3 (ZimT's
+automatic stop), photon recycling, the profiles of every step, a start from a given state, ion
+regions that reach a contact, ZimT's last-region ion currents with several regions of a species.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .batch import Batch, _gpu, descriptor, initial_state
+from .simss_input import TVG
+
+__all__ = ["STOP_FAILED", "TransientResult", "TransientState", "Work", "solve_transient"]
+
+#: `TransientResult.stop`: a failed step ended the run (transient.py:240)
+STOP_FAILED = 2
+
+
+@dataclass(frozen=True)
+class TransientState:
+    """The last state kept, per device (jaxdd transient.py:72-94): `t`, the potential `V` and
+    the densities `n`, `p`, `anion`, `cation` on every point (the ions 0 outside their regions),
+    `V_int`, `J_ext`, `dti`, and the traps' occupations `f_bulk` (interior points) and
+    `f_interface` (intervals)."""
+
+    t: np.ndarray
+    V: np.ndarray
+    n: np.ndarray
+    p: np.ndarray
+    anion: np.ndarray
+    cation: np.ndarray
+    V_int: np.ndarray
+    J_ext: np.ndarray
+    dti: np.ndarray
+    f_bulk: np.ndarray
+    f_interface: np.ndarray
+
+
+@dataclass(frozen=True)
+class TransientResult:
+    """Per device and step (devices × steps), as jaxdd's (transient.py:97-122): `J` the internal
+    current density (A/m²), `J_ext` with the shunt, `V_int`, `V_ext`, `converged`, `iterations`,
+    `accepted` (the steps ZimT keeps); per device `stop` (0, or `STOP_FAILED`); `t` each step's
+    time; `final` the last state kept. ZimT's other tJFile columns are not built (`columns`
+    empty)."""
+
+    J: np.ndarray
+    J_ext: np.ndarray
+    V_int: np.ndarray
+    V_ext: np.ndarray
+    converged: np.ndarray
+    iterations: np.ndarray
+    accepted: np.ndarray
+    stop: np.ndarray
+    t: np.ndarray
+    final: TransientState
+    columns: dict
+
+
+def _steps(tvgs: list[TVG]):
+    if len({len(x.t) for x in tvgs}) != 1:
+        raise ValueError("one tVG for the batch, or one per device, all of one length")
+    for x in tvgs:
+        if np.any(x.oc):
+            raise NotImplementedError("transient at the open circuit (the internal voltage an "
+                                      "unknown): not built")
+        if np.any(np.asarray(x.track) > 1):
+            raise NotImplementedError("Track 2 or 3 (ZimT's automatic stop on equal states): "
+                                      "not built")
+    t, V, G, track = (np.stack([np.asarray(getattr(x, k), dtype=float) for x in tvgs])
+                      for k in ("t", "Vext", "G_frac", "track"))
+    fm = np.array([x.failure_mode for x in tvgs], dtype=np.int32)
+    return t, V, G, track.astype(np.int32), fm
+
+
+def _check_batch(batch: Batch) -> None:
+    devs = batch["devices"]
+    if any(d.R_series > 0 for d in devs):
+        raise NotImplementedError("transient with a series resistance (the internal voltage an "
+                                  "unknown): not built")
+    for d in devs:
+        for mask in (d.anion_mask, d.cation_mask):
+            if mask is not None and (mask[0] or mask[-1]):
+                raise NotImplementedError("mobile ions in a region that reaches a contact: not "
+                                          "built")
+
+
+class Work:
+    """The device-side inputs of one transient run, packed once: the start's plan (the steady
+    state at the first step), the per-point record, the steps, the outputs and the workspace.
+    `run()` solves the start and the transient on the current stream; the outputs stay on the
+    device (`out`)."""
+
+    def __init__(self, batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
+                 bernoulli_name: str = "exact", zimt_current: bool = False):
+        import torch
+        from .adjoint import plan as _plan
+        _check_batch(batch)
+        devs = batch["devices"]
+        tvgs = list(tvg) if isinstance(tvg, (list, tuple)) else [tvg] * len(devs)
+        if len(tvgs) != len(devs):
+            raise ValueError("one tVG for the batch, or one per device, all of one length")
+        t, V, G, track, fm = _steps(tvgs)
+        self.batch, self.tol, self.max_iter = batch, tol, max_iter
+        self.bern = _lib.DD_BERNOULLI[bernoulli_name]
+        self.g = g = _gpu(batch)
+        cuda = g.stat.device
+        Bp, nodes, lanes = batch["Bp"], batch["np_max"] + 2, batch["lane_of"]
+        self.S = S = t.shape[1]
+        self.t, self.V = t, V
+        # the start: the steady state at the first step's voltage and generation, no pre-bias
+        self.plan = _plan(batch, [[float(v)] for v in V[:, 0]], tol=tol, max_iter=max_iter,
+                          bernoulli_name=bernoulli_name)
+        y0 = np.zeros((nodes, 3, Bp))
+        for k, d in enumerate(devs):
+            y0[:len(d.x), :, lanes[k]] = initial_state(d, float(V[k, 0]))
+        self.plan.y0.copy_(torch.from_numpy(y0))
+        scal = g.scal.clone()
+        gf = scal[_lib.C["GFRAC"]].cpu().numpy()
+        gf[lanes] = G[:, 0]
+        scal[_lib.C["GFRAC"]] = torch.from_numpy(gf).to(cuda)
+        scal[_lib.C["PRECOND"]] = 0.0
+        self.scal0 = scal
+        # the per-point record: permittivity and the ions' mobilities
+        X = np.zeros((nodes, _lib.DD_NT, Bp))
+        for k, d in enumerate(devs):
+            m = len(d.x)
+            X[:m, 0, lanes[k]] = d.eps
+            if d.mu_anion is not None:
+                X[:m, 1, lanes[k]] = d.mu_anion
+            if d.mu_cation is not None:
+                X[:m, 2, lanes[k]] = d.mu_cation
+        self.X = torch.from_numpy(X).to(cuda)
+        # the steps: one list for all lanes where every device has the same
+        same = all(np.array_equal(a[0], a[j]) for a in (t, V, G, track) for j in range(len(a)))
+        if same:
+            self.stride = 0
+            cols, tr = (t[0], V[0], G[0]), track[0]
+        else:
+            self.stride = Bp
+
+            def lane_major(a):
+                out = np.zeros((S, Bp), dtype=a.dtype)
+                out[:, lanes] = a.T
+                return out
+            cols, tr = (lane_major(t), lane_major(V), lane_major(G)), lane_major(track)
+        self.tv, self.vv, self.gv = (torch.from_numpy(np.ascontiguousarray(c)).to(cuda)
+                                     for c in cols)
+        self.trk = torch.from_numpy(np.ascontiguousarray(tr, dtype=np.int32)).to(cuda)
+        fml = np.ones(Bp, dtype=np.int32)
+        fml[lanes] = fm
+        self.fm = torch.from_numpy(fml).to(cuda)
+        self.zimt = int(bool(zimt_current))
+        f64, u8, i32 = torch.float64, torch.uint8, torch.int32
+        self.out = {
+            "J": torch.empty((S, Bp), dtype=f64, device=cuda),
+            "J_ext": torch.empty((S, Bp), dtype=f64, device=cuda),
+            "converged": torch.empty((S, Bp), dtype=u8, device=cuda),
+            "iterations": torch.empty((S, Bp), dtype=i32, device=cuda),
+            "accepted": torch.empty((S, Bp), dtype=u8, device=cuda),
+            "stop": torch.empty(Bp, dtype=i32, device=cuda),
+            "state": torch.empty((nodes, 5, Bp), dtype=f64, device=cuda),
+            "logs": torch.zeros((_lib.DD_MAXK, Bp), dtype=f64, device=cuda),
+            "f_bulk": torch.empty((nodes, Bp), dtype=f64, device=cuda),
+            "f_iface": torch.empty((nodes, Bp), dtype=f64, device=cuda),
+        }
+        size = ctypes.c_size_t(0)
+        desc = descriptor(batch, g, self.plan.y0)
+        _lib.check(_lib.lib().dd_transient_workspace_bytes(ctypes.byref(desc),
+                                                           ctypes.byref(size)),
+                   "dd_transient_workspace_bytes")
+        self.ws = torch.empty(size.value, dtype=torch.uint8, device=cuda)
+
+    def run(self):
+        """The start and the transient, on the current stream: `(out, start_converged)`."""
+        import torch
+        from .adjoint import solve_states as _solve_states
+        g = self.g
+        _, ok0, _, ckpt = _solve_states(self.plan, g.stat, self.scal0, g.iface)
+        start, start_logs = ckpt["states"][0], ckpt["logs"][0]
+        steps = _lib.DdSteps(self.S, self.stride, self.tv.data_ptr(), self.vv.data_ptr(),
+                             self.gv.data_ptr(), self.trk.data_ptr(), self.fm.data_ptr(),
+                             self.zimt)
+        o = self.out
+        out = _lib.DdTransientOut(*(o[k].data_ptr() for k in (
+            "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",
+            "f_bulk", "f_iface")))
+        opts = _lib.DdOpts(float(self.tol), int(self.max_iter), int(self.max_iter), 0,
+                           self.bern, _lib.DD_MODE_BATCH, 0, 0)
+        desc = descriptor(self.batch, g, self.plan.y0)
+        _lib.check(_lib.lib().dd_transient(
+            ctypes.byref(desc), self.X.data_ptr(), ctypes.byref(steps), start.data_ptr(),
+            start_logs.data_ptr(), ctypes.byref(opts), ctypes.byref(out), self.ws.data_ptr(),
+            self.ws.numel(), torch.cuda.current_stream(g.stat.device).cuda_stream),
+            "dd_transient")
+        return o, ok0
+
+
+def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
+                    bernoulli_name: str = "exact", zimt_ion_currents: bool = False,
+                    ions=None, vint=None, zimt_current: bool = False, recycle=None,
+                    profiles: bool = False, ion_flux: str = "electrochemical",
+                    initial=None) -> TransientResult:
+    """A batch (`prepare`) through ZimT's time steps `tvg` (a `TVG`, or one per device, all of
+    one length): jaxdd's `solve_transient` (transient.py:537-637) with the same arguments.
+    `zimt_current`: ZimT's sums in the integral current (each point's change over the interval
+    after it); by default over each point's control volume. `ion_flux`: both of jaxdd's are the
+    Scharfetter–Gummel flux without ion sites, the only case built. Not built (raise
+    `NotImplementedError`): `recycle`, `profiles`, `initial`, an internal voltage as an unknown
+    (`vint`, an open circuit, a series resistance), and `zimt_ion_currents` with several regions
+    of a species. `ions` is accepted for the reference's signature: the ions are unknowns of
+    every step here, which leaves devices without mobile ions as they are."""
+    if recycle is not None or profiles or initial is not None:
+        raise NotImplementedError("recycle, profiles and initial: not built")
+    if vint:
+        raise NotImplementedError("the internal voltage as an unknown: not built")
+    if ion_flux not in ("electrochemical", "modified-drift"):
+        raise ValueError(f"ion_flux {ion_flux!r}: one of ('electrochemical', 'modified-drift')")
+    if zimt_ion_currents and (batch["ka"] > 1 or batch["kc"] > 1):
+        raise NotImplementedError("ZimT's last-region ion currents with several regions")
+    del ions
+    work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
+                zimt_current=zimt_current)
+    o, _ = work.run()
+    return result(work, o)
+
+
+def result(work: Work, o) -> TransientResult:
+    """`Work.run()`'s device outputs as a `TransientResult` in the caller's device order."""
+    batch = work.batch
+    lanes = batch["lane_of"]
+    devs = batch["devices"]
+
+    def per_step(name, dtype=None):
+        a = o[name].cpu().numpy()[:, lanes].T
+        return a if dtype is None else a.astype(dtype)
+
+    J, J_ext = per_step("J"), per_step("J_ext")
+    ok, its = per_step("converged", bool), per_step("iterations", int)
+    acc = per_step("accepted", bool)
+    stop = o["stop"].cpu().numpy()[lanes]
+    V_int = work.V.copy()
+    R = np.array([d.R_series for d in devs])
+    V_ext = V_int + J_ext * R[:, None]
+    state = o["state"].cpu().numpy()[:, :, lanes]  # nodes × 5 × devices
+    fb = o["f_bulk"].cpu().numpy()[:, lanes]
+    fi = o["f_iface"].cpu().numpy()[:, lanes]
+    t = work.t
+    n = len(devs)
+    # the last kept step of each device, its time and 1/Δt (Δt from the step kept before it)
+    last = np.full(n, -1)
+    kept_t, kept_dti = np.zeros(n), np.zeros(n)
+    for k in range(n):
+        prev = 0.0
+        for s in range(t.shape[1]):
+            if acc[k, s]:
+                tk = t[k, s]
+                kept_dti[k] = 0.0 if tk == 0 else 1.0 / (tk - prev if tk > prev else 1.0)
+                prev = tk
+                last[k] = s
+        kept_t[k] = prev
+    rows = np.arange(n)
+    Vs, ns, ps, As, Cs, fbs, fis = [], [], [], [], [], [], []
+    for k, d in enumerate(devs):
+        m = len(d.x)
+        st = state[:m, :, k]
+        Vs.append(st[:, 0])
+        ns.append(np.exp(st[:, 1]))
+        ps.append(np.exp(st[:, 2]))
+        am = np.asarray(d.anion_mask, bool) if d.anion_mask is not None else np.zeros(m, bool)
+        cm = np.asarray(d.cation_mask, bool) if d.cation_mask is not None else np.zeros(m, bool)
+        As.append(np.where(am, np.exp(st[:, 3]), 0.0))
+        Cs.append(np.where(cm, np.exp(st[:, 4]), 0.0))
+        fbs.append(fb[1:m - 1, k])
+        fis.append(fi[:m - 1, k])
+
+    def stack(xs):
+        if len({len(x) for x in xs}) == 1:
+            return np.stack(xs)
+        out = np.empty(len(xs), dtype=object)
+        out[:] = xs
+        return out
+
+    at = np.maximum(last, 0)
+    final = TransientState(
+        t=kept_t, V=stack(Vs), n=stack(ns), p=stack(ps), anion=stack(As), cation=stack(Cs),
+        V_int=np.where(last >= 0, V_int[rows, at], V_int[:, 0]),
+        J_ext=np.where(last >= 0, J_ext[rows, at], np.nan), dti=kept_dti, f_bulk=stack(fbs),
+        f_interface=stack(fis))
+    return TransientResult(J=J, J_ext=J_ext, V_int=V_int, V_ext=V_ext, converged=ok,
+                           iterations=its, accepted=acc, stop=stop, t=t, final=final, columns={})

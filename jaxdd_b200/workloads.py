@@ -146,3 +146,18 @@ def drawn_devices(n: int, seed: int = SEED_DRAWN, NP: int | tuple[int, int] = 40
     """Devices `start .. start + n` of the drawn workload (each device's draws depend only on
     the seed and its index). `NP` an int, or `(lo, hi)` for a grid size drawn U{lo..hi}."""
     return [drawn_device(k, seed, NP) for k in range(start, start + n)]
+
+
+def transient_devices(n: int, seed: int = SEED_DRAWN, NP: int = 400, start: int = 0):
+    """Config 5's devices: the drawn workload's devices with free mobile ions (its odd indices:
+    config 2's distributions, ions in the absorber, no pre-bias), `start .. start + n` of them."""
+    return [drawn_device(2 * k + 1, seed, NP) for k in range(start, start + n)]
+
+
+def transient_steps(n_steps: int = 2000, V: float = 0.9):
+    """Config 5's transient: the steady state at 0 V (t = 0), then `n_steps` implicit-Euler
+    steps at `V` log-spaced from 1 ns to 1 s, light on (G_frac 1), failureMode 1."""
+    from .simss_input import TVG
+    t = np.concatenate([[0.0], np.logspace(-9, 0, n_steps)])
+    return TVG.steps(t, np.where(t > 0, V, 0.0), 1.0, 0, failure_mode=1)
+
