@@ -220,9 +220,8 @@ int dd_build(const dd_structure* structure, const double* layer_params,
 /* ---- Transients with mobile ions (jaxdd transient.py:270-465, 537-637) -------------------- */
 #define DD_NT 3 /* per-point transient record fields: permittivity, anion and cation mobility */
 
-/* ZimT's time steps (jaxdd `TVG`, simss_input.py:155-237). Lane l's step k is at
- * [k * stride + (stride ? l : 0)]: one list for every lane (stride 0) or one per lane (stride =
- * lane_stride). The first step is at t = 0 (a steady state); a later t = 0 returns to one. */
+/* ZimT's time steps (jaxdd `TVG`, simss_input.py:155-237). Lane l's step k is at [k] (stride 0:
+ * one list for every lane) or at [k * lane_stride + l] (stride = lane_stride: one per lane). The first step is at t = 0 (a steady state); a later t = 0 returns to one. */
 typedef struct dd_steps {
   int32_t n_steps;
   int32_t stride;

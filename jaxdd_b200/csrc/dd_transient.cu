@@ -668,7 +668,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   const double capV = CAP_V * L.Vt;
 
   for (int k = 0; k < a.steps; ++k) {
-    const size_t so = (size_t)k * ts + (ts ? l : 0);
+    // step k of this lane: one list for all lanes (ts 0) or [step][lane]
+    const size_t so = ts ? (size_t)k * ts + l : (size_t)k;
     const double t_k = a.t[so], V_k = a.V[so];
     L.gfrac = a.G[so];
     const double dti = t_k == 0.0 ? 0.0 : 1.0 / (t_k > t_last ? t_k - t_last : 1.0);
