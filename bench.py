@@ -491,6 +491,174 @@ def build_bench(args, rank: int, world: int, local: int) -> None:
         }), flush=True)
 
 
+def _transient_chunk(args):
+    """Config 5's devices `start .. start + n` (a pool worker)."""
+    start, n, npts = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from jaxdd_b200.batch import prepare
+    from jaxdd_b200.workloads import transient_devices
+    return prepare(transient_devices(n, NP=npts, start=start))
+
+
+def transient_bytes(NPk: int, K: int, w: int = 8) -> int:
+    """Algorithmic bytes of one Newton iteration of one device in time: per point the static
+    record (26 words) and the transient record (3), the iterate (5) and the state before the
+    step (5) read, the new iterate (5) written, and the block sweep's round trip (c' 25 and the
+    1 + K right-hand sides' 5 (1 + K) words, written in the elimination and read back)."""
+    per_point = 26 + 3 + 5 + 5 + 5 + 2 * (25 + 5 * (1 + K))
+    return NPk * per_point * w
+
+
+def transient_bench(args, rank: int, world: int, local: int) -> None:
+    """Config 5's transient half: every device's steady state at 0 V, then 2000 implicit-Euler
+    steps at 0.9 V log-spaced from 1 ns to 1 s, mobile ions as unknowns (5x5 blocks). One step =
+    the start (`dd_solve_states`) and `dd_transient` of the whole batch, inputs resident on the
+    GPU. Devices are independent: with N GPUs every rank solves its own batch (weak scaling)."""
+    import torch
+    from jaxdd_b200 import _lib
+    from jaxdd_b200.batch import concat
+    from jaxdd_b200.transient import Work
+    from jaxdd_b200.workloads import transient_steps
+    n = args.devices
+    procs = args.build_procs or max(1, min(32, (os.cpu_count() or 1) // max(1, world)))
+    t0 = time.perf_counter()
+    tasks = [(rank * n + k, min(CHUNK, n - k), args.np) for k in range(0, n, CHUNK)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        batch = concat(pool.map(_transient_chunk, tasks))
+    build_s = time.perf_counter() - t0
+    cpu = None
+    if rank == 0 and world == 1:
+        # the oracle on one device of the same workload, a bounded number of its steps
+        from jaxdd_b200.workloads import transient_devices
+        from oracle import dd, transient
+        sample_steps = args.cpu_sample * 25
+        tv = transient_steps(args.tsteps)
+        d1 = dd.prepare(transient_devices(1, NP=args.np))
+        t1 = time.perf_counter()
+        transient.solve_transient(d1, tv.t[:sample_steps + 1], tv.Vext[:sample_steps + 1],
+                                  tv.G_frac[:sample_steps + 1])
+        secs = time.perf_counter() - t1
+        cpu = {"value": (sample_steps + 1) / secs / (args.tsteps + 1), "unit": "transients/s",
+               "cores": 1, "kind": "port",
+               "sample": f"the oracle (NumPy FP64) on 1 device, its start and first "
+                         f"{sample_steps} of {args.tsteps} steps, scaled to whole transients"}
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800))
+    tvg = transient_steps(args.tsteps)
+    work = Work(batch, tvg)
+    dev = work.X.device
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        out, ok0 = work.run()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            out, ok0 = work.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # the transient kernel alone (the start is a steady solve at one voltage)
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g = work.g
+    from jaxdd_b200.adjoint import solve_states as _solve_states
+    _, _, _, ckpt = _solve_states(work.plan, g.stat, work.scal0, g.iface)
+    import ctypes
+    steps_c = _lib.DdSteps(work.S, work.stride, work.tv.data_ptr(), work.vv.data_ptr(),
+                           work.gv.data_ptr(), work.trk.data_ptr(), work.fm.data_ptr(), work.zimt)
+    o = work.out
+    out_c = _lib.DdTransientOut(*(o[k].data_ptr() for k in (
+        "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs", "f_bulk",
+        "f_iface")))
+    opts = _lib.DdOpts(float(work.tol), int(work.max_iter), int(work.max_iter), 0, work.bern,
+                       _lib.DD_MODE_BATCH, 0, 0)
+    from jaxdd_b200.batch import descriptor
+    desc = descriptor(batch, g, work.plan.y0)
+    k0.record(stream)
+    _lib.check(_lib.lib().dd_transient(
+        ctypes.byref(desc), work.X.data_ptr(), ctypes.byref(steps_c),
+        ckpt["states"][0].data_ptr(), ckpt["logs"][0].data_ptr(), ctypes.byref(opts),
+        ctypes.byref(out_c), work.ws.data_ptr(), work.ws.numel(), stream.cuda_stream),
+        "dd_transient")
+    k1.record(stream)
+    torch.cuda.synchronize()
+    kernel_ms = k0.elapsed_time(k1)
+    # e2e: the packed inputs from pinned host memory, the start and the transient, the per-step
+    # results back to pinned host memory, all in the timed region
+    dev_in = {"stat": g.stat, "scal": work.scal0, "iface": g.iface, "X": work.X, "y0": work.plan.y0}
+    host_in = {k: v.cpu().pin_memory() for k, v in dev_in.items()}
+    outs = ("J", "J_ext", "converged", "iterations", "accepted")
+    host_out = {k: torch.empty(o[k].shape, dtype=o[k].dtype).pin_memory() for k in outs}
+    h2d = sum(v.numel() * v.element_size() for v in host_in.values())
+    d2h = sum(v.numel() * v.element_size() for v in host_out.values())
+    v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    v0.record(stream)
+    for k, v in dev_in.items():
+        v.copy_(host_in[k], non_blocking=True)
+    out, ok0 = work.run()
+    for k in outs:
+        host_out[k].copy_(o[k], non_blocking=True)
+    v1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = v0.elapsed_time(v1)
+    t = torch.tensor([ms, e2e_ms, kernel_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms, e2e_ms, kernel_ms = (float(x) for x in t.tolist())
+    m = batch["n"]
+    its = o["iterations"][:, :m].to(torch.int64)
+    acc = o["accepted"][:, :m]
+    total_its = int(its.sum())
+    NPs = np.asarray(batch["NP"])
+    K = 2 if batch["ka"] + batch["kc"] <= 2 else 4
+    per_lane_its = its.sum(dim=0).cpu().numpy()
+    alg = float(sum(per_lane_its[j] * transient_bytes(int(NPs[j]), K) for j in range(m)))
+    achieved = alg / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+    S = work.S
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": m * world / (ms / 1e3), "unit": "transients/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"BASELINE config 5, transient half: {m} devices/GPU (drawn "
+                                   "p-i-n stacks with free mobile ions, seed 20261205), NP "
+                                   f"{args.np}, steady state at 0 V then {S - 1} implicit-Euler "
+                                   "steps at 0.9 V log-spaced 1 ns..1 s, 5x5 blocks + 2 ion "
+                                   "slots",
+                       "inputs_vs_l2": "the state and sweep buffers (GBs) exceed L2",
+                       "build_s": round(build_s, 1),
+                       "time_steps_per_s": m * world * S / (ms / 1e3),
+                       "newton_steps_per_time_step": total_its / (m * S),
+                       "us_per_newton_step_per_device": kernel_ms * 1e3 / total_its,
+                       "reference_published_a100": "44,100 time steps/s, 7.22 us per Newton "
+                                                   "step per device (ions, 241 steps, 4096 per "
+                                                   "batch; docs/hardware.md:62-66)",
+                       "transient_kernel_ms": kernel_ms,
+                       "start_converged_fraction": float(ok0[:m].float().mean()),
+                       "converged_fraction": float(o["converged"][:, :m].float().mean()),
+                       "accepted_fraction": float(acc.float().mean())},
+            "e2e": {"value": m * world / (e2e_ms / 1e3), "unit": "transients/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} HBM copy",
+                         "kernel": "dd::tr::transient_kernel (one thread per device)"},
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps * 2,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def workload_name(args, batch, nflat: int) -> str:
     if args.workload == "uneven":
         NPs = batch["NP"]
@@ -511,11 +679,15 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--precision", default="fp64", choices=("fp64",))
     ap.add_argument("--workload", default="config2",
-                    choices=("config2", "uneven", "adjoint", "impedance", "build"),
+                    choices=("config2", "uneven", "adjoint", "impedance", "build", "transient"),
                     help="config2: 16384 devices, NP 400, 61 V (the default); uneven: 32768 "
                          "devices, NP ~ U{150..900}, Nv ~ U{21..121}, one launch; adjoint: "
                          "gradients of a J-V misfit in 14 parameters, 4096 devices; "
-                         "impedance: 8192 devices without mobile ions, 41 frequencies")
+                         "impedance: 8192 devices without mobile ions, 41 frequencies; "
+                         "transient: 8192 devices with mobile ions, 2000 time steps")
+    ap.add_argument("--tsteps", type=int, default=2000,
+                    help="time steps of the transient workload (2000; fewer only for "
+                         "profiling)")
     ap.add_argument("--devices", type=int, default=0)
     ap.add_argument("--np", type=int, default=NP,
                     help="grid points of the fixed-size workload (400; smaller only for "
@@ -528,8 +700,8 @@ def main() -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     uneven = args.workload == "uneven"
     if not args.devices:
-        args.devices = {"uneven": 2 * DEVICES_PER_GPU, "adjoint": 4096,
-                        "impedance": 8192}.get(args.workload, DEVICES_PER_GPU)
+        args.devices = {"uneven": 2 * DEVICES_PER_GPU, "adjoint": 4096, "impedance": 8192,
+                        "transient": 8192}.get(args.workload, DEVICES_PER_GPU)
     if args.impl == "reference":
         reference_arm(args, rank)
         return
@@ -541,6 +713,9 @@ def main() -> None:
         return
     if args.workload == "build":
         build_bench(args, rank, world, local)
+        return
+    if args.workload == "transient":
+        transient_bench(args, rank, world, local)
         return
     if args.devices % 32:
         raise SystemExit("--devices must be a multiple of 32")

@@ -30,6 +30,8 @@ __all__ = ["pin_stack", "pin_texts", "drawn_stack", "drawn_devices", "SEED_DRAWN
 
 #: Seed of the per-device draws (workloads 2 and 3).
 SEED_DRAWN = 20261203
+#: config 5's device draws (the transient and small-signal workload)
+SEED_CONFIG5 = 20261205
 #: 61 voltages from -0.2 to 1.3 V.
 V_SCAN = np.round(np.linspace(-0.2, 1.3, 61), 10)
 #: The uneven workload's grid sizes and voltage counts: NP ~ U{150..900}, Nv ~ U{21..121}.
@@ -148,7 +150,7 @@ def drawn_devices(n: int, seed: int = SEED_DRAWN, NP: int | tuple[int, int] = 40
     return [drawn_device(k, seed, NP) for k in range(start, start + n)]
 
 
-def transient_devices(n: int, seed: int = SEED_DRAWN, NP: int = 400, start: int = 0):
+def transient_devices(n: int, seed: int = SEED_CONFIG5, NP: int = 400, start: int = 0):
     """Config 5's devices: the drawn workload's devices with free mobile ions (its odd indices:
     config 2's distributions, ions in the absorber, no pre-bias), `start .. start + n` of them."""
     return [drawn_device(2 * k + 1, seed, NP) for k in range(start, start + n)]
