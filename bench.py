@@ -531,7 +531,7 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
         # the oracle on one device of the same workload, a bounded number of its steps
         from jaxdd_b200.workloads import transient_devices
         from oracle import dd, transient
-        sample_steps = args.cpu_sample * 25
+        sample_steps = min(args.cpu_sample * 25, args.tsteps)
         tv = transient_steps(args.tsteps)
         d1 = dd.prepare(transient_devices(1, NP=args.np))
         t1 = time.perf_counter()
