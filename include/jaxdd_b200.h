@@ -168,6 +168,27 @@ int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
                   const double* vint, const double* laps, int n_freq, int bernoulli, double* Y,
                   void* workspace, size_t workspace_bytes, void* stream);
 
+#define DD_NT 3 /* per-point record of the transient and the impedance with ions: permittivity,
+                   anion and cation mobility */
+
+/* Scratch bytes dd_admittance_ions needs for this batch and n_freq frequencies. */
+int dd_admittance_ions_workspace_bytes(const dd_batch* batch, int n_freq, size_t* bytes);
+
+/* dd_admittance for devices with free mobile ions (jaxdd `_admittance` with `ions`,
+ * impedance.py:242-353): the ions are unknowns of their own, the 5x5 blocks of a time step of
+ * dt = 1 s from the steady state (its traps at their steady occupation) with (i omega - 1) M
+ * added on the diagonal, the traps' occupations' dynamics on the carriers' blocks, each ion
+ * region's number kept by a border (`_ion_constraints_time`), and each region's ion current in
+ * the linearised current. `state` [np_max+2][3][lane_stride] and `state_logs`
+ * [DD_MAXK][lane_stride] the steady state (dd_solve_states' checkpoint at `vint`, the ions
+ * Boltzmann's of those normalisations); `tstat` [np_max+2][DD_NT][lane_stride] the
+ * permittivity and the ions' mobilities. k_anion and k_cation must be 1; devices without mobile
+ * ions are solved too (their ions' rows identities). Y [n_freq][2][lane_stride]. */
+int dd_admittance_ions(const dd_batch* batch, const double* state, const double* state_logs,
+                       const double* tstat, const double* vint, const double* laps, int n_freq,
+                       int bernoulli, double* Y, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
 /* ---- Device building on the GPU (parameter sweeps) ------------------------------------------
  * The packed record of n devices of one stack structure from their parameters, as jaxdd's
  * `device_tree(structure, params)` (batch.py:142-148, device.py:877-1063) builds them for sweeps:
@@ -218,8 +239,6 @@ int dd_build(const dd_structure* structure, const double* layer_params,
              void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- Transients with mobile ions (jaxdd transient.py:270-465, 537-637) -------------------- */
-#define DD_NT 3 /* per-point transient record fields: permittivity, anion and cation mobility */
-
 /* ZimT's time steps (jaxdd `TVG`, simss_input.py:155-237). Lane l's step k is at [k] (stride 0:
  * one list for every lane) or at [k * lane_stride + l] (stride = lane_stride: one per lane). The first step is at t = 0 (a steady state); a later t = 0 returns to one. */
 typedef struct dd_steps {

@@ -37,7 +37,8 @@ DD_LANE_PREBIAS_FAILED = 1
 EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve",
            "dd_newton_step", "dd_solve_noalloc", "dd_solve_states", "dd_adjoint_workspace_bytes",
            "dd_adjoint", "dd_observables", "dd_admittance_workspace_bytes", "dd_admittance",
-           "dd_build", "dd_transient_workspace_bytes", "dd_transient")
+           "dd_build", "dd_transient_workspace_bytes", "dd_transient",
+           "dd_admittance_ions_workspace_bytes", "dd_admittance_ions")
 
 #: the transient's per-point record fields (include/jaxdd_b200.h DD_NT)
 DD_NT = 3
@@ -135,6 +136,12 @@ def lib() -> ctypes.CDLL:
     so.dd_build.restype = ctypes.c_int
     so.dd_build.argtypes = [ctypes.POINTER(DdStructure), p, p, ctypes.c_int, ctypes.c_int,
                             ctypes.c_int, ctypes.c_int, p, p, p, p, p, ctypes.c_size_t, p]
+    so.dd_admittance_ions_workspace_bytes.restype = ctypes.c_int
+    so.dd_admittance_ions_workspace_bytes.argtypes = [ctypes.POINTER(DdBatch), ctypes.c_int,
+                                                      ctypes.POINTER(ctypes.c_size_t)]
+    so.dd_admittance_ions.restype = ctypes.c_int
+    so.dd_admittance_ions.argtypes = [ctypes.POINTER(DdBatch), p, p, p, p, p, ctypes.c_int,
+                                      ctypes.c_int, p, p, ctypes.c_size_t, p]
     so.dd_transient_workspace_bytes.restype = ctypes.c_int
     so.dd_transient_workspace_bytes.argtypes = [ctypes.POINTER(DdBatch),
                                                 ctypes.POINTER(ctypes.c_size_t)]

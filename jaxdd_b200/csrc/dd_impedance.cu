@@ -22,6 +22,7 @@
 
 #include "dd_layout.h"
 #include "dd_physics.cuh"
+#include "dd_time.cuh"
 #include "../../include/jaxdd_b200.h"
 
 namespace dd {
@@ -541,11 +542,515 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
   }
 }
 
+// ------------------------------------------------------------------------------------ ions
+//
+// With mobile ions (jaxdd `_admittance` with `ions`, impedance.py:242-353) the ions are unknowns
+// of their own: the 5x5 blocks of a time step of dti = 1 from the steady state (the traps at
+// their steady occupation, `_time_terms` without occupations), `B + (iw - 1) M` on the diagonal,
+// the bulk and interface traps' blocks on the carriers' 3x3, and the ion slots as a border that
+// keeps each region's number (`_ion_constraints_time`); the current of a time step, linearised,
+// gains each region's ion current (`_ion_currents`, batch.py:421-483).
+
+// Per node of the ions' record, [node][word][lane]: the 5x5 blocks, the mass, the slot columns
+// U (anion row, cation row), the constraints' border W (at ln a, at ln c), and the ions'
+// densities and exp(-+V/V_T) of the steady state.
+enum { R_A = 0, R_B = 25, R_C = 50, R_M = 75, R_U3 = 80, R_U4, R_W3, R_W4, R_NA, R_NC, R_EVA,
+       R_EVC, R5_WORDS };
+// Per node of a (device, frequency) thread: c' (25 complex) and [-dF | U_a | U_c] (15 complex).
+enum { V_C = 0, V_D = 50, V_WORDS = 80 };
+
+struct IonArgs {
+  const double* X;           // [np+2][DD_NT][Bp]: permittivity, anion and cation mobility
+  const double* state_logs;  // [DD_MAXK][Bp]
+  double* rec5;              // [np+2][R5_WORDS][Bp]
+  double* scr5;              // [np+2][V_WORDS][T]
+};
+
+// A point of the steady state with its ions' logarithms (their Boltzmann profiles).
+__device__ void ion_point(const tr::View& W, int k, double Vint, const double* logs, tr::TP& P) {
+  const Lane& L = W.L;
+  if (k == 0 || k == L.NP + 1) contact(L, k != 0, Vint, P.c);
+  else { P.c.V = *L.y(0, k, 0); P.c.lnn = *L.y(0, k, 1); P.c.lnp = *L.y(0, k, 2); }
+  P.c.n = exp(P.c.lnn);
+  P.c.p = exp(P.c.lnp);
+  P.c.offn = L.st(k, S_OFFN);
+  P.c.offp = L.st(k, S_OFFP);
+  P.c.sl = slots_at(L, k);
+  const bool inner = k >= 1 && k <= L.NP;
+  P.la = inner && P.c.sl.a >= 0 ? logs[P.c.sl.a] + P.c.V * L.iVt : 0.0;
+  P.lc = inner && P.c.sl.c >= 0 ? logs[L.ka + P.c.sl.c] - P.c.V * L.iVt : 0.0;
+  P.a = exp(P.la);
+  P.c2 = exp(P.lc);
+  P.c.da = P.c.sl.a >= 0 ? P.a : 0.0;
+  P.c.dc = P.c.sl.c >= 0 ? P.c2 : 0.0;
+}
+
+__device__ void ion_view(tr::View& W, const Args& a, const IonArgs& b, int l) {
+  lane_init(W.L, a, l);
+  W.L.tot[0] = W.L.sc(C_TOT0);
+  W.L.tot[1] = W.L.sc(C_TOT0 + 1);
+  W.X = b.X;
+  W.Yb = nullptr;
+  W.ybuf = 0;
+  W.simss = a.simss;
+  W.zimt = 0;
+}
+
+// The ions' record of each device: its rows as a step of dti = 1 from the steady state itself.
+__global__ void __launch_bounds__(32) prepare_ions_kernel(Args a, IonArgs b) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= a.B) return;
+  tr::View W;
+  ion_view(W, a, b, l);
+  const Lane& L = W.L;
+  const int NP = L.NP;
+  const double Vint = a.vint[l];
+  double logs[2] = {b.state_logs[l], b.state_logs[(size_t)a.Bp + l]};
+  const double zero[2] = {0.0, 0.0};
+  auto rec = [&](int k, int f) -> double& {
+    return b.rec5[((size_t)k * R5_WORDS + f) * a.Bp + l];
+  };
+  tr::TP pm, pc, pn;
+  ion_point(W, 0, Vint, logs, pm);
+  ion_point(W, 1, Vint, logs, pc);
+  Flux el, er;
+  flux(L, pm.c, pc.c, L.st(0, S_MUN), L.st(0, S_MUP), el);
+  for (int i = 1; i <= NP; ++i) {
+    ion_point(W, i + 1, Vint, logs, pn);
+    flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
+    double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][2], M[5];
+    tr::row5<2, true>(W, i, pm, pc, pn, el, er, L.st(i - 1, S_H), L.st(i, S_H),
+                      (int)L.st(i - 1, S_IFK), (int)L.st(i, S_IFK), 1.0, 0.0, 0.0, 0.0, pc.c.n,
+                      pc.c.p, pc.c.da, pc.c.dc, zero, A, Bm, Cm, r, U, M);
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        rec(i, R_A + 5 * rr + c) = A[rr][c];
+        rec(i, R_B + 5 * rr + c) = Bm[rr][c];
+        rec(i, R_C + 5 * rr + c) = Cm[rr][c];
+      }
+      rec(i, R_M + rr) = M[rr];
+    }
+    rec(i, R_U3) = pc.c.sl.a >= 0 ? U[3][pc.c.sl.a] : 0.0;
+    rec(i, R_U4) = pc.c.sl.c >= 0 ? U[4][L.ka + pc.c.sl.c] : 0.0;
+    // the constraints' border: each region's number in its points' ion logarithms
+    const double hLm = L.st(i - 1, S_H) * L.L, hLp = L.st(i, S_H) * L.L;
+    double w3 = 0.0, w4 = 0.0;
+    if (pc.c.sl.a >= 0 && L.tot[pc.c.sl.a] > 0.0)
+      w3 = 0.5 * ((pm.c.sl.a == pc.c.sl.a ? hLm : 0.0) + (pn.c.sl.a == pc.c.sl.a ? hLp : 0.0)) *
+           pc.a / L.tot[pc.c.sl.a];
+    const int kc = L.ka + pc.c.sl.c;
+    if (pc.c.sl.c >= 0 && L.tot[kc] > 0.0)
+      w4 = 0.5 * ((pm.c.sl.c == pc.c.sl.c ? hLm : 0.0) + (pn.c.sl.c == pc.c.sl.c ? hLp : 0.0)) *
+           pc.c2 / L.tot[kc];
+    rec(i, R_W3) = w3;
+    rec(i, R_W4) = w4;
+    pm = pc; pc = pn; el = er;
+  }
+  for (int k = 0; k <= NP + 1; ++k) {
+    tr::TP P;
+    ion_point(W, k, Vint, logs, P);
+    rec(k, R_NA) = P.c.da;
+    rec(k, R_NC) = P.c.dc;
+    rec(k, R_EVA) = exp(-P.c.V * L.iVt);
+    rec(k, R_EVC) = exp(P.c.V * L.iVt);
+  }
+}
+
+// M^-1 applied in place, M = [[P, Q], [R, S]] complex, by its partition (as `tr::partition`).
+struct CPart {
+  cplx Pi[3][3], PiQ[3][2], R[2][3], Si[2][2];
+};
+
+__device__ void cpartition(const cplx (&M)[5][5], CPart& f) {
+  cplx P[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) P[r][c] = M[r][c];
+  inv3c(P, f.Pi);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+      f.PiQ[r][c] = f.Pi[r][0] * M[0][3 + c] + f.Pi[r][1] * M[1][3 + c] + f.Pi[r][2] * M[2][3 + c];
+  cplx S[2][2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f.R[r][c] = M[3 + r][c];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+      S[r][c] = M[3 + r][3 + c] - (M[3 + r][0] * f.PiQ[0][c] + M[3 + r][1] * f.PiQ[1][c] +
+                                   M[3 + r][2] * f.PiQ[2][c]);
+  }
+  const cplx idet = mk(1.0) / (S[0][0] * S[1][1] - S[0][1] * S[1][0]);
+  f.Si[0][0] = S[1][1] * idet; f.Si[0][1] = mk(0.0) - S[0][1] * idet;
+  f.Si[1][0] = mk(0.0) - S[1][0] * idet; f.Si[1][1] = S[0][0] * idet;
+}
+
+__device__ void capply(const CPart& f, cplx (&v)[5]) {
+  cplx yt[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) yt[r] = f.Pi[r][0] * v[0] + f.Pi[r][1] * v[1] + f.Pi[r][2] * v[2];
+  cplx w[2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+    w[r] = v[3 + r] - (f.R[r][0] * yt[0] + f.R[r][1] * yt[1] + f.R[r][2] * yt[2]);
+  const cplx z0 = f.Si[0][0] * w[0] + f.Si[0][1] * w[1];
+  const cplx z1 = f.Si[1][0] * w[0] + f.Si[1][1] * w[1];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) v[r] = yt[r] - (f.PiQ[r][0] * z0 + f.PiQ[r][1] * z1);
+  v[3] = z0;
+  v[4] = z1;
+}
+
+__global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) {
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < (long)a.Bp * a.nf;
+       t += (long)gridDim.x * blockDim.x) {
+    const int l = (int)(t % a.Bp), q = (int)(t / a.Bp);
+    if (l >= a.B) continue;
+    tr::View W;
+    ion_view(W, a, b, l);
+    const Lane& L = W.L;
+    const int NP = L.NP;
+    const double Vint = a.vint[l];
+    const cplx lap = mk(a.laps[2 * q], a.laps[2 * q + 1]);
+    const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    auto rec = [&](int k, int f) { return a.rec[((size_t)k * P_WORDS + f) * a.Bp + l]; };
+    auto r5 = [&](int k, int f) { return b.rec5[((size_t)k * R5_WORDS + f) * a.Bp + l]; };
+    auto scr = [&](int k, int f) -> double& {
+      return b.scr5[((size_t)k * V_WORDS + f) * a.T + slot];
+    };
+    const double e = L.left;
+    // ---- forward elimination of (J + (iw - 1) M + traps) [dy | X_U] = [-dF/dV | U]
+    cplx cp[5][5], dp[5][3];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) cp[rr][c] = mk(0.0);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dp[rr][c] = mk(0.0);
+    }
+    for (int i = 1; i <= NP; ++i) {
+      cplx A[5][5], Bm[5][5], Cm[5][5];
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          A[rr][c] = mk(r5(i, R_A + 5 * rr + c));
+          Bm[rr][c] = mk(r5(i, R_B + 5 * rr + c));
+          Cm[rr][c] = mk(r5(i, R_C + 5 * rr + c));
+        }
+      const cplx lm1 = lap - mk(1.0);  // the step's dti = 1 is in B already
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) Bm[rr][rr] = Bm[rr][rr] + r5(i, R_M + rr) * lm1;
+      // bulk traps beyond their instantaneous occupation (the carriers' 3x3)
+      const double ta = rec(i, P_TA);
+      const cplx h = mk(0.0) - lap / (lap + mk(ta));
+      const double fsc = L.st(i, S_FAC) * L.st(i, S_SC);
+      const cplx rn = (rec(i, P_TDN) / ta) * h, rp = (rec(i, P_TDP) / ta) * h;
+      Bm[1][1] = Bm[1][1] - (fsc * rec(i, P_TRN)) * rn;
+      Bm[1][2] = Bm[1][2] - (fsc * rec(i, P_TRN)) * rp;
+      Bm[2][1] = Bm[2][1] - (fsc * rec(i, P_TRP)) * rn;
+      Bm[2][2] = Bm[2][2] - (fsc * rec(i, P_TRP)) * rp;
+      if ((int)L.st(i - 1, S_IFK) >= 0 || (int)L.st(i, S_IFK) >= 0) {
+        const double rs[3] = {Q * L.st(i, S_SP), -L.st(i, S_FAC) * L.st(i, S_SC),
+                              -L.st(i, S_FAC) * L.st(i, S_SC)};
+        cplx dA[3][3], dB[3][3], dC[3][3];
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) { dA[rr][c] = mk(0.0); dB[rr][c] = mk(0.0); dC[rr][c] = mk(0.0); }
+        iface_rows(L, i, Vint, lap, rs, dA, dB, dC);
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            A[rr][c] = A[rr][c] + dA[rr][c];
+            Bm[rr][c] = Bm[rr][c] + dB[rr][c];
+            Cm[rr][c] = Cm[rr][c] + dC[rr][c];
+          }
+      }
+      // right-hand sides: -dF/dV (the contacts' potentials), then the slots' columns
+      cplx rhs[5][3];
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+        double dF = 0.0;
+        if (i == 1) dF += r5(1, R_A + 5 * rr) * 0.5 * e;
+        if (i == NP) dF += r5(NP, R_C + 5 * rr) * (-0.5 * e);
+        rhs[rr][0] = mk(-dF);
+        rhs[rr][1] = mk(rr == 3 ? r5(i, R_U3) : 0.0);
+        rhs[rr][2] = mk(rr == 4 ? r5(i, R_U4) : 0.0);
+      }
+      cplx M[5][5];
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          cplx s = Bm[rr][c];
+#pragma unroll
+          for (int k = 0; k < 5; ++k) s = s - A[rr][k] * cp[k][c];
+          M[rr][c] = s;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          cplx s = rhs[rr][c];
+#pragma unroll
+          for (int k = 0; k < 5; ++k) s = s - A[rr][k] * dp[k][c];
+          rhs[rr][c] = s;
+        }
+      }
+      CPart f;
+      cpartition(M, f);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        cplx v[5] = {Cm[0][c], Cm[1][c], Cm[2][c], Cm[3][c], Cm[4][c]};
+        capply(f, v);
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) {
+          cp[rr][c] = v[rr];
+          scr(i, V_C + 2 * (5 * rr + c)) = v[rr].re;
+          scr(i, V_C + 2 * (5 * rr + c) + 1) = v[rr].im;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cplx v[5] = {rhs[0][c], rhs[1][c], rhs[2][c], rhs[3][c], rhs[4][c]};
+        capply(f, v);
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) {
+          dp[rr][c] = v[rr];
+          scr(i, V_D + 2 * (3 * rr + c)) = v[rr].re;
+          scr(i, V_D + 2 * (3 * rr + c) + 1) = v[rr].im;
+        }
+      }
+    }
+    // ---- back substitution, and the slots' Schur complement D - W^T X_U
+    cplx SM[2][2] = {{mk(L.tot[0] > 0.0 ? 0.0 : 1.0), mk(0.0)},
+                     {mk(0.0), mk(L.tot[1] > 0.0 ? 0.0 : 1.0)}};
+    cplx sr[2] = {mk(0.0), mk(0.0)};
+    {
+      cplx xn[5][3];
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xn[rr][c] = mk(0.0);
+      for (int i = NP; i >= 1; --i) {
+        cplx xi[5][3];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            cplx s = mk(scr(i, V_D + 2 * (3 * rr + c)), scr(i, V_D + 2 * (3 * rr + c) + 1));
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+              s = s - mk(scr(i, V_C + 2 * (5 * rr + k)), scr(i, V_C + 2 * (5 * rr + k) + 1)) *
+                          xn[k][c];
+            xi[rr][c] = s;
+          }
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            xn[rr][c] = xi[rr][c];
+            scr(i, V_D + 2 * (3 * rr + c)) = xi[rr][c].re;
+            scr(i, V_D + 2 * (3 * rr + c) + 1) = xi[rr][c].im;
+          }
+        const double w[2] = {r5(i, R_W3), r5(i, R_W4)};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          if (w[k] == 0.0) continue;
+          sr[k] = sr[k] - w[k] * xi[3 + k][0];
+          SM[k][0] = SM[k][0] - w[k] * xi[3 + k][1];
+          SM[k][1] = SM[k][1] - w[k] * xi[3 + k][2];
+        }
+      }
+    }
+    const cplx idet = mk(1.0) / (SM[0][0] * SM[1][1] - SM[0][1] * SM[1][0]);
+    const cplx z0 = (SM[1][1] * sr[0] - SM[0][1] * sr[1]) * idet;
+    const cplx z1 = (SM[0][0] * sr[1] - SM[1][0] * sr[0]) * idet;
+    // dy = X_F - X_U z, written over X_F
+    for (int i = 1; i <= NP; ++i)
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+        const cplx xf = mk(scr(i, V_D + 2 * (3 * rr)), scr(i, V_D + 2 * (3 * rr) + 1));
+        const cplx x1 = mk(scr(i, V_D + 2 * (3 * rr + 1)), scr(i, V_D + 2 * (3 * rr + 1) + 1));
+        const cplx x2 = mk(scr(i, V_D + 2 * (3 * rr + 2)), scr(i, V_D + 2 * (3 * rr + 2) + 1));
+        const cplx dy = xf - (x1 * z0 + x2 * z1);
+        scr(i, V_D + 2 * (3 * rr)) = dy.re;
+        scr(i, V_D + 2 * (3 * rr) + 1) = dy.im;
+      }
+    // ---- the current's tangent: the carriers' and the displacement current as without ions,
+    // then each ion region's (its base and per-dt parts)
+    auto dyv = [&](int k, int c) -> cplx {
+      if (k < 1 || k > NP) return mk(0.0);
+      return mk(scr(k, V_D + 2 * (3 * c)), scr(k, V_D + 2 * (3 * c) + 1));
+    };
+    auto dV = [&](int k) -> cplx {
+      if (k == 0) return mk(0.5 * e);
+      if (k == NP + 1) return mk(-0.5 * e);
+      return dyv(k, 0);
+    };
+    const double sign = -L.left;
+    const double Vt = L.Vt;
+    cplx dsgl[2] = {mk(0.0), mk(0.0)}, ddb_b[2] = {mk(0.0), mk(0.0)}, ddb_t[2] = {mk(0.0), mk(0.0)};
+    cplx diu_b[2] = {mk(0.0), mk(0.0)}, diu_t[2] = {mk(0.0), mk(0.0)};
+    cplx dS_b[2] = {mk(0.0), mk(0.0)}, dS_t[2] = {mk(0.0), mk(0.0)};
+    cplx sumJ_b[2] = {mk(0.0), mk(0.0)}, sumJ_t[2] = {mk(0.0), mk(0.0)};
+    cplx duc_prev_b[2] = {mk(0.0), mk(0.0)}, duc_prev_t[2] = {mk(0.0), mk(0.0)};
+    cplx dJD = mk(0.0);
+    // the ions, per region (one per species): sums over the region's intervals
+    double is_[2] = {0.0, 0.0}, iH[2] = {0.0, 0.0}, aev_f[2] = {0.0, 0.0}, aev_l[2] = {0.0, 0.0};
+    cplx dis[2] = {mk(0.0), mk(0.0)}, diu_i[2] = {mk(0.0), mk(0.0)}, ddbl_i[2] = {mk(0.0), mk(0.0)};
+    cplx dP_i[2] = {mk(0.0), mk(0.0)}, dsum_i[2] = {mk(0.0), mk(0.0)};
+    cplx daev_f[2] = {mk(0.0), mk(0.0)}, daev_l[2] = {mk(0.0), mk(0.0)};
+    int first_i[2] = {-1, -1};
+    double hsum = 0.0, dx_prev = 0.0, h_prev = 0.0;
+    for (int k = 0; k <= NP; ++k) {
+      const double hk = L.st(k, S_H);
+      const double dx = k < NP ? L.st(k, S_DX) : 0.0;
+      const double wk = 0.5 * (dx_prev + dx);
+      const double width = k == 0 ? hk : 0.5 * (h_prev + hk);
+      hsum += hk;
+      cplx dRi_k[2] = {mk(0.0), mk(0.0)}, dRi_k1[2] = {mk(0.0), mk(0.0)};
+      bool trapped = false;
+      for (int ee = k - 1; ee <= k + 1; ++ee)
+        if (ee >= 0 && ee <= NP && (int)L.st(ee, S_IFK) >= 0) trapped = true;
+      if (trapped) {
+        const cplx ln[3] = {dyv(k - 1, 1), dyv(k, 1), dyv(k + 1, 1)};
+        const cplx lp[3] = {dyv(k - 1, 2), dyv(k, 2), dyv(k + 1, 2)};
+        iface_tangent(L, k, Vint, lap, ln, lp, dRi_k[0], dRi_k[1]);
+        if (k + 1 <= NP + 1) {
+          const cplx ln1[3] = {dyv(k, 1), dyv(k + 1, 1), dyv(k + 2, 1)};
+          const cplx lp1[3] = {dyv(k, 2), dyv(k + 1, 2), dyv(k + 2, 2)};
+          iface_tangent(L, k + 1, Vint, lap, ln1, lp1, dRi_k1[0], dRi_k1[1]);
+        }
+      }
+      cplx dU[2] = {mk(0.0), mk(0.0)};
+      if (k >= 1) {
+        const double ta = rec(k, P_TA);
+        const cplx h = mk(0.0) - lap / (lap + mk(ta));
+        const cplx df = ((rec(k, P_TDN) / ta) * h) * dyv(k, 1) + ((rec(k, P_TDP) / ta) * h) * dyv(k, 2);
+        dU[0] = rec(k, P_TRN) * df;
+        dU[1] = rec(k, P_TRP) * df;
+      }
+      const bool iface_k = L.st(k, S_IFK) > -1.5;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const double sn = c == 0 ? -1.0 : 1.0;
+        const double ev = rec(k, c == 0 ? P_EVN : P_EVP), iu = rec(k, c == 0 ? P_IUN : P_IUP);
+        const double mu = L.st(k, c == 0 ? S_MUN : S_MUP);
+        const cplx dev = (ev * sn / Vt) * dV(k);
+        cplx duc_b = mk(0.0), duc_t = mk(0.0);
+        if (k >= 1) {
+          duc_b = rec(k, P_DRN) * dyv(k, 1) + rec(k, P_DRP) * dyv(k, 2) + dRi_k[c] + dU[c];
+          duc_t = rec(k, c == 0 ? P_N : P_P) * dyv(k, 1 + c);
+          diu_b[c] = diu_b[c] + (0.5 * dx_prev) * (duc_prev_b[c] + duc_b);
+          diu_t[c] = diu_t[c] + (0.5 * dx_prev) * (duc_prev_t[c] + duc_t);
+        }
+        dsgl[c] = dsgl[c] + (wk / mu) * dev;
+        ddb_b[c] = ddb_b[c] + (wk * iu / mu) * dev + (wk * ev / mu) * diu_b[c];
+        ddb_t[c] = ddb_t[c] + (wk * ev / mu) * diu_t[c];
+        const cplx dS_prev_b = dS_b[c], dS_prev_t = dS_t[c];
+        if (k >= 1) {
+          dS_b[c] = dS_b[c] + (sn * Q * L.L * width) * duc_b;
+          dS_t[c] = dS_t[c] + (sn * Q * L.L * width) * duc_t;
+        }
+        if (iface_k) {
+          const cplx thr = (sn * 0.5 * Q * L.L * hk) * (dRi_k[c] + dRi_k1[c]);
+          sumJ_b[c] = sumJ_b[c] + hk * (dS_prev_b + thr);
+          sumJ_t[c] = sumJ_t[c] + hk * dS_prev_t;
+        } else {
+          sumJ_b[c] = sumJ_b[c] + hk * dS_b[c];
+          sumJ_t[c] = sumJ_t[c] + hk * dS_t[c];
+        }
+        duc_prev_b[c] = duc_b;
+        duc_prev_t[c] = duc_t;
+      }
+      const double epsk = W.x(k, tr::T_EPS);
+      dJD = dJD + (hk * sign * epsk / (L.L * hk)) * (dV(k + 1) - dV(k));
+      // the ions over interval k (points k, k+1): `_ion_currents` linearised at U = 0
+      const Slots sa = slots_at(L, k), sb = slots_at(L, k + 1);
+#pragma unroll
+      for (int sp = 0; sp < 2; ++sp) {
+        if (!(L.tot[sp] > 0.0)) continue;
+        const double sn = sp == 0 ? -1.0 : 1.0;
+        const bool ina = (sp == 0 ? sa.a : sa.c) == 0, inb = (sp == 0 ? sb.a : sb.c) == 0;
+        const int tf = sp == 0 ? tr::T_MUA : tr::T_MUC;
+        const double na = r5(k, sp == 0 ? R_NA : R_NC), nb = r5(k + 1, sp == 0 ? R_NA : R_NC);
+        const double eva = r5(k, sp == 0 ? R_EVA : R_EVC), evb = r5(k + 1, sp == 0 ? R_EVA : R_EVC);
+        const cplx dlna = dyv(k, 3 + sp), dlnb = dyv(k + 1, 3 + sp);
+        const cplx deva = (eva * sn / Vt) * dV(k), devb = (evb * sn / Vt) * dV(k + 1);
+        if (ina && first_i[sp] < 0) {
+          first_i[sp] = k;
+          aev_f[sp] = na * eva;
+          daev_f[sp] = (na * eva) * dlna + na * deva;
+        }
+        if (inb) {
+          aev_l[sp] = nb * evb;
+          daev_l[sp] = (nb * evb) * dlnb + nb * devb;
+        }
+        if (ina && inb) {
+          const double mua = W.x(k, tf), mub = W.x(k + 1, tf);
+          const double ia = 1.0 / (mua > 0.0 ? mua : 1.0), ib = 1.0 / (mub > 0.0 ? mub : 1.0);
+          const cplx dUa = na * dlna, dUb = nb * dlnb;  // per unit of dti
+          const cplx diu_b2 = diu_i[sp] + (0.5 * dx) * (dUa + dUb);
+          is_[sp] += 0.5 * dx * (eva * ia + evb * ib);
+          dis[sp] = dis[sp] + (0.5 * dx) * (ia * deva + ib * devb);
+          ddbl_i[sp] = ddbl_i[sp] + (0.5 * dx * eva * ia) * diu_i[sp] + (0.5 * dx * evb * ib) * diu_b2;
+          diu_i[sp] = diu_b2;
+          const cplx dstep = k > first_i[sp] ? (sn * Q * L.L * width) * dUa : mk(0.0);
+          dP_i[sp] = dP_i[sp] + dstep;
+          iH[sp] += hk;
+          dsum_i[sp] = dsum_i[sp] + hk * (iface_k ? dP_i[sp] - dstep : dP_i[sp]);
+        }
+      }
+      dx_prev = dx;
+      h_prev = hk;
+    }
+    cplx Yb = mk(0.0), Yt = mk(0.0);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const double sn = c == 0 ? -1.0 : 1.0;
+      const double sgl = a.lsc[(size_t)(L_SN + c) * a.Bp + l], K = a.lsc[(size_t)(L_KN + c) * a.Bp + l];
+      Pt P0, PR;
+      point(L, 0, Vint, P0);
+      point(L, NP + 1, Vint, PR);
+      const double d0 = c == 0 ? P0.n : P0.p, dR = c == 0 ? PR.n : PR.p;
+      const double e0 = exp(sn * ((c == 0 ? P0.offn : P0.offp) + P0.V) / Vt);
+      const double eR = exp(sn * ((c == 0 ? PR.offn : PR.offp) + PR.V) / Vt);
+      const cplx dBc = (Vt * sn) * ((dR * eR * sn / Vt) * dV(NP + 1) - (d0 * e0 * sn / Vt) * dV(0));
+      const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (K / sgl) * dsgl[c];
+      const cplx dK_t = (-sn / sgl) * ddb_t[c];
+      Yb = Yb + sign * (Q * hsum) * dK_b + sign * sumJ_b[c];
+      Yt = Yt + sign * (Q * hsum) * dK_t + sign * sumJ_t[c];
+    }
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) {
+      if (!(L.tot[sp] > 0.0) || first_i[sp] < 0) continue;
+      const double sn = sp == 0 ? -1.0 : 1.0;
+      const double sgl = is_[sp] > 0.0 ? is_[sp] : 1.0;
+      const double K0 = Vt * sn * (aev_l[sp] - aev_f[sp]) / sgl;  // the state's (U = 0)
+      const cplx dK_b = (Vt * sn / sgl) * (daev_l[sp] - daev_f[sp]) - (K0 / sgl) * dis[sp];
+      const cplx dK_t = (-sn / sgl) * ddbl_i[sp];
+      Yb = Yb + sign * (Q * iH[sp]) * dK_b;
+      Yt = Yt + sign * ((Q * iH[sp]) * dK_t + dsum_i[sp]);
+    }
+    Yt = Yt + dJD;
+    const cplx Y = (1.0 / hsum) * (Yb + lap * Yt);
+    a.Y[((size_t)q * 2) * a.Bp + l] = Y.re;
+    a.Y[((size_t)q * 2 + 1) * a.Bp + l] = Y.im;
+  }
+}
+
 }  // namespace imp
 }  // namespace dd
 
 namespace {
 long imp_threads() { return 148L * 256; }
+long imp_ion_threads() { return 148L * 128; }
 }
 
 extern "C" {
@@ -591,6 +1096,58 @@ int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   dd::imp::prepare_kernel<<<(unsigned)((Bp + 63) / 64), 64, 0, s>>>(a);
   dd::imp::admittance_kernel<<<(unsigned)((T + 63) / 64), 64, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+}
+
+int dd_admittance_ions_workspace_bytes(const dd_batch* batch, int n_freq, size_t* bytes) {
+  if (!batch || !bytes || n_freq < 1 || batch->n_lanes < 1 || batch->lane_stride % 32 != 0 ||
+      batch->np_max < 3)
+    return DD_ERR_ARGS;
+  const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
+  long T = (long)Bp * n_freq;
+  if (T > imp_ion_threads()) T = imp_ion_threads();
+  *bytes = (nodes * dd::imp::P_WORDS * Bp + dd::imp::L_WORDS * Bp +
+            nodes * dd::imp::R5_WORDS * Bp + nodes * dd::imp::V_WORDS * (size_t)T) *
+           sizeof(double);
+  return DD_OK;
+}
+
+int dd_admittance_ions(const dd_batch* batch, const double* state, const double* state_logs,
+                       const double* tstat, const double* vint, const double* laps, int n_freq,
+                       int bernoulli, double* Y, void* workspace, size_t workspace_bytes,
+                       void* stream) {
+  if (!batch || !batch->stat || !batch->scal || !batch->iface || !state || !state_logs ||
+      !tstat || !vint || !laps || n_freq < 1 || !Y || !workspace)
+    return DD_ERR_ARGS;
+  if (batch->n_lanes < 1 || batch->lane_stride < batch->n_lanes || batch->lane_stride % 32 != 0 ||
+      batch->np_max < 3 || batch->k_anion != 1 || batch->k_cation != 1)
+    return DD_ERR_ARGS;
+  if (bernoulli != DD_BERNOULLI_EXACT && bernoulli != DD_BERNOULLI_SIMSS) return DD_ERR_ARGS;
+  size_t need;
+  dd_admittance_ions_workspace_bytes(batch, n_freq, &need);
+  if (workspace_bytes < need) return DD_ERR_WORKSPACE;
+  const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
+  dd::imp::Args a{};
+  a.B = batch->n_lanes; a.Bp = batch->lane_stride; a.npmax = batch->np_max; a.ka = batch->k_anion;
+  a.simss = bernoulli == DD_BERNOULLI_SIMSS; a.nf = n_freq;
+  a.S = batch->stat; a.C = batch->scal; a.IFt = batch->iface;
+  a.state = state; a.eps = nullptr; a.vint = vint; a.laps = laps; a.Y = Y;
+  double* ws = static_cast<double*>(workspace);
+  a.rec = ws;
+  a.lsc = ws + nodes * dd::imp::P_WORDS * Bp;
+  dd::imp::IonArgs b{};
+  b.X = tstat;
+  b.state_logs = state_logs;
+  b.rec5 = a.lsc + dd::imp::L_WORDS * Bp;
+  b.scr5 = b.rec5 + nodes * dd::imp::R5_WORDS * Bp;
+  a.scr = nullptr;
+  long T = (long)Bp * n_freq;
+  if (T > imp_ion_threads()) T = imp_ion_threads();
+  a.T = T;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  dd::imp::prepare_kernel<<<(unsigned)((Bp + 63) / 64), 64, 0, s>>>(a);
+  dd::imp::prepare_ions_kernel<<<(unsigned)((Bp + 31) / 32), 32, 0, s>>>(a, b);
+  dd::imp::admittance_ions_kernel<<<(unsigned)((T + 63) / 64), 64, 0, s>>>(a, b);
   return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
 }
 

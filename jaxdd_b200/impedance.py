@@ -1,11 +1,13 @@
 """Impedance in the frequency domain from the steady state's Jacobian: jaxdd's
-`solve_impedance` (src/jaxdd/impedance.py:365-409) for devices without mobile ions.
+`solve_impedance` (src/jaxdd/impedance.py:365-409).
 
 At the steady state of each device at `voltage` (the solve's own, `dd_solve_states`) a small
 voltage drives `(J + iωM)·δy = −(∂F/∂V)·δV`, the traps' occupations following at their own rates;
 `dd_admittance` solves it for every (device, frequency) on the GPU and linearises the current of
-a time step (`Y = δJ/δV`). With a series resistance and a shunt the external
-`Z = 1/(Y + G_shunt) + R_series`.
+a time step (`Y = δJ/δV`). A batch with free mobile ions goes through `dd_admittance_ions`: the
+ions are unknowns of their own (5×5 blocks, each region's number kept by a border), and the
+linearised current has each region's ion current. With a series resistance and a shunt the
+external `Z = 1/(Y + G_shunt) + R_series`.
 """
 
 from __future__ import annotations
@@ -36,6 +38,11 @@ class ImpedanceResult:
         return self.Y.imag / (2 * np.pi * self.frequencies)
 
 
+def _mobile(batch: Batch) -> bool:
+    """Whether any device of the batch has mobile ions (jaxdd impedance.py:391)."""
+    return any(d.anion_total > 0 or d.cation_total > 0 for d in batch["devices"])
+
+
 class Work:
     """The device-side inputs of one impedance run, packed once: the plan of the steady solve at
     `voltage`, the permittivities, the frequencies, the output and the workspace. `run()` solves
@@ -53,10 +60,18 @@ class Work:
         self.bern = _lib.DD_BERNOULLI[bernoulli_name]
         Bp, nodes, lanes = batch["Bp"], batch["np_max"] + 2, batch["lane_of"]
         cuda = self.g.stat.device
-        eps = np.zeros((nodes, Bp))
+        self.ions = _mobile(batch)
+        # the permittivity (and, with ions, the ions' mobilities) at every point
+        X = np.zeros((nodes, _lib.DD_NT, Bp))
         for k, d in enumerate(batch["devices"]):
-            eps[:len(d.x), lanes[k]] = d.eps
-        self.eps = torch.from_numpy(eps).to(cuda)
+            m = len(d.x)
+            X[:m, 0, lanes[k]] = d.eps
+            if d.mu_anion is not None:
+                X[:m, 1, lanes[k]] = d.mu_anion
+            if d.mu_cation is not None:
+                X[:m, 2, lanes[k]] = d.mu_cation
+        self.X = torch.from_numpy(X).to(cuda)
+        self.eps = self.X[:, 0, :].contiguous()
         self.vint = torch.full((Bp,), float(voltage), dtype=torch.float64, device=cuda)
         laps = np.zeros((len(frequencies), 2))
         laps[:, 1] = 2 * np.pi * np.asarray(frequencies, dtype=float)
@@ -65,8 +80,9 @@ class Work:
         self.Y = torch.empty((self.nf, 2, Bp), dtype=torch.float64, device=cuda)
         size = ctypes.c_size_t(0)
         desc = descriptor(batch, self.g, self.plan.y0)
-        _lib.check(_lib.lib().dd_admittance_workspace_bytes(ctypes.byref(desc), self.nf,
-                                                           ctypes.byref(size)),
+        query = (_lib.lib().dd_admittance_ions_workspace_bytes if self.ions
+                 else _lib.lib().dd_admittance_workspace_bytes)
+        _lib.check(query(ctypes.byref(desc), self.nf, ctypes.byref(size)),
                    "dd_admittance_workspace_bytes")
         self.ws = torch.empty(size.value, dtype=torch.uint8, device=cuda)
 
@@ -77,11 +93,18 @@ class Work:
         J, ok, _, ckpt = _solve_states(self.plan, g.stat, g.scal, g.iface)
         state = ckpt["states"][0]
         desc = descriptor(self.batch, g, state)
-        _lib.check(_lib.lib().dd_admittance(
-            ctypes.byref(desc), state.data_ptr(), self.eps.data_ptr(), self.vint.data_ptr(),
-            self.laps.data_ptr(), self.nf, self.bern, self.Y.data_ptr(), self.ws.data_ptr(),
-            self.ws.numel(), torch.cuda.current_stream(g.stat.device).cuda_stream),
-            "dd_admittance")
+        stream = torch.cuda.current_stream(g.stat.device).cuda_stream
+        if self.ions:
+            _lib.check(_lib.lib().dd_admittance_ions(
+                ctypes.byref(desc), state.data_ptr(), ckpt["logs"][0].data_ptr(),
+                self.X.data_ptr(), self.vint.data_ptr(), self.laps.data_ptr(), self.nf,
+                self.bern, self.Y.data_ptr(), self.ws.data_ptr(), self.ws.numel(), stream),
+                "dd_admittance_ions")
+        else:
+            _lib.check(_lib.lib().dd_admittance(
+                ctypes.byref(desc), state.data_ptr(), self.eps.data_ptr(), self.vint.data_ptr(),
+                self.laps.data_ptr(), self.nf, self.bern, self.Y.data_ptr(), self.ws.data_ptr(),
+                self.ws.numel(), stream), "dd_admittance")
         return J, ok, self.Y
 
 
@@ -89,15 +112,17 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
                     max_iter: int = 60, bernoulli_name: str = "exact") -> ImpedanceResult:
     """The impedance of a batch at the internal voltage `voltage` (V) at each of `frequencies`
     (Hz), from the steady state there by one complex linear solve per frequency (jaxdd
-    impedance.py:365-409). Devices with mobile ions are refused (`NotImplementedError`): their
-    small-signal response needs the ions as unknowns of their own, which this build does not
-    carry."""
+    impedance.py:365-409). Free mobile ions move with the voltage as unknowns of their own.
+    Refused (`NotImplementedError`), as the reference refuses them or as this build does not
+    carry them: ions frozen at a pre-bias, several ion regions of a species, the differential
+    current (`currDiffInt = 1`)."""
     devs = batch["devices"]
-    if any(d.anion_total > 0 or d.cation_total > 0 for d in devs):
-        raise NotImplementedError("impedance with mobile ions: not built (the ions' own "
-                                  "equations in the small-signal system)")
+    if _mobile(batch) and any(d.pre_cond and d.fix_ions for d in devs):
+        raise NotImplementedError("impedance with ions frozen at a pre-bias")
     if batch["ka"] != 1 or batch["kc"] != 1:
-        raise NotImplementedError("impedance with ion regions")
+        raise NotImplementedError("impedance with several ion regions of a species")
+    if any(d.curr_diff for d in devs):
+        raise NotImplementedError("impedance with the differential current (currDiffInt = 1)")
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
     work = Work(batch, frequencies, voltage, tol=tol, max_iter=max_iter,
                 bernoulli_name=bernoulli_name)

@@ -1,5 +1,6 @@
 """Oracle (test infrastructure): a CPU restatement of jaxdd's small-signal impedance
-(src/jaxdd/impedance.py) for devices without mobile ions, in FP64/complex128 NumPy.
+(src/jaxdd/impedance.py), in FP64/complex128 NumPy; devices with free mobile ions take them as
+unknowns of their own (`admittance_ions`, built on `oracle.transient`'s 5×5 rows).
 
 Only the tests import this module. It restates, one device at a time:
 
@@ -250,22 +251,119 @@ def admittance(d, full0, Vint, laps, bern):
     return np.array(out)
 
 
+def admittance_ions(d, full0, Vint, laps, bern):
+    """One device's δJ/δV_int at each `iω` of `laps` with its mobile ions as unknowns of their
+    own (`_admittance` with `ions`, impedance.py:242-353): the 5×5 blocks of a time step of
+    `dti` = 1 from the steady state `full0` ((NP + 2) × 5: V, ln n, ln p, ln a, ln c; the
+    ions' 0 outside their regions) with the traps steady (`oracle.transient.assemble`),
+    `Bb + (iω − 1)·M` on the diagonal, the traps' blocks on the carriers' 3×3, the ion slots as
+    a border keeping each region's number (`_ion_constraints_time`), and the current of a time
+    step linearised (the ions' currents included) by complex step."""
+    from . import transient
+    s = {k: v[0] for k, v in d["s"].items()}
+    rec = {k: v[0] for k, v in d["rec"].items()}
+    ti = {k: v[0] for k, v in d["ti"].items()}
+    ion = d["ion"]
+    y = full0[1:-1]
+    NP = y.shape[0]
+    K = ion["a_slots"].shape[1] + ion["c_slots"].shape[1]
+    logs = np.zeros((1, K))
+    n, p = np.exp(y[:, 1]), np.exp(y[:, 2])
+    n_full, p_full = np.exp(full0[:, 1]), np.exp(full0[:, 2])
+    am, cm = s["a_mask"], s["c_mask"]
+    tr = {"dti": np.array([1.0]), "n": n[None], "p": p[None], "a": (np.exp(y[:, 3]) * am)[None],
+          "c": (np.exp(y[:, 4]) * cm)[None], "fb": None, "fi": None}
+    _, A, Bb, C, U, M = transient.assemble(full0[None], d, tr, logs, bern, steady_traps=True,
+                                           mass=True)
+    A, Bb, C, U, M = A[0], Bb[0], C[0], U[0], M[0]
+    _, W, D = transient.constraints(full0[None], logs, ion)
+    W, D = W[0], D[0]
+    e = d["left_elec"][0]
+    dF = np.zeros((NP, 5))
+    dF[0] += A[0][:, 0] * 0.5 * e
+    dF[-1] += C[-1][:, 0] * (-0.5 * e)
+    ma, mc = ion["a_slots"][0].sum(0), ion["c_slots"][0].sum(0)
+    tr0 = {"dti": np.array([0.0]), "n": n_full[None], "p": p_full[None],
+           "a": (np.exp(full0[:, 3]) * ma)[None], "c": (np.exp(full0[:, 4]) * mc)[None],
+           "V": full0[None, :, 0]}
+    h_cs = 1e-30
+
+    def total(y_, V_, dti, dU=None, dRi=None):
+        t = dict(tr0, dti=np.array([dti]))
+        return transient.current(d, transient.full_of(d, y_[None], np.array([V_])), t, bern,
+                                 False, steady_traps=True, dU=dU, dRi=dRi)[0]
+
+    def linear(dy_real, dV, dti):  # J_y dy + J_V dV at dti, by complex step
+        return np.imag(total(y + 1j * h_cs * dy_real, Vint + 1j * h_cs * dV, dti)) / h_cs
+
+    def rates(dU, dRi):
+        J0 = total(y.astype(complex), complex(Vint), 0.0)
+        J1 = total(y.astype(complex), complex(Vint), 0.0, tuple(v[None] for v in dU),
+                   tuple(v[None] for v in dRi))
+        return J1 - J0
+
+    eye = np.eye(5)
+    out = []
+    for lap in laps:
+        Bl = Bb + ((lap - 1.0) * M)[:, :, None] * eye[None]
+        Bl[:, :3, :3] += trap_blocks(s, {k: v[1:-1] for k, v in rec.items()}, n, p, lap)
+        Al, Cl = A.astype(complex), C.astype(complex)
+        if np.any(ti["Nt"] > 0):
+            dA, dB, dC = interface_blocks(s, ti, n_full, p_full, lap)
+            Al[:, :3, :3] += dA
+            Bl[:, :3, :3] += dB
+            Cl[:, :3, :3] += dC
+        rhs = np.concatenate([(-dF).astype(complex)[:, :, None], U.astype(complex)], -1)
+        X = transient.block_thomas(Al[None], Bl[None], Cl[None], rhs[None])[0]
+        XF, XU = X[..., 0], X[..., 1:]
+        schur = D - np.einsum("kir,irl->kl", W, XU)
+        z = np.linalg.solve(schur, -np.einsum("kir,ir->k", W, XF))
+        dy = XF - XU @ z
+        J0 = linear(dy.real, 1.0, 0.0) + 1j * linear(dy.imag, 0.0, 0.0)
+        J1 = linear(dy.real, 1.0, 1.0) + 1j * linear(dy.imag, 0.0, 1.0)
+        a, drive, dR = trap_terms({k: v[1:-1] for k, v in rec.items()}, n, p)
+        rate = drive / a[:, None] * _step_transfer(a, lap)[:, None]
+        df = rate[:, 0] * dy[:, 1] + rate[:, 1] * dy[:, 2]
+        pad = np.zeros(1)
+        dUn = np.concatenate([pad, dR[0] * df, pad])
+        dUp = np.concatenate([pad, dR[1] * df, pad])
+        if np.any(ti["Nt"] > 0):
+            dRn, dRp = interface_rates(ti, n_full, p_full, lap, dy[:, :3])
+        else:
+            dRn = dRp = np.zeros(NP + 2, complex)
+        Ju = rates((dUn, dUp), (dRn, dRp))
+        out.append(J0 + lap * (J1 - J0) + Ju)
+    return np.array(out)
+
+
 def solve_impedance(devices, frequencies, voltage=0.0, tol=1e-10, max_iter=60,
                     bernoulli_name="exact"):
-    """`solve_impedance` (impedance.py:365-409) for devices without mobile ions: `(Y, Z, J,
-    converged)`, Y and Z devices × frequencies."""
+    """`solve_impedance` (impedance.py:365-409): `(Y, Z, J, converged)`, Y and Z devices ×
+    frequencies. Devices with free mobile ions take them as unknowns of their own
+    (`admittance_ions`); ions frozen at a pre-bias are refused, as the reference refuses them."""
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
     laps = 1j * 2 * np.pi * frequencies
     bern = dd.BERNOULLI[bernoulli_name]
     Y, J, ok = [], [], []
     for dev in devices:
         d = dd.prepare([dev])
-        if np.any(d["ion"]["a_totals"] > 0) or np.any(d["ion"]["c_totals"] > 0):
-            raise NotImplementedError("impedance with mobile ions")
+        ions = np.any(d["ion"]["a_totals"] > 0) or np.any(d["ion"]["c_totals"] > 0)
+        if ions and dev.pre_cond and dev.fix_ions:
+            raise NotImplementedError("impedance with ions frozen at a pre-bias")
         st = dd.solve_states(d, [float(voltage)], tol=tol, max_iter=max_iter,
                              bernoulli_name=bernoulli_name)
         full0 = np.stack([st["V"][0, 0], np.log(st["n"][0, 0]), np.log(st["p"][0, 0])], -1)
-        Y.append(admittance(d, full0, float(voltage), laps, bern))
+        if ions:
+            a_m = np.asarray(dev.anion_mask, bool)
+            c_m = np.asarray(dev.cation_mask, bool)
+            la = np.where(a_m, np.log(np.where(a_m, st["anion"][0, 0], 1.0)), 0.0)
+            lc = np.where(c_m, np.log(np.where(c_m, st["cation"][0, 0], 1.0)), 0.0)
+            full5 = np.concatenate([full0, la[:, None], lc[:, None]], -1)
+            full5[0, 3:] = 0.0
+            full5[-1, 3:] = 0.0
+            Y.append(admittance_ions(d, full5, float(voltage), laps, bern))
+        else:
+            Y.append(admittance(d, full0, float(voltage), laps, bern))
         J.append(st["J"][0, 0])
         ok.append(st["converged"][0, 0])
     Y = np.array(Y)

@@ -157,12 +157,15 @@ def _iface_terms(n, p, ti, f_old, dti):
 
 # ----------------------------------------------------------------------------- the system
 
-def assemble(full, d, tr, logs, bern):
+def assemble(full, d, tr, logs, bern, steady_traps=False, mass=False):
     """solver._assemble_ions (solver.py:1364-1475) with `_assemble`'s carriers' rows over a
     step (solver.py:1021-1187, `tr`; `_bulk_rates` and the interface traps over the step):
     residual F (B×NP×5), blocks A, B, C (B×NP×5×5) and slot columns U (B×NP×5×K) from `full`
     (B×(NP+2)×5). `tr`: `dti` (B), the densities before the step on the interior points
-    (`n`, `p`, `a`, `c`, B×NP) and the traps' occupations (`fb` B×NP, `fi` B×(NP+1))."""
+    (`n`, `p`, `a`, `c`, B×NP) and the traps' occupations (`fb` B×NP, `fi` B×(NP+1)).
+    `steady_traps`: the traps at their steady occupation (`_time_terms` without occupations,
+    as the impedance takes it, impedance.py:251). `mass`: also each row's time term on its own
+    unknown per unit of `dti` (B×NP×5; `_assemble_ions(..., mass=True)`)."""
     s, ti, ion = d["s"], d["ti"], d["ion"]
     Vt = _col(d["Vt"])
     dti = _col(tr["dti"])
@@ -191,7 +194,11 @@ def assemble(full, d, tr, logs, bern):
     Vm, nm, pm = V[:, 1:-1], n[:, 1:-1], p[:, 1:-1]
     hm, hp, fac = s["hm"][..., None], s["hp"][..., None], s["fac"]
     zm = np.zeros_like(Vm)
-    Rn, Rp, dRn_n, dRn_p, dRp_n, dRp_p = bulk_rates(nm, pm, s, tr["fb"], dti)
+    if steady_traps:
+        Rn, dRn_n, dRn_p = dd._recombination(nm, pm, s)
+        Rp, dRp_n, dRp_p = Rn, dRn_n, dRn_p
+    else:
+        Rn, Rp, dRn_n, dRn_p, dRp_n, dRp_p = bulk_rates(nm, pm, s, tr["fb"], dti)
     gen = s["G"] * _col(d["g_frac"])
     dnet_n = np.stack([zm, -dRn_n, -dRn_p], -1)
     dnet_p = np.stack([zm, -dRp_n, -dRp_p], -1)
@@ -221,7 +228,10 @@ def assemble(full, d, tr, logs, bern):
     C[..., 1, :3] = hm * dFn1[:, 1:] * sC[..., None]
     C[..., 2, :3] = -hm * dFp1[:, 1:] * sC[..., None]
     if np.any(ti["Nt"] > 0):
-        X, own, up, down = _iface_terms(n, p, ti, tr["fi"], dti)
+        if steady_traps:
+            X, own, up, down = dd._iface_terms(n, p, ti)
+        else:
+            X, own, up, down = _iface_terms(n, p, ti, tr["fi"], dti)
         scale = np.stack([Q * sP, -fac * sC, -fac * sC], 0)  # 3×B×NP
         poisson = poisson + Q * X[0]
         elec = elec - fac * X[1]
@@ -245,6 +255,9 @@ def assemble(full, d, tr, logs, bern):
     ma = ion["a_slots"].sum(1)
     mc = ion["c_slots"].sum(1)
     dti_b = tr["dti"] > 0
+    Mass = np.zeros((nb, NP, 5))
+    Mass[..., 1] = -fac * nm * sC
+    Mass[..., 2] = -fac * pm * sC
     for sn, col, mfull, mu, before, ls, slots, k0 in (
             (-1.0, 3, ma, d["mu_a"], tr["a"], la_pt, ion["a_slots"], 0),
             (1.0, 4, mc, d["mu_c"], tr["c"], lc_pt, ion["c_slots"], ka)):
@@ -301,6 +314,9 @@ def assemble(full, d, tr, logs, bern):
         dls = np.where(mv, fac * dti * els * before * scl, np.where(st, -1.0, 0.0))
         kk = slots.shape[1]
         U[..., col, k0:k0 + kk] = dls[..., None] * np.swapaxes(slots[:, :, 1:-1], 1, 2)
+        Mass[..., col] = np.where(mv, -fac * nc * scl, 0.0)
+    if mass:
+        return F, A, Bb, C, U, Mass
     return F, A, Bb, C, U
 
 
@@ -376,22 +392,33 @@ def width_of(d, zimt):
     return np.concatenate([hh[:, :1], 0.5 * (hh[:, :-1] + hh[:, 1:])], 1)
 
 
-def current(d, full, tr, bern, zimt):
+def current(d, full, tr, bern, zimt, steady_traps=False, dU=None, dRi=None):
     """batch._current over a step (batch.py:302-403, 421-483): SIMsalabim's integral form with
     each density's change in the integrand (summed over `width_of`), the ions' currents region
     by region and the displacement current, averaged over the intervals. `tr` as `assemble`'s
-    but on the full grid: `dti` (B), `n`, `p`, `a`, `c`, `V` (B×(NP+2)), `fb` (B×NP), `fi`."""
+    but on the full grid: `dti` (B), `n`, `p`, `a`, `c`, `V` (B×(NP+2)), `fb` (B×NP), `fi`.
+    `steady_traps`: the traps at their steady occupation; `dU`, `dRi`: each carrier's rates
+    beyond it, bulk and interface, on every point (`tr["dU"]`, `tr["dRi"]`, impedance.py:313).
+    Written for complex inputs too (complex-step derivatives), in the integral form."""
     g_frac = _col(d["g_frac"])
     V, n, p = full[..., 0], np.exp(full[..., 1]), np.exp(full[..., 2])
     Vt, x, h, L = _col(d["Vt"]), d["x"], d["h"], _col(d["L"])
     nb, npts = V.shape
     NP = npts - 2
     dti = _col(tr["dti"])
-    pad = np.zeros((nb, 1))
-    fb = np.concatenate([pad, tr["fb"], pad], 1)
-    Rn, Rp = bulk_rates(n, p, d["rec"], fb, dti)[:2]
+    if steady_traps:
+        Rn = dd._recombination(n, p, d["rec"])[0]
+        Rp = Rn
+    else:
+        pad = np.zeros((nb, 1))
+        fb = np.concatenate([pad, tr["fb"], pad], 1)
+        Rn, Rp = bulk_rates(n, p, d["rec"], fb, dti)[:2]
     if np.any(d["ti"]["Nt"] > 0):
-        val, _ = iface_edges(n[:, :-1], n[:, 1:], p[:, :-1], p[:, 1:], d["ti"], tr["fi"], dti)
+        if steady_traps:
+            val, _ = dd._iface_edges(n[:, :-1], n[:, 1:], p[:, :-1], p[:, 1:], d["ti"])
+        else:
+            val, _ = iface_edges(n[:, :-1], n[:, 1:], p[:, :-1], p[:, 1:], d["ti"], tr["fi"],
+                                 dti)
 
         def points(lo, hi):
             return np.concatenate([lo[:, :1], hi[:, :-1] + lo[:, 1:], hi[:, -1:]], 1)
@@ -399,6 +426,10 @@ def current(d, full, tr, bern, zimt):
         Rin, Rip = points(val[0], val[1]), points(val[2], val[3])
     else:
         Rin = Rip = np.zeros_like(Rn)
+    if dU is not None:
+        Rn, Rp = Rn + dU[0], Rp + dU[1]
+    if dRi is not None:
+        Rin, Rip = Rin + dRi[0], Rip + dRi[1]
     dx = np.diff(x[:, :NP + 1], axis=1)
     width = width_of(d, zimt)
     G = d["G"]
@@ -478,7 +509,7 @@ def ion_currents(d, full, tr, bern, width):
                                         + ev[:, 1:] * int_u[:, 1:] / mu_[:, 1:]) * pair, 1)
             first = np.argmax(mask > 0, 1)
             last = npts - 1 - np.argmax(mask[:, ::-1] > 0, 1)
-            single = np.where(single > 0, single, 1.0)
+            single = np.where(np.real(single) > 0, single, 1.0)
             rows = np.arange(nb)
             ends = sn * (dens[rows, last] * ev[rows, last] - dens[rows, first] * ev[rows, first])
             Kk = (Vt[:, 0] * ends - sn * double) / single

@@ -1,7 +1,9 @@
-"""`solve_impedance` on the GPU (`dd_admittance`) against the oracle's restatement of jaxdd's
-`_admittance` (with bulk and interface traps following at their own rates), and the reference's
-known answers on the GPU's own results: the steady slope at a very low frequency (against the
-GPU's `solve_states` differenced), the geometric capacitance far above every relaxation."""
+"""`solve_impedance` on the GPU (`dd_admittance`, and `dd_admittance_ions` with mobile ions)
+against the oracle's restatement of jaxdd's `_admittance` (with bulk and interface traps following
+at their own rates, the ions as unknowns of their own), and the reference's known answers on the
+GPU's own results: the steady slope at a very low frequency (against the GPU's `solve_states`
+differenced, the ions moving with the voltage), the geometric capacitance far above every
+relaxation."""
 
 import numpy as np
 import pytest
@@ -61,7 +63,36 @@ def test_the_limits_on_the_gpu():
         assert r.capacitance[k, 1] == pytest.approx(geometric, rel=1e-4)
 
 
-def test_mobile_ions_are_refused():
+def test_with_mobile_ions_matches_the_oracle():
+    """`dd_admittance_ions`: config 5's drawn stacks with free mobile ions (5×5 blocks, each
+    region's number kept), and in the same batch the p-i-n cell without ions (its ions' rows
+    identities), against the oracle (`admittance_ions`, and `admittance` for the cell)."""
+    from jaxdd_b200.workloads import transient_devices
+    devs = transient_devices(3, NP=100) + [build_device(setup_from_texts(pin_texts(100)))]
+    r = solve_impedance(prepare(devs), F, voltage=0.8)
+    Yo, Zo, Jo, oko = imp.solve_impedance(devs, F, voltage=0.8)
+    assert np.array_equal(r.converged, oko) and r.converged.all()
+    rel = np.abs(r.Y - Yo) / np.abs(Yo)
+    assert np.max(rel) < 1e-6, rel
+
+
+def test_with_mobile_ions_the_low_frequency_limit_is_the_steady_slope():
+    from jaxdd_b200.workloads import transient_devices
+    devs = transient_devices(2, NP=100)
+    V0, dV = 0.8, 1e-5
+    r = solve_impedance(prepare(devs), [1e-7], voltage=V0, tol=1e-12, max_iter=200)
+    st = solve_states(prepare(devs), [V0 - dV, V0 + dV], tol=1e-12, max_iter=200)
+    slope = (st["J"][:, 1] - st["J"][:, 0]) / (2 * dV)
+    np.testing.assert_allclose(r.Y[:, 0].real, slope, rtol=1e-5)
+    assert np.all(np.abs(r.Y[:, 0].imag) < 1e-4 * np.abs(slope))
+
+
+def test_what_impedance_refuses():
     from jaxdd_b200.workloads import drawn_devices
-    with pytest.raises(NotImplementedError, match="mobile ions"):
+    with pytest.raises(NotImplementedError, match="frozen"):
         solve_impedance(prepare(drawn_devices(2, NP=50)), [1e3])
+    t = pin_texts(50)
+    t["simulation_setup.txt"] = t["simulation_setup.txt"].replace("currDiffInt = 2",
+                                                                  "currDiffInt = 1")
+    with pytest.raises(NotImplementedError, match="differential"):
+        solve_impedance(prepare([build_device(setup_from_texts(t))]), [1e3])

@@ -2,14 +2,17 @@
 (jaxdd tests/test_impedance.py): at a very low frequency the admittance is the steady J-V
 curve's slope, far above every relaxation the capacitance is the layers' geometric one,
 1/∫dx/ε; `Z = 1/(Y + G_shunt) + R_series`. On workload 1's p-i-n cell, with and without
-interface traps."""
+interface traps; with mobile ions as unknowns of their own (config 5's drawn stacks): at 1e-7 Hz
+the steady slope with the ions moving (the reference's bar, 1e-5), far above every relaxation the
+capacitance of the same stack without ions (the ions frozen there), ions frozen at a pre-bias
+refused as the reference refuses them."""
 
 import numpy as np
 import pytest
 
 from jaxdd_b200.device import build_device
 from jaxdd_b200.simss_input import setup_from_texts
-from jaxdd_b200.workloads import pin_texts
+from jaxdd_b200.workloads import SEED_CONFIG5, drawn_texts, pin_texts, transient_devices
 from oracle import dd
 from oracle import impedance as imp
 
@@ -53,3 +56,49 @@ def test_the_series_resistance_and_the_shunt():
     dev = build_device(setup_from_texts(texts))
     Y, Z, _, _ = imp.solve_impedance([dev], [1e3, 1e6], voltage=0.3)
     np.testing.assert_allclose(Z, 1.0 / (Y + 10.0) + 1e-4, rtol=1e-12)
+
+
+def _without_ions(texts):
+    lines = []
+    for line in texts["L2.txt"].splitlines():
+        key = line.split("=")[0].strip()
+        if key in ("N_anion", "N_cation", "mu_anion", "mu_cation", "ionsMayEnter"):
+            line = f"{key} = 0"
+        lines.append(line)
+    return dict(texts, **{"L2.txt": "\n".join(lines) + "\n"})
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_with_ions_low_frequency_is_the_steady_slope(k):
+    dev = transient_devices(1, NP=150, start=k)[0]
+    assert dev.anion_total > 0 and not dev.pre_cond
+    V0, dV = 0.8, 1e-5
+    Y, _, _, ok = imp.solve_impedance([dev], [1e-7], voltage=V0, tol=1e-12, max_iter=200)
+    st = dd.solve_states(dd.prepare([dev]), [V0 - dV, V0 + dV], tol=1e-12, max_iter=200)
+    slope = (st["J"][0, 1] - st["J"][0, 0]) / (2 * dV)
+    assert ok.all()
+    assert Y[0, 0].real == pytest.approx(slope, rel=1e-5)
+    assert abs(Y[0, 0].imag) < 1e-4 * abs(slope)
+
+
+def test_with_ions_high_frequency_is_the_stack_without_them():
+    k = 3
+    texts = drawn_texts(k, np.random.default_rng([SEED_CONFIG5, k]), 150)
+    f = np.array([1e6, 1e16])
+    C = []
+    for t in (texts, _without_ions(texts)):
+        Y, _, _, _ = imp.solve_impedance([build_device(setup_from_texts(t))], f, voltage=0.8)
+        C.append(Y.imag / (2 * np.pi * f))
+    assert C[0][0, 1] == pytest.approx(C[1][0, 1], rel=1e-9)
+    # the ions change the steady state (its band bending), so at 1 MHz the two differ
+    assert C[0][0, 0] != pytest.approx(C[1][0, 0], rel=1e-3)
+
+
+def test_with_ions_frozen_at_a_pre_bias_refused():
+    k = 0  # an even device of the drawn workload: pre-biased, its ions frozen
+    dev = build_device(setup_from_texts(drawn_texts(k, np.random.default_rng([SEED_CONFIG5, k]),
+                                                    60)))
+    assert dev.pre_cond and dev.fix_ions
+    with pytest.raises(NotImplementedError, match="frozen"):
+        imp.solve_impedance([dev], [1e3], voltage=0.5)
+
