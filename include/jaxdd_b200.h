@@ -271,6 +271,11 @@ typedef struct dd_transient_out {
   double* logs;
   double* f_bulk;
   double* f_iface;
+  /* Q [lane_stride]: the integrated current sum_k J_k dt_k over the kept steps (C/m^2); dQ
+   * [2][lane_stride]: its derivatives in ln N_ion (both species' totals) and ln mu_ion (both
+   * species' mobilities), forward mode through every step. Both NULL: not computed. */
+  double* Q;
+  double* dQ;
 } dd_transient_out;
 
 /* Scratch bytes dd_transient needs for this batch. */

@@ -85,7 +85,7 @@ class DdSteps(ctypes.Structure):
 class DdTransientOut(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in (
         "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs", "f_bulk",
-        "f_iface")]
+        "f_iface", "Q", "dQ")]
 
 
 class DdOpts(ctypes.Structure):

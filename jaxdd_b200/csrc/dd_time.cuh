@@ -69,6 +69,7 @@ __device__ __forceinline__ void load_point(const View& W, int buf, int k, double
 struct TrapStep {
   double mean, end, vac;
   double mn, en, vn, mp, ep, vp;
+  double mf, Ef;  // d mean / d f_old (= -d vac / d f_old) and d end / d f_old
 };
 
 __device__ __forceinline__ void trap_step(double Cn, double Cp, double nt0, double pt0, double n,
@@ -99,6 +100,8 @@ __device__ __forceinline__ void trap_step(double Cn, double Cp, double nt0, doub
   o.mp = ds_p * (1.0 - m) + gap * dm * dx_p;
   o.ep = ds_p * (1.0 - E) - gap * E * dx_p;
   o.vp = dv_p * (1.0 - m) + vgap * dm * dx_p;
+  o.mf = m;
+  o.Ef = E;
 }
 
 // Each carrier's recombination over the step at point k (`_bulk_rates` with the traps'
@@ -211,7 +214,8 @@ __device__ __forceinline__ void row5(const View& W, int i, const TP& pm, const T
                                      double fim, double fii, double bn, double bpd, double ba,
                                      double bc, const double* logs, double (&A)[5][5],
                                      double (&B)[5][5], double (&Cm)[5][5], double (&r)[5],
-                                     double (&U)[5][K], double* mass = nullptr) {
+                                     double (&U)[5][K], double* mass = nullptr,
+                                     double* tang = nullptr) {
   const Lane& L = W.L;
   const double iVt = L.iVt;
   const double facl = L.st(i, S_FACL), facm = L.st(i, S_FACM), facu = L.st(i, S_FACU);
@@ -302,6 +306,7 @@ __device__ __forceinline__ void row5(const View& W, int i, const TP& pm, const T
     const double sn = sp == 0 ? -1.0 : 1.0;
     const int slot = sp == 0 ? pc.c.sl.a : pc.c.sl.c;
     const double lcv = sp == 0 ? pc.la : pc.lc;
+    if (tang) { tang[sp] = 0.0; tang[2 + sp] = 0.0; }
     if (slot < 0) {  // held at its value (0)
       r[col] = -lcv;
       B[col][col] = 1.0;
@@ -353,6 +358,13 @@ __device__ __forceinline__ void row5(const View& W, int i, const TP& pm, const T
     B[col][col] = (dlc - fac * dti * nc) * scl;
     U[col][k] = fac * dti * els * before * scl;
     if (mass) mass[col] = -fac * nc * scl;
+    if (tang) {
+      // the row's derivative in the log of the species' mobility (the flux scales with it, and
+      // so does the row's scale) and in the log of its density before the step
+      const double den = fac * dti + hm * cr + hp * cl;
+      tang[sp] = flux * scl - value * (hm * cr + hp * cl) / den;
+      tang[2 + sp] = fac * dti * els * before * scl - value;
+    }
   }
 }
 

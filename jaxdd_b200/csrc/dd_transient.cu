@@ -66,6 +66,12 @@ struct Args {
   double* logs_out;   // [DD_MAXK][Bp]
   double* fb_out;     // [np+2][Bp] or nullptr
   double* fi_out;     // [np+2][Bp] or nullptr
+  // the integrated current and its tangents in ln N_ion and ln mu_ion (nullptr: none)
+  double* Qout;       // [Bp]
+  double* dQout;      // [2][Bp]
+  double* TY;         // [2][2][np+2][5][Bp]: each tangent of the state, two rotating buffers
+  double* TFB;        // [2][np+2][Bp]: of the bulk traps' occupations
+  double* TFI;        // [2][np+2][Bp]: of the interface traps'
 };
 
 // ------------------------------------------------------------------------------------ current
@@ -76,11 +82,54 @@ struct Args {
 // right: each carrier's integral form by prefix sums (sum_e h_e J_e = q K H + sum_e h_e P_e,
 // P_e the prefix of q L w_k U_k; an interface's J the one before it plus its traps'), each ion
 // region's the same over its own intervals, and the displacement current.
-template <int K>
+// The state along a tangent: `buf`'s point plus h times the tangent `tan` (same layout), the
+// contacts as they are.
+__device__ __forceinline__ void load_pert(const View& W, int buf, const double* tan, double h,
+                                          int k, double Vint, TP& P) {
+  load_point(W, buf, k, Vint, P);
+  if (!tan || k == 0 || k == W.L.NP + 1) return;
+  const size_t o = (size_t)k * 5 * W.L.Bp + W.L.l;
+  P.c.V += h * tan[o];
+  P.c.lnn += h * tan[o + W.L.Bp];
+  P.c.lnp += h * tan[o + 2 * W.L.Bp];
+  P.la += h * tan[o + 3 * W.L.Bp];
+  P.lc += h * tan[o + 4 * W.L.Bp];
+  P.c.n = exp(P.c.lnn);
+  P.c.p = exp(P.c.lnp);
+  P.a = exp(P.la);
+  P.c2 = exp(P.lc);
+  P.c.da = P.c.sl.a >= 0 ? P.a : 0.0;
+  P.c.dc = P.c.sl.c >= 0 ? P.c2 : 0.0;
+}
+
+// A perturbation of the current's inputs (PERT): the iterate and the state before the step along
+// their tangents, the traps' occupations along theirs, the ions' mobilities scaled by `mus`.
+struct Pert {
+  const double* tcur;
+  const double* tbef;
+  const double* tfb;
+  const double* tfi;
+  double h, mus;
+};
+
+template <int K, bool PERT = false>
 __device__ double current_t(const View& W, int cur, double Vint, int bef, double Vbef, double dti,
-                            const double* FB, const double* FI) {
+                            const double* FB, const double* FI, const Pert* pt = nullptr) {
   const Lane& L = W.L;
-  const int NP = L.NP, Bp = L.Bp, l = L.l;
+  const double mus = PERT ? pt->mus : 1.0;
+  auto fb_at = [&](int k) {
+    const size_t o = (size_t)k * L.Bp + L.l;
+    return PERT && pt->tfb ? FB[o] + pt->h * pt->tfb[o] : FB[o];
+  };
+  auto fi_at = [&](int k) {
+    const size_t o = (size_t)k * L.Bp + L.l;
+    return PERT && pt->tfi ? FI[o] + pt->h * pt->tfi[o] : FI[o];
+  };
+  auto load_c = [&](int buf, int k, double Vi, TP& P, bool is_cur) {
+    if (PERT) load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P);
+    else load_point(W, buf, k, Vi, P);
+  };
+  const int NP = L.NP;
   const double QL = Q * L.L;
   double single[2] = {0, 0}, dbl[2] = {0, 0}, iu[2] = {0, 0}, P[2] = {0, 0}, bH[2] = {0, 0};
   double corr[2] = {0, 0}, dtot = 0.0, disp = 0.0;
@@ -96,20 +145,19 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     have[k] = false;
   }
   TP pa, pb, qa, qb;  // pa, pb: the iterate at points e, e+1; qa, qb the state before
-  load_point(W, cur, 0, Vint, pa);
-  load_point(W, bef, 0, Vbef, qa);
+  load_c(cur, 0, Vint, pa, true);
+  load_c(bef, 0, Vbef, qa, false);
   double Ri_next[2] = {0, 0};  // interface capture at point e from the interval before it
   for (int e = 0; e <= NP; ++e) {
     const int kb = e + 1;
-    load_point(W, cur, kb, Vint, pb);
-    load_point(W, bef, kb, Vbef, qb);
+    load_c(cur, kb, Vint, pb, true);
+    load_c(bef, kb, Vbef, qb, false);
     const double h = L.st(e, S_H), dx = L.st(e, S_DX);
     const int ifk = (int)L.st(e, S_IFK);
     double tRL[2] = {0, 0}, tRR[2] = {0, 0};
     if (ifk >= 0) {
       Iface t;
-      iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, FI[(size_t)e * Bp + l], dti, t, false,
-                   nullptr);
+      iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, fi_at(e), dti, t, false, nullptr);
       tRL[0] = t.v[0]; tRR[0] = t.v[1]; tRL[1] = t.v[2]; tRR[1] = t.v[3];
     }
     // interface capture at points e and e+1 (point e+1's share of interval e+1 is 0: no two
@@ -119,7 +167,7 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     double Ue[2] = {0, 0};  // point e's U (0 on the contacts)
     if (e >= 1) {
       double Rn, Rp, d0, d1, d2, d3;
-      bulk_rates(L, e, pa.c.n, pa.c.p, FB[(size_t)e * Bp + l], dti, Rn, Rp, d0, d1, d2, d3);
+      bulk_rates(L, e, pa.c.n, pa.c.p, fb_at(e), dti, Rn, Rp, d0, d1, d2, d3);
       const double G = L.st(e, S_G) * L.gfrac;
       Ue[0] = Rn + Ri_a[0] - G + dti * (pa.c.n - qa.c.n);
       Ue[1] = Rp + Ri_a[1] - G + dti * (pa.c.p - qa.c.p);
@@ -182,12 +230,13 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
         // each interval's flux (an interface takes the interval's before it), counted inside
         double Bf, Bb, t1, t2;
         bern_pair(sn * (pb.c.V - pa.c.V) * L.iVt, L.simss, Bf, Bb, t1, t2);
-        const double Jf = sn * Q * W.x(e, an ? T_MUA : T_MUC) * L.Vt * (db * Bb - da * Bf) /
+        const double Jf = sn * Q * mus * W.x(e, an ? T_MUA : T_MUC) * L.Vt * (db * Bb - da * Bf) /
                           (L.L * h);
         if (ina && inb) isum[k] += h * (ifk >= -1 ? Jion_prev[k] : Jf);
         Jion_prev[k] = Jf;
       } else if (ina && inb) {
-        const double mua = W.x(e, an ? T_MUA : T_MUC), mub = W.x(kb, an ? T_MUA : T_MUC);
+        const double mua = mus * W.x(e, an ? T_MUA : T_MUC);
+        const double mub = mus * W.x(kb, an ? T_MUA : T_MUC);
         const double qa2 = eva / (mua > 0.0 ? mua : 1.0);
         const double qb2 = evb / (mub > 0.0 ? mub : 1.0);
         const double Ua = dti * (da - qa_), Ub = dti * (db - qb_);
@@ -241,6 +290,266 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
   return -L.left * tot / H;
 }
 
+// ------------------------------------------------------------------------------------ tangents
+//
+// The integrated current's derivatives in ln N_ion (both species' totals) and ln mu_ion (both
+// species' mobilities), forward mode as jaxdd differentiates its transients (`jax.jvp` through
+// each step's `_converged_jvp`, batch.py:661-737, carried from step to step by the state): at
+// each kept step the tangent of the converged state solves the step's own bordered system at
+// that state, its right-hand side the rows' derivatives along the previous state's and the traps'
+// previous occupations' tangents and in the parameter itself (the ions' fluxes in ln mu, each
+// region's number against its total in ln N); the traps' occupations carry tangents of their
+// own; the current's tangent is the central difference of the current along the full tangent
+// (the current is an explicit function of its inputs; the step's solve is differentiated
+// exactly).
+
+constexpr double TANGENT_H = 1e-6;  // the current's central-difference step along a tangent
+
+template <int K>
+__device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk, double V_k,
+                                          double V_now, double dti, double dt, const double* lg,
+                                          int tb, double* dQ) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = a.Bp, l = L.l;
+  constexpr int NC = 2 + K;  // the two tangents' right-hand sides, then the K slot columns
+  const size_t nodes = (size_t)a.npmax + 2;
+  auto cd = [&](int k, int f) -> double* { return a.CD + ((size_t)k * a.ncd + f) * Bp + l; };
+  auto ty = [&](int p, int b, int k, int c) -> double* {
+    return a.TY + ((((size_t)(p * 2 + b) * nodes + k) * 5 + c) * Bp + l);
+  };
+  auto tfb = [&](int p, int k) { return a.TFB[((size_t)p * nodes + k) * Bp + l]; };
+  auto tfi = [&](int p, int k) { return a.TFI[((size_t)p * nodes + k) * Bp + l]; };
+  const double* FB = a.FB;
+  const double* FI = a.FI;
+  double cpv[5][5], dpv[5][NC];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) cpv[r][c] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) dpv[r][c] = 0.0;
+  }
+  double gnum[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) gnum[q] = 0.0;
+  TP pm, pc, pn;
+  load_point(W, bn, 0, V_k, pm);
+  load_point(W, bn, 1, V_k, pc);
+  Flux el, er;
+  flux(L, pm.c, pc.c, L.st(0, S_MUN), L.st(0, S_MUP), el);
+  for (int i = 1; i <= NP; ++i) {
+    load_point(W, bn, i + 1, V_k, pn);
+    flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
+    const double hm = L.st(i - 1, S_H), hp = L.st(i, S_H);
+    const int ifm = (int)L.st(i - 1, S_IFK), ifi = (int)L.st(i, S_IFK);
+    const double fb = FB[(size_t)i * Bp + l];
+    const double fim = ifm >= 0 ? FI[(size_t)(i - 1) * Bp + l] : 0.0;
+    const double fii = ifi >= 0 ? FI[(size_t)i * Bp + l] : 0.0;
+    const double bnv = exp(*W.y(bk, i, 1)), bpv = exp(*W.y(bk, i, 2));
+    const double bav = pc.c.sl.a >= 0 ? exp(*W.y(bk, i, 3)) : 0.0;
+    const double bcv = pc.c.sl.c >= 0 ? exp(*W.y(bk, i, 4)) : 0.0;
+    double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][K], tang[4];
+    row5<K>(W, i, pm, pc, pn, el, er, hm, hp, ifm, ifi, dti, fb, fim, fii, bnv, bpv, bav, bcv,
+            lg, A, Bm, Cm, r, U, nullptr, tang);
+    {
+      const double hL = hm * L.L;
+      if (pc.c.sl.a >= 0 && pc.c.sl.a == pm.c.sl.a) gnum[pc.c.sl.a] += 0.5 * (pm.a + pc.a) * hL;
+      if (pc.c.sl.c >= 0 && pc.c.sl.c == pm.c.sl.c)
+        gnum[L.ka + pc.c.sl.c] += 0.5 * (pm.c2 + pc.c2) * hL;
+    }
+    // the rows' derivatives along each parameter's tangent
+    const double fac = L.st(i, S_FAC), sC = L.st(i, S_SC), sP = L.st(i, S_SP);
+    double tr_[2][5];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      double d[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      if (dti > 0.0) {
+        // the time terms in the state before the step
+        d[1] += sC * fac * dti * bnv * *ty(p, tb, i, 1);
+        d[2] += sC * fac * dti * bpv * *ty(p, tb, i, 2);
+        d[3] += tang[2] * *ty(p, tb, i, 3);
+        d[4] += tang[3] * *ty(p, tb, i, 4);
+        // the bulk traps through their occupation before the step
+        const double Nt = L.st(i, S_NT);
+        if (Nt > 0.0) {
+          const double Cn = L.st(i, S_CNT), Cp = L.st(i, S_CPT);
+          const double nt0 = L.st(i, S_NT0), pt0 = L.st(i, S_PT0);
+          TrapStep o;
+          trap_step(Cn, Cp, nt0, pt0, pc.c.n, pc.c.p, fb, dti, o);
+          const double dRn = -Nt * Cn * o.mf * (pc.c.n + nt0), dRp = Nt * Cp * o.mf * (pc.c.p + pt0);
+          d[1] += -sC * fac * dRn * tfb(p, i);
+          d[2] += -sC * fac * dRp * tfb(p, i);
+        }
+        // the interface traps of its two intervals through theirs
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+          const int e = side == 0 ? i - 1 : i;
+          const int t = side == 0 ? ifm : ifi;
+          if (t < 0) continue;
+          const double Nt_i = L.itab(t, I_NT);
+          if (!(Nt_i > 0.0)) continue;
+          const TP& qa = side == 0 ? pm : pc;
+          const TP& qb = side == 0 ? pc : pn;
+          const double Cn = L.itab(t, I_CN), Cp = L.itab(t, I_CP);
+          const double nlo = L.itab(t, I_NT0LO), nhi = L.itab(t, I_NT0HI);
+          const double plo = L.itab(t, I_PT0LO), phi = L.itab(t, I_PT0HI);
+          const double iw = L.itab(t, I_IW);
+          const double hq = L.itab(t, I_CHARGE) * 0.5 * Nt_i * iw;
+          TrapStep o;
+          trap_step(Cn, Cp, nlo + nhi, plo + phi, qa.c.n + qb.c.n, qa.c.p + qb.c.p,
+                    side == 0 ? fim : fii, dti, o);
+          // this point is the interval's right end (side 0) or its left end (side 1)
+          const double nme = side == 0 ? pc.c.n + nhi : pc.c.n + nlo;
+          const double pme = side == 0 ? pc.c.p + phi : pc.c.p + plo;
+          const double dRn = -iw * Cn * Nt_i * o.mf * nme, dRp = iw * Cp * Nt_i * o.mf * pme;
+          const double dQt = -hq * o.Ef;
+          const double df = tfi(p, e);
+          d[0] += Q * sP * dQt * df;
+          d[1] += -fac * sC * dRn * df;
+          d[2] += -fac * sC * dRp * df;
+        }
+      }
+      if (p == 1) { d[3] += tang[0]; d[4] += tang[1]; }  // the ions' fluxes in ln mu
+#pragma unroll
+      for (int c = 0; c < 5; ++c) tr_[p][c] = -d[c];
+    }
+    double M[5][5];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        double sm = Bm[rr][c];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) sm -= A[rr][q] * cpv[q][c];
+        M[rr][c] = sm;
+      }
+    double rhs[5][NC];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        double sm = c < 2 ? tr_[c][rr] : U[rr][c - 2];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) sm -= A[rr][q] * dpv[q][c];
+        rhs[rr][c] = sm;
+      }
+    Part f;
+    partition(M, f);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double v[5] = {Cm[0][c], Cm[1][c], Cm[2][c], Cm[3][c], Cm[4][c]};
+      apply(f, v);
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) { cpv[rr][c] = v[rr]; *cd(i, rr * 5 + c) = v[rr]; }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      double v[5] = {rhs[0][c], rhs[1][c], rhs[2][c], rhs[3][c], rhs[4][c]};
+      apply(f, v);
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) { dpv[rr][c] = v[rr]; *cd(i, 25 + rr * NC + c) = v[rr]; }
+    }
+    pm = pc;
+    pc = pn;
+    el = er;
+  }
+  // back substitution, the slots' Schur complement for both tangents
+  double SM[K][K], sr[2][K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const bool has = L.tot[q] > 0.0;
+#pragma unroll
+    for (int q2 = 0; q2 < K; ++q2) SM[q][q2] = (q == q2 && !has) ? 1.0 : 0.0;
+    sr[0][q] = has ? gnum[q] / L.tot[q] : 0.0;  // -d g / d ln N: the number over the total
+    sr[1][q] = 0.0;
+  }
+  {
+    double xn[5][NC];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) xn[rr][c] = 0.0;
+    Slots s_next = slots_at(L, NP + 1), s_here = slots_at(L, NP);
+    for (int i = NP; i >= 1; --i) {
+      double xi[5][NC];
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          double sm = *cd(i, 25 + rr * NC + c);
+#pragma unroll
+          for (int q = 0; q < 5; ++q) sm -= *cd(i, rr * 5 + q) * xn[q][c];
+          xi[rr][c] = sm;
+        }
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          *cd(i, 25 + rr * NC + c) = xi[rr][c];
+          xn[rr][c] = xi[rr][c];
+        }
+      const Slots s_prev = slots_at(L, i - 1);
+      const double hLm = L.st(i - 1, S_H) * L.L, hLp = L.st(i, S_H) * L.L;
+#pragma unroll
+      for (int sp = 0; sp < 2; ++sp) {
+        const int sl = sp == 0 ? s_here.a : s_here.c;
+        if (sl < 0) continue;
+        const int q = sp == 0 ? sl : L.ka + sl;
+        if (!(L.tot[q] > 0.0)) continue;
+        const int slm = sp == 0 ? s_prev.a : s_prev.c, sln = sp == 0 ? s_next.a : s_next.c;
+        const double wpt = 0.5 * ((slm == sl ? hLm : 0.0) + (sln == sl ? hLp : 0.0));
+        const double w = wpt * exp(*W.y(bn, i, 3 + sp)) / L.tot[q];
+        sr[0][q] -= w * xi[3 + sp][0];
+        sr[1][q] -= w * xi[3 + sp][1];
+#pragma unroll
+        for (int q2 = 0; q2 < K; ++q2) SM[q][q2] -= w * xi[3 + sp][2 + q2];
+      }
+      s_next = s_here;
+      s_here = s_prev;
+    }
+  }
+  double z[2][K];
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    double S2[K][K];
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+#pragma unroll
+      for (int q2 = 0; q2 < K; ++q2) S2[q][q2] = SM[q][q2];
+    small_solve<K>(S2, sr[p], z[p]);
+  }
+  // the state's tangents of this step
+  for (int i = 1; i <= NP; ++i)
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        double v = *cd(i, 25 + rr * NC + p);
+#pragma unroll
+        for (int q = 0; q < K; ++q) v -= *cd(i, 25 + rr * NC + 2 + q) * z[p][q];
+        *ty(p, 1 - tb, i, rr) = v;
+      }
+    }
+  // the current's tangent: a central difference along the full tangent
+  if (dt > 0.0) {
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      Pert pt;
+      pt.tcur = a.TY + (size_t)(p * 2 + (1 - tb)) * nodes * 5 * Bp;
+      pt.tbef = a.TY + (size_t)(p * 2 + tb) * nodes * 5 * Bp;
+      pt.tfb = a.TFB + (size_t)p * nodes * Bp;
+      pt.tfi = a.TFI + (size_t)p * nodes * Bp;
+      pt.h = TANGENT_H;
+      pt.mus = p == 1 ? exp(TANGENT_H) : 1.0;
+      const double Jp = current_t<K, true>(W, bn, V_k, bk, V_now, dti, FB, FI, &pt);
+      pt.h = -TANGENT_H;
+      pt.mus = p == 1 ? exp(-TANGENT_H) : 1.0;
+      const double Jm = current_t<K, true>(W, bn, V_k, bk, V_now, dti, FB, FI, &pt);
+      dQ[p] += (Jp - Jm) / (2.0 * TANGENT_H) * dt;
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------ kernel
 
 template <int K>
@@ -288,6 +597,22 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   }
   for (int e = 0; e <= NP; ++e) FI[(size_t)e * Bp + l] = 0.0;
   const int fm = a.fmode[l];
+  // the integrated current and its tangents (zero tangents before the first step)
+  const bool grad = a.TY != nullptr;
+  const size_t tnodes = (size_t)a.npmax + 2;
+  double Qint = 0.0, dQ[2] = {0.0, 0.0};
+  int tb = 0;
+  if (grad) {
+    for (int p = 0; p < 4; ++p)
+      for (int i = 0; i <= NP + 1; ++i)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) a.TY[(((size_t)p * tnodes + i) * 5 + c) * Bp + l] = 0.0;
+    for (int p = 0; p < 2; ++p)
+      for (int i = 0; i <= NP + 1; ++i) {
+        a.TFB[((size_t)p * tnodes + i) * Bp + l] = 0.0;
+        a.TFI[((size_t)p * tnodes + i) * Bp + l] = 0.0;
+      }
+  }
   double V_now = a.V[ts ? l : 0], dti_now = 0.0, t_last = 0.0;
   int track_curr = 0, stop = 0;
   bool first = true;
@@ -566,7 +891,15 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const bool failed = running && !ok && (fm == 0 || (fm == 2 && track_curr == 1));
     const bool keep = running && !failed && finite && (ok || fm == 1 || (fm == 2 && dti == 0.0));
     if (keep) {
-      // the traps' occupations at the step's end, from its solution
+      // the tangents of this step, before the occupations move on (they take the old ones)
+      const double dt = dti > 0.0 ? t_k - t_last : 0.0;
+      Qint += J * dt;
+      if (grad) tangent_step<K>(a, W, bn, bk, V_k, V_now, dti, dt, lg, tb, dQ);
+      // the traps' occupations at the step's end, from its solution (and their tangents)
+      auto tyn = [&](int p, int k, int c) {
+        return (k < 1 || k > NP) ? 0.0
+                                 : a.TY[((((size_t)(p * 2 + 1 - tb)) * tnodes + k) * 5 + c) * Bp + l];
+      };
       TP pa, pb;
       load_point(W, bn, 0, V_k, pa);
       for (int e = 0; e <= NP; ++e) {
@@ -575,18 +908,43 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         if (ifk >= 0) {
           Iface t;
           double end;
-          iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, FI[(size_t)e * Bp + l], dti, t,
-                       false, &end);
+          const double f_old = FI[(size_t)e * Bp + l];
+          iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, f_old, dti, t, false, &end);
           FI[(size_t)e * Bp + l] = end;
+          if (grad && L.itab(ifk, I_NT) > 0.0) {
+            TrapStep o;
+            trap_step(L.itab(ifk, I_CN), L.itab(ifk, I_CP),
+                      L.itab(ifk, I_NT0LO) + L.itab(ifk, I_NT0HI),
+                      L.itab(ifk, I_PT0LO) + L.itab(ifk, I_PT0HI), pa.c.n + pb.c.n,
+                      pa.c.p + pb.c.p, f_old, dti, o);
+#pragma unroll
+            for (int p = 0; p < 2; ++p) {
+              double& tf = a.TFI[((size_t)p * tnodes + e) * Bp + l];
+              tf = o.Ef * tf + o.en * (pa.c.n * tyn(p, e, 1) + pb.c.n * tyn(p, e + 1, 1)) +
+                   o.ep * (pa.c.p * tyn(p, e, 2) + pb.c.p * tyn(p, e + 1, 2));
+            }
+          }
         }
         if (e + 1 <= NP && L.st(e + 1, S_NT) > 0.0) {
           const size_t o = (size_t)(e + 1) * Bp + l;
+          if (grad) {
+            TrapStep ts_;
+            trap_step(L.st(e + 1, S_CNT), L.st(e + 1, S_CPT), L.st(e + 1, S_NT0),
+                      L.st(e + 1, S_PT0), pb.c.n, pb.c.p, FB[o], dti, ts_);
+#pragma unroll
+            for (int p = 0; p < 2; ++p) {
+              double& tf = a.TFB[((size_t)p * tnodes + e + 1) * Bp + l];
+              tf = ts_.Ef * tf + ts_.en * pb.c.n * tyn(p, e + 1, 1) +
+                   ts_.ep * pb.c.p * tyn(p, e + 1, 2);
+            }
+          }
           FB[o] = bulk_end(L, e + 1, pb.c.n, pb.c.p, FB[o], dti);
         }
         pa = pb;
       }
       const int old_p = bp;
       bp = bk; bk = bn; bn = old_p;
+      tb = 1 - tb;
 #pragma unroll
       for (int q = 0; q < K; ++q) { logs_p[q] = logs[q]; logs[q] = lg[q]; }
       V_now = V_k;
@@ -604,6 +962,11 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     a.acc[o] = keep ? 1 : 0;
   }
   a.stop[l] = stop;
+  if (grad) {
+    a.Qout[l] = Qint;
+    a.dQout[l] = dQ[0];
+    a.dQout[(size_t)Bp + l] = dQ[1];
+  }
   for (int i = 0; i <= NP + 1; ++i) {
     TP p;
     load_point(W, bk, i, V_now, p);
@@ -631,14 +994,17 @@ int slots_k_t(const dd_batch* b) { return b->k_anion + b->k_cation <= 2 ? 2 : 4;
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
-void ws_parts(const dd_batch* b, size_t* y, size_t* fb, size_t* fi, size_t* cd, int* ncd) {
+void ws_parts(const dd_batch* b, size_t* y, size_t* fb, size_t* fi, size_t* cd, int* ncd,
+              size_t* tan) {
   const int K = slots_k_t(b);
   const size_t nodes = (size_t)b->np_max + 2, Bp = (size_t)b->lane_stride;
-  *ncd = 25 + 5 * (1 + K);
+  *ncd = 25 + 5 * (2 + K);  // the Newton step's 1 + K columns, or the tangents' 2 + K
   *y = align_up(3 * nodes * 5 * Bp * sizeof(double));
   *fb = align_up(nodes * Bp * sizeof(double));
   *fi = align_up(nodes * Bp * sizeof(double));
   *cd = align_up(nodes * (size_t)(*ncd) * Bp * sizeof(double));
+  // the tangents: two parameters' states (two buffers each) and traps' occupations
+  *tan = align_up(4 * nodes * 5 * Bp * sizeof(double)) + 2 * align_up(2 * nodes * Bp * sizeof(double));
 }
 
 bool batch_ok(const dd_batch* b) {
@@ -652,10 +1018,10 @@ extern "C" {
 
 int dd_transient_workspace_bytes(const dd_batch* batch, size_t* bytes) {
   if (!batch_ok(batch) || !bytes) return DD_ERR_ARGS;
-  size_t y, fb, fi, cd;
+  size_t y, fb, fi, cd, tan;
   int ncd;
-  ws_parts(batch, &y, &fb, &fi, &cd, &ncd);
-  *bytes = y + fb + fi + cd;
+  ws_parts(batch, &y, &fb, &fi, &cd, &ncd, &tan);
+  *bytes = y + fb + fi + cd + tan;
   return DD_OK;
 }
 
@@ -673,10 +1039,11 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
       !out->stop || !out->state || !out->logs)
     return DD_ERR_ARGS;
   if (opts->max_iter < 1 || !(opts->tol > 0.0)) return DD_ERR_ARGS;
-  size_t y, fb, fi, cd;
+  size_t y, fb, fi, cd, tan;
   int ncd;
-  ws_parts(batch, &y, &fb, &fi, &cd, &ncd);
-  if (workspace_bytes < y + fb + fi + cd) return DD_ERR_WORKSPACE;
+  ws_parts(batch, &y, &fb, &fi, &cd, &ncd, &tan);
+  if (workspace_bytes < y + fb + fi + cd + tan) return DD_ERR_WORKSPACE;
+  if ((out->Q == nullptr) != (out->dQ == nullptr)) return DD_ERR_ARGS;
   char* w = static_cast<char*>(workspace);
   dd::tr::Args a;
   a.S = batch->stat; a.C = batch->scal; a.IFt = batch->iface; a.X = tstat;
@@ -697,6 +1064,17 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.J = out->J; a.Jext = out->J_ext; a.conv = out->converged; a.iters = out->iterations;
   a.acc = out->accepted; a.stop = out->stop; a.state_out = out->state; a.logs_out = out->logs;
   a.fb_out = out->f_bulk; a.fi_out = out->f_iface;
+  a.Qout = out->Q; a.dQout = out->dQ;
+  if (out->Q) {
+    const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
+    char* t = w + y + fb + fi + cd;
+    a.TY = reinterpret_cast<double*>(t);
+    a.TFB = reinterpret_cast<double*>(t + align_up(4 * nodes * 5 * Bp * sizeof(double)));
+    a.TFI = reinterpret_cast<double*>(t + align_up(4 * nodes * 5 * Bp * sizeof(double)) +
+                                      align_up(2 * nodes * Bp * sizeof(double)));
+  } else {
+    a.TY = nullptr; a.TFB = nullptr; a.TFI = nullptr;
+  }
   const dim3 grid((batch->n_lanes + 31) / 32), block(32);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (slots_k_t(batch) == 2) dd::tr::transient_kernel<2><<<grid, block, 0, s>>>(a);

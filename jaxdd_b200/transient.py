@@ -25,7 +25,8 @@ from . import _lib
 from .batch import Batch, _gpu, descriptor, initial_state
 from .simss_input import TVG
 
-__all__ = ["STOP_FAILED", "TransientResult", "TransientState", "Work", "solve_transient"]
+__all__ = ["STOP_FAILED", "ChargeGradients", "TransientResult", "TransientState", "Work",
+           "charge_gradients", "solve_transient"]
 
 #: `TransientResult.stop`: a failed step ended the run (transient.py:240)
 STOP_FAILED = 2
@@ -107,7 +108,8 @@ class Work:
     device (`out`)."""
 
     def __init__(self, batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
-                 bernoulli_name: str = "exact", zimt_current: bool = False):
+                 bernoulli_name: str = "exact", zimt_current: bool = False,
+                 gradients: bool = False):
         import torch
         from .adjoint import plan as _plan
         _check_batch(batch)
@@ -179,6 +181,10 @@ class Work:
             "f_bulk": torch.empty((nodes, Bp), dtype=f64, device=cuda),
             "f_iface": torch.empty((nodes, Bp), dtype=f64, device=cuda),
         }
+        self.gradients = gradients
+        if gradients:
+            self.out["Q"] = torch.empty(Bp, dtype=f64, device=cuda)
+            self.out["dQ"] = torch.empty((2, Bp), dtype=f64, device=cuda)
         size = ctypes.c_size_t(0)
         desc = descriptor(batch, g, self.plan.y0)
         _lib.check(_lib.lib().dd_transient_workspace_bytes(ctypes.byref(desc),
@@ -197,9 +203,9 @@ class Work:
                              self.gv.data_ptr(), self.trk.data_ptr(), self.fm.data_ptr(),
                              self.zimt)
         o = self.out
-        out = _lib.DdTransientOut(*(o[k].data_ptr() for k in (
+        out = _lib.DdTransientOut(*(o[k].data_ptr() if k in o else None for k in (
             "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",
-            "f_bulk", "f_iface")))
+            "f_bulk", "f_iface", "Q", "dQ")))
         opts = _lib.DdOpts(float(self.tol), int(self.max_iter), int(self.max_iter), 0,
                            self.bern, _lib.DD_MODE_BATCH, 0, 0)
         desc = descriptor(self.batch, g, self.plan.y0)
@@ -304,3 +310,32 @@ def result(work: Work, o) -> TransientResult:
         f_interface=stack(fis))
     return TransientResult(J=J, J_ext=J_ext, V_int=V_int, V_ext=V_ext, converged=ok,
                            iterations=its, accepted=acc, stop=stop, t=t, final=final, columns={})
+
+
+@dataclass(frozen=True)
+class ChargeGradients:
+    """Per device: `Q` the integrated current `sum_k J_k (t_k - t_(k-1))` over the kept steps
+    (C/m², J the internal current), and its derivatives in the log of the ion density (both
+    species' totals scaled together) and of the ion mobility (both species'); `result` the
+    transient itself."""
+
+    Q: np.ndarray
+    dQ_dlnN_ion: np.ndarray
+    dQ_dlnmu_ion: np.ndarray
+    result: TransientResult
+
+
+def charge_gradients(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
+                     bernoulli_name: str = "exact", zimt_current: bool = False) -> ChargeGradients:
+    """The integrated transient current and its gradient in the ion density and the ion mobility
+    (BASELINE config 5's gradients), in forward mode through every step as jaxdd differentiates
+    its transients (`jax.jvp` through each step's `_converged_jvp`, batch.py:661-737): one
+    `dd_transient` launch with the tangents carried beside the state."""
+    work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
+                zimt_current=zimt_current, gradients=True)
+    o, _ = work.run()
+    lanes = batch["lane_of"]
+    dQ = o["dQ"].cpu().numpy()[:, lanes]
+    return ChargeGradients(Q=o["Q"].cpu().numpy()[lanes], dQ_dlnN_ion=dQ[0], dQ_dlnmu_ion=dQ[1],
+                           result=result(work, o))
+

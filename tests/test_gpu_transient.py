@@ -2,9 +2,10 @@
 oracle (`oracle.transient`) on the same devices and steps, and against ZimT 5.36's own `Jext`
 (the reference's tests/data) at the reference's tolerances: electrons and holes, the bulk traps
 in time, mobile ions over 2 x 50 ms and 2 x 5 s; config 5's transient (drawn devices with mobile
-ions, a step to 0.9 V, log-spaced steps) on fewer steps; ZimT's failure modes; and at config 5's
+ions, a step to 0.9 V, log-spaced steps) on fewer steps; ZimT's failure modes; at config 5's
 2000 steps the properties that hold at any size (every step converged and kept, each region's
-ions kept to their total, the current finite)."""
+ions kept to their total, the current finite); and the integrated current's forward-mode
+gradient in the ion density and mobility against differences of whole transients."""
 
 import numpy as np
 import pytest
@@ -88,3 +89,77 @@ def test_config5_full_steps_hold_their_invariants():
     assert np.all(np.isfinite(r.J_ext))
     for k, d in enumerate(devs):
         assert abs(_number(r.final.anion[k], d.anion_mask, d) / d.anion_total - 1) < 1e-8
+
+
+def _scaled_device(k, lnN=0.0, lnmu=0.0, NP=120):
+    """Config 5's device `k` with its ion density and mobility scaled by e^lnN and e^lnmu."""
+    from jaxdd_b200.simss_input import setup_from_texts
+    from jaxdd_b200.workloads import SEED_CONFIG5, drawn_texts
+    idx = 2 * k + 1
+    t = drawn_texts(idx, np.random.default_rng([SEED_CONFIG5, idx]), NP)
+    lines = []
+    for line in t["L2.txt"].splitlines():
+        key, _, val = (part.strip() for part in line.partition("="))
+        if key in ("N_anion", "N_cation"):
+            line = f"{key} = {float(val) * float(np.exp(lnN))!r}"
+        elif key in ("mu_anion", "mu_cation"):
+            line = f"{key} = {float(val) * float(np.exp(lnmu))!r}"
+        lines.append(line)
+    t["L2.txt"] = "\n".join(lines) + "\n"
+    return build_device(setup_from_texts(t))
+
+
+def _charge(r, t):
+    """The integrated current of each device: J over each kept step's dt."""
+    out = []
+    for k in range(r.J.shape[0]):
+        prev, q = 0.0, 0.0
+        for s in range(t.shape[1]):
+            if r.accepted[k, s]:
+                if t[k, s] > 0:
+                    q += r.J[k, s] * (t[k, s] - prev)
+                prev = t[k, s]
+        out.append(q)
+    return np.array(out)
+
+
+def test_charge_gradients_match_differences_of_whole_transients():
+    """The forward-mode tangents of `dd_transient` (the integrated current's derivatives in
+    ln N_ion and ln mu_ion) against central differences of whole transients of the rebuilt
+    devices, Richardson-extrapolated (steps 1e-3 and 2e-3): on the GPU's own transient and, for
+    one device, the oracle's."""
+    from jaxdd_b200.transient import charge_gradients
+    ks = (0, 1, 2)
+    tvg = transient_steps(40)
+    base = [_scaled_device(k) for k in ks]
+    g = charge_gradients(prepare(base), tvg)
+    assert g.result.converged.all()
+    np.testing.assert_allclose(g.Q, _charge(g.result, g.result.t), rtol=1e-12)
+
+    def fd(which, solve):
+        def q(h):
+            devs = [_scaled_device(k, **{which: h}) for k in ks]
+            return solve(devs)
+        d1 = (q(1e-3) - q(-1e-3)) / 2e-3
+        d2 = (q(2e-3) - q(-2e-3)) / 4e-3
+        return (4 * d1 - d2) / 3
+
+    def gpu(devs):
+        r = solve_transient(prepare(devs), tvg)
+        return _charge(r, r.t)
+
+    # measured: 1e-9 of each derivative; the differences' own accuracy is near 1e-8
+    for which, mine in (("lnN", g.dQ_dlnN_ion), ("lnmu", g.dQ_dlnmu_ion)):
+        ref = fd(which, gpu)
+        assert np.all(np.abs(mine - ref) < 1e-6 * np.abs(ref) + 1e-9 * np.abs(g.Q)), \
+            (which, mine, ref)
+
+    def oracle(devs):
+        o = transient.solve_transient(dd.prepare(devs[:1]), tvg.t, tvg.Vext, tvg.G_frac)
+        t = np.broadcast_to(tvg.t, o["J"].shape)
+        return _charge(type("R", (), {"J": o["J"], "accepted": o["accepted"]})(), t)
+
+    for which, mine in (("lnN", g.dQ_dlnN_ion), ("lnmu", g.dQ_dlnmu_ion)):
+        ref = fd(which, oracle)
+        assert abs(mine[0] - ref[0]) < 1e-6 * abs(ref[0]) + 1e-9 * abs(g.Q[0]), (which, mine[0],
+                                                                                 ref)
