@@ -584,10 +584,21 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
     v1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = v0.elapsed_time(v1)
-    t = torch.tensor([ms, e2e_ms, kernel_ms], device=dev, dtype=torch.float64)
+    # the gradients: the integrated current and its derivatives in ln N_ion and ln mu_ion, the
+    # tangents carried through every step in the same launch
+    gwork = Work(batch, tvg, gradients=True)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    gout, _ = gwork.run()
+    g1.record(stream)
+    torch.cuda.synchronize()
+    grad_ms = g0.elapsed_time(g1)
+    dQ = gout["dQ"][:, :batch["n"]]
+    grad_finite = bool(torch.isfinite(dQ).all())
+    t = torch.tensor([ms, e2e_ms, kernel_ms, grad_ms], device=dev, dtype=torch.float64)
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms, e2e_ms, kernel_ms = (float(x) for x in t.tolist())
+    ms, e2e_ms, kernel_ms, grad_ms = (float(x) for x in t.tolist())
     m = batch["n"]
     its = o["iterations"][:, :m].to(torch.int64)
     acc = o["accepted"][:, :m]
@@ -621,7 +632,12 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
                        "transient_kernel_ms": kernel_ms,
                        "start_converged_fraction": float(ok0[:m].float().mean()),
                        "converged_fraction": float(o["converged"][:, :m].float().mean()),
-                       "accepted_fraction": float(acc.float().mean())},
+                       "accepted_fraction": float(acc.float().mean()),
+                       "gradients": {"value": m * world / (grad_ms / 1e3),
+                                     "unit": "gradients/s (Q and dQ/dln N_ion, dQ/dln mu_ion "
+                                             "per device, forward mode through 2000 steps)",
+                                     "ms": grad_ms, "over_forward": grad_ms / ms,
+                                     "finite": grad_finite}},
             "e2e": {"value": m * world / (e2e_ms / 1e3), "unit": "transients/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
