@@ -55,8 +55,9 @@ __device__ __forceinline__ void load_point(const View& W, int buf, int k, double
   P.c.offn = L.st(k, S_OFFN);
   P.c.offp = L.st(k, S_OFFP);
   P.c.sl = slots_at(L, k);
-  P.a = exp(P.la);
-  P.c2 = exp(P.lc);
+  // the ions' densities where they are mobile (elsewhere their unknown is held at 0)
+  P.a = P.c.sl.a >= 0 ? exp(P.la) : 1.0;
+  P.c2 = P.c.sl.c >= 0 ? exp(P.lc) : 1.0;
   P.c.da = P.c.sl.a >= 0 ? P.a : 0.0;
   P.c.dc = P.c.sl.c >= 0 ? P.c2 : 0.0;
 }
@@ -77,18 +78,20 @@ __device__ __forceinline__ void trap_step(double Cn, double Cp, double nt0, doub
   double a = Cn * (n + nt0) + Cp * (p + pt0);
   const bool pos = a > 0.0;
   if (!pos) a = 1.0;
+  const double ia = 1.0 / a;
   const double da_n = pos ? Cn : 0.0, da_p = pos ? Cp : 0.0;
-  const double steady = (Cn * n + Cp * pt0) / a, vac_s = (Cn * nt0 + Cp * p) / a;
-  const double ds_n = (Cn - steady * da_n) / a, ds_p = -steady * da_p / a;
-  const double dv_n = -vac_s * da_n / a, dv_p = (Cp - vac_s * da_p) / a;
+  const double steady = (Cn * n + Cp * pt0) * ia, vac_s = (Cn * nt0 + Cp * p) * ia;
+  const double ds_n = (Cn - steady * da_n) * ia, ds_p = -steady * da_p * ia;
+  const double dv_n = -vac_s * da_n * ia, dv_p = (Cp - vac_s * da_p) * ia;
   double E = 0.0, m = 0.0, dm = 0.0, dx_n = 0.0, dx_p = 0.0;
   if (dti > 0.0) {
-    const double x = a / dti;
+    const double idti = 1.0 / dti;
+    const double x = a * idti, ix = dti * ia;
     E = exp(-x);
-    m = -expm1(-x) / x;
-    dm = (E - m) / x;
-    dx_n = da_n / dti;
-    dx_p = da_p / dti;
+    m = -expm1(-x) * ix;
+    dm = (E - m) * ix;
+    dx_n = da_n * idti;
+    dx_p = da_p * idti;
   }
   const double gap = f_old - steady, vgap = (1.0 - f_old) - vac_s;
   o.mean = steady + gap * m;

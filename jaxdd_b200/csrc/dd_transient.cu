@@ -96,8 +96,8 @@ __device__ __forceinline__ void load_pert(const View& W, int buf, const double* 
   P.lc += h * tan[o + 4 * W.L.Bp];
   P.c.n = exp(P.c.lnn);
   P.c.p = exp(P.c.lnp);
-  P.a = exp(P.la);
-  P.c2 = exp(P.lc);
+  P.a = P.c.sl.a >= 0 ? exp(P.la) : 1.0;
+  P.c2 = P.c.sl.c >= 0 ? exp(P.lc) : 1.0;
   P.c.da = P.c.sl.a >= 0 ? P.a : 0.0;
   P.c.dc = P.c.sl.c >= 0 ? P.c2 : 0.0;
 }
@@ -208,7 +208,12 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     Jd_prev[0] = Jd[0]; Jd_prev[1] = Jd[1];
     // the displacement current of interval e
     disp += W.x(e, T_EPS) * ((pb.c.V - pa.c.V) - (qb.c.V - qa.c.V));
-    // the ions, region by region
+    // the ions, region by region: exp(+-V/V_T) at the interval's two points, once
+    double exa = 1.0, exb = 1.0, iexa = 1.0, iexb = 1.0;
+    if (L.tot[0] > 0.0 || L.tot[K - 1] > 0.0 || (K > 2 && (L.tot[1] > 0.0 || L.tot[2] > 0.0))) {
+      exa = exp(pa.c.V * L.iVt); exb = exp(pb.c.V * L.iVt);
+      iexa = 1.0 / exa; iexb = 1.0 / exb;
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (!(L.tot[k] > 0.0)) continue;
@@ -219,7 +224,7 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
       const bool inb = (an ? pb.c.sl.a : pb.c.sl.c) == sk;
       const double da = an ? pa.a : pa.c2, db = an ? pb.a : pb.c2;
       const double qa_ = an ? qa.a : qa.c2, qb_ = an ? qb.a : qb.c2;
-      const double eva = exp(sn * pa.c.V * L.iVt), evb = exp(sn * pb.c.V * L.iVt);
+      const double eva = an ? iexa : exa, evb = an ? iexb : exb;
       if (ina && !have[k]) {
         have[k] = true;
         first_k[k] = e;
