@@ -594,6 +594,7 @@ __device__ void ion_view(tr::View& W, const Args& a, const IonArgs& b, int l) {
   W.ybuf = 0;
   W.simss = a.simss;
   W.zimt = 0;
+  W.BD = nullptr;
 }
 
 // The ions' record of each device: its rows as a step of dti = 1 from the steady state itself.

@@ -32,6 +32,7 @@ struct View {
   double* Yb;
   size_t ybuf;
   int simss, zimt;
+  const double* BD;  // the step's state before it as densities [np+2][4][Bp] (n, p, a, c), or null
   __device__ __forceinline__ double x(int k, int f) const {
     return __ldg(X + ((size_t)k * DD_NT + f) * L.Bp + L.l);
   }
@@ -204,6 +205,22 @@ __device__ __forceinline__ void ion_iv(double sn, double x, double na, double nb
   }
 }
 
+// Both species' fluxes over interval k (points a = k, b = k + 1) where both points are in a
+// region of that species (zero otherwise): what row k takes as its right interval and row k + 1
+// as its left one.
+__device__ __forceinline__ void ion_ivs(const View& W, int k, const TP& a, const TP& b,
+                                        IonIv (&o)[2]) {
+  const Lane& L = W.L;
+#pragma unroll
+  for (int sp = 0; sp < 2; ++sp) {
+    const bool both = sp == 0 ? (a.c.sl.a >= 0 && b.c.sl.a >= 0) : (a.c.sl.c >= 0 && b.c.sl.c >= 0);
+    if (!both) { o[sp] = IonIv{0.0, 0.0, 0.0, 0.0}; continue; }
+    const double c = L.Vt * W.x(k, sp == 0 ? T_MUA : T_MUC);
+    ion_iv(sp == 0 ? -1.0 : 1.0, (b.c.V - a.c.V) * L.iVt, sp == 0 ? a.a : a.c2,
+           sp == 0 ? b.a : b.c2, c, W.simss, o[sp]);
+  }
+}
+
 // ------------------------------------------------------------------------------------ rows
 
 // Row i's residual (as -F in r), blocks A, B, C (5x5) and slot columns U (5xK) over the step
@@ -218,7 +235,8 @@ __device__ __forceinline__ void row5(const View& W, int i, const TP& pm, const T
                                      double bc, const double* logs, double (&A)[5][5],
                                      double (&B)[5][5], double (&Cm)[5][5], double (&r)[5],
                                      double (&U)[5][K], double* mass = nullptr,
-                                     double* tang = nullptr) {
+                                     double* tang = nullptr, const double* elogs = nullptr,
+                                     const IonIv* ivl = nullptr, const IonIv* ivr = nullptr) {
   const Lane& L = W.L;
   const double iVt = L.iVt;
   const double facl = L.st(i, S_FACL), facm = L.st(i, S_FACM), facu = L.st(i, S_FACU);
@@ -337,7 +355,8 @@ __device__ __forceinline__ void row5(const View& W, int i, const TP& pm, const T
     double flux = 0.0, dVl = 0.0, dVc = 0.0, dVr = 0.0, dll = 0.0, dlc = 0.0, dlr = 0.0;
     if (inl) {
       IonIv f;
-      ion_iv(sn, (pc.c.V - pm.c.V) * iVt, nl, nc, cl, W.simss, f);
+      if (ivl) f = ivl[sp];  // the interval's fluxes, carried from the row before
+      else ion_iv(sn, (pc.c.V - pm.c.V) * iVt, nl, nc, cl, W.simss, f);
       // anions take -hp F_l, cations +hp F_l
       const double w = sp == 0 ? -hp : hp;
       flux += w * f.F;
@@ -346,14 +365,15 @@ __device__ __forceinline__ void row5(const View& W, int i, const TP& pm, const T
     }
     if (inr) {
       IonIv f;
-      ion_iv(sn, (pn.c.V - pc.c.V) * iVt, nc, nr, cr, W.simss, f);
+      if (ivr) f = ivr[sp];
+      else ion_iv(sn, (pn.c.V - pc.c.V) * iVt, nc, nr, cr, W.simss, f);
       // anions take +hm F_r, cations -hm F_r
       const double w = sp == 0 ? hm : -hm;
       flux += w * f.F;
       dVc -= w * f.gx * iVt; dVr += w * f.gx * iVt;
       dlc += w * f.da; dlr += w * f.db;
     }
-    const double els = exp(ls);
+    const double els = elogs ? elogs[k] : exp(ls);
     const double value = (flux + fac * dti * (els * before - nc)) * scl;
     r[col] = -value;
     A[col][0] = dVl * scl; B[col][0] = dVc * scl; Cm[col][0] = dVr * scl;

@@ -54,6 +54,7 @@ struct Args {
   double* FB;  // [np+2][Bp]
   double* FI;  // [np+2][Bp]
   double* CD;  // [np+2][ncd][Bp]
+  double* BD;  // [np+2][4][Bp]: the state before the step, as densities
   int ncd;
   // outputs
   double* J;
@@ -102,6 +103,18 @@ __device__ __forceinline__ void load_pert(const View& W, int buf, const double* 
   P.c.dc = P.c.sl.c >= 0 ? P.c2 : 0.0;
 }
 
+// The state before the step at point k: its potential from buffer `buf`, its densities from the
+// step's before-state record (`W.BD`); the contacts as they are.
+__device__ __forceinline__ void load_before(const View& W, int buf, int k, double Vint, TP& P) {
+  if (!W.BD || k == 0 || k == W.L.NP + 1) { load_point(W, buf, k, Vint, P); return; }
+  const size_t o = (size_t)k * 4 * W.L.Bp + W.L.l;
+  P.c.V = *W.y(buf, k, 0);
+  P.c.n = W.BD[o];
+  P.c.p = W.BD[o + W.L.Bp];
+  P.a = W.BD[o + 2 * W.L.Bp];
+  P.c2 = W.BD[o + 3 * W.L.Bp];
+}
+
 // A perturbation of the current's inputs (PERT): the iterate and the state before the step along
 // their tangents, the traps' occupations along theirs, the ions' mobilities scaled by `mus`.
 struct Pert {
@@ -127,7 +140,8 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
   };
   auto load_c = [&](int buf, int k, double Vi, TP& P, bool is_cur) {
     if (PERT) load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P);
-    else load_point(W, buf, k, Vi, P);
+    else if (is_cur) load_point(W, buf, k, Vi, P);
+    else load_before(W, buf, k, Vi, P);
   };
   const int NP = L.NP;
   const double QL = Q * L.L;
@@ -576,7 +590,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
 #pragma unroll
   for (int k = 0; k < K; ++k) L.tot[k] = k < a.ka + a.kc ? L.sc(C_TOT0 + k) : 0.0;
   W.X = a.X; W.Yb = a.Yb; W.ybuf = (size_t)(a.npmax + 2) * 5 * a.Bp; W.simss = a.simss;
-  W.zimt = a.zimt;
+  W.zimt = a.zimt; W.BD = a.BD;
   const int NP = L.NP, Bp = a.Bp;
   const int ts = a.tstride;
   double* FB = a.FB;
@@ -648,6 +662,13 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
             const double cap = c == 0 ? capV : CAP_LN;
             *W.y(bn, i, c) = y + clipd(rt * (y - yp), -cap, cap);
           }
+          // the state before the step as densities, once for all its Newton iterations
+          const Slots sl = slots_at(L, i);
+          const size_t ob = (size_t)i * 4 * Bp + l;
+          a.BD[ob] = exp(*W.y(bk, i, 1));
+          a.BD[ob + Bp] = exp(*W.y(bk, i, 2));
+          a.BD[ob + 2 * Bp] = sl.a >= 0 ? exp(*W.y(bk, i, 3)) : 0.0;
+          a.BD[ob + 3 * Bp] = sl.c >= 0 ? exp(*W.y(bk, i, 4)) : 0.0;
           V = *W.y(bn, i, 0);
         } else {
           V = L.VL - 0.5 * L.left * V_k;
@@ -700,20 +721,28 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       load_point(W, bn, 1, V_k, pc);
       Flux el, er;
       flux(L, pm.c, pc.c, L.st(0, S_MUN), L.st(0, S_MUP), el);
+      double elg[K];  // the slots' scales, once per iteration
+#pragma unroll
+      for (int q = 0; q < K; ++q) elg[q] = exp(lg[q]);
+      IonIv ivl[2], ivr[2];  // the ions' fluxes of the row's left and right intervals
+      ion_ivs(W, 0, pm, pc, ivl);
       for (int i = 1; i <= NP; ++i) {
         load_point(W, bn, i + 1, V_k, pn);
         flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
+        ion_ivs(W, i, pc, pn, ivr);
         const double hm = L.st(i - 1, S_H), hp = L.st(i, S_H);
         const int ifm = (int)L.st(i - 1, S_IFK), ifi = (int)L.st(i, S_IFK);
         const double fb = FB[(size_t)i * Bp + l];
         const double fim = ifm >= 0 ? FI[(size_t)(i - 1) * Bp + l] : 0.0;
         const double fii = ifi >= 0 ? FI[(size_t)i * Bp + l] : 0.0;
-        const double bnv = exp(*W.y(bk, i, 1)), bpv = exp(*W.y(bk, i, 2));
-        const double bav = pc.c.sl.a >= 0 ? exp(*W.y(bk, i, 3)) : 0.0;
-        const double bcv = pc.c.sl.c >= 0 ? exp(*W.y(bk, i, 4)) : 0.0;
+        const size_t ob = (size_t)i * 4 * Bp + l;
+        const double bnv = a.BD[ob], bpv = a.BD[ob + Bp];
+        const double bav = a.BD[ob + 2 * Bp], bcv = a.BD[ob + 3 * Bp];
         double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][K];
         row5<K>(W, i, pm, pc, pn, el, er, hm, hp, ifm, ifi, dti, fb, fim, fii, bnv, bpv, bav, bcv,
-                lg, A, Bm, Cm, r, U);
+                lg, A, Bm, Cm, r, U, nullptr, nullptr, elg, ivl, ivr);
+        ivl[0] = ivr[0];
+        ivl[1] = ivr[1];
         // the ions' numbers over interval i-1 (between points i-1 and i)
         {
           const double hL = hm * L.L;
@@ -1007,7 +1036,8 @@ void ws_parts(const dd_batch* b, size_t* y, size_t* fb, size_t* fi, size_t* cd, 
   *y = align_up(3 * nodes * 5 * Bp * sizeof(double));
   *fb = align_up(nodes * Bp * sizeof(double));
   *fi = align_up(nodes * Bp * sizeof(double));
-  *cd = align_up(nodes * (size_t)(*ncd) * Bp * sizeof(double));
+  *cd = align_up(nodes * (size_t)(*ncd) * Bp * sizeof(double))
+        + align_up(nodes * 4 * Bp * sizeof(double));  // and the before-state record
   // the tangents: two parameters' states (two buffers each) and traps' occupations
   *tan = align_up(4 * nodes * 5 * Bp * sizeof(double)) + 2 * align_up(2 * nodes * Bp * sizeof(double));
 }
@@ -1066,6 +1096,7 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.FI = reinterpret_cast<double*>(w + y + fb);
   a.CD = reinterpret_cast<double*>(w + y + fb + fi);
   a.ncd = ncd;
+  a.BD = a.CD + ((size_t)batch->np_max + 2) * ncd * batch->lane_stride;
   a.J = out->J; a.Jext = out->J_ext; a.conv = out->converged; a.iters = out->iterations;
   a.acc = out->accepted; a.stop = out->stop; a.state_out = out->state; a.logs_out = out->logs;
   a.fb_out = out->f_bulk; a.fi_out = out->f_iface;
