@@ -163,10 +163,14 @@ int dd_admittance_workspace_bytes(const dd_batch* batch, int n_freq, size_t* byt
  * dy = -dF/dV per (lane, frequency) and the linearised current of a time step (control-volume
  * widths, each density's change, the displacement current; `eps` [np_max+2][lane_stride] the
  * permittivity at every point). Y [n_freq][2][lane_stride] (re, im). Lanes with mobile ions are
- * not supported (the host refuses them): k_anion and k_cation must be 1. */
+ * not supported (the host refuses them): k_anion and k_cation must be 1. `dt` 0: the continuous
+ * response; dt > 0: what a transient sees through implicit Euler at steps of dt (jaxdd's
+ * `solve_impedance(..., dt=)`, impedance.py:379-383): `laps` then (1 - e^(-i omega dt))/dt and
+ * the traps' occupations those of their exact step (its mean in the rates, its end in the
+ * charge). */
 int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
-                  const double* vint, const double* laps, int n_freq, int bernoulli, double* Y,
-                  void* workspace, size_t workspace_bytes, void* stream);
+                  const double* vint, const double* laps, int n_freq, int bernoulli, double dt,
+                  double* Y, void* workspace, size_t workspace_bytes, void* stream);
 
 #define DD_NT 3 /* per-point record of the transient and the impedance with ions: permittivity,
                    anion and cation mobility */
@@ -183,11 +187,12 @@ int dd_admittance_ions_workspace_bytes(const dd_batch* batch, int n_freq, size_t
  * [DD_MAXK][lane_stride] the steady state (dd_solve_states' checkpoint at `vint`, the ions
  * Boltzmann's of those normalisations); `tstat` [np_max+2][DD_NT][lane_stride] the
  * permittivity and the ions' mobilities. k_anion and k_cation must be 1; devices without mobile
- * ions are solved too (their ions' rows identities). Y [n_freq][2][lane_stride]. */
+ * ions are solved too (their ions' rows identities). Y [n_freq][2][lane_stride]; `dt` as
+ * dd_admittance's. */
 int dd_admittance_ions(const dd_batch* batch, const double* state, const double* state_logs,
                        const double* tstat, const double* vint, const double* laps, int n_freq,
-                       int bernoulli, double* Y, void* workspace, size_t workspace_bytes,
-                       void* stream);
+                       int bernoulli, double dt, double* Y, void* workspace,
+                       size_t workspace_bytes, void* stream);
 
 /* ---- Device building on the GPU (parameter sweeps) ------------------------------------------
  * The packed record of n devices of one stack structure from their parameters, as jaxdd's

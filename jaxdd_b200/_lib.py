@@ -132,7 +132,7 @@ def lib() -> ctypes.CDLL:
                                                  ctypes.POINTER(ctypes.c_size_t)]
     so.dd_admittance.restype = ctypes.c_int
     so.dd_admittance.argtypes = [ctypes.POINTER(DdBatch), p, p, p, p, ctypes.c_int, ctypes.c_int,
-                                 p, p, ctypes.c_size_t, p]
+                                 ctypes.c_double, p, p, ctypes.c_size_t, p]
     so.dd_build.restype = ctypes.c_int
     so.dd_build.argtypes = [ctypes.POINTER(DdStructure), p, p, ctypes.c_int, ctypes.c_int,
                             ctypes.c_int, ctypes.c_int, p, p, p, p, p, ctypes.c_size_t, p]
@@ -141,7 +141,7 @@ def lib() -> ctypes.CDLL:
                                                       ctypes.POINTER(ctypes.c_size_t)]
     so.dd_admittance_ions.restype = ctypes.c_int
     so.dd_admittance_ions.argtypes = [ctypes.POINTER(DdBatch), p, p, p, p, p, ctypes.c_int,
-                                      ctypes.c_int, p, p, ctypes.c_size_t, p]
+                                      ctypes.c_int, ctypes.c_double, p, p, ctypes.c_size_t, p]
     so.dd_transient_workspace_bytes.restype = ctypes.c_int
     so.dd_transient_workspace_bytes.argtypes = [ctypes.POINTER(DdBatch),
                                                 ctypes.POINTER(ctypes.c_size_t)]

@@ -48,6 +48,22 @@ __device__ __forceinline__ cplx operator/(cplx a, cplx b) {
   return {(a.re * r + a.im) / den, (a.im * r - a.re) / den};
 }
 
+// (df - df0)/df0 of a trap level of rate `a` at `lap` (jaxdd `_step_transfer`,
+// impedance.py:107-117), in its rates (hr) and its charge (hc): continuous both -lap/(lap + a);
+// over implicit Euler's steps of dt (lap then (1 - 1/z)/dt) the occupation's mean over a step
+// and its value at the step's end.
+__device__ __forceinline__ void transfer(double a, cplx lap, double dt, cplx& hr, cplx& hc) {
+  if (!(dt > 0.0)) {
+    hr = mk(0.0) - lap / (lap + mk(a));
+    hc = hr;
+    return;
+  }
+  const double x = a * dt, E = exp(-x), m = -expm1(-x) / x;
+  const cplx den = mk(1.0) - E * (mk(1.0) - dt * lap);
+  hr = ((-m * dt) * lap) / den;
+  hc = ((-E * dt) * lap) / den;
+}
+
 // Per node of the steady-state record (first kernel's output), [node][word][lane].
 enum {
   P_A = 0, P_B = 9, P_C = 18,      // the steady blocks
@@ -65,6 +81,7 @@ enum { W_C = 0, W_D = 18, W_WORDS = 24 };
 
 struct Args {
   int B, Bp, npmax, ka, simss, nf;
+  double dt;  // > 0: implicit Euler's steps of dt (the traps' step response); 0: continuous
   const double* S;
   const double* C;
   const double* IFt;
@@ -220,7 +237,8 @@ __global__ void __launch_bounds__(64) prepare_kernel(Args a) {
 // of (ln n_L, ln n_R, ln p_L, ln p_R) in the rates (`rate`), and the occupation's part in the
 // four point rates and the charge (`dR`).
 __device__ void iface_beyond(const Lane& L, int t, double nL, double nR, double pL, double pR,
-                             cplx lap, cplx (&rate)[4], double (&dR)[5]) {
+                             cplx lap, double dt, cplx (&rate)[4], cplx (&crate)[4],
+                             double (&dR)[5]) {
   const double Nt = L.itab(t, I_NT), Cn = L.itab(t, I_CN), Cp = L.itab(t, I_CP);
   const double nlo = L.itab(t, I_NT0LO), nhi = L.itab(t, I_NT0HI);
   const double plo = L.itab(t, I_PT0LO), phi = L.itab(t, I_PT0HI);
@@ -235,17 +253,22 @@ __device__ void iface_beyond(const Lane& L, int t, double nL, double nR, double 
   const double da[4] = {Cn * nL, Cn * nR, Cp * pL, Cp * pR};
   const double db[4] = {Cn * nL, Cn * nR, 0.0, 0.0};
   if (!(Nt > 0.0)) a = 1.0;
-  const cplx h = mk(0.0) - lap / (lap + mk(a));
+  cplx hr, hc;
+  transfer(a, lap, dt, hr, hc);
 #pragma unroll
-  for (int w = 0; w < 4; ++w) rate[w] = ((db[w] - f * da[w]) / a) * h;
+  for (int w = 0; w < 4; ++w) {
+    rate[w] = ((db[w] - f * da[w]) / a) * hr;
+    crate[w] = ((db[w] - f * da[w]) / a) * hc;
+  }
   if (!(Nt > 0.0))
 #pragma unroll
     for (int q = 0; q < 5; ++q) dR[q] = 0.0;
 }
 
 // The interface correction of row i's blocks: edges i-1 (this point its right end) and i (left).
-__device__ void iface_rows(const Lane& L, int i, double Vint, cplx lap, const double* rs,
-                           cplx (&dA)[3][3], cplx (&dB)[3][3], cplx (&dC)[3][3]) {
+__device__ void iface_rows(const Lane& L, int i, double Vint, cplx lap, double dt,
+                           const double* rs, cplx (&dA)[3][3], cplx (&dB)[3][3],
+                           cplx (&dC)[3][3]) {
   for (int side = 0; side < 2; ++side) {
     const int e = side == 0 ? i - 1 : i;  // the edge; this point is its right (0) or left (1) end
     if (e < 1 || e > L.NP - 1) continue;  // edges with both points interior
@@ -254,13 +277,15 @@ __device__ void iface_rows(const Lane& L, int i, double Vint, cplx lap, const do
     Pt p0, p1;
     point(L, e, Vint, p0);
     point(L, e + 1, Vint, p1);
-    cplx rate[4];
+    cplx rate_r[4], rate_c[4];
     double dR[5];
-    iface_beyond(L, t, p0.n, p1.n, p0.p, p1.p, lap, rate, dR);
+    iface_beyond(L, t, p0.n, p1.n, p0.p, p1.p, lap, dt, rate_r, rate_c, dR);
     const bool left_end = side == 1;
     const double rows[3] = {dR[4], left_end ? dR[0] : dR[1], left_end ? dR[2] : dR[3]};
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
+      // the charge (row 0) takes the occupation at a step's end, the rates its mean
+      const cplx (&rate)[4] = r == 0 ? rate_c : rate_r;
       // own logarithms: this point's; other: the edge's other point's
       const cplx own_n = rate[left_end ? 0 : 1], own_p = rate[left_end ? 2 : 3];
       const cplx oth_n = rate[left_end ? 1 : 0], oth_p = rate[left_end ? 3 : 2];
@@ -295,7 +320,7 @@ __device__ void inv3c(const cplx (&M)[3][3], cplx (&Mi)[3][3]) {
 
 // The interface recombination's tangent of point k (edges k-1 and k): the steady occupation's
 // derivatives in the points' logarithms and the traps' extra rates (`_interface_rates`).
-__device__ void iface_tangent(const Lane& L, int k, double Vint, cplx lap,
+__device__ void iface_tangent(const Lane& L, int k, double Vint, cplx lap, double dt,
                               const cplx (&dlnn)[3], const cplx (&dlnp)[3], cplx& tn, cplx& tp) {
   tn = mk(0.0); tp = mk(0.0);
   for (int e = k - 1; e <= k; ++e) {
@@ -317,9 +342,9 @@ __device__ void iface_tangent(const Lane& L, int k, double Vint, cplx lap,
       tp = tp + f.d[w][qp] * v[w];
     }
     // beyond the steady occupation (only edges with both points interior move, as jaxdd's)
-    cplx rate[4];
+    cplx rate[4], crate[4];
     double dR[5];
-    iface_beyond(L, t, p0.n, p1.n, p0.p, p1.p, lap, rate, dR);
+    iface_beyond(L, t, p0.n, p1.n, p0.p, p1.p, lap, dt, rate, crate, dR);
     cplx df = mk(0.0);
 #pragma unroll
     for (int w = 0; w < 4; ++w) df = df + rate[w] * v[w];
@@ -360,7 +385,8 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
       Bm[2][2] = Bm[2][2] + rec(i, P_MP) * lap;
       // bulk traps beyond their instantaneous occupation
       const double ta = rec(i, P_TA);
-      const cplx h = mk(0.0) - lap / (lap + mk(ta));
+      cplx h, hc_unused;
+      transfer(ta, lap, a.dt, h, hc_unused);  // neutral levels: the rates only
       const double fsc = L.st(i, S_FAC) * L.st(i, S_SC);
       const cplx rn = (rec(i, P_TDN) / ta) * h, rp = (rec(i, P_TDP) / ta) * h;
       Bm[1][1] = Bm[1][1] - (fsc * rec(i, P_TRN)) * rn;
@@ -370,7 +396,7 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
       if ((int)L.st(i - 1, S_IFK) >= 0 || (int)L.st(i, S_IFK) >= 0) {
         const double rs[3] = {Q * L.st(i, S_SP), -L.st(i, S_FAC) * L.st(i, S_SC),
                               -L.st(i, S_FAC) * L.st(i, S_SC)};
-        iface_rows(L, i, Vint, lap, rs, A, Bm, Cm);
+        iface_rows(L, i, Vint, lap, a.dt, rs, A, Bm, Cm);
       }
       // the drive: the residual's derivative in V_int (the contacts' potentials)
       cplx r[3] = {mk(0.0), mk(0.0), mk(0.0)};
@@ -461,18 +487,19 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
       if (trapped) {
         const cplx ln[3] = {dyv(k - 1, 1), dyv(k, 1), dyv(k + 1, 1)};
         const cplx lp[3] = {dyv(k - 1, 2), dyv(k, 2), dyv(k + 1, 2)};
-        iface_tangent(L, k, Vint, lap, ln, lp, dRi_k[0], dRi_k[1]);
+        iface_tangent(L, k, Vint, lap, a.dt, ln, lp, dRi_k[0], dRi_k[1]);
         if (k + 1 <= NP + 1) {
           const cplx ln1[3] = {dyv(k, 1), dyv(k + 1, 1), dyv(k + 2, 1)};
           const cplx lp1[3] = {dyv(k, 2), dyv(k + 1, 2), dyv(k + 2, 2)};
-          iface_tangent(L, k + 1, Vint, lap, ln1, lp1, dRi_k1[0], dRi_k1[1]);
+          iface_tangent(L, k + 1, Vint, lap, a.dt, ln1, lp1, dRi_k1[0], dRi_k1[1]);
         }
       }
       // the bulk traps' extra rates at k
       cplx dU[2] = {mk(0.0), mk(0.0)};
       if (k >= 1) {
         const double ta = rec(k, P_TA);
-        const cplx h = mk(0.0) - lap / (lap + mk(ta));
+        cplx h, hc_unused;
+        transfer(ta, lap, a.dt, h, hc_unused);
         const cplx df = ((rec(k, P_TDN) / ta) * h) * dyv(k, 1) + ((rec(k, P_TDP) / ta) * h) * dyv(k, 2);
         dU[0] = rec(k, P_TRN) * df;
         dU[1] = rec(k, P_TRP) * df;
@@ -749,7 +776,8 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       for (int rr = 0; rr < 5; ++rr) Bm[rr][rr] = Bm[rr][rr] + r5(i, R_M + rr) * lm1;
       // bulk traps beyond their instantaneous occupation (the carriers' 3x3)
       const double ta = rec(i, P_TA);
-      const cplx h = mk(0.0) - lap / (lap + mk(ta));
+      cplx h, hc_unused;
+      transfer(ta, lap, a.dt, h, hc_unused);  // neutral levels: the rates only
       const double fsc = L.st(i, S_FAC) * L.st(i, S_SC);
       const cplx rn = (rec(i, P_TDN) / ta) * h, rp = (rec(i, P_TDP) / ta) * h;
       Bm[1][1] = Bm[1][1] - (fsc * rec(i, P_TRN)) * rn;
@@ -764,7 +792,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
         for (int rr = 0; rr < 3; ++rr)
 #pragma unroll
           for (int c = 0; c < 3; ++c) { dA[rr][c] = mk(0.0); dB[rr][c] = mk(0.0); dC[rr][c] = mk(0.0); }
-        iface_rows(L, i, Vint, lap, rs, dA, dB, dC);
+        iface_rows(L, i, Vint, lap, a.dt, rs, dA, dB, dC);
 #pragma unroll
         for (int rr = 0; rr < 3; ++rr)
 #pragma unroll
@@ -922,17 +950,18 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       if (trapped) {
         const cplx ln[3] = {dyv(k - 1, 1), dyv(k, 1), dyv(k + 1, 1)};
         const cplx lp[3] = {dyv(k - 1, 2), dyv(k, 2), dyv(k + 1, 2)};
-        iface_tangent(L, k, Vint, lap, ln, lp, dRi_k[0], dRi_k[1]);
+        iface_tangent(L, k, Vint, lap, a.dt, ln, lp, dRi_k[0], dRi_k[1]);
         if (k + 1 <= NP + 1) {
           const cplx ln1[3] = {dyv(k, 1), dyv(k + 1, 1), dyv(k + 2, 1)};
           const cplx lp1[3] = {dyv(k, 2), dyv(k + 1, 2), dyv(k + 2, 2)};
-          iface_tangent(L, k + 1, Vint, lap, ln1, lp1, dRi_k1[0], dRi_k1[1]);
+          iface_tangent(L, k + 1, Vint, lap, a.dt, ln1, lp1, dRi_k1[0], dRi_k1[1]);
         }
       }
       cplx dU[2] = {mk(0.0), mk(0.0)};
       if (k >= 1) {
         const double ta = rec(k, P_TA);
-        const cplx h = mk(0.0) - lap / (lap + mk(ta));
+        cplx h, hc_unused;
+        transfer(ta, lap, a.dt, h, hc_unused);
         const cplx df = ((rec(k, P_TDN) / ta) * h) * dyv(k, 1) + ((rec(k, P_TDP) / ta) * h) * dyv(k, 2);
         dU[0] = rec(k, P_TRN) * df;
         dU[1] = rec(k, P_TRP) * df;
@@ -1069,8 +1098,8 @@ int dd_admittance_workspace_bytes(const dd_batch* batch, int n_freq, size_t* byt
 }
 
 int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
-                  const double* vint, const double* laps, int n_freq, int bernoulli, double* Y,
-                  void* workspace, size_t workspace_bytes, void* stream) {
+                  const double* vint, const double* laps, int n_freq, int bernoulli, double dt,
+                  double* Y, void* workspace, size_t workspace_bytes, void* stream) {
   if (!batch || !batch->stat || !batch->scal || !batch->iface || !state || !eps || !vint ||
       !laps || n_freq < 1 || !Y || !workspace)
     return DD_ERR_ARGS;
@@ -1085,6 +1114,8 @@ int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
   dd::imp::Args a{};
   a.B = batch->n_lanes; a.Bp = batch->lane_stride; a.npmax = batch->np_max; a.ka = batch->k_anion;
   a.simss = bernoulli == DD_BERNOULLI_SIMSS; a.nf = n_freq;
+  if (dt < 0.0) return DD_ERR_ARGS;
+  a.dt = dt;
   a.S = batch->stat; a.C = batch->scal; a.IFt = batch->iface;
   a.state = state; a.eps = eps; a.vint = vint; a.laps = laps; a.Y = Y;
   double* ws = static_cast<double*>(workspace);
@@ -1115,8 +1146,8 @@ int dd_admittance_ions_workspace_bytes(const dd_batch* batch, int n_freq, size_t
 
 int dd_admittance_ions(const dd_batch* batch, const double* state, const double* state_logs,
                        const double* tstat, const double* vint, const double* laps, int n_freq,
-                       int bernoulli, double* Y, void* workspace, size_t workspace_bytes,
-                       void* stream) {
+                       int bernoulli, double dt, double* Y, void* workspace,
+                       size_t workspace_bytes, void* stream) {
   if (!batch || !batch->stat || !batch->scal || !batch->iface || !state || !state_logs ||
       !tstat || !vint || !laps || n_freq < 1 || !Y || !workspace)
     return DD_ERR_ARGS;
@@ -1131,6 +1162,8 @@ int dd_admittance_ions(const dd_batch* batch, const double* state, const double*
   dd::imp::Args a{};
   a.B = batch->n_lanes; a.Bp = batch->lane_stride; a.npmax = batch->np_max; a.ka = batch->k_anion;
   a.simss = bernoulli == DD_BERNOULLI_SIMSS; a.nf = n_freq;
+  if (dt < 0.0) return DD_ERR_ARGS;
+  a.dt = dt;
   a.S = batch->stat; a.C = batch->scal; a.IFt = batch->iface;
   a.state = state; a.eps = nullptr; a.vint = vint; a.laps = laps; a.Y = Y;
   double* ws = static_cast<double*>(workspace);

@@ -50,7 +50,7 @@ class Work:
     `(J, converged, Y)` (J, converged flat in lane order; Y [frequency][re, im][lane])."""
 
     def __init__(self, batch: Batch, frequencies, voltage: float, tol: float = 1e-10,
-                 max_iter: int = 60, bernoulli_name: str = "exact"):
+                 max_iter: int = 60, bernoulli_name: str = "exact", dt: float | None = None):
         import torch
         from .adjoint import plan as _plan
         self.batch = batch
@@ -73,8 +73,11 @@ class Work:
         self.X = torch.from_numpy(X).to(cuda)
         self.eps = self.X[:, 0, :].contiguous()
         self.vint = torch.full((Bp,), float(voltage), dtype=torch.float64, device=cuda)
-        laps = np.zeros((len(frequencies), 2))
-        laps[:, 1] = 2 * np.pi * np.asarray(frequencies, dtype=float)
+        omega = 2 * np.pi * np.asarray(frequencies, dtype=float)
+        # iω, or over implicit Euler's steps of dt (1 − e^(−iω dt))/dt (impedance.py:379-383)
+        lap = 1j * omega if dt is None else -np.expm1(-1j * omega * dt) / dt
+        laps = np.stack([lap.real, lap.imag], -1)
+        self.dt = 0.0 if dt is None else float(dt)
         self.laps = torch.from_numpy(laps).to(cuda)
         self.nf = len(frequencies)
         self.Y = torch.empty((self.nf, 2, Bp), dtype=torch.float64, device=cuda)
@@ -98,24 +101,27 @@ class Work:
             _lib.check(_lib.lib().dd_admittance_ions(
                 ctypes.byref(desc), state.data_ptr(), ckpt["logs"][0].data_ptr(),
                 self.X.data_ptr(), self.vint.data_ptr(), self.laps.data_ptr(), self.nf,
-                self.bern, self.Y.data_ptr(), self.ws.data_ptr(), self.ws.numel(), stream),
-                "dd_admittance_ions")
+                self.bern, self.dt, self.Y.data_ptr(), self.ws.data_ptr(), self.ws.numel(),
+                stream), "dd_admittance_ions")
         else:
             _lib.check(_lib.lib().dd_admittance(
                 ctypes.byref(desc), state.data_ptr(), self.eps.data_ptr(), self.vint.data_ptr(),
-                self.laps.data_ptr(), self.nf, self.bern, self.Y.data_ptr(), self.ws.data_ptr(),
-                self.ws.numel(), stream), "dd_admittance")
+                self.laps.data_ptr(), self.nf, self.bern, self.dt, self.Y.data_ptr(),
+                self.ws.data_ptr(), self.ws.numel(), stream), "dd_admittance")
         return J, ok, self.Y
 
 
 def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float = 1e-10,
-                    max_iter: int = 60, bernoulli_name: str = "exact") -> ImpedanceResult:
+                    max_iter: int = 60, bernoulli_name: str = "exact",
+                    dt: float | None = None) -> ImpedanceResult:
     """The impedance of a batch at the internal voltage `voltage` (V) at each of `frequencies`
     (Hz), from the steady state there by one complex linear solve per frequency (jaxdd
     impedance.py:365-409). Free mobile ions move with the voltage as unknowns of their own.
     Refused (`NotImplementedError`), as the reference refuses them or as this build does not
     carry them: ions frozen at a pre-bias, several ion regions of a species, the differential
-    current (`currDiffInt = 1`)."""
+    current (`currDiffInt = 1`). `dt` (s): instead of the continuous response, what
+    `solve_transient` sees through implicit Euler at steps of `dt` (its time terms at
+    `(1 − e^(−iω dt))/dt`, the traps' occupations over each step as it solves them)."""
     devs = batch["devices"]
     if _mobile(batch) and any(d.pre_cond and d.fix_ions for d in devs):
         raise NotImplementedError("impedance with ions frozen at a pre-bias")
@@ -124,8 +130,10 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
     if any(d.curr_diff for d in devs):
         raise NotImplementedError("impedance with the differential current (currDiffInt = 1)")
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
+    if dt is not None and not dt > 0:
+        raise ValueError(f"dt must be positive, got {dt}")
     work = Work(batch, frequencies, voltage, tol=tol, max_iter=max_iter,
-                bernoulli_name=bernoulli_name)
+                bernoulli_name=bernoulli_name, dt=dt)
     J, ok, Y = work.run()
     lanes = batch["lane_of"]
     p = work.plan

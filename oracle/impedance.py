@@ -27,10 +27,17 @@ from jaxdd_b200.constants import Q
 from . import dd
 
 
-def _step_transfer(a, lap):
-    """(δf − δf₀)/δf₀ of a level of rate `a` at `iω` = `lap`, continuous: −iω/(iω + a) (in the
-    rates and in the charge alike, impedance.py:106-117)."""
-    return -lap / (lap + a)
+def _step_transfer(a, lap, dt=None):
+    """(δf − δf₀)/δf₀ of a level of rate `a` at `iω` = `lap` (impedance.py:107-117), in the rates
+    and in the charge: continuous both −iω/(iω + a); over implicit Euler's steps of `dt` (`lap`
+    then `(1 − z⁻¹)/dt`) the occupation's mean over a step and its value at the step's end."""
+    if dt is None:
+        h = -lap / (lap + a)
+        return h, h
+    x = a * dt
+    E, m = np.exp(-x), -np.expm1(-x) / x
+    den = 1.0 - E * (1.0 - lap * dt)
+    return -m * lap * dt / den, -E * lap * dt / den
 
 
 def trap_terms(rec, n, p):
@@ -47,11 +54,12 @@ def trap_terms(rec, n, p):
     return a, drive, dR
 
 
-def trap_blocks(s, rec, n, p, lap):
+def trap_blocks(s, rec, n, p, lap, dt=None):
     """`_trap_blocks` (impedance.py:197-212): the bulk traps' correction to each interior
-    point's own block (NP × 3 × 3), the continuity rows' `−fac·sC·dR·δf`."""
+    point's own block (NP × 3 × 3), the continuity rows' `−fac·sC·dR·δf` (neutral levels: the
+    rates only)."""
     a, drive, dR = trap_terms(rec, n, p)
-    rate = drive / a[:, None] * _step_transfer(a, lap)[:, None]
+    rate = drive / a[:, None] * _step_transfer(a, lap, dt)[0][:, None]
     blk = np.zeros((n.shape[0], 3, 3), complex)
     for row, k in ((1, 0), (2, 1)):
         for col in (1, 2):
@@ -59,10 +67,11 @@ def trap_blocks(s, rec, n, p, lap):
     return blk
 
 
-def interface_beyond(ti, n, p, lap):
+def interface_beyond(ti, n, p, lap, dt=None):
     """`_interface_beyond` (impedance.py:120-158), one level: per edge the occupation beyond its
-    steady response per unit of (ln n_L, ln n_R, ln p_L, ln p_R), and its part in the four point
-    rates and the charge."""
+    steady response per unit of (ln n_L, ln n_R, ln p_L, ln p_R), in the rates and in the charge
+    (`rate`, `charge`: equal but for `dt`), and its part in the four point rates and the
+    charge."""
     Nt, Cn, Cp, iw = ti["Nt"], ti["Cn"], ti["Cp"], ti["iw"]
     nL, nR, pL, pR = n[:-1], n[1:], p[:-1], p[1:]
     nt0, pt0 = ti["nt0_lo"] + ti["nt0_hi"], ti["pt0_lo"] + ti["pt0_hi"]
@@ -80,20 +89,21 @@ def interface_beyond(ti, n, p, lap):
     drive = db - fa[:, None] * da
     a = np.where(traps, a, 1.0)
     unit = drive / a[:, None]
-    h = _step_transfer(a, lap)
-    return unit * h[:, None], np.where(traps, dR, 0.0)
+    h_rate, h_charge = _step_transfer(a, lap, dt)
+    return unit * h_rate[:, None], unit * h_charge[:, None], np.where(traps, dR, 0.0)
 
 
-def interface_blocks(s, ti, n, p, lap):
+def interface_blocks(s, ti, n, p, lap, dt=None):
     """`_interface_blocks` (impedance.py:161-194): each edge's occupation beyond its steady
     response in its two points' rates and charge, as corrections to (A, B, C)."""
-    rate, dR = interface_beyond(ti, n, p, lap)
+    rate, charge, dR = interface_beyond(ti, n, p, lap, dt)
     NP = n.shape[0] - 2
 
     def block(side, cols):
         jn, jp = (0, 2) if cols == 0 else (1, 3)
-        rows = [dR[4], dR[0 if side == 0 else 1], dR[2 if side == 0 else 3]]
-        return np.stack([np.stack([d * rate[:, jn], d * rate[:, jp]], -1) for d in rows], -2)
+        rows = [(dR[4], charge), (dR[0 if side == 0 else 1], rate),
+                (dR[2 if side == 0 else 3], rate)]
+        return np.stack([np.stack([d * r[:, jn], d * r[:, jp]], -1) for d, r in rows], -2)
 
     def scaled(b, k):
         rs = np.stack([Q * s["sP"][k], -s["fac"][k] * s["sC"][k], -s["fac"][k] * s["sC"][k]], -1)
@@ -110,10 +120,10 @@ def interface_blocks(s, ti, n, p, lap):
     return dA, dB, dC
 
 
-def interface_rates(ti, n, p, lap, dy3):
+def interface_rates(ti, n, p, lap, dy3, dt=None):
     """`_interface_rates` (impedance.py:178-194 region): each point's electron and hole rate of
     the interface traps beyond their steady occupation at the response `dy3`."""
-    rate, dR = interface_beyond(ti, n, p, lap)
+    rate, _, dR = interface_beyond(ti, n, p, lap, dt)
     full = np.pad(dy3, ((1, 1), (0, 0)))
     logs = np.stack([full[:-1, 1], full[1:, 1], full[:-1, 2], full[1:, 2]], -1)
     df = np.sum(rate * logs, -1)
@@ -182,7 +192,7 @@ def current_tr(d, full, dti, before, Vbefore, width, dU=None, dRi=None):
     return np.sum(hh * (Jn + Jp + JD)) / np.sum(hh)
 
 
-def admittance(d, full0, Vint, laps, bern):
+def admittance(d, full0, Vint, laps, bern, dt=None):
     """One device's δJ/δV_int at each `iω` of `laps` about its steady state `full0`
     (`_admittance` without ions, impedance.py:230-353). `d` the oracle's 1-lane tree."""
     s = {k: v[0] for k, v in d["s"].items()}
@@ -226,10 +236,10 @@ def admittance(d, full0, Vint, laps, bern):
     out = []
     for lap in laps:
         Bl = Bb + lap * M[:, :, None] * np.eye(3)[None]
-        Bl = Bl + trap_blocks(s, {k: v[1:-1] for k, v in rec.items()}, n, p, lap)
+        Bl = Bl + trap_blocks(s, {k: v[1:-1] for k, v in rec.items()}, n, p, lap, dt)
         Al, Cl = A.astype(complex), C.astype(complex)
         if np.any(ti["Nt"] > 0):
-            dA, dB, dC = interface_blocks(s, ti, n_full, p_full, lap)
+            dA, dB, dC = interface_blocks(s, ti, n_full, p_full, lap, dt)
             Al, Bl, Cl = Al + dA, Bl + dB, Cl + dC
         rhs = (-dF).astype(complex)[:, :, None]
         dy = dd.block_thomas(Al[None], Bl[None], Cl[None], rhs[None])[0, :, :, 0]
@@ -237,13 +247,13 @@ def admittance(d, full0, Vint, laps, bern):
         J1 = linear(dy.real, 1.0, 1.0) + 1j * linear(dy.imag, 0.0, 1.0)
         # the bulk traps' rates beyond their steady occupation (`beyond`)
         a, drive, dR = trap_terms({k: v[1:-1] for k, v in rec.items()}, n, p)
-        rate = drive / a[:, None] * _step_transfer(a, lap)[:, None]
+        rate = drive / a[:, None] * _step_transfer(a, lap, dt)[0][:, None]
         df = rate[:, 0] * dy[:, 1] + rate[:, 1] * dy[:, 2]
         pad = np.zeros(1)
         dUn = np.concatenate([pad, dR[0] * df, pad])
         dUp = np.concatenate([pad, dR[1] * df, pad])
         if np.any(ti["Nt"] > 0):
-            dRn, dRp = interface_rates(ti, n_full, p_full, lap, dy)
+            dRn, dRp = interface_rates(ti, n_full, p_full, lap, dy, dt)
         else:
             dRn = dRp = np.zeros(NP + 2, complex)
         Ju = rates((dUn, dUp), (dRn, dRp))
@@ -251,7 +261,7 @@ def admittance(d, full0, Vint, laps, bern):
     return np.array(out)
 
 
-def admittance_ions(d, full0, Vint, laps, bern):
+def admittance_ions(d, full0, Vint, laps, bern, dt=None):
     """One device's δJ/δV_int at each `iω` of `laps` with its mobile ions as unknowns of their
     own (`_admittance` with `ions`, impedance.py:242-353): the 5×5 blocks of a time step of
     `dti` = 1 from the steady state `full0` ((NP + 2) × 5: V, ln n, ln p, ln a, ln c; the
@@ -306,10 +316,10 @@ def admittance_ions(d, full0, Vint, laps, bern):
     out = []
     for lap in laps:
         Bl = Bb + ((lap - 1.0) * M)[:, :, None] * eye[None]
-        Bl[:, :3, :3] += trap_blocks(s, {k: v[1:-1] for k, v in rec.items()}, n, p, lap)
+        Bl[:, :3, :3] += trap_blocks(s, {k: v[1:-1] for k, v in rec.items()}, n, p, lap, dt)
         Al, Cl = A.astype(complex), C.astype(complex)
         if np.any(ti["Nt"] > 0):
-            dA, dB, dC = interface_blocks(s, ti, n_full, p_full, lap)
+            dA, dB, dC = interface_blocks(s, ti, n_full, p_full, lap, dt)
             Al[:, :3, :3] += dA
             Bl[:, :3, :3] += dB
             Cl[:, :3, :3] += dC
@@ -322,13 +332,13 @@ def admittance_ions(d, full0, Vint, laps, bern):
         J0 = linear(dy.real, 1.0, 0.0) + 1j * linear(dy.imag, 0.0, 0.0)
         J1 = linear(dy.real, 1.0, 1.0) + 1j * linear(dy.imag, 0.0, 1.0)
         a, drive, dR = trap_terms({k: v[1:-1] for k, v in rec.items()}, n, p)
-        rate = drive / a[:, None] * _step_transfer(a, lap)[:, None]
+        rate = drive / a[:, None] * _step_transfer(a, lap, dt)[0][:, None]
         df = rate[:, 0] * dy[:, 1] + rate[:, 1] * dy[:, 2]
         pad = np.zeros(1)
         dUn = np.concatenate([pad, dR[0] * df, pad])
         dUp = np.concatenate([pad, dR[1] * df, pad])
         if np.any(ti["Nt"] > 0):
-            dRn, dRp = interface_rates(ti, n_full, p_full, lap, dy[:, :3])
+            dRn, dRp = interface_rates(ti, n_full, p_full, lap, dy[:, :3], dt)
         else:
             dRn = dRp = np.zeros(NP + 2, complex)
         Ju = rates((dUn, dUp), (dRn, dRp))
@@ -337,12 +347,14 @@ def admittance_ions(d, full0, Vint, laps, bern):
 
 
 def solve_impedance(devices, frequencies, voltage=0.0, tol=1e-10, max_iter=60,
-                    bernoulli_name="exact"):
+                    bernoulli_name="exact", dt=None):
     """`solve_impedance` (impedance.py:365-409): `(Y, Z, J, converged)`, Y and Z devices ×
     frequencies. Devices with free mobile ions take them as unknowns of their own
     (`admittance_ions`); ions frozen at a pre-bias are refused, as the reference refuses them."""
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
     laps = 1j * 2 * np.pi * frequencies
+    if dt is not None:  # implicit Euler's steps of dt: iω as (1 − z⁻¹)/dt (impedance.py:379-383)
+        laps = -np.expm1(-laps * dt) / dt
     bern = dd.BERNOULLI[bernoulli_name]
     Y, J, ok = [], [], []
     for dev in devices:
@@ -361,9 +373,9 @@ def solve_impedance(devices, frequencies, voltage=0.0, tol=1e-10, max_iter=60,
             full5 = np.concatenate([full0, la[:, None], lc[:, None]], -1)
             full5[0, 3:] = 0.0
             full5[-1, 3:] = 0.0
-            Y.append(admittance_ions(d, full5, float(voltage), laps, bern))
+            Y.append(admittance_ions(d, full5, float(voltage), laps, bern, dt))
         else:
-            Y.append(admittance(d, full0, float(voltage), laps, bern))
+            Y.append(admittance(d, full0, float(voltage), laps, bern, dt))
         J.append(st["J"][0, 0])
         ok.append(st["converged"][0, 0])
     Y = np.array(Y)

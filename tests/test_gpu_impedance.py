@@ -96,3 +96,54 @@ def test_what_impedance_refuses():
                                                                   "currDiffInt = 1")
     with pytest.raises(NotImplementedError, match="differential"):
         solve_impedance(prepare([build_device(setup_from_texts(t))]), [1e3])
+
+
+def _fast_ion_stack(NP=60):
+    """One of config 5's stacks with its ions at 1e-9 m²/Vs: they follow at 1 kHz."""
+    from jaxdd_b200.workloads import SEED_CONFIG5
+    k = 1
+    texts = drawn_texts(k, np.random.default_rng([SEED_CONFIG5, k]), NP)
+    texts["L2.txt"] = "\n".join(
+        f"{line.split('=')[0].strip()} = 1e-9"
+        if line.split("=")[0].strip() in ("mu_anion", "mu_cation") else line
+        for line in texts["L2.txt"].splitlines()) + "\n"
+    return build_device(setup_from_texts(texts))
+
+
+def _gpu_sine_response(dev, V0, f, amp, per_period=40, periods=20, fitted=4):
+    """The GPU transient's admittance at `f` from a sine of `amp` on `V0` (jaxdd
+    tests/test_impedance.py:47-63's protocol)."""
+    from jaxdd_b200.simss_input import TVG
+    from jaxdd_b200.transient import solve_transient
+    dt = 1.0 / (f * per_period)
+    k = np.arange(1, per_period * periods + 1)
+    t = np.concatenate([[0.0], k * dt])
+    V = np.concatenate([[V0], V0 + amp * np.sin(2 * np.pi * f * k * dt)])
+    r = solve_transient(prepare([dev]), TVG.steps(t, V, float(dev.G_frac), 0), tol=1e-12,
+                        max_iter=60)
+    assert r.converged.all()
+    m = k > per_period * (periods - fitted)
+    ph = 2 * np.pi * f * k[m] * dt
+    X = np.stack([np.ones(m.sum()), np.sin(ph), np.cos(ph)], -1)
+    c = np.linalg.lstsq(X, r.J[0, 1:][m], rcond=None)[0]
+    return (c[1] + 1j * c[2]) / amp, dt
+
+
+@pytest.mark.parametrize("case", ["ions", "interface"])
+def test_the_dt_form_is_the_gpu_transients_response(case):
+    """The two GPU paths against each other: `solve_impedance(..., dt=)` (`dd_admittance_ions`,
+    `dd_admittance`) is the GPU transient's (`dd_transient`) response to a small sine at steps of
+    dt, with mobile ions following at 1 kHz, and with interface traps at 10 kHz (1e-6 and 1e-7,
+    the reference's bars), and the oracle's dt form."""
+    if case == "ions":
+        dev, V0, f, amp, bar = _fast_ion_stack(), 0.8, 1e3, 1e-4, 1e-6
+    else:
+        t = pin_texts(60)
+        for name in ("L1.txt", "L2.txt"):
+            t[name] = t[name].replace("N_t_int = 0", "N_t_int = 1e15")
+        dev, V0, f, amp, bar = build_device(setup_from_texts(t)), 0.6, 1e4, 1e-5, 1e-7
+    Yt, dt = _gpu_sine_response(dev, V0, f, amp, periods=20 if case == "ions" else 12)
+    r = solve_impedance(prepare([dev]), [f], voltage=V0, tol=1e-12, max_iter=200, dt=dt)
+    assert abs(r.Y[0, 0] / Yt - 1) < bar
+    Yo = imp.solve_impedance([dev], [f], voltage=V0, tol=1e-12, max_iter=200, dt=dt)[0][0, 0]
+    assert abs(r.Y[0, 0] / Yo - 1) < 1e-6
