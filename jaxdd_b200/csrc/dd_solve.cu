@@ -1387,6 +1387,13 @@ namespace {
 
 int slots_k(const dd_batch* b) { return b->k_anion + b->k_cation <= 2 ? 2 : 4; }
 
+// Threads per block of the solve (two per device, the pairs adjacent lanes of a warp). One warp
+// a block spreads a batch's warps over the 148 SMs more evenly than two (at config 2's 16384
+// devices: at most 7 warps on an SM instead of 8; 2.2 % faster measured).
+#ifndef DD_SOLVE_BLOCK
+#define DD_SOLVE_BLOCK 32
+#endif
+
 size_t ws_elems(const dd_batch* b, size_t* y_e, size_t* fx_e, size_t* cd_e, int* ncd) {
   const int K = slots_k(b);
   *ncd = 12 + 3 * K;
@@ -1464,7 +1471,8 @@ int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opt
   a.J = J; a.ok = converged; a.its = iterations; a.status = lane_status; a.steps = lane_steps;
   a.tol = opts->tol; a.max_iter = opts->max_iter; a.start_iter = opts->start_iter;
   a.strict = opts->strict; a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS; a.mode = opts->mode;
-  const dim3 grid((2 * batch->lane_stride + 63) / 64), block(64);
+  const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
+      block(DD_SOLVE_BLOCK);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (slots_k(batch) == 2) dd::solve_kernel<2><<<grid, block, 0, s>>>(a);
   else dd::solve_kernel<4><<<grid, block, 0, s>>>(a);
@@ -1496,7 +1504,8 @@ int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_op
   a.strict = opts->strict; a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS; a.mode = opts->mode;
   a.states = states; a.state_logs = state_logs; a.prebias = prebias;
   a.prebias_logs = prebias_logs; a.nv_max = nv_max;
-  const dim3 grid((2 * batch->lane_stride + 63) / 64), block(64);
+  const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
+      block(DD_SOLVE_BLOCK);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (slots_k(batch) == 2) dd::solve_kernel<2><<<grid, block, 0, s>>>(a);
   else dd::solve_kernel<4><<<grid, block, 0, s>>>(a);
@@ -1516,7 +1525,8 @@ int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double*
   a.Y = y;  // the caller's state is the iterate buffer
   a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS;
   a.logs_io = logs; a.vint = vint; a.share = share; a.size_out = size; a.J_out = J;
-  const dim3 grid((2 * batch->lane_stride + 63) / 64), block(64);
+  const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
+      block(DD_SOLVE_BLOCK);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (slots_k(batch) == 2) dd::step_kernel<2><<<grid, block, 0, s>>>(a);
   else dd::step_kernel<4><<<grid, block, 0, s>>>(a);
