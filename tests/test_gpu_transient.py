@@ -163,3 +163,18 @@ def test_charge_gradients_match_differences_of_whole_transients():
         ref = fd(which, oracle)
         assert abs(mine[0] - ref[0]) < 1e-6 * abs(ref[0]) + 1e-9 * abs(g.Q[0]), (which, mine[0],
                                                                                  ref)
+
+
+def test_uneven_devices_and_their_own_steps_in_one_launch():
+    """Devices of different grid sizes (`prepare(..., ragged=True)`) each with its own step list
+    (the steps' per-lane layout) in one launch: each device's result is its transient alone."""
+    devs = [drawn_device(k, NP=n) for k, n in ((1, 60), (3, 90), (5, 75))]
+    tvgs = [transient_steps(30, V=v) for v in (0.9, 0.7, 1.0)]
+    r = solve_transient(prepare(devs, ragged=True), tvgs)
+    assert r.converged.all()
+    for k, (d, tv) in enumerate(zip(devs, tvgs)):
+        alone = solve_transient(prepare([d]), tv)
+        np.testing.assert_array_equal(r.iterations[k], alone.iterations[0])
+        scale = np.max(np.abs(alone.J[0]))
+        assert np.max(np.abs(r.J[k] - alone.J[0])) < 1e-12 * scale
+        np.testing.assert_allclose(r.final.V[k], alone.final.V[0], rtol=0, atol=1e-12)
