@@ -560,7 +560,7 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
     k0.record(stream)
     _lib.check(_lib.lib().dd_transient(
         ctypes.byref(desc), work.X.data_ptr(), ctypes.byref(steps_c),
-        ckpt["states"][0].data_ptr(), ckpt["logs"][0].data_ptr(), ctypes.byref(opts),
+        ckpt["states"][0].data_ptr(), ckpt["logs"][0].data_ptr(), None, ctypes.byref(opts),
         ctypes.byref(out_c), work.ws.data_ptr(), work.ws.numel(), stream.cuda_stream),
         "dd_transient")
     k1.record(stream)

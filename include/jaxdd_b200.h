@@ -281,7 +281,28 @@ typedef struct dd_transient_out {
    * species' mobilities), forward mode through every step. Both NULL: not computed. */
   double* Q;
   double* dQ;
+  /* Each step's state (`profiles`, jaxdd transient.py:449-451): prof_state
+   * [n_steps][np_max+2][5][lane_stride] the step's solution (contacts included, the ions' 0
+   * outside their regions), prof_f_bulk and prof_f_iface [n_steps][np_max+2][lane_stride] the
+   * traps' occupations at its end, prof_dti [n_steps][lane_stride]; kept or not. All NULL: none. */
+  double* prof_state;
+  double* prof_f_bulk;
+  double* prof_f_iface;
+  double* prof_dti;
 } dd_transient_out;
+
+/* A state to start from instead of the steady state at the first step (jaxdd's
+ * `solve_transient(..., initial=)`, transient.py:321-331): state [np_max+2][5][lane_stride]
+ * (V, ln n, ln p, ln a, ln c; the interior points used, the ions' where mobile), f_bulk and
+ * f_iface [np_max+2][lane_stride] the traps' occupations, scalars [4][lane_stride]: the state's
+ * t, V_int, J_ext and dti. The slots' scales start at 1 and the first step's guess is the state
+ * itself (no extrapolation). */
+typedef struct dd_transient_init {
+  const double* state;
+  const double* f_bulk;
+  const double* f_iface;
+  const double* scalars;
+} dd_transient_init;
 
 /* Scratch bytes dd_transient needs for this batch. */
 int dd_transient_workspace_bytes(const dd_batch* batch, size_t* bytes);
@@ -295,13 +316,14 @@ int dd_transient_workspace_bytes(const dd_batch* batch, size_t* bytes);
  * [np_max+2][DD_NT][lane_stride] the permittivity and the ions' mobilities at each point;
  * `start` [np_max+2][3][lane_stride] and `start_logs` [DD_MAXK][lane_stride] the steady state
  * at the first step (dd_solve_states at steps->v[0] with the generation factor
- * steps->g_frac[0] and no pre-bias). opts: tol, max_iter (Newton per step), bernoulli. Not
+ * steps->g_frac[0] and no pre-bias), or `initial` (then start and start_logs may be NULL). opts:
+ * tol, max_iter (Newton per step), bernoulli. Not
  * supported (the host refuses them): an open circuit, a series resistance, Track 2 or 3, ion
  * regions that reach a contact. */
 int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* steps,
-                 const double* start, const double* start_logs, const dd_opts* opts,
-                 const dd_transient_out* out, void* workspace, size_t workspace_bytes,
-                 void* stream);
+                 const double* start, const double* start_logs, const dd_transient_init* initial,
+                 const dd_opts* opts, const dd_transient_out* out, void* workspace,
+                 size_t workspace_bytes, void* stream);
 
 /* One damped Newton step per lane from the state y (`[(np_max+2)][3][lane_stride]`, interior
  * nodes used) and the ion normalisations logs (`[K][lane_stride]`) at the voltage Vint

@@ -85,7 +85,11 @@ class DdSteps(ctypes.Structure):
 class DdTransientOut(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in (
         "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs", "f_bulk",
-        "f_iface", "Q", "dQ")]
+        "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface", "prof_dti")]
+
+
+class DdTransientInit(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in ("state", "f_bulk", "f_iface", "scalars")]
 
 
 class DdOpts(ctypes.Structure):
@@ -147,8 +151,8 @@ def lib() -> ctypes.CDLL:
                                                 ctypes.POINTER(ctypes.c_size_t)]
     so.dd_transient.restype = ctypes.c_int
     so.dd_transient.argtypes = [ctypes.POINTER(DdBatch), p, ctypes.POINTER(DdSteps), p, p,
-                                ctypes.POINTER(DdOpts), ctypes.POINTER(DdTransientOut), p,
-                                ctypes.c_size_t, p]
+                                ctypes.POINTER(DdTransientInit), ctypes.POINTER(DdOpts),
+                                ctypes.POINTER(DdTransientOut), p, ctypes.c_size_t, p]
     so.dd_solve_noalloc.restype = ctypes.c_int
     so.dd_solve_noalloc.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
                                     ctypes.POINTER(DdOpts), p, p, p, p, p, p]

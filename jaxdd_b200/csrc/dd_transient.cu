@@ -73,6 +73,15 @@ struct Args {
   double* TY;         // [2][2][np+2][5][Bp]: each tangent of the state, two rotating buffers
   double* TFB;        // [2][np+2][Bp]: of the bulk traps' occupations
   double* TFI;        // [2][np+2][Bp]: of the interface traps'
+  // each step's state (nullptr: none) and a given state to start from (nullptr: steady)
+  double* prof_state;  // [S][np+2][5][Bp]
+  double* prof_fb;     // [S][np+2][Bp]
+  double* prof_fi;     // [S][np+2][Bp]
+  double* prof_dti;    // [S][Bp]
+  const double* init_state;  // [np+2][5][Bp]
+  const double* init_fb;     // [np+2][Bp]
+  const double* init_fi;     // [np+2][Bp]
+  const double* init_scal;   // [4][Bp]: t, V_int, J_ext, dti
 };
 
 // ------------------------------------------------------------------------------------ current
@@ -323,6 +332,45 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
 // exactly).
 
 constexpr double TANGENT_H = 1e-6;  // the current's central-difference step along a tangent
+
+// Step k's solution on every point (V, ln n, ln p, and ln a, ln c where the ions are mobile,
+// else 0) and the traps' occupations at its end from the ones before it, kept or not
+// (`snapshot(after)`, `fb_new`, `fi_new`, transient.py:444): out of line, so that the step
+// loop's registers stay its own.
+__device__ __noinline__ void write_profile(const Args& a, const View& W, int bn, int k,
+                                           double V_k, double dti) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = a.Bp, l = L.l;
+  const size_t nodes = (size_t)a.npmax + 2;
+  TP pa, pb;
+  load_point(W, bn, 0, V_k, pa);
+  for (int i = 0; i <= NP + 1; ++i) {
+    TP P;
+    load_point(W, bn, i, V_k, P);
+    const double v5[5] = {P.c.V, P.c.lnn, P.c.lnp, P.c.sl.a >= 0 ? P.la : 0.0,
+                          P.c.sl.c >= 0 ? P.lc : 0.0};
+#pragma unroll
+    for (int c = 0; c < 5; ++c) a.prof_state[(((size_t)k * nodes + i) * 5 + c) * Bp + l] = v5[c];
+    a.prof_fb[((size_t)k * nodes + i) * Bp + l] =
+        (i >= 1 && i <= NP && L.st(i, S_NT) > 0.0)
+            ? bulk_end(L, i, P.c.n, P.c.p, a.FB[(size_t)i * Bp + l], dti)
+            : 0.0;
+  }
+  for (int e = 0; e <= NP; ++e) {
+    load_point(W, bn, e + 1, V_k, pb);
+    const int ifk = (int)L.st(e, S_IFK);
+    double end = 0.0;
+    if (ifk >= 0) {
+      Iface t;
+      iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, a.FI[(size_t)e * Bp + l], dti, t,
+                   false, &end);
+    }
+    a.prof_fi[((size_t)k * nodes + e) * Bp + l] = end;
+    pa = pb;
+  }
+  a.prof_fi[((size_t)k * nodes + NP + 1) * Bp + l] = 0.0;
+  a.prof_dti[(size_t)k * Bp + l] = dti;
+}
 
 template <int K>
 __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk, double V_k,
@@ -598,23 +646,37 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   auto cd = [&](int k, int f) -> double* { return a.CD + ((size_t)k * a.ncd + f) * Bp + l; };
   constexpr int NC = 1 + K;  // right-hand sides: -F and the K slot columns
 
-  // ---- the start: the steady state at the first step, with the ions' densities as unknowns
+  // ---- the start: the steady state at the first step, with the ions' densities as unknowns,
+  // or a given state (its slots' scales 1)
   int bk = 0, bp = 1, bn = 2;  // kept, kept before it, iterate
+  const bool given = a.init_state != nullptr;
   double logs[K], logs_p[K];
 #pragma unroll
-  for (int k = 0; k < K; ++k) { logs[k] = a.logs0[(size_t)k * Bp + l]; logs_p[k] = logs[k]; }
+  for (int k = 0; k < K; ++k) {
+    logs[k] = given ? 0.0 : a.logs0[(size_t)k * Bp + l];
+    logs_p[k] = logs[k];
+  }
   for (int i = 1; i <= NP; ++i) {
-    const double V = a.y0[((size_t)i * 3 + 0) * Bp + l];
     const Slots sl = slots_at(L, i);
-    const double v5[5] = {V, a.y0[((size_t)i * 3 + 1) * Bp + l],
-                          a.y0[((size_t)i * 3 + 2) * Bp + l],
-                          sl.a >= 0 ? logs[sl.a] + V * L.iVt : 0.0,
-                          sl.c >= 0 ? logs[L.ka + sl.c] - V * L.iVt : 0.0};
+    double v5[5];
+    if (given) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) v5[c] = a.init_state[((size_t)i * 5 + c) * Bp + l];
+      if (sl.a < 0) v5[3] = 0.0;
+      if (sl.c < 0) v5[4] = 0.0;
+    } else {
+      const double V = a.y0[((size_t)i * 3 + 0) * Bp + l];
+      v5[0] = V;
+      v5[1] = a.y0[((size_t)i * 3 + 1) * Bp + l];
+      v5[2] = a.y0[((size_t)i * 3 + 2) * Bp + l];
+      v5[3] = sl.a >= 0 ? logs[sl.a] + V * L.iVt : 0.0;
+      v5[4] = sl.c >= 0 ? logs[L.ka + sl.c] - V * L.iVt : 0.0;
+    }
 #pragma unroll
     for (int c = 0; c < 5; ++c) { *W.y(bk, i, c) = v5[c]; *W.y(bp, i, c) = v5[c]; }
-    FB[(size_t)i * Bp + l] = 0.0;
+    FB[(size_t)i * Bp + l] = given ? a.init_fb[(size_t)i * Bp + l] : 0.0;
   }
-  for (int e = 0; e <= NP; ++e) FI[(size_t)e * Bp + l] = 0.0;
+  for (int e = 0; e <= NP; ++e) FI[(size_t)e * Bp + l] = given ? a.init_fi[(size_t)e * Bp + l] : 0.0;
   const int fm = a.fmode[l];
   // the integrated current and its tangents (zero tangents before the first step)
   const bool grad = a.TY != nullptr;
@@ -632,7 +694,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         a.TFI[((size_t)p * tnodes + i) * Bp + l] = 0.0;
       }
   }
-  double V_now = a.V[ts ? l : 0], dti_now = 0.0, t_last = 0.0;
+  double V_now = given ? a.init_scal[(size_t)Bp + l] : a.V[ts ? l : 0];
+  double dti_now = given ? a.init_scal[(size_t)3 * Bp + l] : 0.0;
+  double t_last = given ? a.init_scal[l] : 0.0;
   int track_curr = 0, stop = 0;
   bool first = true;
   const double capV = CAP_V * L.Vt;
@@ -920,6 +984,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const bool ok = done;
     const double J = jh[STALL_STEPS];
     const double J_ext = J + L.Gshunt * V_k;
+    if (a.prof_state) write_profile(a, W, bn, k, V_k, dti);
     // ---- ZimT's main loop (transient.py:419-445)
     const bool running = stop == 0;
     const bool failed = running && !ok && (fm == 0 || (fm == 2 && track_curr == 1));
@@ -1061,11 +1126,17 @@ int dd_transient_workspace_bytes(const dd_batch* batch, size_t* bytes) {
 }
 
 int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* steps,
-                 const double* start, const double* start_logs, const dd_opts* opts,
-                 const dd_transient_out* out, void* workspace, size_t workspace_bytes,
-                 void* stream) {
+                 const double* start, const double* start_logs, const dd_transient_init* initial,
+                 const dd_opts* opts, const dd_transient_out* out, void* workspace,
+                 size_t workspace_bytes, void* stream) {
   if (!batch_ok(batch) || !batch->stat || !batch->scal || !batch->iface || !tstat || !steps ||
-      !start || !start_logs || !opts || !out || !workspace)
+      !opts || !out || !workspace)
+    return DD_ERR_ARGS;
+  if (initial ? (!initial->state || !initial->f_bulk || !initial->f_iface || !initial->scalars)
+              : (!start || !start_logs))
+    return DD_ERR_ARGS;
+  const bool prof = out->prof_state || out->prof_f_bulk || out->prof_f_iface || out->prof_dti;
+  if (prof && !(out->prof_state && out->prof_f_bulk && out->prof_f_iface && out->prof_dti))
     return DD_ERR_ARGS;
   if (steps->n_steps < 1 || !steps->t || !steps->v || !steps->g_frac || !steps->track ||
       !steps->failure_mode || (steps->stride != 0 && steps->stride != batch->lane_stride))
@@ -1101,6 +1172,12 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.acc = out->accepted; a.stop = out->stop; a.state_out = out->state; a.logs_out = out->logs;
   a.fb_out = out->f_bulk; a.fi_out = out->f_iface;
   a.Qout = out->Q; a.dQout = out->dQ;
+  a.prof_state = out->prof_state; a.prof_fb = out->prof_f_bulk; a.prof_fi = out->prof_f_iface;
+  a.prof_dti = out->prof_dti;
+  a.init_state = initial ? initial->state : nullptr;
+  a.init_fb = initial ? initial->f_bulk : nullptr;
+  a.init_fi = initial ? initial->f_iface : nullptr;
+  a.init_scal = initial ? initial->scalars : nullptr;
   if (out->Q) {
     const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
     char* t = w + y + fb + fi + cd;

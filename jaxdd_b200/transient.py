@@ -8,10 +8,13 @@ carried from step to step, the current with each density's change, the ions' cur
 displacement current, and ZimT's main loop (which steps are kept, each step's Δt from the last
 one kept).
 
+With `profiles=True` every step's state is written beside its current (`TransientResult.state`);
+with `initial=` (a `TransientState`) the devices start from that state instead of a steady one.
+
 The voltage is given at every step. Refused (`NotImplementedError`), not approximated: an open
 circuit or a series resistance (the internal voltage an unknown), `Track` 2 or 3 (ZimT's
-automatic stop), photon recycling, the profiles of every step, a start from a given state, ion
-regions that reach a contact, ZimT's last-region ion currents with several regions of a species.
+automatic stop), photon recycling, ion regions that reach a contact, ZimT's last-region ion
+currents with several regions of a species.
 """
 
 from __future__ import annotations
@@ -54,11 +57,13 @@ class TransientState:
 
 @dataclass(frozen=True)
 class TransientResult:
-    """Per device and step (devices × steps), as jaxdd's (transient.py:97-122): `J` the internal
+    """Per device and step (devices × steps), as jaxdd's (transient.py:97-135): `J` the internal
     current density (A/m²), `J_ext` with the shunt, `V_int`, `V_ext`, `converged`, `iterations`,
     `accepted` (the steps ZimT keeps); per device `stop` (0, or `STOP_FAILED`); `t` each step's
-    time; `final` the last state kept. ZimT's other tJFile columns are not built (`columns`
-    empty)."""
+    time; `final` the last state kept; with `profiles=True` `profiles` `{"V", "n", "p", "anion",
+    "cation", "f_bulk", "f_interface", "dti"}` (devices × steps × points, or per device where
+    the grids differ), from which `state(k)` is step k's state. ZimT's other tJFile columns are
+    not built (`columns` empty)."""
 
     J: np.ndarray
     J_ext: np.ndarray
@@ -71,6 +76,87 @@ class TransientResult:
     t: np.ndarray
     final: TransientState
     columns: dict
+    profiles: dict | None = None
+
+    def state(self, k: int) -> TransientState:
+        """Every device's state at step `k` (jaxdd transient.py:124-135): the step's solution,
+        as the next step starts from it where the step was kept."""
+        if self.profiles is None:
+            raise ValueError("a step's state needs the profiles: solve_transient(profiles=True)")
+        prof = self.profiles
+
+        def at(a):
+            if a.dtype == object:
+                return _stack([row[k] for row in a])
+            return a[:, k]
+        return TransientState(
+            t=self.t[:, k], V=at(prof["V"]), n=at(prof["n"]), p=at(prof["p"]),
+            anion=at(prof["anion"]), cation=at(prof["cation"]), V_int=self.V_int[:, k],
+            J_ext=self.J_ext[:, k], dti=prof["dti"][:, k], f_bulk=at(prof["f_bulk"]),
+            f_interface=at(prof["f_interface"]))
+
+
+def _stack(xs):
+    """Per-device arrays stacked, or an object array of them where their lengths differ."""
+    if len({np.shape(x) for x in xs}) == 1:
+        return np.stack(xs)
+    out = np.empty(len(xs), dtype=object)
+    out[:] = xs
+    return out
+
+
+def _per_device(name, value, lengths):
+    """`initial.<name>` as one float array per device of the given lengths."""
+    shape = (len(lengths), *sorted(set(lengths)))
+    bad = ValueError(f"initial.{name}: one value per device and point, {shape}, got "
+                     f"{np.shape(value) if np.asarray(value).dtype != object else 'ragged'}")
+    if isinstance(value, np.ndarray) and value.dtype != object and value.ndim != 2:
+        raise bad
+    try:
+        rows = list(value)
+    except TypeError:
+        raise bad from None
+    if len(rows) != len(lengths):
+        raise bad
+    out = [np.asarray(r, dtype=float) for r in rows]
+    if any(r.shape != (m,) for r, m in zip(out, lengths)):
+        raise bad
+    return out
+
+
+def _checked_initial(initial: TransientState, devs, t) -> dict:
+    """`solve_transient`'s `initial` checked against the devices and their steps as jaxdd
+    checks it (transient.py:498-534), with the same messages: one value per device and point,
+    per device for the scalars; the bulk traps' occupations on the interior points, the
+    interface traps' on the intervals (not read where no device has interface traps); every
+    first time after the state's; the densities positive, the ions where they are mobile."""
+    n = len(devs)
+    points = [len(d.x) for d in devs]
+    st = {f: _per_device(f, getattr(initial, f), points)
+          for f in ("V", "n", "p", "anion", "cation")}
+    for f in ("t", "V_int", "J_ext", "dti"):
+        v = np.asarray(getattr(initial, f), dtype=float)
+        if v.shape != (n,):
+            raise ValueError(f"initial.{f}: one value per device ({n}), got {v.shape}")
+        st[f] = v
+    st["f_bulk"] = _per_device("f_bulk", initial.f_bulk, [m - 2 for m in points])
+    fi = initial.f_interface
+    if not any(d.interface is not None for d in devs):
+        st["f_interface"] = [np.zeros(m - 1) for m in points]
+    else:
+        st["f_interface"] = _per_device("f_interface", fi, [m - 1 for m in points])
+    if not np.all(np.asarray(t)[:, 0] > st["t"]):
+        raise ValueError("a transient from a state starts after it: every device's first time "
+                         "must exceed its state's t")
+    if not all(np.all(a > 0) for a in st["n"] + st["p"]):
+        raise ValueError("initial.n and initial.p must be positive on every point")
+    for name, mask in (("anion", "anion_mask"), ("cation", "cation_mask")):
+        for d, a in zip(devs, st[name]):
+            m = getattr(d, mask)
+            if m is not None and np.any(np.asarray(m, bool) & ~(a > 0)):
+                raise ValueError(f"initial.{name} must be positive where the device's "
+                                 f"{name}s are mobile")
+    return st
 
 
 def _steps(tvgs: list[TVG]):
@@ -109,7 +195,7 @@ class Work:
 
     def __init__(self, batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
                  bernoulli_name: str = "exact", zimt_current: bool = False,
-                 gradients: bool = False):
+                 gradients: bool = False, profiles: bool = False, initial=None):
         import torch
         from .adjoint import plan as _plan
         _check_batch(batch)
@@ -118,6 +204,7 @@ class Work:
         if len(tvgs) != len(devs):
             raise ValueError("one tVG for the batch, or one per device, all of one length")
         t, V, G, track, fm = _steps(tvgs)
+        init = None if initial is None else _checked_initial(initial, devs, t)
         self.batch, self.tol, self.max_iter = batch, tol, max_iter
         self.bern = _lib.DD_BERNOULLI[bernoulli_name]
         self.g = g = _gpu(batch)
@@ -185,6 +272,33 @@ class Work:
         if gradients:
             self.out["Q"] = torch.empty(Bp, dtype=f64, device=cuda)
             self.out["dQ"] = torch.empty((2, Bp), dtype=f64, device=cuda)
+        if profiles:
+            self.out["prof_state"] = torch.empty((S, nodes, 5, Bp), dtype=f64, device=cuda)
+            self.out["prof_f_bulk"] = torch.empty((S, nodes, Bp), dtype=f64, device=cuda)
+            self.out["prof_f_iface"] = torch.empty((S, nodes, Bp), dtype=f64, device=cuda)
+            self.out["prof_dti"] = torch.empty((S, Bp), dtype=f64, device=cuda)
+        # the given state to start from: V, ln n, ln p, and ln a, ln c where the ions are mobile
+        self.initial = init
+        if init is not None:
+            st = np.zeros((nodes, 5, Bp))
+            fb, fi, sc = np.zeros((nodes, Bp)), np.zeros((nodes, Bp)), np.zeros((4, Bp))
+            for k, d in enumerate(devs):
+                m, ln = len(d.x), lanes[k]
+                st[:m, 0, ln] = init["V"][k]
+                st[:m, 1, ln] = np.log(init["n"][k])
+                st[:m, 2, ln] = np.log(init["p"][k])
+                for c, (name, mask) in enumerate((("anion", d.anion_mask),
+                                                  ("cation", d.cation_mask)), start=3):
+                    if mask is not None:
+                        mob = np.asarray(mask, bool)
+                        st[:m, c, ln] = np.where(mob, np.log(np.where(mob, init[name][k], 1.0)),
+                                                 0.0)
+                fb[1:m - 1, ln] = init["f_bulk"][k]
+                fi[:m - 1, ln] = init["f_interface"][k]
+                sc[:, ln] = [init[f][k] for f in ("t", "V_int", "J_ext", "dti")]
+            self.init = {name: torch.from_numpy(a).to(cuda)
+                         for name, a in (("state", st), ("f_bulk", fb), ("f_iface", fi),
+                                         ("scalars", sc))}
         size = ctypes.c_size_t(0)
         desc = descriptor(batch, g, self.plan.y0)
         _lib.check(_lib.lib().dd_transient_workspace_bytes(ctypes.byref(desc),
@@ -193,26 +307,34 @@ class Work:
         self.ws = torch.empty(size.value, dtype=torch.uint8, device=cuda)
 
     def run(self):
-        """The start and the transient, on the current stream: `(out, start_converged)`."""
+        """The start and the transient, on the current stream: `(out, start_converged)`
+        (`start_converged` None from a given state)."""
         import torch
         from .adjoint import solve_states as _solve_states
         g = self.g
-        _, ok0, _, ckpt = _solve_states(self.plan, g.stat, self.scal0, g.iface)
-        start, start_logs = ckpt["states"][0], ckpt["logs"][0]
+        if self.initial is None:
+            _, ok0, _, ckpt = _solve_states(self.plan, g.stat, self.scal0, g.iface)
+            start, start_logs = ckpt["states"][0].data_ptr(), ckpt["logs"][0].data_ptr()
+            init = None
+        else:
+            ok0, start, start_logs = None, None, None
+            init = ctypes.byref(_lib.DdTransientInit(*(self.init[k].data_ptr() for k in (
+                "state", "f_bulk", "f_iface", "scalars"))))
         steps = _lib.DdSteps(self.S, self.stride, self.tv.data_ptr(), self.vv.data_ptr(),
                              self.gv.data_ptr(), self.trk.data_ptr(), self.fm.data_ptr(),
                              self.zimt)
         o = self.out
         out = _lib.DdTransientOut(*(o[k].data_ptr() if k in o else None for k in (
             "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",
-            "f_bulk", "f_iface", "Q", "dQ")))
+            "f_bulk", "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface",
+            "prof_dti")))
         opts = _lib.DdOpts(float(self.tol), int(self.max_iter), int(self.max_iter), 0,
                            self.bern, _lib.DD_MODE_BATCH, 0, 0)
         desc = descriptor(self.batch, g, self.plan.y0)
         _lib.check(_lib.lib().dd_transient(
-            ctypes.byref(desc), self.X.data_ptr(), ctypes.byref(steps), start.data_ptr(),
-            start_logs.data_ptr(), ctypes.byref(opts), ctypes.byref(out), self.ws.data_ptr(),
-            self.ws.numel(), torch.cuda.current_stream(g.stat.device).cuda_stream),
+            ctypes.byref(desc), self.X.data_ptr(), ctypes.byref(steps), start, start_logs, init,
+            ctypes.byref(opts), ctypes.byref(out), self.ws.data_ptr(), self.ws.numel(),
+            torch.cuda.current_stream(g.stat.device).cuda_stream),
             "dd_transient")
         return o, ok0
 
@@ -226,13 +348,17 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
     one length): jaxdd's `solve_transient` (transient.py:537-637) with the same arguments.
     `zimt_current`: ZimT's sums in the integral current (each point's change over the interval
     after it); by default over each point's control volume. `ion_flux`: both of jaxdd's are the
-    Scharfetter–Gummel flux without ion sites, the only case built. Not built (raise
-    `NotImplementedError`): `recycle`, `profiles`, `initial`, an internal voltage as an unknown
-    (`vint`, an open circuit, a series resistance), and `zimt_ion_currents` with several regions
-    of a species. `ions` is accepted for the reference's signature: the ions are unknowns of
-    every step here, which leaves devices without mobile ions as they are."""
-    if recycle is not None or profiles or initial is not None:
-        raise NotImplementedError("recycle, profiles and initial: not built")
+    Scharfetter–Gummel flux without ion sites, the only case built. `profiles`: every step's
+    state (`TransientResult.profiles`, `state(k)`). `initial` (a `TransientState`, e.g. a
+    result's `final` or `state(k)`): every device starts from it instead of from a steady state,
+    its slots' scales 1 and the first step's guess the state itself (no extrapolation), checked
+    as jaxdd checks it (`ValueError`). Not built (raise `NotImplementedError`): `recycle`, an
+    internal voltage as an unknown (`vint`, an open circuit, a series resistance), and
+    `zimt_ion_currents` with several regions of a species. `ions` is accepted for the
+    reference's signature: the ions are unknowns of every step here, which leaves devices
+    without mobile ions as they are."""
+    if recycle is not None:
+        raise NotImplementedError("photon recycling in transients: not built")
     if vint:
         raise NotImplementedError("the internal voltage as an unknown: not built")
     if ion_flux not in ("electrochemical", "modified-drift"):
@@ -241,7 +367,7 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
         raise NotImplementedError("ZimT's last-region ion currents with several regions")
     del ions
     work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
-                zimt_current=zimt_current)
+                zimt_current=zimt_current, profiles=profiles, initial=initial)
     o, _ = work.run()
     return result(work, o)
 
@@ -268,11 +394,14 @@ def result(work: Work, o) -> TransientResult:
     fi = o["f_iface"].cpu().numpy()[:, lanes]
     t = work.t
     n = len(devs)
-    # the last kept step of each device, its time and 1/Δt (Δt from the step kept before it)
+    init = work.initial
+    # the last kept step of each device, its time and 1/Δt (Δt from the step kept before it);
+    # from a given state its time and 1/Δt until a step is kept
     last = np.full(n, -1)
-    kept_t, kept_dti = np.zeros(n), np.zeros(n)
+    kept_t = np.zeros(n) if init is None else init["t"].copy()
+    kept_dti = np.zeros(n) if init is None else init["dti"].copy()
     for k in range(n):
-        prev = 0.0
+        prev = kept_t[k]
         for s in range(t.shape[1]):
             if acc[k, s]:
                 tk = t[k, s]
@@ -281,6 +410,32 @@ def result(work: Work, o) -> TransientResult:
                 last[k] = s
         kept_t[k] = prev
     rows = np.arange(n)
+    fields = _states(devs, state, fb, fi)
+    at = np.maximum(last, 0)
+    V0 = V_int[:, 0] if init is None else init["V_int"]
+    J0 = np.full(n, np.nan) if init is None else init["J_ext"]
+    final = TransientState(
+        t=kept_t, **fields, V_int=np.where(last >= 0, V_int[rows, at], V0),
+        J_ext=np.where(last >= 0, J_ext[rows, at], J0), dti=kept_dti)
+    profiles = None
+    if "prof_state" in o:
+        ps = o["prof_state"].cpu().numpy()[..., lanes]  # steps × nodes × 5 × devices
+        pfb = o["prof_f_bulk"].cpu().numpy()[..., lanes]
+        pfi = o["prof_f_iface"].cpu().numpy()[..., lanes]
+        steps = [_states(devs, ps[s], pfb[s], pfi[s]) for s in range(t.shape[1])]
+        profiles = {name: _stack([np.stack([st[name][k] for st in steps]) for k in range(n)])
+                    for name in steps[0]}
+        profiles["dti"] = o["prof_dti"].cpu().numpy()[:, lanes].T
+    return TransientResult(J=J, J_ext=J_ext, V_int=V_int, V_ext=V_ext, converged=ok,
+                           iterations=its, accepted=acc, stop=stop, t=t, final=final, columns={},
+                           profiles=profiles)
+
+
+def _states(devs, state, fb, fi) -> dict:
+    """`TransientState`'s arrays from the kernel's (state nodes × 5 × devices, the traps'
+    occupations nodes × devices): the densities from their logarithms, the ions where they are
+    mobile, the bulk traps' occupations on the interior points, the interface traps' on the
+    intervals."""
     Vs, ns, ps, As, Cs, fbs, fis = [], [], [], [], [], [], []
     for k, d in enumerate(devs):
         m = len(d.x)
@@ -294,22 +449,8 @@ def result(work: Work, o) -> TransientResult:
         Cs.append(np.where(cm, np.exp(st[:, 4]), 0.0))
         fbs.append(fb[1:m - 1, k])
         fis.append(fi[:m - 1, k])
-
-    def stack(xs):
-        if len({len(x) for x in xs}) == 1:
-            return np.stack(xs)
-        out = np.empty(len(xs), dtype=object)
-        out[:] = xs
-        return out
-
-    at = np.maximum(last, 0)
-    final = TransientState(
-        t=kept_t, V=stack(Vs), n=stack(ns), p=stack(ps), anion=stack(As), cation=stack(Cs),
-        V_int=np.where(last >= 0, V_int[rows, at], V_int[:, 0]),
-        J_ext=np.where(last >= 0, J_ext[rows, at], np.nan), dti=kept_dti, f_bulk=stack(fbs),
-        f_interface=stack(fis))
-    return TransientResult(J=J, J_ext=J_ext, V_int=V_int, V_ext=V_ext, converged=ok,
-                           iterations=its, accepted=acc, stop=stop, t=t, final=final, columns={})
+    return {"V": _stack(Vs), "n": _stack(ns), "p": _stack(ps), "anion": _stack(As),
+            "cation": _stack(Cs), "f_bulk": _stack(fbs), "f_interface": _stack(fis)}
 
 
 @dataclass(frozen=True)

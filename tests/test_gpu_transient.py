@@ -178,3 +178,94 @@ def test_uneven_devices_and_their_own_steps_in_one_launch():
         scale = np.max(np.abs(alone.J[0]))
         assert np.max(np.abs(r.J[k] - alone.J[0])) < 1e-12 * scale
         np.testing.assert_allclose(r.final.V[k], alone.final.V[0], rtol=0, atol=1e-12)
+
+
+def _part(tvg, part):
+    """The steps `part` (a slice) of `tvg`."""
+    import dataclasses
+    return dataclasses.replace(tvg, **{k: getattr(tvg, k)[part]
+                                       for k in ("t", "Vext", "oc", "G_frac", "track", "dti")})
+
+
+def _split_case(case):
+    """A device and its steps: two of ZimT's cases (mobile ions through a sweep and back; bulk
+    traps with light on and off), and the p-i-n cell with interface traps through a sweep."""
+    if case in ZIMT:
+        setup, tvg, _ = zimt_case(case)
+        return build_device(setup, grid="simss"), tvg, dict(bernoulli_name="simss",
+                                                            zimt_current=True)
+    from jaxdd_b200.simss_input import setup_from_texts
+    from jaxdd_b200.workloads import pin_texts
+    t = pin_texts(60)
+    for name in ("L1.txt", "L2.txt"):
+        t[name] = t[name].replace("N_t_int = 0", "N_t_int = 1e15")
+    times = np.concatenate([[0.0], np.logspace(-9, -4, 50)])
+    V = np.concatenate([[0.0], np.linspace(0.0, 0.9, 25), np.linspace(0.9, 0.0, 25)])
+    return build_device(setup_from_texts(t)), TVG.steps(times, V), {}
+
+
+@pytest.fixture(scope="module", params=["zimt_ions_fast_light", "zimt_traps_photo_light",
+                                        "interface"])
+def unsplit(request):
+    dev, tvg, kw = _split_case(request.param)
+    batch = prepare([dev])
+    return request.param, dev, batch, tvg, kw, solve_transient(batch, tvg, profiles=True, **kw)
+
+
+def test_a_transient_split_at_a_step_goes_on_as_the_unsplit_one(unsplit):
+    """jaxdd tests/test_transient_state.py:41-70 on the GPU: split at its middle step and
+    continued from the first half's last state (`final`) or from that step's state in the
+    unsplit run's profiles (`state(k)`), a transient gives the unsplit one's currents to 1e-9
+    of their scale, its densities and ions to 1e-6 and its potential to 1e-9 V; the last state
+    kept is the last step's."""
+    case, dev, batch, tvg, kw, full = unsplit
+    assert full.converged.all() and full.accepted.all()
+    k = len(tvg.t) // 2
+    first = solve_transient(batch, _part(tvg, slice(0, k + 1)), **kw)
+    rest = _part(tvg, slice(k + 1, None))
+    scale = np.max(np.abs(full.J_ext))
+    for start in (first.final, full.state(k)):
+        r = solve_transient(batch, rest, initial=start, profiles=True, **kw)
+        assert r.converged.all(), case
+        np.testing.assert_allclose(r.J_ext[0], full.J_ext[0, k + 1:], rtol=0, atol=1e-9 * scale)
+        for name in ("n", "p", "anion", "cation"):
+            np.testing.assert_allclose(r.profiles[name][0], full.profiles[name][0, k + 1:],
+                                       rtol=1e-6, err_msg=f"{case}: {name}")
+        np.testing.assert_allclose(r.profiles["V"][0], full.profiles["V"][0, k + 1:], rtol=0,
+                                   atol=1e-9)
+        np.testing.assert_array_equal(r.t[0], tvg.t[k + 1:])
+    last = full.state(-1)
+    for name in ("V", "n", "p", "anion", "cation", "f_bulk", "f_interface", "V_int", "dti", "t"):
+        np.testing.assert_allclose(getattr(full.final, name), getattr(last, name), rtol=1e-12,
+                                   atol=1e-15, err_msg=name)
+    # the traps carry their occupations across the split
+    if case != "zimt_ions_fast_light":
+        occ = "f_interface" if case == "interface" else "f_bulk"
+        assert np.any(full.profiles[occ][0] != 0)
+        r = solve_transient(batch, rest, initial=full.state(k), profiles=True, **kw)
+        np.testing.assert_allclose(r.profiles[occ][0], full.profiles[occ][0, k + 1:],
+                                   rtol=1e-6, atol=1e-12)
+
+
+def test_the_profiles_ions_hold_each_species_total(unsplit):
+    """At every step the profiles' ions (0 outside their regions) count each region's total,
+    trapezoidal as the solver counts them, to 1e-9."""
+    case, dev, _, _, _, full = unsplit
+    for name, mask, total in (("anion", dev.anion_mask, dev.anion_total),
+                              ("cation", dev.cation_mask, dev.cation_total)):
+        dens = full.profiles[name][0]
+        if mask is None or not total:
+            assert not dens.any(), case
+            continue
+        m = np.asarray(mask, bool)
+        assert np.all(dens[:, ~m] == 0), case
+        for step in dens:
+            assert abs(_number(step, m, dev) / total - 1) < 1e-9, case
+
+
+def test_a_step_state_needs_the_profiles():
+    setup, tvg, _ = zimt_case("zimt_photo_light")
+    r = solve_transient(prepare([build_device(setup, grid="simss")]), _part(tvg, slice(0, 3)),
+                        bernoulli_name="simss")
+    with pytest.raises(ValueError, match="profiles=True"):
+        r.state(1)

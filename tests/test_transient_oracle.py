@@ -123,3 +123,33 @@ def test_what_the_transient_refuses():
     b["R_series"] = np.array([1e-4])
     with pytest.raises(NotImplementedError, match="series resistance"):
         transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3])
+
+
+def test_a_given_state_is_checked_before_any_solve():
+    """`solve_transient(..., initial=)` refuses, before it touches a GPU, what jaxdd refuses
+    (tests/test_transient_state.py:93-114): a first time not after the state's, a state of
+    another grid, densities that are not positive."""
+    import dataclasses
+
+    from jaxdd_b200.batch import prepare
+    from jaxdd_b200.transient import TransientState, solve_transient
+    setup, tvg, _ = zimt_case("zimt_photo_light")
+    dev = build_device(setup, grid="simss")
+    batch = prepare([dev])
+    ones = np.ones((1, len(dev.x)))
+    good = TransientState(t=np.array([0.0]), V=0 * ones, n=1e10 * ones, p=1e10 * ones,
+                          anion=0 * ones, cation=0 * ones, V_int=np.zeros(1), J_ext=np.zeros(1),
+                          dti=np.zeros(1), f_bulk=np.zeros((1, len(dev.x) - 2)),
+                          f_interface=np.zeros(1))
+    later = dataclasses.replace(tvg, **{k: getattr(tvg, k)[1:]
+                                        for k in ("t", "Vext", "oc", "G_frac", "track", "dti")})
+    with pytest.raises(ValueError, match="starts after it"):
+        solve_transient(batch, later, initial=dataclasses.replace(good, t=np.array([1.0])))
+    with pytest.raises(ValueError, match=r"initial\.n"):
+        solve_transient(batch, later, initial=dataclasses.replace(good, n=np.ones((1, 3))))
+    with pytest.raises(ValueError, match="positive"):
+        solve_transient(batch, later, initial=dataclasses.replace(good, p=0 * ones))
+    with pytest.raises(ValueError, match=r"initial\.V_int"):
+        solve_transient(batch, later, initial=dataclasses.replace(good, V_int=np.zeros(2)))
+    with pytest.raises(ValueError, match=r"initial\.f_bulk"):
+        solve_transient(batch, later, initial=dataclasses.replace(good, f_bulk=np.zeros((1, 4))))
