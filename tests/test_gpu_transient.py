@@ -42,6 +42,21 @@ def test_zimt_transients_match_the_oracle_and_zimt(case):
     assert np.mean(r.iterations[0] == o["iterations"][0]) > 0.95
 
 
+def test_zimt_transients_in_one_batch_each_with_its_own_steps():
+    """jaxdd test_solver.py:719-737 on the GPU: ZimT's transients of 241 steps as one batch, each
+    device with its own steps (the integral current beside the differential one, bulk traps,
+    charged interface traps, mobile ions): each within its bar of ZimT's `Jext`."""
+    cases = sorted(c for c in ZIMT if c != "zimt_steady_light")
+    runs = [zimt_case(c) for c in cases]
+    batch = prepare([build_device(setup, grid="simss") for setup, _, _ in runs])
+    r = solve_transient(batch, [tvg for _, tvg, _ in runs], bernoulli_name="simss",
+                        zimt_current=True)
+    assert r.converged.all() and r.accepted.all()
+    for k, (case, (_, _, ref)) in enumerate(zip(cases, runs)):
+        scale = np.max(np.abs(ref["Jext"]))
+        assert np.max(np.abs(r.J_ext[k] - ref["Jext"])) < ZIMT[case] * scale, case
+
+
 def test_config5_transient_matches_the_oracle():
     devs = [drawn_device(k) for k in (1, 3, 5)]
     tvg = transient_steps(40)

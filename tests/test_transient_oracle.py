@@ -1,7 +1,10 @@
 """The transient oracle pinned on ZimT 5.36's own transients (the reference's tests/data, copied
 to tests/golden/inputs): `Jext` through 241 steps to the reference's tolerances
 (test_solver.py:544-581: 1e-9 of the scale for electrons and holes and for the traps, 1e-7 with
-mobile ions), ZimT's Bernoulli function and sums (`zimt_current`). Also: the tVG reader's checks,
+mobile ions), ZimT's Bernoulli function and sums (`zimt_current`): light on and off, a sweep to
+1.2 V and back in 2 x 100 ns in the integral and the differential current, the absorber's traps,
+charged interface traps through the sweep, mobile ions over 2 x 50 ms and 2 x 5 s, and steady
+states at t = 0 (test_solver.py:454-470). Also: the tVG reader's checks,
 the traps' step against its closed form and its derivatives, the ions' number kept in every step,
 and the refusals of what is out of scope."""
 
@@ -15,7 +18,9 @@ from oracle import dd, transient
 INPUTS = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "inputs"
 
 ZIMT = {"zimt_photo_light": 1e-9, "zimt_traps_photo_light": 1e-9,
-        "zimt_ions_fast_light": 1e-7, "zimt_ions_slow_light": 1e-7}
+        "zimt_ions_fast_light": 1e-7, "zimt_ions_slow_light": 1e-7,
+        "zimt_sweep_light": 1e-9, "zimt_sweep_diff_light": 1e-9,
+        "zimt_iface_sweep_light": 1e-9, "zimt_steady_light": 1e-9}
 
 
 def zimt_case(case):
