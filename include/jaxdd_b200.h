@@ -256,6 +256,8 @@ typedef struct dd_steps {
   const int32_t* failure_mode; /* [lane_stride]: 0 stop at a failed step, 1 keep it, 2 skip it */
   int32_t zimt_sums;           /* 1: ZimT's sums in the integral current (each point's change over
                                   the interval after it); 0: over its control volume (jaxdd's) */
+  int32_t zimt_ion_last;       /* 1: each species' last ion region's current alone, as ZimT 5.36
+                                  has it with several regions; 0: every region's (jaxdd's) */
 } dd_steps;
 
 /* Outputs of dd_transient (device pointers). Per step and lane [n_steps][lane_stride]: J (A/m^2,

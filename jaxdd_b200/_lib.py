@@ -79,7 +79,8 @@ class DdStructure(ctypes.Structure):
 class DdSteps(ctypes.Structure):
     _fields_ = [("n_steps", ctypes.c_int32), ("stride", ctypes.c_int32), ("t", ctypes.c_void_p),
                 ("v", ctypes.c_void_p), ("g_frac", ctypes.c_void_p), ("track", ctypes.c_void_p),
-                ("failure_mode", ctypes.c_void_p), ("zimt_sums", ctypes.c_int32)]
+                ("failure_mode", ctypes.c_void_p), ("zimt_sums", ctypes.c_int32),
+                ("zimt_ion_last", ctypes.c_int32)]
 
 
 class DdTransientOut(ctypes.Structure):

@@ -32,6 +32,7 @@ struct View {
   double* Yb;
   size_t ybuf;
   int simss, zimt;
+  int ion_last = 0;  // each species' last ion region's current alone (ZimT 5.36's)
   const double* BD;  // the step's state before it as densities [np+2][4][Bp] (n, p, a, c), or null
   __device__ __forceinline__ double x(int k, int f) const {
     return __ldg(X + ((size_t)k * DD_NT + f) * L.Bp + L.l);
@@ -61,6 +62,41 @@ __device__ __forceinline__ void load_point(const View& W, int buf, int k, double
   P.c2 = P.c.sl.c >= 0 ? exp(P.lc) : 1.0;
   P.c.da = P.c.sl.a >= 0 ? P.a : 0.0;
   P.c.dc = P.c.sl.c >= 0 ? P.c2 : 0.0;
+}
+
+// A contact's ions where a region reaches it (`_ion_full`, solver.py:1315-1346): from its
+// neighbour in buffer `buf`, so that nothing flows over the contact's interval,
+// ln a_0 = ln a_1 + ln(B(x)/B(-x)) with x = (V_1 - V_0)/V_T (the cations' the other way, the right
+// contact's mirrored), Boltzmann's (the ratio -x) in the steady state dti = 0. `dr`, if given:
+// d ln a / d V of the neighbour (the cations' its negative). A no-op on interior points and
+// where no region reaches the contact.
+__device__ __forceinline__ void contact_ions(const View& W, int buf, int k, double dti, TP& P,
+                                             double* dr = nullptr) {
+  const Lane& L = W.L;
+  if ((k != 0 && k != L.NP + 1) || (P.c.sl.a < 0 && P.c.sl.c < 0)) return;
+  const bool right = k != 0;
+  const int nb = right ? L.NP : 1;
+  const double Vn = *W.y(buf, nb, 0);
+  const double x = (right ? P.c.V - Vn : Vn - P.c.V) * L.iVt;
+  double r = -x, drx = -1.0;
+  if (dti > 0.0) {
+    double Bf, Bb, dBf, dBb;
+    bern_pair(x, W.simss, Bf, Bb, dBf, dBb);
+    r = log(Bf) - log(Bb);
+    drx = dBf / Bf + dBb / Bb;
+  }
+  const double s = right ? -1.0 : 1.0;  // the step from the neighbour, anions
+  if (dr) *dr = drx * L.iVt;  // on either side r'(x) / V_T
+  if (P.c.sl.a >= 0) {
+    P.la = *W.y(buf, nb, 3) + s * r;
+    P.a = exp(P.la);
+    P.c.da = P.a;
+  }
+  if (P.c.sl.c >= 0) {
+    P.lc = *W.y(buf, nb, 4) - s * r;
+    P.c2 = exp(P.lc);
+    P.c.dc = P.c2;
+  }
 }
 
 // ------------------------------------------------------------------------------------ traps

@@ -48,7 +48,7 @@ struct Args {
   const double* y0;     // [np+2][3][Bp]
   const double* logs0;  // [DD_MAXK][Bp]
   double tol;
-  int max_iter, simss, zimt;
+  int max_iter, simss, zimt, ion_last;
   // workspace
   double* Yb;  // [3][np+2][5][Bp]
   double* FB;  // [np+2][Bp]
@@ -136,7 +136,8 @@ struct Pert {
 
 template <int K, bool PERT = false>
 __device__ double current_t(const View& W, int cur, double Vint, int bef, double Vbef, double dti,
-                            const double* FB, const double* FI, const Pert* pt = nullptr) {
+                            double dti_bef, const double* FB, const double* FI,
+                            const Pert* pt = nullptr) {
   const Lane& L = W.L;
   const double mus = PERT ? pt->mus : 1.0;
   auto fb_at = [&](int k) {
@@ -151,6 +152,7 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     if (PERT) load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P);
     else if (is_cur) load_point(W, buf, k, Vi, P);
     else load_before(W, buf, k, Vi, P);
+    contact_ions(W, buf, k, is_cur ? dti : dti_bef, P);
   };
   const int NP = L.NP;
   const double QL = Q * L.L;
@@ -284,6 +286,14 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
   }
   const double H = L.Hsum;
   double tot = 0.0;
+  // ZimT 5.36's ion currents with several regions: each species' last region's alone
+  int last_a = -1, last_c = -1;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (L.tot[k] > 0.0) {
+      if (k < L.ka) last_a = k;
+      else last_c = k;
+    }
   if (!L.currdiff) {
     Pt c0, cN;
     contact(L, 0, Vint, c0);
@@ -305,6 +315,7 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     if (!(L.tot[k] > 0.0) || !have[k]) continue;
+    if (W.ion_last && k != (k < L.ka ? last_a : last_c)) continue;
     const double sn = k < L.ka ? -1.0 : 1.0;
     if (!L.currdiff) {
       const double sgl = is[k] > 0.0 ? is[k] : 1.0;
@@ -347,6 +358,7 @@ __device__ __noinline__ void write_profile(const Args& a, const View& W, int bn,
   for (int i = 0; i <= NP + 1; ++i) {
     TP P;
     load_point(W, bn, i, V_k, P);
+    contact_ions(W, bn, i, dti, P);
     const double v5[5] = {P.c.V, P.c.lnn, P.c.lnp, P.c.sl.a >= 0 ? P.la : 0.0,
                           P.c.sl.c >= 0 ? P.lc : 0.0};
 #pragma unroll
@@ -374,8 +386,8 @@ __device__ __noinline__ void write_profile(const Args& a, const View& W, int bn,
 
 template <int K>
 __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk, double V_k,
-                                          double V_now, double dti, double dt, const double* lg,
-                                          int tb, double* dQ) {
+                                          double V_now, double dti, double dti_now, double dt,
+                                          const double* lg, int tb, double* dQ) {
   const Lane& L = W.L;
   const int NP = L.NP, Bp = a.Bp, l = L.l;
   constexpr int NC = 2 + K;  // the two tangents' right-hand sides, then the K slot columns
@@ -608,10 +620,10 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
       pt.tfi = a.TFI + (size_t)p * nodes * Bp;
       pt.h = TANGENT_H;
       pt.mus = p == 1 ? exp(TANGENT_H) : 1.0;
-      const double Jp = current_t<K, true>(W, bn, V_k, bk, V_now, dti, FB, FI, &pt);
+      const double Jp = current_t<K, true>(W, bn, V_k, bk, V_now, dti, dti_now, FB, FI, &pt);
       pt.h = -TANGENT_H;
       pt.mus = p == 1 ? exp(-TANGENT_H) : 1.0;
-      const double Jm = current_t<K, true>(W, bn, V_k, bk, V_now, dti, FB, FI, &pt);
+      const double Jm = current_t<K, true>(W, bn, V_k, bk, V_now, dti, dti_now, FB, FI, &pt);
       dQ[p] += (Jp - Jm) / (2.0 * TANGENT_H) * dt;
     }
   }
@@ -638,7 +650,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
 #pragma unroll
   for (int k = 0; k < K; ++k) L.tot[k] = k < a.ka + a.kc ? L.sc(C_TOT0 + k) : 0.0;
   W.X = a.X; W.Yb = a.Yb; W.ybuf = (size_t)(a.npmax + 2) * 5 * a.Bp; W.simss = a.simss;
-  W.zimt = a.zimt; W.BD = a.BD;
+  W.zimt = a.zimt; W.BD = a.BD; W.ion_last = a.ion_last;
   const int NP = L.NP, Bp = a.Bp;
   const int ts = a.tstride;
   double* FB = a.FB;
@@ -782,6 +794,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       for (int q = 0; q < K; ++q) gnum[q] = 0.0;
       TP pm, pc, pn;
       load_point(W, bn, 0, V_k, pm);
+      contact_ions(W, bn, 0, dti, pm);
       load_point(W, bn, 1, V_k, pc);
       Flux el, er;
       flux(L, pm.c, pc.c, L.st(0, S_MUN), L.st(0, S_MUP), el);
@@ -792,6 +805,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       ion_ivs(W, 0, pm, pc, ivl);
       for (int i = 1; i <= NP; ++i) {
         load_point(W, bn, i + 1, V_k, pn);
+        contact_ions(W, bn, i + 1, dti, pn);
         flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
         ion_ivs(W, i, pc, pn, ivr);
         const double hm = L.st(i - 1, S_H), hp = L.st(i, S_H);
@@ -857,6 +871,13 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         pc = pn;
         el = er;
       }
+      // the ions' numbers over the last interval, where a region reaches the right contact
+      {
+        const double hL = L.st(NP, S_H) * L.L;
+        if (pc.c.sl.a >= 0 && pc.c.sl.a == pm.c.sl.a) gnum[pc.c.sl.a] += 0.5 * (pm.a + pc.a) * hL;
+        if (pc.c.sl.c >= 0 && pc.c.sl.c == pm.c.sl.c)
+          gnum[L.ka + pc.c.sl.c] += 0.5 * (pm.c2 + pc.c2) * hL;
+      }
       // -------- back substitution with the slots' Schur complement
       double SM[K][K], sr[K];
 #pragma unroll
@@ -902,10 +923,22 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
             if (!(L.tot[q] > 0.0)) continue;
             const int slm = sp == 0 ? s_prev.a : s_prev.c, sln = sp == 0 ? s_next.a : s_next.c;
             const double wpt = 0.5 * ((slm == sl ? hLm : 0.0) + (sln == sl ? hLp : 0.0));
-            const double w = wpt * exp(*W.y(bn, i, 3 + sp)) / L.tot[q];
-            sr[q] -= w * xi[3 + sp][0];
+            double w = wpt * exp(*W.y(bn, i, 3 + sp)) / L.tot[q], wv = 0.0;
+            // a region that reaches a contact: the contact's density follows this point's
+            if ((i == 1 && slm == sl) || (i == NP && sln == sl)) {
+              const int kc = i == 1 ? 0 : NP + 1;
+              TP P;
+              load_point(W, bn, kc, V_k, P);
+              double dr;
+              contact_ions(W, bn, kc, dti, P, &dr);
+              const double wc = 0.5 * (i == 1 ? hLm : hLp) * (sp == 0 ? P.a : P.c2) / L.tot[q];
+              w += wc;
+              wv = wc * (sp == 0 ? dr : -dr);
+            }
+            sr[q] -= w * xi[3 + sp][0] + wv * xi[0][0];
 #pragma unroll
-            for (int q2 = 0; q2 < K; ++q2) SM[q][q2] -= w * xi[3 + sp][1 + q2];
+            for (int q2 = 0; q2 < K; ++q2)
+              SM[q][q2] -= w * xi[3 + sp][1 + q2] + wv * xi[0][1 + q2];
           }
           s_next = s_here;
           s_here = s_prev;
@@ -961,7 +994,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
 #pragma unroll
       for (int q = 0; q < K; ++q) finite = finite && isfinite(lg[q]);
       // -------- the current at the new iterate and the stops
-      const double J = current_t<K>(W, bn, V_k, bk, V_now, dti, FB, FI);
+      const double J = current_t<K>(W, bn, V_k, bk, V_now, dti, dti_now, FB, FI);
 #pragma unroll
       for (int q = 0; q < STALL_STEPS; ++q) { sh[q] = sh[q + 1]; jh[q] = jh[q + 1]; }
       sh[STALL_STEPS] = size;
@@ -993,7 +1026,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       // the tangents of this step, before the occupations move on (they take the old ones)
       const double dt = dti > 0.0 ? t_k - t_last : 0.0;
       Qint += J * dt;
-      if (grad) tangent_step<K>(a, W, bn, bk, V_k, V_now, dti, dt, lg, tb, dQ);
+      if (grad) tangent_step<K>(a, W, bn, bk, V_k, V_now, dti, dti_now, dt, lg, tb, dQ);
       // the traps' occupations at the step's end, from its solution (and their tangents)
       auto tyn = [&](int p, int k, int c) {
         return (k < 1 || k > NP) ? 0.0
@@ -1069,6 +1102,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   for (int i = 0; i <= NP + 1; ++i) {
     TP p;
     load_point(W, bk, i, V_now, p);
+    contact_ions(W, bk, i, dti_now, p);
     const double v5[5] = {p.c.V, p.c.lnn, p.c.lnp, p.la, p.lc};
 #pragma unroll
     for (int c = 0; c < 5; ++c) a.state_out[((size_t)i * 5 + c) * Bp + l] = v5[c];
@@ -1162,6 +1196,7 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.tol = opts->tol; a.max_iter = opts->max_iter;
   a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS;
   a.zimt = steps->zimt_sums != 0;
+  a.ion_last = steps->zimt_ion_last != 0;
   a.Yb = reinterpret_cast<double*>(w);
   a.FB = reinterpret_cast<double*>(w + y);
   a.FI = reinterpret_cast<double*>(w + y + fb);

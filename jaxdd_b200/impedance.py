@@ -118,8 +118,8 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
     (Hz), from the steady state there by one complex linear solve per frequency (jaxdd
     impedance.py:365-409). Free mobile ions move with the voltage as unknowns of their own.
     Refused (`NotImplementedError`), as the reference refuses them or as this build does not
-    carry them: ions frozen at a pre-bias, several ion regions of a species, the differential
-    current (`currDiffInt = 1`). `dt` (s): instead of the continuous response, what
+    carry them: ions frozen at a pre-bias, several ion regions of a species, an ion region that
+    reaches a contact, the differential current (`currDiffInt = 1`). `dt` (s): instead of the continuous response, what
     `solve_transient` sees through implicit Euler at steps of `dt` (its time terms at
     `(1 − e^(−iω dt))/dt`, the traps' occupations over each step as it solves them)."""
     devs = batch["devices"]
@@ -127,6 +127,9 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
         raise NotImplementedError("impedance with ions frozen at a pre-bias")
     if batch["ka"] != 1 or batch["kc"] != 1:
         raise NotImplementedError("impedance with several ion regions of a species")
+    from .transient import reaches_contact
+    if _mobile(batch) and any(reaches_contact(d) for d in devs):
+        raise NotImplementedError("impedance with an ion region that reaches a contact")
     if any(d.curr_diff for d in devs):
         raise NotImplementedError("impedance with the differential current (currDiffInt = 1)")
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))

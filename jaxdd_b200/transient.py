@@ -13,8 +13,7 @@ with `initial=` (a `TransientState`) the devices start from that state instead o
 
 The voltage is given at every step. Refused (`NotImplementedError`), not approximated: an open
 circuit or a series resistance (the internal voltage an unknown), `Track` 2 or 3 (ZimT's
-automatic stop), photon recycling, ion regions that reach a contact, ZimT's last-region ion
-currents with several regions of a species.
+automatic stop), photon recycling.
 """
 
 from __future__ import annotations
@@ -175,16 +174,16 @@ def _steps(tvgs: list[TVG]):
     return t, V, G, track.astype(np.int32), fm
 
 
+def reaches_contact(d) -> bool:
+    """Whether a region of mobile ions of device `d` reaches a contact."""
+    return any(m is not None and bool(m[0] or m[-1]) for m in (d.anion_mask, d.cation_mask))
+
+
 def _check_batch(batch: Batch) -> None:
     devs = batch["devices"]
     if any(d.R_series > 0 for d in devs):
         raise NotImplementedError("transient with a series resistance (the internal voltage an "
                                   "unknown): not built")
-    for d in devs:
-        for mask in (d.anion_mask, d.cation_mask):
-            if mask is not None and (mask[0] or mask[-1]):
-                raise NotImplementedError("mobile ions in a region that reaches a contact: not "
-                                          "built")
 
 
 class Work:
@@ -195,11 +194,15 @@ class Work:
 
     def __init__(self, batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
                  bernoulli_name: str = "exact", zimt_current: bool = False,
-                 gradients: bool = False, profiles: bool = False, initial=None):
+                 gradients: bool = False, profiles: bool = False, initial=None,
+                 zimt_ion_currents: bool = False):
         import torch
         from .adjoint import plan as _plan
         _check_batch(batch)
         devs = batch["devices"]
+        if gradients and any(reaches_contact(d) for d in devs):
+            raise NotImplementedError("the transient's gradients with an ion region that reaches "
+                                      "a contact: not built")
         tvgs = list(tvg) if isinstance(tvg, (list, tuple)) else [tvg] * len(devs)
         if len(tvgs) != len(devs):
             raise ValueError("one tVG for the batch, or one per device, all of one length")
@@ -255,6 +258,7 @@ class Work:
         fml[lanes] = fm
         self.fm = torch.from_numpy(fml).to(cuda)
         self.zimt = int(bool(zimt_current))
+        self.ion_last = int(bool(zimt_ion_currents))
         f64, u8, i32 = torch.float64, torch.uint8, torch.int32
         self.out = {
             "J": torch.empty((S, Bp), dtype=f64, device=cuda),
@@ -322,7 +326,7 @@ class Work:
                 "state", "f_bulk", "f_iface", "scalars"))))
         steps = _lib.DdSteps(self.S, self.stride, self.tv.data_ptr(), self.vv.data_ptr(),
                              self.gv.data_ptr(), self.trk.data_ptr(), self.fm.data_ptr(),
-                             self.zimt)
+                             self.zimt, self.ion_last)
         o = self.out
         out = _lib.DdTransientOut(*(o[k].data_ptr() if k in o else None for k in (
             "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",
@@ -352,9 +356,12 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
     state (`TransientResult.profiles`, `state(k)`). `initial` (a `TransientState`, e.g. a
     result's `final` or `state(k)`): every device starts from it instead of from a steady state,
     its slots' scales 1 and the first step's guess the state itself (no extrapolation), checked
-    as jaxdd checks it (`ValueError`). Not built (raise `NotImplementedError`): `recycle`, an
-    internal voltage as an unknown (`vint`, an open circuit, a series resistance), and
-    `zimt_ion_currents` with several regions of a species. `ions` is accepted for the
+    as jaxdd checks it (`ValueError`). `zimt_ion_currents`: with several ion regions of a
+    species each species' last region's current alone, as ZimT 5.36 has it; by default every
+    region's. An ion region that reaches a contact takes the contact's density from its
+    neighbour, nothing flowing over the contact's interval (jaxdd's `_ion_full`). Not built
+    (raise `NotImplementedError`): `recycle`, an internal voltage as an unknown (`vint`, an open
+    circuit, a series resistance). `ions` is accepted for the
     reference's signature: the ions are unknowns of every step here, which leaves devices
     without mobile ions as they are."""
     if recycle is not None:
@@ -363,11 +370,10 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
         raise NotImplementedError("the internal voltage as an unknown: not built")
     if ion_flux not in ("electrochemical", "modified-drift"):
         raise ValueError(f"ion_flux {ion_flux!r}: one of ('electrochemical', 'modified-drift')")
-    if zimt_ion_currents and (batch["ka"] > 1 or batch["kc"] > 1):
-        raise NotImplementedError("ZimT's last-region ion currents with several regions")
     del ions
     work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
-                zimt_current=zimt_current, profiles=profiles, initial=initial)
+                zimt_current=zimt_current, profiles=profiles, initial=initial,
+                zimt_ion_currents=zimt_ion_currents)
     o, _ = work.run()
     return result(work, o)
 

@@ -362,6 +362,9 @@ def solve_impedance(devices, frequencies, voltage=0.0, tol=1e-10, max_iter=60,
         ions = np.any(d["ion"]["a_totals"] > 0) or np.any(d["ion"]["c_totals"] > 0)
         if ions and dev.pre_cond and dev.fix_ions:
             raise NotImplementedError("impedance with ions frozen at a pre-bias")
+        masks, _ = dd._masks(d["ion"])
+        if ions and (np.any(masks[:, :, 0] > 0) or np.any(masks[:, :, -1] > 0)):
+            raise NotImplementedError("impedance with an ion region that reaches a contact")
         st = dd.solve_states(d, [float(voltage)], tol=tol, max_iter=max_iter,
                              bernoulli_name=bernoulli_name)
         full0 = np.stack([st["V"][0, 0], np.log(st["n"][0, 0]), np.log(st["p"][0, 0])], -1)

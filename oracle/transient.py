@@ -13,8 +13,8 @@ product imports it.
 
 Scope (the rest is refused, never approximated): the voltage given at every step (no open
 circuit, no series resistance), `Track` 0 or 1 (no automatic stop on equal states), no photon
-recycling, no free ends, no ion sites, ion regions inside the device (not reaching a contact),
-the steady scope of `oracle.dd` otherwise. With no mobile ions the same 5-column system holds
+recycling, no free ends, no ion sites, the steady scope of `oracle.dd` otherwise. An ion region
+that reaches a contact takes the contact's density from its neighbour (`ion_full`). With no mobile ions the same 5-column system holds
 the ions' rows at 0 (identity rows); the solution is the reference's 3-column one.
 
 Derivatives that the reference takes by `jax.jvp` (the ions' rows, the traps over a step) are
@@ -320,10 +320,12 @@ def assemble(full, d, tr, logs, bern, steady_traps=False, mass=False):
     return F, A, Bb, C, U
 
 
-def constraints(full, logs, ion):
+def constraints(full, logs, ion, dV=None):
     """solver._ion_constraints_time (solver.py:1349-1361): each slot's number of ions over its
-    total, less 1, from the ions' own densities; with its derivatives `W` (B×K×NP×5, in each
-    interior point's ion logarithm) and the held slots' identity rows. Returns `(g, W, D)`."""
+    total, less 1, from the ions' own densities (the contacts' from `ion_full`); with its
+    derivatives `W` (B×K×NP×5, in each interior point's ion logarithm, and where a region
+    reaches a contact in its neighbour's potential through the contact's density, `dV` from
+    `ion_full`) and the held slots' identity rows. Returns `(g, W, D)`."""
     masks, totals = dd._masks(ion)
     ka = ion["a_slots"].shape[1]
     nb, K, npts = masks.shape
@@ -340,6 +342,13 @@ def constraints(full, logs, ion):
     for k in range(K):
         W[:, k, :, col[k]] = np.where(has[:, k, None], wpt[:, k] * dens[:, k, 1:-1] / tot[:, k, None],
                                       0.0)
+        if dV is None:
+            continue
+        # a contact's density follows its neighbour's ln density and potential
+        for side, (c_pt, n_pt, iv) in enumerate(((0, 0, 0), (-1, -1, -1))):
+            w = np.where(has[:, k], 0.5 * pair[:, k, iv] * dens[:, k, c_pt] / tot[:, k], 0.0)
+            W[:, k, n_pt, col[k]] += w
+            W[:, k, n_pt, 0] += w * dV[:, side, col[k] - 3]
     D = np.zeros((nb, K, K))
     D[:, np.arange(K), np.arange(K)] = held
     return g, W, D
@@ -478,7 +487,8 @@ def current(d, full, tr, bern, zimt, steady_traps=False, dU=None, dRi=None):
 def ion_currents(d, full, tr, bern, width):
     """batch._ion_currents (batch.py:421-483): each region's current over the step from its
     integral form with the densities' change as the integrand; 0 outside, every region's
-    counted. The anions' and cations' summed, on the NP + 1 intervals."""
+    counted, or with `tr["ion_last"]` (B, true) each species' last region's alone (ZimT 5.36's
+    with several regions). The anions' and cations' summed, on the NP + 1 intervals."""
     ion = d["ion"]
     Vt, x, h, L = _col(d["Vt"]), d["x"], d["h"], _col(d["L"])
     V = full[..., 0]
@@ -490,6 +500,10 @@ def ion_currents(d, full, tr, bern, width):
     ka = ion["a_slots"].shape[1]
     out = np.zeros((nb, NP + 1))
     e = np.arange(NP + 1)
+    idx = np.arange(masks.shape[1])[None]
+    last_a = np.max(np.where((totals > 0) & (idx < ka), idx, -1), 1)
+    last_c = np.max(np.where((totals > 0) & (idx >= ka), idx, -1), 1)
+    only_last = np.asarray(tr.get("ion_last", np.zeros(nb, bool)), bool)
     for k in range(masks.shape[1]):
         anion = k < ka
         sn = -1.0 if anion else 1.0
@@ -524,7 +538,7 @@ def ion_currents(d, full, tr, bern, width):
                 L * h[:, :NP + 1])
             J = np.where(diff[:, None], flux, J)
         J = np.where(d["iface"], np.roll(J, 1, axis=1), J)
-        counted = totals[:, k] > 0
+        counted = (totals[:, k] > 0) & (~only_last | (k == (last_a if anion else last_c)))
         out = out + np.where((pair > 0) & counted[:, None], J, 0.0)
     return out
 
@@ -536,20 +550,52 @@ def _caps(Vt):
                     -1)[:, None, :]
 
 
-def full_of(d, y, Vint):
+def full_of(d, y, Vint, bern=None, dti=None):
     """`y` (B×NP×5) with the contacts' rows (batch._full, batch.py:262-267); the contacts' ions
-    0 (the regions do not reach them)."""
+    0, or with `bern` and `dti` (B) each region's that reaches a contact (`ion_full`)."""
     bnd = dd.bounds(d, Vint)
     b = np.concatenate([bnd, np.zeros(bnd.shape[:2] + (2,))], -1)
-    return np.concatenate([b[:, :1], y, b[:, 1:]], 1)
+    full = np.concatenate([b[:, :1], y, b[:, 1:]], 1)
+    return full if bern is None else ion_full(d, full, bern, dti)[0]
+
+
+def ion_full(d, full, bern, dti):
+    """solver._ion_full (solver.py:1315-1346) without ion sites or free ends: each contact's
+    ions where a region reaches it, from its neighbour so that nothing flows over the contact's
+    interval (`ln a_0 = ln a_1 + ln(B(x)/B(-x))`, x = (V_1 - V_0)/V_T, the cations' the other
+    way; Boltzmann's, the ratio -x, in the steady state `dti = 0`), 0 elsewhere. Returns the
+    full state and each contact's ln a, ln c derivative in its neighbour's potential
+    (B×2×2: left, right × anion, cation)."""
+    ion = d["ion"]
+    Vt = d["Vt"]
+    ma, mc = ion["a_slots"].sum(1), ion["c_slots"].sum(1)
+    V = full[..., 0]
+    moving = np.asarray(dti, dtype=float) > 0
+
+    def ratio(x):
+        Bf, dBf = bern(x)
+        Bb, dBb = bern(-x)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return (np.where(moving, np.log(Bf) - np.log(Bb), -x),
+                    np.where(moving, dBf / Bf + dBb / Bb, -1.0))
+
+    r0, dr0 = ratio((V[:, 1] - V[:, 0]) / Vt)
+    rN, drN = ratio((V[:, -1] - V[:, -2]) / Vt)
+    out = full.copy()
+    out[:, 0, 3] = np.where(ma[:, 0] > 0, full[:, 1, 3] + r0, 0.0)
+    out[:, 0, 4] = np.where(mc[:, 0] > 0, full[:, 1, 4] - r0, 0.0)
+    out[:, -1, 3] = np.where(ma[:, -1] > 0, full[:, -2, 3] - rN, 0.0)
+    out[:, -1, 4] = np.where(mc[:, -1] > 0, full[:, -2, 4] + rN, 0.0)
+    dV = np.stack([np.stack([dr0, -dr0], -1), np.stack([drN, -drN], -1)], 1) / Vt[:, None, None]
+    return out, dV
 
 
 def newton_step(y, logs, d, Vint, tr, bern):
     """One damped Newton step of a time step (batch.py:759-785 with `_system`'s 5-column form,
     518-530)."""
-    full = full_of(d, y, Vint)
+    full, dV = ion_full(d, full_of(d, y, Vint), bern, tr["dti"])
     F, A, Bb, C, U = assemble(full, d, tr, logs, bern)
-    g, W, D = constraints(full, logs, d["ion"])
+    g, W, D = constraints(full, logs, d["ion"], dV)
     delta, d_logs = bordered_solve(A, Bb, C, U, W, D, -F, -g)
     caps = _caps(d["Vt"])
     stepv = dd.density_steps(y, delta, np.clip(delta, -caps, caps), d["s"]["n_floor"])
@@ -586,7 +632,8 @@ def newton_loop(y, logs, d, Vint, tr, trc, bern, tol, max_iter, zimt):
         dl = dd.take(d, idx)
         new, logs_new, size = newton_step(y[idx], logs[idx], dl, Vint[idx], _take_tr(tr, idx),
                                           bern)
-        J = current(dl, full_of(dl, new, Vint[idx]), _take_tr(trc, idx), bern, zimt)
+        J = current(dl, full_of(dl, new, Vint[idx], bern, trc["dti"][idx]), _take_tr(trc, idx),
+                    bern, zimt)
         sh = np.concatenate([size_h[idx, 1:], size[:, None]], 1)
         jh = np.concatenate([J_h[idx, 1:], J[:, None]], 1)
         n_it = it[idx] + 1
@@ -617,17 +664,16 @@ def check_scope(d, oc=None, track=None):
                                   "unknown)")
     if track is not None and np.any(np.asarray(track) > 1):
         raise NotImplementedError("Track 2 or 3 (ZimT's automatic stop on equal states)")
-    masks, _ = dd._masks(d["ion"])
-    if np.any(masks[:, :, 0] > 0) or np.any(masks[:, :, -1] > 0):
-        raise NotImplementedError("mobile ions in a region that reaches a contact")
 
 
 def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, max_iter=200,
-                    bernoulli_name="exact", zimt_current=False):
+                    bernoulli_name="exact", zimt_current=False, zimt_ion_currents=False):
     """transient.solve_transient / _solve_one (transient.py:270-465, 537-637) for every lane at
     once. `t`, `V`, `G_frac`, `track`: (S,) for every device or (B, S); `failure_mode` scalar
-    or (B,). Returns a dict: `J`, `J_ext`, `converged`, `iterations`, `accepted` (B×S), `stop`
-    (B), and the final state (`y` B×NP×5, `logs`, `f_bulk`, `f_interface`)."""
+    or (B,). `zimt_ion_currents`: each species' last region's ion current alone, as ZimT 5.36
+    has it with several regions. Returns a dict: `J`, `J_ext`, `converged`, `iterations`,
+    `accepted` (B×S), `stop` (B), and the final state (`y` B×NP×5, `logs`, `f_bulk`,
+    `f_interface`)."""
     d = batch
     nb = d["Vt"].shape[0]
     S = np.shape(t)[-1]
@@ -671,13 +717,14 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     for k in range(S):
         t_k, V_k, G_k = t[:, k], V[:, k], G_frac[:, k]
         dti_k = np.where(t_k == 0, 0.0, 1.0 / np.where(t_k > t_last, t_k - t_last, 1.0))
-        before = full_of(d, y, V_now)
+        before = full_of(d, y, V_now, bern, dti_now)
         tr = {"dti": dti_k, "n": np.exp(before[:, 1:-1, 1]), "p": np.exp(before[:, 1:-1, 2]),
               "a": np.exp(before[:, 1:-1, 3]) * s["a_mask"],
               "c": np.exp(before[:, 1:-1, 4]) * s["c_mask"], "fb": fb, "fi": fi}
         trc = {"dti": dti_k, "n": np.exp(before[..., 1]), "p": np.exp(before[..., 2]),
                "a": np.exp(before[..., 3]) * ma, "c": np.exp(before[..., 4]) * mc,
-               "V": before[..., 0], "fb": fb, "fi": fi}
+               "V": before[..., 0], "fb": fb, "fi": fi,
+               "ion_last": np.full(nb, bool(zimt_ion_currents))}
         moving = (dti_k > 0) & (dti_now > 0) & (not first)
         rt = np.where(moving, dti_now / np.where(moving, dti_k, 1.0), 0.0)
         guess = y + np.clip(_col(rt)[..., None] * (y - y_prev), -caps, caps)

@@ -35,9 +35,11 @@ CASES = (
     # ZimT 5.36 transients (with their tVG.txt and ZimT's tj.dat): electrons and holes, the
     # absorber's traps, and mobile ions over 2 x 50 ms and 2 x 5 s; a sweep to 1.2 V and back in
     # 2 x 100 ns in the integral and the differential current, charged interface traps through
-    # it, and steady states at t = 0
+    # it, steady states at t = 0; ion regions that reach a contact (a region of two layers over
+    # 2 x 5 s, with the differential current over 2 x 50 ms, two regions per species)
     "zimt_photo_light", "zimt_traps_photo_light", "zimt_ions_fast_light", "zimt_ions_slow_light",
     "zimt_sweep_light", "zimt_sweep_diff_light", "zimt_iface_sweep_light", "zimt_steady_light",
+    "zimt_region_slow_light", "zimt_region_diff_light", "zimt_regions2_light",
 )
 
 

@@ -57,6 +57,35 @@ def test_zimt_transients_in_one_batch_each_with_its_own_steps():
         assert np.max(np.abs(r.J_ext[k] - ref["Jext"])) < ZIMT[case] * scale, case
 
 
+def test_two_ion_regions_per_species_reaching_the_contacts():
+    """Anions and cations in both transport layers, every region reaching a contact (its density
+    there from its neighbour's), through a sweep to 0.9 V and back: the GPU against the oracle
+    with every region's ion current and with ZimT's last region's (1e-9 of the scale; measured
+    1.2e-10), and in the latter against ZimT's `Jext` to 1e-8 (`zimt_ion_currents`,
+    test_solver.py:618-637); the final state's ions each region's total."""
+    setup, tvg, ref = zimt_case("zimt_regions2_light")
+    dev = build_device(setup, grid="simss")
+    scale = np.max(np.abs(ref["Jext"]))
+    for last in (False, True):
+        r = solve_transient(prepare([dev]), tvg, bernoulli_name="simss", zimt_current=True,
+                            zimt_ion_currents=last)
+        o = transient.solve_transient(dd.prepare([dev]), tvg.t, tvg.Vext, tvg.G_frac, tvg.track,
+                                      tvg.failure_mode, bernoulli_name="simss",
+                                      zimt_current=True, zimt_ion_currents=last)
+        assert r.converged.all() and o["converged"].all()
+        assert np.max(np.abs(r.J_ext[0] - o["J_ext"][0])) < 1e-9 * scale, last
+        if last:
+            assert np.max(np.abs(r.J_ext[0] - ref["Jext"])) < 1e-8 * scale
+    ion = dd.prepare([dev])["ion"]
+    for name, slots, totals in (("anion", ion["a_slots"][0], ion["a_totals"][0]),
+                                ("cation", ion["c_slots"][0], ion["c_totals"][0])):
+        dens = getattr(r.final, name)[0]
+        for mask, total in zip(slots, totals):
+            m = mask > 0
+            assert m[0] or m[-1]
+            assert abs(_number(np.where(m, dens, 0.0), m, dev) / total - 1) < 1e-9, name
+
+
 def test_config5_transient_matches_the_oracle():
     devs = [drawn_device(k) for k in (1, 3, 5)]
     tvg = transient_steps(40)

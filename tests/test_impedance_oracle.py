@@ -103,6 +103,29 @@ def test_with_ions_frozen_at_a_pre_bias_refused():
         imp.solve_impedance([dev], [1e3], voltage=0.5)
 
 
+def test_with_an_ion_region_that_reaches_a_contact_refused():
+    """The impedance's ions are carried for regions inside the device only: a region that
+    reaches a contact is refused by the oracle and by `solve_impedance` before any solve (the
+    transient, `solve_transient`, takes it)."""
+    from jaxdd_b200.batch import prepare
+    from jaxdd_b200.impedance import solve_impedance
+    from tests.test_transient_oracle import zimt_case
+    dev = build_device(zimt_case("zimt_region_slow_light")[0], grid="simss")
+    with pytest.raises(NotImplementedError, match="reaches a contact"):
+        imp.solve_impedance([dev], [1e3], voltage=0.5)
+    with pytest.raises(NotImplementedError, match="reaches a contact"):
+        solve_impedance(prepare([dev]), [1e3], voltage=0.5)
+
+
+def test_the_transients_gradients_refuse_an_ion_region_that_reaches_a_contact():
+    from jaxdd_b200.batch import prepare
+    from jaxdd_b200.transient import charge_gradients
+    from tests.test_transient_oracle import zimt_case
+    setup, tvg, _ = zimt_case("zimt_region_slow_light")
+    with pytest.raises(NotImplementedError, match="reaches a contact"):
+        charge_gradients(prepare([build_device(setup, grid="simss")]), tvg)
+
+
 
 def _sine_response(dev, V0, f, amp=1e-4, per_period=40, periods=20, fitted=4):
     """The oracle transient's admittance at `f`: `J = J₀ + amp·(Re Y·sin + Im Y·cos)` fitted over

@@ -3,8 +3,10 @@ to tests/golden/inputs): `Jext` through 241 steps to the reference's tolerances
 (test_solver.py:544-581: 1e-9 of the scale for electrons and holes and for the traps, 1e-7 with
 mobile ions), ZimT's Bernoulli function and sums (`zimt_current`): light on and off, a sweep to
 1.2 V and back in 2 x 100 ns in the integral and the differential current, the absorber's traps,
-charged interface traps through the sweep, mobile ions over 2 x 50 ms and 2 x 5 s, and steady
-states at t = 0 (test_solver.py:454-470). Also: the tVG reader's checks,
+charged interface traps through the sweep, mobile ions over 2 x 50 ms and 2 x 5 s, in a region
+of two layers that reaches a contact (its density there from its neighbour's, nothing flowing
+over the contact's interval), two regions per species with ZimT's last-region ion currents, and
+steady states at t = 0 (test_solver.py:454-470, 618-637). Also: the tVG reader's checks,
 the traps' step against its closed form and its derivatives, the ions' number kept in every step,
 and the refusals of what is out of scope."""
 
@@ -20,7 +22,8 @@ INPUTS = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "inp
 ZIMT = {"zimt_photo_light": 1e-9, "zimt_traps_photo_light": 1e-9,
         "zimt_ions_fast_light": 1e-7, "zimt_ions_slow_light": 1e-7,
         "zimt_sweep_light": 1e-9, "zimt_sweep_diff_light": 1e-9,
-        "zimt_iface_sweep_light": 1e-9, "zimt_steady_light": 1e-9}
+        "zimt_iface_sweep_light": 1e-9, "zimt_steady_light": 1e-9,
+        "zimt_region_slow_light": 1e-7, "zimt_region_diff_light": 1e-7}
 
 
 def zimt_case(case):
@@ -118,6 +121,23 @@ def test_tvg_as_zimt_reads_it():
     assert steps.dti[0] == 0 and np.isclose(steps.dti[2], 1 / 9e-9)
     with pytest.raises(ValueError):
         TVG.steps([1e-9, 1e-8], 0.9)
+
+
+def test_two_ion_regions_per_species_as_zimt_counts_their_currents():
+    """Anions and cations in both transport layers, each region reaching a contact, through a
+    sweep to 0.9 V and back in 2 x 50 ms: with ZimT's last-region ion currents
+    (`zimt_ion_currents`) ZimT's `Jext` to 1e-8 of its scale (test_solver.py:618-637); every
+    region's current (the default) differs from it by more."""
+    setup, tvg, ref = zimt_case("zimt_regions2_light")
+    b = dd.prepare([build_device(setup, grid="simss")])
+    scale = np.max(np.abs(ref["Jext"]))
+    last = transient.solve_transient(b, tvg.t, tvg.Vext, tvg.G_frac, tvg.track, tvg.failure_mode,
+                                     bernoulli_name="simss", zimt_current=True,
+                                     zimt_ion_currents=True)
+    assert last["converged"].all()
+    assert np.max(np.abs(last["J_ext"][0] - ref["Jext"])) < 1e-8 * scale
+    every = zimt_transient(b, tvg)
+    assert np.max(np.abs(every["J_ext"][0] - ref["Jext"])) > 1e-7 * scale
 
 
 def test_what_the_transient_refuses():
