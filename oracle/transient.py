@@ -11,11 +11,12 @@ ZimT's main loop (which steps are kept, `failureMode`, each step's Δt from the 
 Vectorised over a batch of devices of one grid size, as the reference's `vmap`; nothing in the
 product imports it.
 
-Scope (the rest is refused, never approximated): the voltage given at every step (no open
-circuit, no series resistance), `Track` 0 or 1 (no automatic stop on equal states), no photon
-recycling, no free ends, no ion sites, the steady scope of `oracle.dd` otherwise. An ion region
-that reaches a contact takes the contact's density from its neighbour (`ion_full`). With no mobile ions the same 5-column system holds
-the ions' rows at 0 (identity rows); the solution is the reference's 3-column one.
+Scope (the rest is refused, never approximated): the voltage given at every step, or the
+internal voltage an unknown of each step (the open circuit, a series resistance); `Track` 0 or
+1 (no automatic stop on equal states), no photon recycling, no free ends, no ion sites, the
+steady scope of `oracle.dd` otherwise. An ion region that reaches a contact takes the contact's
+density from its neighbour (`ion_full`). With no mobile ions the same 5-column system holds the
+ions' rows at 0 (identity rows); the solution is the reference's 3-column one.
 
 Derivatives that the reference takes by `jax.jvp` (the ions' rows, the traps over a step) are
 written out by hand; they are exact, as autodiff is.
@@ -610,15 +611,73 @@ def newton_step(y, logs, d, Vint, tr, bern):
     return new, logs + d_logs, size
 
 
+def newton_step_vint(y, logs, Vint, d, tr, trc, bern, zimt, oc, Vext):
+    """One damped Newton step with the internal voltage an unknown (batch._system_vint,
+    batch.py:552-592, and the step of _newton_loop, 759-785): its column the rows' derivatives in
+    it through the contacts' potentials (`V_0 = V0 + e Vint/2`, `V_N+1 = VL - e Vint/2`), its row
+    the external current over the current scale at the open circuit (`oc`), else
+    `(Vint + R_series J_ext - Vext)/V_T`. The row's products with the block sweep's solutions
+    (dense in the grid) are complex-step derivatives of the current along each solution, exact
+    as the reference's `jax.value_and_grad`; its own derivative in Vint the same. Returns the new
+    state, slots, voltage and step size."""
+    full, dV = ion_full(d, full_of(d, y, Vint), bern, tr["dti"])
+    F, A, Bb, C, U = assemble(full, d, tr, logs, bern)
+    g, W, D = constraints(full, logs, d["ion"], dV)
+    e = d["left_elec"]
+    Uv = np.zeros(F.shape)
+    Uv[:, 0] += A[:, 0, :, 0] * _col(0.5 * e)
+    Uv[:, -1] += C[:, -1, :, 0] * _col(-0.5 * e)
+    Vt, R, Js = d["Vt"], d["R_series"], d["J_scale"]
+    G_shunt = d["G_shunt"]
+
+    def J_ext(y_, V_):
+        return current(d, full_of(d, y_, V_), trc, bern, zimt) + G_shunt * V_
+
+    Je = J_ext(y, Vint)
+    h = np.where(oc, Je / Js, (Vint + R * Je - Vext) / Vt)
+    coef = np.where(oc, 1.0 / Js, R / Vt)
+    X = block_thomas(A, Bb, C, np.concatenate([-F[..., None], U, Uv[..., None]], -1))
+    delta = 1e-20
+    hX = np.stack([coef * np.imag(J_ext(y + 1j * delta * X[..., c], Vint)) / delta
+                   for c in range(X.shape[-1])], -1)
+    dJ_dV = np.imag(J_ext(y, Vint + 1j * delta)) / delta
+    h_V = np.where(oc, dJ_dV / Js, (1.0 + R * dJ_dV) / Vt)
+    K = W.shape[1]
+    WX = np.einsum("bkir,birc->bkc", W, X)
+    rows = np.concatenate([WX, hX[:, None, :]], 1)  # (K+1) rows × (1 + K + 1) columns
+    Dv = np.zeros((y.shape[0], K + 1, K + 1))
+    Dv[:, :K, :K] = D
+    Dv[:, K, K] = h_V
+    schur = Dv - rows[:, :, 1:]
+    rg = -np.concatenate([g, h[:, None]], 1) - rows[:, :, 0]
+    z = np.linalg.solve(schur, rg[..., None])[..., 0]
+    dy = X[..., 0] - np.einsum("birk,bk->bir", X[..., 1:], z)
+    caps = _caps(Vt)
+    stepv = dd.density_steps(y, dy, np.clip(dy, -caps, caps), d["s"]["n_floor"])
+    d_logs = np.clip(z[:, :K], -ION_LOG_CAP, ION_LOG_CAP)
+    d_V = np.clip(z[:, K], -dd.STEP_CAPS[0] * Vt, dd.STEP_CAPS[0] * Vt)
+    new = y + stepv
+    with np.errstate(over="ignore", invalid="ignore"):
+        dens = np.exp(new[..., 1:])
+        weight = dens / (dens + d["s"]["n_floor"][..., None])
+        size = np.maximum(np.maximum(np.max(np.abs(stepv[..., 0]), 1) / Vt,
+                                     np.max(np.abs(stepv[..., 1:]) * weight, axis=(1, 2))),
+                          np.maximum(np.max(np.abs(d_logs), 1), np.abs(d_V) / Vt))
+    return new, logs + d_logs, Vint + d_V, size
+
+
 def _take_tr(tr, idx):
     return {k: v[idx] for k, v in tr.items()}
 
 
-def newton_loop(y, logs, d, Vint, tr, trc, bern, tol, max_iter, zimt):
+def newton_loop(y, logs, d, Vint, tr, trc, bern, tol, max_iter, zimt, vint=None):
     """batch._newton_loop (batch.py:740-848) over a time step: `tr` the step's terms on the
-    interior points (`assemble`), `trc` on the full grid (`current`)."""
+    interior points (`assemble`), `trc` on the full grid (`current`). `vint`: `(oc, Vext)` (B
+    each) with the internal voltage an unknown from `Vint` (`newton_step_vint`; the current's
+    settling then no stop); returns the voltage too."""
     nb = y.shape[0]
     y, logs = y.copy(), logs.copy()
+    Vint = np.array(Vint, dtype=float)
     S = dd.STALL_STEPS
     size_h = np.full((nb, S + 1), np.inf)
     J_h = np.full((nb, S + 1), np.inf)
@@ -630,8 +689,13 @@ def newton_loop(y, logs, d, Vint, tr, trc, bern, tol, max_iter, zimt):
             break
         idx = np.flatnonzero(active)
         dl = dd.take(d, idx)
-        new, logs_new, size = newton_step(y[idx], logs[idx], dl, Vint[idx], _take_tr(tr, idx),
-                                          bern)
+        if vint is None:
+            new, logs_new, size = newton_step(y[idx], logs[idx], dl, Vint[idx],
+                                              _take_tr(tr, idx), bern)
+        else:
+            new, logs_new, Vint[idx], size = newton_step_vint(
+                y[idx], logs[idx], Vint[idx], dl, _take_tr(tr, idx), _take_tr(trc, idx), bern,
+                zimt, vint[0][idx], vint[1][idx])
         J = current(dl, full_of(dl, new, Vint[idx], bern, trc["dti"][idx]), _take_tr(trc, idx),
                     bern, zimt)
         sh = np.concatenate([size_h[idx, 1:], size[:, None]], 1)
@@ -646,9 +710,13 @@ def newton_loop(y, logs, d, Vint, tr, trc, bern, tol, max_iter, zimt):
                        & (np.max(np.abs(jh - jh[:, -1:]), 1) < dd.CURRENT_TOL * scale))
             quadratic = (n_it > 1) & (size_now < dd.QUADRATIC_TOL) & (
                 size_now < dd.QUADRATIC_RATIO * prev)
+            if vint is not None:
+                settled = np.zeros_like(settled)
             conv = (size_now < tol) | stalled | settled | quadratic
         y[idx], logs[idx] = new, logs_new
         size_h[idx], J_h[idx], it[idx], done[idx] = sh, jh, n_it, conv
+    if vint is not None:
+        return y, logs, J_h[:, -1], done, it, Vint
     return y, logs, J_h[:, -1], done, it
 
 
@@ -656,31 +724,38 @@ def newton_loop(y, logs, d, Vint, tr, trc, bern, tol, max_iter, zimt):
 
 def check_scope(d, oc=None, track=None):
     """What this restatement (and the product) supports; the rest raises."""
-    if np.any(d["R_series"] > 0):
-        raise NotImplementedError("transient with a series resistance (the internal voltage an "
-                                  "unknown)")
-    if oc is not None and np.any(oc):
-        raise NotImplementedError("transient at the open circuit (the internal voltage an "
-                                  "unknown)")
+    vint = np.any(d["R_series"] > 0) or (oc is not None and np.any(oc))
+    masks, _ = dd._masks(d["ion"])
+    if vint and (np.any(masks[:, :, 0] > 0) or np.any(masks[:, :, -1] > 0)):
+        raise NotImplementedError("the internal voltage an unknown with an ion region that "
+                                  "reaches a contact")
     if track is not None and np.any(np.asarray(track) > 1):
         raise NotImplementedError("Track 2 or 3 (ZimT's automatic stop on equal states)")
 
 
 def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, max_iter=200,
-                    bernoulli_name="exact", zimt_current=False, zimt_ion_currents=False):
+                    bernoulli_name="exact", zimt_current=False, zimt_ion_currents=False,
+                    oc=None):
     """transient.solve_transient / _solve_one (transient.py:270-465, 537-637) for every lane at
     once. `t`, `V`, `G_frac`, `track`: (S,) for every device or (B, S); `failure_mode` scalar
     or (B,). `zimt_ion_currents`: each species' last region's ion current alone, as ZimT 5.36
-    has it with several regions. Returns a dict: `J`, `J_ext`, `converged`, `iterations`,
-    `accepted` (B×S), `stop` (B), and the final state (`y` B×NP×5, `logs`, `f_bulk`,
-    `f_interface`)."""
+    has it with several regions. `oc` (B×S or S, true at the open circuit, `V` unread there):
+    where any step of the batch has it or any device a series resistance, the internal voltage
+    is an unknown of every step (`newton_step_vint`), from the last one at the open circuit
+    (extrapolated as the state) or the external voltage less the last current's drop, the steady
+    start at 0 V where the first step is at the open circuit (transient.py:290-300, 389-405).
+    Returns a dict: `J`, `J_ext`, `V_int`, `converged`, `iterations`, `accepted` (B×S), `stop`
+    (B), and the final state (`y` B×NP×5, `logs`, `f_bulk`, `f_interface`)."""
     d = batch
     nb = d["Vt"].shape[0]
     S = np.shape(t)[-1]
     t, V, G_frac = (np.broadcast_to(np.asarray(a, dtype=float), (nb, S)) for a in (t, V, G_frac))
+    oc = np.zeros((nb, S), bool) if oc is None else np.broadcast_to(np.asarray(oc, bool), (nb, S))
+    V = np.where(oc, 0.0, V)
+    vint = bool(oc.any() or np.any(d["R_series"] > 0))
     track = np.zeros((nb, S), int) if track is None else np.broadcast_to(np.asarray(track), (nb, S))
     fm = np.broadcast_to(np.asarray(failure_mode), (nb,))
-    check_scope(d, track=track)
+    check_scope(d, oc=oc, track=track)
     bern = dd.BERNOULLI[bernoulli_name]
     Vt = d["Vt"]
     NP = d["x"].shape[1] - 2
@@ -689,7 +764,7 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
 
     # the steady state at the first step (transient.py:301-320): `_start`, then Newton
     d0 = dict(d, g_frac=G_frac[:, 0])
-    V0 = V[:, 0]
+    V0 = np.where(oc[:, 0], 0.0, V[:, 0])
     y3, logs, _ = dd.start(d0, V0, bern, tol, max_iter)
     y3s, logs_s, J_s, ok_s, _ = dd.newton_loop(y3, logs, d0, V0, bern, tol, max_iter)
     y3 = np.where(ok_s[:, None, None], y3s, y3)
@@ -710,7 +785,8 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     track_curr = np.zeros(nb, int)
     stop = np.zeros(nb, int)
     caps = _caps(Vt)
-    out = {k: np.zeros((nb, S)) for k in ("J", "J_ext")}
+    out = {k: np.zeros((nb, S)) for k in ("J", "J_ext", "V_int")}
+    v_cap = dd.STEP_CAPS[0] * Vt
     out.update(converged=np.zeros((nb, S), bool), iterations=np.zeros((nb, S), int),
                accepted=np.zeros((nb, S), bool))
     ma, mc = ion["a_slots"].sum(1), ion["c_slots"].sum(1)
@@ -729,13 +805,24 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
         rt = np.where(moving, dti_now / np.where(moving, dti_k, 1.0), 0.0)
         guess = y + np.clip(_col(rt)[..., None] * (y - y_prev), -caps, caps)
         logs_guess = logs + np.clip(_col(rt) * (logs - logs_prev), -ION_LOG_CAP, ION_LOG_CAP)
-        steady = dd.ion_logs(full_of(d, guess, V_k)[..., 0], ion, Vt)
+        if vint:  # the internal voltage's start (transient.py:398-401)
+            V_g = np.where(oc[:, k], V_now + np.clip(rt * (V_now - V_before), -v_cap, v_cap),
+                           V_k - d["R_series"] * J_ext_now)
+        else:
+            V_g = V_k
+        steady = dd.ion_logs(full_of(d, guess, V_g)[..., 0], ion, Vt)
         logs_guess = np.where(_col(dti_k) > 0, np.where(_col(moving), logs_guess, 0.0), steady)
         dk = dict(d, g_frac=G_k)
-        y_new, logs_new, J, ok, it = newton_loop(guess, logs_guess, dk, V_k, tr, trc, bern, tol,
-                                                 max_iter, zimt_current)
-        J_ext = J + d["G_shunt"] * V_k
-        after = full_of(d, y_new, V_k)
+        if vint:
+            y_new, logs_new, J, ok, it, V_new = newton_loop(
+                guess, logs_guess, dk, V_g, tr, trc, bern, tol, max_iter, zimt_current,
+                vint=(oc[:, k], V_k))
+        else:
+            y_new, logs_new, J, ok, it = newton_loop(guess, logs_guess, dk, V_k, tr, trc, bern,
+                                                     tol, max_iter, zimt_current)
+            V_new = V_k
+        J_ext = J + d["G_shunt"] * V_new
+        after = full_of(d, y_new, V_new)
         n_a, p_a = np.exp(after[..., 1]), np.exp(after[..., 2])
         fb_new = bulk_occupation(n_a[:, 1:-1], p_a[:, 1:-1], s, fb, _col(dti_k))
         fi_new = iface_occupation(n_a, p_a, d["ti"], fi, _col(dti_k))
@@ -748,7 +835,7 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
         y, y_prev = np.where(kk, y_new, y), np.where(kk, y, y_prev)
         logs, logs_prev = (np.where(keep[:, None], logs_new, logs),
                            np.where(keep[:, None], logs, logs_prev))
-        V_before, V_now = np.where(keep, V_now, V_before), np.where(keep, V_k, V_now)
+        V_before, V_now = np.where(keep, V_now, V_before), np.where(keep, V_new, V_now)
         J_ext_now = np.where(keep, J_ext, J_ext_now)
         dti_now = np.where(keep, dti_k, dti_now)
         fb = np.where(keep[:, None], fb_new, fb)
@@ -757,7 +844,7 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
         t_last = np.where(keep, t_k, t_last)
         stop = np.where(failed, STOP_FAILED, stop)
         first = False
-        out["J"][:, k], out["J_ext"][:, k] = J, J_ext
+        out["J"][:, k], out["J_ext"][:, k], out["V_int"][:, k] = J, J_ext, V_new
         out["converged"][:, k], out["iterations"][:, k], out["accepted"][:, k] = ok, it, keep
     out.update(stop=stop, y=y, logs=logs, f_bulk=fb, f_interface=fi)
     return out

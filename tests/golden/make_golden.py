@@ -40,6 +40,9 @@ CASES = (
     "zimt_photo_light", "zimt_traps_photo_light", "zimt_ions_fast_light", "zimt_ions_slow_light",
     "zimt_sweep_light", "zimt_sweep_diff_light", "zimt_iface_sweep_light", "zimt_steady_light",
     "zimt_region_slow_light", "zimt_region_diff_light", "zimt_regions2_light",
+    # the internal voltage an unknown: the photovoltage at the open circuit after a light pulse,
+    # a sweep through a series resistance and a shunt
+    "zimt_tpv_light", "zimt_rseries_sweep_light",
 )
 
 

@@ -140,13 +140,46 @@ def test_two_ion_regions_per_species_as_zimt_counts_their_currents():
     assert np.max(np.abs(every["J_ext"][0] - ref["Jext"])) > 1e-7 * scale
 
 
+def zimt_vint(batch, tvg):
+    """ZimT's steps with the internal voltage an unknown where they are at the open circuit."""
+    return transient.solve_transient(batch, tvg.t, tvg.Vext, tvg.G_frac, tvg.track,
+                                     tvg.failure_mode, bernoulli_name="simss", zimt_current=True,
+                                     oc=tvg.oc)
+
+
+def test_the_photovoltage_at_the_open_circuit_reproduces_zimt():
+    """The open circuit, the internal voltage an unknown of each step's Newton solve: ZimT
+    5.36's photovoltage through a light pulse of 1 µs and 1 ms after, 151 steps, to 1e-10 V;
+    the current 0 to 1e-10 of the photocurrent (test_solver.py:740-752)."""
+    setup, tvg, ref = zimt_case("zimt_tpv_light")
+    r = zimt_vint(dd.prepare([build_device(setup, grid="simss")]), tvg)
+    assert r["converged"].all() and tvg.oc.all()
+    assert np.max(np.abs(r["V_int"][0] - ref["Vint"])) < 1e-10
+    assert np.max(np.abs(r["J_ext"])) < 1e-10 * np.max(ref["JphotoL2"])
+
+
+def test_a_series_resistance_in_time_reproduces_zimt():
+    """`R_series` with a shunt, `Vint` the unknown whose `Vint + Jext R_series` is the given
+    `Vext`: ZimT 5.36's `Jext` through a sweep to 1.2 V and back in 2 x 100 ns to 1e-9 of its
+    scale, `Vint` to 1e-9 V (test_solver.py:770-780)."""
+    setup, tvg, ref = zimt_case("zimt_rseries_sweep_light")
+    dev = build_device(setup, grid="simss")
+    r = zimt_vint(dd.prepare([dev]), tvg)
+    assert r["converged"].all()
+    assert np.max(np.abs(r["J_ext"][0] - ref["Jext"])) < 1e-9 * np.max(np.abs(ref["Jext"]))
+    assert np.max(np.abs(r["V_int"][0] - ref["Vint"])) < 1e-9
+    assert np.max(np.abs(r["V_int"][0] + dev.R_series * r["J_ext"][0] - tvg.Vext)) < 1e-9
+
+
 def test_what_the_transient_refuses():
     setup, tvg, _ = zimt_case("zimt_photo_light")
     b = dd.prepare([build_device(setup, grid="simss")])
     with pytest.raises(NotImplementedError, match="Track"):
         transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3], [0, 1, 2])
+    setup, tvg, _ = zimt_case("zimt_region_slow_light")
+    b = dd.prepare([build_device(setup, grid="simss")])
     b["R_series"] = np.array([1e-4])
-    with pytest.raises(NotImplementedError, match="series resistance"):
+    with pytest.raises(NotImplementedError, match="reaches a contact"):
         transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3])
 
 
