@@ -258,6 +258,13 @@ typedef struct dd_steps {
                                   the interval after it); 0: over its control volume (jaxdd's) */
   int32_t zimt_ion_last;       /* 1: each species' last ion region's current alone, as ZimT 5.36
                                   has it with several regions; 0: every region's (jaxdd's) */
+  /* The internal voltage an unknown of every step (jaxdd's `vint`, batch.py:552-592): 0 the
+   * voltage `v` given; 1 each step's row the external current at the open circuit (`oc`),
+   * else `V_int + R_series J_ext = v`. */
+  int32_t vint;
+  const uint8_t* oc;           /* per step, in `t`'s layout: 1 at the open circuit (`v` unread) */
+  const double* r_series;      /* [lane_stride]: Ohm m^2 */
+  const double* start_j_ext;   /* [lane_stride]: the external current of the start (A/m^2) */
 } dd_steps;
 
 /* Outputs of dd_transient (device pointers). Per step and lane [n_steps][lane_stride]: J (A/m^2,
@@ -291,6 +298,9 @@ typedef struct dd_transient_out {
   double* prof_f_bulk;
   double* prof_f_iface;
   double* prof_dti;
+  /* V_int [n_steps][lane_stride]: each step's internal voltage (the solution's with `vint`, else
+   * the given one). NULL: not written. */
+  double* V_int;
 } dd_transient_out;
 
 /* A state to start from instead of the steady state at the first step (jaxdd's

@@ -80,13 +80,15 @@ class DdSteps(ctypes.Structure):
     _fields_ = [("n_steps", ctypes.c_int32), ("stride", ctypes.c_int32), ("t", ctypes.c_void_p),
                 ("v", ctypes.c_void_p), ("g_frac", ctypes.c_void_p), ("track", ctypes.c_void_p),
                 ("failure_mode", ctypes.c_void_p), ("zimt_sums", ctypes.c_int32),
-                ("zimt_ion_last", ctypes.c_int32)]
+                ("zimt_ion_last", ctypes.c_int32), ("vint", ctypes.c_int32),
+                ("oc", ctypes.c_void_p), ("r_series", ctypes.c_void_p),
+                ("start_j_ext", ctypes.c_void_p)]
 
 
 class DdTransientOut(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in (
         "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs", "f_bulk",
-        "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface", "prof_dti")]
+        "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface", "prof_dti", "V_int")]
 
 
 class DdTransientInit(ctypes.Structure):

@@ -82,6 +82,12 @@ struct Args {
   const double* init_fb;     // [np+2][Bp]
   const double* init_fi;     // [np+2][Bp]
   const double* init_scal;   // [4][Bp]: t, V_int, J_ext, dti
+  // the internal voltage an unknown of every step (vint): each step's open circuit (same layout
+  // as t), each lane's series resistance and its external current at the start
+  const uint8_t* oc;
+  const double* rser;    // [Bp]
+  const double* jext0;   // [Bp]
+  double* Vout;          // [S][Bp]: each step's internal voltage (nullptr: not written)
 };
 
 // ------------------------------------------------------------------------------------ current
@@ -92,18 +98,18 @@ struct Args {
 // right: each carrier's integral form by prefix sums (sum_e h_e J_e = q K H + sum_e h_e P_e,
 // P_e the prefix of q L w_k U_k; an interface's J the one before it plus its traps'), each ion
 // region's the same over its own intervals, and the displacement current.
-// The state along a tangent: `buf`'s point plus h times the tangent `tan` (same layout), the
-// contacts as they are.
+// The state along a tangent: `buf`'s point plus h times the tangent `tan` (point k's field r at
+// (k * tn + r * tf) * Bp + l: tn = 5, tf = 1 for a state's layout), the contacts as they are.
 __device__ __forceinline__ void load_pert(const View& W, int buf, const double* tan, double h,
-                                          int k, double Vint, TP& P) {
+                                          int k, double Vint, TP& P, int tn = 5, int tf = 1) {
   load_point(W, buf, k, Vint, P);
   if (!tan || k == 0 || k == W.L.NP + 1) return;
-  const size_t o = (size_t)k * 5 * W.L.Bp + W.L.l;
+  const size_t o = (size_t)k * tn * W.L.Bp + W.L.l, f = (size_t)tf * W.L.Bp;
   P.c.V += h * tan[o];
-  P.c.lnn += h * tan[o + W.L.Bp];
-  P.c.lnp += h * tan[o + 2 * W.L.Bp];
-  P.la += h * tan[o + 3 * W.L.Bp];
-  P.lc += h * tan[o + 4 * W.L.Bp];
+  P.c.lnn += h * tan[o + f];
+  P.c.lnp += h * tan[o + 2 * f];
+  P.la += h * tan[o + 3 * f];
+  P.lc += h * tan[o + 4 * f];
   P.c.n = exp(P.c.lnn);
   P.c.p = exp(P.c.lnp);
   P.a = P.c.sl.a >= 0 ? exp(P.la) : 1.0;
@@ -132,6 +138,7 @@ struct Pert {
   const double* tfb;
   const double* tfi;
   double h, mus;
+  int tn = 5, tf = 1;  // the strides of `tcur` (load_pert)
 };
 
 template <int K, bool PERT = false>
@@ -149,7 +156,8 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     return PERT && pt->tfi ? FI[o] + pt->h * pt->tfi[o] : FI[o];
   };
   auto load_c = [&](int buf, int k, double Vi, TP& P, bool is_cur) {
-    if (PERT) load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P);
+    if (PERT) load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P,
+                        is_cur ? pt->tn : 5, is_cur ? pt->tf : 1);
     else if (is_cur) load_point(W, buf, k, Vi, P);
     else load_before(W, buf, k, Vi, P);
     contact_ions(W, buf, k, is_cur ? dti : dti_bef, P);
@@ -631,7 +639,65 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
 
 // ------------------------------------------------------------------------------------ kernel
 
-template <int K>
+constexpr double VINT_H = 1e-6;  // the vint row's central-difference step (V_T, ln units)
+
+// With the internal voltage an unknown (`vint`), its row of the bordered system (`_vint_row`,
+// batch.py:552-563): at the open circuit the external current over the current scale, else
+// (V_int + R_series J_ext - V_ext) / V_T, at the iterate. `row` receives its Schur row over the
+// border's unknowns (the K slots, then the voltage), `res` its right-hand side less the row's
+// product with the sweep's solution of -F. The row's derivatives along the sweep's solutions
+// (the columns of CD after the back substitution, dense in the grid) and in V_int are central
+// differences of the current, each along a solution scaled to a step of VINT_H (V_T in the
+// potential): the reference takes them by reverse-mode autodiff (`jax.value_and_grad`).
+template <int K, int NC>
+__device__ __noinline__ void vint_row(const Args& a, const View& W, int bn, int bk, double Vi,
+                                      double Vext, double V_now, double dti, double dti_now,
+                                      bool oc, double (&row)[K + 1], double& res) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = a.Bp, l = L.l;
+  const double* FB = a.FB;
+  const double* FI = a.FI;
+  const double Rs = a.rser[l];
+  const double Je = current_t<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI) + L.Gshunt * Vi;
+  res = -(oc ? Je / L.Jscale : (Vi + Rs * Je - Vext) * L.iVt);
+  const double eV = VINT_H * L.Vt;
+  const double dJV = (current_t<K>(W, bn, Vi + eV, bk, V_now, dti, dti_now, FB, FI) -
+                      current_t<K>(W, bn, Vi - eV, bk, V_now, dti, dti_now, FB, FI)) /
+                         (2.0 * eV) +
+                     L.Gshunt;
+#pragma unroll
+  for (int q = 0; q < K; ++q) row[q] = 0.0;
+  row[K] = oc ? dJV / L.Jscale : (1.0 + Rs * dJV) * L.iVt;
+  const double coef = oc ? 1.0 / L.Jscale : Rs * L.iVt;
+  if (coef == 0.0) return;  // V_int = V_ext: a row of the voltage alone
+  for (int c = 0; c < NC; ++c) {
+    double m = 0.0;
+    for (int i = 1; i <= NP; ++i)
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+        const double v = fabs(a.CD[((size_t)i * a.ncd + 25 + rr * NC + c) * Bp + l]);
+        m = fmax(m, rr == 0 ? v * L.iVt : v);
+      }
+    if (!(m > 0.0) || !isfinite(m)) continue;  // a zero solution: no change
+    Pert pt;
+    pt.tcur = a.CD + (size_t)(25 + c) * Bp;
+    pt.tbef = nullptr;
+    pt.tfb = nullptr;
+    pt.tfi = nullptr;
+    pt.h = VINT_H / m;
+    pt.mus = 1.0;
+    pt.tn = a.ncd;
+    pt.tf = NC;
+    const double Jp = current_t<K, true>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI, &pt);
+    pt.h = -pt.h;
+    const double Jm = current_t<K, true>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI, &pt);
+    const double dJ = coef * (Jp - Jm) * m / (2.0 * VINT_H);
+    if (c == 0) res -= dJ;
+    else row[c - 1] -= dJ;
+  }
+}
+
+template <int K, bool VINT>
 __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= a.n) return;
@@ -656,7 +722,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   double* FB = a.FB;
   double* FI = a.FI;
   auto cd = [&](int k, int f) -> double* { return a.CD + ((size_t)k * a.ncd + f) * Bp + l; };
-  constexpr int NC = 1 + K;  // right-hand sides: -F and the K slot columns
+  // right-hand sides: -F, the K slot columns and with VINT the internal voltage's
+  constexpr int NC = VINT ? 2 + K : 1 + K;
+  constexpr int KV = VINT ? K + 1 : K;  // the border's unknowns
 
   // ---- the start: the steady state at the first step, with the ions' densities as unknowns,
   // or a given state (its slots' scales 1)
@@ -709,6 +777,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   double V_now = given ? a.init_scal[(size_t)Bp + l] : a.V[ts ? l : 0];
   double dti_now = given ? a.init_scal[(size_t)3 * Bp + l] : 0.0;
   double t_last = given ? a.init_scal[l] : 0.0;
+  // the internal voltage kept before the last one, and the external current of the last
+  double V_before = V_now;
+  double J_ext_now = given ? a.init_scal[(size_t)2 * Bp + l] : (VINT ? a.jext0[l] : 0.0);
   int track_curr = 0, stop = 0;
   bool first = true;
   const double capV = CAP_V * L.Vt;
@@ -721,13 +792,21 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const double dti = t_k == 0.0 ? 0.0 : 1.0 / (t_k > t_last ? t_k - t_last : 1.0);
     const bool moving = dti > 0.0 && dti_now > 0.0 && !first;
     const double rt = moving ? dti_now / dti : 0.0;
+    // the internal voltage of the iterate: given, or with VINT an unknown from the last one at
+    // the open circuit (extrapolated as the state), else the external voltage less the last
+    // current's drop (transient.py:398-401)
+    const bool oc_k = VINT && a.oc[so] != 0;
+    double Vi = V_k;
+    if (VINT)
+      Vi = oc_k ? V_now + clipd(rt * (V_now - V_before), -capV, capV)
+                : V_k - a.rser[l] * J_ext_now;
     // ---- the step's start: the last two kept states extrapolated, held to one step's caps;
     // into a steady state the slots' Boltzmann normalisations of it
     double num[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) num[q] = 0.0;
     {
-      double Vprev = L.V0 + 0.5 * L.left * V_k;
+      double Vprev = L.V0 + 0.5 * L.left * Vi;
       Slots slp = slots_at(L, 0);
       for (int i = 1; i <= NP + 1; ++i) {
         double V;
@@ -747,7 +826,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
           a.BD[ob + 3 * Bp] = sl.c >= 0 ? exp(*W.y(bk, i, 4)) : 0.0;
           V = *W.y(bn, i, 0);
         } else {
-          V = L.VL - 0.5 * L.left * V_k;
+          V = L.VL - 0.5 * L.left * Vi;
         }
         if (!(dti > 0.0)) {
           const Slots sl = slots_at(L, i);
@@ -793,9 +872,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
 #pragma unroll
       for (int q = 0; q < K; ++q) gnum[q] = 0.0;
       TP pm, pc, pn;
-      load_point(W, bn, 0, V_k, pm);
+      load_point(W, bn, 0, Vi, pm);
       contact_ions(W, bn, 0, dti, pm);
-      load_point(W, bn, 1, V_k, pc);
+      load_point(W, bn, 1, Vi, pc);
       Flux el, er;
       flux(L, pm.c, pc.c, L.st(0, S_MUN), L.st(0, S_MUP), el);
       double elg[K];  // the slots' scales, once per iteration
@@ -804,7 +883,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       IonIv ivl[2], ivr[2];  // the ions' fluxes of the row's left and right intervals
       ion_ivs(W, 0, pm, pc, ivl);
       for (int i = 1; i <= NP; ++i) {
-        load_point(W, bn, i + 1, V_k, pn);
+        load_point(W, bn, i + 1, Vi, pn);
         contact_ions(W, bn, i + 1, dti, pn);
         flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
         ion_ivs(W, i, pc, pn, ivr);
@@ -819,6 +898,14 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][K];
         row5<K>(W, i, pm, pc, pn, el, er, hm, hp, ifm, ifi, dti, fb, fim, fii, bnv, bpv, bav, bcv,
                 lg, A, Bm, Cm, r, U, nullptr, nullptr, elg, ivl, ivr);
+        // with VINT the rows' derivatives in the internal voltage, through the contacts'
+        // potentials V0 + left Vint / 2 and VL - left Vint / 2 (`_system_vint`'s column)
+        double uv[5];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr)
+          uv[rr] = VINT ? (i == 1 ? A[rr][0] * 0.5 * L.left : 0.0) +
+                              (i == NP ? Cm[rr][0] * (-0.5 * L.left) : 0.0)
+                        : 0.0;
         ivl[0] = ivr[0];
         ivl[1] = ivr[1];
         // the ions' numbers over interval i-1 (between points i-1 and i)
@@ -845,7 +932,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         for (int rr = 0; rr < 5; ++rr) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
-            double s = c == 0 ? r[rr] : U[rr][c - 1];
+            double s = c == 0 ? r[rr] : (VINT && c == NC - 1) ? uv[rr] : U[rr][c - 1];
 #pragma unroll
             for (int q = 0; q < 5; ++q) s -= A[rr][q] * dpv[q][c];
             rhs[rr][c] = s;
@@ -879,13 +966,13 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
           gnum[L.ka + pc.c.sl.c] += 0.5 * (pm.c2 + pc.c2) * hL;
       }
       // -------- back substitution with the slots' Schur complement
-      double SM[K][K], sr[K];
+      double SM[KV][KV], sr[KV];
 #pragma unroll
-      for (int q = 0; q < K; ++q) {
-        const bool has = L.tot[q] > 0.0;
+      for (int q = 0; q < KV; ++q) {
+        const bool has = q < K && L.tot[q] > 0.0;
 #pragma unroll
-        for (int q2 = 0; q2 < K; ++q2) SM[q][q2] = (q == q2 && !has) ? 1.0 : 0.0;
-        sr[q] = -(has ? gnum[q] / L.tot[q] - 1.0 : lg[q]);
+        for (int q2 = 0; q2 < KV; ++q2) SM[q][q2] = (q == q2 && !has) ? 1.0 : 0.0;
+        sr[q] = q < K ? -(has ? gnum[q] / L.tot[q] - 1.0 : lg[q]) : 0.0;
       }
       {
         double xn[5][NC];
@@ -928,7 +1015,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
             if ((i == 1 && slm == sl) || (i == NP && sln == sl)) {
               const int kc = i == 1 ? 0 : NP + 1;
               TP P;
-              load_point(W, bn, kc, V_k, P);
+              load_point(W, bn, kc, Vi, P);
               double dr;
               contact_ions(W, bn, kc, dti, P, &dr);
               const double wc = 0.5 * (i == 1 ? hLm : hLp) * (sp == 0 ? P.a : P.c2) / L.tot[q];
@@ -937,15 +1024,17 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
             }
             sr[q] -= w * xi[3 + sp][0] + wv * xi[0][0];
 #pragma unroll
-            for (int q2 = 0; q2 < K; ++q2)
+            for (int q2 = 0; q2 < KV; ++q2)
               SM[q][q2] -= w * xi[3 + sp][1 + q2] + wv * xi[0][1 + q2];
           }
           s_next = s_here;
           s_here = s_prev;
         }
       }
-      double z[K];
-      small_solve<K>(SM, sr, z);
+      if constexpr (VINT)
+        vint_row<K, NC>(a, W, bn, bk, Vi, V_k, V_now, dti, dti_now, oc_k, SM[K], sr[K]);
+      double z[KV];
+      small_solve<KV>(SM, sr, z);
       // -------- the damped update (batch.py:759-785)
       double size = 0.0, dl_max = 0.0;
 #pragma unroll
@@ -954,13 +1043,18 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         dl_max = nanmax(dl_max, fabs(dlq));
         lg[q] += dlq;
       }
+      if constexpr (VINT) {  // the voltage's step held to the potential's cap
+        const double dV = clipd(z[K], -capV, capV);
+        dl_max = nanmax(dl_max, fabs(dV) * L.iVt);
+        Vi += dV;
+      }
       for (int i = 1; i <= NP; ++i) {
         double d5[5];
 #pragma unroll
         for (int rr = 0; rr < 5; ++rr) {
           double s = *cd(i, 25 + rr * NC);
 #pragma unroll
-          for (int q = 0; q < K; ++q) s -= *cd(i, 25 + rr * NC + 1 + q) * z[q];
+          for (int q = 0; q < KV; ++q) s -= *cd(i, 25 + rr * NC + 1 + q) * z[q];
           d5[rr] = s;
         }
         double y5[5];
@@ -994,7 +1088,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
 #pragma unroll
       for (int q = 0; q < K; ++q) finite = finite && isfinite(lg[q]);
       // -------- the current at the new iterate and the stops
-      const double J = current_t<K>(W, bn, V_k, bk, V_now, dti, dti_now, FB, FI);
+      const double J = current_t<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI);
 #pragma unroll
       for (int q = 0; q < STALL_STEPS; ++q) { sh[q] = sh[q + 1]; jh[q] = jh[q + 1]; }
       sh[STALL_STEPS] = size;
@@ -1008,7 +1102,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
 #pragma unroll
       for (int q = 0; q <= STALL_STEPS; ++q) jdev = nanmax(jdev, fabs(jh[q] - J));
       const bool stalled = it > STALL_STEPS && smax < ROUND_OFF_FLOOR && smin1 >= 0.1 * sh[0];
-      const bool settled = it > STALL_STEPS && size < CURRENT_STEP_CAP &&
+      const bool settled = !VINT && it > STALL_STEPS && size < CURRENT_STEP_CAP &&
                            jdev < CURRENT_TOL * (L.Jscale + fabs(J));
       const bool quad = it > 1 && size < QUADRATIC_TOL &&
                         size < QUADRATIC_RATIO * sh[STALL_STEPS - 1];
@@ -1016,8 +1110,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     }
     const bool ok = done;
     const double J = jh[STALL_STEPS];
-    const double J_ext = J + L.Gshunt * V_k;
-    if (a.prof_state) write_profile(a, W, bn, k, V_k, dti);
+    const double J_ext = J + L.Gshunt * Vi;
+    if (a.prof_state) write_profile(a, W, bn, k, Vi, dti);
     // ---- ZimT's main loop (transient.py:419-445)
     const bool running = stop == 0;
     const bool failed = running && !ok && (fm == 0 || (fm == 2 && track_curr == 1));
@@ -1026,16 +1120,16 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       // the tangents of this step, before the occupations move on (they take the old ones)
       const double dt = dti > 0.0 ? t_k - t_last : 0.0;
       Qint += J * dt;
-      if (grad) tangent_step<K>(a, W, bn, bk, V_k, V_now, dti, dti_now, dt, lg, tb, dQ);
+      if (grad) tangent_step<K>(a, W, bn, bk, Vi, V_now, dti, dti_now, dt, lg, tb, dQ);
       // the traps' occupations at the step's end, from its solution (and their tangents)
       auto tyn = [&](int p, int k, int c) {
         return (k < 1 || k > NP) ? 0.0
                                  : a.TY[((((size_t)(p * 2 + 1 - tb)) * tnodes + k) * 5 + c) * Bp + l];
       };
       TP pa, pb;
-      load_point(W, bn, 0, V_k, pa);
+      load_point(W, bn, 0, Vi, pa);
       for (int e = 0; e <= NP; ++e) {
-        load_point(W, bn, e + 1, V_k, pb);
+        load_point(W, bn, e + 1, Vi, pb);
         const int ifk = (int)L.st(e, S_IFK);
         if (ifk >= 0) {
           Iface t;
@@ -1079,7 +1173,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       tb = 1 - tb;
 #pragma unroll
       for (int q = 0; q < K; ++q) { logs_p[q] = logs[q]; logs[q] = lg[q]; }
-      V_now = V_k;
+      V_before = V_now;
+      V_now = Vi;
+      J_ext_now = J_ext;
       dti_now = dti;
       track_curr = a.track[so];
       t_last = t_k;
@@ -1092,6 +1188,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     a.conv[o] = ok ? 1 : 0;
     a.iters[o] = it;
     a.acc[o] = keep ? 1 : 0;
+    if (a.Vout) a.Vout[o] = Vi;
   }
   a.stop[l] = stop;
   if (grad) {
@@ -1175,6 +1272,9 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   if (steps->n_steps < 1 || !steps->t || !steps->v || !steps->g_frac || !steps->track ||
       !steps->failure_mode || (steps->stride != 0 && steps->stride != batch->lane_stride))
     return DD_ERR_ARGS;
+  if (steps->vint && (!steps->oc || !steps->r_series || !steps->start_j_ext)) return DD_ERR_ARGS;
+  // the vint row's derivatives take a state's perturbation from every point: no gradients
+  if (steps->vint && out->Q) return DD_ERR_ARGS;
   if (!out->J || !out->J_ext || !out->converged || !out->iterations || !out->accepted ||
       !out->stop || !out->state || !out->logs)
     return DD_ERR_ARGS;
@@ -1213,6 +1313,8 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.init_fb = initial ? initial->f_bulk : nullptr;
   a.init_fi = initial ? initial->f_iface : nullptr;
   a.init_scal = initial ? initial->scalars : nullptr;
+  a.oc = steps->oc; a.rser = steps->r_series; a.jext0 = steps->start_j_ext;
+  a.Vout = out->V_int;
   if (out->Q) {
     const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
     char* t = w + y + fb + fi + cd;
@@ -1225,8 +1327,14 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   }
   const dim3 grid((batch->n_lanes + 31) / 32), block(32);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (slots_k_t(batch) == 2) dd::tr::transient_kernel<2><<<grid, block, 0, s>>>(a);
-  else dd::tr::transient_kernel<4><<<grid, block, 0, s>>>(a);
+  const bool k2 = slots_k_t(batch) == 2;
+  if (steps->vint) {
+    if (k2) dd::tr::transient_kernel<2, true><<<grid, block, 0, s>>>(a);
+    else dd::tr::transient_kernel<4, true><<<grid, block, 0, s>>>(a);
+  } else {
+    if (k2) dd::tr::transient_kernel<2, false><<<grid, block, 0, s>>>(a);
+    else dd::tr::transient_kernel<4, false><<<grid, block, 0, s>>>(a);
+  }
   return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
 }
 

@@ -11,9 +11,9 @@ one kept).
 With `profiles=True` every step's state is written beside its current (`TransientResult.state`);
 with `initial=` (a `TransientState`) the devices start from that state instead of a steady one.
 
-The voltage is given at every step. Refused (`NotImplementedError`), not approximated: an open
-circuit or a series resistance (the internal voltage an unknown), `Track` 2 or 3 (ZimT's
-automatic stop), photon recycling.
+The voltage is given at every step, or with an open circuit or a series resistance the internal
+voltage is an unknown of each step's Newton solve. Refused (`NotImplementedError`), not
+approximated: `Track` 2 or 3 (ZimT's automatic stop), photon recycling.
 """
 
 from __future__ import annotations
@@ -162,16 +162,14 @@ def _steps(tvgs: list[TVG]):
     if len({len(x.t) for x in tvgs}) != 1:
         raise ValueError("one tVG for the batch, or one per device, all of one length")
     for x in tvgs:
-        if np.any(x.oc):
-            raise NotImplementedError("transient at the open circuit (the internal voltage an "
-                                      "unknown): not built")
         if np.any(np.asarray(x.track) > 1):
             raise NotImplementedError("Track 2 or 3 (ZimT's automatic stop on equal states): "
                                       "not built")
     t, V, G, track = (np.stack([np.asarray(getattr(x, k), dtype=float) for x in tvgs])
                       for k in ("t", "Vext", "G_frac", "track"))
+    oc = np.stack([np.asarray(x.oc, dtype=bool) for x in tvgs])
     fm = np.array([x.failure_mode for x in tvgs], dtype=np.int32)
-    return t, V, G, track.astype(np.int32), fm
+    return t, np.where(oc, 0.0, V), G, track.astype(np.int32), fm, oc
 
 
 def reaches_contact(d) -> bool:
@@ -179,11 +177,18 @@ def reaches_contact(d) -> bool:
     return any(m is not None and bool(m[0] or m[-1]) for m in (d.anion_mask, d.cation_mask))
 
 
-def _check_batch(batch: Batch) -> None:
+def _check_batch(batch: Batch, vint: bool, gradients: bool) -> None:
     devs = batch["devices"]
-    if any(d.R_series > 0 for d in devs):
-        raise NotImplementedError("transient with a series resistance (the internal voltage an "
-                                  "unknown): not built")
+    if vint and any(reaches_contact(d) for d in devs):
+        raise NotImplementedError("the internal voltage an unknown (an open circuit, a series "
+                                  "resistance) with an ion region that reaches a contact: not "
+                                  "built")
+    if gradients and vint:
+        raise NotImplementedError("the transient's gradients with the internal voltage an "
+                                  "unknown: not built")
+    if gradients and any(reaches_contact(d) for d in devs):
+        raise NotImplementedError("the transient's gradients with an ion region that reaches "
+                                  "a contact: not built")
 
 
 class Work:
@@ -195,18 +200,19 @@ class Work:
     def __init__(self, batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
                  bernoulli_name: str = "exact", zimt_current: bool = False,
                  gradients: bool = False, profiles: bool = False, initial=None,
-                 zimt_ion_currents: bool = False):
+                 zimt_ion_currents: bool = False, vint: bool = False):
         import torch
         from .adjoint import plan as _plan
-        _check_batch(batch)
         devs = batch["devices"]
-        if gradients and any(reaches_contact(d) for d in devs):
-            raise NotImplementedError("the transient's gradients with an ion region that reaches "
-                                      "a contact: not built")
         tvgs = list(tvg) if isinstance(tvg, (list, tuple)) else [tvg] * len(devs)
         if len(tvgs) != len(devs):
             raise ValueError("one tVG for the batch, or one per device, all of one length")
-        t, V, G, track, fm = _steps(tvgs)
+        t, V, G, track, fm, oc = _steps(tvgs)
+        R = np.array([d.R_series for d in devs])
+        # the internal voltage an unknown of every device's steps where any is at the open
+        # circuit or has a series resistance (transient.py:600-601)
+        self.vint = vint = bool(vint or oc.any() or np.any(R > 0))
+        _check_batch(batch, vint, gradients)
         init = None if initial is None else _checked_initial(initial, devs, t)
         self.batch, self.tol, self.max_iter = batch, tol, max_iter
         self.bern = _lib.DD_BERNOULLI[bernoulli_name]
@@ -215,12 +221,14 @@ class Work:
         Bp, nodes, lanes = batch["Bp"], batch["np_max"] + 2, batch["lane_of"]
         self.S = S = t.shape[1]
         self.t, self.V = t, V
-        # the start: the steady state at the first step's voltage and generation, no pre-bias
-        self.plan = _plan(batch, [[float(v)] for v in V[:, 0]], tol=tol, max_iter=max_iter,
+        # the start: the steady state at the first step's voltage (0 V at the open circuit) and
+        # generation, no pre-bias
+        V0 = np.where(oc[:, 0], 0.0, V[:, 0])
+        self.plan = _plan(batch, [[float(v)] for v in V0], tol=tol, max_iter=max_iter,
                           bernoulli_name=bernoulli_name)
         y0 = np.zeros((nodes, 3, Bp))
         for k, d in enumerate(devs):
-            y0[:len(d.x), :, lanes[k]] = initial_state(d, float(V[k, 0]))
+            y0[:len(d.x), :, lanes[k]] = initial_state(d, float(V0[k]))
         self.plan.y0.copy_(torch.from_numpy(y0))
         scal = g.scal.clone()
         gf = scal[_lib.C["GFRAC"]].cpu().numpy()
@@ -239,10 +247,11 @@ class Work:
                 X[:m, 2, lanes[k]] = d.mu_cation
         self.X = torch.from_numpy(X).to(cuda)
         # the steps: one list for all lanes where every device has the same
-        same = all(np.array_equal(a[0], a[j]) for a in (t, V, G, track) for j in range(len(a)))
+        same = all(np.array_equal(a[0], a[j]) for a in (t, V, G, track, oc)
+                   for j in range(len(a)))
         if same:
             self.stride = 0
-            cols, tr = (t[0], V[0], G[0]), track[0]
+            cols, tr, ocs = (t[0], V[0], G[0]), track[0], oc[0]
         else:
             self.stride = Bp
 
@@ -251,6 +260,15 @@ class Work:
                 out[:, lanes] = a.T
                 return out
             cols, tr = (lane_major(t), lane_major(V), lane_major(G)), lane_major(track)
+            ocs = lane_major(oc)
+        self.ocv = torch.from_numpy(np.ascontiguousarray(ocs, dtype=np.uint8)).to(cuda)
+        rl = np.zeros(Bp)
+        rl[lanes] = R
+        self.rser = torch.from_numpy(rl).to(cuda)
+        gv0 = np.zeros(Bp)  # the shunt's current at the start, where its solve failed
+        gv0[lanes] = batch["G_shunt"] * V0
+        self.gv0 = torch.from_numpy(gv0).to(cuda)
+        self.jext0 = torch.zeros(Bp, dtype=torch.float64, device=cuda)
         self.tv, self.vv, self.gv = (torch.from_numpy(np.ascontiguousarray(c)).to(cuda)
                                      for c in cols)
         self.trk = torch.from_numpy(np.ascontiguousarray(tr, dtype=np.int32)).to(cuda)
@@ -267,6 +285,7 @@ class Work:
             "iterations": torch.empty((S, Bp), dtype=i32, device=cuda),
             "accepted": torch.empty((S, Bp), dtype=u8, device=cuda),
             "stop": torch.empty(Bp, dtype=i32, device=cuda),
+            "V_int": torch.empty((S, Bp), dtype=f64, device=cuda),
             "state": torch.empty((nodes, 5, Bp), dtype=f64, device=cuda),
             "logs": torch.zeros((_lib.DD_MAXK, Bp), dtype=f64, device=cuda),
             "f_bulk": torch.empty((nodes, Bp), dtype=f64, device=cuda),
@@ -317,21 +336,26 @@ class Work:
         from .adjoint import solve_states as _solve_states
         g = self.g
         if self.initial is None:
-            _, ok0, _, ckpt = _solve_states(self.plan, g.stat, self.scal0, g.iface)
+            J0, ok0, _, ckpt = _solve_states(self.plan, g.stat, self.scal0, g.iface)
             start, start_logs = ckpt["states"][0].data_ptr(), ckpt["logs"][0].data_ptr()
             init = None
+            # the start's external current (the shunt's included), its shunt's alone where the
+            # start failed (transient.py:453-456)
+            off = self.plan.offsets.long().clamp(max=J0.numel() - 1)
+            self.jext0.copy_(torch.where(ok0[off] > 0, J0[off], self.gv0))
         else:
             ok0, start, start_logs = None, None, None
             init = ctypes.byref(_lib.DdTransientInit(*(self.init[k].data_ptr() for k in (
                 "state", "f_bulk", "f_iface", "scalars"))))
         steps = _lib.DdSteps(self.S, self.stride, self.tv.data_ptr(), self.vv.data_ptr(),
                              self.gv.data_ptr(), self.trk.data_ptr(), self.fm.data_ptr(),
-                             self.zimt, self.ion_last)
+                             self.zimt, self.ion_last, int(self.vint), self.ocv.data_ptr(),
+                             self.rser.data_ptr(), self.jext0.data_ptr())
         o = self.out
         out = _lib.DdTransientOut(*(o[k].data_ptr() if k in o else None for k in (
             "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",
             "f_bulk", "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface",
-            "prof_dti")))
+            "prof_dti", "V_int")))
         opts = _lib.DdOpts(float(self.tol), int(self.max_iter), int(self.max_iter), 0,
                            self.bern, _lib.DD_MODE_BATCH, 0, 0)
         desc = descriptor(self.batch, g, self.plan.y0)
@@ -359,21 +383,22 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
     as jaxdd checks it (`ValueError`). `zimt_ion_currents`: with several ion regions of a
     species each species' last region's current alone, as ZimT 5.36 has it; by default every
     region's. An ion region that reaches a contact takes the contact's density from its
-    neighbour, nothing flowing over the contact's interval (jaxdd's `_ion_full`). Not built
-    (raise `NotImplementedError`): `recycle`, an internal voltage as an unknown (`vint`, an open
-    circuit, a series resistance). `ions` is accepted for the
+    neighbour, nothing flowing over the contact's interval (jaxdd's `_ion_full`). Where any step
+    is at the open circuit (`TVG.oc`) or any device has a series resistance, the internal
+    voltage is an unknown of every device's steps (`vint`, also forced by `vint=True`): its row
+    the external current at the open circuit, else `V_int + J_ext R_series = V_ext`. Not built
+    (raise `NotImplementedError`): `recycle`; the internal voltage an unknown with an ion region
+    that reaches a contact. `ions` is accepted for the
     reference's signature: the ions are unknowns of every step here, which leaves devices
     without mobile ions as they are."""
     if recycle is not None:
         raise NotImplementedError("photon recycling in transients: not built")
-    if vint:
-        raise NotImplementedError("the internal voltage as an unknown: not built")
     if ion_flux not in ("electrochemical", "modified-drift"):
         raise ValueError(f"ion_flux {ion_flux!r}: one of ('electrochemical', 'modified-drift')")
     del ions
     work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
                 zimt_current=zimt_current, profiles=profiles, initial=initial,
-                zimt_ion_currents=zimt_ion_currents)
+                zimt_ion_currents=zimt_ion_currents, vint=bool(vint))
     o, _ = work.run()
     return result(work, o)
 
@@ -392,7 +417,7 @@ def result(work: Work, o) -> TransientResult:
     ok, its = per_step("converged", bool), per_step("iterations", int)
     acc = per_step("accepted", bool)
     stop = o["stop"].cpu().numpy()[lanes]
-    V_int = work.V.copy()
+    V_int = per_step("V_int")
     R = np.array([d.R_series for d in devs])
     V_ext = V_int + J_ext * R[:, None]
     state = o["state"].cpu().numpy()[:, :, lanes]  # nodes × 5 × devices

@@ -1,7 +1,9 @@
 """The transient on the GPU (`dd_transient` through `jaxdd_b200.solve_transient`) against the
 oracle (`oracle.transient`) on the same devices and steps, and against ZimT 5.36's own `Jext`
 (the reference's tests/data) at the reference's tolerances: electrons and holes, the bulk traps
-in time, mobile ions over 2 x 50 ms and 2 x 5 s; config 5's transient (drawn devices with mobile
+in time, mobile ions over 2 x 50 ms and 2 x 5 s, ion regions that reach a contact, the internal
+voltage an unknown (the open circuit's photovoltage, a series resistance); a state carried
+across a split (`profiles`, `initial`); config 5's transient (drawn devices with mobile
 ions, a step to 0.9 V, log-spaced steps) on fewer steps; ZimT's failure modes; at config 5's
 2000 steps the properties that hold at any size (every step converged and kept, each region's
 ions kept to their total, the current finite); and the integrated current's forward-mode
@@ -84,6 +86,46 @@ def test_two_ion_regions_per_species_reaching_the_contacts():
             m = mask > 0
             assert m[0] or m[-1]
             assert abs(_number(np.where(m, dens, 0.0), m, dev) / total - 1) < 1e-9, name
+
+
+def test_the_photovoltage_at_the_open_circuit():
+    """The internal voltage an unknown of each step (`vint`, the open circuit): ZimT 5.36's
+    photovoltage through a light pulse of 1 µs and 1 ms after to 1e-10 V, the current 0 to
+    1e-10 of the photocurrent (test_solver.py:740-752), the oracle's voltage to 1e-12 V."""
+    from tests.test_transient_oracle import zimt_vint
+    setup, tvg, ref = zimt_case("zimt_tpv_light")
+    dev = build_device(setup, grid="simss")
+    r = solve_transient(prepare([dev]), tvg, bernoulli_name="simss", zimt_current=True)
+    o = zimt_vint(dd.prepare([dev]), tvg)
+    assert r.converged.all() and r.accepted.all()
+    assert np.max(np.abs(r.V_int[0] - ref["Vint"])) < 1e-10
+    assert np.max(np.abs(r.V_int[0] - o["V_int"][0])) < 1e-12
+    assert np.max(np.abs(r.J_ext)) < 1e-10 * np.max(ref["JphotoL2"])
+    np.testing.assert_array_equal(r.V_ext, r.V_int)
+
+
+def test_a_series_resistance_beside_given_voltages_and_ions_in_a_batch():
+    """jaxdd test_solver.py:770-780 and 862-875 on the GPU: the series resistance's sweep (Vint
+    the unknown whose Vint + Jext R_series is Vext) beside a device with the voltage given (its
+    row Vint = Vext) and one with mobile ions (5x5 blocks with the voltage's border), each
+    device its own steps: ZimT's Jext to 1e-9 (1e-7 with the ions) of its scale, Vint to 1e-9 V;
+    the oracle's to 1e-10 of the scale."""
+    from tests.test_transient_oracle import zimt_vint
+    names = ("zimt_rseries_sweep_light", "zimt_photo_light", "zimt_ions_fast_light")
+    cases = [zimt_case(c) for c in names]
+    devs = [build_device(setup, grid="simss") for setup, _, _ in cases]
+    r = solve_transient(prepare(devs), [tvg for _, tvg, _ in cases], bernoulli_name="simss",
+                        zimt_current=True)
+    assert r.converged.all()
+    for k, ((_, tvg, ref), tol) in enumerate(zip(cases, (1e-9, 1e-9, 1e-7))):
+        scale = np.max(np.abs(ref["Jext"]))
+        assert np.max(np.abs(r.J_ext[k] - ref["Jext"])) < tol * scale, names[k]
+        assert np.max(np.abs(r.V_ext[k] - tvg.Vext)) < 1e-9, names[k]
+    assert np.max(np.abs(r.V_int[0] - cases[0][2]["Vint"])) < 1e-9
+    assert np.max(np.abs(r.V_int[1:] - np.stack([t.Vext for _, t, _ in cases[1:]]))) < 1e-12
+    o = zimt_vint(dd.prepare(devs[:1]), cases[0][1])
+    scale = np.max(np.abs(o["J_ext"][0]))
+    assert np.max(np.abs(r.J_ext[0] - o["J_ext"][0])) < 1e-10 * scale
 
 
 def test_config5_transient_matches_the_oracle():
