@@ -252,7 +252,8 @@ typedef struct dd_steps {
   const double* t;             /* s */
   const double* v;             /* internal voltage, V */
   const double* g_frac;        /* generation factor */
-  const int32_t* track;        /* ZimT's Track: 0 or 1 (2 and 3, the automatic stop, not built) */
+  const int32_t* track;        /* ZimT's Track 0-3 (1 the reference state; 2 and 3 the automatic
+                                  stop on five equal states in a row, `convVar` 1) */
   const int32_t* failure_mode; /* [lane_stride]: 0 stop at a failed step, 1 keep it, 2 skip it */
   int32_t zimt_sums;           /* 1: ZimT's sums in the integral current (each point's change over
                                   the interval after it); 0: over its control volume (jaxdd's) */
@@ -265,13 +266,18 @@ typedef struct dd_steps {
   const uint8_t* oc;           /* per step, in `t`'s layout: 1 at the open circuit (`v` unread) */
   const double* r_series;      /* [lane_stride]: Ohm m^2 */
   const double* start_j_ext;   /* [lane_stride]: the external current of the start (A/m^2) */
+  /* [lane_stride] each: how the automatic stop compares two states (ZimT's tolPois in V,
+   * tolDens relative). NULL: no two states are equal (Track 2 and 3 never stop). */
+  const double* tol_pois;
+  const double* tol_dens;
 } dd_steps;
 
 /* Outputs of dd_transient (device pointers). Per step and lane [n_steps][lane_stride]: J (A/m^2,
  * internal, SIMsalabim's sign), J_ext (with the shunt), converged, iterations, accepted (the
- * step is kept: ZimT's tJFile rows); per lane stop (0 through every step, 2 at a failed step:
- * failureMode 0, or 2 with Track 1). The last kept state: state [np_max+2][5][lane_stride]
- * (V, ln n, ln p, ln a, ln c; the ions' 0 outside their regions), logs [DD_MAXK][lane_stride]
+ * step is kept: ZimT's tJFile rows); per lane stop (0 through every step, 1 where ZimT's
+ * automatic stop found the state static, 2 at a failed step: failureMode 0, or 2 with Track 1).
+ * The last kept state: state [np_max+2][5][lane_stride] (V, ln n, ln p, ln a, ln c; the ions'
+ * 0 outside their regions), logs [DD_MAXK][lane_stride]
  * (the slots' scales), f_bulk and f_iface [np_max+2][lane_stride] (the traps' occupations at
  * the points and on the intervals; either may be NULL). */
 typedef struct dd_transient_out {

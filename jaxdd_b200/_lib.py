@@ -82,7 +82,8 @@ class DdSteps(ctypes.Structure):
                 ("failure_mode", ctypes.c_void_p), ("zimt_sums", ctypes.c_int32),
                 ("zimt_ion_last", ctypes.c_int32), ("vint", ctypes.c_int32),
                 ("oc", ctypes.c_void_p), ("r_series", ctypes.c_void_p),
-                ("start_j_ext", ctypes.c_void_p)]
+                ("start_j_ext", ctypes.c_void_p), ("tol_pois", ctypes.c_void_p),
+                ("tol_dens", ctypes.c_void_p)]
 
 
 class DdTransientOut(ctypes.Structure):

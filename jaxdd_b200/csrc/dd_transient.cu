@@ -88,6 +88,11 @@ struct Args {
   const double* rser;    // [Bp]
   const double* jext0;   // [Bp]
   double* Vout;          // [S][Bp]: each step's internal voltage (nullptr: not written)
+  // ZimT's automatic stop: how two states compare (tolPois, tolDens per lane) and the
+  // reference state's V, n, p, a, c on every point
+  const double* tolp;    // [Bp]
+  const double* told;    // [Bp]
+  double* REF;           // [np+2][5][Bp]
 };
 
 // ------------------------------------------------------------------------------------ current
@@ -640,6 +645,64 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
 // ------------------------------------------------------------------------------------ kernel
 
 constexpr double VINT_H = 1e-6;  // the vint row's central-difference step (V_T, ln units)
+constexpr int MIN_COUNT_STATIC = 5;  // ZimT's equal states in a row that stop a transient
+constexpr int STOP_STATIC = 1, STOP_FAILED = 2;
+
+// The state of buffer `buf` (contacts at Vint, their ions at dti) on every point as the
+// automatic stop compares states (`summary`, transient.py:361-368): V, n, p and the ions'
+// densities where they are mobile, 0 elsewhere.
+__device__ __forceinline__ void summary_at(const View& W, int buf, int i, double Vint, double dti,
+                                           double (&v)[5]) {
+  TP P;
+  load_point(W, buf, i, Vint, P);
+  contact_ions(W, buf, i, dti, P);
+  v[0] = P.c.V; v[1] = P.c.n; v[2] = P.c.p;
+  v[3] = P.c.sl.a >= 0 ? P.a : 0.0;
+  v[4] = P.c.sl.c >= 0 ? P.c2 : 0.0;
+}
+
+// ZimT's `States_Are_Equal` with convVar 1 (transient.py:243-262) of the reference state (REF)
+// and the last kept one (buffer `buf`): the potentials within tolPois (the Euclidean norm over
+// the grid), each density relatively within tolDens. The generation factors compared apart.
+__device__ __noinline__ bool states_equal(const Args& a, const View& W, int buf, double Vint,
+                                          double dti) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = a.Bp, l = L.l;
+  double dv = 0.0, d2[4] = {0, 0, 0, 0}, c2[4] = {0, 0, 0, 0}, r2[4] = {0, 0, 0, 0};
+  for (int i = 0; i <= NP + 1; ++i) {
+    double v[5];
+    summary_at(W, buf, i, Vint, dti, v);
+    const double* rf = a.REF + (size_t)i * 5 * Bp + l;
+    const double e = v[0] - rf[0];
+    dv += e * e;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const double r = rf[(size_t)(f + 1) * Bp], d = v[f + 1] - r;
+      d2[f] += d * d;
+      c2[f] += v[f + 1] * v[f + 1];
+      r2[f] += r * r;
+    }
+  }
+  bool eq = sqrt(dv) < a.tolp[l];
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const double scale = 0.5 * (sqrt(c2[f]) + sqrt(r2[f]));
+    const double rel = scale > 0.0 ? sqrt(d2[f]) / scale : 0.0;
+    eq = eq && rel < a.told[l];
+  }
+  return eq;
+}
+
+__device__ __noinline__ void write_ref(const Args& a, const View& W, int buf, double Vint,
+                                       double dti) {
+  const int NP = W.L.NP, Bp = a.Bp, l = W.L.l;
+  for (int i = 0; i <= NP + 1; ++i) {
+    double v[5];
+    summary_at(W, buf, i, Vint, dti, v);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) a.REF[((size_t)i * 5 + f) * Bp + l] = v[f];
+  }
+}
 
 // With the internal voltage an unknown (`vint`), its row of the bordered system (`_vint_row`,
 // batch.py:552-563): at the open circuit the external current over the current scale, else
@@ -780,7 +843,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   // the internal voltage kept before the last one, and the external current of the last
   double V_before = V_now;
   double J_ext_now = given ? a.init_scal[(size_t)2 * Bp + l] : (VINT ? a.jext0[l] : 0.0);
-  int track_curr = 0, stop = 0;
+  int track_curr = 0, stop = 0, count = 0;
+  double G_cur = -1.0, G_ref = -1.0;  // the generation factors of the kept and reference states
   bool first = true;
   const double capV = CAP_V * L.Vt;
 
@@ -1179,8 +1243,25 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       dti_now = dti;
       track_curr = a.track[so];
       t_last = t_k;
+      G_cur = L.gfrac;
     }
-    if (failed) stop = 2;
+    // ZimT's automatic stop by the last state kept (transient.py:432-442): Track 1 makes it the
+    // reference where the step converged; 2 and 3 count equal states in a row (where the step
+    // converged or failureMode is 1), 3 then makes it the reference
+    const bool counted = running && !failed && (track_curr == 2 || track_curr == 3) &&
+                         (ok || fm == 1);
+    if (counted)
+      count = (a.tolp && a.told && G_ref == G_cur && states_equal(a, W, bk, V_now, dti_now))
+                  ? count + 1
+                  : 0;
+    const bool becomes_ref = running && !failed &&
+                             ((track_curr == 1 && ok) || (track_curr == 3 && (ok || fm == 1)));
+    if (becomes_ref && a.REF) {
+      write_ref(a, W, bk, V_now, dti_now);
+      G_ref = G_cur;
+    }
+    if (failed) stop = STOP_FAILED;
+    else if (running && count >= MIN_COUNT_STATIC) stop = STOP_STATIC;
     first = false;
     const size_t o = (size_t)k * Bp + l;
     a.J[o] = J;
@@ -1236,6 +1317,8 @@ void ws_parts(const dd_batch* b, size_t* y, size_t* fb, size_t* fi, size_t* cd, 
         + align_up(nodes * 4 * Bp * sizeof(double));  // and the before-state record
   // the tangents: two parameters' states (two buffers each) and traps' occupations
   *tan = align_up(4 * nodes * 5 * Bp * sizeof(double)) + 2 * align_up(2 * nodes * Bp * sizeof(double));
+  // and the automatic stop's reference state
+  *tan += align_up(nodes * 5 * Bp * sizeof(double));
 }
 
 bool batch_ok(const dd_batch* b) {
@@ -1315,6 +1398,12 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.init_scal = initial ? initial->scalars : nullptr;
   a.oc = steps->oc; a.rser = steps->r_series; a.jext0 = steps->start_j_ext;
   a.Vout = out->V_int;
+  a.tolp = steps->tol_pois; a.told = steps->tol_dens;
+  {
+    const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
+    a.REF = reinterpret_cast<double*>(w + y + fb + fi + cd + tan) -
+            nodes * 5 * Bp;  // the last part of the tangents' region
+  }
   if (out->Q) {
     const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
     char* t = w + y + fb + fi + cd;

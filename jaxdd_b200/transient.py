@@ -13,7 +13,8 @@ with `initial=` (a `TransientState`) the devices start from that state instead o
 
 The voltage is given at every step, or with an open circuit or a series resistance the internal
 voltage is an unknown of each step's Newton solve. Refused (`NotImplementedError`), not
-approximated: `Track` 2 or 3 (ZimT's automatic stop), photon recycling.
+approximated: ZimT's automatic stop (`Track` 2 or 3) with `convVar` 2-4 (the states' currents
+compared by errJ), photon recycling.
 """
 
 from __future__ import annotations
@@ -27,11 +28,11 @@ from . import _lib
 from .batch import Batch, _gpu, descriptor, initial_state
 from .simss_input import TVG
 
-__all__ = ["STOP_FAILED", "ChargeGradients", "TransientResult", "TransientState", "Work",
+__all__ = ["STOP_FAILED", "STOP_STATIC", "ChargeGradients", "TransientResult", "TransientState", "Work",
            "charge_gradients", "solve_transient"]
 
 #: `TransientResult.stop`: a failed step ended the run (transient.py:240)
-STOP_FAILED = 2
+STOP_STATIC, STOP_FAILED = 1, 2
 
 
 @dataclass(frozen=True)
@@ -58,7 +59,8 @@ class TransientState:
 class TransientResult:
     """Per device and step (devices × steps), as jaxdd's (transient.py:97-135): `J` the internal
     current density (A/m²), `J_ext` with the shunt, `V_int`, `V_ext`, `converged`, `iterations`,
-    `accepted` (the steps ZimT keeps); per device `stop` (0, or `STOP_FAILED`); `t` each step's
+    `accepted` (the steps ZimT keeps); per device `stop` (0, `STOP_STATIC` where ZimT's automatic
+    stop found the state static, or `STOP_FAILED`); `t` each step's
     time; `final` the last state kept; with `profiles=True` `profiles` `{"V", "n", "p", "anion",
     "cation", "f_bulk", "f_interface", "dti"}` (devices × steps × points, or per device where
     the grids differ), from which `state(k)` is step k's state. ZimT's other tJFile columns are
@@ -162,14 +164,15 @@ def _steps(tvgs: list[TVG]):
     if len({len(x.t) for x in tvgs}) != 1:
         raise ValueError("one tVG for the batch, or one per device, all of one length")
     for x in tvgs:
-        if np.any(np.asarray(x.track) > 1):
-            raise NotImplementedError("Track 2 or 3 (ZimT's automatic stop on equal states): "
-                                      "not built")
+        if np.any(np.asarray(x.track) > 1) and x.conv_var != 1:
+            raise NotImplementedError("Track 2 or 3 with convVar 2-4 (states compared by their "
+                                      "currents and ZimT's errJ): not built")
     t, V, G, track = (np.stack([np.asarray(getattr(x, k), dtype=float) for x in tvgs])
                       for k in ("t", "Vext", "G_frac", "track"))
     oc = np.stack([np.asarray(x.oc, dtype=bool) for x in tvgs])
     fm = np.array([x.failure_mode for x in tvgs], dtype=np.int32)
-    return t, np.where(oc, 0.0, V), G, track.astype(np.int32), fm, oc
+    tols = np.array([[x.tol_pois, x.tol_dens] for x in tvgs], dtype=float)
+    return t, np.where(oc, 0.0, V), G, track.astype(np.int32), fm, oc, tols
 
 
 def reaches_contact(d) -> bool:
@@ -207,7 +210,7 @@ class Work:
         tvgs = list(tvg) if isinstance(tvg, (list, tuple)) else [tvg] * len(devs)
         if len(tvgs) != len(devs):
             raise ValueError("one tVG for the batch, or one per device, all of one length")
-        t, V, G, track, fm, oc = _steps(tvgs)
+        t, V, G, track, fm, oc, tols = _steps(tvgs)
         R = np.array([d.R_series for d in devs])
         # the internal voltage an unknown of every device's steps where any is at the open
         # circuit or has a series resistance (transient.py:600-601)
@@ -269,6 +272,9 @@ class Work:
         gv0[lanes] = batch["G_shunt"] * V0
         self.gv0 = torch.from_numpy(gv0).to(cuda)
         self.jext0 = torch.zeros(Bp, dtype=torch.float64, device=cuda)
+        tl = np.zeros((2, Bp))  # the automatic stop's tolPois and tolDens
+        tl[:, lanes] = tols.T
+        self.tols = torch.from_numpy(tl).to(cuda)
         self.tv, self.vv, self.gv = (torch.from_numpy(np.ascontiguousarray(c)).to(cuda)
                                      for c in cols)
         self.trk = torch.from_numpy(np.ascontiguousarray(tr, dtype=np.int32)).to(cuda)
@@ -350,7 +356,8 @@ class Work:
         steps = _lib.DdSteps(self.S, self.stride, self.tv.data_ptr(), self.vv.data_ptr(),
                              self.gv.data_ptr(), self.trk.data_ptr(), self.fm.data_ptr(),
                              self.zimt, self.ion_last, int(self.vint), self.ocv.data_ptr(),
-                             self.rser.data_ptr(), self.jext0.data_ptr())
+                             self.rser.data_ptr(), self.jext0.data_ptr(), self.tols[0].data_ptr(),
+                             self.tols[1].data_ptr())
         o = self.out
         out = _lib.DdTransientOut(*(o[k].data_ptr() if k in o else None for k in (
             "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",

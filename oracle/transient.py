@@ -12,11 +12,11 @@ Vectorised over a batch of devices of one grid size, as the reference's `vmap`; 
 product imports it.
 
 Scope (the rest is refused, never approximated): the voltage given at every step, or the
-internal voltage an unknown of each step (the open circuit, a series resistance); `Track` 0 or
-1 (no automatic stop on equal states), no photon recycling, no free ends, no ion sites, the
-steady scope of `oracle.dd` otherwise. An ion region that reaches a contact takes the contact's
-density from its neighbour (`ion_full`). With no mobile ions the same 5-column system holds the
-ions' rows at 0 (identity rows); the solution is the reference's 3-column one.
+internal voltage an unknown of each step (the open circuit, a series resistance); ZimT's
+automatic stop (`Track` 2, 3) with `convVar = 1`; no photon recycling, no free ends, no ion
+sites, the steady scope of `oracle.dd` otherwise. An ion region that reaches a contact takes the
+contact's density from its neighbour (`ion_full`). With no mobile ions the same 5-column system
+holds the ions' rows at 0 (identity rows); the solution is the reference's 3-column one.
 
 Derivatives that the reference takes by `jax.jvp` (the ions' rows, the traps over a step) are
 written out by hand; they are exact, as autodiff is.
@@ -33,7 +33,8 @@ from oracle import dd
 
 Q = dd.Q
 ION_LOG_CAP = dd.ION_LOG_CAP
-STOP_FAILED = 2  # transient.py:240
+STOP_STATIC, STOP_FAILED = 1, 2  # transient.py:240
+MIN_COUNT_STATIC = 5  # transient.py:238
 
 
 def _col(v):
@@ -722,20 +723,46 @@ def newton_loop(y, logs, d, Vint, tr, trc, bern, tol, max_iter, zimt, vint=None)
 
 # ----------------------------------------------------------------------------- the steps
 
-def check_scope(d, oc=None, track=None):
+def summary(d, full):
+    """What two states compare by (transient.py:361-368) without the current: `V`, `n`, `p`,
+    `a`, `c` on every point (B×(NP+2) each, the ions where mobile)."""
+    ion = d["ion"]
+    ma, mc = ion["a_slots"].sum(1), ion["c_slots"].sum(1)
+    return {"V": full[..., 0], "n": np.exp(full[..., 1]), "p": np.exp(full[..., 2]),
+            "a": np.exp(full[..., 3]) * ma, "c": np.exp(full[..., 4]) * mc}
+
+
+def states_equal(A, B, GA, GB, tol_pois, tol_dens):
+    """ZimT's `States_Are_Equal` with `convVar = 1` (transient.py:243-262): the same `G_frac`,
+    the potentials within `tolPois` (V, the Euclidean norm over the grid), each density
+    relatively within `tolDens`."""
+    def norm(v):
+        return np.sqrt(np.sum(v ** 2, axis=1))
+
+    def rel(a, b):
+        scale = 0.5 * (norm(a) + norm(b))
+        return np.where(scale > 0, norm(a - b) / np.where(scale > 0, scale, 1.0), 0.0)
+
+    dens = np.all(np.stack([rel(A[k], B[k]) for k in ("n", "p", "a", "c")]) < tol_dens, 0)
+    return (GA == GB) & (norm(A["V"] - B["V"]) < tol_pois) & dens
+
+
+def check_scope(d, oc=None, track=None, conv_var=None):
     """What this restatement (and the product) supports; the rest raises."""
     vint = np.any(d["R_series"] > 0) or (oc is not None and np.any(oc))
     masks, _ = dd._masks(d["ion"])
     if vint and (np.any(masks[:, :, 0] > 0) or np.any(masks[:, :, -1] > 0)):
         raise NotImplementedError("the internal voltage an unknown with an ion region that "
                                   "reaches a contact")
-    if track is not None and np.any(np.asarray(track) > 1):
-        raise NotImplementedError("Track 2 or 3 (ZimT's automatic stop on equal states)")
+    if track is not None and np.any(np.asarray(track) > 1) and conv_var is not None and np.any(
+            np.asarray(conv_var) != 1):
+        raise NotImplementedError("Track 2 or 3 with convVar 2-4 (the states' currents compared "
+                                  "by ZimT's errJ)")
 
 
 def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, max_iter=200,
                     bernoulli_name="exact", zimt_current=False, zimt_ion_currents=False,
-                    oc=None):
+                    oc=None, conv_var=1, tol_pois=1e-6, tol_dens=1e-6):
     """transient.solve_transient / _solve_one (transient.py:270-465, 537-637) for every lane at
     once. `t`, `V`, `G_frac`, `track`: (S,) for every device or (B, S); `failure_mode` scalar
     or (B,). `zimt_ion_currents`: each species' last region's ion current alone, as ZimT 5.36
@@ -744,8 +771,10 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     is an unknown of every step (`newton_step_vint`), from the last one at the open circuit
     (extrapolated as the state) or the external voltage less the last current's drop, the steady
     start at 0 V where the first step is at the open circuit (transient.py:290-300, 389-405).
+    `conv_var`, `tol_pois`, `tol_dens` (scalars or B): how ZimT's automatic stop compares two
+    states (`TVG`'s `convVar`, `tolPois`, `tolDens`; only `convVar = 1` with `Track` 2 or 3).
     Returns a dict: `J`, `J_ext`, `V_int`, `converged`, `iterations`, `accepted` (B×S), `stop`
-    (B), and the final state (`y` B×NP×5, `logs`, `f_bulk`, `f_interface`)."""
+    (B: 0, `STOP_STATIC` or `STOP_FAILED`), and the final state (`y` B×NP×5, `logs`, `f_bulk`, `f_interface`)."""
     d = batch
     nb = d["Vt"].shape[0]
     S = np.shape(t)[-1]
@@ -755,7 +784,9 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     vint = bool(oc.any() or np.any(d["R_series"] > 0))
     track = np.zeros((nb, S), int) if track is None else np.broadcast_to(np.asarray(track), (nb, S))
     fm = np.broadcast_to(np.asarray(failure_mode), (nb,))
-    check_scope(d, oc=oc, track=track)
+    check_scope(d, oc=oc, track=track, conv_var=conv_var)
+    tol_pois, tol_dens = (np.broadcast_to(np.asarray(v, dtype=float), (nb,))
+                          for v in (tol_pois, tol_dens))
     bern = dd.BERNOULLI[bernoulli_name]
     Vt = d["Vt"]
     NP = d["x"].shape[1] - 2
@@ -784,6 +815,10 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     first = True
     track_curr = np.zeros(nb, int)
     stop = np.zeros(nb, int)
+    # the automatic stop: the last state kept and the reference state, blank (G -1) at first
+    cur = ref = None
+    G_cur, G_ref = np.full(nb, -1.0), np.full(nb, -1.0)
+    count = np.zeros(nb, int)
     caps = _caps(Vt)
     out = {k: np.zeros((nb, S)) for k in ("J", "J_ext", "V_int")}
     v_cap = dd.STEP_CAPS[0] * Vt
@@ -842,7 +877,22 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
         fi = np.where(keep[:, None], fi_new, fi)
         track_curr = np.where(keep, track[:, k], track_curr)
         t_last = np.where(keep, t_k, t_last)
-        stop = np.where(failed, STOP_FAILED, stop)
+        # ZimT's automatic stop by the last state kept (transient.py:429-442): Track 1 makes it
+        # the reference where the step converged; 2 and 3 count equal states in a row (where the
+        # step converged or failureMode is 1), 3 then makes it the reference
+        now = summary(d, full_of(d, y_new, V_new, bern, dti_k))
+        cur = now if cur is None else {f: np.where(keep[:, None], now[f], cur[f]) for f in now}
+        G_cur = np.where(keep, G_k, G_cur)
+        ref = {f: np.zeros_like(v) for f, v in cur.items()} if ref is None else ref
+        counted = running & ~failed & ((track_curr == 2) | (track_curr == 3)) & (ok | (fm == 1))
+        equal = states_equal(ref, cur, G_ref, G_cur, tol_pois, tol_dens)
+        count = np.where(counted, np.where(equal, count + 1, 0), count)
+        becomes_ref = running & ~failed & (((track_curr == 1) & ok)
+                                           | ((track_curr == 3) & (ok | (fm == 1))))
+        ref = {f: np.where(becomes_ref[:, None], cur[f], ref[f]) for f in cur}
+        G_ref = np.where(becomes_ref, G_cur, G_ref)
+        static = running & (count >= MIN_COUNT_STATIC)
+        stop = np.where(failed, STOP_FAILED, np.where(static, STOP_STATIC, stop))
         first = False
         out["J"][:, k], out["J_ext"][:, k], out["V_int"][:, k] = J, J_ext, V_new
         out["converged"][:, k], out["iterations"][:, k], out["accepted"][:, k] = ok, it, keep

@@ -43,6 +43,9 @@ CASES = (
     # the internal voltage an unknown: the photovoltage at the open circuit after a light pulse,
     # a sweep through a series resistance and a shunt
     "zimt_tpv_light", "zimt_rseries_sweep_light",
+    # ZimT's automatic stop on the photovoltage after a pulse (Track 2 against the steady state
+    # before it, Track 3 against the step before)
+    "zimt_track_tpv_light", "zimt_track_tpv3_light",
 )
 
 

@@ -128,6 +128,25 @@ def test_a_series_resistance_beside_given_voltages_and_ions_in_a_batch():
     assert np.max(np.abs(r.J_ext[0] - o["J_ext"][0])) < 1e-10 * scale
 
 
+@pytest.mark.parametrize("case", ["zimt_track_tpv_light", "zimt_track_tpv3_light"])
+def test_the_automatic_stop(case):
+    """ZimT's automatic stop (Track 2 and 3, five equal states in a row) on the photovoltage
+    after a pulse: stopped where the oracle stops and as ZimT 5.36 within one step, the kept
+    steps' Vint to 1e-10 V of ZimT's (test_solver.py:782-799)."""
+    from jaxdd_b200.transient import STOP_STATIC
+    from tests.test_transient_oracle import zimt_track
+    setup, tvg, ref = zimt_case(case)
+    dev = build_device(setup, grid="simss")
+    r = solve_transient(prepare([dev]), tvg, bernoulli_name="simss", zimt_current=True)
+    o = zimt_track(dd.prepare([dev]), tvg)
+    rows = int(r.accepted[0].sum())
+    assert r.stop[0] == STOP_STATIC and abs(rows - len(ref)) <= 1 and rows < len(tvg.t)
+    np.testing.assert_array_equal(r.accepted, o["accepted"])
+    assert r.accepted[0, :rows].all() and r.converged[0, :rows].all()
+    rows = min(rows, len(ref))
+    assert np.max(np.abs(r.V_int[0, :rows] - ref["Vint"][:rows])) < 1e-10
+
+
 def test_config5_transient_matches_the_oracle():
     devs = [drawn_device(k) for k in (1, 3, 5)]
     tvg = transient_steps(40)

@@ -171,11 +171,54 @@ def test_a_series_resistance_in_time_reproduces_zimt():
     assert np.max(np.abs(r["V_int"][0] + dev.R_series * r["J_ext"][0] - tvg.Vext)) < 1e-9
 
 
+def zimt_track(batch, tvg):
+    """ZimT's steps with the automatic stop's controls (`convVar`, `tolPois`, `tolDens`)."""
+    return transient.solve_transient(batch, tvg.t, tvg.Vext, tvg.G_frac, tvg.track,
+                                     tvg.failure_mode, bernoulli_name="simss", zimt_current=True,
+                                     oc=tvg.oc, conv_var=tvg.conv_var, tol_pois=tvg.tol_pois,
+                                     tol_dens=tvg.tol_dens)
+
+
+@pytest.mark.parametrize("case", ["zimt_track_tpv_light", "zimt_track_tpv3_light"])
+def test_the_automatic_stop_reproduces_zimt(case):
+    """ZimT's automatic stop (five equal states in a row) on the photovoltage after a pulse:
+    each step compared with the steady state before the pulse (Track 1 there, 2 after it), and
+    each with the one before (Track 3); stopped as ZimT 5.36 within one step (its states
+    compare within tolPois 1e-12 V, where ZimT's own error decides the step), Vint of the kept
+    steps to 1e-10 V (test_solver.py:782-799)."""
+    setup, tvg, ref = zimt_case(case)
+    r = zimt_track(dd.prepare([build_device(setup, grid="simss")]), tvg)
+    rows = int(r["accepted"][0].sum())
+    assert r["stop"][0] == transient.STOP_STATIC and abs(rows - len(ref)) <= 1
+    assert rows < len(tvg.t)
+    assert r["accepted"][0, :rows].all() and r["converged"][0, :rows].all()
+    rows = min(rows, len(ref))
+    assert np.max(np.abs(r["V_int"][0, :rows] - ref["Vint"][:rows])) < 1e-10
+
+
+def test_states_compare_as_zimt_compares_them():
+    """`states_equal` as ZimT's `States_Are_Equal` with convVar 1 (test_solver.py:802-824):
+    never at another G_frac or with the potentials apart by tolPois, the densities each
+    within tolDens."""
+    base = {"V": np.zeros((1, 4)), "n": np.ones((1, 4)), "p": np.ones((1, 4)),
+            "a": np.zeros((1, 4)), "c": np.zeros((1, 4))}
+    G = np.ones(1)
+
+    def eq(B, GB=G):
+        return bool(transient.states_equal(base, B, G, GB, 1e-6, 1e-6)[0])
+    assert eq(base)
+    assert not eq(dict(base, n=np.ones((1, 4)) * (1 + 1e-5)))
+    assert eq(dict(base, n=np.ones((1, 4)) * (1 + 1e-7)))
+    assert not eq(base, np.full(1, 0.5))
+    assert not eq(dict(base, V=np.full((1, 4), 1e-6)))
+
+
 def test_what_the_transient_refuses():
     setup, tvg, _ = zimt_case("zimt_photo_light")
     b = dd.prepare([build_device(setup, grid="simss")])
     with pytest.raises(NotImplementedError, match="Track"):
-        transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3], [0, 1, 2])
+        transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3], [0, 1, 2],
+                                  conv_var=2)
     setup, tvg, _ = zimt_case("zimt_region_slow_light")
     b = dd.prepare([build_device(setup, grid="simss")])
     b["R_series"] = np.array([1e-4])
