@@ -411,6 +411,17 @@ def current(d, full, tr, bern, zimt, steady_traps=False, dU=None, dRi=None):
     `steady_traps`: the traps at their steady occupation; `dU`, `dRi`: each carrier's rates
     beyond it, bulk and interface, on every point (`tr["dU"]`, `tr["dRi"]`, impedance.py:313).
     Written for complex inputs too (complex-step derivatives), in the integral form."""
+    parts, _ = current_parts(d, full, tr, bern, zimt, steady_traps, dU, dRi)
+    total = sum(parts.values())
+    hh = d["h"][:, :full.shape[1] - 1]
+    return np.sum(hh * total, 1) / np.sum(hh, 1)
+
+
+def current_parts(d, full, tr, bern, zimt, steady_traps=False, dU=None, dRi=None):
+    """batch._current_parts over a step (batch.py:316-403): the current's parts on each
+    interval (B×(NP+1), SIMsalabim's sign), `Jn`, `Jp`, `Ja`, `Jc`, `JD`, and on the points what
+    ZimT's output columns take: `n`, `p`, the generation `gen`, each carrier's recombination `Rn`,
+    `Rp` (bulk, the direct included) and interface `Rin`, `Rip`."""
     g_frac = _col(d["g_frac"])
     V, n, p = full[..., 0], np.exp(full[..., 1]), np.exp(full[..., 2])
     Vt, x, h, L = _col(d["Vt"]), d["x"], d["h"], _col(d["L"])
@@ -477,20 +488,22 @@ def current(d, full, tr, bern, zimt, steady_traps=False, dU=None, dRi=None):
         return np.where(d["iface"], np.roll(J, 1, axis=1) + through, J)
 
     sign = -_col(d["left_elec"])
-    total = sign * (carrier(-1.0, V + d["offset_n"], n, d["mu_n"], Rn, Rin, tr["n"])
-                    + carrier(1.0, V + d["offset_p"], p, d["mu_p"], Rp, Rip, tr["p"]))
-    total = total + sign * ion_currents(d, full, tr, bern, width)
-    total = total + sign * d["eps"][:, :NP + 1] * (np.diff(V, axis=1) - np.diff(tr["V"], axis=1)) \
-        * dti / (L * h[:, :NP + 1])
-    hh = h[:, :NP + 1]
-    return np.sum(hh * total, 1) / np.sum(hh, 1)
+    Ja, Jc = ion_currents(d, full, tr, bern, width, apart=True)
+    parts = {"Jn": sign * carrier(-1.0, V + d["offset_n"], n, d["mu_n"], Rn, Rin, tr["n"]),
+             "Jp": sign * carrier(1.0, V + d["offset_p"], p, d["mu_p"], Rp, Rip, tr["p"]),
+             "Ja": sign * Ja, "Jc": sign * Jc,
+             "JD": sign * d["eps"][:, :NP + 1] * (np.diff(V, axis=1) - np.diff(tr["V"], axis=1))
+             * dti / (L * h[:, :NP + 1])}
+    points = {"n": n, "p": p, "gen": G * g_frac, "Rn": Rn, "Rp": Rp, "Rin": Rin, "Rip": Rip}
+    return parts, points
 
 
-def ion_currents(d, full, tr, bern, width):
+def ion_currents(d, full, tr, bern, width, apart=False):
     """batch._ion_currents (batch.py:421-483): each region's current over the step from its
     integral form with the densities' change as the integrand; 0 outside, every region's
     counted, or with `tr["ion_last"]` (B, true) each species' last region's alone (ZimT 5.36's
-    with several regions). The anions' and cations' summed, on the NP + 1 intervals."""
+    with several regions). The anions' and cations' summed, on the NP + 1 intervals, or with
+    `apart` each species' `(Ja, Jc)`."""
     ion = d["ion"]
     Vt, x, h, L = _col(d["Vt"]), d["x"], d["h"], _col(d["L"])
     V = full[..., 0]
@@ -500,7 +513,7 @@ def ion_currents(d, full, tr, bern, width):
     dti = _col(tr["dti"])
     masks, totals = dd._masks(ion)
     ka = ion["a_slots"].shape[1]
-    out = np.zeros((nb, NP + 1))
+    out = [np.zeros((nb, NP + 1)), np.zeros((nb, NP + 1))]
     e = np.arange(NP + 1)
     idx = np.arange(masks.shape[1])[None]
     last_a = np.max(np.where((totals > 0) & (idx < ka), idx, -1), 1)
@@ -541,7 +554,72 @@ def ion_currents(d, full, tr, bern, width):
             J = np.where(diff[:, None], flux, J)
         J = np.where(d["iface"], np.roll(J, 1, axis=1), J)
         counted = (totals[:, k] > 0) & (~only_last | (k == (last_a if anion else last_c)))
-        out = out + np.where((pair > 0) & counted[:, None], J, 0.0)
+        out[0 if anion else 1] = out[0 if anion else 1] + np.where(
+            (pair > 0) & counted[:, None], J, 0.0)
+    return tuple(out) if apart else out[0] + out[1]
+
+
+def columns(layers, d, parts, points, full, J, J_ext):
+    """transient._columns (transient.py:163-222): ZimT's tJFile columns beyond the voltages and
+    currents at one step, per device of the batch (`layers` each device's `(i0, i1)`): `errJ`,
+    the current's rms deviation over the grid from its average; per layer the QFLS averaged on
+    the grid, the photocurrent and each carrier's direct and bulk recombination as currents
+    (`EquiCurr`), and at each layer's right end the interface traps' recombination of each
+    carrier; the minority carriers' currents at the contacts, the shunt's, the ions' and the
+    displacement current averaged; each layer's voltage drop. Per-layer columns B×(most
+    layers), 0 past a device's own."""
+    nb, npts = full.shape[:2]
+    NP = npts - 2
+    x, h, L, Vt = d["x"], d["h"], d["L"], d["Vt"]
+    hh = h[:, :NP + 1]
+    total = sum(parts.values())
+    dev = np.concatenate([total, total[:, -1:]], 1) - _col(J)
+    out = {"errJ": np.sqrt(np.sum(dev ** 2, 1) / (NP + 1))}
+    nl = max(len(i0) for i0, _ in layers)
+    per = {k: np.zeros((nb, nl)) for k in ("QFLS", "Jphoto", "Jdir", "JbulkElec", "JbulkHoles",
+                                           "JintElec", "JintHoles", "VL")}
+    n, p, V = points["n"], points["p"], full[..., 0]
+    ni2 = d["rec"]["ni2"]
+    qfls = _col(Vt) * (np.log(n) + np.log(p) - np.log(ni2))
+    direct = d["rec"]["kd"] * (n * p - ni2)
+    hpad = np.concatenate([h, np.zeros((nb, npts - h.shape[1]))], 1)
+    for b, (i0, i1) in enumerate(layers):
+        def interior(v):
+            v = v.copy()
+            v[0] = v[-1] = 0.0
+            return v
+
+        for j, (a, e) in enumerate(zip(i0, i1)):
+            w = hh[b, a:e]
+            norm = np.sum(w) if np.sum(w) > 0 else 1.0
+
+            def average(v):
+                return np.sum(w * v[a:e]) / norm
+
+            def equi(v):
+                return Q * average(interior(v)) * (x[b, e] - x[b, a])
+
+            per["QFLS"][b, j] = average(0.5 * (qfls[b, :-1] + qfls[b, 1:]))
+            per["Jphoto"][b, j] = equi(points["gen"][b])
+            per["Jdir"][b, j] = equi(direct[b])
+            per["JbulkElec"][b, j] = equi(points["Rn"][b] - direct[b])
+            per["JbulkHoles"][b, j] = equi(points["Rp"][b] - direct[b])
+            nxt = e + 1 if e + 1 < npts else 0  # `roll`: the point after the layer's last
+            per["JintElec"][b, j] = Q * L[b] * hpad[b, e] * (points["Rin"][b, e]
+                                                            + points["Rin"][b, nxt])
+            per["JintHoles"][b, j] = Q * L[b] * hpad[b, e] * (points["Rip"][b, e]
+                                                             + points["Rip"][b, nxt])
+            per["VL"][b, j] = V[b, e] - V[b, a]
+    out.update(per)
+
+    def mean(v):
+        return np.sum(hh * v, 1) / np.sum(hh, 1)
+
+    Jn, Jp = parts["Jn"], parts["Jp"]
+    out["JminLeft"] = np.where(n[:, 0] < p[:, 0], Jn[:, 0], Jp[:, 0])
+    out["JminRight"] = np.where(n[:, -1] < p[:, -1], Jn[:, -1], Jp[:, -1])
+    out["JShunt"] = J_ext - J
+    out["Jnion"], out["Jpion"], out["JD"] = mean(parts["Ja"]), mean(parts["Jc"]), mean(parts["JD"])
     return out
 
 
@@ -762,7 +840,7 @@ def check_scope(d, oc=None, track=None, conv_var=None):
 
 def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, max_iter=200,
                     bernoulli_name="exact", zimt_current=False, zimt_ion_currents=False,
-                    oc=None, conv_var=1, tol_pois=1e-6, tol_dens=1e-6):
+                    oc=None, conv_var=1, tol_pois=1e-6, tol_dens=1e-6, layers=None):
     """transient.solve_transient / _solve_one (transient.py:270-465, 537-637) for every lane at
     once. `t`, `V`, `G_frac`, `track`: (S,) for every device or (B, S); `failure_mode` scalar
     or (B,). `zimt_ion_currents`: each species' last region's ion current alone, as ZimT 5.36
@@ -773,6 +851,8 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     start at 0 V where the first step is at the open circuit (transient.py:290-300, 389-405).
     `conv_var`, `tol_pois`, `tol_dens` (scalars or B): how ZimT's automatic stop compares two
     states (`TVG`'s `convVar`, `tolPois`, `tolDens`; only `convVar = 1` with `Track` 2 or 3).
+    `layers` (each device's `(i0, i1)`): also ZimT's tJFile columns of every step (`columns`,
+    as `out["columns"][name]`, B×S or B×S×layers).
     Returns a dict: `J`, `J_ext`, `V_int`, `converged`, `iterations`, `accepted` (B×S), `stop`
     (B: 0, `STOP_STATIC` or `STOP_FAILED`), and the final state (`y` B×NP×5, `logs`, `f_bulk`, `f_interface`)."""
     d = batch
@@ -822,6 +902,7 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     caps = _caps(Vt)
     out = {k: np.zeros((nb, S)) for k in ("J", "J_ext", "V_int")}
     v_cap = dd.STEP_CAPS[0] * Vt
+    cols = {}
     out.update(converged=np.zeros((nb, S), bool), iterations=np.zeros((nb, S), int),
                accepted=np.zeros((nb, S), bool))
     ma, mc = ion["a_slots"].sum(1), ion["c_slots"].sum(1)
@@ -895,6 +976,13 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
         stop = np.where(failed, STOP_FAILED, np.where(static, STOP_STATIC, stop))
         first = False
         out["J"][:, k], out["J_ext"][:, k], out["V_int"][:, k] = J, J_ext, V_new
+        if layers is not None:
+            fl = full_of(d, y_new, V_new, bern, dti_k)
+            parts, points = current_parts(dk, fl, trc, bern, zimt_current)
+            for name, v in columns(layers, d, parts, points, fl, J, J_ext).items():
+                cols.setdefault(name, np.zeros((nb, S) + v.shape[1:]))[:, k] = v
         out["converged"][:, k], out["iterations"][:, k], out["accepted"][:, k] = ok, it, keep
     out.update(stop=stop, y=y, logs=logs, f_bulk=fb, f_interface=fi)
+    if layers is not None:
+        out["columns"] = cols
     return out

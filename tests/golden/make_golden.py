@@ -46,6 +46,8 @@ CASES = (
     # ZimT's automatic stop on the photovoltage after a pulse (Track 2 against the steady state
     # before it, Track 3 against the step before)
     "zimt_track_tpv_light", "zimt_track_tpv3_light",
+    # the sweep with each layer's voltage drop written (`specialOutput = spv`)
+    "zimt_sweep_spv_light",
 )
 
 
