@@ -270,6 +270,11 @@ typedef struct dd_steps {
    * tolDens relative). NULL: no two states are equal (Track 2 and 3 never stop). */
   const double* tol_pois;
   const double* tol_dens;
+  /* For ZimT's tJFile columns (dd_transient_out.columns): each lane's layers, [3][n_layers]
+   * [lane_stride] (each layer's first point i0, its last i1, its thickness x[i1] - x[i0]),
+   * 1 <= n_layers <= 8 (i0 = -1 past a lane's own layers: its columns there 0). */
+  int32_t n_layers;
+  const double* layers;
 } dd_steps;
 
 /* Outputs of dd_transient (device pointers). Per step and lane [n_steps][lane_stride]: J (A/m^2,
@@ -307,6 +312,11 @@ typedef struct dd_transient_out {
   /* V_int [n_steps][lane_stride]: each step's internal voltage (the solution's with `vint`, else
    * the given one). NULL: not written. */
   double* V_int;
+  /* ZimT's tJFile columns of each step (jaxdd transient.py:163-222), [n_steps][7 + 8 n_layers]
+   * [lane_stride]: errJ, JminLeft, JminRight, JShunt, Jnion, Jpion, JD, then per layer (each
+   * n_layers wide) QFLS, Jphoto, Jdir, JbulkElec, JbulkHoles, JintElec, JintHoles (at the
+   * layer's right end), VL. NULL: none. */
+  double* columns;
 } dd_transient_out;
 
 /* A state to start from instead of the steady state at the first step (jaxdd's

@@ -42,6 +42,10 @@ EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve
 
 #: the transient's per-point record fields (include/jaxdd_b200.h DD_NT)
 DD_NT = 3
+#: the tJFile columns: the scalar ones, then 8 per layer, at most this many layers
+DD_COL_SCALARS, DD_COL_MAXL = 7, 8
+COL_SCALARS = ("errJ", "JminLeft", "JminRight", "JShunt", "Jnion", "Jpion", "JD")
+COL_LAYER = ("QFLS", "Jphoto", "Jdir", "JbulkElec", "JbulkHoles", "JintElec", "JintHoles", "VL")
 
 #: include/jaxdd_b200.h's per-layer and per-device parameter fields of dd_build
 LAYER_FIELDS = ("L", "eps_r", "E_c", "E_v", "N_c", "N_D", "N_A", "mu_n", "mu_p", "k_direct",
@@ -83,13 +87,15 @@ class DdSteps(ctypes.Structure):
                 ("zimt_ion_last", ctypes.c_int32), ("vint", ctypes.c_int32),
                 ("oc", ctypes.c_void_p), ("r_series", ctypes.c_void_p),
                 ("start_j_ext", ctypes.c_void_p), ("tol_pois", ctypes.c_void_p),
-                ("tol_dens", ctypes.c_void_p)]
+                ("tol_dens", ctypes.c_void_p), ("n_layers", ctypes.c_int32),
+                ("layers", ctypes.c_void_p)]
 
 
 class DdTransientOut(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in (
         "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs", "f_bulk",
-        "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface", "prof_dti", "V_int")]
+        "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface", "prof_dti", "V_int",
+        "columns")]
 
 
 class DdTransientInit(ctypes.Structure):

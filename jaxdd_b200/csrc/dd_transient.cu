@@ -93,6 +93,11 @@ struct Args {
   const double* tolp;    // [Bp]
   const double* told;    // [Bp]
   double* REF;           // [np+2][5][Bp]
+  // ZimT's tJFile columns of each step (nullptr: none): each lane's layers' first and last
+  // points and the columns [S][7 + 8 nlay][Bp]
+  const double* LAY;     // [3][nlay][Bp]: i0, i1, the thickness x[i1] - x[i0]
+  int nlay;
+  double* COL;
 };
 
 // ------------------------------------------------------------------------------------ current
@@ -146,10 +151,19 @@ struct Pert {
   int tn = 5, tf = 1;  // the strides of `tcur` (load_pert)
 };
 
+// The constants of the current's integral form that `current_t` finds in its pass: each
+// carrier's and each ion region's K (J_e = q K + the prefix of its steps), which regions count.
+template <int K>
+struct CurK {
+  double kc[2], ki[K];
+  int first[K];
+  bool counted[K];
+};
+
 template <int K, bool PERT = false>
 __device__ double current_t(const View& W, int cur, double Vint, int bef, double Vbef, double dti,
                             double dti_bef, const double* FB, const double* FI,
-                            const Pert* pt = nullptr) {
+                            const Pert* pt = nullptr, CurK<K>* ck = nullptr) {
   const Lane& L = W.L;
   const double mus = PERT ? pt->mus : 1.0;
   auto fb_at = [&](int k) {
@@ -321,9 +335,21 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
                                  sn * d0 * exp(sn * (c0.V + off0) * L.iVt)) - sn * dbl[s]) /
                         single[s];
       tot += Q * Kc * H + bH[s] + corr[s];
+      if (ck) ck->kc[s] = Kc;
     }
   } else {
     tot = dtot;
+  }
+  if (ck) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      ck->counted[k] = L.tot[k] > 0.0 && have[k] &&
+                       !(W.ion_last && k != (k < L.ka ? last_a : last_c));
+      ck->first[k] = first_k[k];
+      const double sn = k < L.ka ? -1.0 : 1.0;
+      const double sgl = is[k] > 0.0 ? is[k] : 1.0;
+      ck->ki[k] = (L.Vt * sn * (last_v[k] - first_v[k]) - sn * idb[k]) / sgl;
+    }
   }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
@@ -340,6 +366,200 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
   }
   tot += dti * disp / L.L;
   return -L.left * tot / H;
+}
+
+// ------------------------------------------------------------------------------------ columns
+//
+// ZimT's tJFile columns of a step (`transient._columns`, transient.py:163-222, from
+// `_current_parts`, batch.py:316-403): a second pass over the intervals with the constants of
+// `current_t`'s pass forms each interval's current as `_current_parts` does (each carrier's
+// q K plus the prefix of its steps, an interface's the interval's before it plus its traps';
+// each counted ion region's the same inside it; the displacement current), and from them the
+// current's rms deviation over the grid, the minority carriers' currents at the contacts and
+// the means; per layer (intervals i0 <= e < i1) the QFLS and, as currents, the generation and
+// the direct and bulk recombination averaged over the layer, at its last point the interface
+// traps' recombination, and its voltage drop. Columns: errJ, JminLeft, JminRight, JShunt,
+// Jnion, Jpion, JD, then per layer QFLS, Jphoto, Jdir, JbulkElec, JbulkHoles, JintElec,
+// JintHoles, VL (each nlay wide).
+constexpr int COL_MAXL = 8;  // the most layers a device's columns take
+constexpr int COL_SCALARS = 7;
+
+template <int K>
+__device__ __noinline__ void columns_t(const Args& a, const View& W, int cur, double Vint, int bef,
+                                       double Vbef, double dti, double dti_bef, double J,
+                                       double J_ext, int step) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = a.Bp, l = L.l, nl = a.nlay;
+  const double* FB = a.FB;
+  const double* FI = a.FI;
+  CurK<K> ck;
+  current_t<K>(W, cur, Vint, bef, Vbef, dti, dti_bef, FB, FI, nullptr, &ck);
+  int i0[COL_MAXL], i1[COL_MAXL];
+  double qf[COL_MAXL], hs[COL_MAXL], gen[COL_MAXL], dir[COL_MAXL], bn[COL_MAXL], bp[COL_MAXL];
+  double jin[COL_MAXL], jip[COL_MAXL], vl[COL_MAXL];
+  for (int j = 0; j < COL_MAXL; ++j) {
+    i0[j] = j < nl ? (int)a.LAY[(size_t)j * Bp + l] : -1;
+    i1[j] = j < nl ? (int)a.LAY[(size_t)(nl + j) * Bp + l] : -1;
+    qf[j] = hs[j] = gen[j] = dir[j] = bn[j] = bp[j] = jin[j] = jip[j] = vl[j] = 0.0;
+  }
+  const double QL = Q * L.L, sg = -L.left;
+  TP pa, pb, qa, qb;
+  load_point(W, cur, 0, Vint, pa);
+  contact_ions(W, cur, 0, dti, pa);
+  load_before(W, bef, 0, Vbef, qa);
+  contact_ions(W, bef, 0, dti_bef, qa);
+  double Ri_next[2] = {0, 0}, P[2] = {0, 0}, Jd_prev[2] = {0, 0}, iP[K], Jion_prev[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) { iP[k] = 0.0; Jion_prev[k] = 0.0; }
+  double dev2 = 0.0, ja = 0.0, jc = 0.0, jdm = 0.0, jmin_l = 0.0, jmin_r = 0.0, last_tot = 0.0;
+  for (int e = 0; e <= NP; ++e) {
+    const int kb = e + 1;
+    load_point(W, cur, kb, Vint, pb);
+    contact_ions(W, cur, kb, dti, pb);
+    load_before(W, bef, kb, Vbef, qb);
+    contact_ions(W, bef, kb, dti_bef, qb);
+    const double h = L.st(e, S_H);
+    const int ifk = (int)L.st(e, S_IFK);
+    double tRL[2] = {0, 0}, tRR[2] = {0, 0};
+    if (ifk >= 0) {
+      Iface t;
+      iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, FI[(size_t)e * Bp + l], dti, t, false,
+                   nullptr);
+      tRL[0] = t.v[0]; tRR[0] = t.v[1]; tRL[1] = t.v[2]; tRR[1] = t.v[3];
+    }
+    const double Ri_a[2] = {Ri_next[0] + tRL[0], Ri_next[1] + tRL[1]};
+    const double Ri_b[2] = {tRR[0], tRR[1]};
+    double Ue[2] = {0, 0}, Rb[2] = {0, 0};
+    if (e >= 1) {
+      double d0, d1, d2, d3;
+      bulk_rates(L, e, pa.c.n, pa.c.p, FB[(size_t)e * Bp + l], dti, Rb[0], Rb[1], d0, d1, d2, d3);
+      const double G = L.st(e, S_G) * L.gfrac;
+      Ue[0] = Rb[0] + Ri_a[0] - G + dti * (pa.c.n - qa.c.n);
+      Ue[1] = Rb[1] + Ri_a[1] - G + dti * (pa.c.p - qa.c.p);
+    }
+    const double width = W.zimt ? h : (e == 0 ? h : 0.5 * (L.st(e - 1, S_H) + h));
+    double Jc2[2];
+#pragma unroll
+    for (int s2 = 0; s2 < 2; ++s2) {
+      const double sn = s2 == 0 ? -1.0 : 1.0;
+      const double stp = e >= 1 ? sn * QL * width * Ue[s2] : 0.0;
+      P[s2] += stp;
+      const double through = sn * 0.5 * QL * h * (Ri_a[s2] + Ri_b[s2]);
+      double Jv;
+      if (!L.currdiff) {
+        const double pre = Q * ck.kc[s2] + P[s2];
+        Jv = ifk >= -1 ? pre - stp + through : pre;
+      } else {
+        const double Vga = pa.c.V + (s2 == 0 ? pa.c.offn : pa.c.offp);
+        const double Vgb = pb.c.V + (s2 == 0 ? pb.c.offn : pb.c.offp);
+        double Bf, Bb, t1, t2;
+        bern_pair(sn * (Vgb - Vga) * L.iVt, L.simss, Bf, Bb, t1, t2);
+        const double da = s2 == 0 ? pa.c.n : pa.c.p, db = s2 == 0 ? pb.c.n : pb.c.p;
+        const double Jf = sn * Q * L.st(e, s2 == 0 ? S_MUN : S_MUP) * L.Vt * (db * Bb - da * Bf) /
+                          (L.L * h);
+        Jv = ifk >= -1 ? Jd_prev[s2] + through : Jf;
+        Jd_prev[s2] = Jf;
+      }
+      Jc2[s2] = sg * Jv;
+    }
+    // the ions, region by region (counted ones), inside each region's intervals
+    double Jion[2] = {0, 0};
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!(L.tot[k] > 0.0)) continue;
+      const bool an = k < L.ka;
+      const int sk = an ? k : k - L.ka;
+      const double sn = an ? -1.0 : 1.0;
+      const bool ina = (an ? pa.c.sl.a : pa.c.sl.c) == sk;
+      const bool inb = (an ? pb.c.sl.a : pb.c.sl.c) == sk;
+      const double da = an ? pa.a : pa.c2, db = an ? pb.a : pb.c2;
+      const double qa_ = an ? qa.a : qa.c2;
+      double Jv = 0.0;
+      if (L.currdiff) {
+        double Bf, Bb, t1, t2;
+        bern_pair(sn * (pb.c.V - pa.c.V) * L.iVt, L.simss, Bf, Bb, t1, t2);
+        const double Jf = sn * Q * W.x(e, an ? T_MUA : T_MUC) * L.Vt * (db * Bb - da * Bf) /
+                          (L.L * h);
+        Jv = ifk >= -1 ? Jion_prev[k] : Jf;
+        Jion_prev[k] = Jf;
+      } else {
+        const double stp =
+            (ina && inb && e > ck.first[k]) ? sn * QL * width * dti * (da - qa_) : 0.0;
+        iP[k] += stp;
+        const double pre = Q * ck.ki[k] + iP[k];
+        Jv = ifk >= -1 ? pre - stp : pre;
+      }
+      if (ck.counted[k] && ina && inb) Jion[an ? 0 : 1] += sg * Jv;
+    }
+    const double JD = sg * W.x(e, T_EPS) * ((pb.c.V - pa.c.V) - (qb.c.V - qa.c.V)) * dti /
+                      (L.L * h);
+    const double total = Jc2[0] + Jc2[1] + Jion[0] + Jion[1] + JD;
+    dev2 += (total - J) * (total - J);
+    last_tot = total;
+    ja += h * Jion[0];
+    jc += h * Jion[1];
+    jdm += h * JD;
+    if (e == 0) jmin_l = pa.c.n < pa.c.p ? Jc2[0] : Jc2[1];
+    if (e == NP) jmin_r = pb.c.n < pb.c.p ? Jc2[0] : Jc2[1];
+    // per layer: the interval's averages, the points' rates, the interface's at its last point
+    const double qfls_a = L.Vt * (pa.c.lnn + pa.c.lnp - log(L.st(e, S_NI2)));
+    const double qfls_b = L.Vt * (pb.c.lnn + pb.c.lnp - log(L.st(kb, S_NI2)));
+    const double direct = e >= 1 ? L.st(e, S_KD) * (pa.c.n * pa.c.p - L.st(e, S_NI2)) : 0.0;
+    const double G = e >= 1 ? L.st(e, S_G) * L.gfrac : 0.0;
+    for (int j = 0; j < nl && j < COL_MAXL; ++j) {
+      if (i0[j] < 0) continue;  // past the lane's own layers
+      if (e >= i0[j] && e < i1[j]) {
+        qf[j] += h * 0.5 * (qfls_a + qfls_b);
+        hs[j] += h;
+        gen[j] += h * G;
+        dir[j] += h * direct;
+        bn[j] += h * (e >= 1 ? Rb[0] - direct : 0.0);
+        bp[j] += h * (e >= 1 ? Rb[1] - direct : 0.0);
+      }
+      if (e == i0[j]) vl[j] -= pa.c.V;
+      if (e == i1[j]) {
+        vl[j] += pa.c.V;
+        jin[j] += QL * h * Ri_a[0];
+        jip[j] += QL * h * Ri_a[1];
+      }
+      if (e == i1[j] + 1) {
+        const double hl = L.st(i1[j], S_H);
+        jin[j] += QL * hl * Ri_a[0];
+        jip[j] += QL * hl * Ri_a[1];
+      }
+      if (kb == i1[j] && kb == NP + 1) vl[j] += pb.c.V;
+    }
+    Ri_next[0] = Ri_b[0];
+    Ri_next[1] = Ri_b[1];
+    pa = pb;
+    qa = qb;
+  }
+  // the point after a layer's last where that is the right contact: its capture Ri_next
+  for (int j = 0; j < nl && j < COL_MAXL; ++j)
+    if (i0[j] >= 0 && i1[j] + 1 == NP + 1) {
+      const double hl = L.st(i1[j], S_H);
+      jin[j] += QL * hl * Ri_next[0];
+      jip[j] += QL * hl * Ri_next[1];
+    }
+  dev2 += (last_tot - J) * (last_tot - J);
+  const double H = L.Hsum;
+  const int ncol = COL_SCALARS + 8 * nl;
+  double* out = a.COL + (size_t)step * ncol * Bp + l;
+  out[0] = sqrt(dev2 / (NP + 1));
+  out[(size_t)1 * Bp] = jmin_l;
+  out[(size_t)2 * Bp] = jmin_r;
+  out[(size_t)3 * Bp] = J_ext - J;
+  out[(size_t)4 * Bp] = ja / H;
+  out[(size_t)5 * Bp] = jc / H;
+  out[(size_t)6 * Bp] = jdm / H;
+  for (int j = 0; j < nl && j < COL_MAXL; ++j) {
+    const double norm = hs[j] > 0.0 ? hs[j] : 1.0;
+    const double thick = a.LAY[(size_t)(2 * nl + j) * Bp + l];
+    double v[8] = {qf[j] / norm, Q * gen[j] / norm * thick, Q * dir[j] / norm * thick,
+                   Q * bn[j] / norm * thick, Q * bp[j] / norm * thick, jin[j], jip[j], vl[j]};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) out[(size_t)(COL_SCALARS + c * nl + j) * Bp] = v[c];
+  }
 }
 
 // ------------------------------------------------------------------------------------ tangents
@@ -1176,6 +1396,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const double J = jh[STALL_STEPS];
     const double J_ext = J + L.Gshunt * Vi;
     if (a.prof_state) write_profile(a, W, bn, k, Vi, dti);
+    if (a.COL) columns_t<K>(a, W, bn, Vi, bk, V_now, dti, dti_now, J, J_ext, k);
     // ---- ZimT's main loop (transient.py:419-445)
     const bool running = stop == 0;
     const bool failed = running && !ok && (fm == 0 || (fm == 2 && track_curr == 1));
@@ -1399,6 +1620,8 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.oc = steps->oc; a.rser = steps->r_series; a.jext0 = steps->start_j_ext;
   a.Vout = out->V_int;
   a.tolp = steps->tol_pois; a.told = steps->tol_dens;
+  a.LAY = steps->layers; a.nlay = steps->n_layers; a.COL = out->columns;
+  if (a.COL && (!a.LAY || a.nlay < 1 || a.nlay > dd::tr::COL_MAXL)) return DD_ERR_ARGS;
   {
     const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
     a.REF = reinterpret_cast<double*>(w + y + fb + fi + cd + tan) -

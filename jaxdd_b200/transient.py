@@ -28,8 +28,8 @@ from . import _lib
 from .batch import Batch, _gpu, descriptor, initial_state
 from .simss_input import TVG
 
-__all__ = ["STOP_FAILED", "STOP_STATIC", "ChargeGradients", "TransientResult", "TransientState", "Work",
-           "charge_gradients", "solve_transient"]
+__all__ = ["STOP_FAILED", "STOP_STATIC", "ChargeGradients", "TransientResult", "TransientState",
+           "Work", "charge_gradients", "solve_transient", "tj_columns"]
 
 #: `TransientResult.stop`: a failed step ended the run (transient.py:240)
 STOP_STATIC, STOP_FAILED = 1, 2
@@ -63,8 +63,9 @@ class TransientResult:
     stop found the state static, or `STOP_FAILED`); `t` each step's
     time; `final` the last state kept; with `profiles=True` `profiles` `{"V", "n", "p", "anion",
     "cation", "f_bulk", "f_interface", "dti"}` (devices × steps × points, or per device where
-    the grids differ), from which `state(k)` is step k's state. ZimT's other tJFile columns are
-    not built (`columns` empty)."""
+    the grids differ), from which `state(k)` is step k's state. `columns` ZimT's other tJFile
+    columns (jaxdd transient.py:163-222; devices × steps, the per-layer ones devices × steps ×
+    the batch's most layers), `n_layers` each device's; `tj_columns` names them as ZimT does."""
 
     J: np.ndarray
     J_ext: np.ndarray
@@ -78,6 +79,7 @@ class TransientResult:
     final: TransientState
     columns: dict
     profiles: dict | None = None
+    n_layers: np.ndarray | None = None
 
     def state(self, k: int) -> TransientState:
         """Every device's state at step `k` (jaxdd transient.py:124-135): the step's solution,
@@ -203,7 +205,8 @@ class Work:
     def __init__(self, batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
                  bernoulli_name: str = "exact", zimt_current: bool = False,
                  gradients: bool = False, profiles: bool = False, initial=None,
-                 zimt_ion_currents: bool = False, vint: bool = False):
+                 zimt_ion_currents: bool = False, vint: bool = False,
+                 columns: bool = False):
         import torch
         from .adjoint import plan as _plan
         devs = batch["devices"]
@@ -272,6 +275,21 @@ class Work:
         gv0[lanes] = batch["G_shunt"] * V0
         self.gv0 = torch.from_numpy(gv0).to(cuda)
         self.jext0 = torch.zeros(Bp, dtype=torch.float64, device=cuda)
+        # ZimT's tJFile columns: each lane's layers (first and last point, thickness)
+        self.n_layers = np.array([len(d.i0) for d in devs])
+        self.nl = int(self.n_layers.max()) if columns else 0
+        if columns:
+            if self.nl > _lib.DD_COL_MAXL:
+                raise NotImplementedError(f"the tJFile columns of more than "
+                                          f"{_lib.DD_COL_MAXL} layers")
+            lay = np.zeros((3, self.nl, Bp))
+            lay[0] = -1.0
+            for k, d in enumerate(devs):
+                m = len(d.i0)
+                lay[0, :m, lanes[k]] = d.i0
+                lay[1, :m, lanes[k]] = d.i1
+                lay[2, :m, lanes[k]] = [d.x[b] - d.x[a] for a, b in zip(d.i0, d.i1)]
+            self.lay = torch.from_numpy(lay).to(cuda)
         tl = np.zeros((2, Bp))  # the automatic stop's tolPois and tolDens
         tl[:, lanes] = tols.T
         self.tols = torch.from_numpy(tl).to(cuda)
@@ -292,6 +310,8 @@ class Work:
             "accepted": torch.empty((S, Bp), dtype=u8, device=cuda),
             "stop": torch.empty(Bp, dtype=i32, device=cuda),
             "V_int": torch.empty((S, Bp), dtype=f64, device=cuda),
+            **({"columns": torch.zeros((S, _lib.DD_COL_SCALARS + 8 * self.nl, Bp), dtype=f64,
+                                       device=cuda)} if self.nl else {}),
             "state": torch.empty((nodes, 5, Bp), dtype=f64, device=cuda),
             "logs": torch.zeros((_lib.DD_MAXK, Bp), dtype=f64, device=cuda),
             "f_bulk": torch.empty((nodes, Bp), dtype=f64, device=cuda),
@@ -357,12 +377,13 @@ class Work:
                              self.gv.data_ptr(), self.trk.data_ptr(), self.fm.data_ptr(),
                              self.zimt, self.ion_last, int(self.vint), self.ocv.data_ptr(),
                              self.rser.data_ptr(), self.jext0.data_ptr(), self.tols[0].data_ptr(),
-                             self.tols[1].data_ptr())
+                             self.tols[1].data_ptr(), self.nl,
+                             self.lay.data_ptr() if self.nl else None)
         o = self.out
         out = _lib.DdTransientOut(*(o[k].data_ptr() if k in o else None for k in (
             "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",
             "f_bulk", "f_iface", "Q", "dQ", "prof_state", "prof_f_bulk", "prof_f_iface",
-            "prof_dti", "V_int")))
+            "prof_dti", "V_int", "columns")))
         opts = _lib.DdOpts(float(self.tol), int(self.max_iter), int(self.max_iter), 0,
                            self.bern, _lib.DD_MODE_BATCH, 0, 0)
         desc = descriptor(self.batch, g, self.plan.y0)
@@ -378,7 +399,7 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
                     bernoulli_name: str = "exact", zimt_ion_currents: bool = False,
                     ions=None, vint=None, zimt_current: bool = False, recycle=None,
                     profiles: bool = False, ion_flux: str = "electrochemical",
-                    initial=None) -> TransientResult:
+                    initial=None, columns: bool = True) -> TransientResult:
     """A batch (`prepare`) through ZimT's time steps `tvg` (a `TVG`, or one per device, all of
     one length): jaxdd's `solve_transient` (transient.py:537-637) with the same arguments.
     `zimt_current`: ZimT's sums in the integral current (each point's change over the interval
@@ -395,7 +416,9 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
     voltage is an unknown of every device's steps (`vint`, also forced by `vint=True`): its row
     the external current at the open circuit, else `V_int + J_ext R_series = V_ext`. Not built
     (raise `NotImplementedError`): `recycle`; the internal voltage an unknown with an ion region
-    that reaches a contact. `ions` is accepted for the
+    that reaches a contact. `columns` (this build's switch, on by default as jaxdd always forms
+    them): ZimT's tJFile columns of every step in `TransientResult.columns`, from one more pass
+    over each step's solution on the GPU. `ions` is accepted for the
     reference's signature: the ions are unknowns of every step here, which leaves devices
     without mobile ions as they are."""
     if recycle is not None:
@@ -405,7 +428,7 @@ def solve_transient(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
     del ions
     work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
                 zimt_current=zimt_current, profiles=profiles, initial=initial,
-                zimt_ion_currents=zimt_ion_currents, vint=bool(vint))
+                zimt_ion_currents=zimt_ion_currents, vint=bool(vint), columns=columns)
     o, _ = work.run()
     return result(work, o)
 
@@ -464,9 +487,40 @@ def result(work: Work, o) -> TransientResult:
         profiles = {name: _stack([np.stack([st[name][k] for st in steps]) for k in range(n)])
                     for name in steps[0]}
         profiles["dti"] = o["prof_dti"].cpu().numpy()[:, lanes].T
+    columns = {}
+    if "columns" in o:
+        c = o["columns"].cpu().numpy()[..., lanes]  # steps × columns × devices
+        nl = work.nl
+        for q, name in enumerate(_lib.COL_SCALARS):
+            columns[name] = c[:, q].T
+        for q, name in enumerate(_lib.COL_LAYER):
+            base = _lib.DD_COL_SCALARS + q * nl
+            columns[name] = np.transpose(c[:, base:base + nl], (2, 0, 1))
     return TransientResult(J=J, J_ext=J_ext, V_int=V_int, V_ext=V_ext, converged=ok,
-                           iterations=its, accepted=acc, stop=stop, t=t, final=final, columns={},
-                           profiles=profiles)
+                           iterations=its, accepted=acc, stop=stop, t=t, final=final,
+                           columns=columns, profiles=profiles, n_layers=work.n_layers)
+
+
+def tj_columns(result: TransientResult, k: int = 0, spv: bool = False) -> dict:
+    """Device `k`'s steps as ZimT 5.36's tJFile names its columns, in its order (jaxdd
+    transient.py:228-250): `Vext Jext errJ Vint Jint`, per layer `QFLS`, `Jphoto`, `Jdir`,
+    `JbulkElec`, `JbulkHoles`, per interface `JintElec`, `JintHoles`, then `JminLeft JminRight
+    JShunt Jnion Jpion JD`; with `spv` each layer's voltage drop `VL1`, `VL2`, ..."""
+    if not result.columns:
+        raise ValueError("no columns: solve_transient(..., columns=True)")
+    c = {name: np.asarray(v)[k] for name, v in result.columns.items()}
+    nl = int(result.n_layers[k])
+    out = {"Vext": result.V_ext[k], "Jext": result.J_ext[k], "errJ": c["errJ"],
+           "Vint": result.V_int[k], "Jint": result.J[k]}
+    for name in ("QFLS", "Jphoto", "Jdir", "JbulkElec", "JbulkHoles"):
+        out.update({f"{name}L{j + 1}": c[name][:, j] for j in range(nl)})
+    for name in ("JintElec", "JintHoles"):
+        out.update({f"{name}L{j + 1}L{j + 2}": c[name][:, j] for j in range(nl - 1)})
+    out.update({name: c[name] for name in ("JminLeft", "JminRight", "JShunt", "Jnion", "Jpion",
+                                           "JD")})
+    if spv:
+        out.update({f"VL{j + 1}": c["VL"][:, j] for j in range(nl)})
+    return out
 
 
 def _states(devs, state, fb, fi) -> dict:

@@ -147,6 +147,43 @@ def test_the_automatic_stop(case):
     assert np.max(np.abs(r.V_int[0, :rows] - ref["Vint"][:rows])) < 1e-10
 
 
+@pytest.mark.parametrize("case", ["zimt_photo_light", "zimt_sweep_diff_light",
+                                  "zimt_iface_sweep_light", "zimt_ions_slow_light",
+                                  "zimt_rseries_sweep_light", "zimt_sweep_spv_light"])
+def test_zimts_columns(case):
+    """ZimT's tJFile columns (`TransientResult.columns`, `tj_columns`) on the GPU against ZimT
+    5.36's own at the reference's tolerances (test_solver.py:517-541) and against the oracle's
+    (`transient.columns`): the currents to 1e-9 of the scale, the voltages to 1e-9 V; errJ
+    (the rms of each interval's current about the mean, which the densities below the floor
+    move: 2.7e-6 of the scale seen after the light switches) and the QFLS at the reference's
+    bars against ZimT."""
+    from jaxdd_b200.transient import tj_columns
+    from tests.test_transient_oracle import COLUMN_CASES, check_columns, tj_named
+    setup, tvg, ref = zimt_case(case)
+    dev = build_device(setup, grid="simss")
+    r = solve_transient(prepare([dev]), tvg, bernoulli_name="simss", zimt_current=True)
+    assert r.converged.all()
+    nl = len(dev.i0)
+    qfls, steady = COLUMN_CASES[case]
+    check_columns(r.columns, 0, nl, ref, qfls, steady)
+    o = transient.solve_transient(dd.prepare([dev]), tvg.t, tvg.Vext, tvg.G_frac, tvg.track,
+                                  tvg.failure_mode, bernoulli_name="simss", zimt_current=True,
+                                  oc=tvg.oc, layers=[(dev.i0, dev.i1)])
+    mine, theirs = tj_named(r.columns, 0, nl, True), tj_named(o["columns"], 0, nl, True)
+    scale = max(np.max(np.abs(ref["Jext"])), np.max(ref["JphotoL2"]))
+    rows = np.ones(len(ref), bool) if steady else ref["t"] > 0
+    for name, v in mine.items():
+        err = np.abs(v - theirs[name])
+        if name.startswith("QFLS"):
+            assert np.max(err[rows]) < qfls, name
+        elif name == "errJ":
+            assert np.max(err) < 1e-5 * scale, name
+        else:
+            assert np.max(err) < (1e-9 if name.startswith("V") else 1e-9 * scale), name
+    named = tj_columns(r, 0, spv="VL1" in ref.dtype.names)
+    assert set(named) | {"t", "G_frac"} == set(ref.dtype.names)
+
+
 def test_config5_transient_matches_the_oracle():
     devs = [drawn_device(k) for k in (1, 3, 5)]
     tvg = transient_steps(40)
