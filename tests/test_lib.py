@@ -133,3 +133,46 @@ def test_the_header_compiles_as_c():
     r = subprocess.run([gcc, "-x", "c", "-std=c99", "-Wall", "-Werror", "-fsyntax-only",
                         str(ROOT / "include" / "jaxdd_b200.h")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_the_transient_refuses_inconsistent_arguments_before_any_launch():
+    """`dd_transient`'s checks, which return before any CUDA call: a start or a given state
+    half given, profiles half asked, the internal voltage an unknown without its steps' data or
+    with the gradients, columns without layers, and a workspace below its query. The pointers
+    are placeholders the checks never read through."""
+    import ctypes
+    so = _lib.lib()
+    desc = _lib.DdBatch(32, 32, 100, 1, 1, 1, 1, 1, 1)
+    size = ctypes.c_size_t(0)
+    assert so.dd_transient_workspace_bytes(ctypes.byref(desc), ctypes.byref(size)) == 0
+    ws = size.value
+    opts = _lib.DdOpts(1e-10, 60, 60, 0, 0, 0, 0, 0)
+
+    def steps(**kw):
+        base = dict(n_steps=4, stride=0, t=1, v=1, g_frac=1, track=1, failure_mode=1)
+        base.update(kw)
+        return _lib.DdSteps(**base)
+
+    def out(**kw):
+        base = {k: 1 for k in ("J", "J_ext", "converged", "iterations", "accepted", "stop",
+                               "state", "logs")}
+        base.update(kw)
+        return _lib.DdTransientOut(**base)
+
+    def call(st=None, o=None, start=1, logs=1, init=None, bytes_=ws):
+        return so.dd_transient(ctypes.byref(desc), 1, ctypes.byref(st or steps()), start, logs,
+                               init, ctypes.byref(opts), ctypes.byref(o or out()), 1, bytes_,
+                               None)
+
+    ARGS, WORKSPACE = 1, 2
+    assert call(start=None) == ARGS  # no start and no given state
+    half = _lib.DdTransientInit(1, 1, None, 1)
+    assert call(init=ctypes.byref(half)) == ARGS
+    assert call(o=out(prof_state=1, prof_f_bulk=1)) == ARGS  # profiles half asked
+    assert call(st=steps(vint=1)) == ARGS  # the internal voltage without its steps' data
+    vint = dict(vint=1, oc=1, r_series=1, start_j_ext=1)
+    assert call(st=steps(**vint), o=out(Q=1, dQ=1)) == ARGS  # and with the gradients
+    assert call(st=steps(stride=7)) == ARGS
+    assert call(o=out(columns=1)) == ARGS  # columns without layers
+    assert call(st=steps(n_layers=9, layers=1), o=out(columns=1)) == ARGS  # too many layers
+    assert call(bytes_=ws - 1) == WORKSPACE
