@@ -253,7 +253,7 @@ typedef struct dd_steps {
   const double* v;             /* internal voltage, V */
   const double* g_frac;        /* generation factor */
   const int32_t* track;        /* ZimT's Track 0-3 (1 the reference state; 2 and 3 the automatic
-                                  stop on five equal states in a row, `convVar` 1) */
+                                  stop on five equal states in a row, `conv_var` below) */
   const int32_t* failure_mode; /* [lane_stride]: 0 stop at a failed step, 1 keep it, 2 skip it */
   int32_t zimt_sums;           /* 1: ZimT's sums in the integral current (each point's change over
                                   the interval after it); 0: over its control volume (jaxdd's) */
@@ -275,6 +275,10 @@ typedef struct dd_steps {
    * 1 <= n_layers <= 8 (i0 = -1 past a lane's own layers: its columns there 0). */
   int32_t n_layers;
   const double* layers;
+  /* [lane_stride] each: ZimT's convVar (1 the densities, 2 the currents within tol_curr or the
+   * smaller errJ of the two states, 3 either, 4 both) and tolCurr (A/m^2). NULL: convVar 1. */
+  const int32_t* conv_var;
+  const double* tol_curr;
 } dd_steps;
 
 /* Outputs of dd_transient (device pointers). Per step and lane [n_steps][lane_stride]: J (A/m^2,

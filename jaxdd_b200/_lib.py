@@ -88,7 +88,8 @@ class DdSteps(ctypes.Structure):
                 ("oc", ctypes.c_void_p), ("r_series", ctypes.c_void_p),
                 ("start_j_ext", ctypes.c_void_p), ("tol_pois", ctypes.c_void_p),
                 ("tol_dens", ctypes.c_void_p), ("n_layers", ctypes.c_int32),
-                ("layers", ctypes.c_void_p)]
+                ("layers", ctypes.c_void_p), ("conv_var", ctypes.c_void_p),
+                ("tol_curr", ctypes.c_void_p)]
 
 
 class DdTransientOut(ctypes.Structure):

@@ -92,6 +92,8 @@ struct Args {
   // reference state's V, n, p, a, c on every point
   const double* tolp;    // [Bp]
   const double* told;    // [Bp]
+  const int32_t* convv;  // [Bp]: ZimT's convVar (nullptr: 1, the densities)
+  const double* tolc;    // [Bp]: tolCurr (A/m^2)
   double* REF;           // [np+2][5][Bp]
   // ZimT's tJFile columns of each step (nullptr: none): each lane's layers' first and last
   // points and the columns [S][7 + 8 nlay][Bp]
@@ -387,7 +389,7 @@ constexpr int COL_SCALARS = 7;
 template <int K>
 __device__ __noinline__ void columns_t(const Args& a, const View& W, int cur, double Vint, int bef,
                                        double Vbef, double dti, double dti_bef, double J,
-                                       double J_ext, int step) {
+                                       double J_ext, int step, double* err = nullptr) {
   const Lane& L = W.L;
   const int NP = L.NP, Bp = a.Bp, l = L.l, nl = a.nlay;
   const double* FB = a.FB;
@@ -542,6 +544,8 @@ __device__ __noinline__ void columns_t(const Args& a, const View& W, int cur, do
       jip[j] += QL * hl * Ri_next[1];
     }
   dev2 += (last_tot - J) * (last_tot - J);
+  if (err) *err = sqrt(dev2 / (NP + 1));
+  if (!a.COL) return;
   const double H = L.Hsum;
   const int ncol = COL_SCALARS + 8 * nl;
   double* out = a.COL + (size_t)step * ncol * Bp + l;
@@ -885,7 +889,7 @@ __device__ __forceinline__ void summary_at(const View& W, int buf, int i, double
 // and the last kept one (buffer `buf`): the potentials within tolPois (the Euclidean norm over
 // the grid), each density relatively within tolDens. The generation factors compared apart.
 __device__ __noinline__ bool states_equal(const Args& a, const View& W, int buf, double Vint,
-                                          double dti) {
+                                          double dti, int cv, double dJ, double err) {
   const Lane& L = W.L;
   const int NP = L.NP, Bp = a.Bp, l = L.l;
   double dv = 0.0, d2[4] = {0, 0, 0, 0}, c2[4] = {0, 0, 0, 0}, r2[4] = {0, 0, 0, 0};
@@ -903,14 +907,18 @@ __device__ __noinline__ bool states_equal(const Args& a, const View& W, int buf,
       r2[f] += r * r;
     }
   }
-  bool eq = sqrt(dv) < a.tolp[l];
+  bool dens = true;
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     const double scale = 0.5 * (sqrt(c2[f]) + sqrt(r2[f]));
     const double rel = scale > 0.0 ? sqrt(d2[f]) / scale : 0.0;
-    eq = eq && rel < a.told[l];
+    dens = dens && rel < a.told[l];
   }
-  return eq;
+  // by convVar: the densities (1), the currents within tolCurr or the smaller errJ (2), either
+  // (3), both (4)
+  const bool curr = cv != 1 && fabs(dJ) <= fmax(a.tolc[l], err);
+  const bool by = cv == 1 ? dens : cv == 2 ? curr : cv == 3 ? (curr || dens) : (curr && dens);
+  return sqrt(dv) < a.tolp[l] && by;
 }
 
 __device__ __noinline__ void write_ref(const Args& a, const View& W, int buf, double Vint,
@@ -1065,6 +1073,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   double J_ext_now = given ? a.init_scal[(size_t)2 * Bp + l] : (VINT ? a.jext0[l] : 0.0);
   int track_curr = 0, stop = 0, count = 0;
   double G_cur = -1.0, G_ref = -1.0;  // the generation factors of the kept and reference states
+  // and their currents and errJ, for convVar 2-4
+  double J_cur = 0.0, J_ref = 0.0, err_cur = 0.0, err_ref = 0.0;
+  const int cv = a.convv && a.tolc ? a.convv[l] : 1;
   bool first = true;
   const double capV = CAP_V * L.Vt;
 
@@ -1396,7 +1407,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const double J = jh[STALL_STEPS];
     const double J_ext = J + L.Gshunt * Vi;
     if (a.prof_state) write_profile(a, W, bn, k, Vi, dti);
-    if (a.COL) columns_t<K>(a, W, bn, Vi, bk, V_now, dti, dti_now, J, J_ext, k);
+    double err_k = 0.0;  // the step's errJ, where its convVar compares currents
+    if (a.COL || cv != 1)
+      columns_t<K>(a, W, bn, Vi, bk, V_now, dti, dti_now, J, J_ext, k, cv != 1 ? &err_k : nullptr);
     // ---- ZimT's main loop (transient.py:419-445)
     const bool running = stop == 0;
     const bool failed = running && !ok && (fm == 0 || (fm == 2 && track_curr == 1));
@@ -1465,6 +1478,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       track_curr = a.track[so];
       t_last = t_k;
       G_cur = L.gfrac;
+      J_cur = J;
+      err_cur = err_k;
     }
     // ZimT's automatic stop by the last state kept (transient.py:432-442): Track 1 makes it the
     // reference where the step converged; 2 and 3 count equal states in a row (where the step
@@ -1472,7 +1487,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const bool counted = running && !failed && (track_curr == 2 || track_curr == 3) &&
                          (ok || fm == 1);
     if (counted)
-      count = (a.tolp && a.told && G_ref == G_cur && states_equal(a, W, bk, V_now, dti_now))
+      count = (a.tolp && a.told && G_ref == G_cur &&
+               states_equal(a, W, bk, V_now, dti_now, cv, J_ref - J_cur, fmin(err_ref, err_cur)))
                   ? count + 1
                   : 0;
     const bool becomes_ref = running && !failed &&
@@ -1480,6 +1496,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     if (becomes_ref && a.REF) {
       write_ref(a, W, bk, V_now, dti_now);
       G_ref = G_cur;
+      J_ref = J_cur;
+      err_ref = err_cur;
     }
     if (failed) stop = STOP_FAILED;
     else if (running && count >= MIN_COUNT_STATIC) stop = STOP_STATIC;
@@ -1620,6 +1638,7 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   a.oc = steps->oc; a.rser = steps->r_series; a.jext0 = steps->start_j_ext;
   a.Vout = out->V_int;
   a.tolp = steps->tol_pois; a.told = steps->tol_dens;
+  a.convv = steps->conv_var; a.tolc = steps->tol_curr;
   a.LAY = steps->layers; a.nlay = steps->n_layers; a.COL = out->columns;
   if (a.COL && (!a.LAY || a.nlay < 1 || a.nlay > dd::tr::COL_MAXL)) return DD_ERR_ARGS;
   {

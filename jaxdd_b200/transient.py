@@ -13,8 +13,7 @@ with `initial=` (a `TransientState`) the devices start from that state instead o
 
 The voltage is given at every step, or with an open circuit or a series resistance the internal
 voltage is an unknown of each step's Newton solve. Refused (`NotImplementedError`), not
-approximated: ZimT's automatic stop (`Track` 2 or 3) with `convVar` 2-4 (the states' currents
-compared by errJ), photon recycling.
+approximated: photon recycling.
 """
 
 from __future__ import annotations
@@ -165,15 +164,12 @@ def _checked_initial(initial: TransientState, devs, t) -> dict:
 def _steps(tvgs: list[TVG]):
     if len({len(x.t) for x in tvgs}) != 1:
         raise ValueError("one tVG for the batch, or one per device, all of one length")
-    for x in tvgs:
-        if np.any(np.asarray(x.track) > 1) and x.conv_var != 1:
-            raise NotImplementedError("Track 2 or 3 with convVar 2-4 (states compared by their "
-                                      "currents and ZimT's errJ): not built")
     t, V, G, track = (np.stack([np.asarray(getattr(x, k), dtype=float) for x in tvgs])
                       for k in ("t", "Vext", "G_frac", "track"))
     oc = np.stack([np.asarray(x.oc, dtype=bool) for x in tvgs])
     fm = np.array([x.failure_mode for x in tvgs], dtype=np.int32)
-    tols = np.array([[x.tol_pois, x.tol_dens] for x in tvgs], dtype=float)
+    tols = np.array([[x.tol_pois, x.tol_dens, x.tol_curr, x.conv_var] for x in tvgs],
+                    dtype=float)
     return t, np.where(oc, 0.0, V), G, track.astype(np.int32), fm, oc, tols
 
 
@@ -290,9 +286,12 @@ class Work:
                 lay[1, :m, lanes[k]] = d.i1
                 lay[2, :m, lanes[k]] = [d.x[b] - d.x[a] for a, b in zip(d.i0, d.i1)]
             self.lay = torch.from_numpy(lay).to(cuda)
-        tl = np.zeros((2, Bp))  # the automatic stop's tolPois and tolDens
-        tl[:, lanes] = tols.T
+        tl = np.zeros((3, Bp))  # the automatic stop's tolPois, tolDens and tolCurr
+        tl[:, lanes] = tols[:, :3].T
         self.tols = torch.from_numpy(tl).to(cuda)
+        cvl = np.ones(Bp, dtype=np.int32)  # and its convVar
+        cvl[lanes] = tols[:, 3].astype(np.int32)
+        self.cv = torch.from_numpy(cvl).to(cuda)
         self.tv, self.vv, self.gv = (torch.from_numpy(np.ascontiguousarray(c)).to(cuda)
                                      for c in cols)
         self.trk = torch.from_numpy(np.ascontiguousarray(tr, dtype=np.int32)).to(cuda)
@@ -378,7 +377,8 @@ class Work:
                              self.zimt, self.ion_last, int(self.vint), self.ocv.data_ptr(),
                              self.rser.data_ptr(), self.jext0.data_ptr(), self.tols[0].data_ptr(),
                              self.tols[1].data_ptr(), self.nl,
-                             self.lay.data_ptr() if self.nl else None)
+                             self.lay.data_ptr() if self.nl else None, self.cv.data_ptr(),
+                             self.tols[2].data_ptr())
         o = self.out
         out = _lib.DdTransientOut(*(o[k].data_ptr() if k in o else None for k in (
             "J", "J_ext", "converged", "iterations", "accepted", "stop", "state", "logs",

@@ -13,8 +13,8 @@ product imports it.
 
 Scope (the rest is refused, never approximated): the voltage given at every step, or the
 internal voltage an unknown of each step (the open circuit, a series resistance); ZimT's
-automatic stop (`Track` 2, 3) with `convVar = 1`; no photon recycling, no free ends, no ion
-sites, the steady scope of `oracle.dd` otherwise. An ion region that reaches a contact takes the
+automatic stop (`Track` 2, 3); no photon recycling, no free ends, no ion sites, the steady
+scope of `oracle.dd` otherwise. An ion region that reaches a contact takes the
 contact's density from its neighbour (`ion_full`). With no mobile ions the same 5-column system
 holds the ions' rows at 0 (identity rows); the solution is the reference's 3-column one.
 
@@ -810,10 +810,12 @@ def summary(d, full):
             "a": np.exp(full[..., 3]) * ma, "c": np.exp(full[..., 4]) * mc}
 
 
-def states_equal(A, B, GA, GB, tol_pois, tol_dens):
-    """ZimT's `States_Are_Equal` with `convVar = 1` (transient.py:243-262): the same `G_frac`,
-    the potentials within `tolPois` (V, the Euclidean norm over the grid), each density
-    relatively within `tolDens`."""
+def states_equal(A, B, GA, GB, tol_pois, tol_dens, conv_var=1, tol_curr=None, JA=None, JB=None,
+                 errA=None, errB=None):
+    """ZimT's `States_Are_Equal` (transient.py:243-262): the same `G_frac`, the potentials within
+    `tolPois` (V, the Euclidean norm over the grid), then by `convVar` each density relatively
+    within `tolDens` (1), the currents `J` within `tolCurr` or the smaller of the two states'
+    errJ (2), either (3) or both (4)."""
     def norm(v):
         return np.sqrt(np.sum(v ** 2, axis=1))
 
@@ -822,7 +824,14 @@ def states_equal(A, B, GA, GB, tol_pois, tol_dens):
         return np.where(scale > 0, norm(a - b) / np.where(scale > 0, scale, 1.0), 0.0)
 
     dens = np.all(np.stack([rel(A[k], B[k]) for k in ("n", "p", "a", "c")]) < tol_dens, 0)
-    return (GA == GB) & (norm(A["V"] - B["V"]) < tol_pois) & dens
+    cv = np.asarray(conv_var)
+    if np.all(cv == 1):
+        by = dens
+    else:
+        curr = np.abs(JA - JB) <= np.maximum(tol_curr, np.minimum(errA, errB))
+        by = np.where(cv == 1, dens, np.where(cv == 2, curr, np.where(cv == 3, curr | dens,
+                                                                      curr & dens)))
+    return (GA == GB) & (norm(A["V"] - B["V"]) < tol_pois) & by
 
 
 def check_scope(d, oc=None, track=None, conv_var=None):
@@ -832,15 +841,12 @@ def check_scope(d, oc=None, track=None, conv_var=None):
     if vint and (np.any(masks[:, :, 0] > 0) or np.any(masks[:, :, -1] > 0)):
         raise NotImplementedError("the internal voltage an unknown with an ion region that "
                                   "reaches a contact")
-    if track is not None and np.any(np.asarray(track) > 1) and conv_var is not None and np.any(
-            np.asarray(conv_var) != 1):
-        raise NotImplementedError("Track 2 or 3 with convVar 2-4 (the states' currents compared "
-                                  "by ZimT's errJ)")
 
 
 def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, max_iter=200,
                     bernoulli_name="exact", zimt_current=False, zimt_ion_currents=False,
-                    oc=None, conv_var=1, tol_pois=1e-6, tol_dens=1e-6, layers=None):
+                    oc=None, conv_var=1, tol_pois=1e-6, tol_dens=1e-6, tol_curr=1e-3,
+                    layers=None):
     """transient.solve_transient / _solve_one (transient.py:270-465, 537-637) for every lane at
     once. `t`, `V`, `G_frac`, `track`: (S,) for every device or (B, S); `failure_mode` scalar
     or (B,). `zimt_ion_currents`: each species' last region's ion current alone, as ZimT 5.36
@@ -849,8 +855,8 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     is an unknown of every step (`newton_step_vint`), from the last one at the open circuit
     (extrapolated as the state) or the external voltage less the last current's drop, the steady
     start at 0 V where the first step is at the open circuit (transient.py:290-300, 389-405).
-    `conv_var`, `tol_pois`, `tol_dens` (scalars or B): how ZimT's automatic stop compares two
-    states (`TVG`'s `convVar`, `tolPois`, `tolDens`; only `convVar = 1` with `Track` 2 or 3).
+    `conv_var`, `tol_pois`, `tol_dens`, `tol_curr` (scalars or B): how ZimT's automatic stop
+    compares two states (`TVG`'s `convVar`, `tolPois`, `tolDens`, `tolCurr`).
     `layers` (each device's `(i0, i1)`): also ZimT's tJFile columns of every step (`columns`,
     as `out["columns"][name]`, B×S or B×S×layers).
     Returns a dict: `J`, `J_ext`, `V_int`, `converged`, `iterations`, `accepted` (B×S), `stop`
@@ -865,8 +871,10 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     track = np.zeros((nb, S), int) if track is None else np.broadcast_to(np.asarray(track), (nb, S))
     fm = np.broadcast_to(np.asarray(failure_mode), (nb,))
     check_scope(d, oc=oc, track=track, conv_var=conv_var)
-    tol_pois, tol_dens = (np.broadcast_to(np.asarray(v, dtype=float), (nb,))
-                          for v in (tol_pois, tol_dens))
+    tol_pois, tol_dens, tol_curr = (np.broadcast_to(np.asarray(v, dtype=float), (nb,))
+                                    for v in (tol_pois, tol_dens, tol_curr))
+    conv_var = np.broadcast_to(np.asarray(conv_var), (nb,))
+    by_current = bool(np.any(conv_var != 1))
     bern = dd.BERNOULLI[bernoulli_name]
     Vt = d["Vt"]
     NP = d["x"].shape[1] - 2
@@ -898,6 +906,7 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
     # the automatic stop: the last state kept and the reference state, blank (G -1) at first
     cur = ref = None
     G_cur, G_ref = np.full(nb, -1.0), np.full(nb, -1.0)
+    J_cur, J_ref, err_cur, err_ref = (np.zeros(nb) for _ in range(4))
     count = np.zeros(nb, int)
     caps = _caps(Vt)
     out = {k: np.zeros((nb, S)) for k in ("J", "J_ext", "V_int")}
@@ -964,14 +973,23 @@ def solve_transient(batch, t, V, G_frac, track=None, failure_mode=1, tol=1e-10, 
         now = summary(d, full_of(d, y_new, V_new, bern, dti_k))
         cur = now if cur is None else {f: np.where(keep[:, None], now[f], cur[f]) for f in now}
         G_cur = np.where(keep, G_k, G_cur)
+        if by_current:  # the step's current and its errJ (`columns`)
+            parts, _ = current_parts(dk, full_of(d, y_new, V_new, bern, dti_k), trc, bern,
+                                     zimt_current)
+            total = sum(parts.values())
+            dev = np.concatenate([total, total[:, -1:]], 1) - _col(J)
+            err = np.sqrt(np.sum(dev ** 2, 1) / (NP + 1))
+            J_cur, err_cur = np.where(keep, J, J_cur), np.where(keep, err, err_cur)
         ref = {f: np.zeros_like(v) for f, v in cur.items()} if ref is None else ref
         counted = running & ~failed & ((track_curr == 2) | (track_curr == 3)) & (ok | (fm == 1))
-        equal = states_equal(ref, cur, G_ref, G_cur, tol_pois, tol_dens)
+        equal = states_equal(ref, cur, G_ref, G_cur, tol_pois, tol_dens, conv_var, tol_curr,
+                             J_ref, J_cur, err_ref, err_cur)
         count = np.where(counted, np.where(equal, count + 1, 0), count)
         becomes_ref = running & ~failed & (((track_curr == 1) & ok)
                                            | ((track_curr == 3) & (ok | (fm == 1))))
         ref = {f: np.where(becomes_ref[:, None], cur[f], ref[f]) for f in cur}
         G_ref = np.where(becomes_ref, G_cur, G_ref)
+        J_ref, err_ref = np.where(becomes_ref, J_cur, J_ref), np.where(becomes_ref, err_cur, err_ref)
         static = running & (count >= MIN_COUNT_STATIC)
         stop = np.where(failed, STOP_FAILED, np.where(static, STOP_STATIC, stop))
         first = False

@@ -184,6 +184,21 @@ def test_zimts_columns(case):
     assert set(named) | {"t", "G_frac"} == set(ref.dtype.names)
 
 
+def test_the_automatic_stop_by_convvar():
+    """ZimT's automatic stop comparing states by their densities or currents (convVar 1-4) on
+    the photo transient with Track 3 on every step, tolDens 1e-4 and tolCurr 1e-9 A/m² (errJ
+    decides): stopped where the oracle stops, within one step (errJ's last digits, moved by the
+    densities below the floor, decide a comparison at its threshold)."""
+    from tests.test_transient_oracle import loose_tvg, zimt_track_loose
+    for cv in (1, 2, 3, 4):
+        setup, tvg = loose_tvg(cv)
+        r = solve_transient(prepare([build_device(setup, grid="simss")]), tvg,
+                            bernoulli_name="simss", zimt_current=True, columns=False)
+        o = zimt_track_loose(cv)
+        assert r.stop[0] == o["stop"][0] == 1, cv
+        assert abs(int(r.accepted[0].sum()) - int(o["accepted"][0].sum())) <= 1, cv
+
+
 def test_config5_transient_matches_the_oracle():
     devs = [drawn_device(k) for k in (1, 3, 5)]
     tvg = transient_steps(40)

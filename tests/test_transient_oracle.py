@@ -176,7 +176,21 @@ def zimt_track(batch, tvg):
     return transient.solve_transient(batch, tvg.t, tvg.Vext, tvg.G_frac, tvg.track,
                                      tvg.failure_mode, bernoulli_name="simss", zimt_current=True,
                                      oc=tvg.oc, conv_var=tvg.conv_var, tol_pois=tvg.tol_pois,
-                                     tol_dens=tvg.tol_dens)
+                                     tol_dens=tvg.tol_dens, tol_curr=tvg.tol_curr)
+
+
+def loose_tvg(cv):
+    """ZimT's photo steps with Track 3 on every step, tolPois and tolDens 1e-4, tolCurr 1e-9 and
+    convVar `cv`."""
+    import dataclasses
+    setup, tvg, _ = zimt_case("zimt_photo_light")
+    return setup, dataclasses.replace(tvg, track=np.full(len(tvg.t), 3), conv_var=cv,
+                                      tol_pois=1e-4, tol_dens=1e-4, tol_curr=1e-9)
+
+
+def zimt_track_loose(cv):
+    setup, tvg = loose_tvg(cv)
+    return zimt_track(dd.prepare([build_device(setup, grid="simss")]), tvg)
 
 
 @pytest.mark.parametrize("case", ["zimt_track_tpv_light", "zimt_track_tpv3_light"])
@@ -197,20 +211,35 @@ def test_the_automatic_stop_reproduces_zimt(case):
 
 
 def test_states_compare_as_zimt_compares_them():
-    """`states_equal` as ZimT's `States_Are_Equal` with convVar 1 (test_solver.py:802-824):
-    never at another G_frac or with the potentials apart by tolPois, the densities each
-    within tolDens."""
+    """`states_equal` as ZimT's `States_Are_Equal` (test_solver.py:802-824): never at another
+    G_frac or with the potentials apart by tolPois; then by convVar the densities (1), the
+    current within tolCurr or the smaller errJ (2), either (3) or both (4)."""
     base = {"V": np.zeros((1, 4)), "n": np.ones((1, 4)), "p": np.ones((1, 4)),
             "a": np.zeros((1, 4)), "c": np.zeros((1, 4))}
-    G = np.ones(1)
+    G, one = np.ones(1), np.ones(1)
+    dens_off = dict(base, n=np.ones((1, 4)) * (1 + 1e-5))
 
-    def eq(B, GB=G):
-        return bool(transient.states_equal(base, B, G, GB, 1e-6, 1e-6)[0])
-    assert eq(base)
-    assert not eq(dict(base, n=np.ones((1, 4)) * (1 + 1e-5)))
-    assert eq(dict(base, n=np.ones((1, 4)) * (1 + 1e-7)))
-    assert not eq(base, np.full(1, 0.5))
-    assert not eq(dict(base, V=np.full((1, 4), 1e-6)))
+    def eq(B, cv, GB=G, JB=1.0, errA=0.0, errB=0.0):
+        return bool(transient.states_equal(base, B, G, GB, 1e-6, 1e-6, cv, 1e-3, one,
+                                           JB * one, errA * one, errB * one)[0])
+    expect = {1: (False, True), 2: (True, False), 3: (True, True), 4: (False, False)}
+    for cv, (with_dens_off, with_curr_off) in expect.items():
+        assert eq(base, cv)
+        assert eq(dens_off, cv) == with_dens_off, cv
+        assert eq(base, cv, JB=1.1) == with_curr_off, cv
+        assert not eq(base, cv, GB=np.full(1, 0.5))
+        assert not eq(dict(base, V=np.full((1, 4), 1e-6)), cv)
+    assert eq(dict(base, n=np.ones((1, 4)) * (1 + 1e-7)), 1)
+    assert eq(base, 2, JB=1.1, errA=0.3, errB=0.2)  # within both states' errJ
+
+
+def test_the_automatic_stop_compares_as_convvar_says():
+    """ZimT's photo transient with Track 3 on every step, the densities compared loosely
+    (tolDens 1e-4) and the currents strictly (tolCurr 1e-9 A/m², so errJ decides): comparing
+    currents (convVar 2, or with the densities 4) stops later than comparing densities (1, or
+    either 3)."""
+    rows = {cv: int(zimt_track_loose(cv)["accepted"][0].sum()) for cv in (1, 2, 3, 4)}
+    assert rows[1] == rows[3] < rows[2] == rows[4], rows
 
 
 LAYER_COLUMNS = ("QFLS", "Jphoto", "Jdir", "JbulkElec", "JbulkHoles")
@@ -278,9 +307,6 @@ def test_the_oracle_reproduces_zimts_columns(case):
 def test_what_the_transient_refuses():
     setup, tvg, _ = zimt_case("zimt_photo_light")
     b = dd.prepare([build_device(setup, grid="simss")])
-    with pytest.raises(NotImplementedError, match="Track"):
-        transient.solve_transient(b, tvg.t[:3], tvg.Vext[:3], tvg.G_frac[:3], [0, 1, 2],
-                                  conv_var=2)
     setup, tvg, _ = zimt_case("zimt_region_slow_light")
     b = dd.prepare([build_device(setup, grid="simss")])
     b["R_series"] = np.array([1e-4])
