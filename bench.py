@@ -1,10 +1,10 @@
 """Benchmark: J-V curves per second of the batched steady-state solve on B200.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference] [--precision fp64]
-                    [--workload config2|uneven]
+                    [--workload curves|uneven|adjoint|impedance|build|transient]
     python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N ...
 
-Workload: BASELINE's configuration 2 — 16384 devices per GPU drawn from seed 20261203 (grid
+Workload: the drawn J-V curves — 16384 devices per GPU drawn from seed 20261203 (grid
 NP = 400, 61 voltages from -0.2 to 1.3 V; half pre-biased at 1.0 V with their ions frozen, half
 with free ions; interface and bulk traps, doping and ion densities drawn), synthetic SIMsalabim
 inputs built by `jaxdd_b200.workloads`. One step = one `solve_batch` of the whole batch (every
@@ -17,7 +17,7 @@ Reports (one JSON line, rank 0): `value` (curves/s, inputs resident on the GPU, 
 HBM copy bandwidth), `cpu_baseline` (the FP64 CPU oracle on one core, a bounded sample of the
 same workload), clocks sampled during the timed region.
 
-`--workload uneven`: BASELINE's configuration 3 in FP64 — 32768 devices per GPU in one launch,
+`--workload uneven`: uneven grids in FP64 — 32768 devices per GPU in one launch,
 each with its own grid size NP ~ U{150..900} and voltage count Nv ~ U{21..121} over -0.2..1.3 V
 (otherwise the same draws).
 
@@ -336,7 +336,7 @@ def adjoint_bench(args, rank: int, world: int, local: int) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_grad,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"BASELINE config 4: {n} devices/GPU (drawn p-i-n stacks, "
+            "config": {"workload": f"J-V misfit gradients: {n} devices/GPU (drawn p-i-n stacks, "
                                    f"seed 20261203, explicit work functions), NP {NP}, "
                                    f"{len(V_SCAN)} voltages; loss sum of squared J misfits to "
                                    "curves at parameters perturbed log-normally (sigma 0.2, "
@@ -354,8 +354,8 @@ def adjoint_bench(args, rank: int, world: int, local: int) -> None:
 
 
 def impedance_bench(args, rank: int, world: int, local: int) -> None:
-    """Config 5's small-signal half: each device's admittance at 41 log-spaced frequencies from
-    1 Hz to 1 MHz about 0.8 V, config 5's devices with free mobile ions (the ions unknowns of
+    """The small-signal workload: each device's admittance at 41 log-spaced frequencies from
+    1 Hz to 1 MHz about 0.8 V, the drawn stacks with free mobile ions (the ions unknowns of
     their own). One step = the steady solve at 0.8 V (`dd_solve_states`) and
     `dd_admittance_ions`, inputs resident on the GPU."""
     import torch
@@ -400,7 +400,7 @@ def impedance_bench(args, rank: int, world: int, local: int) -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic",
-            "config": {"workload": f"BASELINE config 5, small-signal half: {n} devices/GPU "
+            "config": {"workload": f"admittance spectra: {n} devices/GPU "
                                    "(drawn p-i-n stacks with free mobile ions, seed 20261205), "
                                    f"NP {args.np}, 41 frequencies 1 Hz..1 MHz at 0.8 V, the "
                                    "ions unknowns of their own (5x5 blocks + 2 ion slots)",
@@ -470,7 +470,7 @@ def build_bench(args, rank: int, world: int, local: int) -> None:
 
 
 def _transient_chunk(args):
-    """Config 5's devices `start .. start + n` (a pool worker)."""
+    """The mobile-ion stacks `start .. start + n` (a pool worker)."""
     start, n, npts = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from jaxdd_b200.batch import prepare
@@ -488,7 +488,7 @@ def transient_bytes(NPk: int, K: int, w: int = 8) -> int:
 
 
 def transient_bench(args, rank: int, world: int, local: int) -> None:
-    """Config 5's transient half: every device's steady state at 0 V, then 2000 implicit-Euler
+    """The transient workload: every device's steady state at 0 V, then 2000 implicit-Euler
     steps at 0.9 V log-spaced from 1 ns to 1 s, mobile ions as unknowns (5x5 blocks). One step =
     the start (`dd_solve_states`) and `dd_transient` of the whole batch, inputs resident on the
     GPU. Devices are independent: with N GPUs every rank solves its own batch (weak scaling)."""
@@ -616,7 +616,7 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"BASELINE config 5, transient half: {m} devices/GPU (drawn "
+            "config": {"workload": f"transients with mobile ions: {m} devices/GPU (drawn "
                                    "p-i-n stacks with free mobile ions, seed 20261205), NP "
                                    f"{args.np}, steady state at 0 V then {S - 1} implicit-Euler "
                                    "steps at 0.9 V log-spaced 1 ns..1 s, 5x5 blocks + 2 ion "
@@ -656,11 +656,11 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
 def workload_name(args, batch, nflat: int) -> str:
     if args.workload == "uneven":
         NPs = batch["NP"]
-        return (f"BASELINE config 3 in FP64: drawn p-i-n stacks (seed 20261203), {args.devices} "
+        return (f"uneven grids in FP64: drawn p-i-n stacks (seed 20261203), {args.devices} "
                 f"devices/GPU in one launch, NP U{{150..900}} (mean {NPs.mean():.0f}), voltage "
                 f"counts U{{21..121}} (mean {nflat / batch['n']:.1f}) over -0.2..1.3 V, half "
                 "frozen after a 1.0 V pre-bias, half free ions")
-    return (f"BASELINE config 2: drawn p-i-n stacks (seed 20261203), {args.devices} devices/GPU, "
+    return (f"drawn J-V curves: p-i-n stacks (seed 20261203), {args.devices} devices/GPU, "
             f"NP {args.np}, {nflat // batch['n']} voltages -0.2..1.3 V, half frozen after a 1.0 V "
             "pre-bias, half free ions")
 
@@ -672,9 +672,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--precision", default="fp64", choices=("fp64",))
-    ap.add_argument("--workload", default="config2",
-                    choices=("config2", "uneven", "adjoint", "impedance", "build", "transient"),
-                    help="config2: 16384 devices, NP 400, 61 V (the default); uneven: 32768 "
+    ap.add_argument("--workload", default="curves",
+                    choices=("curves", "uneven", "adjoint", "impedance", "build", "transient"),
+                    help="curves: 16384 devices, NP 400, 61 V (the default); uneven: 32768 "
                          "devices, NP ~ U{150..900}, Nv ~ U{21..121}, one launch; adjoint: "
                          "gradients of a J-V misfit in 14 parameters, 4096 devices; "
                          "impedance: 8192 devices with mobile ions, 41 frequencies; "

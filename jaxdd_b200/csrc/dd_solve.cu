@@ -48,7 +48,7 @@ __device__ __constant__ double c_stage_share[4] = {1.0 / 64, 1.0 / 16, 1.0 / 4, 
 // A hint to bring one line into L1 ahead of its use: each node's record and state are read from
 // HBM one after another along the sweep, and too few warps run per SM to hide that latency.
 // The sweeps ask for the node DD_PREFETCH_AHEAD positions ahead of the one they work on.
-// Measured on config 2: one position ahead 20,644 curves/s, two 19,976, four 17,715 (L1 is
+// Measured on the drawn J-V curves (16384 devices, NP 400, 61 V): one position ahead 20,644 curves/s, two 19,976, four 17,715 (L1 is
 // too small for more nodes' lines per warp); L2 hints further ahead on top of it made it slower.
 #ifndef DD_PREFETCH_AHEAD
 #define DD_PREFETCH_AHEAD 1
@@ -1388,7 +1388,7 @@ namespace {
 int slots_k(const dd_batch* b) { return b->k_anion + b->k_cation <= 2 ? 2 : 4; }
 
 // Threads per block of the solve (two per device, the pairs adjacent lanes of a warp). One warp
-// a block spreads a batch's warps over the 148 SMs more evenly than two (at config 2's 16384
+// a block spreads a batch's warps over the 148 SMs more evenly than two (at the drawn J-V curves' 16384
 // devices: at most 7 warps on an SM instead of 8; 2.2 % faster measured).
 #ifndef DD_SOLVE_BLOCK
 #define DD_SOLVE_BLOCK 32

@@ -561,7 +561,7 @@ class ChargeGradients:
 def charge_gradients(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
                      bernoulli_name: str = "exact", zimt_current: bool = False) -> ChargeGradients:
     """The integrated transient current and its gradient in the ion density and the ion mobility
-    (BASELINE config 5's gradients), in forward mode through every step as jaxdd differentiates
+    (the transient workload's gradients), in forward mode through every step as jaxdd differentiates
     its transients (`jax.jvp` through each step's `_converged_jvp`, batch.py:661-737): one
     `dd_transient` launch with the tangents carried beside the state."""
     work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,

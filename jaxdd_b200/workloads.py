@@ -28,10 +28,10 @@ from .simss_input import setup_from_texts
 __all__ = ["pin_stack", "pin_texts", "drawn_stack", "drawn_devices", "SEED_DRAWN", "V_SCAN", "ragged_plan",
            "ragged_voltages", "drawn_device"]
 
-#: Seed of the per-device draws (workloads 2 and 3).
+#: Seed of the per-device draws (the drawn J-V curves and the uneven grids).
 SEED_DRAWN = 20261203
-#: config 5's device draws (the transient and small-signal workload)
-SEED_CONFIG5 = 20261205
+#: Seed of the mobile-ion stacks' draws (the transient and small-signal workloads).
+SEED_ION_STACKS = 20261205
 #: 61 voltages from -0.2 to 1.3 V.
 V_SCAN = np.round(np.linspace(-0.2, 1.3, 61), 10)
 #: The uneven workload's grid sizes and voltage counts: NP ~ U{150..900}, Nv ~ U{21..121}.
@@ -150,14 +150,15 @@ def drawn_devices(n: int, seed: int = SEED_DRAWN, NP: int | tuple[int, int] = 40
     return [drawn_device(k, seed, NP) for k in range(start, start + n)]
 
 
-def transient_devices(n: int, seed: int = SEED_CONFIG5, NP: int = 400, start: int = 0):
-    """Config 5's devices: the drawn workload's devices with free mobile ions (its odd indices:
-    config 2's distributions, ions in the absorber, no pre-bias), `start .. start + n` of them."""
+def transient_devices(n: int, seed: int = SEED_ION_STACKS, NP: int = 400, start: int = 0):
+    """The mobile-ion stacks: the drawn workload's devices with free mobile ions (its odd
+    indices: the drawn J-V curves' distributions, ions in the absorber, no pre-bias),
+    `start .. start + n` of them."""
     return [drawn_device(2 * k + 1, seed, NP) for k in range(start, start + n)]
 
 
 def transient_steps(n_steps: int = 2000, V: float = 0.9):
-    """Config 5's transient: the steady state at 0 V (t = 0), then `n_steps` implicit-Euler
+    """The transient workload's steps: the steady state at 0 V (t = 0), then `n_steps` implicit-Euler
     steps at `V` log-spaced from 1 ns to 1 s, light on (G_frac 1), failureMode 1."""
     from .simss_input import TVG
     t = np.concatenate([[0.0], np.logspace(-9, 0, n_steps)])

@@ -64,7 +64,7 @@ def test_the_limits_on_the_gpu():
 
 
 def test_with_mobile_ions_matches_the_oracle():
-    """`dd_admittance_ions`: config 5's drawn stacks with free mobile ions (5×5 blocks, each
+    """`dd_admittance_ions`: the drawn mobile-ion stacks with free mobile ions (5×5 blocks, each
     region's number kept), and in the same batch the p-i-n cell without ions (its ions' rows
     identities), against the oracle (`admittance_ions`, and `admittance` for the cell)."""
     from jaxdd_b200.workloads import transient_devices
@@ -99,10 +99,10 @@ def test_what_impedance_refuses():
 
 
 def _fast_ion_stack(NP=60):
-    """One of config 5's stacks with its ions at 1e-9 m²/Vs: they follow at 1 kHz."""
-    from jaxdd_b200.workloads import SEED_CONFIG5
+    """One of the drawn mobile-ion stacks with its ions at 1e-9 m²/Vs: they follow at 1 kHz."""
+    from jaxdd_b200.workloads import SEED_ION_STACKS
     k = 1
-    texts = drawn_texts(k, np.random.default_rng([SEED_CONFIG5, k]), NP)
+    texts = drawn_texts(k, np.random.default_rng([SEED_ION_STACKS, k]), NP)
     texts["L2.txt"] = "\n".join(
         f"{line.split('=')[0].strip()} = 1e-9"
         if line.split("=")[0].strip() in ("mu_anion", "mu_cation") else line

@@ -3,8 +3,8 @@ oracle (`oracle.transient`) on the same devices and steps, and against ZimT 5.36
 (the reference's tests/data) at the reference's tolerances: electrons and holes, the bulk traps
 in time, mobile ions over 2 x 50 ms and 2 x 5 s, ion regions that reach a contact, the internal
 voltage an unknown (the open circuit's photovoltage, a series resistance); a state carried
-across a split (`profiles`, `initial`); config 5's transient (drawn devices with mobile
-ions, a step to 0.9 V, log-spaced steps) on fewer steps; ZimT's failure modes; at config 5's
+across a split (`profiles`, `initial`); the transient workload (drawn devices with mobile
+ions, a step to 0.9 V, log-spaced steps) on fewer steps; ZimT's failure modes; at the transient workload's
 2000 steps the properties that hold at any size (every step converged and kept, each region's
 ions kept to their total, the current finite); and the integrated current's forward-mode
 gradient in the ion density and mobility against differences of whole transients."""
@@ -199,7 +199,7 @@ def test_the_automatic_stop_by_convvar():
         assert abs(int(r.accepted[0].sum()) - int(o["accepted"][0].sum())) <= 1, cv
 
 
-def test_config5_transient_matches_the_oracle():
+def test_ion_stacks_transient_matches_the_oracle():
     devs = [drawn_device(k) for k in (1, 3, 5)]
     tvg = transient_steps(40)
     r = solve_transient(prepare(devs), tvg)
@@ -239,7 +239,7 @@ def test_failure_modes_as_the_oracle():
         assert np.max(np.abs(r.J_ext[0][kept] - o["J_ext"][0][kept])) < 1e-8 * scale
 
 
-def test_config5_full_steps_hold_their_invariants():
+def test_ion_stacks_full_steps_hold_their_invariants():
     devs = [drawn_device(k) for k in range(1, 129, 2)]
     r = solve_transient(prepare(devs), transient_steps(2000))
     assert r.converged.mean() > 0.999 and r.accepted.all()
@@ -249,11 +249,11 @@ def test_config5_full_steps_hold_their_invariants():
 
 
 def _scaled_device(k, lnN=0.0, lnmu=0.0, NP=120):
-    """Config 5's device `k` with its ion density and mobility scaled by e^lnN and e^lnmu."""
+    """The mobile-ion stack `k` with its ion density and mobility scaled by e^lnN and e^lnmu."""
     from jaxdd_b200.simss_input import setup_from_texts
-    from jaxdd_b200.workloads import SEED_CONFIG5, drawn_texts
+    from jaxdd_b200.workloads import SEED_ION_STACKS, drawn_texts
     idx = 2 * k + 1
-    t = drawn_texts(idx, np.random.default_rng([SEED_CONFIG5, idx]), NP)
+    t = drawn_texts(idx, np.random.default_rng([SEED_ION_STACKS, idx]), NP)
     lines = []
     for line in t["L2.txt"].splitlines():
         key, _, val = (part.strip() for part in line.partition("="))

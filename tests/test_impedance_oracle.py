@@ -2,7 +2,7 @@
 (jaxdd tests/test_impedance.py): at a very low frequency the admittance is the steady J-V
 curve's slope, far above every relaxation the capacitance is the layers' geometric one,
 1/∫dx/ε; `Z = 1/(Y + G_shunt) + R_series`. On workload 1's p-i-n cell, with and without
-interface traps; with mobile ions as unknowns of their own (config 5's drawn stacks): at 1e-7 Hz
+interface traps; with mobile ions as unknowns of their own (the drawn mobile-ion stacks): at 1e-7 Hz
 the steady slope with the ions moving (the reference's bar, 1e-5), far above every relaxation the
 capacitance of the same stack without ions (the ions frozen there), ions frozen at a pre-bias
 refused as the reference refuses them."""
@@ -12,7 +12,7 @@ import pytest
 
 from jaxdd_b200.device import build_device
 from jaxdd_b200.simss_input import setup_from_texts
-from jaxdd_b200.workloads import SEED_CONFIG5, drawn_texts, pin_texts, transient_devices
+from jaxdd_b200.workloads import SEED_ION_STACKS, drawn_texts, pin_texts, transient_devices
 from oracle import dd
 from oracle import impedance as imp
 
@@ -83,7 +83,7 @@ def test_with_ions_low_frequency_is_the_steady_slope(k):
 
 def test_with_ions_high_frequency_is_the_stack_without_them():
     k = 3
-    texts = drawn_texts(k, np.random.default_rng([SEED_CONFIG5, k]), 150)
+    texts = drawn_texts(k, np.random.default_rng([SEED_ION_STACKS, k]), 150)
     f = np.array([1e6, 1e16])
     C = []
     for t in (texts, _without_ions(texts)):
@@ -96,7 +96,7 @@ def test_with_ions_high_frequency_is_the_stack_without_them():
 
 def test_with_ions_frozen_at_a_pre_bias_refused():
     k = 0  # an even device of the drawn workload: pre-biased, its ions frozen
-    dev = build_device(setup_from_texts(drawn_texts(k, np.random.default_rng([SEED_CONFIG5, k]),
+    dev = build_device(setup_from_texts(drawn_texts(k, np.random.default_rng([SEED_ION_STACKS, k]),
                                                     60)))
     assert dev.pre_cond and dev.fix_ions
     with pytest.raises(NotImplementedError, match="frozen"):
@@ -149,11 +149,11 @@ def _sine_response(dev, V0, f, amp=1e-4, per_period=40, periods=20, fitted=4):
 def test_with_ions_the_dt_form_is_the_transients_response():
     """With `dt` the admittance is what the transient (itself pinned on ZimT) sees through implicit
     Euler at steps of `dt`: its response to a 0.1 mV sine (40 steps a period, 20 periods) on a
-    config 5 stack whose ions (μ 1e-9 m²/Vs) follow at 1 kHz, the traps' occupations' dynamics
+    mobile-ion stack whose ions (μ 1e-9 m²/Vs) follow at 1 kHz, the traps' occupations' dynamics
     included: to 1e-6 (measured 1.3e-8; the reference's bar with ions). The continuous response
     differs from it by implicit Euler's error (4 % here)."""
     k = 1
-    texts = drawn_texts(k, np.random.default_rng([SEED_CONFIG5, k]), 60)
+    texts = drawn_texts(k, np.random.default_rng([SEED_ION_STACKS, k]), 60)
     texts["L2.txt"] = "\n".join(
         f"{line.split('=')[0].strip()} = 1e-9"
         if line.split("=")[0].strip() in ("mu_anion", "mu_cation") else line
