@@ -862,7 +862,10 @@ def main() -> None:
                        "converged_fraction": ok_frac, "build_s": round(build_s, 1)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "peak_kind": ("measured (MEASURED_PEAKS.json hbm_gbs)"
+                                       if peak_kind == "measured" else
+                                       "fallback (an earlier B200 copy-bandwidth measurement; "
+                                       "MEASURED_PEAKS.json absent)"),
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": None if cpu is None else {
                 "value": cpu[0], "unit": "curves/s", "cores": 1, "kind": "port",
