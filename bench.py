@@ -53,6 +53,20 @@ CHUNK = 512  # devices per build task (a multiple of 32)
 KERNEL_TAG = "twisted two-thread fused Newton, 26-word static record"
 
 
+def traffic_entry(precision: str, workload: str, devices: int, npts: int) -> dict | None:
+    """The ncu capture of the solve kernel's DRAM traffic per launch (profiles/traffic.json) for
+    this kernel build (KERNEL_TAG), precision and workload, or None when none matches."""
+    try:
+        rec = json.loads((ROOT / "profiles" / "traffic.json").read_text())
+    except (OSError, ValueError):
+        return None
+    entry = rec.get(f"solve_kernel_{precision}_{workload}")
+    if (not entry or entry.get("devices") != devices or entry.get("NP") != npts
+            or KERNEL_TAG not in entry.get("kernel", "")):
+        return None
+    return entry
+
+
 def _peaks() -> tuple[float, str]:
     try:
         data = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -75,8 +89,9 @@ def _build_chunk(args):
 def build_workload(n: int, start: int, procs: int, uneven: bool = False, npts: int = NP):
     """The packed batch of devices [start, start + n), built in `procs` spawned processes (before
     any CUDA call in this one). `uneven` (the uneven workload): devices ordered by grid size,
-    then voltage count, so that a warp's lanes do alike work; returns the batch and each
-    device's voltage count (None for the fixed-size workload)."""
+    then voltage count, so that a warp's lanes do alike work; returns the batch, each device's
+    voltage count (None for the fixed-size workload) and each device's draw index in the
+    batch's order."""
     from jaxdd_b200.batch import concat
     indices = np.arange(start, start + n)
     nv = None
@@ -91,7 +106,7 @@ def build_workload(n: int, start: int, procs: int, uneven: bool = False, npts: i
     else:
         with mp.get_context("spawn").Pool(procs) as pool:
             parts = pool.map(_build_chunk, tasks)
-    return concat(parts, ragged=uneven), nv
+    return concat(parts, ragged=uneven), nv, indices
 
 
 class Clocks:
@@ -653,6 +668,59 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
         torch.distributed.destroy_process_group()
 
 
+def _parity_worker(args):
+    """The oracle's curves of a few devices of the timed workload (one pool task): devices of
+    one grid size and voltage list in one batch, as jaxdd's `solve_batch` takes them."""
+    idx, npts, volts = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from jaxdd_b200.workloads import drawn_device
+    from oracle import dd
+    b = dd.prepare([drawn_device(int(k), NP=npts) for k in idx])
+    J, ok, _ = dd.solve_batch(b, np.asarray(volts))
+    return J, ok, b["J_scale"]
+
+
+def parity_sample(batch, draw_idx, lists, J, ok, offsets, npts, procs: int,
+                  lanes_wanted: int = 256) -> dict:
+    """The timed launch's own curves checked against the oracle (outside the timed region): a
+    fixed-stride sample of the batch's devices (the frozen and the free ones alternate in the
+    draw order) and every device with a point that did not converge (up to 64 of them); each
+    device's J within 1e-6 of its current scale, its converged flags equal to the oracle's."""
+    n = batch["n"]
+    lanes = batch["lane_of"]
+    stride = max(1, n // lanes_wanted)
+    pick = list(range(0, n, stride))[:lanes_wanted]
+    bad = [k for k in range(n) if not ok[offsets[lanes[k]]:offsets[lanes[k]]
+                                          + len(lists[k])].all()]
+    pick = sorted(set(pick) | set(bad[:64]))
+    groups: dict = {}
+    for k in pick:
+        NPk = len(batch["devices"][k].x) - 2
+        groups.setdefault((NPk, len(lists[k])), []).append(k)
+    tasks, owners = [], []
+    for (NPk, _), ks in groups.items():
+        for c in range(0, len(ks), 8):
+            part = ks[c:c + 8]
+            tasks.append(([int(draw_idx[k]) for k in part], npts, lists[part[0]]))
+            owners.append(part)
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(max(1, min(procs, len(tasks)))) as pool:
+        res = pool.map(_parity_worker, tasks)
+    worst, flags_equal = 0.0, True
+    for part, (Jo, oko, scale) in zip(owners, res):
+        for j, k in enumerate(part):
+            sl = slice(offsets[lanes[k]], offsets[lanes[k]] + len(lists[k]))
+            mine = ok[sl].astype(bool)
+            flags_equal = flags_equal and bool(np.array_equal(mine, oko[j]))
+            both = oko[j] & mine
+            if both.any():
+                worst = max(worst, float(np.max(np.abs(J[sl][both] - Jo[j][both])) / scale[j]))
+    return {"lanes": len(pick), "unconverged_lanes": len(bad),
+            "max_err_over_scale": worst, "flags_equal": flags_equal, "tol": 1e-6,
+            "oracle": "FP64 NumPy oracle (oracle/dd.py)",
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
 def workload_name(args, batch, nflat: int) -> str:
     if args.workload == "uneven":
         NPs = batch["NP"]
@@ -688,6 +756,9 @@ def main() -> None:
                          "profiling the same occupancy on less memory)")
     ap.add_argument("--build-procs", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--parity-lanes", type=int, default=256,
+                    help="devices of the timed launch checked against the oracle after the "
+                         "timed region (0: none)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -716,7 +787,8 @@ def main() -> None:
     cores = os.cpu_count() or 1
     procs = args.build_procs or max(1, min(32, cores // max(1, world)))
     t0 = time.perf_counter()
-    batch, nv_dev = build_workload(args.devices, rank * args.devices, procs, uneven, args.np)
+    batch, nv_dev, draw_idx = build_workload(args.devices, rank * args.devices, procs, uneven,
+                                             args.np)
     build_s = time.perf_counter() - t0
     cpu = cpu_sample(args.cpu_sample, uneven) if rank == 0 and world == 1 else None
 
@@ -725,7 +797,7 @@ def main() -> None:
     import torch
     from jaxdd_b200 import _lib
     from jaxdd_b200.batch import _gpu, descriptor, initial_state
-    from jaxdd_b200.workloads import V_SCAN, ragged_voltages
+    from jaxdd_b200.workloads import RAGGED_NP, V_SCAN, ragged_voltages
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -796,6 +868,11 @@ def main() -> None:
     value = curves / (ms_max / 1e3)
     ok_frac = float(ok.float().mean().item())
     lane_steps = steps.cpu().numpy()
+    parity = None
+    if rank == 0 and args.parity_lanes > 0:
+        parity = parity_sample(batch, draw_idx, lists, J.cpu().numpy(), ok.cpu().numpy(),
+                               offsets, RAGGED_NP if uneven else args.np, procs,
+                               args.parity_lanes)
 
     # e2e: the C ABI from pinned host buffers, the copies inside the timed region
     host = {name: torch.from_numpy(arr).pin_memory() for name, arr in
@@ -837,15 +914,8 @@ def main() -> None:
     e2e_value = curves / (float(t.item()) / 1e3)
 
     peak, peak_kind = _peaks()
-    traffic = None
-    try:  # the ncu capture of the same kernel and workload (profiles/), per launch
-        rec = json.loads((ROOT / "profiles" / "traffic.json").read_text())
-        entry = rec.get(f"solve_kernel_{args.precision}_{args.workload}")
-        if (entry and entry["devices"] == args.devices and entry["NP"] == args.np
-                and KERNEL_TAG in entry["kernel"]):
-            traffic = entry["dram_bytes_per_launch"]
-    except (OSError, ValueError, KeyError):
-        traffic = None
+    entry = traffic_entry(args.precision, args.workload, args.devices, args.np)
+    traffic = entry["dram_bytes_per_launch"] if entry else None
     alg = algorithmic_bytes(batch, lane_steps, 8 if args.precision == "fp64" else 4)
     achieved = alg / (ms / 1e3) / 1e9
     if rank == 0:
@@ -860,6 +930,7 @@ def main() -> None:
                        "l2": f"inputs larger than L2 ({batch['stat'].nbytes / 1e9:.2f} GB of "
                              "statics per launch)",
                        "converged_fraction": ok_frac, "build_s": round(build_s, 1)},
+            "parity": parity,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": ("measured (MEASURED_PEAKS.json hbm_gbs)"

@@ -29,7 +29,7 @@ extern "C" {
 #define DD_OK 0
 #define DD_ERR_ARGS 1       /* a size, pointer or option out of range */
 #define DD_ERR_WORKSPACE 2  /* workspace smaller than dd_workspace_bytes */
-#define DD_ERR_LAUNCH 3     /* the CUDA launch failed (cudaGetLastError) */
+#define DD_ERR_LAUNCH 3     /* the CUDA launch failed (the launch's own error) */
 #define DD_ERR_DEVICE 4     /* no sm_100 device current */
 #define DD_ERR_SCRATCH 5    /* dd_solve_noalloc: the batch needs more scratch than
                                DD_NOALLOC_SCRATCH_BYTES */
@@ -378,8 +378,11 @@ int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double*
  * whose dd_workspace_bytes exceeds it is refused with DD_ERR_SCRATCH (at 400 nodes a lane
  * stride of at most 640 with two ion slots, 544 with four); use dd_solve with a workspace for larger batches.
  * The first call on each device, with that device current, looks the array's address up
- * (cudaGetSymbolAddress) and keeps it; make that first call before any stream capture.
- * DD_ERR_DEVICE if the lookup fails. All calls on a device share the one array and it keeps what
+ * (cudaGetSymbolAddress) and keeps it, with the id of the device's context; a later call in
+ * another context of that device (after cudaDeviceReset, say, which frees the array with the
+ * module) looks it up again. Make the first call on a device, and the first after such a reset,
+ * before any stream capture. DD_ERR_DEVICE if the lookup fails or the current device is not an
+ * sm_100 part. All calls on a device share the one array and it keeps what
  * the last call left (the kernel writes every word before reading it, so nothing needs
  * clearing): calls whose work overlaps on the device race and give wrong results, so order them
  * on one stream or one at a time. Results are those of dd_solve on the same inputs. */

@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dd_launch.h"
 #include "dd_layout.h"
 #include "dd_physics.cuh"
 #include "../../include/jaxdd_b200.h"
@@ -844,6 +845,8 @@ int dd_adjoint(const dd_batch* batch, const dd_voltages* volts, const dd_opts* o
   a.FXbar = ws + nodes * 2 * Bp;
   a.scr = ws + nodes * 2 * Bp * 2;
   a.T = T; a.chunks = chunks;
+  int st = dd::device_status();
+  if (st != DD_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(stat_bar, 0, nodes * dd::DD_NF * Bp * sizeof(double), s) != cudaSuccess ||
       cudaMemsetAsync(scal_bar, 0, (dd::DD_NS_BASE + dd::DD_MAXK) * Bp * sizeof(double), s) != cudaSuccess ||
@@ -853,15 +856,15 @@ int dd_adjoint(const dd_batch* batch, const dd_voltages* volts, const dd_opts* o
   // one warp a block: the threads spread over the 148 SMs more evenly than in pairs of warps
   const dim3 block(32), lanes((a.Bp + 31) / 32), pts((T + 31) / 32);
   if (adj_slots(batch) == 2) {
-    dd::adj::frozen_kernel<2><<<lanes, block, 0, s>>>(a);
-    dd::adj::points_kernel<2><<<pts, block, 0, s>>>(a);
-    dd::adj::prebias_kernel<2><<<lanes, block, 0, s>>>(a);
+    st = dd::launch(dd::adj::frozen_kernel<2>, lanes, block, 0, s, a);
+    if (st == DD_OK) st = dd::launch(dd::adj::points_kernel<2>, pts, block, 0, s, a);
+    if (st == DD_OK) st = dd::launch(dd::adj::prebias_kernel<2>, lanes, block, 0, s, a);
   } else {
-    dd::adj::frozen_kernel<4><<<lanes, block, 0, s>>>(a);
-    dd::adj::points_kernel<4><<<pts, block, 0, s>>>(a);
-    dd::adj::prebias_kernel<4><<<lanes, block, 0, s>>>(a);
+    st = dd::launch(dd::adj::frozen_kernel<4>, lanes, block, 0, s, a);
+    if (st == DD_OK) st = dd::launch(dd::adj::points_kernel<4>, pts, block, 0, s, a);
+    if (st == DD_OK) st = dd::launch(dd::adj::prebias_kernel<4>, lanes, block, 0, s, a);
   }
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  return st;
 }
 
 }  // extern "C"

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dd_launch.h"
 #include "dd_layout.h"
 #include "../../include/jaxdd_b200.h"
 
@@ -240,7 +241,8 @@ extern "C" int dd_build(const dd_structure* structure, const double* layer_param
   a.npmax = st.np; a.ka = k_anion; a.kc = k_cation;
   a.S = stat; a.C = scal; a.I = iface; a.y0 = y0;
   a.h = static_cast<double*>(workspace);
+  const int dst = dd::device_status();
+  if (dst != DD_OK) return dst;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  dd::bld::build_kernel<<<(n_devices + 63) / 64, 64, 0, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  return dd::launch(dd::bld::build_kernel, dim3((n_devices + 63) / 64), dim3(64), 0, s, a);
 }

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dd_launch.h"
 #include "dd_layout.h"
 #include "dd_physics.cuh"
 #include "dd_time.cuh"
@@ -1125,10 +1126,13 @@ int dd_admittance(const dd_batch* batch, const double* state, const double* eps,
   long T = (long)Bp * n_freq;
   if (T > imp_threads()) T = imp_threads();
   a.T = T;
+  int st = dd::device_status();
+  if (st != DD_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  dd::imp::prepare_kernel<<<(unsigned)((Bp + 63) / 64), 64, 0, s>>>(a);
-  dd::imp::admittance_kernel<<<(unsigned)((T + 63) / 64), 64, 0, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  st = dd::launch(dd::imp::prepare_kernel, dim3((unsigned)((Bp + 63) / 64)), dim3(64), 0, s, a);
+  if (st == DD_OK)
+    st = dd::launch(dd::imp::admittance_kernel, dim3((unsigned)((T + 63) / 64)), dim3(64), 0, s, a);
+  return st;
 }
 
 int dd_admittance_ions_workspace_bytes(const dd_batch* batch, int n_freq, size_t* bytes) {
@@ -1178,11 +1182,17 @@ int dd_admittance_ions(const dd_batch* batch, const double* state, const double*
   long T = (long)Bp * n_freq;
   if (T > imp_ion_threads()) T = imp_ion_threads();
   a.T = T;
+  int st = dd::device_status();
+  if (st != DD_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  dd::imp::prepare_kernel<<<(unsigned)((Bp + 63) / 64), 64, 0, s>>>(a);
-  dd::imp::prepare_ions_kernel<<<(unsigned)((Bp + 31) / 32), 32, 0, s>>>(a, b);
-  dd::imp::admittance_ions_kernel<<<(unsigned)((T + 63) / 64), 64, 0, s>>>(a, b);
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  st = dd::launch(dd::imp::prepare_kernel, dim3((unsigned)((Bp + 63) / 64)), dim3(64), 0, s, a);
+  if (st == DD_OK)
+    st = dd::launch(dd::imp::prepare_ions_kernel, dim3((unsigned)((Bp + 31) / 32)), dim3(32), 0,
+                    s, a, b);
+  if (st == DD_OK)
+    st = dd::launch(dd::imp::admittance_ions_kernel, dim3((unsigned)((T + 63) / 64)), dim3(64),
+                    0, s, a, b);
+  return st;
 }
 
 }  // extern "C"

@@ -35,6 +35,7 @@
 
 #include <mutex>
 
+#include "dd_launch.h"
 #include "dd_layout.h"
 #include "dd_physics.cuh"
 #include "../../include/jaxdd_b200.h"
@@ -1142,6 +1143,7 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
       scan_begin();
     } else {
       if (pre_cond && fix_ions) freeze<K>(L, logs);
+      copy_state(L, 1, 0);  // the carry: the first voltage's ADV_KEEP reads it
       copyv<K>(lgA, logs);
       k = 0; last_keep = 1;  // the start is the carry
       scan_begin();
@@ -1466,6 +1468,7 @@ int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opt
   size_t need;
   dd_workspace_bytes(batch, &need);
   if (workspace_bytes < need) return DD_ERR_WORKSPACE;
+  if ((st = dd::device_status()) != DD_OK) return st;
   dd::Args a = make_args(batch, workspace);
   a.V = volts->v; a.voff = volts->offset; a.vcnt = volts->count;
   a.J = J; a.ok = converged; a.its = iterations; a.status = lane_status; a.steps = lane_steps;
@@ -1474,9 +1477,8 @@ int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opt
   const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
       block(DD_SOLVE_BLOCK);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (slots_k(batch) == 2) dd::solve_kernel<2><<<grid, block, 0, s>>>(a);
-  else dd::solve_kernel<4><<<grid, block, 0, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  return slots_k(batch) == 2 ? dd::launch(dd::solve_kernel<2>, grid, block, 0, s, a)
+                             : dd::launch(dd::solve_kernel<4>, grid, block, 0, s, a);
 }
 
 int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts,
@@ -1497,6 +1499,7 @@ int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_op
   size_t need;
   dd_workspace_bytes(batch, &need);
   if (workspace_bytes < need) return DD_ERR_WORKSPACE;
+  if ((st = dd::device_status()) != DD_OK) return st;
   dd::Args a = make_args(batch, workspace);
   a.V = volts->v; a.voff = volts->offset; a.vcnt = volts->count;
   a.J = J; a.ok = converged; a.its = iterations; a.status = lane_status; a.steps = lane_steps;
@@ -1507,9 +1510,8 @@ int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_op
   const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
       block(DD_SOLVE_BLOCK);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (slots_k(batch) == 2) dd::solve_kernel<2><<<grid, block, 0, s>>>(a);
-  else dd::solve_kernel<4><<<grid, block, 0, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  return slots_k(batch) == 2 ? dd::launch(dd::solve_kernel<2>, grid, block, 0, s, a)
+                             : dd::launch(dd::solve_kernel<4>, grid, block, 0, s, a);
 }
 
 int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double* vint,
@@ -1521,6 +1523,7 @@ int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double*
   size_t need;
   dd_workspace_bytes(batch, &need);
   if (workspace_bytes < need) return DD_ERR_WORKSPACE;
+  if ((st = dd::device_status()) != DD_OK) return st;
   dd::Args a = make_args(batch, workspace);
   a.Y = y;  // the caller's state is the iterate buffer
   a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS;
@@ -1528,9 +1531,8 @@ int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double*
   const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
       block(DD_SOLVE_BLOCK);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (slots_k(batch) == 2) dd::step_kernel<2><<<grid, block, 0, s>>>(a);
-  else dd::step_kernel<4><<<grid, block, 0, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  return slots_k(batch) == 2 ? dd::launch(dd::step_kernel<2>, grid, block, 0, s, a)
+                             : dd::launch(dd::step_kernel<4>, grid, block, 0, s, a);
 }
 
 }  // extern "C"
@@ -1541,8 +1543,8 @@ int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double*
 // module loads on a device. Every call on a device uses the same array: whatever the last call
 // left there stays, and two calls whose launches overlap (two streams, two host threads) race on
 // it. The solve kernel writes each word of its scratch before it reads it (the starting state
-// from y0, the sweep's records node by node, the extrapolation buffers before any
-// extrapolation uses them), so nothing has to be cleared between calls.
+// from y0, the sweep's records node by node, the carries before any voltage's start reads them),
+// so nothing has to be cleared between calls.
 
 namespace {
 
@@ -1550,21 +1552,55 @@ static __device__ __align__(256) double noalloc_scratch[DD_NOALLOC_SCRATCH_BYTES
 
 constexpr int kMaxDevices = 64;
 std::mutex noalloc_mutex;
+// per device: the array's address and the id of the context it was looked up in
 void* noalloc_ptr[kMaxDevices] = {};
+unsigned long long noalloc_ctx[kMaxDevices] = {};
 
-// The array's address on the current device, looked up once per device (with that device
-// current) and kept. nullptr if there is no usable device or the lookup failed.
+// The driver's id of the context current on this thread (0 when there is none, or the driver
+// does not offer the query). A context torn down and re-created (cudaDeviceReset, then any
+// runtime call) gets a new id, and the library's module, with this array, is loaded anew in it.
+unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault) == cudaSuccess && f)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault) == cudaSuccess && f)
+      get_id = reinterpret_cast<GetId>(f);
+    cudaGetLastError();  // a failed lookup is not the caller's error
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// The array's address on the current device, looked up (with that device current) on the first
+// call and again whenever the device's context is not the one of the last lookup; nullptr if
+// there is no usable device or the lookup failed.
 void* noalloc_scratch_ptr() {
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return nullptr;
+  }
   std::lock_guard<std::mutex> guard(noalloc_mutex);
-  if (!noalloc_ptr[dev]) {
+  const unsigned long long ctx = current_context_id();
+  if (!noalloc_ptr[dev] || ctx == 0 || ctx != noalloc_ctx[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, noalloc_scratch) != cudaSuccess || !p) {
       cudaGetLastError();  // so that the caller's next cudaGetLastError does not report it
+      noalloc_ptr[dev] = nullptr;
       return nullptr;
     }
     noalloc_ptr[dev] = p;
+    // the lookup made the device's primary context current if none was
+    noalloc_ctx[dev] = ctx != 0 ? ctx : current_context_id();
   }
   return noalloc_ptr[dev];
 }
@@ -1578,6 +1614,8 @@ extern "C" int dd_solve_noalloc(const dd_batch* batch, const dd_voltages* volts,
   size_t need = 0;
   if (dd_workspace_bytes(batch, &need) != DD_OK) return DD_ERR_ARGS;
   if (need > (size_t)DD_NOALLOC_SCRATCH_BYTES) return DD_ERR_SCRATCH;
+  const int dst = dd::device_status();
+  if (dst != DD_OK) return dst;
   void* scratch = noalloc_scratch_ptr();
   if (!scratch) return DD_ERR_DEVICE;
   return dd_solve(batch, volts, opts, J, converged, iterations, lane_status, lane_steps, scratch,

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dd_launch.h"
 #include "dd_layout.h"
 #include "dd_physics.cuh"
 #include "../../include/jaxdd_b200.h"
@@ -136,8 +137,10 @@ extern "C" int dd_observables(const dd_batch* batch, const dd_voltages* volts,
   a.oplqy = plqy;
   const long T = (long)batch->lane_stride * nv_max;
   const dim3 block(64), grid((unsigned)((T + 63) / 64));
+  const int st = dd::device_status();
+  if (st != DD_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (batch->k_anion + batch->k_cation <= 2) dd::obs::observe_kernel<2><<<grid, block, 0, s>>>(a);
-  else dd::obs::observe_kernel<4><<<grid, block, 0, s>>>(a);
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  return batch->k_anion + batch->k_cation <= 2
+             ? dd::launch(dd::obs::observe_kernel<2>, grid, block, 0, s, a)
+             : dd::launch(dd::obs::observe_kernel<4>, grid, block, 0, s, a);
 }

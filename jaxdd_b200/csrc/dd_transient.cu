@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dd_launch.h"
 #include "dd_layout.h"
 #include "dd_physics.cuh"
 #include "dd_time.cuh"
@@ -1656,17 +1657,16 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   } else {
     a.TY = nullptr; a.TFB = nullptr; a.TFI = nullptr;
   }
+  const int dst = dd::device_status();
+  if (dst != DD_OK) return dst;
   const dim3 grid((batch->n_lanes + 31) / 32), block(32);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool k2 = slots_k_t(batch) == 2;
-  if (steps->vint) {
-    if (k2) dd::tr::transient_kernel<2, true><<<grid, block, 0, s>>>(a);
-    else dd::tr::transient_kernel<4, true><<<grid, block, 0, s>>>(a);
-  } else {
-    if (k2) dd::tr::transient_kernel<2, false><<<grid, block, 0, s>>>(a);
-    else dd::tr::transient_kernel<4, false><<<grid, block, 0, s>>>(a);
-  }
-  return cudaGetLastError() == cudaSuccess ? DD_OK : DD_ERR_LAUNCH;
+  if (steps->vint)
+    return k2 ? dd::launch(dd::tr::transient_kernel<2, true>, grid, block, 0, s, a)
+              : dd::launch(dd::tr::transient_kernel<4, true>, grid, block, 0, s, a);
+  return k2 ? dd::launch(dd::tr::transient_kernel<2, false>, grid, block, 0, s, a)
+            : dd::launch(dd::tr::transient_kernel<4, false>, grid, block, 0, s, a);
 }
 
 }  // extern "C"
