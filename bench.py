@@ -14,16 +14,18 @@ device's full J-V curve). Devices are independent: with N GPUs every rank solves
 Reports (one JSON line, rank 0): `value` (curves/s, inputs resident on the GPU, CUDA events),
 `e2e` (the same through the C ABI from pinned host buffers, copies in the timed region),
 `roofline` (the kernel's algorithmic bytes per launch over its event time, against the measured
-HBM copy bandwidth), `cpu_baseline` (the FP64 CPU oracle on one core, a bounded sample of the
-same workload), clocks sampled during the timed region.
+HBM copy bandwidth), `cpu_baseline` (the compiled C++ restatement of the FP64 oracle on one
+core, a bounded sample of the same workload), `parity` (a fixed-stride sample of the timed
+launch's own curves against that restatement), clocks sampled during the timed region.
 
 `--workload uneven`: uneven grids in FP64 — 32768 devices per GPU in one launch,
 each with its own grid size NP ~ U{150..900} and voltage count Nv ~ U{21..121} over -0.2..1.3 V
 (otherwise the same draws).
 
 `--impl reference`: jaxdd itself needs JAX, which is not installed; its CPU path is stood in for
-by the FP64 oracle (a CPU restatement of its arithmetic), one single-threaded process per host
-core, each solving a small batch of the same workload (jaxdd benchmarks/run.py's protocol).
+by the compiled C++ restatement of its FP64 solve_batch (oracle/dd_cpu.cpp, pinned to the NumPy
+oracle), one single-threaded process per host core, each solving batch 2 of the same workload
+(jaxdd benchmarks/run.py's protocol).
 """
 
 from __future__ import annotations
@@ -184,41 +186,41 @@ def algorithmic_bytes(batch, steps, w: int = 8) -> float:
     return total
 
 
-def cpu_sample(n: int = 8, uneven: bool = False):
-    """The oracle on one core over `n` devices of the workload (a bounded sample); the uneven
-    workload's one device at a time (the oracle, like jaxdd, takes one grid size and one
-    voltage list per batch)."""
-    from jaxdd_b200.workloads import (RAGGED_NP, V_SCAN, drawn_device, drawn_devices,
-                                      ragged_plan, ragged_voltages)
-    from oracle import dd
+def cpu_sample(n: int = 256, uneven: bool = False, npts: int = NP):
+    """The compiled CPU restatement of the oracle (oracle/dd_cpu.cpp: jaxdd's solve_batch, one
+    device at a time, single-threaded) on one core over `n` devices of the workload (a bounded
+    sample, devices not in the timed batch); `(curves/s, seconds)` of the solves alone."""
+    from jaxdd_b200.workloads import (RAGGED_NP, V_SCAN, drawn_device, ragged_plan,
+                                      ragged_voltages)
+    from oracle import cpu, dd
+    idx = np.arange(10 ** 6, 10 ** 6 + n)
     if uneven:
-        idx = np.arange(10 ** 6, 10 ** 6 + n)
         _, nv = ragged_plan(idx)
-        devs = [drawn_device(int(k), NP=RAGGED_NP) for k in idx]
-        t0 = time.perf_counter()
-        for d, m in zip(devs, nv):
-            dd.solve_batch(dd.prepare([d]), ragged_voltages(m))
-        dt = time.perf_counter() - t0
-        return n / dt, dt
-    devs = drawn_devices(n, NP=NP, start=10 ** 6)
+        jobs = [(dd.prepare([drawn_device(int(k), NP=RAGGED_NP)]), ragged_voltages(m))
+                for k, m in zip(idx, nv)]
+    else:
+        jobs = [(dd.prepare([drawn_device(int(k), NP=npts) for k in idx]), V_SCAN)]
+    cpu.lib()
     t0 = time.perf_counter()
-    dd.solve_batch(dd.prepare(devs), V_SCAN)
+    for tree, V in jobs:
+        cpu.solve_batch(tree, V)
     dt = time.perf_counter() - t0
     return n / dt, dt
 
 
 def _ref_worker(args):
-    """One single-threaded process of the reference arm: solve `n` devices, `reps` times (the
-    uneven workload's one device per batch, as jaxdd needs one grid size and voltage list per
-    batch)."""
+    """One single-threaded process of the reference arm, pinned to its core: solve its `n`
+    devices `reps` times with the compiled CPU restatement of the oracle (the uneven workload's
+    one device per batch, as jaxdd needs one grid size and voltage list per batch)."""
     core, start, n, reps, uneven = args
     try:
         os.sched_setaffinity(0, {core})
     except (AttributeError, OSError):
         pass
+    os.environ["OMP_NUM_THREADS"] = "1"
     from jaxdd_b200.workloads import (RAGGED_NP, V_SCAN, drawn_device, drawn_devices,
                                       ragged_plan, ragged_voltages)
-    from oracle import dd
+    from oracle import cpu, dd
     if uneven:
         idx = np.arange(start, start + n)
         _, nv = ragged_plan(idx)
@@ -226,11 +228,12 @@ def _ref_worker(args):
                 for k, m in zip(idx, nv)]
     else:
         jobs = [(dd.prepare(drawn_devices(n, NP=NP, start=start)), V_SCAN)]
+    cpu.lib()
     times = []
     for _ in range(reps):
         t0 = time.perf_counter()
         for b, V in jobs:
-            dd.solve_batch(b, V)
+            cpu.solve_batch(b, V)
         times.append(time.perf_counter() - t0)
     return times
 
@@ -264,7 +267,10 @@ def reference_arm(args, rank: int) -> None:
         "cpu_baseline": {"value": rate, "unit": "curves/s", "cores": cores, "kind": "port",
                          "sample": f"{cores} processes x {per} devices x {args.steps} timed "
                                    f"steps (+{args.warmup} warm-up), wall {wall:.0f} s; "
-                                   "jaxdd needs JAX (absent): the FP64 oracle stands in"},
+                                   "jaxdd needs JAX (absent): the compiled C++ restatement of "
+                                   "its FP64 solve_batch stands in (oracle/dd_cpu.cpp, pinned "
+                                   "to the NumPy oracle at 1e-10 of the current scale)",
+                         "jaxdd_published_per_core": "~58 curves/s (jaxdd docs/hardware.md)"},
         "e2e": {"value": rate, "unit": "curves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -524,7 +530,7 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
         # the oracle on one device of the same workload, a bounded number of its steps
         from jaxdd_b200.workloads import transient_devices
         from oracle import dd, transient
-        sample_steps = min(args.cpu_sample * 25, args.tsteps)
+        sample_steps = min(200, args.tsteps)
         tv = transient_steps(args.tsteps)
         d1 = dd.prepare(transient_devices(1, NP=args.np))
         t1 = time.perf_counter()
@@ -670,18 +676,19 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
 
 def _parity_worker(args):
     """The oracle's curves of a few devices of the timed workload (one pool task): devices of
-    one grid size and voltage list in one batch, as jaxdd's `solve_batch` takes them."""
+    one grid size and voltage list in one batch, as jaxdd's `solve_batch` takes them, solved by
+    the compiled restatement of the oracle (pinned to oracle/dd.py at 1e-10 of the scale)."""
     idx, npts, volts = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from jaxdd_b200.workloads import drawn_device
-    from oracle import dd
+    from oracle import cpu, dd
     b = dd.prepare([drawn_device(int(k), NP=npts) for k in idx])
-    J, ok, _ = dd.solve_batch(b, np.asarray(volts))
+    J, ok, _ = cpu.solve_batch(b, np.asarray(volts))
     return J, ok, b["J_scale"]
 
 
 def parity_sample(batch, draw_idx, lists, J, ok, offsets, npts, procs: int,
-                  lanes_wanted: int = 256) -> dict:
+                  lanes_wanted: int = 1024) -> dict:
     """The timed launch's own curves checked against the oracle (outside the timed region): a
     fixed-stride sample of the batch's devices (the frozen and the free ones alternate in the
     draw order) and every device with a point that did not converge (up to 64 of them); each
@@ -717,7 +724,8 @@ def parity_sample(batch, draw_idx, lists, J, ok, offsets, npts, procs: int,
                 worst = max(worst, float(np.max(np.abs(J[sl][both] - Jo[j][both])) / scale[j]))
     return {"lanes": len(pick), "unconverged_lanes": len(bad),
             "max_err_over_scale": worst, "flags_equal": flags_equal, "tol": 1e-6,
-            "oracle": "FP64 NumPy oracle (oracle/dd.py)",
+            "oracle": "C++ restatement of the FP64 oracle (oracle/dd_cpu.cpp; pinned to "
+                      "oracle/dd.py at 1e-10 of the scale)",
             "seconds": round(time.perf_counter() - t0, 1)}
 
 
@@ -755,8 +763,10 @@ def main() -> None:
                     help="grid points of the fixed-size workload (400; smaller only for "
                          "profiling the same occupancy on less memory)")
     ap.add_argument("--build-procs", type=int, default=0)
-    ap.add_argument("--cpu-sample", type=int, default=8)
-    ap.add_argument("--parity-lanes", type=int, default=256,
+    ap.add_argument("--cpu-sample", type=int, default=256,
+                    help="devices the compiled CPU restatement solves on one core for "
+                         "cpu_baseline")
+    ap.add_argument("--parity-lanes", type=int, default=1024,
                     help="devices of the timed launch checked against the oracle after the "
                          "timed region (0: none)")
     args = ap.parse_args()
@@ -790,7 +800,8 @@ def main() -> None:
     batch, nv_dev, draw_idx = build_workload(args.devices, rank * args.devices, procs, uneven,
                                              args.np)
     build_s = time.perf_counter() - t0
-    cpu = cpu_sample(args.cpu_sample, uneven) if rank == 0 and world == 1 else None
+    cpu = (cpu_sample(args.cpu_sample, uneven, args.np)
+           if rank == 0 and world == 1 and args.cpu_sample > 0 else None)
 
     import ctypes
 
@@ -940,8 +951,9 @@ def main() -> None:
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": None if cpu is None else {
                 "value": cpu[0], "unit": "curves/s", "cores": 1, "kind": "port",
-                "sample": f"{args.cpu_sample} devices of the same workload, one batch, "
-                          f"{cpu[1]:.1f} s on one core (FP64 NumPy oracle; jaxdd needs JAX)"},
+                "sample": f"{args.cpu_sample} devices of the same workload (outside the timed "
+                          f"batch), {cpu[1]:.1f} s on one core: the compiled C++ restatement "
+                          "of jaxdd's FP64 solve_batch (oracle/dd_cpu.cpp; jaxdd needs JAX)"},
             "e2e": {"value": e2e_value, "unit": "curves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": args.steps,
