@@ -73,9 +73,12 @@ typedef struct dd_voltages {
 
 #define DD_PRECISION_FP64 0  /* everything in FP64: the only precision dd_solve accepts */
 #define DD_PRECISION_MIXED 1 /* FP32 Jacobian and block sweep, FP64 residual, update and current:
-                                refused (DD_ERR_ARGS). Measured: the FP32 block sweep of these
-                                systems converges only linearly and, on some devices, not at all,
-                                so it cannot give jaxdd's converged flags. */
+                                refused (DD_ERR_ARGS). Measured: an FP32 sweep (each node's rows
+                                and unknowns scaled first) contracts Newton's step only linearly;
+                                even used per device only while the last step exceeds 0.1, it
+                                takes 9 % more steps and changes 3 of 3,904 converged flags of the
+                                drawn J-V curves (oracle.mixed_sweep), so it can neither give
+                                jaxdd's flags nor be 2x faster. */
 
 typedef struct dd_opts {
   double tol;         /* Newton's step tolerance (solve_batch tol, default 1e-10) */

@@ -141,3 +141,37 @@ def solve_batch(tree: dict, voltages, tol: float = 1e-10, max_iter: int = 60,
             raise ValueError(f"ddc_solve_batch refused device {b} ({st})")
         del keep
     return J, ok.astype(bool), its
+
+
+def solve_batch_mixed(tree: dict, voltages, theta: float, tol: float = 1e-10,
+                      max_iter: int = 60, bernoulli_name: str = "exact"):
+    """`solve_batch` (one pass at `max_iter`) with the per-lane mixed-precision sweep of
+    oracle/dd_cpu.cpp: an FP32 block sweep (each node's rows and unknowns scaled by its diagonal
+    block) while the lane's last Newton step exceeds `theta`, FP64 after. Returns `(J,
+    converged, iterations, stats)`, stats per device: steps with an FP32 sweep, steps with an
+    FP64 one, the geometric mean of the step-size ratio after an FP32 step, how many ratios."""
+    so = lib()
+    if not hasattr(so, "_mixed_bound"):
+        so.ddc_solve_batch_mixed.restype = ctypes.c_int
+        so.ddc_solve_batch_mixed.argtypes = [
+            ctypes.POINTER(DdcDevice), _D, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+            ctypes.c_int, ctypes.c_double, _D, ctypes.POINTER(ctypes.c_uint8),
+            ctypes.POINTER(ctypes.c_int32), _D]
+        so._mixed_bound = True
+    V = _arr(voltages)
+    nb = tree["x"].shape[0]
+    J = np.zeros((nb, V.size))
+    ok = np.zeros((nb, V.size), dtype=np.uint8)
+    its = np.zeros((nb, V.size), dtype=np.int32)
+    stats = np.zeros((nb, 4))
+    for b in range(nb):
+        d, keep = device(tree, b)
+        st = so.ddc_solve_batch_mixed(
+            ctypes.byref(d), V.ctypes.data_as(_D), V.size, tol, max_iter,
+            1 if bernoulli_name == "simss" else 0, float(theta), J[b].ctypes.data_as(_D),
+            ok[b].ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            its[b].ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), stats[b].ctypes.data_as(_D))
+        if st != 0:
+            raise ValueError(f"ddc_solve_batch_mixed refused device {b} ({st})")
+        del keep
+    return J, ok.astype(bool), its, stats

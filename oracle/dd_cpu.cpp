@@ -397,6 +397,88 @@ void block_thomas(const System& s, Vec& dmat, int mc) {
   }
 }
 
+// The mixed-precision experiment (`ddc_solve_batch_mixed`): the block sweep in FP32 — the
+// inexact Newton of an FP32 Jacobian solve — after each node's unknowns and rows are scaled by
+// the largest entries of its diagonal block (with rows alone the FP32 elimination overflows where
+// a depleted layer's continuity rows are 1e-20 of the Poisson row). The residual, the step's
+// damping and size, the current and every stop stay FP64.
+void block_thomas32(const System& s, Vec& dmat, int mc) {
+  // per-node column scales (node j's unknowns in units of cs[j]) and row scales, both from the
+  // diagonal blocks B, then the factorisation, carries and substitutions in float
+  const int NP = s.NP;
+  std::vector<double> cs((size_t)NP * 3), rs((size_t)NP * 3);
+  for (int i = 0; i < NP; ++i)
+    for (int q = 0; q < 3; ++q) {
+      double mx = 0;
+      for (int r = 0; r < 3; ++r) mx = std::fmax(mx, std::fabs(s.B[(size_t)i * 9 + 3 * r + q]));
+      cs[(size_t)i * 3 + q] = mx > 0 ? 1.0 / mx : 1.0;
+    }
+  for (int i = 0; i < NP; ++i)
+    for (int r = 0; r < 3; ++r) {
+      double mx = 0;
+      for (int q = 0; q < 3; ++q) mx = std::fmax(mx, std::fabs(s.B[(size_t)i * 9 + 3 * r + q] * cs[(size_t)i * 3 + q]));
+      rs[(size_t)i * 3 + r] = mx > 0 ? 1.0 / mx : 1.0;
+    }
+  std::vector<float> cp((size_t)NP * 9), dp((size_t)NP * 3 * mc);
+  float c_prev[9] = {0}, M[9];
+  std::vector<float> R((size_t)3 * (3 + mc)), d_prev((size_t)3 * mc, 0.f);
+  const int w = 3 + mc;
+  for (int i = 0; i < NP; ++i) {
+    float A[9], B[9], C[9], rr[3][8];
+    for (int r = 0; r < 3; ++r) {
+      const double sc = rs[(size_t)i * 3 + r];
+      for (int q = 0; q < 3; ++q) {
+        A[3 * r + q] = i > 0 ? (float)(s.A[(size_t)i * 9 + 3 * r + q] * sc * cs[(size_t)(i - 1) * 3 + q]) : 0.f;
+        B[3 * r + q] = (float)(s.B[(size_t)i * 9 + 3 * r + q] * sc * cs[(size_t)i * 3 + q]);
+        C[3 * r + q] = i + 1 < NP ? (float)(s.C[(size_t)i * 9 + 3 * r + q] * sc * cs[(size_t)(i + 1) * 3 + q]) : 0.f;
+      }
+      for (int q = 0; q < mc; ++q) rr[r][q] = (float)(dmat[((size_t)i * 3 + r) * mc + q] * sc);
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q)
+        M[3 * r + q] = B[3 * r + q] - (A[3 * r] * c_prev[q] + A[3 * r + 1] * c_prev[3 + q] + A[3 * r + 2] * c_prev[6 + q]);
+    for (int r = 0; r < 3; ++r) {
+      for (int q = 0; q < 3; ++q) R[r * w + q] = C[3 * r + q];
+      for (int q = 0; q < mc; ++q)
+        R[r * w + 3 + q] = rr[r][q] - (A[3 * r] * d_prev[q] + A[3 * r + 1] * d_prev[mc + q] + A[3 * r + 2] * d_prev[2 * mc + q]);
+    }
+    for (int col = 0; col < 3; ++col) {
+      int piv = col; float best = std::fabs(M[col * 3 + col]);
+      for (int r = col + 1; r < 3; ++r) if (std::fabs(M[r * 3 + col]) > best) { best = std::fabs(M[r * 3 + col]); piv = r; }
+      if (piv != col) { for (int q = 0; q < 3; ++q) std::swap(M[col * 3 + q], M[piv * 3 + q]); for (int q = 0; q < w; ++q) std::swap(R[col * w + q], R[piv * w + q]); }
+      const float inv = 1.f / M[col * 3 + col];
+      for (int r = col + 1; r < 3; ++r) { const float f = M[r * 3 + col] * inv; for (int q = col + 1; q < 3; ++q) M[r * 3 + q] -= f * M[col * 3 + q]; for (int q = 0; q < w; ++q) R[r * w + q] -= f * R[col * w + q]; }
+    }
+    for (int r = 2; r >= 0; --r) for (int q = 0; q < w; ++q) { float v = R[r * w + q]; for (int k = r + 1; k < 3; ++k) v -= M[r * 3 + k] * R[k * w + q]; R[r * w + q] = v / M[r * 3 + r]; }
+    for (int r = 0; r < 3; ++r) {
+      for (int q = 0; q < 3; ++q) c_prev[3 * r + q] = R[r * w + q];
+      for (int q = 0; q < mc; ++q) d_prev[(size_t)r * mc + q] = R[r * w + 3 + q];
+    }
+    std::memcpy(&cp[(size_t)i * 9], c_prev, sizeof(c_prev));
+    std::memcpy(&dp[(size_t)i * 3 * mc], d_prev.data(), sizeof(float) * 3 * mc);
+  }
+  std::vector<float> nxt((size_t)3 * mc, 0.f), t((size_t)3 * mc);
+  for (int i = NP - 1; i >= 0; --i) {
+    const float* c = &cp[(size_t)i * 9];
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < mc; ++q)
+        t[(size_t)r * mc + q] = dp[((size_t)i * 3 + r) * mc + q] - (c[3 * r] * nxt[q] + c[3 * r + 1] * nxt[mc + q] + c[3 * r + 2] * nxt[2 * mc + q]);
+    nxt = t;
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < mc; ++q) dmat[((size_t)i * 3 + r) * mc + q] = nxt[(size_t)r * mc + q] * cs[(size_t)i * 3 + r];
+  }
+}
+
+struct Mixed {
+  double theta = -1.0;       // FP32 sweep while the lane's last step exceeds it (< 0: never)
+  double last = INFINITY;    // the lane's last step size in this Newton loop
+  bool use32 = false;
+  long steps32 = 0, steps64 = 0;
+  double log_contraction = 0.0;  // sum of ln(size_k / size_{k-1}) after an FP32 step
+  long contractions = 0;
+};
+Mixed g_mixed;
+
 // `bordered_solve` (batch.py:595-603): delta (NP x 3) and the normalisations' step z (K)
 void bordered_solve(const System& s, Vec& delta, Vec& z) {
   const int NP = s.NP, K = s.K, mc = 1 + K;
@@ -406,7 +488,8 @@ void bordered_solve(const System& s, Vec& delta, Vec& z) {
       X[((size_t)j * 3 + r) * mc] = -s.F[3 * j + r];
       for (int k = 0; k < K; ++k) X[((size_t)j * 3 + r) * mc + 1 + k] = s.U[((size_t)j * 3 + r) * K + k];
     }
-  block_thomas(s, X, mc);
+  if (g_mixed.use32) block_thomas32(s, X, mc);
+  else block_thomas(s, X, mc);
   Vec schur((size_t)K * K), rhs(K);
   for (int k = 0; k < K; ++k) {
     double wf = 0.0;
@@ -577,8 +660,18 @@ LoopOut newton_loop(const Model& m, Vec& y, Vec& logs, double Vint, double tol, 
   int it = 0;
   bool done = false;
   Vec full((size_t)3 * (m.NP + 2));
+  g_mixed.last = INFINITY;
   while (!done && it < max_iter && !std::isnan(sh[STALL_STEPS])) {
+    const bool was32 = g_mixed.use32 && it > 0;
+    g_mixed.use32 = g_mixed.theta >= 0.0 && !(g_mixed.last <= g_mixed.theta);
+    if (g_mixed.use32) ++g_mixed.steps32;
+    else ++g_mixed.steps64;
     const double size = newton_step(m, y, logs, Vint, s);
+    if (was32 && g_mixed.last > 0.0 && size > 0.0 && std::isfinite(size)) {
+      g_mixed.log_contraction += std::log(size / g_mixed.last);
+      ++g_mixed.contractions;
+    }
+    g_mixed.last = size;
     set_bounds(m, Vint, full);
     std::memcpy(&full[3], y.data(), sizeof(double) * 3 * m.NP);
     const double J = current(m, full);
@@ -894,4 +987,26 @@ int ddc_solve_batch(const ddc_device* dev, const double* voltages, int nv, doubl
     iterations[order[k]] = itss[k];
   }
   return 0;
+}
+
+// jaxdd's solve_batch with the per-lane mixed-precision sweep (`Mixed`): an FP32 sweep while the
+// lane's last Newton step in scaled units exceeds `theta`, FP64 for the finish. stats[0..3]: the
+// steps with an FP32 sweep, those with an FP64 one, the geometric mean of the step-size ratio
+// after an FP32 step, the number of such ratios. One pass at max_iter.
+extern "C" int ddc_solve_batch_mixed(const ddc_device* dev, const double* voltages, int nv,
+                                     double tol, int max_iter, int simss, double theta,
+                                     double* J, uint8_t* converged, int32_t* iterations,
+                                     double* stats) {
+  g_mixed = Mixed();
+  g_mixed.theta = theta;
+  const int st = ddc_solve_batch(dev, voltages, nv, tol, max_iter, 0, simss, J, converged,
+                                 iterations);
+  if (stats) {
+    stats[0] = (double)g_mixed.steps32;
+    stats[1] = (double)g_mixed.steps64;
+    stats[2] = g_mixed.contractions ? std::exp(g_mixed.log_contraction / g_mixed.contractions) : NAN;
+    stats[3] = (double)g_mixed.contractions;
+  }
+  g_mixed = Mixed();
+  return st;
 }

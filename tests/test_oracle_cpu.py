@@ -50,3 +50,18 @@ def test_refuses_a_device_it_cannot_solve():
     tree = dd.prepare(drawn_devices(1, NP=60))
     with pytest.raises(ValueError):
         cpu.solve_batch(tree, np.array([]))
+
+
+def test_the_mixed_precision_experiment_without_fp32_is_the_fp64_solve():
+    """`solve_batch_mixed` with no FP32 sweep (theta < 0) is one pass of `solve_batch`; with
+    FP32 sweeps on large steps it still reaches the same curves where both converge."""
+    from jaxdd_b200.workloads import V_SCAN, drawn_devices
+    tree = dd.prepare(drawn_devices(2, NP=100))
+    J, ok, its = cpu.solve_batch(tree, V_SCAN, first_max_iter=60)
+    Jm, okm, itsm, st = cpu.solve_batch_mixed(tree, V_SCAN, -1.0)
+    assert np.array_equal(J, Jm) and np.array_equal(ok, okm) and np.array_equal(its, itsm)
+    assert np.all(st[:, 0] == 0) and np.all(st[:, 1] > 0)
+    J3, ok3, _, st3 = cpu.solve_batch_mixed(tree, V_SCAN, 0.1)
+    assert np.all(st3[:, 0] > 0)
+    both = ok3 & ok
+    assert np.all(np.abs(J3 - J)[both] <= 1e-8 * np.repeat(tree["J_scale"], V_SCAN.size)[both.ravel()])
