@@ -106,11 +106,8 @@ __device__ void lane_init(Lane& L, const Args& a, int l) {
   L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l;
   L.ka = a.ka; L.K = K;
   L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L);
-  L.V0 = L.sc(C_V0); L.VL = L.sc(C_VL); L.left = L.sc(C_LEFT);
-  L.lnnL = L.sc(C_LNNL); L.lnpL = L.sc(C_LNPL); L.lnnR = L.sc(C_LNNR); L.lnpR = L.sc(C_LNPR);
-  L.Jscale = L.sc(C_JSCALE); L.Gshunt = L.sc(C_GSHUNT); L.gfrac = L.sc(C_GFRAC);
-  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor); L.Hsum = L.sc(C_HSUM);
-  L.NP = (int)L.sc(C_NP);
+      L.gfrac = L.sc(C_GFRAC);
+  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor);   L.NP = (int)L.sc(C_NP);
   L.mid = (int)L.sc(C_MID);
   L.currdiff = L.sc(C_CURRDIFF) > 0.0; L.simss = a.simss;
   // the slots' totals: rows past k_anion + k_cation need not exist in scal
@@ -164,7 +161,7 @@ __device__ void current_bar(const Lane& L, const Scr& w, const Out& o, double Vi
                             const double* logs, double Jbar, Bar& cb) {
   const int NP = L.NP;
   const double Vt = L.Vt, iVt = L.iVt, gf = L.gfrac, LL = L.L;
-  const double sign = -L.left;
+  const double sign = -L.left();
   // the interface points' recombination (each trapped interval adds to both its ends)
   for (int k = 0; k <= NP + 1; ++k) {
     w.at(k, R_RIN) = 0.0; w.at(k, R_RIP) = 0.0; w.at(k, R_BRN) = 0.0; w.at(k, R_BRP) = 0.0;
@@ -256,7 +253,7 @@ __device__ void current_bar(const Lane& L, const Scr& w, const Out& o, double Vi
   bool iface_next = false;
   for (int k = NP; k >= 0; --k) {
     const double hk = L.st(k, S_H);
-    const double a_k = Jbar * sign * hk / L.Hsum;
+    const double a_k = Jbar * sign * hk / L.Hsum();
     const bool iface_k = L.st(k, S_IFK) > -1.5;
     const double b_k = (iface_k ? 0.0 : a_k) + (iface_next ? a_next : 0.0);
     Bsum += b_k;
@@ -289,8 +286,8 @@ __device__ void current_bar(const Lane& L, const Scr& w, const Out& o, double Vi
         hbar += a_k * sn * 0.5 * Q * LL * ri;
         Lbar += a_k * sn * 0.5 * Q * hk * ri;
       }
-      Jtot += sign * hk * (Jp - Q * Kc[c]) / L.Hsum;
-      hbar += Jbar * sign * (Jp - Q * Kc[c]) / L.Hsum;
+      Jtot += sign * hk * (Jp - Q * Kc[c]) / L.Hsum();
+      hbar += Jbar * sign * (Jp - Q * Kc[c]) / L.Hsum();
       // S_k = sum_{m<=k} sn Q L h_m Uc_m, weighted by the suffix sum of b
       if (k >= 1) {
         ucbar[c] += sn * Q * LL * hk * Bsum;
@@ -340,7 +337,7 @@ __device__ void current_bar(const Lane& L, const Scr& w, const Out& o, double Vi
     a_next = a_k;
     iface_next = iface_k;
   }
-  o.c(C_HSUM, -Jbar * Jtot / L.Hsum);
+  o.c(C_HSUM, -Jbar * Jtot / L.Hsum());
   o.c(C_L, Lbar);
   o.c(C_GFRAC, gfbar);
   // the interface recombination's adjoint into dJ/dy and the table
@@ -664,7 +661,7 @@ __device__ double contacts_out(const Lane& L, const Out& o, const Bar& cb) {
   o.c(C_LNPL, cb.pL);
   o.c(C_LNNR, cb.nR);
   o.c(C_LNPR, cb.pR);
-  return 0.5 * L.left * (cb.V0 - cb.VR);
+  return 0.5 * L.left() * (cb.V0 - cb.VR);
 }
 
 __device__ __forceinline__ bool finite_state(const Lane& L, const double* logs) {

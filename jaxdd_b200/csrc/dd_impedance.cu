@@ -100,11 +100,8 @@ struct Args {
 __device__ void lane_init(Lane& L, const Args& a, int l) {
   L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l; L.ka = a.ka; L.K = 2;
   L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L);
-  L.V0 = L.sc(C_V0); L.VL = L.sc(C_VL); L.left = L.sc(C_LEFT);
-  L.lnnL = L.sc(C_LNNL); L.lnpL = L.sc(C_LNPL); L.lnnR = L.sc(C_LNNR); L.lnpR = L.sc(C_LNPR);
-  L.Jscale = L.sc(C_JSCALE); L.Gshunt = L.sc(C_GSHUNT); L.gfrac = L.sc(C_GFRAC);
-  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor); L.Hsum = L.sc(C_HSUM);
-  L.NP = (int)L.sc(C_NP);
+      L.gfrac = L.sc(C_GFRAC);
+  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor);   L.NP = (int)L.sc(C_NP);
   L.mid = 0; L.currdiff = 0; L.simss = a.simss;
   L.tot[0] = 0.0; L.tot[1] = 0.0;
   L.FX = nullptr; L.CD = nullptr; L.ncd = 0; L.ybuf = 0;
@@ -367,7 +364,7 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
     const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
     auto rec = [&](int k, int f) { return a.rec[((size_t)k * P_WORDS + f) * a.Bp + l]; };
     auto scr = [&](int k, int f) -> double& { return a.scr[((size_t)k * W_WORDS + f) * a.T + slot]; };
-    const double e = L.left;
+    const double e = L.left();
     // ---- forward elimination of (J + iw M + traps) dy = -dF/dV
     cplx cp[3][3], dp[3];
 #pragma unroll
@@ -464,7 +461,7 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
       if (k == NP + 1) return mk(-0.5 * e);
       return dyv(k, 0);
     };
-    const double sign = -L.left;
+    const double sign = -L.left();
     const double Vt = L.Vt;
     cplx dsgl[2] = {mk(0.0), mk(0.0)}, ddb_b[2] = {mk(0.0), mk(0.0)}, ddb_t[2] = {mk(0.0), mk(0.0)};
     cplx diu_b[2] = {mk(0.0), mk(0.0)}, diu_t[2] = {mk(0.0), mk(0.0)};
@@ -752,7 +749,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
     auto scr = [&](int k, int f) -> double& {
       return b.scr5[((size_t)k * V_WORDS + f) * a.T + slot];
     };
-    const double e = L.left;
+    const double e = L.left();
     // ---- forward elimination of (J + (iw - 1) M + traps) [dy | X_U] = [-dF/dV | U]
     cplx cp[5][5], dp[5][3];
 #pragma unroll
@@ -923,7 +920,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       if (k == NP + 1) return mk(-0.5 * e);
       return dyv(k, 0);
     };
-    const double sign = -L.left;
+    const double sign = -L.left();
     const double Vt = L.Vt;
     cplx dsgl[2] = {mk(0.0), mk(0.0)}, ddb_b[2] = {mk(0.0), mk(0.0)}, ddb_t[2] = {mk(0.0), mk(0.0)};
     cplx diu_b[2] = {mk(0.0), mk(0.0)}, diu_t[2] = {mk(0.0), mk(0.0)};

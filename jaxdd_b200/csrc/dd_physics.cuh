@@ -1,7 +1,9 @@
 // Device-side physics shared by the solve (dd_solve.cu) and its adjoint (dd_adjoint.cu): the
 // reference's constants and stops, the Bernoulli function, one interval's Scharfetter-Gummel
 // fluxes, recombination, interface traps, the ions' numbers, and the per-lane view of the packed
-// batch (`Lane`). Everything is inline: each translation unit gets its own copy.
+// batch (`Lane`). Everything is inline: each translation unit gets its own copy. The helpers that
+// read a node's static record take any lane view with Lane's members (`st`, `afix`, `cfix`, ...):
+// the solve's sweeps pass one that reads the record from shared memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -70,6 +72,29 @@ __device__ __forceinline__ void bern_pair(double x, int simss, double& bf, doubl
   else { bb = b; dbb = db; bf = b + a; dbf = -db - 1.0; }
 }
 
+// Element i of a small register array (0 where i is outside 0 .. N-1), and the update of one
+// element, by predicated selects over the array: an index known only at run time into a
+// register array would move the whole array to local memory.
+template <int N>
+__device__ __forceinline__ double pick(const double* a, int i) {
+  double v = 0.0;
+#pragma unroll
+  for (int q = 0; q < N; ++q) v = q == i ? a[q] : v;
+  return v;
+}
+template <int N>
+__device__ __forceinline__ void add_at(double* a, int i, double v) {
+#pragma unroll
+  for (int q = 0; q < N; ++q)
+    if (q == i) a[q] += v;
+}
+template <int N>
+__device__ __forceinline__ void set_at(double* a, int i, double v) {
+#pragma unroll
+  for (int q = 0; q < N; ++q)
+    if (q == i) a[q] = v;
+}
+
 // ------------------------------------------------------------------------------------ lane
 
 struct Lane {
@@ -78,8 +103,7 @@ struct Lane {
   const double* __restrict__ C;
   const double* __restrict__ IFt;
   int Bp, l, NP, ka, K;
-  double Vt, iVt, L, V0, VL, left, lnnL, lnpL, lnnR, lnpR, Jscale, Gshunt, gfrac, nfloor,
-      lognf, Hsum;
+  double Vt, iVt, L, gfrac, nfloor, lognf;
   int currdiff, simss;
   double tot[DD_MAXK];
   // dynamic
@@ -100,6 +124,18 @@ struct Lane {
     return __ldg(S + ((size_t)k * DD_NF + f) * Bp + l);
   }
   __device__ __forceinline__ double sc(int f) const { return __ldg(C + (size_t)f * Bp + l); }
+  // Scalars read once or twice per Newton step are read from the record when needed rather
+  // than held in registers through the sweeps.
+  __device__ __forceinline__ double V0() const { return sc(C_V0); }
+  __device__ __forceinline__ double VL() const { return sc(C_VL); }
+  __device__ __forceinline__ double left() const { return sc(C_LEFT); }
+  __device__ __forceinline__ double lnnL() const { return sc(C_LNNL); }
+  __device__ __forceinline__ double lnpL() const { return sc(C_LNPL); }
+  __device__ __forceinline__ double lnnR() const { return sc(C_LNNR); }
+  __device__ __forceinline__ double lnpR() const { return sc(C_LNPR); }
+  __device__ __forceinline__ double Jscale() const { return sc(C_JSCALE); }
+  __device__ __forceinline__ double Gshunt() const { return sc(C_GSHUNT); }
+  __device__ __forceinline__ double Hsum() const { return sc(C_HSUM); }
   __device__ __forceinline__ double itab(int row, int f) const {
     return __ldg(IFt + ((size_t)row * DD_NIF + f) * Bp + l);
   }
@@ -115,7 +151,9 @@ struct Lane {
   __device__ __forceinline__ double cfix(int k) const {
     return frozen ? FX[((size_t)k * 2 + 1) * Bp + l] : share * st(k, S_CFIX);
   }
-  __device__ __forceinline__ double total(int k) const { return frozen ? 0.0 : share * tot[k]; }
+  __device__ __forceinline__ double total(int k) const {
+    return frozen ? 0.0 : share * pick<DD_MAXK>(tot, k);
+  }
 };
 
 // Slot of a point for each species, -1 where the species is not mobile there (or frozen).
@@ -123,7 +161,8 @@ struct Slots {
   int a, c;
 };
 
-__device__ __forceinline__ Slots slots_at(const Lane& L, int k) {
+template <class LT>
+__device__ __forceinline__ Slots slots_at(const LT& L, int k) {
   Slots s;
   s.a = (int)L.st(k, S_ASLOT);
   s.c = (int)L.st(k, S_CSLOT);
@@ -148,10 +187,22 @@ __device__ __forceinline__ void pt_fill(const Lane& L, Pt& P, int k, const doubl
   P.dc = P.sl.c >= 0 ? exp(logs[L.ka + P.sl.c] - P.V * L.iVt) : 0.0;
 }
 
+// pt_fill with the K normalisations in registers (read by selects, `pick`).
+template <int K, class LT>
+__device__ __forceinline__ void pt_fill_k(const LT& L, Pt& P, int k, const double* logs) {
+  P.n = exp(P.lnn);
+  P.p = exp(P.lnp);
+  P.offn = L.st(k, S_OFFN);
+  P.offp = L.st(k, S_OFFP);
+  P.sl = slots_at(L, k);
+  P.da = P.sl.a >= 0 ? exp(pick<K>(logs, P.sl.a) + P.V * L.iVt) : 0.0;
+  P.dc = P.sl.c >= 0 ? exp(pick<K>(logs, L.ka + P.sl.c) - P.V * L.iVt) : 0.0;
+}
+
 // The contacts' states (`_bounds`, batch.py:255-259).
 __device__ __forceinline__ void contact(const Lane& L, int right, double Vint, Pt& P) {
-  if (!right) { P.V = L.V0 + 0.5 * L.left * Vint; P.lnn = L.lnnL; P.lnp = L.lnpL; }
-  else { P.V = L.VL - 0.5 * L.left * Vint; P.lnn = L.lnnR; P.lnp = L.lnpR; }
+  if (!right) { P.V = L.V0() + 0.5 * L.left() * Vint; P.lnn = L.lnnL(); P.lnp = L.lnpL(); }
+  else { P.V = L.VL() - 0.5 * L.left() * Vint; P.lnn = L.lnnR(); P.lnp = L.lnpR(); }
 }
 
 // One interval's Scharfetter-Gummel fluxes and their derivatives in its two points'
@@ -179,7 +230,8 @@ __device__ __forceinline__ void flux(const Lane& L, const Pt& a, const Pt& b, do
 }
 
 // Direct + SRH recombination at a point, and n dR/dn, p dR/dp (solver.py:734-745).
-__device__ __forceinline__ void recomb(const Lane& L, int k, double n, double p, double& R,
+template <class LT>
+__device__ __forceinline__ void recomb(const LT& L, int k, double n, double p, double& R,
                                        double& dRn, double& dRp) {
   const double kd = L.st(k, S_KD), ni2 = L.st(k, S_NI2), Nt = L.st(k, S_NT);
   R = kd * (n * p - ni2);
@@ -243,8 +295,8 @@ static __device__ void iface_edge(const Lane& L, int t, double nL, double nR, do
 template <int K>
 __device__ __forceinline__ void ion_edge(const Lane& L, const Pt& a, const Pt& b, double hL,
                                          double* num) {
-  if (a.sl.a >= 0 && a.sl.a == b.sl.a) num[a.sl.a] += 0.5 * (a.da + b.da) * hL;
-  if (a.sl.c >= 0 && a.sl.c == b.sl.c) num[L.ka + a.sl.c] += 0.5 * (a.dc + b.dc) * hL;
+  if (a.sl.a >= 0 && a.sl.a == b.sl.a) add_at<K>(num, a.sl.a, 0.5 * (a.da + b.da) * hL);
+  if (a.sl.c >= 0 && a.sl.c == b.sl.c) add_at<K>(num, L.ka + a.sl.c, 0.5 * (a.dc + b.dc) * hL);
 }
 
 // The constraints' derivative in a point's potential (the reference's jacrev of
@@ -259,7 +311,7 @@ __device__ __forceinline__ void ion_w(const Lane& L, const Pt& pm, const Pt& pc,
     const double tk = L.total(k);
     if (tk > 0.0) {
       const double wpt = 0.5 * ((pm.sl.a == k ? hLm : 0.0) + (pn.sl.a == k ? hLp : 0.0));
-      W[k] = wpt * pc.da * L.iVt / tk;
+      set_at<K>(W, k, wpt * pc.da * L.iVt / tk);
     }
   }
   if (pc.sl.c >= 0) {
@@ -267,7 +319,7 @@ __device__ __forceinline__ void ion_w(const Lane& L, const Pt& pm, const Pt& pc,
     const double tk = L.total(k);
     if (tk > 0.0) {
       const double wpt = 0.5 * ((pm.sl.c == pc.sl.c ? hLm : 0.0) + (pn.sl.c == pc.sl.c ? hLp : 0.0));
-      W[k] = -wpt * pc.dc * L.iVt / tk;
+      set_at<K>(W, k, -wpt * pc.dc * L.iVt / tk);
     }
   }
 }
@@ -317,8 +369,8 @@ __device__ void small_solve(double (&M)[K][K], double (&r)[K], double (&z)[K]) {
 // (which turns their sign, as the mirrored equations want), the Poisson stencil's two sides swap
 // (fL, fU), and A couples to the point behind, C to the one ahead, as in the unmirrored frame.
 // Only the interface traps, which know their physical left and right, read `mirror`.
-template <int K>
-__device__ __forceinline__ void assemble_row(const Lane& L, int i, const Pt& pm, const Pt& pc,
+template <int K, class LT>
+__device__ __forceinline__ void assemble_row(const LT& L, int i, const Pt& pm, const Pt& pc,
                                              const Pt& pn, const Flux& el, const Flux& er,
                                              double hm, double hp, int ifk_m, int ifk_i,
                                              bool noise, bool mirror, double (&A)[3][3],
@@ -381,8 +433,8 @@ __device__ __forceinline__ void assemble_row(const Lane& L, int i, const Pt& pm,
     rhs[0] = -pois * sP; rhs[1] = -elec * sC; rhs[2] = -hole * sC;
 #pragma unroll
     for (int k = 0; k < K; ++k) U0[k] = 0.0;
-    if (pc.sl.a >= 0) U0[pc.sl.a] = -Q * pc.da * sP;
-    if (pc.sl.c >= 0) U0[L.ka + pc.sl.c] = Q * pc.dc * sP;
+    if (pc.sl.a >= 0) set_at<K>(U0, pc.sl.a, -Q * pc.da * sP);
+    if (pc.sl.c >= 0) set_at<K>(U0, L.ka + pc.sl.c, Q * pc.dc * sP);
     ion_w<K>(L, pm, pc, pn, hm * L.L, hp * L.L, W);
   } else {
     const double ym[3] = {fabs(pm.V), fabs(pm.lnn), fabs(pm.lnp)};

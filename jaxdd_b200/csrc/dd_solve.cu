@@ -44,6 +44,13 @@ namespace dd {
 
 __device__ __constant__ double c_stage_share[4] = {1.0 / 64, 1.0 / 16, 1.0 / 4, 1.0};
 
+// Threads per block of the solve (two per device, the pairs adjacent lanes of a warp). One warp
+// a block spreads a batch's warps over the 148 SMs more evenly than two (at the drawn J-V curves' 16384
+// devices: at most 7 warps on an SM instead of 8; 2.2 % faster measured).
+#ifndef DD_SOLVE_BLOCK
+#define DD_SOLVE_BLOCK 32
+#endif
+
 // ------------------------------------------------------------------------------------ prefetch
 
 // A hint to bring one line into L1 ahead of its use: each node's record and state are read from
@@ -302,6 +309,14 @@ __device__ __forceinline__ double sg_flux(const Lane& L, int s, const Pt& a, con
 
 // ------------------------------------------------------------------------------------ Newton step
 
+// Word j < 30 + 2K of the meeting row's record (its right-hand side, A, B, C, ion columns and
+// border), held between half 0's assembly of the row and the solve at the meeting: the sweep
+// records of node 0 (a contact) and of node mid (the meeting row is not eliminated), which no
+// elimination writes; 2 (12 + 3K) >= 30 + 2K words.
+__device__ __forceinline__ double* meet_word(const Lane& L, int j) {
+  return j < L.ncd ? L.cd(0, j) : L.cd(L.mid, j - L.ncd);
+}
+
 struct StepOut {
   double size;
   double J;
@@ -326,23 +341,32 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
   // position -> node; the interval between positions p and p + 1 -> its physical index
 #define NODE(p) (top ? (p) : NP + 1 - (p))
 #define EDGE(p) (top ? (p) : NP - (p))
-  // the boundary points: each half loads its own (and makes its start there) and hands the
-  // state to the other
-  Pt pb, px;
-  load_state(L, NODE(nown), adv, ratio, pb);
-  px.V = xchg(L, pb.V); px.lnn = xchg(L, pb.lnn); px.lnp = xchg(L, pb.lnp);
-  pt_fill(L, pb, NODE(nown), logs);
-  pt_fill(L, px, NODE(nown + 1), logs);
+  // the boundary points: each half makes its own start there (load_state writes it to the
+  // iterate, where it is read again when needed) and hands the state to the other half, which
+  // keeps only (V, ln n, ln p) of it and fills in the rest where it uses it
+  double xb[3];
+  {
+    Pt t;
+    load_state(L, NODE(nown), adv, ratio, t);
+    xb[0] = xchg(L, t.V); xb[1] = xchg(L, t.lnn); xb[2] = xchg(L, t.lnp);
+  }
+  auto own_boundary = [&](Pt& P) {
+    P.V = *L.y(0, NODE(nown), 0); P.lnn = *L.y(0, NODE(nown), 1); P.lnp = *L.y(0, NODE(nown), 2);
+    pt_fill_k<K>(L, P, NODE(nown), logs);
+  };
+  auto other_boundary = [&](Pt& P) {
+    P.V = xb[0]; P.lnn = xb[1]; P.lnp = xb[2];
+    pt_fill_k<K>(L, P, NODE(nown + 1), logs);
+  };
 
   Carry<K> cr;
   cr.zero();
-  double Am[3][3], Bmm[3][3], Cmm[3][3], rm[3], Um[K], Wm[K];
   {
     Pt pm, pc, pn;
     contact(L, top ? 0 : 1, Vint, pm);
-    pt_fill(L, pm, NODE(0), logs);
-    if (nown == 1) pc = pb;
-    else { load_state(L, NODE(1), adv, ratio, pc); pt_fill(L, pc, NODE(1), logs); }
+    pt_fill_k<K>(L, pm, NODE(0), logs);
+    if (nown == 1) own_boundary(pc);
+    else { load_state(L, NODE(1), adv, ratio, pc); pt_fill_k<K>(L, pc, NODE(1), logs); }
     Flux el;
     int e = EDGE(0);
     double h_m = L.st(e, S_H);
@@ -351,9 +375,9 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
     int ifk_m = (int)L.st(e, S_IFK);
     for (int p = 1; p <= nown; ++p) {
       if (p + DD_PREFETCH_AHEAD <= nown + 1) prefetch_node(L, NODE(p + DD_PREFETCH_AHEAD));
-      if (p + 1 == nown) pn = pb;
-      else if (p == nown) pn = px;
-      else { load_state(L, NODE(p + 1), adv, ratio, pn); pt_fill(L, pn, NODE(p + 1), logs); }
+      if (p + 1 == nown) own_boundary(pn);
+      else if (p == nown) other_boundary(pn);
+      else { load_state(L, NODE(p + 1), adv, ratio, pn); pt_fill_k<K>(L, pn, NODE(p + 1), logs); }
       e = EDGE(p);
       const double h_i = L.st(e, S_H);
       const int ifk_i = (int)L.st(e, S_IFK);
@@ -367,14 +391,20 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
         cr.eliminate(A, Bm, Cm, rhs, U0, W);
         cr.store(L, NODE(p));
       } else {
+        // the meeting row waits in memory until both halves are through (kept in registers it
+        // would hold them over the whole loop)
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
-          rm[r] = rhs[r];
+          *meet_word(L, r) = rhs[r];
 #pragma unroll
-          for (int q = 0; q < 3; ++q) { Am[r][q] = A[r][q]; Bmm[r][q] = Bm[r][q]; Cmm[r][q] = Cm[r][q]; }
+          for (int q = 0; q < 3; ++q) {
+            *meet_word(L, 3 + 3 * r + q) = A[r][q];
+            *meet_word(L, 12 + 3 * r + q) = Bm[r][q];
+            *meet_word(L, 21 + 3 * r + q) = Cm[r][q];
+          }
         }
 #pragma unroll
-        for (int k = 0; k < K; ++k) { Um[k] = U0[k]; Wm[k] = W[k]; }
+        for (int k = 0; k < K; ++k) { *meet_word(L, 30 + k) = U0[k]; *meet_word(L, 30 + K + k) = W[k]; }
       }
       pm = pc; pc = pn; el = er; h_m = h_i; ifk_m = ifk_i;
     }
@@ -386,6 +416,19 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
 #pragma unroll
   for (int k = 0; k < K; ++k) z[k] = 0.0;
   if (top) {
+    double Am[3][3], Bmm[3][3], Cmm[3][3], rm[3], Um[K], Wm[K];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      rm[r] = *meet_word(L, r);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        Am[r][q] = *meet_word(L, 3 + 3 * r + q);
+        Bmm[r][q] = *meet_word(L, 12 + 3 * r + q);
+        Cmm[r][q] = *meet_word(L, 21 + 3 * r + q);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) { Um[k] = *meet_word(L, 30 + k); Wm[k] = *meet_word(L, 30 + K + k); }
     // gamma x_mid = [r | U]_mid - A d'_{mid-1} - C d''_{mid+1}, gamma = B - A c' - C a''
     double G[3][3], Gi[3][3];
 #pragma unroll
@@ -492,8 +535,10 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
     }
     double sz_dummy = 0.0;
     bool fin_dummy = true;
+    Pt px;
+    px.V = xb[0]; px.lnn = xb[1]; px.lnp = xb[2];
     damp(L, x1, px, pq, sz_dummy, fin_dummy);
-    pq.offn = px.offn; pq.offp = px.offp;
+    pq.offn = L.st(m + 1, S_OFFN); pq.offp = L.st(m + 1, S_OFFP);
     double R, d1, d2;
     recomb(L, m + 1, pq.n, pq.p, R, d1, d2);
     const double Ug = L.st(m + 1, S_G) * gfrac;
@@ -523,8 +568,7 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
       }
       xn[0] = x[0]; xn[1] = x[1]; xn[2] = x[2];
       Pt old;
-      if (p == nown) old = pb;
-      else { old.V = *L.y(0, i, 0); old.lnn = *L.y(0, i, 1); old.lnp = *L.y(0, i, 2); }
+      old.V = *L.y(0, i, 0); old.lnn = *L.y(0, i, 1); old.lnp = *L.y(0, i, 2);
       if (noise) {
         const double en = exp(old.lnn), ep = exp(old.lnp);
         out.size = nanmax(out.size, fabs(x[0]) * L.iVt);
@@ -637,7 +681,7 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
     out.size = nanmax(out.size, osize);
     out.finite = out.finite && ofin;
     if (!noise) {
-      const double H = L.Hsum;
+      const double H = L.Hsum();
       double tot = 0.0;
       if (!L.currdiff) {
         // half 0's suffix sums lack half 1's totals A_B and H_B; half 1's prefix sums are
@@ -664,7 +708,7 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
       } else {
         tot = cp.dtot + ot.dtot;
       }
-      out.J = -L.left * tot / H;
+      out.J = -L.left() * tot / H;
     } else {
       out.J = 0.0;
     }
@@ -683,10 +727,11 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
 
 // A point's potential and its mobile ions' densities only (the Poisson start and the ions'
 // normalisations need no more of it).
+template <int K>
 __device__ __forceinline__ void pt_ions(const Lane& L, Pt& P, int k, const double* logs) {
   P.sl = slots_at(L, k);
-  P.da = P.sl.a >= 0 ? exp(logs[P.sl.a] + P.V * L.iVt) : 0.0;
-  P.dc = P.sl.c >= 0 ? exp(logs[L.ka + P.sl.c] - P.V * L.iVt) : 0.0;
+  P.da = P.sl.a >= 0 ? exp(pick<K>(logs, P.sl.a) + P.V * L.iVt) : 0.0;
+  P.dc = P.sl.c >= 0 ? exp(pick<K>(logs, L.ka + P.sl.c) - P.V * L.iVt) : 0.0;
 }
 
 __device__ __forceinline__ void own_range(const Lane& L, int& lo, int& hi) {
@@ -709,12 +754,12 @@ __device__ void ion_logs(const Lane& L, double Vint, double* logs) {
   int e0, e1;
   if (L.half == 0) { e0 = 0; e1 = m; contact(L, 0, Vint, a); }
   else { e0 = m + 1; e1 = L.NP; a.V = vb; }
-  pt_ions(L, a, e0, zero);
+  pt_ions<K>(L, a, e0, zero);
   for (int e = e0; e <= e1; ++e) {
     if (e + 1 == L.NP + 1) contact(L, 1, Vint, b);
     else if (e + 1 == m + 1 && L.half == 0) b.V = vx;
     else b.V = *L.y(0, e + 1, 0);
-    pt_ions(L, b, e + 1, zero);
+    pt_ions<K>(L, b, e + 1, zero);
     ion_edge<K>(L, a, b, L.st(e, S_H) * L.L, num);
     a = b;
   }
@@ -746,8 +791,8 @@ __device__ double poisson_step(Lane& L, double Vint, bool coupled, double* logs)
   const int kb = top ? m : m + 1, kx = top ? m + 1 : m;
   pb.V = *L.y(0, kb, 0); pb.lnn = *L.y(0, kb, 1); pb.lnp = *L.y(0, kb, 2);
   px.V = xchg(L, pb.V); px.lnn = xchg(L, pb.lnn); px.lnp = xchg(L, pb.lnp);
-  pt_ions(L, pb, kb, logs);
-  pt_ions(L, px, kx, logs);
+  pt_ions<K>(L, pb, kb, logs);
+  pt_ions<K>(L, px, kx, logs);
   double num[K], w[K], dU[K], Sm[K][K], sv[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
@@ -773,8 +818,8 @@ __device__ double poisson_step(Lane& L, double Vint, bool coupled, double* logs)
     up = i < NP ? facu * sP : 0.0;
 #pragma unroll
     for (int k = 0; k < K; ++k) U[k] = 0.0;
-    if (pc.sl.a >= 0) U[pc.sl.a] = -Q * pc.da * sP;
-    if (pc.sl.c >= 0) U[L.ka + pc.sl.c] = Q * pc.dc * sP;
+    if (pc.sl.a >= 0) set_at<K>(U, pc.sl.a, -Q * pc.da * sP);
+    if (pc.sl.c >= 0) set_at<K>(U, L.ka + pc.sl.c, Q * pc.dc * sP);
     ion_w<K>(L, pm, pc, pn, hm * L.L, hp * L.L, W);
   };
   // X couples to the eliminated side, Y to the rest
@@ -803,15 +848,15 @@ __device__ double poisson_step(Lane& L, double Vint, bool coupled, double* logs)
   if (top) {
     Pt pm, pc, pn;
     contact(L, 0, Vint, pm);
-    pt_ions(L, pm, 0, logs);
+    pt_ions<K>(L, pm, 0, logs);
     if (m == 1) pc = pb;
-    else { pc.V = *L.y(0, 1, 0); pc.lnn = *L.y(0, 1, 1); pc.lnp = *L.y(0, 1, 2); pt_ions(L, pc, 1, logs); }
+    else { pc.V = *L.y(0, 1, 0); pc.lnn = *L.y(0, 1, 1); pc.lnp = *L.y(0, 1, 2); pt_ions<K>(L, pc, 1, logs); }
     double h_m = L.st(0, S_H);
     ion_edge<K>(L, pm, pc, h_m * L.L, num);
     for (int i = 1; i <= m; ++i) {
       if (i + 1 == m) pn = pb;
       else if (i == m) pn = px;
-      else { pn.V = *L.y(0, i + 1, 0); pn.lnn = *L.y(0, i + 1, 1); pn.lnp = *L.y(0, i + 1, 2); pt_ions(L, pn, i + 1, logs); }
+      else { pn.V = *L.y(0, i + 1, 0); pn.lnn = *L.y(0, i + 1, 1); pn.lnp = *L.y(0, i + 1, 2); pt_ions<K>(L, pn, i + 1, logs); }
       const double h_i = L.st(i, S_H);
       ion_edge<K>(L, pc, pn, h_i * L.L, num);
       double lo, mid, up, F, U[K], W[K];
@@ -827,15 +872,15 @@ __device__ double poisson_step(Lane& L, double Vint, bool coupled, double* logs)
   } else {
     Pt pl, pc, pn;
     contact(L, 1, Vint, pn);
-    pt_ions(L, pn, NP + 1, logs);
+    pt_ions<K>(L, pn, NP + 1, logs);
     if (NP == m + 1) pc = pb;
-    else { pc.V = *L.y(0, NP, 0); pc.lnn = *L.y(0, NP, 1); pc.lnp = *L.y(0, NP, 2); pt_ions(L, pc, NP, logs); }
+    else { pc.V = *L.y(0, NP, 0); pc.lnn = *L.y(0, NP, 1); pc.lnp = *L.y(0, NP, 2); pt_ions<K>(L, pc, NP, logs); }
     double h_i = L.st(NP, S_H);
     ion_edge<K>(L, pc, pn, h_i * L.L, num);
     for (int i = NP; i >= m + 1; --i) {
       if (i - 1 == m) pl = px;
       else if (i - 1 == m + 1) pl = pb;
-      else { pl.V = *L.y(0, i - 1, 0); pl.lnn = *L.y(0, i - 1, 1); pl.lnp = *L.y(0, i - 1, 2); pt_ions(L, pl, i - 1, logs); }
+      else { pl.V = *L.y(0, i - 1, 0); pl.lnn = *L.y(0, i - 1, 1); pl.lnp = *L.y(0, i - 1, 2); pt_ions<K>(L, pl, i - 1, logs); }
       const double h_m = L.st(i - 1, S_H);
       if (i - 1 >= m + 1) ion_edge<K>(L, pl, pc, h_m * L.L, num);
       double lo, mid, up, F, U[K], W[K];
@@ -943,7 +988,7 @@ __device__ void freeze(Lane& L, const double* logs) {
   for (int i = lo; i <= hi; ++i) {
     Pt P;
     P.V = *L.y(0, i, 0);
-    pt_ions(L, P, i, logs);
+    pt_ions<K>(L, P, i, logs);
     L.FX[((size_t)i * 2) * L.Bp + L.l] = L.afix(i) + P.da;
     L.FX[((size_t)i * 2 + 1) * L.Bp + L.l] = L.cfix(i) + P.dc;
   }
@@ -1026,11 +1071,8 @@ __device__ void lane_init(Lane& L, const Args& a, int l, int half) {
   L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l;
   L.ka = a.ka; L.K = K;
   L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L);
-  L.V0 = L.sc(C_V0); L.VL = L.sc(C_VL); L.left = L.sc(C_LEFT);
-  L.lnnL = L.sc(C_LNNL); L.lnpL = L.sc(C_LNPL); L.lnnR = L.sc(C_LNNR); L.lnpR = L.sc(C_LNPR);
-  L.Jscale = L.sc(C_JSCALE); L.Gshunt = L.sc(C_GSHUNT); L.gfrac = L.sc(C_GFRAC);
-  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor); L.Hsum = L.sc(C_HSUM);
-  L.NP = (int)L.sc(C_NP);
+      L.gfrac = L.sc(C_GFRAC);
+  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor);   L.NP = (int)L.sc(C_NP);
   L.mid = (int)L.sc(C_MID);
   L.currdiff = L.sc(C_CURRDIFF) > 0.0; L.simss = a.simss;
   // the slots' totals: rows past k_anion + k_cation need not exist in scal
@@ -1045,6 +1087,16 @@ __device__ void lane_init(Lane& L, const Args& a, int l, int half) {
   L.base = wl & ~1;
   L.mask = 3u << L.base;
 }
+
+// One lane's program bookkeeping between Newton steps (see solve_kernel).
+template <int K>
+struct Prog {
+  double lgA[K], lgB[K], lgC[K];  // normalisations: last carry, the one before, the stage start
+  double hs[4], hJ[4];            // the last four steps' sizes and currents
+  double noise_floor, before, Vlast, Vbefore;
+  int pit, ctx, it, cap, nsz, stage, k, below, last_keep, jcur, n_border, n_plain;
+  bool floor_known, pending_noise, ok_f, kept_f, solved, pre_ok, ok_c;
+};
 
 enum Phase { PH_POISSON = 0, PH_NEWTON, PH_DONE };
 enum Ctx {
@@ -1077,57 +1129,63 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
   }
   bool mobile = false;
 #pragma unroll
-  for (int k = 0; k < K; ++k) mobile = mobile || L.tot[k] > 0.0;
+  for (int q = 0; q < K; ++q) mobile = mobile || L.tot[q] > 0.0;
 
-  double logs[K], lgA[K], lgB[K], lgC[K];
+  // the program's bookkeeping between steps lives in shared memory (one record per thread),
+  // so that the sweeps have the registers to themselves
+  __shared__ Prog<K> progs[DD_SOLVE_BLOCK];
+  Prog<K>& g = progs[threadIdx.x];
+  double logs[K];
 #pragma unroll
-  for (int k = 0; k < K; ++k) { logs[k] = 0.0; lgA[k] = 0.0; lgB[k] = 0.0; lgC[k] = 0.0; }
-  int phase = PH_POISSON, pit = 0;
+  for (int q = 0; q < K; ++q) { logs[q] = 0.0; g.lgA[q] = 0.0; g.lgB[q] = 0.0; g.lgC[q] = 0.0; }
+  int phase = PH_POISSON;
+  g.pit = 0;
   const int pcap = jv ? a.max_iter : a.start_iter;
-  int ctx = 0, it = 0, cap = 0, adv = ADV_NONE;
+  int adv = ADV_NONE;
+  g.ctx = 0; g.it = 0; g.cap = 0;
   double Vint = first, ratio = 0.0;
-  double hs[4], hJ[4];
-  int nsz = 0;
-  bool floor_known = false, pending_noise = false;
-  double noise_floor = 0.0;
-  bool ok_f = false, kept_f = false, solved = false, pre_ok = true, ok_c = false;
-  int stage = 0;
-  double before = 1.0;
-  int k = 0, below = 0, last_keep = 0;
-  double Vlast = first, Vbefore = first;
-  int jcur = 0;
+  g.nsz = 0;
+  g.floor_known = false; g.pending_noise = false;
+  g.noise_floor = 0.0;
+  g.ok_f = false; g.kept_f = false; g.solved = false; g.pre_ok = true; g.ok_c = false;
+  g.stage = 0;
+  g.before = 1.0;
+  g.k = 0; g.below = 0; g.last_keep = 0;
+  g.Vlast = first; g.Vbefore = first;
+  g.jcur = 0;
+  g.n_border = 0; g.n_plain = 0;
   if (!jv) {
-    while (below < nv && Vl[below] < first) ++below;  // searchsorted, left
+    while (g.below < nv && Vl[g.below] < first) ++g.below;  // searchsorted, left
   }
   if (top) a.status[l] = DD_LANE_OK;
 
   auto begin = [&](int c, double v, double share, int cp_, int ad, double ra) {
-    ctx = c; Vint = v; L.share = share; cap = cp_; adv = ad; ratio = ra;
-    it = 0; nsz = 0; floor_known = false; pending_noise = false;
+    g.ctx = c; Vint = v; L.share = share; g.cap = cp_; adv = ad; ratio = ra;
+    g.it = 0; g.nsz = 0; g.floor_known = false; g.pending_noise = false;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) { hs[q] = INFINITY; hJ[q] = INFINITY; }
+    for (int q = 0; q < 4; ++q) { g.hs[q] = INFINITY; g.hJ[q] = INFINITY; }
     phase = PH_NEWTON;
   };
   auto scan_begin = [&]() {
-    if (k >= nv) { phase = PH_DONE; return; }
+    if (g.k >= nv) { phase = PH_DONE; return; }
     if (!jv) {
-      jcur = k < nv - below ? below + k : nv - 1 - k;
-      const double v = Vl[jcur];
-      if (k == 0 || k == nv - below) {
-        Vlast = first; Vbefore = first;
-        copyv<K>(logs, lgC); copyv<K>(lgA, lgC); copyv<K>(lgB, lgC);
+      g.jcur = g.k < nv - g.below ? g.below + g.k : nv - 1 - g.k;
+      const double v = Vl[g.jcur];
+      if (g.k == 0 || g.k == nv - g.below) {
+        g.Vlast = first; g.Vbefore = first;
+        copyv<K>(logs, g.lgC); copyv<K>(g.lgA, g.lgC); copyv<K>(g.lgB, g.lgC);
         begin(X_SCAN, v, 1.0, a.max_iter, ADV_TURN, 0.0);
       } else {
-        const double ra = Vlast != Vbefore ? (v - Vlast) / (Vlast - Vbefore) : 0.0;
+        const double ra = g.Vlast != g.Vbefore ? (v - g.Vlast) / (g.Vlast - g.Vbefore) : 0.0;
 #pragma unroll
         for (int q = 0; q < K; ++q)
-          logs[q] = lgA[q] + (ra != 0.0 ? clipd(ra * (lgA[q] - lgB[q]), -ION_LOG_CAP, ION_LOG_CAP) : 0.0);
-        begin(X_SCAN, v, 1.0, a.max_iter, last_keep ? ADV_KEEP : ADV_NOKEEP, ra);
+          logs[q] = g.lgA[q] + (ra != 0.0 ? clipd(ra * (g.lgA[q] - g.lgB[q]), -ION_LOG_CAP, ION_LOG_CAP) : 0.0);
+        begin(X_SCAN, v, 1.0, a.max_iter, g.last_keep ? ADV_KEEP : ADV_NOKEEP, ra);
       }
     } else {
-      jcur = k;
-      copyv<K>(logs, lgA);
-      begin(X_JV_SCAN, Vl[k], 1.0, a.max_iter, last_keep ? ADV_KEEP : ADV_NOKEEP, 0.0);
+      g.jcur = g.k;
+      copyv<K>(logs, g.lgA);
+      begin(X_JV_SCAN, Vl[g.k], 1.0, a.max_iter, g.last_keep ? ADV_KEEP : ADV_NOKEEP, 0.0);
     }
   };
   auto freeze_and_scan = [&]() {
@@ -1136,30 +1194,30 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
     if (!jv) {
       const bool fr = pre_cond && fix_ions;
       if (fr) freeze<K>(L, logs);
-      pre_ok = pre_ok || !fr;
+      g.pre_ok = g.pre_ok || !fr;
       copy_state(L, 3, 0);
-      copyv<K>(lgC, logs);
-      k = 0;
+      copyv<K>(g.lgC, logs);
+      g.k = 0;
       scan_begin();
     } else {
       if (pre_cond && fix_ions) freeze<K>(L, logs);
       copy_state(L, 1, 0);  // the carry: the first voltage's ADV_KEEP reads it
-      copyv<K>(lgA, logs);
-      k = 0; last_keep = 1;  // the start is the carry
+      copyv<K>(g.lgA, logs);
+      g.k = 0; g.last_keep = 1;  // the start is the carry
       scan_begin();
     }
   };
   auto batch_pre = [&]() {
     L.share = 1.0;
-    if (solved) { pre_ok = true; freeze_and_scan(); }
+    if (g.solved) { g.pre_ok = true; freeze_and_scan(); }
     else begin(X_PRE, first, 1.0, a.start_iter, ADV_NONE, 0.0);
   };
   auto stage_begin = [&]() {
-    const double share = c_stage_share[stage];
-    const double sh = log(share / before);
+    const double share = c_stage_share[g.stage];
+    const double sh = log(share / g.before);
 #pragma unroll
     for (int q = 0; q < K; ++q) logs[q] += sh;
-    if (!jv) { copy_state(L, 3, 0); copyv<K>(lgC, logs); }
+    if (!jv) { copy_state(L, 3, 0); copyv<K>(g.lgC, logs); }
     begin(jv ? X_JV_STAGE : X_STAGE, first, share, jv ? a.max_iter : a.start_iter, ADV_NONE, 0.0);
   };
   auto jv_pre = [&]() {
@@ -1168,21 +1226,20 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
     else freeze_and_scan();
   };
 
-  int n_border = 0, n_plain = 0;
   while (phase != PH_DONE) {
     if (phase == PH_POISSON) {
       const double size = poisson_step<K>(L, first, jv ? mobile : true, logs);
-      ++pit;
-      const bool stop = jv ? (size < POISSON_TOL || pit >= pcap) : (!(size > POISSON_TOL) || pit >= pcap);
+      ++g.pit;
+      const bool stop = jv ? (size < POISSON_TOL || g.pit >= pcap) : (!(size > POISSON_TOL) || g.pit >= pcap);
       if (!stop) continue;
       ion_logs<K>(L, first, logs);
       if (!jv) {
         copy_state(L, 1, 0);
-        copyv<K>(lgA, logs);
+        copyv<K>(g.lgA, logs);
         begin(X_START_F, first, 1.0, a.start_iter, ADV_NONE, 0.0);
       } else if (mobile) {
         copy_state(L, 1, 0);
-        copyv<K>(lgA, logs);
+        copyv<K>(g.lgA, logs);
         begin(X_JV_START, first, 1.0, a.max_iter, ADV_NONE, 0.0);
       } else {
         jv_pre();
@@ -1191,134 +1248,136 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
     }
     bool end = false, conv = false, fin = true;
     double Jv = 0.0;
-    if (pending_noise) {
-      const StepOut o = newton_step<K>(L, Vint, logs, ADV_NONE, 0.0, true);
-      ++n_plain;
-      noise_floor = o.size; floor_known = true; pending_noise = false;
+    // one call site of the step (the round-off step with `noise`): the step's code once
+    const bool noise = g.pending_noise;
+    const StepOut o = newton_step<K>(L, Vint, logs, noise ? (int)ADV_NONE : adv,
+                                     noise ? 0.0 : ratio, noise);
+    if (noise) {
+      ++g.n_plain;
+      g.noise_floor = o.size; g.floor_known = true; g.pending_noise = false;
       double mx = 0.0;
-      for (int q = 4 - (nsz < 4 ? nsz : 4); q < 4; ++q) mx = nanmax(mx, hs[q]);
-      if (mx < noise_floor) { end = true; conv = true; }
-      else if (it >= cap) { end = true; conv = false; }
-      Jv = hJ[3];
+      for (int q = 4 - (g.nsz < 4 ? g.nsz : 4); q < 4; ++q) mx = nanmax(mx, g.hs[q]);
+      if (mx < g.noise_floor) { end = true; conv = true; }
+      else if (g.it >= g.cap) { end = true; conv = false; }
+      Jv = g.hJ[3];
       if (!end) continue;
     } else {
-      const StepOut o = newton_step<K>(L, Vint, logs, adv, ratio, false);
       adv = ADV_NONE;
-      ++it;
+      ++g.it;
       bool border = false;
 #pragma unroll
       for (int q = 0; q < K; ++q) border = border || L.total(q) > 0.0;
-      if (border) ++n_border; else ++n_plain;
+      if (border) ++g.n_border; else ++g.n_plain;
 #pragma unroll
-      for (int q = 0; q < 3; ++q) { hs[q] = hs[q + 1]; hJ[q] = hJ[q + 1]; }
-      hs[3] = o.size; hJ[3] = o.J;
-      ++nsz;
+      for (int q = 0; q < 3; ++q) { g.hs[q] = g.hs[q + 1]; g.hJ[q] = g.hJ[q + 1]; }
+      g.hs[3] = o.size; g.hJ[3] = o.J;
+      ++g.nsz;
       Jv = o.J;
       fin = o.finite && finitev<K>(logs);
       const double size = o.size;
       const bool isn = size != size;
-      const bool settle = ctx >= X_JV_START;
+      const bool settle = g.ctx >= X_JV_START;
       if (!settle) {
-        double mx = hs[0], mn = hs[1];
+        double mx = g.hs[0], mn = g.hs[1];
 #pragma unroll
-        for (int q = 1; q < 4; ++q) mx = nanmax(mx, hs[q]);
+        for (int q = 1; q < 4; ++q) mx = nanmax(mx, g.hs[q]);
 #pragma unroll
-        for (int q = 2; q < 4; ++q) mn = (hs[q] < mn || hs[q] != hs[q]) ? hs[q] : mn;
-        const bool stalled = it > STALL_STEPS && mx < ROUND_OFF_FLOOR && mn >= 0.1 * hs[0];
+        for (int q = 2; q < 4; ++q) mn = (g.hs[q] < mn || g.hs[q] != g.hs[q]) ? g.hs[q] : mn;
+        const bool stalled = g.it > STALL_STEPS && mx < ROUND_OFF_FLOOR && mn >= 0.1 * g.hs[0];
         double dJ = 0.0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) dJ = nanmax(dJ, fabs(hJ[q] - hJ[3]));
-        const bool settled = it > STALL_STEPS && size < CURRENT_STEP_CAP &&
-                             dJ < CURRENT_TOL * (L.Jscale + fabs(hJ[3]));
-        const bool quad = it > 1 && size < QUADRATIC_TOL && size < QUADRATIC_RATIO * hs[2];
+        for (int q = 0; q < 4; ++q) dJ = nanmax(dJ, fabs(g.hJ[q] - g.hJ[3]));
+        const bool settled = g.it > STALL_STEPS && size < CURRENT_STEP_CAP &&
+                             dJ < CURRENT_TOL * (L.Jscale() + fabs(g.hJ[3]));
+        const bool quad = g.it > 1 && size < QUADRATIC_TOL && size < QUADRATIC_RATIO * g.hs[2];
         conv = a.strict ? (size < a.tol || stalled) : (size < a.tol || stalled || settled || quad);
-        end = conv || it >= cap || isn;
+        end = conv || g.it >= g.cap || isn;
       } else {
         if (isn) { end = true; conv = false; }
         else {
-          const int n4 = nsz < 4 ? nsz : 4;
+          const int n4 = g.nsz < 4 ? g.nsz : 4;
           double mx = 0.0, mn = INFINITY;
-          for (int q = 4 - n4; q < 4; ++q) mx = nanmax(mx, hs[q]);
-          for (int q = 4 - n4 + 1; q < 4; ++q) mn = fmin(mn, hs[q]);
-          bool done = size < a.tol || (nsz >= 4 && mx < ROUND_OFF_FLOOR && mn >= 0.1 * hs[0]);
-          if (!done && nsz >= 4 && mx < NOISE_FLOOR_CAP) {
-            if (!floor_known) { pending_noise = true; continue; }
-            done = mx < noise_floor;
+          for (int q = 4 - n4; q < 4; ++q) mx = nanmax(mx, g.hs[q]);
+          for (int q = 4 - n4 + 1; q < 4; ++q) mn = fmin(mn, g.hs[q]);
+          bool done = size < a.tol || (g.nsz >= 4 && mx < ROUND_OFF_FLOOR && mn >= 0.1 * g.hs[0]);
+          if (!done && g.nsz >= 4 && mx < NOISE_FLOOR_CAP) {
+            if (!g.floor_known) { g.pending_noise = true; continue; }
+            done = mx < g.noise_floor;
           }
           if (done) { end = true; conv = true; }
-          else if (it >= cap) { end = true; conv = false; }
+          else if (g.it >= g.cap) { end = true; conv = false; }
         }
       }
       if (!end) continue;
     }
-    switch (ctx) {
+    switch (g.ctx) {
       case X_START_F: {
-        ok_f = conv; kept_f = fin;
-        if (ok_f || !mobile) {
-          if (!kept_f) { copy_state(L, 0, 1); copyv<K>(logs, lgA); }
-          solved = ok_f;
+        g.ok_f = conv; g.kept_f = fin;
+        if (g.ok_f || !mobile) {
+          if (!g.kept_f) { copy_state(L, 0, 1); copyv<K>(logs, g.lgA); }
+          g.solved = g.ok_f;
           batch_pre();
         } else {
-          copy_state(L, 2, 0); copyv<K>(lgB, logs);
-          copy_state(L, 0, 1); copyv<K>(logs, lgA);
-          before = 1.0; stage = 0;
+          copy_state(L, 2, 0); copyv<K>(g.lgB, logs);
+          copy_state(L, 0, 1); copyv<K>(logs, g.lgA);
+          g.before = 1.0; g.stage = 0;
           stage_begin();
         }
         break;
       }
       case X_STAGE: {
-        ok_c = conv;
-        if (!fin) { copy_state(L, 0, 3); copyv<K>(logs, lgC); }
-        before = c_stage_share[stage];
-        ++stage;
-        if (stage < 4) { stage_begin(); break; }
-        const bool staged = ok_c;
+        g.ok_c = conv;
+        if (!fin) { copy_state(L, 0, 3); copyv<K>(logs, g.lgC); }
+        g.before = c_stage_share[g.stage];
+        ++g.stage;
+        if (g.stage < 4) { stage_begin(); break; }
+        const bool staged = g.ok_c;
         if (!staged) {
-          if (kept_f) { copy_state(L, 0, 2); copyv<K>(logs, lgB); }
-          else { copy_state(L, 0, 1); copyv<K>(logs, lgA); }
+          if (g.kept_f) { copy_state(L, 0, 2); copyv<K>(logs, g.lgB); }
+          else { copy_state(L, 0, 1); copyv<K>(logs, g.lgA); }
         }
-        solved = staged;
+        g.solved = staged;
         batch_pre();
         break;
       }
       case X_PRE: {
-        pre_ok = conv;
+        g.pre_ok = conv;
         freeze_and_scan();
         break;
       }
       case X_SCAN: {
-        const int pos = voff + jcur;
+        const int pos = voff + g.jcur;
         if (top) {
-          a.J[pos] = Jv + L.Gshunt * Vint;
-          a.ok[pos] = (conv && pre_ok) ? 1 : 0;
-          a.its[pos] = it;
+          a.J[pos] = Jv + L.Gshunt() * Vint;
+          a.ok[pos] = (conv && g.pre_ok) ? 1 : 0;
+          a.its[pos] = g.it;
         }
-        if (a.states && jcur < a.nv_max)
-          save_state<K>(L, a.states + (size_t)jcur * (a.npmax + 2) * 3 * a.Bp,
-                        a.state_logs + (size_t)jcur * DD_MAXK * a.Bp, logs);
+        if (a.states && g.jcur < a.nv_max)
+          save_state<K>(L, a.states + (size_t)g.jcur * (a.npmax + 2) * 3 * a.Bp,
+                        a.state_logs + (size_t)g.jcur * DD_MAXK * a.Bp, logs);
         const bool keep = conv && fin;
         if (keep) {
-          copyv<K>(lgB, lgA); copyv<K>(lgA, logs);
-          Vbefore = Vlast; Vlast = Vint; last_keep = 1;
+          copyv<K>(g.lgB, g.lgA); copyv<K>(g.lgA, logs);
+          g.Vbefore = g.Vlast; g.Vlast = Vint; g.last_keep = 1;
         } else {
-          last_keep = 0;
+          g.last_keep = 0;
         }
-        ++k;
+        ++g.k;
         scan_begin();
         break;
       }
       case X_JV_START: {
         if (conv) { jv_pre(); break; }
-        copy_state(L, 0, 1); copyv<K>(logs, lgA);
-        before = 1.0; stage = 0;
+        copy_state(L, 0, 1); copyv<K>(logs, g.lgA);
+        g.before = 1.0; g.stage = 0;
         stage_begin();
         break;
       }
       case X_JV_STAGE: {
-        before = c_stage_share[stage];
-        if (!conv) { copy_state(L, 0, 1); copyv<K>(logs, lgA); jv_pre(); break; }
-        ++stage;
-        if (stage < 4) stage_begin();
+        g.before = c_stage_share[g.stage];
+        if (!conv) { copy_state(L, 0, 1); copyv<K>(logs, g.lgA); jv_pre(); break; }
+        ++g.stage;
+        if (g.stage < 4) stage_begin();
         else jv_pre();
         break;
       }
@@ -1335,28 +1394,28 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
         break;
       }
       case X_JV_SCAN: {
-        const int pos = voff + jcur;
+        const int pos = voff + g.jcur;
         if (top) {
-          a.J[pos] = Jv + L.Gshunt * Vint;
+          a.J[pos] = Jv + L.Gshunt() * Vint;
           a.ok[pos] = conv ? 1 : 0;
-          a.its[pos] = it;
+          a.its[pos] = g.it;
         }
-        if (a.states && jcur < a.nv_max)
-          save_state<K>(L, a.states + (size_t)jcur * (a.npmax + 2) * 3 * a.Bp,
-                        a.state_logs + (size_t)jcur * DD_MAXK * a.Bp, logs);
+        if (a.states && g.jcur < a.nv_max)
+          save_state<K>(L, a.states + (size_t)g.jcur * (a.npmax + 2) * 3 * a.Bp,
+                        a.state_logs + (size_t)g.jcur * DD_MAXK * a.Bp, logs);
         const bool keep = conv && fin;
-        if (keep) { copyv<K>(lgA, logs); last_keep = 1; }
-        else last_keep = 0;
-        ++k;
+        if (keep) { copyv<K>(g.lgA, logs); g.last_keep = 1; }
+        else g.last_keep = 0;
+        ++g.k;
         scan_begin();
         break;
       }
     }
   }
   if (a.steps && top) {
-    a.steps[l] = n_border;
-    a.steps[a.Bp + l] = n_plain;
-    a.steps[2 * a.Bp + l] = pit;
+    a.steps[l] = g.n_border;
+    a.steps[a.Bp + l] = g.n_plain;
+    a.steps[2 * a.Bp + l] = g.pit;
   }
 }
 
@@ -1389,12 +1448,6 @@ namespace {
 
 int slots_k(const dd_batch* b) { return b->k_anion + b->k_cation <= 2 ? 2 : 4; }
 
-// Threads per block of the solve (two per device, the pairs adjacent lanes of a warp). One warp
-// a block spreads a batch's warps over the 148 SMs more evenly than two (at the drawn J-V curves' 16384
-// devices: at most 7 warps on an SM instead of 8; 2.2 % faster measured).
-#ifndef DD_SOLVE_BLOCK
-#define DD_SOLVE_BLOCK 32
-#endif
 
 size_t ws_elems(const dd_batch* b, size_t* y_e, size_t* fx_e, size_t* cd_e, int* ncd) {
   const int K = slots_k(b);

@@ -47,9 +47,7 @@ __global__ void __launch_bounds__(64) observe_kernel(Args a) {
   Lane L;
   L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l; L.ka = a.ka; L.K = K;
   L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L);
-  L.V0 = L.sc(C_V0); L.VL = L.sc(C_VL); L.left = L.sc(C_LEFT);
-  L.lnnL = L.sc(C_LNNL); L.lnpL = L.sc(C_LNPL); L.lnnR = L.sc(C_LNNR); L.lnpR = L.sc(C_LNPR);
-  L.gfrac = L.sc(C_GFRAC);
+      L.gfrac = L.sc(C_GFRAC);
   L.NP = (int)L.sc(C_NP);
   L.share = 1.0; L.frozen = false; L.FX = nullptr; L.CD = nullptr; L.ybuf = 0;
   const int NP = L.NP;

@@ -314,7 +314,7 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     pa = pb;
     qa = qb;
   }
-  const double H = L.Hsum;
+  const double H = L.Hsum();
   double tot = 0.0;
   // ZimT 5.36's ion currents with several regions: each species' last region's alone
   int last_a = -1, last_c = -1;
@@ -368,7 +368,7 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     }
   }
   tot += dti * disp / L.L;
-  return -L.left * tot / H;
+  return -L.left() * tot / H;
 }
 
 // ------------------------------------------------------------------------------------ columns
@@ -405,7 +405,7 @@ __device__ __noinline__ void columns_t(const Args& a, const View& W, int cur, do
     i1[j] = j < nl ? (int)a.LAY[(size_t)(nl + j) * Bp + l] : -1;
     qf[j] = hs[j] = gen[j] = dir[j] = bn[j] = bp[j] = jin[j] = jip[j] = vl[j] = 0.0;
   }
-  const double QL = Q * L.L, sg = -L.left;
+  const double QL = Q * L.L, sg = -L.left();
   TP pa, pb, qa, qb;
   load_point(W, cur, 0, Vint, pa);
   contact_ions(W, cur, 0, dti, pa);
@@ -547,7 +547,7 @@ __device__ __noinline__ void columns_t(const Args& a, const View& W, int cur, do
   dev2 += (last_tot - J) * (last_tot - J);
   if (err) *err = sqrt(dev2 / (NP + 1));
   if (!a.COL) return;
-  const double H = L.Hsum;
+  const double H = L.Hsum();
   const int ncol = COL_SCALARS + 8 * nl;
   double* out = a.COL + (size_t)step * ncol * Bp + l;
   out[0] = sqrt(dev2 / (NP + 1));
@@ -950,17 +950,17 @@ __device__ __noinline__ void vint_row(const Args& a, const View& W, int bn, int 
   const double* FB = a.FB;
   const double* FI = a.FI;
   const double Rs = a.rser[l];
-  const double Je = current_t<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI) + L.Gshunt * Vi;
-  res = -(oc ? Je / L.Jscale : (Vi + Rs * Je - Vext) * L.iVt);
+  const double Je = current_t<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI) + L.Gshunt() * Vi;
+  res = -(oc ? Je / L.Jscale() : (Vi + Rs * Je - Vext) * L.iVt);
   const double eV = VINT_H * L.Vt;
   const double dJV = (current_t<K>(W, bn, Vi + eV, bk, V_now, dti, dti_now, FB, FI) -
                       current_t<K>(W, bn, Vi - eV, bk, V_now, dti, dti_now, FB, FI)) /
                          (2.0 * eV) +
-                     L.Gshunt;
+                     L.Gshunt();
 #pragma unroll
   for (int q = 0; q < K; ++q) row[q] = 0.0;
-  row[K] = oc ? dJV / L.Jscale : (1.0 + Rs * dJV) * L.iVt;
-  const double coef = oc ? 1.0 / L.Jscale : Rs * L.iVt;
+  row[K] = oc ? dJV / L.Jscale() : (1.0 + Rs * dJV) * L.iVt;
+  const double coef = oc ? 1.0 / L.Jscale() : Rs * L.iVt;
   if (coef == 0.0) return;  // V_int = V_ext: a row of the voltage alone
   for (int c = 0; c < NC; ++c) {
     double m = 0.0;
@@ -998,11 +998,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   L.S = a.S; L.C = a.C; L.IFt = a.IFt; L.Bp = a.Bp; L.l = l;
   L.NP = (int)L.sc(C_NP);
   L.ka = a.ka; L.K = K;
-  L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L); L.V0 = L.sc(C_V0); L.VL = L.sc(C_VL);
-  L.left = L.sc(C_LEFT); L.lnnL = L.sc(C_LNNL); L.lnpL = L.sc(C_LNPL); L.lnnR = L.sc(C_LNNR);
-  L.lnpR = L.sc(C_LNPR); L.Jscale = L.sc(C_JSCALE); L.Gshunt = L.sc(C_GSHUNT);
-  L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor); L.Hsum = L.sc(C_HSUM);
-  L.currdiff = L.sc(C_CURRDIFF) > 0.0; L.simss = a.simss;
+  L.Vt = L.sc(C_VT); L.iVt = 1.0 / L.Vt; L.L = L.sc(C_L);       L.nfloor = L.sc(C_NFLOOR); L.lognf = log(L.nfloor);   L.currdiff = L.sc(C_CURRDIFF) > 0.0; L.simss = a.simss;
   L.frozen = false; L.share = 1.0;
   // the slots' totals: rows past k_anion + k_cation need not exist in scal
 #pragma unroll
@@ -1102,7 +1098,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
 #pragma unroll
     for (int q = 0; q < K; ++q) num[q] = 0.0;
     {
-      double Vprev = L.V0 + 0.5 * L.left * Vi;
+      double Vprev = L.V0() + 0.5 * L.left() * Vi;
       Slots slp = slots_at(L, 0);
       for (int i = 1; i <= NP + 1; ++i) {
         double V;
@@ -1122,7 +1118,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
           a.BD[ob + 3 * Bp] = sl.c >= 0 ? exp(*W.y(bk, i, 4)) : 0.0;
           V = *W.y(bn, i, 0);
         } else {
-          V = L.VL - 0.5 * L.left * Vi;
+          V = L.VL() - 0.5 * L.left() * Vi;
         }
         if (!(dti > 0.0)) {
           const Slots sl = slots_at(L, i);
@@ -1199,8 +1195,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         double uv[5];
 #pragma unroll
         for (int rr = 0; rr < 5; ++rr)
-          uv[rr] = VINT ? (i == 1 ? A[rr][0] * 0.5 * L.left : 0.0) +
-                              (i == NP ? Cm[rr][0] * (-0.5 * L.left) : 0.0)
+          uv[rr] = VINT ? (i == 1 ? A[rr][0] * 0.5 * L.left() : 0.0) +
+                              (i == NP ? Cm[rr][0] * (-0.5 * L.left()) : 0.0)
                         : 0.0;
         ivl[0] = ivr[0];
         ivl[1] = ivr[1];
@@ -1399,14 +1395,14 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       for (int q = 0; q <= STALL_STEPS; ++q) jdev = nanmax(jdev, fabs(jh[q] - J));
       const bool stalled = it > STALL_STEPS && smax < ROUND_OFF_FLOOR && smin1 >= 0.1 * sh[0];
       const bool settled = !VINT && it > STALL_STEPS && size < CURRENT_STEP_CAP &&
-                           jdev < CURRENT_TOL * (L.Jscale + fabs(J));
+                           jdev < CURRENT_TOL * (L.Jscale() + fabs(J));
       const bool quad = it > 1 && size < QUADRATIC_TOL &&
                         size < QUADRATIC_RATIO * sh[STALL_STEPS - 1];
       done = size < a.tol || stalled || settled || quad;
     }
     const bool ok = done;
     const double J = jh[STALL_STEPS];
-    const double J_ext = J + L.Gshunt * Vi;
+    const double J_ext = J + L.Gshunt() * Vi;
     if (a.prof_state) write_profile(a, W, bn, k, Vi, dti);
     double err_k = 0.0;  // the step's errJ, where its convVar compares currents
     if (a.COL || cv != 1)
