@@ -92,7 +92,7 @@ typedef struct dd_opts {
 } dd_opts;
 
 /* Scratch bytes dd_solve needs for this batch (four state buffers, the frozen-ion profile,
- * the sweep's c'/d' per node, per-lane records). */
+ * the sweep's c'/d' per node, the work queue's counter). */
 int dd_workspace_bytes(const dd_batch* batch, size_t* bytes);
 
 /* The J-V curves of a batch: jaxdd's solve_batch (DD_MODE_BATCH; batch.py:1136-1162, one pass
@@ -101,10 +101,28 @@ int dd_workspace_bytes(const dd_batch* batch, size_t* bytes);
  * iterations at each flat voltage position; lane_status per lane; lane_steps (may be NULL)
  * [3][lane_stride] the steps each lane took in all: Newton steps with the ions' border (mobile
  * ions), Newton steps without it, Poisson steps. Asynchronous on `stream` (a cudaStream_t,
- * NULL the legacy default stream). */
+ * NULL the legacy default stream). A batch of more devices than the GPU holds at once is solved
+ * from a work queue (each pair of threads takes the next device when its own is done, in lane
+ * order) unless dd_tune chose otherwise for its shape; the results do not depend on it. */
 int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts, double* J,
              uint8_t* converged, int32_t* iterations, int32_t* lane_status, int32_t* lane_steps,
              void* workspace, size_t workspace_bytes, void* stream);
+
+/* Launch forms of the solve (threads per block; the work queue for a batch larger than the GPU
+ * holds at once, or one pair of threads per device) that dd_tune chooses among. */
+#define DD_SOLVE_FORMS 4
+
+/* The solve's autotuner: runs dd_solve on this batch once in each launch form (synchronising
+ * `stream` to time each with events), keeps the fastest for later dd_solve and dd_solve_states
+ * calls in this process on batches of the same shape (device, ion slots, np_max, lane count
+ * within a factor of two), and returns its index in `form` and, unless NULL, each form's time
+ * in `times_ms` [DD_SOLVE_FORMS]. The outputs are dd_solve's (every form gives the same). Untuned
+ * shapes take form 0. No counterpart in the reference, which compiles one XLA program per
+ * shape. */
+int dd_tune(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts, double* J,
+            uint8_t* converged, int32_t* iterations, int32_t* lane_status, int32_t* lane_steps,
+            void* workspace, size_t workspace_bytes, void* stream, int32_t* form,
+            float* times_ms);
 
 /* dd_solve that also keeps what differentiating the curves needs (jaxdd keeps the same under
  * `jax.checkpoint`: the converged solution per voltage, `_tangent`, batch.py:676-680): for each

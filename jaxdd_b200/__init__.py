@@ -9,7 +9,7 @@ GPU (no CPU fallback: without the built library the solvers raise).
 """
 
 from .batch import (Batch, external_voltages, prepare, solve_batch, solve_states,
-                    solve_uneven)
+                    solve_uneven, tune)
 from .device import Device, build_device, layer_points, make_grid
 from .simss_input import (TVG, Layer, Setup, check_supported, read_setup, read_tvg,
                           setup_from_texts, simss_voltages)
@@ -22,5 +22,5 @@ __all__ = [
     "Batch", "Device", "JVResult", "Layer", "Setup", "TVG", "TransientResult", "TransientState",
     "build_device", "check_supported", "external_voltages", "layer_points", "make_grid",
     "prepare", "read_setup", "read_tvg", "setup_from_texts", "simss_voltages", "solve_batch",
-    "solve_jv", "solve_states", "solve_transient", "solve_uneven",
+    "solve_jv", "solve_states", "solve_transient", "solve_uneven", "tune",
 ]

@@ -34,7 +34,7 @@ DD_PRECISION = {"fp64": 0, "mixed": 1}
 DD_LANE_PREBIAS_FAILED = 1
 
 #: every symbol include/jaxdd_b200.h declares
-EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve",
+EXPORTS = ("dd_abi_version", "dd_status_string", "dd_workspace_bytes", "dd_solve", "dd_tune",
            "dd_newton_step", "dd_solve_noalloc", "dd_solve_states", "dd_adjoint_workspace_bytes",
            "dd_adjoint", "dd_observables", "dd_admittance_workspace_bytes", "dd_admittance",
            "dd_build", "dd_transient_workspace_bytes", "dd_transient",
@@ -57,6 +57,10 @@ DD_MAXLAYERS = 16
 #: dd_solve_noalloc's fixed scratch (include/jaxdd_b200.h DD_NOALLOC_SCRATCH_BYTES)
 DD_NOALLOC_SCRATCH_BYTES = 64 << 20
 DD_ERR_SCRATCH = 5
+#: include/jaxdd_b200.h DD_SOLVE_FORMS: the solve's launch forms (block, work queue)
+DD_SOLVE_FORMS = 4
+SOLVE_FORMS = ({"block": 32, "queue": True}, {"block": 64, "queue": True},
+               {"block": 32, "queue": False}, {"block": 64, "queue": False})
 
 
 class DdBatch(ctypes.Structure):
@@ -125,6 +129,9 @@ def lib() -> ctypes.CDLL:
     so.dd_solve.restype = ctypes.c_int
     so.dd_solve.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
                             ctypes.POINTER(DdOpts), p, p, p, p, p, p, ctypes.c_size_t, p]
+    so.dd_tune.restype = ctypes.c_int
+    so.dd_tune.argtypes = [ctypes.POINTER(DdBatch), ctypes.POINTER(DdVoltages),
+                           ctypes.POINTER(DdOpts), p, p, p, p, p, p, ctypes.c_size_t, p, p, p]
     so.dd_newton_step.restype = ctypes.c_int
     so.dd_newton_step.argtypes = [ctypes.POINTER(DdBatch), p, p, p, ctypes.c_double,
                                   ctypes.POINTER(DdOpts), p, p, p, ctypes.c_size_t, p]

@@ -284,10 +284,12 @@ def descriptor(batch: Batch, g, y0) -> _lib.DdBatch:
 
 def run(batch: Batch, volts_lane: list[np.ndarray], firsts: np.ndarray, *, tol: float,
         max_iter: int, start_iter: int, strict: bool, bernoulli_name: str, mode: int,
-        precision: str = "fp64", jv_start: bool = False, sync: bool = True):
+        precision: str = "fp64", jv_start: bool = False, sync: bool = True,
+        tune: bool = False):
     """Launch the solve on the packed batch. `volts_lane[k]`: device k's voltages in the order
     the kernel takes them; `firsts[k]`: its start voltage. Returns device tensors
-    (J, ok, its, status) in lane order and the flat offsets."""
+    (J, ok, its, status) in lane order and the flat offsets. `tune`: through the autotuner
+    (`dd_tune`, every launch form timed once), its choice left in `batch["_tuned"]`."""
     import torch
     g = _gpu(batch)
     B, Bp, npmax = batch["n"], batch["Bp"], batch["np_max"]
@@ -322,10 +324,18 @@ def run(batch: Batch, volts_lane: list[np.ndarray], firsts: np.ndarray, *, tol: 
                        _lib.DD_BERNOULLI[bernoulli_name], mode, _lib.DD_PRECISION[precision], 0)
     ws = g.workspace(desc)
     stream = torch.cuda.current_stream().cuda_stream
-    _lib.check(_lib.lib().dd_solve(ctypes.byref(desc), ctypes.byref(volts), ctypes.byref(opts),
-                                   J.data_ptr(), ok.data_ptr(), its.data_ptr(), status.data_ptr(),
-                                   steps.data_ptr(), ws.data_ptr(), ws.numel(), stream),
-               "dd_solve")
+    outs = (J.data_ptr(), ok.data_ptr(), its.data_ptr(), status.data_ptr(), steps.data_ptr(),
+            ws.data_ptr(), ws.numel(), stream)
+    if tune:
+        form = ctypes.c_int32(-1)
+        times = (ctypes.c_float * _lib.DD_SOLVE_FORMS)()
+        _lib.check(_lib.lib().dd_tune(ctypes.byref(desc), ctypes.byref(volts), ctypes.byref(opts),
+                                      *outs, ctypes.byref(form), times), "dd_tune")
+        batch["_tuned"] = dict(_lib.SOLVE_FORMS[form.value], form=form.value,
+                               times_ms=[float(t) for t in times])
+    else:
+        _lib.check(_lib.lib().dd_solve(ctypes.byref(desc), ctypes.byref(volts),
+                                       ctypes.byref(opts), *outs), "dd_solve")
     batch["_last_steps"] = steps
     if sync:
         torch.cuda.synchronize()
@@ -358,6 +368,23 @@ def solve_batch(batch: Batch, voltages, tol: float = 1e-10, max_iter: int = 60,
         strict=strict, bernoulli_name=bernoulli_name, mode=_lib.DD_MODE_BATCH,
         precision=precision)
     return _gather(batch, J, ok, its, offsets, len(vs), inv)
+
+
+def tune(batch: Batch, voltages, tol: float = 1e-10, max_iter: int = 60,
+         bernoulli_name: str = "exact") -> dict:
+    """Time every launch form of the solve on this batch at `voltages` (`dd_tune`) and keep the
+    fastest for later solves of batches of its shape in this process: `{"form", "block",
+    "queue", "times_ms"}`. `voltages` one list for every device, or one list per device (as
+    `solve_uneven` takes them)."""
+    devs = batch["devices"]
+    if len(voltages) == len(devs) and np.ndim(voltages[0]) == 1:
+        lists = [np.sort(np.asarray(v, dtype=float).reshape(-1)) for v in voltages]
+    else:
+        lists = [np.sort(np.asarray(voltages, dtype=float).reshape(-1))] * len(devs)
+    firsts = np.array([d.V_pre if d.pre_cond else v[0] for d, v in zip(devs, lists)])
+    run(batch, lists, firsts, tol=tol, max_iter=max_iter, start_iter=max_iter, strict=False,
+        bernoulli_name=bernoulli_name, mode=_lib.DD_MODE_BATCH, tune=True)
+    return batch.pop("_tuned")
 
 
 def solve_uneven(batch: Batch, voltages: list, tol: float = 1e-10, max_iter: int = 60,

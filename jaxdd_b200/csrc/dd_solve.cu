@@ -34,6 +34,8 @@
 #include <stdint.h>
 
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "dd_launch.h"
 #include "dd_layout.h"
@@ -79,6 +81,64 @@ __device__ __forceinline__ void prefetch_cd(const Lane& L, int k) {
   if (k < 1 || k > L.NP) return;
   for (int f = 0; f < L.ncd; ++f) prefetch_line(L.cd(k, f));
 }
+
+// Node k's iterate (the state the forward sweep starts from, the back substitution updates).
+__device__ __forceinline__ void prefetch_state(const Lane& L, int k) {
+  if (k < 0 || k > L.NP + 1) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) prefetch_line(L.y(0, k, c));
+}
+
+// ------------------------------------------------------------------------------------ staging
+//
+// The sweeps read each node's static record (DD_NF words) from a ring of three records in shared
+// memory instead of from global memory field by field where each is used. A record is copied in
+// by cp.async (8 bytes a thread, every thread its own lane's words: a warp's copy of one field is
+// 16 consecutive words of each of two nodes) two positions before the sweep reaches it and waited
+// for one position before, so the copy's latency passes behind a whole position's arithmetic.
+// Ring slot = position mod 3; the block's ring is [slot][field][thread], each thread owning one
+// column, so a warp's read of one field is 32 consecutive words.
+constexpr int RING = 3;
+
+// A lane whose static record reads come from the ring: the positions the sweep is at (p and
+// p + 1) must be staged and waited for.
+template <int BS>
+struct Staged : Lane {
+  double* ring;  // this thread's column of the block's ring (BS threads a block)
+  __device__ __forceinline__ int pos(int k) const { return half == 0 ? k : NP + 1 - k; }
+  __device__ __forceinline__ double st(int k, int f) const {
+    return ring[((pos(k) % RING) * DD_NF + f) * BS];
+  }
+  __device__ __forceinline__ double afix(int k) const {
+    return frozen ? FX[((size_t)k * 2) * Bp + l] : share * st(k, S_AFIX);
+  }
+  __device__ __forceinline__ double cfix(int k) const {
+    return frozen ? FX[((size_t)k * 2 + 1) * Bp + l] : share * st(k, S_CFIX);
+  }
+};
+
+// Copy position p's record (node p of half 0, NP + 1 - p of half 1) into its ring slot as one
+// commit group; an empty group when p is outside 0 .. last, so that every position commits one.
+template <int BS>
+__device__ __forceinline__ void stage(const Staged<BS>& R, int p, int last) {
+  if (p >= 0 && p <= last) {
+    const int k = R.half == 0 ? p : R.NP + 1 - p;
+    const double* src = R.S + (size_t)k * DD_NF * R.Bp + R.l;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(R.ring + (p % RING) * DD_NF * BS);
+#pragma unroll
+    for (int f = 0; f < DD_NF; ++f)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst + f * BS * 8),
+                   "l"(src + (size_t)f * R.Bp)
+                   : "memory");
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// Every staged position but the newest is in the ring.
+__device__ __forceinline__ void staged_all_but_newest() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+// Every staged position is in the ring (no copy into it is left in flight).
+__device__ __forceinline__ void staged_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // ------------------------------------------------------------------------------------ pair
 
@@ -331,9 +391,9 @@ struct StepOut {
 // is node p (half 0) or node NP + 1 - p (half 1), p = 0 its contact, p = nown its boundary
 // point (mid, or mid + 1) and p = nown + 1 the other half's. Half 0 assembles the meeting row
 // mid at p = nown instead of eliminating it.
-template <int K>
+template <int K, int BS>
 __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, double ratio,
-                               bool noise) {
+                               bool noise, double* ring) {
   const int NP = L.NP, m = L.mid;
   const bool top = L.half == 0;
   const bool mir = !top;
@@ -350,13 +410,23 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
     load_state(L, NODE(nown), adv, ratio, t);
     xb[0] = xchg(L, t.V); xb[1] = xchg(L, t.lnn); xb[2] = xchg(L, t.lnp);
   }
+  // the sweeps' static records from the ring: positions 0 (the contact) .. nown + 1 (the other
+  // half's boundary point); 0 and 1 waited for, 2 on its way
+  Staged<BS> R;
+  static_cast<Lane&>(R) = L;
+  R.ring = ring;
+  const int last = nown + 1;
+  stage(R, 0, last);
+  stage(R, 1, last);
+  stage(R, 2, last);
+  staged_all_but_newest();
   auto own_boundary = [&](Pt& P) {
     P.V = *L.y(0, NODE(nown), 0); P.lnn = *L.y(0, NODE(nown), 1); P.lnp = *L.y(0, NODE(nown), 2);
-    pt_fill_k<K>(L, P, NODE(nown), logs);
+    pt_fill_k<K>(R, P, NODE(nown), logs);
   };
   auto other_boundary = [&](Pt& P) {
     P.V = xb[0]; P.lnn = xb[1]; P.lnp = xb[2];
-    pt_fill_k<K>(L, P, NODE(nown + 1), logs);
+    pt_fill_k<K>(R, P, NODE(nown + 1), logs);
   };
 
   Carry<K> cr;
@@ -364,28 +434,30 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
   {
     Pt pm, pc, pn;
     contact(L, top ? 0 : 1, Vint, pm);
-    pt_fill_k<K>(L, pm, NODE(0), logs);
+    pt_fill_k<K>(R, pm, NODE(0), logs);
     if (nown == 1) own_boundary(pc);
-    else { load_state(L, NODE(1), adv, ratio, pc); pt_fill_k<K>(L, pc, NODE(1), logs); }
+    else { load_state(L, NODE(1), adv, ratio, pc); pt_fill_k<K>(R, pc, NODE(1), logs); }
     Flux el;
     int e = EDGE(0);
-    double h_m = L.st(e, S_H);
-    flux(L, pm, pc, L.st(e, S_MUN), L.st(e, S_MUP), el);
+    double h_m = R.st(e, S_H);
+    flux(L, pm, pc, R.st(e, S_MUN), R.st(e, S_MUP), el);
     ion_edge<K>(L, pm, pc, h_m * L.L, cr.num);
-    int ifk_m = (int)L.st(e, S_IFK);
+    int ifk_m = (int)R.st(e, S_IFK);
     for (int p = 1; p <= nown; ++p) {
-      if (p + DD_PREFETCH_AHEAD <= nown + 1) prefetch_node(L, NODE(p + DD_PREFETCH_AHEAD));
+      stage(R, p + 2, last);
+      if (p + 2 <= last) prefetch_state(L, NODE(p + 2));
+      staged_all_but_newest();  // positions p and p + 1
       if (p + 1 == nown) own_boundary(pn);
       else if (p == nown) other_boundary(pn);
-      else { load_state(L, NODE(p + 1), adv, ratio, pn); pt_fill_k<K>(L, pn, NODE(p + 1), logs); }
+      else { load_state(L, NODE(p + 1), adv, ratio, pn); pt_fill_k<K>(R, pn, NODE(p + 1), logs); }
       e = EDGE(p);
-      const double h_i = L.st(e, S_H);
-      const int ifk_i = (int)L.st(e, S_IFK);
+      const double h_i = R.st(e, S_H);
+      const int ifk_i = (int)R.st(e, S_IFK);
       Flux er;
-      flux(L, pc, pn, L.st(e, S_MUN), L.st(e, S_MUP), er);
+      flux(L, pc, pn, R.st(e, S_MUN), R.st(e, S_MUP), er);
       if (p < nown || top) ion_edge<K>(L, pc, pn, h_i * L.L, cr.num);  // interval mid is half 0's
       double A[3][3], Bm[3][3], Cm[3][3], rhs[3], U0[K], W[K];
-      assemble_row<K>(L, NODE(p), pm, pc, pn, el, er, h_m, h_i, ifk_m, ifk_i, noise, mir, A, Bm,
+      assemble_row<K>(R, NODE(p), pm, pc, pn, el, er, h_m, h_i, ifk_m, ifk_i, noise, mir, A, Bm,
                       Cm, rhs, U0, W);
       if (p < nown || !top) {
         cr.eliminate(A, Bm, Cm, rhs, U0, W);
@@ -544,12 +616,16 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
     const double Ug = L.st(m + 1, S_G) * gfrac;
     U_qq[0] = R - Ug; U_qq[1] = R - Ug;  // intervals mid, mid+1 hold no traps (the split's choice)
   }
+  // positions nown and nown + 1 are in the ring from the forward sweep; each position stages
+  // the one after it
   for (int p = nown; p >= 0; --p) {
     const int i = NODE(p);
+    stage(R, p - 1, last);
     if (p > DD_PREFETCH_AHEAD) {
       prefetch_cd(L, NODE(p - DD_PREFETCH_AHEAD));
-      prefetch_node(L, NODE(p - DD_PREFETCH_AHEAD));
+      prefetch_state(L, NODE(p - DD_PREFETCH_AHEAD));
     }
+    staged_all_but_newest();  // positions p and p + 1
     Pt pi;
     if (p >= 1) {
       double x[3];
@@ -583,12 +659,12 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
       contact(L, top ? 0 : 1, Vint, pi);
       pi.n = exp(pi.lnn); pi.p = exp(pi.lnp);
     }
-    pi.offn = L.st(i, S_OFFN); pi.offp = L.st(i, S_OFFP);
+    pi.offn = R.st(i, S_OFFN); pi.offp = R.st(i, S_OFFP);
     // the interval between this point and the one further in (not half 1's at its boundary)
     const bool own_in = top || p < nown;
     const int ein = EDGE(p);
-    const double h_in = L.st(ein, S_H), dx_in = L.st(ein, S_DX);
-    const int ifk_in = (int)L.st(ein, S_IFK);
+    const double h_in = R.st(ein, S_H), dx_in = R.st(ein, S_DX);
+    const int ifk_in = (int)R.st(ein, S_IFK);
     double Ri_i[2] = {0.0, 0.0};
     if (own_in && ifk_in >= 0) {
       Iface t;
@@ -603,18 +679,18 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
     if (L.currdiff && own_in) {
       const Pt& a = top ? pi : pq;
       const Pt& b = top ? pq : pi;
-      Jd[0] = sg_flux(L, 0, a, b, L.st(ein, S_MUN), h_in);
-      Jd[1] = sg_flux(L, 1, a, b, L.st(ein, S_MUP), h_in);
+      Jd[0] = sg_flux(L, 0, a, b, R.st(ein, S_MUN), h_in);
+      Jd[1] = sg_flux(L, 1, a, b, R.st(ein, S_MUP), h_in);
       if (ifk_in < -1) cp.dtot += h_in * (Jd[0] + Jd[1]);
     }
     // the point further in is final now: its U, the trapezoid of its inner interval, its sums
     if (p < nown) {
       const int k = NODE(p + 1);
-      const double Ug = L.st(k, S_G) * gfrac;
+      const double Ug = R.st(k, S_G) * gfrac;
       const double ck = 0.5 * (dx_in + dx_q);
       const bool inner_own = top || p + 1 < nown;  // half 1's boundary point: its inner interval is mid
       if (inner_own) H_run += h_q;
-      const double hk = L.st(k, S_H);  // b_k takes the width of interval k
+      const double hk = R.st(k, S_H);  // b_k takes the width of interval k
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         const double sn = s == 0 ? -1.0 : 1.0;
@@ -642,18 +718,19 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
       Jd1[0] = Jd[0]; Jd1[1] = Jd[1];
     }
     if (p >= 1) {
-      double R, d1, d2;
-      recomb(L, i, pi.n, pi.p, R, d1, d2);
-      R_q = R;
+      double Rr, d1, d2;
+      recomb(R, i, pi.n, pi.p, Rr, d1, d2);
+      R_q = Rr;
     } else {
       R_q = 0.0;
     }
-    qv_q[0] = exp(-(pi.V + pi.offn) * L.iVt) / L.st(i, S_MUN);
-    qv_q[1] = exp((pi.V + pi.offp) * L.iVt) / L.st(i, S_MUP);
+    qv_q[0] = exp(-(pi.V + pi.offn) * L.iVt) / R.st(i, S_MUN);
+    qv_q[1] = exp((pi.V + pi.offp) * L.iVt) / R.st(i, S_MUP);
     Ri_q[0] = Ri_i[0]; Ri_q[1] = Ri_i[1];
     h_q = h_in; dx_q = dx_in; ifk_q = ifk_in;
     pq = pi;
   }
+  staged_all();  // no copy into the ring left in flight (the noise step leaves the loop early)
   if (!noise) {
     // the contact: its inner interval (half 0: interval 0; half 1: interval NP, dx = 0); the
     // left contact counts in the current's sums, the right one does not (q_k for k <= NP)
@@ -1058,6 +1135,9 @@ struct Args {
   double* prebias;       // [np+2][3][Bp]
   double* prebias_logs;  // [DD_MAXK][Bp]
   int nv_max;
+  // the work queue (null: one device per pair): its counter and the pairs of the grid
+  int* queue;
+  int pairs;
   // dd_newton_step
   double* logs_io;
   const double* vint;
@@ -1106,11 +1186,9 @@ enum Ctx {
 
 // The whole J-V program of one device, run by both threads of its pair: every decision is
 // taken on values both hold bit for bit (half 0's, broadcast), so the two never part ways.
-template <int K>
-__global__ void __launch_bounds__(64) solve_kernel(Args a) {
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int l = tid >> 1, half = tid & 1;
-  if (l >= a.B) return;
+template <int K, int BS>
+__device__ __forceinline__ void run_lane(const Args& a, int l, int half, Prog<K>& g,
+                                         double* ring) {
   Lane L;
   lane_init<K>(L, a, l, half);
   const bool top = half == 0;
@@ -1131,10 +1209,6 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
 #pragma unroll
   for (int q = 0; q < K; ++q) mobile = mobile || L.tot[q] > 0.0;
 
-  // the program's bookkeeping between steps lives in shared memory (one record per thread),
-  // so that the sweeps have the registers to themselves
-  __shared__ Prog<K> progs[DD_SOLVE_BLOCK];
-  Prog<K>& g = progs[threadIdx.x];
   double logs[K];
 #pragma unroll
   for (int q = 0; q < K; ++q) { logs[q] = 0.0; g.lgA[q] = 0.0; g.lgB[q] = 0.0; g.lgC[q] = 0.0; }
@@ -1250,8 +1324,8 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
     double Jv = 0.0;
     // one call site of the step (the round-off step with `noise`): the step's code once
     const bool noise = g.pending_noise;
-    const StepOut o = newton_step<K>(L, Vint, logs, noise ? (int)ADV_NONE : adv,
-                                     noise ? 0.0 : ratio, noise);
+    const StepOut o = newton_step<K, BS>(L, Vint, logs, noise ? (int)ADV_NONE : adv,
+                                     noise ? 0.0 : ratio, noise, ring);
     if (noise) {
       ++g.n_plain;
       g.noise_floor = o.size; g.floor_known = true; g.pending_noise = false;
@@ -1419,6 +1493,31 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
   }
 }
 
+// The solve: each pair of threads runs one device's whole program (run_lane). With a work queue
+// (`a.queue`, a batch of more devices than the GPU holds at once) the grid is what the GPU holds
+// and a pair that finishes a device takes the next one from the queue, so no pair waits for the
+// slowest device of its warp; devices are taken in lane order (the packer puts the largest
+// grids first). The program's bookkeeping between steps lives in shared memory (one record per
+// thread), so that the sweeps have the registers to themselves, beside the sweeps' ring. BS
+// threads a block; the ring (RING * DD_NF * BS words) is the launch's dynamic shared memory.
+template <int K, int BS>
+__global__ void __launch_bounds__(64) solve_kernel(Args a) {
+  __shared__ Prog<K> progs[BS];
+  extern __shared__ double ring[];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int half = tid & 1;
+  const int base = (threadIdx.x & 31) & ~1;
+  const unsigned pair = 3u << base;
+  int l = tid >> 1;
+  while (l < a.B) {
+    run_lane<K, BS>(a, l, half, progs[threadIdx.x], ring + threadIdx.x);
+    if (!a.queue) break;
+    int next = 0;
+    if (half == 0) next = a.pairs + atomicAdd(a.queue, 1);
+    l = __shfl_sync(pair, next, base);
+  }
+}
+
 // One Newton step per lane from a given state (dd_newton_step).
 template <int K>
 __global__ void __launch_bounds__(64) step_kernel(Args a) {
@@ -1431,7 +1530,9 @@ __global__ void __launch_bounds__(64) step_kernel(Args a) {
   double logs[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) logs[k] = a.logs_io[(size_t)k * a.Bp + l];
-  const StepOut o = newton_step<K>(L, a.vint[l], logs, ADV_NONE, 0.0, false);
+  __shared__ double ring[RING * DD_NF * DD_SOLVE_BLOCK];
+  const StepOut o = newton_step<K, DD_SOLVE_BLOCK>(L, a.vint[l], logs, ADV_NONE, 0.0, false,
+                                                   ring + threadIdx.x);
   if (half == 0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) a.logs_io[(size_t)k * a.Bp + l] = logs[k];
@@ -1449,6 +1550,9 @@ namespace {
 int slots_k(const dd_batch* b) { return b->k_anion + b->k_cation <= 2 ? 2 : 4; }
 
 
+// The work queue's counter: its own 256 bytes at the workspace's end.
+constexpr size_t QUEUE_ELEMS = 32;
+
 size_t ws_elems(const dd_batch* b, size_t* y_e, size_t* fx_e, size_t* cd_e, int* ncd) {
   const int K = slots_k(b);
   *ncd = 12 + 3 * K;
@@ -1456,7 +1560,112 @@ size_t ws_elems(const dd_batch* b, size_t* y_e, size_t* fx_e, size_t* cd_e, int*
   *y_e = (size_t)dd::DD_NBUF * nodes * 3 * b->lane_stride;
   *fx_e = nodes * 2 * b->lane_stride;
   *cd_e = nodes * (size_t)(*ncd) * b->lane_stride;
-  return *y_e + *fx_e + *cd_e;
+  return *y_e + *fx_e + *cd_e + QUEUE_ELEMS;
+}
+
+// ------------------------------------------------------------------ launch forms and tuning
+//
+// A launch form of the solve: threads per block (two per device) and whether a batch of more
+// devices than the GPU holds at once runs from the work queue (as many pairs as the GPU holds,
+// each taking the next device when done) or as one pair per device (the hardware starting
+// blocks as others finish). Every form gives the same results. `dd_tune` times them on a batch
+// and keeps the fastest for batches of its shape; untuned shapes take form 0.
+struct Form {
+  int block;
+  bool queue;
+};
+constexpr Form FORMS[DD_SOLVE_FORMS] = {{32, true}, {64, true}, {32, false}, {64, false}};
+
+template <int K>
+const void* solve_kernel_ptr(int block) {
+  return block == 64 ? (const void*)dd::solve_kernel<K, 64> : (const void*)dd::solve_kernel<K, 32>;
+}
+
+// The dynamic shared memory of a block (the sweeps' ring), allowed above the default 48 KB a
+// block for the 64-thread form.
+size_t ring_bytes(int block) { return sizeof(double) * dd::RING * dd::DD_NF * block; }
+
+bool allow_ring(const void* kernel, int block) {
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)ring_bytes(block)) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
+
+// The pairs the GPU holds at once for this kernel and block size (its occupancy), 0 if unknown.
+long pairs_held(const void* kernel, int block) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, ring_bytes(block)) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return (long)sms * per_sm * (block / 2);
+}
+
+// Launch the solve in form `f`: the work queue's counter (the workspace's last 256 bytes) is
+// zeroed on the stream first when the queue is used.
+int launch_solve(const dd_batch* b, dd::Args& a, void* ws, cudaStream_t s, const Form& f) {
+  const int K = slots_k(b);
+  const void* kernel = K == 2 ? solve_kernel_ptr<2>(f.block) : solve_kernel_ptr<4>(f.block);
+  if (!allow_ring(kernel, f.block)) return DD_ERR_LAUNCH;
+  const long held = f.queue ? pairs_held(kernel, f.block) : 0;
+  a.queue = nullptr;
+  a.pairs = 0;
+  dim3 grid((2 * b->lane_stride + f.block - 1) / f.block);
+  if (held > 0 && b->n_lanes > held) {
+    size_t ye, fe, ce;
+    int ncd;
+    const size_t at = ws_elems(b, &ye, &fe, &ce, &ncd) - QUEUE_ELEMS;
+    a.queue = reinterpret_cast<int*>(static_cast<double*>(ws) + at);
+    a.pairs = (int)held;
+    if (cudaMemsetAsync(a.queue, 0, sizeof(int), s) != cudaSuccess) return DD_ERR_LAUNCH;
+    grid = dim3((unsigned)(2 * held / f.block));
+  }
+  const dim3 block(f.block);
+  const size_t smem = ring_bytes(f.block);
+  if (K == 2)
+    return f.block == 64 ? dd::launch(dd::solve_kernel<2, 64>, grid, block, smem, s, a)
+                         : dd::launch(dd::solve_kernel<2, 32>, grid, block, smem, s, a);
+  return f.block == 64 ? dd::launch(dd::solve_kernel<4, 64>, grid, block, smem, s, a)
+                       : dd::launch(dd::solve_kernel<4, 32>, grid, block, smem, s, a);
+}
+
+// The tuned forms of this process: by device, ion slots, grid size and lane count (within a
+// factor of two).
+struct TuneKey {
+  int dev, K, np_max, lanes_log2;
+  bool operator==(const TuneKey& o) const {
+    return dev == o.dev && K == o.K && np_max == o.np_max && lanes_log2 == o.lanes_log2;
+  }
+};
+std::mutex tune_mutex;
+std::vector<std::pair<TuneKey, int>> tuned;
+
+bool tune_key(const dd_batch* b, TuneKey& k) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  int lg = 0;
+  while ((1L << lg) < b->n_lanes) ++lg;
+  k = TuneKey{dev, slots_k(b), b->np_max, lg};
+  return true;
+}
+
+const Form& form_for(const dd_batch* b) {
+  TuneKey k;
+  if (tune_key(b, k)) {
+    std::lock_guard<std::mutex> guard(tune_mutex);
+    for (const auto& e : tuned)
+      if (e.first == k) return FORMS[e.second];
+  }
+  return FORMS[0];
 }
 
 int check_batch(const dd_batch* b) {
@@ -1527,11 +1736,7 @@ int dd_solve(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opt
   a.J = J; a.ok = converged; a.its = iterations; a.status = lane_status; a.steps = lane_steps;
   a.tol = opts->tol; a.max_iter = opts->max_iter; a.start_iter = opts->start_iter;
   a.strict = opts->strict; a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS; a.mode = opts->mode;
-  const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
-      block(DD_SOLVE_BLOCK);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  return slots_k(batch) == 2 ? dd::launch(dd::solve_kernel<2>, grid, block, 0, s, a)
-                             : dd::launch(dd::solve_kernel<4>, grid, block, 0, s, a);
+  return launch_solve(batch, a, workspace, static_cast<cudaStream_t>(stream), form_for(batch));
 }
 
 int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts,
@@ -1560,11 +1765,63 @@ int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_op
   a.strict = opts->strict; a.simss = opts->bernoulli == DD_BERNOULLI_SIMSS; a.mode = opts->mode;
   a.states = states; a.state_logs = state_logs; a.prebias = prebias;
   a.prebias_logs = prebias_logs; a.nv_max = nv_max;
-  const dim3 grid((2 * batch->lane_stride + DD_SOLVE_BLOCK - 1) / DD_SOLVE_BLOCK),
-      block(DD_SOLVE_BLOCK);
+  return launch_solve(batch, a, workspace, static_cast<cudaStream_t>(stream), form_for(batch));
+}
+
+int dd_tune(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts, double* J,
+            uint8_t* converged, int32_t* iterations, int32_t* lane_status, int32_t* lane_steps,
+            void* workspace, size_t workspace_bytes, void* stream, int32_t* form,
+            float* times_ms) {
+  if (!form) return DD_ERR_ARGS;
+  int st = check_batch(batch);
+  if (st != DD_OK) return st;
+  TuneKey key;
+  if (!tune_key(batch, key)) return DD_ERR_DEVICE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  return slots_k(batch) == 2 ? dd::launch(dd::solve_kernel<2>, grid, block, 0, s, a)
-                             : dd::launch(dd::solve_kernel<4>, grid, block, 0, s, a);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) {
+    cudaGetLastError();
+    return DD_ERR_LAUNCH;
+  }
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    cudaEventDestroy(e0);
+    return DD_ERR_LAUNCH;
+  }
+  int best = -1;
+  float best_ms = 0.0f;
+  for (int f = 0; f < DD_SOLVE_FORMS && st == DD_OK; ++f) {
+    {  // the form being timed is the shape's form for this one solve
+      std::lock_guard<std::mutex> guard(tune_mutex);
+      bool found = false;
+      for (auto& e : tuned)
+        if (e.first == key) { e.second = f; found = true; }
+      if (!found) tuned.push_back({key, f});
+    }
+    float ms = 0.0f;
+    if (cudaEventRecord(e0, s) != cudaSuccess) st = DD_ERR_LAUNCH;
+    if (st == DD_OK)
+      st = dd_solve(batch, volts, opts, J, converged, iterations, lane_status, lane_steps,
+                    workspace, workspace_bytes, stream);
+    if (st == DD_OK && (cudaEventRecord(e1, s) != cudaSuccess ||
+                        cudaEventSynchronize(e1) != cudaSuccess ||
+                        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+      st = DD_ERR_LAUNCH;
+    if (st == DD_OK) {
+      if (times_ms) times_ms[f] = ms;
+      if (best < 0 || ms < best_ms) { best = f; best_ms = ms; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  {
+    std::lock_guard<std::mutex> guard(tune_mutex);
+    for (auto& e : tuned)
+      if (e.first == key) e.second = best < 0 ? 0 : best;
+  }
+  if (st != DD_OK) return st;
+  *form = best;
+  return DD_OK;
 }
 
 int dd_newton_step(const dd_batch* batch, double* y, double* logs, const double* vint,

@@ -42,7 +42,8 @@ def test_workspace_query_and_argument_checks():
     size = ctypes.c_size_t(0)
     assert _lib.lib().dd_workspace_bytes(ctypes.byref(desc), ctypes.byref(size)) == 0
     nodes = b["np_max"] + 2
-    assert size.value == 8 * nodes * b["Bp"] * (4 * 3 + 2 + 12 + 3 * 2)
+    # four state buffers, the frozen ions, the sweep's c'/d' (two slots), the queue's counter
+    assert size.value == 8 * nodes * b["Bp"] * (4 * 3 + 2 + 12 + 3 * 2) + 256
     bad = _lib.DdBatch(b["n"], 31, b["np_max"], 1, 1, 1, 1, 1, 1)
     assert _lib.lib().dd_workspace_bytes(ctypes.byref(bad), ctypes.byref(size)) == 1
 
