@@ -766,6 +766,8 @@ def main() -> None:
     ap.add_argument("--cpu-sample", type=int, default=256,
                     help="devices the compiled CPU restatement solves on one core for "
                          "cpu_baseline")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="skip the autotuner (the solve's default launch form)")
     ap.add_argument("--parity-lanes", type=int, default=1024,
                     help="devices of the timed launch checked against the oracle after the "
                          "timed region (0: none)")
@@ -860,6 +862,18 @@ def main() -> None:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    # the autotuner (outside the timed region): every launch form timed once on this batch, the
+    # fastest kept for the solves below
+    launch_form = None
+    if args.tune:
+        form = ctypes.c_int32(-1)
+        times = (ctypes.c_float * _lib.DD_SOLVE_FORMS)()
+        _lib.check(so.dd_tune(ctypes.byref(desc), ctypes.byref(volts), ctypes.byref(opts),
+                              J.data_ptr(), ok.data_ptr(), its.data_ptr(), status.data_ptr(),
+                              steps.data_ptr(), ws.data_ptr(), ws.numel(), stream.cuda_stream,
+                              ctypes.byref(form), times), "dd_tune")
+        launch_form = dict(_lib.SOLVE_FORMS[form.value], form=form.value,
+                           tune_ms=[round(float(t), 1) for t in times])
     for _ in range(args.warmup):
         launch()
     barrier()
@@ -940,7 +954,8 @@ def main() -> None:
                        "precision": args.precision, "devices_per_gpu": args.devices,
                        "l2": f"inputs larger than L2 ({batch['stat'].nbytes / 1e9:.2f} GB of "
                              "statics per launch)",
-                       "converged_fraction": ok_frac, "build_s": round(build_s, 1)},
+                       "converged_fraction": ok_frac, "build_s": round(build_s, 1),
+                       "launch": launch_form},
             "parity": parity,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
