@@ -20,7 +20,7 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 
-def _solve(st, P, D, V, form_lanes):
+def _solve(st, P, D, V):
     """dd_solve of the devices of parameter columns P, D (built on the GPU) at voltages V."""
     stat, scal, iface, y0, Bp = build(st, P, D)
     n = P.shape[-1]
@@ -67,8 +67,8 @@ def test_the_work_queue_gives_every_device_its_own_curve():
     P, D = parameters(st, setups, first=np.full(len(setups), V[0]))
     n = 24576
     pick = np.arange(n) % len(setups)
-    Jq, okq, itq, stq = _solve(st, P[:, :, pick], D[:, pick], V, n)
-    J1, ok1, it1, st1 = _solve(st, P, D, V, len(setups))
+    Jq, okq, itq, stq = _solve(st, P[:, :, pick], D[:, pick], V)
+    J1, ok1, it1, st1 = _solve(st, P, D, V)
     assert ok1.mean() > 0.9
     assert np.array_equal(Jq, J1[pick], equal_nan=True)
     assert np.array_equal(okq, ok1[pick]) and np.array_equal(itq, it1[pick])
