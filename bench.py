@@ -52,7 +52,7 @@ DEVICES_PER_GPU = 16384
 NP = 400
 CHUNK = 512  # devices per build task (a multiple of 32)
 #: which kernel build profiles/traffic.json must describe for its traffic to be reported
-KERNEL_TAG = "twisted two-thread fused Newton, 26-word static record"
+KERNEL_TAG = "twisted two-thread fused Newton, shared-memory staged record"
 
 
 def traffic_entry(precision: str, workload: str, devices: int, npts: int) -> dict | None:

@@ -11,6 +11,18 @@
 
 #include "dd_layout.h"
 
+// The transcendental functions of the hot loops, as the including file wants them: inline by
+// default; a file may define these first to route every call site through one shared copy.
+#ifndef DD_EXP
+#define DD_EXP(x) exp(x)
+#endif
+#ifndef DD_EXPM1
+#define DD_EXPM1(x) expm1(x)
+#endif
+#ifndef DD_LOG1P
+#define DD_LOG1P(x) log1p(x)
+#endif
+
 namespace dd {
 
 constexpr double Q = 1.6022e-19;
@@ -57,7 +69,7 @@ __device__ __forceinline__ void bern_abs(double a, int simss, double& b, double&
     db = -0.5 + a / 6.0 - a * a * a / 180.0;
     return;
   }
-  const double e = expm1(a);
+  const double e = DD_EXPM1(a);
   b = a / e;
   db = (1.0 - b) / e - b;  // 1/e - a(e+1)/e^2, finite where e overflows
 }
@@ -190,13 +202,13 @@ __device__ __forceinline__ void pt_fill(const Lane& L, Pt& P, int k, const doubl
 // pt_fill with the K normalisations in registers (read by selects, `pick`).
 template <int K, class LT>
 __device__ __forceinline__ void pt_fill_k(const LT& L, Pt& P, int k, const double* logs) {
-  P.n = exp(P.lnn);
-  P.p = exp(P.lnp);
+  P.n = DD_EXP(P.lnn);
+  P.p = DD_EXP(P.lnp);
   P.offn = L.st(k, S_OFFN);
   P.offp = L.st(k, S_OFFP);
   P.sl = slots_at(L, k);
-  P.da = P.sl.a >= 0 ? exp(pick<K>(logs, P.sl.a) + P.V * L.iVt) : 0.0;
-  P.dc = P.sl.c >= 0 ? exp(pick<K>(logs, L.ka + P.sl.c) - P.V * L.iVt) : 0.0;
+  P.da = P.sl.a >= 0 ? DD_EXP(pick<K>(logs, P.sl.a) + P.V * L.iVt) : 0.0;
+  P.dc = P.sl.c >= 0 ? DD_EXP(pick<K>(logs, L.ka + P.sl.c) - P.V * L.iVt) : 0.0;
 }
 
 // The contacts' states (`_bounds`, batch.py:255-259).

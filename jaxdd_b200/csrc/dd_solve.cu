@@ -37,6 +37,21 @@
 #include <utility>
 #include <vector>
 
+// With DD_OUTLINE_MATH 1 the sweeps' expm1 (the Bernoulli function), with 2 also their exp and
+// log1p, have one out-of-line copy that every call site shares instead of a copy inlined at each
+// site: the step's code is large enough that instruction fetch, not arithmetic, limits how often
+// a warp issues.
+#if defined(DD_OUTLINE_MATH) && DD_OUTLINE_MATH >= 1
+__device__ __noinline__ double dd_expm1_shared(double x) { return expm1(x); }
+#define DD_EXPM1(x) dd_expm1_shared(x)
+#endif
+#if defined(DD_OUTLINE_MATH) && DD_OUTLINE_MATH >= 2
+__device__ __noinline__ double dd_exp_shared(double x) { return exp(x); }
+__device__ __noinline__ double dd_log1p_shared(double x) { return log1p(x); }
+#define DD_EXP(x) dd_exp_shared(x)
+#define DD_LOG1P(x) dd_log1p_shared(x)
+#endif
+
 #include "dd_launch.h"
 #include "dd_layout.h"
 #include "dd_physics.cuh"
@@ -311,12 +326,12 @@ __device__ __forceinline__ void damp(const Lane& L, const double (&x)[3], const 
     const double d = x[1 + s];
     const bool below = yy < L.lognf;
     const bool pos = d > -1.0;
-    double in_n = pos ? log1p(below ? d : 0.0) : -CAP_LN;
+    double in_n = pos ? DD_LOG1P(below ? d : 0.0) : -CAP_LN;
     in_n = clipd(in_n, -FLOOR_DROP_CAP, CAP_LN);
     sd[s] = below ? in_n : clipd(d, -CAP_LN, CAP_LN);
   }
   nw.V = old.V + sV; nw.lnn = old.lnn + sd[0]; nw.lnp = old.lnp + sd[1];
-  nw.n = exp(nw.lnn); nw.p = exp(nw.lnp);
+  nw.n = DD_EXP(nw.lnn); nw.p = DD_EXP(nw.lnp);
   size = nanmax(size, fabs(sV) * L.iVt);
   size = nanmax(size, fabs(sd[0]) * (nw.n / (nw.n + L.nfloor)));
   size = nanmax(size, fabs(sd[1]) * (nw.p / (nw.p + L.nfloor)));
@@ -724,8 +739,8 @@ __device__ StepOut newton_step(Lane& L, double Vint, double* logs, int adv, doub
     } else {
       R_q = 0.0;
     }
-    qv_q[0] = exp(-(pi.V + pi.offn) * L.iVt) / R.st(i, S_MUN);
-    qv_q[1] = exp((pi.V + pi.offp) * L.iVt) / R.st(i, S_MUP);
+    qv_q[0] = DD_EXP(-(pi.V + pi.offn) * L.iVt) / R.st(i, S_MUN);
+    qv_q[1] = DD_EXP((pi.V + pi.offp) * L.iVt) / R.st(i, S_MUP);
     Ri_q[0] = Ri_i[0]; Ri_q[1] = Ri_i[1];
     h_q = h_in; dx_q = dx_in; ifk_q = ifk_in;
     pq = pi;
