@@ -1201,13 +1201,16 @@ enum Ctx {
 
 // The whole J-V program of one device, run by both threads of its pair: every decision is
 // taken on values both hold bit for bit (half 0's, broadcast), so the two never part ways.
-template <int K, int BS>
+template <int K, int BS, bool GENERIC>
 __device__ __forceinline__ void run_lane(const Args& a, int l, int half, Prog<K>& g,
                                          double* ring) {
   Lane L;
   lane_init<K>(L, a, l, half);
+  // The common launch (batch mode, the exact Bernoulli function) is compiled without the others'
+  // paths, which would otherwise sit in the sweeps' code and cost instruction fetch.
+  if (!GENERIC) L.simss = 0;
   const bool top = half == 0;
-  const bool jv = a.mode == DD_MODE_JV;
+  const bool jv = GENERIC && a.mode == DD_MODE_JV;
   const int voff = a.voff[l], nv = a.vcnt[l];
   if (nv <= 0) return;
   const double* Vl = a.V + voff;
@@ -1338,7 +1341,7 @@ __device__ __forceinline__ void run_lane(const Args& a, int l, int half, Prog<K>
     bool end = false, conv = false, fin = true;
     double Jv = 0.0;
     // one call site of the step (the round-off step with `noise`): the step's code once
-    const bool noise = g.pending_noise;
+    const bool noise = GENERIC && g.pending_noise;
     const StepOut o = newton_step<K, BS>(L, Vint, logs, noise ? (int)ADV_NONE : adv,
                                      noise ? 0.0 : ratio, noise, ring);
     if (noise) {
@@ -1515,7 +1518,8 @@ __device__ __forceinline__ void run_lane(const Args& a, int l, int half, Prog<K>
 // grids first). The program's bookkeeping between steps lives in shared memory (one record per
 // thread), so that the sweeps have the registers to themselves, beside the sweeps' ring. BS
 // threads a block; the ring (RING * DD_NF * BS words) is the launch's dynamic shared memory.
-template <int K, int BS>
+// GENERIC: any mode and Bernoulli function; otherwise batch mode with the exact one only.
+template <int K, int BS, bool GENERIC>
 __global__ void __launch_bounds__(64) solve_kernel(Args a) {
   __shared__ Prog<K> progs[BS];
   extern __shared__ double ring[];
@@ -1525,7 +1529,7 @@ __global__ void __launch_bounds__(64) solve_kernel(Args a) {
   const unsigned pair = 3u << base;
   int l = tid >> 1;
   while (l < a.B) {
-    run_lane<K, BS>(a, l, half, progs[threadIdx.x], ring + threadIdx.x);
+    run_lane<K, BS, GENERIC>(a, l, half, progs[threadIdx.x], ring + threadIdx.x);
     if (!a.queue) break;
     int next = 0;
     if (half == 0) next = a.pairs + atomicAdd(a.queue, 1);
@@ -1592,8 +1596,12 @@ struct Form {
 constexpr Form FORMS[DD_SOLVE_FORMS] = {{32, true}, {64, true}, {32, false}, {64, false}};
 
 template <int K>
-const void* solve_kernel_ptr(int block) {
-  return block == 64 ? (const void*)dd::solve_kernel<K, 64> : (const void*)dd::solve_kernel<K, 32>;
+const void* solve_kernel_ptr(int block, bool generic) {
+  if (generic)
+    return block == 64 ? (const void*)dd::solve_kernel<K, 64, true>
+                       : (const void*)dd::solve_kernel<K, 32, true>;
+  return block == 64 ? (const void*)dd::solve_kernel<K, 64, false>
+                     : (const void*)dd::solve_kernel<K, 32, false>;
 }
 
 // The dynamic shared memory of a block (the sweeps' ring), allowed above the default 48 KB a
@@ -1626,7 +1634,10 @@ long pairs_held(const void* kernel, int block) {
 // zeroed on the stream first when the queue is used.
 int launch_solve(const dd_batch* b, dd::Args& a, void* ws, cudaStream_t s, const Form& f) {
   const int K = slots_k(b);
-  const void* kernel = K == 2 ? solve_kernel_ptr<2>(f.block) : solve_kernel_ptr<4>(f.block);
+  // the specialised kernel for batch mode with the exact Bernoulli function, else the generic one
+  const bool generic = a.mode != DD_MODE_BATCH || a.simss;
+  const void* kernel = K == 2 ? solve_kernel_ptr<2>(f.block, generic)
+                              : solve_kernel_ptr<4>(f.block, generic);
   if (!allow_ring(kernel, f.block)) return DD_ERR_LAUNCH;
   const long held = f.queue ? pairs_held(kernel, f.block) : 0;
   a.queue = nullptr;
@@ -1643,11 +1654,9 @@ int launch_solve(const dd_batch* b, dd::Args& a, void* ws, cudaStream_t s, const
   }
   const dim3 block(f.block);
   const size_t smem = ring_bytes(f.block);
-  if (K == 2)
-    return f.block == 64 ? dd::launch(dd::solve_kernel<2, 64>, grid, block, smem, s, a)
-                         : dd::launch(dd::solve_kernel<2, 32>, grid, block, smem, s, a);
-  return f.block == 64 ? dd::launch(dd::solve_kernel<4, 64>, grid, block, smem, s, a)
-                       : dd::launch(dd::solve_kernel<4, 32>, grid, block, smem, s, a);
+  void* args[] = {&a};
+  return cudaLaunchKernel(kernel, grid, block, args, smem, s) == cudaSuccess ? DD_OK
+                                                                            : DD_ERR_LAUNCH;
 }
 
 // The tuned forms of this process: by device, ion slots, grid size and lane count (within a
