@@ -470,6 +470,12 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
     cplx duc_prev_b[2] = {mk(0.0), mk(0.0)}, duc_prev_t[2] = {mk(0.0), mk(0.0)};
     cplx dJD = mk(0.0);
     double hsum = 0.0, dx_prev = 0.0, h_prev = 0.0;
+    // `currDiffInt = 1`: each interval's Scharfetter-Gummel flux instead of the integral form
+    // (jaxdd batch.py:366-369), its tangent from the points at both ends of the interval
+    const bool cdiff = L.sc(C_CURRDIFF) > 0.0;
+    cplx jd_prev[2] = {mk(0.0), mk(0.0)};
+    Pt Pa, Pb;
+    if (cdiff) point(L, 0, Vint, Pa);
     for (int k = 0; k <= NP; ++k) {
       const double hk = L.st(k, S_H);
       const double dx = k < NP ? L.st(k, S_DX) : 0.0;
@@ -503,6 +509,7 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
         dU[1] = rec(k, P_TRP) * df;
       }
       const bool iface_k = L.st(k, S_IFK) > -1.5;
+      if (cdiff) point(L, k + 1, Vint, Pb);
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const double sn = c == 0 ? -1.0 : 1.0;
@@ -524,8 +531,22 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
           dS_b[c] = dS_b[c] + (sn * Q * L.L * width) * duc_b;
           dS_t[c] = dS_t[c] + (sn * Q * L.L * width) * duc_t;
         }
-        if (iface_k) {
-          const cplx thr = (sn * 0.5 * Q * L.L * hk) * (dRi_k[c] + dRi_k1[c]);
+        const cplx thr = (sn * 0.5 * Q * L.L * hk) * (dRi_k[c] + dRi_k1[c]);
+        if (cdiff) {
+          // d[sn q mu V_T (d1 B(-x) - d0 B(x))]/(L h), x = sn (Vg1 - Vg0)/V_T; across an
+          // interface the interval before it plus the current through its traps
+          const double d0 = c == 0 ? Pa.n : Pa.p, d1 = c == 0 ? Pb.n : Pb.p;
+          const double g0 = Pa.V + (c == 0 ? Pa.offn : Pa.offp);
+          const double g1 = Pb.V + (c == 0 ? Pb.offn : Pb.offp);
+          double bf, bb, dbf, dbb;
+          bern_pair(sn * (g1 - g0) / Vt, L.simss, bf, bb, dbf, dbb);
+          const cplx dxk = (sn / Vt) * (dV(k + 1) - dV(k));
+          const cplx djd = (sn * Q * mu * Vt / (L.L * hk)) *
+                           (d1 * (bb * dyv(k + 1, 1 + c) - dbb * dxk) -
+                            d0 * (bf * dyv(k, 1 + c) + dbf * dxk));
+          sumJ_b[c] = sumJ_b[c] + hk * (iface_k ? jd_prev[c] + thr : djd);
+          jd_prev[c] = djd;
+        } else if (iface_k) {
           sumJ_b[c] = sumJ_b[c] + hk * (dS_prev_b + thr);
           sumJ_t[c] = sumJ_t[c] + hk * dS_prev_t;
         } else {
@@ -540,6 +561,7 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
       dJD = dJD + (hk * sign * epsk / (L.L * hk)) * (dV(k + 1) - dV(k));
       dx_prev = dx;
       h_prev = hk;
+      if (cdiff) Pa = Pb;
     }
     // K's tangent and the total
     cplx Yb = mk(0.0), Yt = mk(0.0);
@@ -557,8 +579,12 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
       const cplx dBc = (Vt * sn) * ((dR * eR * sn / Vt) * dV(NP + 1) - (d0 * e0 * sn / Vt) * dV(0));
       const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (K / sgl) * dsgl[c];
       const cplx dK_t = (-sn / sgl) * ddb_t[c];
-      Yb = Yb + sign * (Q * hsum) * dK_b + sign * sumJ_b[c];
-      Yt = Yt + sign * (Q * hsum) * dK_t + sign * sumJ_t[c];
+      if (!cdiff) {  // the differential current has no K
+        Yb = Yb + sign * (Q * hsum) * dK_b;
+        Yt = Yt + sign * (Q * hsum) * dK_t;
+      }
+      Yb = Yb + sign * sumJ_b[c];
+      Yt = Yt + sign * sumJ_t[c];
     }
     Yt = Yt + dJD;
     const cplx Y = (1.0 / hsum) * (Yb + lap * Yt);
@@ -935,6 +961,13 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
     cplx daev_f[2] = {mk(0.0), mk(0.0)}, daev_l[2] = {mk(0.0), mk(0.0)};
     int first_i[2] = {-1, -1};
     double hsum = 0.0, dx_prev = 0.0, h_prev = 0.0;
+    // `currDiffInt = 1`: each interval's Scharfetter-Gummel flux for the carriers and the ions
+    // (jaxdd batch.py:366-369, 471-479), from the points at both ends of the interval
+    const bool cdiff = L.sc(C_CURRDIFF) > 0.0;
+    cplx jd_prev[2] = {mk(0.0), mk(0.0)}, jdi_prev[2] = {mk(0.0), mk(0.0)};
+    cplx dsumd_i[2] = {mk(0.0), mk(0.0)};
+    Pt Pa, Pb;
+    if (cdiff) point(L, 0, Vint, Pa);
     for (int k = 0; k <= NP; ++k) {
       const double hk = L.st(k, S_H);
       const double dx = k < NP ? L.st(k, S_DX) : 0.0;
@@ -965,6 +998,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
         dU[1] = rec(k, P_TRP) * df;
       }
       const bool iface_k = L.st(k, S_IFK) > -1.5;
+      if (cdiff) point(L, k + 1, Vint, Pb);
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const double sn = c == 0 ? -1.0 : 1.0;
@@ -986,8 +1020,20 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
           dS_b[c] = dS_b[c] + (sn * Q * L.L * width) * duc_b;
           dS_t[c] = dS_t[c] + (sn * Q * L.L * width) * duc_t;
         }
-        if (iface_k) {
-          const cplx thr = (sn * 0.5 * Q * L.L * hk) * (dRi_k[c] + dRi_k1[c]);
+        const cplx thr = (sn * 0.5 * Q * L.L * hk) * (dRi_k[c] + dRi_k1[c]);
+        if (cdiff) {  // as without ions
+          const double d0 = c == 0 ? Pa.n : Pa.p, d1 = c == 0 ? Pb.n : Pb.p;
+          const double g0 = Pa.V + (c == 0 ? Pa.offn : Pa.offp);
+          const double g1 = Pb.V + (c == 0 ? Pb.offn : Pb.offp);
+          double bf, bb, dbf, dbb;
+          bern_pair(sn * (g1 - g0) / Vt, L.simss, bf, bb, dbf, dbb);
+          const cplx dxk = (sn / Vt) * (dV(k + 1) - dV(k));
+          const cplx djd = (sn * Q * mu * Vt / (L.L * hk)) *
+                           (d1 * (bb * dyv(k + 1, 1 + c) - dbb * dxk) -
+                            d0 * (bf * dyv(k, 1 + c) + dbf * dxk));
+          sumJ_b[c] = sumJ_b[c] + hk * (iface_k ? jd_prev[c] + thr : djd);
+          jd_prev[c] = djd;
+        } else if (iface_k) {
           sumJ_b[c] = sumJ_b[c] + hk * (dS_prev_b + thr);
           sumJ_t[c] = sumJ_t[c] + hk * dS_prev_t;
         } else {
@@ -1020,6 +1066,15 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
           aev_l[sp] = nb * evb;
           daev_l[sp] = (nb * evb) * dlnb + nb * devb;
         }
+        if (cdiff) {  // the region's flux on interval k; across an interface the one before it
+          double bf, bb, dbf, dbb;
+          bern_pair(sn * (Pb.V - Pa.V) / Vt, L.simss, bf, bb, dbf, dbb);
+          const cplx dxk = (sn / Vt) * (dV(k + 1) - dV(k));
+          const cplx djd = (sn * Q * W.x(k, tf) * Vt / (L.L * hk)) *
+                           (nb * (bb * dlnb - dbb * dxk) - na * (bf * dlna + dbf * dxk));
+          if (ina && inb) dsumd_i[sp] = dsumd_i[sp] + hk * (iface_k ? jdi_prev[sp] : djd);
+          jdi_prev[sp] = djd;
+        }
         if (ina && inb) {
           const double mua = W.x(k, tf), mub = W.x(k + 1, tf);
           const double ia = 1.0 / (mua > 0.0 ? mua : 1.0), ib = 1.0 / (mub > 0.0 ? mub : 1.0);
@@ -1037,6 +1092,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       }
       dx_prev = dx;
       h_prev = hk;
+      if (cdiff) Pa = Pb;
     }
     cplx Yb = mk(0.0), Yt = mk(0.0);
 #pragma unroll
@@ -1052,12 +1108,20 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       const cplx dBc = (Vt * sn) * ((dR * eR * sn / Vt) * dV(NP + 1) - (d0 * e0 * sn / Vt) * dV(0));
       const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (K / sgl) * dsgl[c];
       const cplx dK_t = (-sn / sgl) * ddb_t[c];
-      Yb = Yb + sign * (Q * hsum) * dK_b + sign * sumJ_b[c];
-      Yt = Yt + sign * (Q * hsum) * dK_t + sign * sumJ_t[c];
+      if (!cdiff) {  // the differential current has no K
+        Yb = Yb + sign * (Q * hsum) * dK_b;
+        Yt = Yt + sign * (Q * hsum) * dK_t;
+      }
+      Yb = Yb + sign * sumJ_b[c];
+      Yt = Yt + sign * sumJ_t[c];
     }
 #pragma unroll
     for (int sp = 0; sp < 2; ++sp) {
       if (!(L.tot[sp] > 0.0) || first_i[sp] < 0) continue;
+      if (cdiff) {
+        Yb = Yb + sign * dsumd_i[sp];
+        continue;
+      }
       const double sn = sp == 0 ? -1.0 : 1.0;
       const double sgl = is_[sp] > 0.0 ? is_[sp] : 1.0;
       const double K0 = Vt * sn * (aev_l[sp] - aev_f[sp]) / sgl;  // the state's (U = 0)

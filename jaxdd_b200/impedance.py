@@ -119,7 +119,9 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
     impedance.py:365-409). Free mobile ions move with the voltage as unknowns of their own.
     Refused (`NotImplementedError`), as the reference refuses them or as this build does not
     carry them: ions frozen at a pre-bias, several ion regions of a species, an ion region that
-    reaches a contact, the differential current (`currDiffInt = 1`). `dt` (s): instead of the continuous response, what
+    reaches a contact. With the differential current (`currDiffInt = 1`) the current's tangent is
+    each interval's Scharfetter–Gummel flux's, the ions' too. `dt` (s): instead of the continuous
+    response, what
     `solve_transient` sees through implicit Euler at steps of `dt` (its time terms at
     `(1 − e^(−iω dt))/dt`, the traps' occupations over each step as it solves them)."""
     devs = batch["devices"]
@@ -130,8 +132,6 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
     from .transient import reaches_contact
     if _mobile(batch) and any(reaches_contact(d) for d in devs):
         raise NotImplementedError("impedance with an ion region that reaches a contact")
-    if any(d.curr_diff for d in devs):
-        raise NotImplementedError("impedance with the differential current (currDiffInt = 1)")
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
     if dt is not None and not dt > 0:
         raise ValueError(f"dt must be positive, got {dt}")

@@ -109,6 +109,26 @@ def _stencils(dev) -> dict:
 _TI_KEYS = ("Nt", "Cn", "Cp", "nt0_lo", "pt0_lo", "nt0_hi", "pt0_hi", "iw", "charge", "cwe")
 
 
+def bern_complex(x, simss=False):
+    """The Bernoulli function (`bern_exact` or `bern_simss`, solver.py:95-121) at complex
+    arguments near the real axis, for complex-step derivatives: each branch chosen by the real
+    part, every branch analytic."""
+    x = np.asarray(x, dtype=complex)
+    a = np.abs(x.real)
+    if not simss:
+        small = a < SERIES_BELOW
+        safe = np.where(small, 1.0, x)
+        return np.where(small, 1.0 - x / 2.0 + x * x / 12.0 - x ** 4 / 720.0,
+                        safe / np.expm1(safe))
+    safe = np.where(a < 1.5, 2.0, x)
+    full = safe / np.expm1(safe)
+    o1 = 1.0 - 0.5 * x
+    o2 = 1.0 - x * (0.5 - x / 12.0)
+    o4 = 1.0 + x * (-0.5 + x * (1.0 / 12.0 - x * x / 720.0))
+    return np.where(a < 0.05, o1, np.where(a < 0.45, o2, np.where(a < 1.5, o4, full)))
+
+
+
 def _slots_of(mask, total, masks, totals):
     if masks is None:
         return mask[None].astype(float), np.array([float(total)])

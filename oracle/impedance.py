@@ -134,11 +134,13 @@ def interface_rates(ti, n, p, lap, dy3, dt=None):
     return points(dR[0] * df, dR[1] * df), points(dR[2] * df, dR[3] * df)
 
 
-def current_tr(d, full, dti, before, Vbefore, width, dU=None, dRi=None):
+def current_tr(d, full, dti, before, Vbefore, width, dU=None, dRi=None, simss=False):
     """`batch._current` over a time step (`tr`: the state `before`, `dti`, control-volume widths;
     no ions, no bulk occupations carried; `dU`, `dRi` each carrier's rates beyond the steady
     traps'): one lane of the oracle's tree `d` (1-lane arrays), `full` (NP + 2) × 3, complex
-    allowed (complex-step derivatives)."""
+    allowed (complex-step derivatives). Where `curr_diff` each interval carries its
+    Scharfetter–Gummel flux (`Calc_Curr_Diff`, batch.py:383-386) with SIMsalabim's Bernoulli
+    function if `simss`."""
     V, n, p = full[:, 0], np.exp(full[:, 1]), np.exp(full[:, 2])
     Vt, x, h, L = d["Vt"][0], d["x"][0], d["h"][0], d["L"][0]
     NP = x.shape[0] - 2
@@ -180,6 +182,10 @@ def current_tr(d, full, dti, before, Vbefore, width, dU=None, dRi=None):
         K = (Vt * (sn * dens[NP + 1] * np.exp(sn * Vg[NP + 1] / Vt)
                    - sn * dens[0] * np.exp(sn * Vg[0] / Vt)) - sn * double) / single
         J = Q * K + np.concatenate([[0.0], np.cumsum(sn * Q * L * width[1:NP + 1] * U[1:NP + 1])])
+        if d["curr_diff"][0] > 0:
+            dVg = sn * np.diff(Vg) / Vt
+            J = sn * Q * mu[:NP + 1] * Vt * (dens[1:] * dd.bern_complex(-dVg, simss)
+                                             - dens[:-1] * dd.bern_complex(dVg, simss)) / (L * h[:NP + 1])
         through = sn * 0.5 * Q * L * h[:NP + 1] * (R_i[:NP + 1] + R_i[1:])
         return np.where(d["iface"][0], np.roll(J, 1) + through, J)
 
@@ -223,14 +229,17 @@ def admittance(d, full0, Vint, laps, bern, dt=None):
 
     h_cs = 1e-30
 
+    simss = bern is dd.bern_simss
+
     def linear(dy_real, dV, dti):  # J_y dy + J_V dV at dti, by complex step
         y = y3 + 1j * h_cs * dy_real
         V = Vint + 1j * h_cs * dV
-        return np.imag(current_tr(d, full_of(y, V), dti, before, Vb, width)) / h_cs
+        return np.imag(current_tr(d, full_of(y, V), dti, before, Vb, width,
+                                  simss=simss)) / h_cs
 
     def rates(dU, dRi):  # linear in both
-        J0 = current_tr(d, full0.astype(complex), 0.0, before, Vb, width)
-        J1 = current_tr(d, full0.astype(complex), 0.0, before, Vb, width, dU, dRi)
+        J0 = current_tr(d, full0.astype(complex), 0.0, before, Vb, width, simss=simss)
+        J1 = current_tr(d, full0.astype(complex), 0.0, before, Vb, width, dU, dRi, simss=simss)
         return J1 - J0
 
     out = []

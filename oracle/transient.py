@@ -403,6 +403,13 @@ def width_of(d, zimt):
     return np.concatenate([hh[:, :1], 0.5 * (hh[:, :-1] + hh[:, 1:])], 1)
 
 
+def _bern_of(bern, x):
+    """`bern`'s B(x); at complex `x` (complex-step derivatives) its analytic continuation."""
+    if np.iscomplexobj(x):
+        return dd.bern_complex(x, bern is dd.bern_simss)
+    return bern(x)[0]
+
+
 def current(d, full, tr, bern, zimt, steady_traps=False, dU=None, dRi=None):
     """batch._current over a step (batch.py:302-403, 421-483): SIMsalabim's integral form with
     each density's change in the integrand (summed over `width_of`), the ions' currents region
@@ -479,8 +486,7 @@ def current_parts(d, full, tr, bern, zimt, steady_traps=False, dU=None, dRi=None
         diff = d["curr_diff"] > 0
         if np.any(diff):
             dV = sn * np.diff(Vg, axis=1) / Vt
-            Bm, _ = bern(-dV)
-            Bp, _ = bern(dV)
+            Bm, Bp = _bern_of(bern, -dV), _bern_of(bern, dV)
             flux = sn * Q * mu[:, :NP + 1] * Vt * (dens[:, 1:] * Bm - dens[:, :-1] * Bp) / (
                 L * h[:, :NP + 1])
             J = np.where(diff[:, None], flux, J)
@@ -547,8 +553,7 @@ def ion_currents(d, full, tr, bern, width, apart=False):
         diff = d["curr_diff"] > 0
         if np.any(diff):
             dV = sn * np.diff(V, axis=1) / Vt
-            Bm, _ = bern(-dV)
-            Bp, _ = bern(dV)
+            Bm, Bp = _bern_of(bern, -dV), _bern_of(bern, dV)
             flux = sn * Q * mu[:, :NP + 1] * Vt * (dens[:, 1:] * Bm - dens[:, :-1] * Bp) / (
                 L * h[:, :NP + 1])
             J = np.where(diff[:, None], flux, J)

@@ -91,14 +91,9 @@ def test_what_impedance_refuses():
     from jaxdd_b200.workloads import drawn_devices
     with pytest.raises(NotImplementedError, match="frozen"):
         solve_impedance(prepare(drawn_devices(2, NP=50)), [1e3])
-    t = pin_texts(50)
-    t["simulation_setup.txt"] = t["simulation_setup.txt"].replace("currDiffInt = 2",
-                                                                  "currDiffInt = 1")
-    with pytest.raises(NotImplementedError, match="differential"):
-        solve_impedance(prepare([build_device(setup_from_texts(t))]), [1e3])
 
 
-def _fast_ion_stack(NP=60):
+def _fast_ion_stack(NP=60, differential=False):
     """One of the drawn mobile-ion stacks with its ions at 1e-9 m²/Vs: they follow at 1 kHz."""
     from jaxdd_b200.workloads import SEED_ION_STACKS
     k = 1
@@ -107,7 +102,44 @@ def _fast_ion_stack(NP=60):
         f"{line.split('=')[0].strip()} = 1e-9"
         if line.split("=")[0].strip() in ("mu_anion", "mu_cation") else line
         for line in texts["L2.txt"].splitlines()) + "\n"
-    return build_device(setup_from_texts(texts))
+    return build_device(setup_from_texts(_differential(texts) if differential else texts))
+
+
+def _differential(texts):
+    """The same device with SIMsalabim's differential current (`currDiffInt = 1`)."""
+    setup = texts["simulation_setup.txt"]
+    assert "currDiffInt = 2" in setup
+    return dict(texts, **{"simulation_setup.txt": setup.replace("currDiffInt = 2",
+                                                                "currDiffInt = 1")})
+
+
+@pytest.mark.parametrize("bernoulli_name", ["exact", "simss"])
+def test_the_differential_current_matches_the_oracle(bernoulli_name):
+    """`currDiffInt = 1` (each interval's Scharfetter–Gummel flux in the current, jaxdd
+    batch.py:366-369, 471-479) in both kernels: the p-i-n cell with and without interface traps
+    and two drawn stacks without ions (`dd_admittance`), then two mobile-ion stacks with the
+    differential current beside one with the integral form (`dd_admittance_ions`), against the
+    oracle to 1e-6."""
+    from jaxdd_b200.workloads import SEED_ION_STACKS
+    plain = []
+    for interface in (False, True):
+        t = pin_texts(100)
+        if interface:
+            for name in ("L1.txt", "L2.txt"):
+                t[name] = t[name].replace("N_t_int = 0", "N_t_int = 1e15")
+        plain.append(build_device(setup_from_texts(_differential(t))))
+    ions = [build_device(setup_from_texts(_differential(drawn_texts(
+        k, np.random.default_rng([SEED_ION_STACKS, k]), 100)))) for k in (1, 3)]
+    ions.append(build_device(setup_from_texts(drawn_texts(
+        5, np.random.default_rng([SEED_ION_STACKS, 5]), 100))))
+    assert [d.curr_diff for d in ions] == [True, True, False]
+    for devs, V0 in ((plain, 0.7), (ions, 0.8)):
+        r = solve_impedance(prepare(devs), F, voltage=V0, bernoulli_name=bernoulli_name)
+        Yo, Zo, Jo, oko = imp.solve_impedance(devs, F, voltage=V0,
+                                              bernoulli_name=bernoulli_name)
+        assert np.array_equal(r.converged, oko) and r.converged.all()
+        rel = np.abs(r.Y - Yo) / np.abs(Yo)
+        assert np.max(rel) < 1e-6, rel
 
 
 def _gpu_sine_response(dev, V0, f, amp, per_period=40, periods=20, fitted=4):
@@ -129,20 +161,25 @@ def _gpu_sine_response(dev, V0, f, amp, per_period=40, periods=20, fitted=4):
     return (c[1] + 1j * c[2]) / amp, dt
 
 
-@pytest.mark.parametrize("case", ["ions", "interface"])
+@pytest.mark.parametrize("case", ["ions", "interface", "ions-differential",
+                                  "interface-differential"])
 def test_the_dt_form_is_the_gpu_transients_response(case):
     """The two GPU paths against each other: `solve_impedance(..., dt=)` (`dd_admittance_ions`,
     `dd_admittance`) is the GPU transient's (`dd_transient`) response to a small sine at steps of
     dt, with mobile ions following at 1 kHz, and with interface traps at 10 kHz (1e-6 and 1e-7,
     the reference's bars), and the oracle's dt form."""
-    if case == "ions":
-        dev, V0, f, amp, bar = _fast_ion_stack(), 0.8, 1e3, 1e-4, 1e-6
+    differential = case.endswith("-differential")
+    if case.startswith("ions"):
+        dev, V0, f, amp, bar = _fast_ion_stack(differential=differential), 0.8, 1e3, 1e-4, 1e-6
     else:
         t = pin_texts(60)
         for name in ("L1.txt", "L2.txt"):
             t[name] = t[name].replace("N_t_int = 0", "N_t_int = 1e15")
+        if differential:
+            t = _differential(t)
         dev, V0, f, amp, bar = build_device(setup_from_texts(t)), 0.6, 1e4, 1e-5, 1e-7
-    Yt, dt = _gpu_sine_response(dev, V0, f, amp, periods=20 if case == "ions" else 12)
+    assert dev.curr_diff == differential
+    Yt, dt = _gpu_sine_response(dev, V0, f, amp, periods=20 if case.startswith("ions") else 12)
     r = solve_impedance(prepare([dev]), [f], voltage=V0, tol=1e-12, max_iter=200, dt=dt)
     assert abs(r.Y[0, 0] / Yt - 1) < bar
     Yo = imp.solve_impedance([dev], [f], voltage=V0, tol=1e-12, max_iter=200, dt=dt)[0][0, 0]

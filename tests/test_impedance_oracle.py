@@ -176,3 +176,54 @@ def test_with_interface_traps_the_dt_form_is_the_transients_response():
     Yc = imp.solve_impedance([dev], [1e4], voltage=0.6, tol=1e-12, max_iter=200)[0][0, 0]
     assert abs(Yd / Yt - 1) < 1e-7
     assert abs(Yc / Yt - 1) > 1e-2
+
+
+def _differential(texts):
+    """The same device with SIMsalabim's differential current (`currDiffInt = 1`)."""
+    setup = texts["simulation_setup.txt"]
+    assert "currDiffInt = 2" in setup
+    return dict(texts, **{"simulation_setup.txt": setup.replace("currDiffInt = 2",
+                                                                "currDiffInt = 1")})
+
+
+def test_the_differential_current_low_frequency_is_the_steady_slope():
+    """With `currDiffInt = 1` every interval carries its Scharfetter–Gummel flux (jaxdd
+    batch.py:366-369); its tangent (complex step through the flux, the Bernoulli function
+    continued to complex arguments) gives the steady slope at 1e-7 Hz. dV 1e-4: the differential
+    current cancels large fluxes, so a smaller difference is round-off (4e-6 at dV 1e-6)."""
+    dev = build_device(setup_from_texts(_differential(pin_texts(60))))
+    assert dev.curr_diff
+    V0, dV = 0.6, 1e-4
+    for name in ("exact", "simss"):
+        Y, _, _, ok = imp.solve_impedance([dev], [1e-7], voltage=V0, tol=1e-12, max_iter=200,
+                                          bernoulli_name=name)
+        st = dd.solve_states(dd.prepare([dev]), [V0 - dV, V0 + dV], tol=1e-13, max_iter=200,
+                             bernoulli_name=name)
+        slope = (st["J"][0, 1] - st["J"][0, 0]) / (2 * dV)
+        assert ok.all()
+        assert Y[0, 0].real == pytest.approx(slope, rel=1e-6)
+
+
+@pytest.mark.parametrize("case", ["ions", "interface"])
+def test_the_differential_current_dt_form_is_the_transients_response(case):
+    """The differential current's admittance with `dt` against the oracle transient's response to
+    a small sine (its current the same fluxes, from its own solve): with mobile ions following at
+    1 kHz (their own fluxes too, jaxdd batch.py:471-479) to 1e-6, with interface traps to 1e-7
+    (measured 1.4e-8 and 6e-9)."""
+    if case == "ions":
+        k = 1
+        texts = drawn_texts(k, np.random.default_rng([SEED_ION_STACKS, k]), 60)
+        texts["L2.txt"] = "\n".join(
+            f"{line.split('=')[0].strip()} = 1e-9"
+            if line.split("=")[0].strip() in ("mu_anion", "mu_cation") else line
+            for line in texts["L2.txt"].splitlines()) + "\n"
+        V0, f, amp, periods, bar = 0.8, 1e3, 1e-4, 20, 1e-6
+    else:
+        texts = pin_texts(60)
+        for name in ("L1.txt", "L2.txt"):
+            texts[name] = texts[name].replace("N_t_int = 0", "N_t_int = 1e15")
+        V0, f, amp, periods, bar = 0.6, 1e4, 1e-5, 12, 1e-7
+    dev = build_device(setup_from_texts(_differential(texts)))
+    Yt, dt = _sine_response(dev, V0, f, amp=amp, periods=periods)
+    Yd = imp.solve_impedance([dev], [f], voltage=V0, tol=1e-12, max_iter=200, dt=dt)[0][0, 0]
+    assert abs(Yd / Yt - 1) < bar
