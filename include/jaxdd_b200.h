@@ -207,9 +207,11 @@ int dd_admittance_ions_workspace_bytes(const dd_batch* batch, int n_freq, size_t
  * the linearised current. `state` [np_max+2][3][lane_stride] and `state_logs`
  * [DD_MAXK][lane_stride] the steady state (dd_solve_states' checkpoint at `vint`, the ions
  * Boltzmann's of those normalisations); `tstat` [np_max+2][DD_NT][lane_stride] the
- * permittivity and the ions' mobilities. k_anion and k_cation must be 1; devices without mobile
- * ions are solved too (their ions' rows identities). Y [n_freq][2][lane_stride]; `dt` as
- * dd_admittance's. */
+ * permittivity and the ions' mobilities. Several regions of a species each keep their own
+ * number (a slot each: k_anion + k_cation <= DD_MAXK, the border K columns wide); devices without
+ * mobile ions are solved too (their ions' rows identities). The differential current
+ * (`currDiffInt = 1`) is each interval's Scharfetter-Gummel flux's tangent, the ions' too.
+ * Y [n_freq][2][lane_stride]; `dt` as dd_admittance's. */
 int dd_admittance_ions(const dd_batch* batch, const double* state, const double* state_logs,
                        const double* tstat, const double* vint, const double* laps, int n_freq,
                        int bernoulli, double dt, double* Y, void* workspace,

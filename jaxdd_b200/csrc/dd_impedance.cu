@@ -82,6 +82,7 @@ enum { W_C = 0, W_D = 18, W_WORDS = 24 };
 
 struct Args {
   int B, Bp, npmax, ka, simss, nf;
+  int K;  // ion slots, anion slots first (2 .. DD_MAXK; the ions' kernels)
   double dt;  // > 0: implicit Euler's steps of dt (the traps' step response); 0: continuous
   const double* S;
   const double* C;
@@ -568,7 +569,7 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
       const double sn = c == 0 ? -1.0 : 1.0;
-      const double sgl = a.lsc[(size_t)(L_SN + c) * a.Bp + l], K = a.lsc[(size_t)(L_KN + c) * a.Bp + l];
+      const double sgl = a.lsc[(size_t)(L_SN + c) * a.Bp + l], Kc = a.lsc[(size_t)(L_KN + c) * a.Bp + l];
       // the contacts' densities are fixed; their exp(sn Vg / V_T) move with the voltage
       Pt P0, PR;
       point(L, 0, Vint, P0);
@@ -577,7 +578,7 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
       const double e0 = exp(sn * ((c == 0 ? P0.offn : P0.offp) + P0.V) / Vt);
       const double eR = exp(sn * ((c == 0 ? PR.offn : PR.offp) + PR.V) / Vt);
       const cplx dBc = (Vt * sn) * ((dR * eR * sn / Vt) * dV(NP + 1) - (d0 * e0 * sn / Vt) * dV(0));
-      const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (K / sgl) * dsgl[c];
+      const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (Kc / sgl) * dsgl[c];
       const cplx dK_t = (-sn / sgl) * ddb_t[c];
       if (!cdiff) {  // the differential current has no K
         Yb = Yb + sign * (Q * hsum) * dK_b;
@@ -607,8 +608,15 @@ __global__ void __launch_bounds__(64) admittance_kernel(Args a) {
 // densities and exp(-+V/V_T) of the steady state.
 enum { R_A = 0, R_B = 25, R_C = 50, R_M = 75, R_U3 = 80, R_U4, R_W3, R_W4, R_NA, R_NC, R_EVA,
        R_EVC, R5_WORDS };
-// Per node of a (device, frequency) thread: c' (25 complex) and [-dF | U_a | U_c] (15 complex).
-enum { V_C = 0, V_D = 50, V_WORDS = 80 };
+// At a contact (nodes 0 and np+1, whose rows' words are free) where an ion region reaches it,
+// per species (anion, cation): its ln density from its neighbour's, `_ion_full`'s at a step
+// (dti = 1: ln(B(x)/B(-x))) and Boltzmann's (dti = 0); d(ln density)/d(V of the neighbour) of
+// the first; and the region's number's derivative in the neighbour's potential through it.
+enum { CT_LNR = R_A, CT_SR = R_A + 2, CT_LNB = R_A + 4, CT_WV = R_A + 6, CT_WORDS = 8 };
+// Per node of a (device, frequency) thread: c' (25 complex) and [-dF | U_0 .. U_K-1] (5 (1 + K)
+// complex; each slot's column, anion slots first).
+enum { V_C = 0, V_D = 50 };
+__host__ __device__ constexpr int vwords(int K) { return V_D + 10 * (1 + K); }
 
 struct IonArgs {
   const double* X;           // [np+2][DD_NT][Bp]: permittivity, anion and cation mobility
@@ -638,8 +646,7 @@ __device__ void ion_point(const tr::View& W, int k, double Vint, const double* l
 
 __device__ void ion_view(tr::View& W, const Args& a, const IonArgs& b, int l) {
   lane_init(W.L, a, l);
-  W.L.tot[0] = W.L.sc(C_TOT0);
-  W.L.tot[1] = W.L.sc(C_TOT0 + 1);
+  for (int k = 0; k < DD_MAXK; ++k) W.L.tot[k] = k < a.K ? W.L.sc(C_TOT0 + k) : 0.0;
   W.X = b.X;
   W.Yb = nullptr;
   W.ybuf = 0;
@@ -649,6 +656,7 @@ __device__ void ion_view(tr::View& W, const Args& a, const IonArgs& b, int l) {
 }
 
 // The ions' record of each device: its rows as a step of dti = 1 from the steady state itself.
+template <int K>
 __global__ void __launch_bounds__(32) prepare_ions_kernel(Args a, IonArgs b) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= a.B) return;
@@ -657,8 +665,9 @@ __global__ void __launch_bounds__(32) prepare_ions_kernel(Args a, IonArgs b) {
   const Lane& L = W.L;
   const int NP = L.NP;
   const double Vint = a.vint[l];
-  double logs[2] = {b.state_logs[l], b.state_logs[(size_t)a.Bp + l]};
-  const double zero[2] = {0.0, 0.0};
+  double logs[K], zero[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) { logs[k] = b.state_logs[(size_t)k * a.Bp + l]; zero[k] = 0.0; }
   auto rec = [&](int k, int f) -> double& {
     return b.rec5[((size_t)k * R5_WORDS + f) * a.Bp + l];
   };
@@ -670,8 +679,8 @@ __global__ void __launch_bounds__(32) prepare_ions_kernel(Args a, IonArgs b) {
   for (int i = 1; i <= NP; ++i) {
     ion_point(W, i + 1, Vint, logs, pn);
     flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
-    double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][2], M[5];
-    tr::row5<2, true>(W, i, pm, pc, pn, el, er, L.st(i - 1, S_H), L.st(i, S_H),
+    double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][K], M[5];
+    tr::row5<K, true>(W, i, pm, pc, pn, el, er, L.st(i - 1, S_H), L.st(i, S_H),
                       (int)L.st(i - 1, S_IFK), (int)L.st(i, S_IFK), 1.0, 0.0, 0.0, 0.0, pc.c.n,
                       pc.c.p, pc.c.da, pc.c.dc, zero, A, Bm, Cm, r, U, M);
 #pragma unroll
@@ -684,8 +693,8 @@ __global__ void __launch_bounds__(32) prepare_ions_kernel(Args a, IonArgs b) {
       }
       rec(i, R_M + rr) = M[rr];
     }
-    rec(i, R_U3) = pc.c.sl.a >= 0 ? U[3][pc.c.sl.a] : 0.0;
-    rec(i, R_U4) = pc.c.sl.c >= 0 ? U[4][L.ka + pc.c.sl.c] : 0.0;
+    rec(i, R_U3) = pc.c.sl.a >= 0 ? pick<K>(U[3], pc.c.sl.a) : 0.0;
+    rec(i, R_U4) = pc.c.sl.c >= 0 ? pick<K>(U[4], L.ka + pc.c.sl.c) : 0.0;
     // the constraints' border: each region's number in its points' ion logarithms
     const double hLm = L.st(i - 1, S_H) * L.L, hLp = L.st(i, S_H) * L.L;
     double w3 = 0.0, w4 = 0.0;
@@ -707,6 +716,45 @@ __global__ void __launch_bounds__(32) prepare_ions_kernel(Args a, IonArgs b) {
     rec(k, R_NC) = P.c.dc;
     rec(k, R_EVA) = exp(-P.c.V * L.iVt);
     rec(k, R_EVC) = exp(P.c.V * L.iVt);
+  }
+  // the contacts that an ion region reaches (`_ion_full`, solver.py:1315-1346): no flux over
+  // the contact's interval at a step, Boltzmann's in the steady state; the region's number
+  // (trapezoidal over its intervals, `_ion_constraints_time`) takes the contact's share
+  for (int side = 0; side < 2; ++side) {
+    const int c = side == 0 ? 0 : NP + 1, nb = side == 0 ? 1 : NP;
+    tr::TP Pc, Pn;
+    ion_point(W, c, Vint, logs, Pc);
+    ion_point(W, nb, Vint, logs, Pn);
+    const double x = side == 0 ? (Pn.c.V - Pc.c.V) * L.iVt : (Pc.c.V - Pn.c.V) * L.iVt;
+    double bf, bb, dbf, dbb;
+    bern_pair(x, L.simss, bf, bb, dbf, dbb);
+    const double r = log(bf) - log(bb), dr = dbf / bf + dbb / bb;
+    const double hL = L.st(side == 0 ? 0 : NP, S_H) * L.L;
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) {
+      const int reg = sp == 0 ? Pc.c.sl.a : Pc.c.sl.c;
+      const int regn = sp == 0 ? Pn.c.sl.a : Pn.c.sl.c;
+      const int q = sp == 0 ? reg : L.ka + reg;
+      double lnR = 0.0, sR = 0.0, lnB = 0.0, wv = 0.0;
+      if (reg >= 0) {
+        const double lnn = sp == 0 ? Pn.la : Pn.lc;
+        // anions: ln a_0 = ln a_1 + r(x), ln a_N+1 = ln a_N - r(x); the cations the other way
+        const double sg = (sp == 0) == (side == 0) ? 1.0 : -1.0;
+        lnR = lnn + sg * r;
+        sR = (sp == 0 ? 1.0 : -1.0) * dr * L.iVt;
+        lnB = lnn + (sp == 0 ? 1.0 : -1.0) * (Pc.c.V - Pn.c.V) * L.iVt;
+        const double tq = pick<K>(L.tot, q);
+        if (regn == reg && tq > 0.0) {
+          const double w = 0.5 * hL * exp(lnR) / tq;
+          rec(nb, sp == 0 ? R_W3 : R_W4) += w;
+          wv = w * sR;
+        }
+      }
+      rec(c, CT_LNR + sp) = lnR;
+      rec(c, CT_SR + sp) = sR;
+      rec(c, CT_LNB + sp) = lnB;
+      rec(c, CT_WV + sp) = wv;
+    }
   }
 }
 
@@ -758,7 +806,35 @@ __device__ void capply(const CPart& f, cplx (&v)[5]) {
   v[4] = z1;
 }
 
+// The K x K system M z = r (complex) by Gauss-Jordan elimination with partial pivoting, z over r.
+template <int K>
+__device__ void csolve(cplx (&M)[K][K], cplx (&r)[K]) {
+  for (int c = 0; c < K; ++c) {
+    int piv = c;
+    double best = M[c][c].re * M[c][c].re + M[c][c].im * M[c][c].im;
+    for (int rr = c + 1; rr < K; ++rr) {
+      const double v = M[rr][c].re * M[rr][c].re + M[rr][c].im * M[rr][c].im;
+      if (v > best) { best = v; piv = rr; }
+    }
+    if (piv != c) {
+      for (int q = 0; q < K; ++q) { const cplx t = M[c][q]; M[c][q] = M[piv][q]; M[piv][q] = t; }
+      const cplx t = r[c]; r[c] = r[piv]; r[piv] = t;
+    }
+    const cplx inv = mk(1.0) / M[c][c];
+    for (int q = 0; q < K; ++q) M[c][q] = M[c][q] * inv;
+    r[c] = r[c] * inv;
+    for (int rr = 0; rr < K; ++rr) {
+      if (rr == c) continue;
+      const cplx f = M[rr][c];
+      for (int q = 0; q < K; ++q) M[rr][q] = M[rr][q] - f * M[c][q];
+      r[rr] = r[rr] - f * r[c];
+    }
+  }
+}
+
+template <int K>
 __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) {
+  constexpr int NC = 1 + K, VW = vwords(K);
   for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < (long)a.Bp * a.nf;
        t += (long)gridDim.x * blockDim.x) {
     const int l = (int)(t % a.Bp), q = (int)(t / a.Bp);
@@ -773,17 +849,17 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
     auto rec = [&](int k, int f) { return a.rec[((size_t)k * P_WORDS + f) * a.Bp + l]; };
     auto r5 = [&](int k, int f) { return b.rec5[((size_t)k * R5_WORDS + f) * a.Bp + l]; };
     auto scr = [&](int k, int f) -> double& {
-      return b.scr5[((size_t)k * V_WORDS + f) * a.T + slot];
+      return b.scr5[((size_t)k * VW + f) * a.T + slot];
     };
     const double e = L.left();
     // ---- forward elimination of (J + (iw - 1) M + traps) [dy | X_U] = [-dF/dV | U]
-    cplx cp[5][5], dp[5][3];
+    cplx cp[5][5], dp[5][NC];
 #pragma unroll
     for (int rr = 0; rr < 5; ++rr) {
 #pragma unroll
       for (int c = 0; c < 5; ++c) cp[rr][c] = mk(0.0);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) dp[rr][c] = mk(0.0);
+      for (int c = 0; c < NC; ++c) dp[rr][c] = mk(0.0);
     }
     for (int i = 1; i <= NP; ++i) {
       cplx A[5][5], Bm[5][5], Cm[5][5];
@@ -826,16 +902,21 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
             Cm[rr][c] = Cm[rr][c] + dC[rr][c];
           }
       }
-      // right-hand sides: -dF/dV (the contacts' potentials), then the slots' columns
-      cplx rhs[5][3];
+      // right-hand sides: -dF/dV (the contacts' potentials), then the slots' columns (the
+      // point's anion slot in the anions' row, its cation slot in the cations')
+      const Slots si = slots_at(L, i);
+      const int ja = si.a >= 0 ? si.a : -1, jc = si.c >= 0 ? L.ka + si.c : -1;
+      const double u3 = r5(i, R_U3), u4 = r5(i, R_U4);
+      cplx rhs[5][NC];
 #pragma unroll
       for (int rr = 0; rr < 5; ++rr) {
         double dF = 0.0;
         if (i == 1) dF += r5(1, R_A + 5 * rr) * 0.5 * e;
         if (i == NP) dF += r5(NP, R_C + 5 * rr) * (-0.5 * e);
         rhs[rr][0] = mk(-dF);
-        rhs[rr][1] = mk(rr == 3 ? r5(i, R_U3) : 0.0);
-        rhs[rr][2] = mk(rr == 4 ? r5(i, R_U4) : 0.0);
+#pragma unroll
+        for (int c = 1; c < NC; ++c)
+          rhs[rr][c] = mk(rr == 3 && c - 1 == ja ? u3 : rr == 4 && c - 1 == jc ? u4 : 0.0);
       }
       cplx M[5][5];
 #pragma unroll
@@ -848,7 +929,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
           M[rr][c] = s;
         }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < NC; ++c) {
           cplx s = rhs[rr][c];
 #pragma unroll
           for (int k = 0; k < 5; ++k) s = s - A[rr][k] * dp[k][c];
@@ -869,34 +950,39 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
         }
       }
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
+      for (int c = 0; c < NC; ++c) {
         cplx v[5] = {rhs[0][c], rhs[1][c], rhs[2][c], rhs[3][c], rhs[4][c]};
         capply(f, v);
 #pragma unroll
         for (int rr = 0; rr < 5; ++rr) {
           dp[rr][c] = v[rr];
-          scr(i, V_D + 2 * (3 * rr + c)) = v[rr].re;
-          scr(i, V_D + 2 * (3 * rr + c) + 1) = v[rr].im;
+          scr(i, V_D + 2 * (NC * rr + c)) = v[rr].re;
+          scr(i, V_D + 2 * (NC * rr + c) + 1) = v[rr].im;
         }
       }
     }
     // ---- back substitution, and the slots' Schur complement D - W^T X_U
-    cplx SM[2][2] = {{mk(L.tot[0] > 0.0 ? 0.0 : 1.0), mk(0.0)},
-                     {mk(0.0), mk(L.tot[1] > 0.0 ? 0.0 : 1.0)}};
-    cplx sr[2] = {mk(0.0), mk(0.0)};
+    // (the held slots, without ions, an identity row)
+    cplx SM[K][K], sr[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      sr[q] = mk(0.0);
+#pragma unroll
+      for (int c = 0; c < K; ++c) SM[q][c] = mk(q == c && !(L.tot[q] > 0.0) ? 1.0 : 0.0);
+    }
     {
-      cplx xn[5][3];
+      cplx xn[5][NC];
 #pragma unroll
       for (int rr = 0; rr < 5; ++rr)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) xn[rr][c] = mk(0.0);
+        for (int c = 0; c < NC; ++c) xn[rr][c] = mk(0.0);
       for (int i = NP; i >= 1; --i) {
-        cplx xi[5][3];
+        cplx xi[5][NC];
 #pragma unroll
         for (int rr = 0; rr < 5; ++rr)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            cplx s = mk(scr(i, V_D + 2 * (3 * rr + c)), scr(i, V_D + 2 * (3 * rr + c) + 1));
+          for (int c = 0; c < NC; ++c) {
+            cplx s = mk(scr(i, V_D + 2 * (NC * rr + c)), scr(i, V_D + 2 * (NC * rr + c) + 1));
 #pragma unroll
             for (int k = 0; k < 5; ++k)
               s = s - mk(scr(i, V_C + 2 * (5 * rr + k)), scr(i, V_C + 2 * (5 * rr + k) + 1)) *
@@ -906,40 +992,67 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
 #pragma unroll
         for (int rr = 0; rr < 5; ++rr)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
+          for (int c = 0; c < NC; ++c) {
             xn[rr][c] = xi[rr][c];
-            scr(i, V_D + 2 * (3 * rr + c)) = xi[rr][c].re;
-            scr(i, V_D + 2 * (3 * rr + c) + 1) = xi[rr][c].im;
+            scr(i, V_D + 2 * (NC * rr + c)) = xi[rr][c].re;
+            scr(i, V_D + 2 * (NC * rr + c) + 1) = xi[rr][c].im;
           }
-        const double w[2] = {r5(i, R_W3), r5(i, R_W4)};
+        // each slot's constraint row: its number in its points' ion logarithms
+        const Slots si = slots_at(L, i);
+        const int ja = si.a >= 0 ? si.a : -1, jc = si.c >= 0 ? L.ka + si.c : -1;
+        const double w3 = r5(i, R_W3), w4 = r5(i, R_W4);
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          if (w[k] == 0.0) continue;
-          sr[k] = sr[k] - w[k] * xi[3 + k][0];
-          SM[k][0] = SM[k][0] - w[k] * xi[3 + k][1];
-          SM[k][1] = SM[k][1] - w[k] * xi[3 + k][2];
+        for (int q = 0; q < K; ++q) {
+          const bool an = q == ja && w3 != 0.0, ca = q == jc && w4 != 0.0;
+          if (!an && !ca) continue;
+          const double w = an ? w3 : w4;
+          const int row = an ? 3 : 4;
+          sr[q] = sr[q] - w * (row == 3 ? xi[3][0] : xi[4][0]);
+#pragma unroll
+          for (int c = 0; c < K; ++c)
+            SM[q][c] = SM[q][c] - w * (row == 3 ? xi[3][1 + c] : xi[4][1 + c]);
+        }
+        // a region that reaches the contact beside this point: the contact's density in the
+        // number follows this point's potential, and V_int through the contact's (-dg)
+        if (i == 1 || i == NP) {
+          const int c = i == 1 ? 0 : NP + 1;
+          const Slots sc = slots_at(L, c);
+          const double dVc = i == 1 ? 0.5 * e : -0.5 * e;
+#pragma unroll
+          for (int sp = 0; sp < 2; ++sp) {
+            const int reg = sp == 0 ? sc.a : sc.c;
+            const double wv = r5(c, CT_WV + sp);
+            if (reg < 0 || wv == 0.0) continue;
+            const int qq = sp == 0 ? reg : L.ka + reg;
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+              if (q != qq) continue;
+              sr[q] = sr[q] - wv * xi[0][0] + mk(wv * dVc);
+#pragma unroll
+              for (int cc = 0; cc < K; ++cc) SM[q][cc] = SM[q][cc] - wv * xi[0][1 + cc];
+            }
+          }
         }
       }
     }
-    const cplx idet = mk(1.0) / (SM[0][0] * SM[1][1] - SM[0][1] * SM[1][0]);
-    const cplx z0 = (SM[1][1] * sr[0] - SM[0][1] * sr[1]) * idet;
-    const cplx z1 = (SM[0][0] * sr[1] - SM[1][0] * sr[0]) * idet;
+    csolve<K>(SM, sr);
     // dy = X_F - X_U z, written over X_F
     for (int i = 1; i <= NP; ++i)
 #pragma unroll
       for (int rr = 0; rr < 5; ++rr) {
-        const cplx xf = mk(scr(i, V_D + 2 * (3 * rr)), scr(i, V_D + 2 * (3 * rr) + 1));
-        const cplx x1 = mk(scr(i, V_D + 2 * (3 * rr + 1)), scr(i, V_D + 2 * (3 * rr + 1) + 1));
-        const cplx x2 = mk(scr(i, V_D + 2 * (3 * rr + 2)), scr(i, V_D + 2 * (3 * rr + 2) + 1));
-        const cplx dy = xf - (x1 * z0 + x2 * z1);
-        scr(i, V_D + 2 * (3 * rr)) = dy.re;
-        scr(i, V_D + 2 * (3 * rr) + 1) = dy.im;
+        cplx dy = mk(scr(i, V_D + 2 * (NC * rr)), scr(i, V_D + 2 * (NC * rr) + 1));
+#pragma unroll
+        for (int c = 0; c < K; ++c)
+          dy = dy - mk(scr(i, V_D + 2 * (NC * rr + 1 + c)), scr(i, V_D + 2 * (NC * rr + 1 + c) + 1)) *
+                        sr[c];
+        scr(i, V_D + 2 * (NC * rr)) = dy.re;
+        scr(i, V_D + 2 * (NC * rr) + 1) = dy.im;
       }
     // ---- the current's tangent: the carriers' and the displacement current as without ions,
     // then each ion region's (its base and per-dt parts)
     auto dyv = [&](int k, int c) -> cplx {
       if (k < 1 || k > NP) return mk(0.0);
-      return mk(scr(k, V_D + 2 * (3 * c)), scr(k, V_D + 2 * (3 * c) + 1));
+      return mk(scr(k, V_D + 2 * (NC * c)), scr(k, V_D + 2 * (NC * c) + 1));
     };
     auto dV = [&](int k) -> cplx {
       if (k == 0) return mk(0.5 * e);
@@ -954,18 +1067,33 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
     cplx sumJ_b[2] = {mk(0.0), mk(0.0)}, sumJ_t[2] = {mk(0.0), mk(0.0)};
     cplx duc_prev_b[2] = {mk(0.0), mk(0.0)}, duc_prev_t[2] = {mk(0.0), mk(0.0)};
     cplx dJD = mk(0.0);
-    // the ions, per region (one per species): sums over the region's intervals
-    double is_[2] = {0.0, 0.0}, iH[2] = {0.0, 0.0}, aev_f[2] = {0.0, 0.0}, aev_l[2] = {0.0, 0.0};
-    cplx dis[2] = {mk(0.0), mk(0.0)}, diu_i[2] = {mk(0.0), mk(0.0)}, ddbl_i[2] = {mk(0.0), mk(0.0)};
-    cplx dP_i[2] = {mk(0.0), mk(0.0)}, dsum_i[2] = {mk(0.0), mk(0.0)};
-    cplx daev_f[2] = {mk(0.0), mk(0.0)}, daev_l[2] = {mk(0.0), mk(0.0)};
-    int first_i[2] = {-1, -1};
+    // the ions, per region (slot; anion slots first): sums over the region's intervals. The
+    // current of a step (dti = 1) and the steady one (dti = 0) differ where a region reaches a
+    // contact: its density there `_ion_full`'s of each (R, B), and its change over the step from
+    // a density of 1 before it (`_full`'s masked contact) in the integrand (values `iu_v`,
+    // `dbl_v`)
+    double is_[K], iH[K], aevB_f[K], aevB_l[K], aevR_f[K], aevR_l[K], iu_v[K], dbl_v[K];
+    cplx dis[K], diu_i[K], ddbl_i[K], dP_i[K], dsum_i[K];
+    cplx daevB_f[K], daevB_l[K], daevR_f[K], daevR_l[K];
+    int first_i[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      is_[j] = 0.0; iH[j] = 0.0; aevB_f[j] = 0.0; aevB_l[j] = 0.0; aevR_f[j] = 0.0;
+      aevR_l[j] = 0.0; iu_v[j] = 0.0; dbl_v[j] = 0.0;
+      dis[j] = mk(0.0); diu_i[j] = mk(0.0); ddbl_i[j] = mk(0.0); dP_i[j] = mk(0.0);
+      dsum_i[j] = mk(0.0); daevB_f[j] = mk(0.0); daevB_l[j] = mk(0.0); daevR_f[j] = mk(0.0);
+      daevR_l[j] = mk(0.0);
+      first_i[j] = -1;
+    }
     double hsum = 0.0, dx_prev = 0.0, h_prev = 0.0;
     // `currDiffInt = 1`: each interval's Scharfetter-Gummel flux for the carriers and the ions
     // (jaxdd batch.py:366-369, 471-479), from the points at both ends of the interval
     const bool cdiff = L.sc(C_CURRDIFF) > 0.0;
-    cplx jd_prev[2] = {mk(0.0), mk(0.0)}, jdi_prev[2] = {mk(0.0), mk(0.0)};
-    cplx dsumd_i[2] = {mk(0.0), mk(0.0)};
+    cplx jd_prev[2] = {mk(0.0), mk(0.0)}, jdiB_prev[K], jdiR_prev[K], dsumdB_i[K], dsumdR_i[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      jdiB_prev[j] = mk(0.0); jdiR_prev[j] = mk(0.0); dsumdB_i[j] = mk(0.0); dsumdR_i[j] = mk(0.0);
+    }
     Pt Pa, Pb;
     if (cdiff) point(L, 0, Vint, Pa);
     for (int k = 0; k <= NP; ++k) {
@@ -1045,49 +1173,81 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       }
       const double epsk = W.x(k, tr::T_EPS);
       dJD = dJD + (hk * sign * epsk / (L.L * hk)) * (dV(k + 1) - dV(k));
-      // the ions over interval k (points k, k+1): `_ion_currents` linearised at U = 0
+      // the ions over interval k (points k, k+1): `_ion_currents` linearised at the state
       const Slots sa = slots_at(L, k), sb = slots_at(L, k + 1);
 #pragma unroll
-      for (int sp = 0; sp < 2; ++sp) {
-        if (!(L.tot[sp] > 0.0)) continue;
+      for (int j = 0; j < K; ++j) {
+        if (!(L.tot[j] > 0.0)) continue;
+        const int sp = j < L.ka ? 0 : 1, reg = sp == 0 ? j : j - L.ka;
         const double sn = sp == 0 ? -1.0 : 1.0;
-        const bool ina = (sp == 0 ? sa.a : sa.c) == 0, inb = (sp == 0 ? sb.a : sb.c) == 0;
+        const bool ina = (sp == 0 ? sa.a : sa.c) == reg, inb = (sp == 0 ? sb.a : sb.c) == reg;
+        if (!ina && !inb) continue;
         const int tf = sp == 0 ? tr::T_MUA : tr::T_MUC;
-        const double na = r5(k, sp == 0 ? R_NA : R_NC), nb = r5(k + 1, sp == 0 ? R_NA : R_NC);
         const double eva = r5(k, sp == 0 ? R_EVA : R_EVC), evb = r5(k + 1, sp == 0 ? R_EVA : R_EVC);
-        const cplx dlna = dyv(k, 3 + sp), dlnb = dyv(k + 1, 3 + sp);
         const cplx deva = (eva * sn / Vt) * dV(k), devb = (evb * sn / Vt) * dV(k + 1);
-        if (ina && first_i[sp] < 0) {
-          first_i[sp] = k;
-          aev_f[sp] = na * eva;
-          daev_f[sp] = (na * eva) * dlna + na * deva;
+        // each point's density and d ln(density), the step's (R) and the steady state's (B):
+        // a contact's from its neighbour's, an inner point's its own
+        double nBa, nRa, nBb, nRb;
+        cplx dBa, dRa, dBb, dRb;
+        auto end_point = [&](int pt, double& nB, double& nR, cplx& dB, cplx& dR) {
+          const int nbp = pt == 0 ? 1 : NP;
+          const cplx dl = dyv(nbp, 3 + sp), dv = dV(nbp) - dV(pt);
+          nB = exp(r5(pt, CT_LNB + sp));
+          nR = exp(r5(pt, CT_LNR + sp));
+          dB = dl + ((sp == 0 ? -1.0 : 1.0) / Vt) * dv;
+          dR = dl + r5(pt, CT_SR + sp) * dv;
+        };
+        if (k == 0) end_point(0, nBa, nRa, dBa, dRa);
+        else { nBa = nRa = r5(k, sp == 0 ? R_NA : R_NC); dBa = dRa = dyv(k, 3 + sp); }
+        if (k + 1 == NP + 1) end_point(NP + 1, nBb, nRb, dBb, dRb);
+        else { nBb = nRb = r5(k + 1, sp == 0 ? R_NA : R_NC); dBb = dRb = dyv(k + 1, 3 + sp); }
+        if (ina && first_i[j] < 0) {
+          first_i[j] = k;
+          aevB_f[j] = nBa * eva;
+          daevB_f[j] = (nBa * eva) * dBa + nBa * deva;
+          aevR_f[j] = nRa * eva;
+          daevR_f[j] = (nRa * eva) * dRa + nRa * deva;
         }
         if (inb) {
-          aev_l[sp] = nb * evb;
-          daev_l[sp] = (nb * evb) * dlnb + nb * devb;
+          aevB_l[j] = nBb * evb;
+          daevB_l[j] = (nBb * evb) * dBb + nBb * devb;
+          aevR_l[j] = nRb * evb;
+          daevR_l[j] = (nRb * evb) * dRb + nRb * devb;
         }
         if (cdiff) {  // the region's flux on interval k; across an interface the one before it
           double bf, bb, dbf, dbb;
           bern_pair(sn * (Pb.V - Pa.V) / Vt, L.simss, bf, bb, dbf, dbb);
           const cplx dxk = (sn / Vt) * (dV(k + 1) - dV(k));
-          const cplx djd = (sn * Q * W.x(k, tf) * Vt / (L.L * hk)) *
-                           (nb * (bb * dlnb - dbb * dxk) - na * (bf * dlna + dbf * dxk));
-          if (ina && inb) dsumd_i[sp] = dsumd_i[sp] + hk * (iface_k ? jdi_prev[sp] : djd);
-          jdi_prev[sp] = djd;
+          const double pre = sn * Q * W.x(k, tf) * Vt / (L.L * hk);
+          const cplx jB = pre * ((nBb * bb) * dBb - (nBb * dbb) * dxk - (nBa * bf) * dBa -
+                                 (nBa * dbf) * dxk);
+          const cplx jR = pre * ((nRb * bb) * dRb - (nRb * dbb) * dxk - (nRa * bf) * dRa -
+                                 (nRa * dbf) * dxk);
+          if (ina && inb) {
+            dsumdB_i[j] = dsumdB_i[j] + hk * (iface_k ? jdiB_prev[j] : jB);
+            dsumdR_i[j] = dsumdR_i[j] + hk * (iface_k ? jdiR_prev[j] : jR);
+          }
+          jdiB_prev[j] = jB;
+          jdiR_prev[j] = jR;
         }
         if (ina && inb) {
           const double mua = W.x(k, tf), mub = W.x(k + 1, tf);
           const double ia = 1.0 / (mua > 0.0 ? mua : 1.0), ib = 1.0 / (mub > 0.0 ? mub : 1.0);
-          const cplx dUa = na * dlna, dUb = nb * dlnb;  // per unit of dti
-          const cplx diu_b2 = diu_i[sp] + (0.5 * dx) * (dUa + dUb);
-          is_[sp] += 0.5 * dx * (eva * ia + evb * ib);
-          dis[sp] = dis[sp] + (0.5 * dx) * (ia * deva + ib * devb);
-          ddbl_i[sp] = ddbl_i[sp] + (0.5 * dx * eva * ia) * diu_i[sp] + (0.5 * dx * evb * ib) * diu_b2;
-          diu_i[sp] = diu_b2;
-          const cplx dstep = k > first_i[sp] ? (sn * Q * L.L * width) * dUa : mk(0.0);
-          dP_i[sp] = dP_i[sp] + dstep;
-          iH[sp] += hk;
-          dsum_i[sp] = dsum_i[sp] + hk * (iface_k ? dP_i[sp] - dstep : dP_i[sp]);
+          const cplx dUa = nRa * dRa, dUb = nRb * dRb;  // per unit of dti
+          const double Uva = k == 0 ? nRa - 1.0 : 0.0, Uvb = k + 1 == NP + 1 ? nRb - 1.0 : 0.0;
+          const cplx diu_b2 = diu_i[j] + (0.5 * dx) * (dUa + dUb);
+          const double iu_b2 = iu_v[j] + 0.5 * dx * (Uva + Uvb);
+          is_[j] += 0.5 * dx * (eva * ia + evb * ib);
+          dis[j] = dis[j] + (0.5 * dx) * (ia * deva + ib * devb);
+          dbl_v[j] += 0.5 * dx * (eva * ia * iu_v[j] + evb * ib * iu_b2);
+          ddbl_i[j] = ddbl_i[j] + (0.5 * dx * eva * ia) * diu_i[j] + (0.5 * dx * evb * ib) * diu_b2 +
+                      (0.5 * dx * ia * iu_v[j]) * deva + (0.5 * dx * ib * iu_b2) * devb;
+          diu_i[j] = diu_b2;
+          iu_v[j] = iu_b2;
+          const cplx dstep = k > first_i[j] ? (sn * Q * L.L * width) * dUa : mk(0.0);
+          dP_i[j] = dP_i[j] + dstep;
+          iH[j] += hk;
+          dsum_i[j] = dsum_i[j] + hk * (iface_k ? dP_i[j] - dstep : dP_i[j]);
         }
       }
       dx_prev = dx;
@@ -1098,7 +1258,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
       const double sn = c == 0 ? -1.0 : 1.0;
-      const double sgl = a.lsc[(size_t)(L_SN + c) * a.Bp + l], K = a.lsc[(size_t)(L_KN + c) * a.Bp + l];
+      const double sgl = a.lsc[(size_t)(L_SN + c) * a.Bp + l], Kc = a.lsc[(size_t)(L_KN + c) * a.Bp + l];
       Pt P0, PR;
       point(L, 0, Vint, P0);
       point(L, NP + 1, Vint, PR);
@@ -1106,7 +1266,7 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       const double e0 = exp(sn * ((c == 0 ? P0.offn : P0.offp) + P0.V) / Vt);
       const double eR = exp(sn * ((c == 0 ? PR.offn : PR.offp) + PR.V) / Vt);
       const cplx dBc = (Vt * sn) * ((dR * eR * sn / Vt) * dV(NP + 1) - (d0 * e0 * sn / Vt) * dV(0));
-      const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (K / sgl) * dsgl[c];
+      const cplx dK_b = (1.0 / sgl) * (dBc - sn * ddb_b[c]) - (Kc / sgl) * dsgl[c];
       const cplx dK_t = (-sn / sgl) * ddb_t[c];
       if (!cdiff) {  // the differential current has no K
         Yb = Yb + sign * (Q * hsum) * dK_b;
@@ -1116,19 +1276,23 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       Yt = Yt + sign * sumJ_t[c];
     }
 #pragma unroll
-    for (int sp = 0; sp < 2; ++sp) {
-      if (!(L.tot[sp] > 0.0) || first_i[sp] < 0) continue;
-      if (cdiff) {
-        Yb = Yb + sign * dsumd_i[sp];
+    for (int j = 0; j < K; ++j) {
+      if (!(L.tot[j] > 0.0) || first_i[j] < 0) continue;
+      if (cdiff) {  // the steady state's fluxes, and the step's less them per unit of dti
+        Yb = Yb + sign * dsumdB_i[j];
+        Yt = Yt + sign * (dsumdR_i[j] - dsumdB_i[j]);
         continue;
       }
-      const double sn = sp == 0 ? -1.0 : 1.0;
-      const double sgl = is_[sp] > 0.0 ? is_[sp] : 1.0;
-      const double K0 = Vt * sn * (aev_l[sp] - aev_f[sp]) / sgl;  // the state's (U = 0)
-      const cplx dK_b = (Vt * sn / sgl) * (daev_l[sp] - daev_f[sp]) - (K0 / sgl) * dis[sp];
-      const cplx dK_t = (-sn / sgl) * ddbl_i[sp];
-      Yb = Yb + sign * (Q * iH[sp]) * dK_b;
-      Yt = Yt + sign * ((Q * iH[sp]) * dK_t + dsum_i[sp]);
+      const double sn = j < L.ka ? -1.0 : 1.0;
+      const double sgl = is_[j] > 0.0 ? is_[j] : 1.0;
+      // K at dti = 0 (the steady state's) and at dti = 1, and their tangents
+      const double K0 = Vt * sn * (aevB_l[j] - aevB_f[j]) / sgl;
+      const double K1 = (Vt * sn * (aevR_l[j] - aevR_f[j]) - sn * dbl_v[j]) / sgl;
+      const cplx dK0 = (Vt * sn / sgl) * (daevB_l[j] - daevB_f[j]) - (K0 / sgl) * dis[j];
+      const cplx dK1 = (1.0 / sgl) * ((Vt * sn) * (daevR_l[j] - daevR_f[j]) - sn * ddbl_i[j]) -
+                       (K1 / sgl) * dis[j];
+      Yb = Yb + sign * (Q * iH[j]) * dK0;
+      Yt = Yt + sign * ((Q * iH[j]) * (dK1 - dK0) + dsum_i[j]);
     }
     Yt = Yt + dJD;
     const cplx Y = (1.0 / hsum) * (Yb + lap * Yt);
@@ -1203,8 +1367,10 @@ int dd_admittance_ions_workspace_bytes(const dd_batch* batch, int n_freq, size_t
   const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
   long T = (long)Bp * n_freq;
   if (T > imp_ion_threads()) T = imp_ion_threads();
+  const int K = batch->k_anion + batch->k_cation;
+  if (batch->k_anion < 1 || batch->k_cation < 1 || K > dd::DD_MAXK) return DD_ERR_ARGS;
   *bytes = (nodes * dd::imp::P_WORDS * Bp + dd::imp::L_WORDS * Bp +
-            nodes * dd::imp::R5_WORDS * Bp + nodes * dd::imp::V_WORDS * (size_t)T) *
+            nodes * dd::imp::R5_WORDS * Bp + nodes * dd::imp::vwords(K) * (size_t)T) *
            sizeof(double);
   return DD_OK;
 }
@@ -1221,11 +1387,12 @@ int dd_admittance_ions(const dd_batch* batch, const double* state, const double*
     return DD_ERR_ARGS;
   if (bernoulli != DD_BERNOULLI_EXACT && bernoulli != DD_BERNOULLI_SIMSS) return DD_ERR_ARGS;
   size_t need;
-  dd_admittance_ions_workspace_bytes(batch, n_freq, &need);
+  if (dd_admittance_ions_workspace_bytes(batch, n_freq, &need) != DD_OK) return DD_ERR_ARGS;
   if (workspace_bytes < need) return DD_ERR_WORKSPACE;
   const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
   dd::imp::Args a{};
   a.B = batch->n_lanes; a.Bp = batch->lane_stride; a.npmax = batch->np_max; a.ka = batch->k_anion;
+  a.K = batch->k_anion + batch->k_cation;
   a.simss = bernoulli == DD_BERNOULLI_SIMSS; a.nf = n_freq;
   if (dt < 0.0) return DD_ERR_ARGS;
   a.dt = dt;
@@ -1247,12 +1414,21 @@ int dd_admittance_ions(const dd_batch* batch, const double* state, const double*
   if (st != DD_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   st = dd::launch(dd::imp::prepare_kernel, dim3((unsigned)((Bp + 63) / 64)), dim3(64), 0, s, a);
-  if (st == DD_OK)
-    st = dd::launch(dd::imp::prepare_ions_kernel, dim3((unsigned)((Bp + 31) / 32)), dim3(32), 0,
-                    s, a, b);
-  if (st == DD_OK)
-    st = dd::launch(dd::imp::admittance_ions_kernel, dim3((unsigned)((T + 63) / 64)), dim3(64),
-                    0, s, a, b);
+  if (st != DD_OK) return st;
+  const dim3 gp((unsigned)((Bp + 31) / 32)), ga((unsigned)((T + 63) / 64));
+  switch (a.K) {  // the slots: one region of each species, or several
+    case 2:
+      st = dd::launch(dd::imp::prepare_ions_kernel<2>, gp, dim3(32), 0, s, a, b);
+      if (st == DD_OK) st = dd::launch(dd::imp::admittance_ions_kernel<2>, ga, dim3(64), 0, s, a, b);
+      break;
+    case 3:
+      st = dd::launch(dd::imp::prepare_ions_kernel<3>, gp, dim3(32), 0, s, a, b);
+      if (st == DD_OK) st = dd::launch(dd::imp::admittance_ions_kernel<3>, ga, dim3(64), 0, s, a, b);
+      break;
+    default:
+      st = dd::launch(dd::imp::prepare_ions_kernel<4>, gp, dim3(32), 0, s, a, b);
+      if (st == DD_OK) st = dd::launch(dd::imp::admittance_ions_kernel<4>, ga, dim3(64), 0, s, a, b);
+  }
   return st;
 }
 

@@ -117,9 +117,9 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
     """The impedance of a batch at the internal voltage `voltage` (V) at each of `frequencies`
     (Hz), from the steady state there by one complex linear solve per frequency (jaxdd
     impedance.py:365-409). Free mobile ions move with the voltage as unknowns of their own.
-    Refused (`NotImplementedError`), as the reference refuses them or as this build does not
-    carry them: ions frozen at a pre-bias, several ion regions of a species, an ion region that
-    reaches a contact. With the differential current (`currDiffInt = 1`) the current's tangent is
+    Several ion regions of a species each keep their own number; a region that reaches a contact
+    takes the contact's ions from its neighbour's (jaxdd's `_ion_full`). Refused
+    (`NotImplementedError`), as the reference refuses them: ions frozen at a pre-bias. With the differential current (`currDiffInt = 1`) the current's tangent is
     each interval's Scharfetter–Gummel flux's, the ions' too. `dt` (s): instead of the continuous
     response, what
     `solve_transient` sees through implicit Euler at steps of `dt` (its time terms at
@@ -127,11 +127,6 @@ def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float 
     devs = batch["devices"]
     if _mobile(batch) and any(d.pre_cond and d.fix_ions for d in devs):
         raise NotImplementedError("impedance with ions frozen at a pre-bias")
-    if batch["ka"] != 1 or batch["kc"] != 1:
-        raise NotImplementedError("impedance with several ion regions of a species")
-    from .transient import reaches_contact
-    if _mobile(batch) and any(reaches_contact(d) for d in devs):
-        raise NotImplementedError("impedance with an ion region that reaches a contact")
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
     if dt is not None and not dt > 0:
         raise ValueError(f"dt must be positive, got {dt}")

@@ -20,6 +20,8 @@ written for complex inputs and is analytic in them), exact to round-off.
 
 from __future__ import annotations
 
+import warnings
+
 import numpy as np
 
 from jaxdd_b200.constants import Q
@@ -295,8 +297,17 @@ def admittance_ions(d, full0, Vint, laps, bern, dt=None):
     _, A, Bb, C, U, M = transient.assemble(full0[None], d, tr, logs, bern, steady_traps=True,
                                            mass=True)
     A, Bb, C, U, M = A[0], Bb[0], C[0], U[0], M[0]
-    _, W, D = transient.constraints(full0[None], logs, ion)
+    # each slot's number, the contacts' ions from their neighbours where a region reaches one
+    # (`_ion_full` at the step's dti = 1): its derivatives in the interior unknowns, W, and in
+    # V_int (through the contacts' potentials), dg, by complex step
+    full1, dVc = transient.ion_full(d, full0[None], bern, np.array([1.0]))
+    _, W, D = transient.constraints(full1, logs, ion, dVc)
     W, D = W[0], D[0]
+    g_of = transient.full_of(d, y[None].astype(complex), np.array([Vint + 1j * 1e-30]), bern,
+                             np.array([1.0]))
+    with warnings.catch_warnings():  # W of a complex state, unused, cast to real
+        warnings.simplefilter("ignore", np.exceptions.ComplexWarning)
+        dg = np.imag(transient.constraints(g_of, logs, ion)[0][0]) / 1e-30
     e = d["left_elec"][0]
     dF = np.zeros((NP, 5))
     dF[0] += A[0][:, 0] * 0.5 * e
@@ -307,10 +318,10 @@ def admittance_ions(d, full0, Vint, laps, bern, dt=None):
            "V": full0[None, :, 0]}
     h_cs = 1e-30
 
-    def total(y_, V_, dti, dU=None, dRi=None):
+    def total(y_, V_, dti, dU=None, dRi=None):  # the contacts' ions `_ion_full`'s at dti
         t = dict(tr0, dti=np.array([dti]))
-        return transient.current(d, transient.full_of(d, y_[None], np.array([V_])), t, bern,
-                                 False, steady_traps=True, dU=dU, dRi=dRi)[0]
+        full = transient.full_of(d, y_[None], np.array([V_]), bern, np.array([dti]))
+        return transient.current(d, full, t, bern, False, steady_traps=True, dU=dU, dRi=dRi)[0]
 
     def linear(dy_real, dV, dti):  # J_y dy + J_V dV at dti, by complex step
         return np.imag(total(y + 1j * h_cs * dy_real, Vint + 1j * h_cs * dV, dti)) / h_cs
@@ -336,7 +347,7 @@ def admittance_ions(d, full0, Vint, laps, bern, dt=None):
         X = transient.block_thomas(Al[None], Bl[None], Cl[None], rhs[None])[0]
         XF, XU = X[..., 0], X[..., 1:]
         schur = D - np.einsum("kir,irl->kl", W, XU)
-        z = np.linalg.solve(schur, -np.einsum("kir,ir->k", W, XF))
+        z = np.linalg.solve(schur, -dg - np.einsum("kir,ir->k", W, XF))
         dy = XF - XU @ z
         J0 = linear(dy.real, 1.0, 0.0) + 1j * linear(dy.imag, 0.0, 0.0)
         J1 = linear(dy.real, 1.0, 1.0) + 1j * linear(dy.imag, 0.0, 1.0)
@@ -371,9 +382,6 @@ def solve_impedance(devices, frequencies, voltage=0.0, tol=1e-10, max_iter=60,
         ions = np.any(d["ion"]["a_totals"] > 0) or np.any(d["ion"]["c_totals"] > 0)
         if ions and dev.pre_cond and dev.fix_ions:
             raise NotImplementedError("impedance with ions frozen at a pre-bias")
-        masks, _ = dd._masks(d["ion"])
-        if ions and (np.any(masks[:, :, 0] > 0) or np.any(masks[:, :, -1] > 0)):
-            raise NotImplementedError("impedance with an ion region that reaches a contact")
         st = dd.solve_states(d, [float(voltage)], tol=tol, max_iter=max_iter,
                              bernoulli_name=bernoulli_name)
         full0 = np.stack([st["V"][0, 0], np.log(st["n"][0, 0]), np.log(st["p"][0, 0])], -1)

@@ -650,7 +650,8 @@ def ion_full(d, full, bern, dti):
     interval (`ln a_0 = ln a_1 + ln(B(x)/B(-x))`, x = (V_1 - V_0)/V_T, the cations' the other
     way; Boltzmann's, the ratio -x, in the steady state `dti = 0`), 0 elsewhere. Returns the
     full state and each contact's ln a, ln c derivative in its neighbour's potential
-    (B×2×2: left, right × anion, cation)."""
+    (B×2×2: left, right × anion, cation; 0 for a complex `full`, whose contacts' values are
+    continued analytically for complex-step derivatives)."""
     ion = d["ion"]
     Vt = d["Vt"]
     ma, mc = ion["a_slots"].sum(1), ion["c_slots"].sum(1)
@@ -658,6 +659,10 @@ def ion_full(d, full, bern, dti):
     moving = np.asarray(dti, dtype=float) > 0
 
     def ratio(x):
+        if np.iscomplexobj(x):  # complex-step derivatives: the value alone, continued
+            simss = bern is dd.bern_simss
+            r = np.log(dd.bern_complex(x, simss)) - np.log(dd.bern_complex(-x, simss))
+            return np.where(moving, r, -x), np.zeros(x.shape)
         Bf, dBf = bern(x)
         Bb, dBb = bern(-x)
         with np.errstate(divide="ignore", invalid="ignore"):

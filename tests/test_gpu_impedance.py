@@ -184,3 +184,48 @@ def test_the_dt_form_is_the_gpu_transients_response(case):
     assert abs(r.Y[0, 0] / Yt - 1) < bar
     Yo = imp.solve_impedance([dev], [f], voltage=V0, tol=1e-12, max_iter=200, dt=dt)[0][0, 0]
     assert abs(r.Y[0, 0] / Yo - 1) < 1e-6
+
+
+@pytest.mark.parametrize("differential", [False, True])
+def test_two_ion_regions_of_each_species_match_the_oracle(differential):
+    """`dd_admittance_ions` with four slots (two regions of each species, each its own column of
+    the border and its own current), beside two one-region mobile-ion stacks and the p-i-n cell
+    without ions in the same launch, with the integral and the differential current, against the
+    oracle to 1e-6."""
+    from jaxdd_b200.workloads import SEED_ION_STACKS
+    from tests.test_impedance_oracle import two_region_texts
+    texts = [two_region_texts(100), two_region_texts(100, "1e-9")]
+    texts += [drawn_texts(k, np.random.default_rng([SEED_ION_STACKS, k]), 100) for k in (1, 3)]
+    texts.append(pin_texts(100))
+    devs = [build_device(setup_from_texts(_differential(t) if differential else t))
+            for t in texts]
+    b = prepare(devs)
+    assert b["ka"] == 2 and b["kc"] == 2
+    r = solve_impedance(b, F, voltage=0.8)
+    Yo, Zo, Jo, oko = imp.solve_impedance(devs, F, voltage=0.8)
+    assert np.array_equal(r.converged, oko) and r.converged.all()
+    rel = np.abs(r.Y - Yo) / np.abs(Yo)
+    assert np.max(rel) < 1e-6, rel
+
+
+@pytest.mark.parametrize("bernoulli_name", ["exact", "simss"])
+@pytest.mark.parametrize("differential", [False, True])
+def test_ion_regions_at_a_contact_match_the_oracle(bernoulli_name, differential):
+    """Ion regions that reach a contact: a region of two layers at the left contact (two slots)
+    and two regions of each species at both contacts (four), in one launch each, the contact's
+    ions from its neighbour's in each region's number (its derivatives in the neighbour's
+    potential and, through the contact's, in V_int) and in the current (the step's and the
+    steady state's forms, jaxdd's density of 1 before the step there), with the integral and the
+    differential current and both Bernoulli functions, against the oracle to 1e-6."""
+    from tests.test_impedance_oracle import contact_texts
+    for case in ("zimt_region_slow_light", "two_regions_light"):
+        texts = contact_texts(case, 200)
+        devs = [build_device(setup_from_texts(_differential(texts) if differential else texts),
+                             grid="simss")]
+        assert devs[0].anion_mask[0]
+        r = solve_impedance(prepare(devs), F, voltage=0.5, bernoulli_name=bernoulli_name)
+        Yo, Zo, Jo, oko = imp.solve_impedance(devs, F, voltage=0.5,
+                                              bernoulli_name=bernoulli_name)
+        assert np.array_equal(r.converged, oko) and r.converged.all()
+        rel = np.abs(r.Y - Yo) / np.abs(Yo)
+        assert np.max(rel) < 1e-6, (case, rel)

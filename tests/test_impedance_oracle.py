@@ -103,18 +103,58 @@ def test_with_ions_frozen_at_a_pre_bias_refused():
         imp.solve_impedance([dev], [1e3], voltage=0.5)
 
 
-def test_with_an_ion_region_that_reaches_a_contact_refused():
-    """The impedance's ions are carried for regions inside the device only: a region that
-    reaches a contact is refused by the oracle and by `solve_impedance` before any solve (the
-    transient, `solve_transient`, takes it)."""
-    from jaxdd_b200.batch import prepare
-    from jaxdd_b200.impedance import solve_impedance
-    from tests.test_transient_oracle import zimt_case
-    dev = build_device(zimt_case("zimt_region_slow_light")[0], grid="simss")
-    with pytest.raises(NotImplementedError, match="reaches a contact"):
-        imp.solve_impedance([dev], [1e3], voltage=0.5)
-    with pytest.raises(NotImplementedError, match="reaches a contact"):
-        solve_impedance(prepare([dev]), [1e3], voltage=0.5)
+def contact_texts(case, NP=None, mu=None):
+    """The input texts of a golden case (tests/golden/inputs), with `NP` points and the ions'
+    mobility `mu` (m²/Vs) where given."""
+    import re
+    from tests.test_transient_oracle import INPUTS
+    texts = {f.name: f.read_text() for f in (INPUTS / case).iterdir() if f.suffix == ".txt"}
+    for name in texts:
+        if name.startswith("L") and mu is not None:
+            texts[name] = re.sub(r"^(mu_anion|mu_cation)\s*=\s*[0-9.eE+-]+",
+                                 lambda m: f"{m.group(1)} = {mu}", texts[name], flags=re.M)
+    if NP is not None:
+        texts["simulation_setup.txt"] = re.sub(r"^NP\s*=\s*\d+", f"NP = {NP}",
+                                               texts["simulation_setup.txt"], flags=re.M)
+    return texts
+
+
+@pytest.mark.parametrize("case", ["zimt_region_slow_light", "two_regions_light"])
+def test_ion_regions_that_reach_a_contact(case):
+    """Ion regions that reach a contact (a region of two layers at the left contact; two regions
+    of each species, one at each contact): the contact's ions from its neighbour's
+    (`_ion_full`: at the step's dti = 1 in each region's number, whose derivative in V_int
+    through the contact's potential joins the border's right-hand side, Boltzmann's in the
+    current at dti = 0). At 1e-7 Hz the steady slope (1e-5, the reference's bar with ions;
+    measured 9e-10). Far above every relaxation the capacitance is not the geometric one: the
+    contact's ions follow the potential at once (their neighbour's density through the potential
+    step), so keeping each region's number moves its inner ions (6e-4 and 3e-4 below it here)."""
+    dev = build_device(setup_from_texts(contact_texts(case)), grid="simss")
+    assert dev.anion_mask[0] and dev.cation_mask[0]
+    V0, dV = 0.5, 1e-5
+    Y, _, _, ok = imp.solve_impedance([dev], [1e-7, 1e14], voltage=V0, tol=1e-12, max_iter=200)
+    st = dd.solve_states(dd.prepare([dev]), [V0 - dV, V0 + dV], tol=1e-12, max_iter=200)
+    slope = (st["J"][0, 1] - st["J"][0, 0]) / (2 * dV)
+    assert ok.all()
+    assert Y[0, 0].real == pytest.approx(slope, rel=1e-5)
+    x, eps = np.asarray(dev.x), np.asarray(dev.eps)
+    geometric = 1.0 / np.sum(np.diff(x) * 0.5 * (1 / eps[:-1] + 1 / eps[1:]))
+    assert 1e-4 < 1 - Y[0, 1].imag / (2 * np.pi * 1e14) / geometric < 1e-3
+
+
+def test_ion_regions_at_both_contacts_against_the_transient():
+    """With `dt`, two regions of each species reaching both contacts, the ions at 1e-9 m²/Vs,
+    against the oracle transient's response to a 10 µV sine at 100 kHz. jaxdd's `_admittance`
+    takes the contact's ions before the step as a density of 1 (`_full`'s masked contact), so its
+    linearised current keeps a term of the contact's density that the transient, whose contact
+    before a step is the last step's, has not: 6.5e-6 between the two (the bar 1e-5); with the
+    contact's own density before the step they agree to 4.5e-9. This build follows jaxdd."""
+    dev = build_device(setup_from_texts(contact_texts("two_regions_light", 60, "1e-9")),
+                       grid="simss")
+    assert dev.anion_mask[0] and dev.anion_mask[-1]
+    Yt, dt = _sine_response(dev, 0.5, 1e5, amp=1e-5)
+    Yd = imp.solve_impedance([dev], [1e5], voltage=0.5, tol=1e-12, max_iter=200, dt=dt)[0][0, 0]
+    assert 1e-6 < abs(Yd / Yt - 1) < 1e-5
 
 
 def test_the_transients_gradients_refuse_an_ion_region_that_reaches_a_contact():
@@ -227,3 +267,48 @@ def test_the_differential_current_dt_form_is_the_transients_response(case):
     Yt, dt = _sine_response(dev, V0, f, amp=amp, periods=periods)
     Yd = imp.solve_impedance([dev], [f], voltage=V0, tol=1e-12, max_iter=200, dt=dt)[0][0, 0]
     assert abs(Yd / Yt - 1) < bar
+
+
+def two_region_texts(NP=100, mu="1e-12"):
+    """A five-layer stack with two ion regions of each species inside it: HTL 20 nm / absorber
+    200 nm (anions and cations 1e23 m^-3) / spacer 20 nm without ions / absorber 250 nm (anions
+    3e22, cations 5e22 m^-3) / ETL 30 nm, the ions' mobility `mu` (m²/Vs)."""
+    from jaxdd_b200.workloads import _layer, _setup
+    setup = _setup(NP).replace("l3 = L3.txt\n", "l3 = L3.txt\nl4 = L4.txt\nl5 = L5.txt\n")
+    absorber = dict(eps_r="24", E_c="4.0", E_v="5.6", mu_n="1e-4", mu_p="1e-4",
+                    N_t_bulk="1e20", E_t_bulk="4.8", k_direct="1e-17", G_ehp="2.5e27",
+                    layerGen="1", mu_anion=mu, mu_cation=mu, ionsMayEnter="1")
+    return {"simulation_setup.txt": setup,
+            "L1.txt": _layer(L="20e-9", eps_r="3.5", E_c="2.6", E_v="5.6", mu_n="1e-6",
+                             mu_p="1e-6", N_A="1e22"),
+            "L2.txt": _layer(L="200e-9", N_anion="1e23", N_cation="1e23", **absorber),
+            "L3.txt": _layer(L="20e-9", eps_r="24", E_c="4.0", E_v="5.6", mu_n="1e-4",
+                             mu_p="1e-4"),
+            "L4.txt": _layer(L="250e-9", N_anion="3e22", N_cation="5e22", **absorber),
+            "L5.txt": _layer(L="30e-9", eps_r="10", E_c="4.0", E_v="7.2", mu_n="1e-5",
+                             mu_p="1e-5", N_D="1e22")}
+
+
+def test_two_ion_regions_of_each_species():
+    """Several ion regions of a species (jaxdd's `_admittance` with a slot per region, its
+    border keeping each region's number): at 1e-7 Hz the steady slope with the ions moving
+    (1e-5, the reference's bar with ions; measured 1.5e-9), far above every relaxation the
+    geometric capacitance, and with `dt` the oracle transient's response to a 0.1 mV sine at
+    1 kHz, the ions at 1e-9 m²/Vs (1e-6; measured 3.5e-9)."""
+    dev = build_device(setup_from_texts(two_region_texts()))
+    b = dd.prepare([dev])
+    assert b["ion"]["a_slots"].shape[1] == 2 and b["ion"]["c_slots"].shape[1] == 2
+    assert not (dev.anion_mask[0] or dev.anion_mask[-1])
+    V0, dV = 0.8, 1e-5
+    Y, _, _, ok = imp.solve_impedance([dev], [1e-7, 1e14], voltage=V0, tol=1e-12, max_iter=200)
+    st = dd.solve_states(b, [V0 - dV, V0 + dV], tol=1e-12, max_iter=200)
+    slope = (st["J"][0, 1] - st["J"][0, 0]) / (2 * dV)
+    assert ok.all()
+    assert Y[0, 0].real == pytest.approx(slope, rel=1e-5)
+    x, eps = np.asarray(dev.x), np.asarray(dev.eps)
+    geometric = 1.0 / np.sum(np.diff(x) * 0.5 * (1 / eps[:-1] + 1 / eps[1:]))
+    assert Y[0, 1].imag / (2 * np.pi * 1e14) == pytest.approx(geometric, rel=1e-4)
+    dev = build_device(setup_from_texts(two_region_texts(60, "1e-9")))
+    Yt, dt = _sine_response(dev, 0.8, 1e3)
+    Yd = imp.solve_impedance([dev], [1e3], voltage=0.8, tol=1e-12, max_iter=200, dt=dt)[0][0, 0]
+    assert abs(Yd / Yt - 1) < 1e-6
