@@ -68,15 +68,16 @@ __device__ __forceinline__ void load_point(const View& W, int buf, int k, double
 // neighbour in buffer `buf`, so that nothing flows over the contact's interval,
 // ln a_0 = ln a_1 + ln(B(x)/B(-x)) with x = (V_1 - V_0)/V_T (the cations' the other way, the right
 // contact's mirrored), Boltzmann's (the ratio -x) in the steady state dti = 0. `dr`, if given:
-// d ln a / d V of the neighbour (the cations' its negative). A no-op on interior points and
-// where no region reaches the contact.
+// d ln a / d V of the neighbour (the cations' its negative). `nbp`, if given: the neighbour's
+// point itself (a state along a tangent) instead of buffer `buf`'s. A no-op on interior points
+// and where no region reaches the contact.
 __device__ __forceinline__ void contact_ions(const View& W, int buf, int k, double dti, TP& P,
-                                             double* dr = nullptr) {
+                                             double* dr = nullptr, const TP* nbp = nullptr) {
   const Lane& L = W.L;
   if ((k != 0 && k != L.NP + 1) || (P.c.sl.a < 0 && P.c.sl.c < 0)) return;
   const bool right = k != 0;
   const int nb = right ? L.NP : 1;
-  const double Vn = *W.y(buf, nb, 0);
+  const double Vn = nbp ? nbp->c.V : *W.y(buf, nb, 0);
   const double x = (right ? P.c.V - Vn : Vn - P.c.V) * L.iVt;
   double r = -x, drx = -1.0;
   if (dti > 0.0) {
@@ -88,12 +89,12 @@ __device__ __forceinline__ void contact_ions(const View& W, int buf, int k, doub
   const double s = right ? -1.0 : 1.0;  // the step from the neighbour, anions
   if (dr) *dr = drx * L.iVt;  // on either side r'(x) / V_T
   if (P.c.sl.a >= 0) {
-    P.la = *W.y(buf, nb, 3) + s * r;
+    P.la = (nbp ? nbp->la : *W.y(buf, nb, 3)) + s * r;
     P.a = exp(P.la);
     P.c.da = P.a;
   }
   if (P.c.sl.c >= 0) {
-    P.lc = *W.y(buf, nb, 4) - s * r;
+    P.lc = (nbp ? nbp->lc : *W.y(buf, nb, 4)) - s * r;
     P.c2 = exp(P.lc);
     P.c.dc = P.c2;
   }

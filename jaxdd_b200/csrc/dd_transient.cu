@@ -178,9 +178,17 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     return PERT && pt->tfi ? FI[o] + pt->h * pt->tfi[o] : FI[o];
   };
   auto load_c = [&](int buf, int k, double Vi, TP& P, bool is_cur) {
-    if (PERT) load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P,
-                        is_cur ? pt->tn : 5, is_cur ? pt->tf : 1);
-    else if (is_cur) load_point(W, buf, k, Vi, P);
+    if (PERT) {
+      load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P, is_cur ? pt->tn : 5,
+                is_cur ? pt->tf : 1);
+      if (k == 0 || k == L.NP + 1) {  // a contact's ions follow its neighbour along the tangent
+        TP nbp;
+        load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k == 0 ? 1 : L.NP, Vi, nbp,
+                  is_cur ? pt->tn : 5, is_cur ? pt->tf : 1);
+        contact_ions(W, buf, k, is_cur ? dti : dti_bef, P, nullptr, &nbp);
+        return;
+      }
+    } else if (is_cur) load_point(W, buf, k, Vi, P);
     else load_before(W, buf, k, Vi, P);
     contact_ions(W, buf, k, is_cur ? dti : dti_bef, P);
   };
@@ -652,10 +660,22 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
   TP pm, pc, pn;
   load_point(W, bn, 0, V_k, pm);
   load_point(W, bn, 1, V_k, pc);
+  // a region that reaches a contact: the contact's ions from its neighbour's (their share of the
+  // region's number; d ln a / d V of the neighbour in dr_c)
+  double dr_c[2] = {0.0, 0.0};
+  contact_ions(W, bn, 0, dti, pm, &dr_c[0]);
   Flux el, er;
   flux(L, pm.c, pc.c, L.st(0, S_MUN), L.st(0, S_MUP), el);
+  double lnc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};  // [side][species]: the contacts' ln density
+  lnc[0][0] = pm.la;
+  lnc[0][1] = pm.lc;
   for (int i = 1; i <= NP; ++i) {
     load_point(W, bn, i + 1, V_k, pn);
+    if (i == NP) {
+      contact_ions(W, bn, NP + 1, dti, pn, &dr_c[1]);
+      lnc[1][0] = pn.la;
+      lnc[1][1] = pn.lc;
+    }
     flux(L, pc.c, pn.c, L.st(i, S_MUN), L.st(i, S_MUP), er);
     const double hm = L.st(i - 1, S_H), hp = L.st(i, S_H);
     const int ifm = (int)L.st(i - 1, S_IFK), ifi = (int)L.st(i, S_IFK);
@@ -673,6 +693,12 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
       if (pc.c.sl.a >= 0 && pc.c.sl.a == pm.c.sl.a) gnum[pc.c.sl.a] += 0.5 * (pm.a + pc.a) * hL;
       if (pc.c.sl.c >= 0 && pc.c.sl.c == pm.c.sl.c)
         gnum[L.ka + pc.c.sl.c] += 0.5 * (pm.c2 + pc.c2) * hL;
+      if (i == NP) {  // the last interval, to the right contact
+        const double hLr = hp * L.L;
+        if (pc.c.sl.a >= 0 && pc.c.sl.a == pn.c.sl.a) gnum[pc.c.sl.a] += 0.5 * (pc.a + pn.a) * hLr;
+        if (pc.c.sl.c >= 0 && pc.c.sl.c == pn.c.sl.c)
+          gnum[L.ka + pc.c.sl.c] += 0.5 * (pc.c2 + pn.c2) * hLr;
+      }
     }
     // the rows' derivatives along each parameter's tangent
     const double fac = L.st(i, S_FAC), sC = L.st(i, S_SC), sP = L.st(i, S_SP);
@@ -820,6 +846,19 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
         sr[1][q] -= w * xi[3 + sp][1];
 #pragma unroll
         for (int q2 = 0; q2 < K; ++q2) SM[q][q2] -= w * xi[3 + sp][2 + q2];
+        // the contact beside this point in the same region: its share of the number follows
+        // this point's ln density and potential
+        const int side = i == 1 ? 0 : i == NP ? 1 : -1;
+        const int slc = side == 0 ? slm : sln;
+        if (side >= 0 && slc == sl) {
+          const double hLc = side == 0 ? hLm : hLp;
+          const double wc = 0.5 * hLc * exp(lnc[side][sp]) / L.tot[q];
+          const double wv = wc * (sp == 0 ? dr_c[side] : -dr_c[side]);
+          sr[0][q] -= wc * xi[3 + sp][0] + wv * xi[0][0];
+          sr[1][q] -= wc * xi[3 + sp][1] + wv * xi[0][1];
+#pragma unroll
+          for (int q2 = 0; q2 < K; ++q2) SM[q][q2] -= wc * xi[3 + sp][2 + q2] + wv * xi[0][2 + q2];
+        }
       }
       s_next = s_here;
       s_here = s_prev;

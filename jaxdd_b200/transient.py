@@ -187,9 +187,6 @@ def _check_batch(batch: Batch, vint: bool, gradients: bool) -> None:
     if gradients and vint:
         raise NotImplementedError("the transient's gradients with the internal voltage an "
                                   "unknown: not built")
-    if gradients and any(reaches_contact(d) for d in devs):
-        raise NotImplementedError("the transient's gradients with an ion region that reaches "
-                                  "a contact: not built")
 
 
 class Work:

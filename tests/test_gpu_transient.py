@@ -322,6 +322,61 @@ def test_charge_gradients_match_differences_of_whole_transients():
                                                                                  ref)
 
 
+def _scaled_contact_device(case, lnN=0.0, lnmu=0.0, NP=100):
+    """A golden case whose ion regions reach the contacts, its ions' densities and mobilities
+    scaled by e^lnN and e^lnmu, at NP points."""
+    import re
+    from jaxdd_b200.simss_input import setup_from_texts
+    from tests.test_impedance_oracle import contact_texts
+    texts = contact_texts(case, NP)
+    for name, text in texts.items():
+        if not name.startswith("L"):
+            continue
+        for key, f in (("N_anion", lnN), ("N_cation", lnN), ("mu_anion", lnmu),
+                       ("mu_cation", lnmu)):
+            text = re.sub(rf"^{key}\s*=\s*([0-9.eE+-]+)",
+                          lambda m: f"{key} = {float(m.group(1)) * float(np.exp(f))!r}", text,
+                          flags=re.M)
+        texts[name] = text
+    return build_device(setup_from_texts(texts), grid="simss")
+
+
+@pytest.mark.parametrize("case", ["zimt_region_slow_light", "two_regions_light"])
+def test_charge_gradients_with_ion_regions_at_the_contacts(case):
+    """The tangents where ion regions reach the contacts (the contacts' ions from their
+    neighbours in each region's number and in the current, along each tangent too): against
+    central differences of whole GPU transients of the rebuilt device, Richardson-extrapolated,
+    and, for the differences, the oracle's transient."""
+    from jaxdd_b200.transient import charge_gradients
+    tvg = transient_steps(40)
+    base = [_scaled_contact_device(case)]
+    assert base[0].anion_mask[0]
+    g = charge_gradients(prepare(base), tvg)
+    assert g.result.converged.all()
+
+    def fd(which, solve):
+        def q(h):
+            return solve([_scaled_contact_device(case, **{which: h})])
+        d1 = (q(1e-3) - q(-1e-3)) / 2e-3
+        d2 = (q(2e-3) - q(-2e-3)) / 4e-3
+        return (4 * d1 - d2) / 3
+
+    def gpu(devs):
+        r = solve_transient(prepare(devs), tvg)
+        return _charge(r, r.t)
+
+    def oracle(devs):
+        o = transient.solve_transient(dd.prepare(devs), tvg.t, tvg.Vext, tvg.G_frac)
+        t = np.broadcast_to(tvg.t, o["J"].shape)
+        return _charge(type("R", (), {"J": o["J"], "accepted": o["accepted"]})(), t)
+
+    for which, mine in (("lnN", g.dQ_dlnN_ion), ("lnmu", g.dQ_dlnmu_ion)):
+        for solve in (gpu, oracle):
+            ref = fd(which, solve)
+            assert np.all(np.abs(mine - ref) < 1e-6 * np.abs(ref) + 1e-9 * np.abs(g.Q)), \
+                (which, solve.__name__, mine, ref)
+
+
 def test_uneven_devices_and_their_own_steps_in_one_launch():
     """Devices of different grid sizes (`prepare(..., ragged=True)`) each with its own step list
     (the steps' per-lane layout) in one launch: each device's result is its transient alone."""

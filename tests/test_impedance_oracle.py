@@ -157,16 +157,6 @@ def test_ion_regions_at_both_contacts_against_the_transient():
     assert 1e-6 < abs(Yd / Yt - 1) < 1e-5
 
 
-def test_the_transients_gradients_refuse_an_ion_region_that_reaches_a_contact():
-    from jaxdd_b200.batch import prepare
-    from jaxdd_b200.transient import charge_gradients
-    from tests.test_transient_oracle import zimt_case
-    setup, tvg, _ = zimt_case("zimt_region_slow_light")
-    with pytest.raises(NotImplementedError, match="reaches a contact"):
-        charge_gradients(prepare([build_device(setup, grid="simss")]), tvg)
-
-
-
 def _sine_response(dev, V0, f, amp=1e-4, per_period=40, periods=20, fitted=4):
     """The oracle transient's admittance at `f`: `J = J₀ + amp·(Re Y·sin + Im Y·cos)` fitted over
     the last periods of a sine of `amp` on `V0` at constant steps (jaxdd
