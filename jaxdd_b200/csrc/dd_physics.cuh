@@ -70,14 +70,9 @@ __device__ __forceinline__ void bern_abs(double a, int simss, double& b, double&
     return;
   }
   const double e = DD_EXPM1(a);
-#ifdef DD_RECIP
-  const double r = 1.0 / e;
+  const double r = 1.0 / e;  // one reciprocal for both quotients
   b = a * r;
   db = (1.0 - b) * r - b;  // 1/e - a(e+1)/e^2, finite where e overflows
-#else
-  b = a / e;
-  db = (1.0 - b) / e - b;  // 1/e - a(e+1)/e^2, finite where e overflows
-#endif
 }
 
 // B(x), B(-x) and their derivatives B'(x), B'(-x) (as functions of their own argument).
@@ -260,18 +255,12 @@ __device__ __forceinline__ void recomb(const LT& L, int k, double n, double p, d
     const double nt0 = L.st(k, S_NT0), pt0 = L.st(k, S_PT0);
     const double den = Cn * (n + nt0) + Cp * (p + pt0);
     const double kk = Nt * Cn * Cp;
-#ifdef DD_RECIP
+    // one reciprocal for the three quotients (an FP64 division is a long instruction sequence)
     const double iden = 1.0 / den;
     const double srh = kk * (n * p - nt0 * pt0) * iden;
     R += srh;
     dRn += n * (kk * p - srh * Cn) * iden;
     dRp += p * (kk * n - srh * Cp) * iden;
-#else
-    const double srh = kk * (n * p - nt0 * pt0) / den;
-    R += srh;
-    dRn += n * (kk * p - srh * Cn) / den;
-    dRp += p * (kk * n - srh * Cp) / den;
-#endif
   }
 }
 

@@ -1153,6 +1153,9 @@ struct Args {
   // the work queue (null: one device per pair): its counter and the pairs of the grid
   int* queue;
   int pairs;
+  // 1: only the lanes with the differential current (the generic kernel's second launch after
+  // the specialised one, which leaves them)
+  int diff_only;
   // dd_newton_step
   double* logs_io;
   const double* vint;
@@ -1206,9 +1209,17 @@ __device__ __forceinline__ void run_lane(const Args& a, int l, int half, Prog<K>
                                          double* ring) {
   Lane L;
   lane_init<K>(L, a, l, half);
-  // The common launch (batch mode, the exact Bernoulli function) is compiled without the others'
-  // paths, which would otherwise sit in the sweeps' code and cost instruction fetch.
-  if (!GENERIC) L.simss = 0;
+  // The common launch (batch mode, the exact Bernoulli function, the integral current) is
+  // compiled without the others' paths, which would otherwise sit in the sweeps' code and cost
+  // instruction fetch: it leaves the lanes with the differential current to a second launch of
+  // the generic kernel, which takes those alone.
+  if (!GENERIC) {
+    L.simss = 0;
+    if (L.currdiff) return;
+    L.currdiff = 0;
+  } else if (a.diff_only && !L.currdiff) {
+    return;
+  }
   const bool top = half == 0;
   const bool jv = GENERIC && a.mode == DD_MODE_JV;
   const int voff = a.voff[l], nv = a.vcnt[l];
@@ -1634,29 +1645,40 @@ long pairs_held(const void* kernel, int block) {
 // zeroed on the stream first when the queue is used.
 int launch_solve(const dd_batch* b, dd::Args& a, void* ws, cudaStream_t s, const Form& f) {
   const int K = slots_k(b);
-  // the specialised kernel for batch mode with the exact Bernoulli function, else the generic one
-  const bool generic = a.mode != DD_MODE_BATCH || a.simss;
-  const void* kernel = K == 2 ? solve_kernel_ptr<2>(f.block, generic)
-                              : solve_kernel_ptr<4>(f.block, generic);
-  if (!allow_ring(kernel, f.block)) return DD_ERR_LAUNCH;
-  const long held = f.queue ? pairs_held(kernel, f.block) : 0;
-  a.queue = nullptr;
-  a.pairs = 0;
-  dim3 grid((2 * b->lane_stride + f.block - 1) / f.block);
-  if (held > 0 && b->n_lanes > held) {
-    size_t ye, fe, ce;
-    int ncd;
-    const size_t at = ws_elems(b, &ye, &fe, &ce, &ncd) - QUEUE_ELEMS;
-    a.queue = reinterpret_cast<int*>(static_cast<double*>(ws) + at);
-    a.pairs = (int)held;
-    if (cudaMemsetAsync(a.queue, 0, sizeof(int), s) != cudaSuccess) return DD_ERR_LAUNCH;
-    grid = dim3((unsigned)(2 * held / f.block));
-  }
-  const dim3 block(f.block);
-  const size_t smem = ring_bytes(f.block);
-  void* args[] = {&a};
-  return cudaLaunchKernel(kernel, grid, block, args, smem, s) == cudaSuccess ? DD_OK
-                                                                            : DD_ERR_LAUNCH;
+  auto go = [&](bool generic) {
+    const void* kernel = K == 2 ? solve_kernel_ptr<2>(f.block, generic)
+                                : solve_kernel_ptr<4>(f.block, generic);
+    if (!allow_ring(kernel, f.block)) return DD_ERR_LAUNCH;
+    const long held = f.queue ? pairs_held(kernel, f.block) : 0;
+    a.queue = nullptr;
+    a.pairs = 0;
+    dim3 grid((2 * b->lane_stride + f.block - 1) / f.block);
+    if (held > 0 && b->n_lanes > held) {
+      size_t ye, fe, ce;
+      int ncd;
+      const size_t at = ws_elems(b, &ye, &fe, &ce, &ncd) - QUEUE_ELEMS;
+      a.queue = reinterpret_cast<int*>(static_cast<double*>(ws) + at);
+      a.pairs = (int)held;
+      if (cudaMemsetAsync(a.queue, 0, sizeof(int), s) != cudaSuccess) return DD_ERR_LAUNCH;
+      grid = dim3((unsigned)(2 * held / f.block));
+    }
+    void* args[] = {&a};
+    return cudaLaunchKernel(kernel, grid, dim3(f.block), args, ring_bytes(f.block), s) ==
+                   cudaSuccess
+               ? DD_OK
+               : DD_ERR_LAUNCH;
+  };
+  // batch mode with the exact Bernoulli function: the specialised kernel, then the generic one
+  // for the lanes with the differential current (it returns at once for the others); else the
+  // generic one alone
+  a.diff_only = 0;
+  if (a.mode != DD_MODE_BATCH || a.simss) return go(true);
+  const int st = go(false);
+  if (st != DD_OK) return st;
+  a.diff_only = 1;
+  const int st2 = go(true);
+  a.diff_only = 0;
+  return st2;
 }
 
 // The tuned forms of this process: by device, ion slots, grid size and lane count (within a

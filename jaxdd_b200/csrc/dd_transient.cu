@@ -589,6 +589,7 @@ __device__ __noinline__ void columns_t(const Args& a, const View& W, int cur, do
 // exactly).
 
 constexpr double TANGENT_H = 1e-6;  // the current's central-difference step along a tangent
+constexpr double VINT_H = 1e-6;  // the vint row's central-difference step (V_T, ln units)
 
 // Step k's solution on every point (V, ln n, ln p, and ln a, ln c where the ions are mobile,
 // else 0) and the traps' occupations at its end from the ones before it, kept or not
@@ -630,13 +631,84 @@ __device__ __noinline__ void write_profile(const Args& a, const View& W, int bn,
   a.prof_dti[(size_t)k * Bp + l] = dti;
 }
 
-template <int K>
-__device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk, double V_k,
-                                          double V_now, double dti, double dti_now, double dt,
-                                          const double* lg, int tb, double* dQ) {
+// The tangent's V_int row (`vint` with gradients): the row's coefficients over the border's
+// columns (the K slots, then the voltage: `vint_row`'s, over the tangent sweep's columns 2 ..)
+// and, per parameter, its right-hand side: less the row's derivative along the tangent sweep's
+// own solution (column p), the state before the step and its V_int along theirs, the traps'
+// occupations along theirs and, for ln mu, the ions' mobilities.
+template <int K, int NC>
+__device__ __noinline__ void vint_tangent_row(const Args& a, const View& W, int bn, int bk,
+                                              double Vi, double V_now, double tVb[2], double dti,
+                                              double dti_now, bool oc, int tb,
+                                              double (&row)[K + 1], double (&res)[2]) {
   const Lane& L = W.L;
   const int NP = L.NP, Bp = a.Bp, l = L.l;
-  constexpr int NC = 2 + K;  // the two tangents' right-hand sides, then the K slot columns
+  const size_t nodes = (size_t)a.npmax + 2;
+  const double* FB = a.FB;
+  const double* FI = a.FI;
+  const double Rs = a.rser[l];
+  const double eV = VINT_H * L.Vt;
+  const double dJV = (current_t<K>(W, bn, Vi + eV, bk, V_now, dti, dti_now, FB, FI) -
+                      current_t<K>(W, bn, Vi - eV, bk, V_now, dti, dti_now, FB, FI)) /
+                         (2.0 * eV) +
+                     L.Gshunt();
+#pragma unroll
+  for (int q = 0; q < K; ++q) row[q] = 0.0;
+  row[K] = oc ? dJV / L.Jscale() : (1.0 + Rs * dJV) * L.iVt;
+  res[0] = 0.0;
+  res[1] = 0.0;
+  const double coef = oc ? 1.0 / L.Jscale() : Rs * L.iVt;
+  if (coef == 0.0) return;  // V_int = V_ext: a row of the voltage alone
+  for (int c = 0; c < NC; ++c) {
+    double m = 0.0;
+    for (int i = 1; i <= NP; ++i)
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+        const double v = fabs(a.CD[((size_t)i * a.ncd + 25 + rr * NC + c) * Bp + l]);
+        m = fmax(m, rr == 0 ? v * L.iVt : v);
+      }
+    Pert pt;
+    pt.tcur = a.CD + (size_t)(25 + c) * Bp;
+    pt.tn = a.ncd;
+    pt.tf = NC;
+    pt.tbef = nullptr;
+    pt.tfb = nullptr;
+    pt.tfi = nullptr;
+    pt.mus = 1.0;
+    double hb = 0.0;  // the V_int before the step along its tangent
+    if (c < 2) {      // a parameter's column: all its inputs along their tangents
+      pt.tbef = a.TY + (size_t)(c * 2 + tb) * nodes * 5 * Bp;
+      pt.tfb = a.TFB + (size_t)c * nodes * Bp;
+      pt.tfi = a.TFI + (size_t)c * nodes * Bp;
+      m = fmax(m, 1.0);
+      hb = tVb[c];
+    } else if (!(m > 0.0) || !isfinite(m)) {
+      continue;  // a zero solution: no change
+    }
+    const double h = VINT_H / m;
+    pt.h = h;
+    if (c == 1) pt.mus = exp(h);
+    const double Jp = current_t<K, true>(W, bn, Vi, bk, V_now + h * hb, dti, dti_now, FB, FI, &pt);
+    pt.h = -h;
+    if (c == 1) pt.mus = exp(-h);
+    const double Jm = current_t<K, true>(W, bn, Vi, bk, V_now - h * hb, dti, dti_now, FB, FI, &pt);
+    const double dJ = coef * (Jp - Jm) / (2.0 * h);
+    if (c < 2) res[c] -= dJ;
+    else row[c - 2] -= dJ;
+  }
+}
+
+template <int K, bool VINT>
+__device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk, double V_k,
+                                          double V_now, double dti, double dti_now, double dt,
+                                          const double* lg, int tb, double* dQ,
+                                          double (&tV)[2][2], bool oc) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = a.Bp, l = L.l;
+  // the two tangents' right-hand sides, then the K slot columns and, with the internal voltage
+  // an unknown, its column (the rows' derivative in V_int: `_system_vint`'s)
+  constexpr int NC = 2 + K + (VINT ? 1 : 0);
+  constexpr int KV = K + (VINT ? 1 : 0);
   const size_t nodes = (size_t)a.npmax + 2;
   auto cd = [&](int k, int f) -> double* { return a.CD + ((size_t)k * a.ncd + f) * Bp + l; };
   auto ty = [&](int p, int b, int k, int c) -> double* {
@@ -771,7 +843,9 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
     for (int rr = 0; rr < 5; ++rr)
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        double sm = c < 2 ? tr_[c][rr] : U[rr][c - 2];
+        const double uv = (i == 1 ? A[rr][0] * 0.5 * L.left() : 0.0) +
+                          (i == NP ? Cm[rr][0] * (-0.5 * L.left()) : 0.0);
+        double sm = c < 2 ? tr_[c][rr] : (VINT && c == NC - 1) ? uv : U[rr][c - 2];
 #pragma unroll
         for (int q = 0; q < 5; ++q) sm -= A[rr][q] * dpv[q][c];
         rhs[rr][c] = sm;
@@ -797,12 +871,12 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
     el = er;
   }
   // back substitution, the slots' Schur complement for both tangents
-  double SM[K][K], sr[2][K];
+  double SM[KV][KV], sr[2][KV];
 #pragma unroll
-  for (int q = 0; q < K; ++q) {
-    const bool has = L.tot[q] > 0.0;
+  for (int q = 0; q < KV; ++q) {
+    const bool has = q < K && L.tot[q] > 0.0;
 #pragma unroll
-    for (int q2 = 0; q2 < K; ++q2) SM[q][q2] = (q == q2 && !has) ? 1.0 : 0.0;
+    for (int q2 = 0; q2 < KV; ++q2) SM[q][q2] = (q == q2 && !has) ? 1.0 : 0.0;
     sr[0][q] = has ? gnum[q] / L.tot[q] : 0.0;  // -d g / d ln N: the number over the total
     sr[1][q] = 0.0;
   }
@@ -845,7 +919,7 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
         sr[0][q] -= w * xi[3 + sp][0];
         sr[1][q] -= w * xi[3 + sp][1];
 #pragma unroll
-        for (int q2 = 0; q2 < K; ++q2) SM[q][q2] -= w * xi[3 + sp][2 + q2];
+        for (int q2 = 0; q2 < KV; ++q2) SM[q][q2] -= w * xi[3 + sp][2 + q2];
         // the contact beside this point in the same region: its share of the number follows
         // this point's ln density and potential
         const int side = i == 1 ? 0 : i == NP ? 1 : -1;
@@ -857,22 +931,32 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
           sr[0][q] -= wc * xi[3 + sp][0] + wv * xi[0][0];
           sr[1][q] -= wc * xi[3 + sp][1] + wv * xi[0][1];
 #pragma unroll
-          for (int q2 = 0; q2 < K; ++q2) SM[q][q2] -= wc * xi[3 + sp][2 + q2] + wv * xi[0][2 + q2];
+          for (int q2 = 0; q2 < KV; ++q2) SM[q][q2] -= wc * xi[3 + sp][2 + q2] + wv * xi[0][2 + q2];
         }
       }
       s_next = s_here;
       s_here = s_prev;
     }
   }
-  double z[2][K];
+  if constexpr (VINT) {  // the voltage's row: its coefficients and, per parameter, its side
+    double rowv[K + 1], resv[2];
+    double tVb[2] = {tV[0][tb], tV[1][tb]};
+    vint_tangent_row<K, NC>(a, W, bn, bk, V_k, V_now, tVb, dti, dti_now, oc, tb, rowv, resv);
+#pragma unroll
+    for (int q2 = 0; q2 < KV; ++q2) SM[K][q2] = rowv[q2];
+    sr[0][K] = resv[0];
+    sr[1][K] = resv[1];
+  }
+  double z[2][KV];
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
-    double S2[K][K];
+    double S2[KV][KV];
 #pragma unroll
-    for (int q = 0; q < K; ++q)
+    for (int q = 0; q < KV; ++q)
 #pragma unroll
-      for (int q2 = 0; q2 < K; ++q2) S2[q][q2] = SM[q][q2];
-    small_solve<K>(S2, sr[p], z[p]);
+      for (int q2 = 0; q2 < KV; ++q2) S2[q][q2] = SM[q][q2];
+    small_solve<KV>(S2, sr[p], z[p]);
+    tV[p][1 - tb] = VINT ? z[p][KV - 1] : 0.0;  // the step's V_int along the tangent
   }
   // the state's tangents of this step
   for (int i = 1; i <= NP; ++i)
@@ -882,7 +966,7 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
       for (int p = 0; p < 2; ++p) {
         double v = *cd(i, 25 + rr * NC + p);
 #pragma unroll
-        for (int q = 0; q < K; ++q) v -= *cd(i, 25 + rr * NC + 2 + q) * z[p][q];
+        for (int q = 0; q < KV; ++q) v -= *cd(i, 25 + rr * NC + 2 + q) * z[p][q];
         *ty(p, 1 - tb, i, rr) = v;
       }
     }
@@ -895,12 +979,15 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
       pt.tbef = a.TY + (size_t)(p * 2 + tb) * nodes * 5 * Bp;
       pt.tfb = a.TFB + (size_t)p * nodes * Bp;
       pt.tfi = a.TFI + (size_t)p * nodes * Bp;
+      const double hv = TANGENT_H * tV[p][1 - tb], hb = TANGENT_H * tV[p][tb];
       pt.h = TANGENT_H;
       pt.mus = p == 1 ? exp(TANGENT_H) : 1.0;
-      const double Jp = current_t<K, true>(W, bn, V_k, bk, V_now, dti, dti_now, FB, FI, &pt);
+      const double Jp =
+          current_t<K, true>(W, bn, V_k + hv, bk, V_now + hb, dti, dti_now, FB, FI, &pt);
       pt.h = -TANGENT_H;
       pt.mus = p == 1 ? exp(-TANGENT_H) : 1.0;
-      const double Jm = current_t<K, true>(W, bn, V_k, bk, V_now, dti, dti_now, FB, FI, &pt);
+      const double Jm =
+          current_t<K, true>(W, bn, V_k - hv, bk, V_now - hb, dti, dti_now, FB, FI, &pt);
       dQ[p] += (Jp - Jm) / (2.0 * TANGENT_H) * dt;
     }
   }
@@ -908,7 +995,6 @@ __device__ __noinline__ void tangent_step(const Args& a, View& W, int bn, int bk
 
 // ------------------------------------------------------------------------------------ kernel
 
-constexpr double VINT_H = 1e-6;  // the vint row's central-difference step (V_T, ln units)
 constexpr int MIN_COUNT_STATIC = 5;  // ZimT's equal states in a row that stop a transient
 constexpr int STOP_STATIC = 1, STOP_FAILED = 2;
 
@@ -1089,6 +1175,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
   const bool grad = a.TY != nullptr;
   const size_t tnodes = (size_t)a.npmax + 2;
   double Qint = 0.0, dQ[2] = {0.0, 0.0};
+  double tVv[2][2] = {{0.0, 0.0}, {0.0, 0.0}};  // V_int along each tangent: [parameter][buffer]
   int tb = 0;
   if (grad) {
     for (int p = 0; p < 4; ++p)
@@ -1454,7 +1541,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       // the tangents of this step, before the occupations move on (they take the old ones)
       const double dt = dti > 0.0 ? t_k - t_last : 0.0;
       Qint += J * dt;
-      if (grad) tangent_step<K>(a, W, bn, bk, Vi, V_now, dti, dti_now, dt, lg, tb, dQ);
+      if (grad) tangent_step<K, VINT>(a, W, bn, bk, Vi, V_now, dti, dti_now, dt, lg, tb, dQ, tVv, oc_k);
       // the traps' occupations at the step's end, from its solution (and their tangents)
       auto tyn = [&](int p, int k, int c) {
         return (k < 1 || k > NP) ? 0.0
@@ -1584,7 +1671,9 @@ void ws_parts(const dd_batch* b, size_t* y, size_t* fb, size_t* fi, size_t* cd, 
               size_t* tan) {
   const int K = slots_k_t(b);
   const size_t nodes = (size_t)b->np_max + 2, Bp = (size_t)b->lane_stride;
-  *ncd = 25 + 5 * (2 + K);  // the Newton step's 1 + K columns, or the tangents' 2 + K
+  // the Newton step's 1 + K columns (2 + K with the internal voltage an unknown), or the
+  // tangents' 2 + K (3 + K)
+  *ncd = 25 + 5 * (3 + K);
   *y = align_up(3 * nodes * 5 * Bp * sizeof(double));
   *fb = align_up(nodes * Bp * sizeof(double));
   *fi = align_up(nodes * Bp * sizeof(double));
@@ -1631,8 +1720,8 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
       !steps->failure_mode || (steps->stride != 0 && steps->stride != batch->lane_stride))
     return DD_ERR_ARGS;
   if (steps->vint && (!steps->oc || !steps->r_series || !steps->start_j_ext)) return DD_ERR_ARGS;
-  // the vint row's derivatives take a state's perturbation from every point: no gradients
-  if (steps->vint && out->Q) return DD_ERR_ARGS;
+  // the gradients with the internal voltage an unknown: not with an ion region at a contact
+  // (the host refuses that case for the transient itself)
   if (!out->J || !out->J_ext || !out->converged || !out->iterations || !out->accepted ||
       !out->stop || !out->state || !out->logs)
     return DD_ERR_ARGS;

@@ -178,15 +178,12 @@ def reaches_contact(d) -> bool:
     return any(m is not None and bool(m[0] or m[-1]) for m in (d.anion_mask, d.cation_mask))
 
 
-def _check_batch(batch: Batch, vint: bool, gradients: bool) -> None:
+def _check_batch(batch: Batch, vint: bool) -> None:
     devs = batch["devices"]
     if vint and any(reaches_contact(d) for d in devs):
         raise NotImplementedError("the internal voltage an unknown (an open circuit, a series "
                                   "resistance) with an ion region that reaches a contact: not "
                                   "built")
-    if gradients and vint:
-        raise NotImplementedError("the transient's gradients with the internal voltage an "
-                                  "unknown: not built")
 
 
 class Work:
@@ -211,7 +208,7 @@ class Work:
         # the internal voltage an unknown of every device's steps where any is at the open
         # circuit or has a series resistance (transient.py:600-601)
         self.vint = vint = bool(vint or oc.any() or np.any(R > 0))
-        _check_batch(batch, vint, gradients)
+        _check_batch(batch, vint)
         init = None if initial is None else _checked_initial(initial, devs, t)
         self.batch, self.tol, self.max_iter = batch, tol, max_iter
         self.bern = _lib.DD_BERNOULLI[bernoulli_name]
@@ -556,13 +553,16 @@ class ChargeGradients:
 
 
 def charge_gradients(batch: Batch, tvg, tol: float = 1e-10, max_iter: int = 200,
-                     bernoulli_name: str = "exact", zimt_current: bool = False) -> ChargeGradients:
+                     bernoulli_name: str = "exact", zimt_current: bool = False,
+                     vint: bool = False) -> ChargeGradients:
     """The integrated transient current and its gradient in the ion density and the ion mobility
     (the transient workload's gradients), in forward mode through every step as jaxdd differentiates
     its transients (`jax.jvp` through each step's `_converged_jvp`, batch.py:661-737): one
-    `dd_transient` launch with the tangents carried beside the state."""
+    `dd_transient` launch with the tangents carried beside the state. With the internal voltage
+    an unknown (`vint`, as `solve_transient` decides it: an open circuit, a series resistance)
+    it has a tangent of its own, from the tangent system's voltage row."""
     work = Work(batch, tvg, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
-                zimt_current=zimt_current, gradients=True)
+                zimt_current=zimt_current, gradients=True, vint=vint)
     o, _ = work.run()
     lanes = batch["lane_of"]
     dQ = o["dQ"].cpu().numpy()[:, lanes]

@@ -248,12 +248,16 @@ def test_ion_stacks_full_steps_hold_their_invariants():
         assert abs(_number(r.final.anion[k], d.anion_mask, d) / d.anion_total - 1) < 1e-8
 
 
-def _scaled_device(k, lnN=0.0, lnmu=0.0, NP=120):
-    """The mobile-ion stack `k` with its ion density and mobility scaled by e^lnN and e^lnmu."""
+def _scaled_device(k, lnN=0.0, lnmu=0.0, NP=120, R_series=0.0):
+    """The mobile-ion stack `k` with its ion density and mobility scaled by e^lnN and e^lnmu
+    (and a series resistance, Ohm m², where given)."""
     from jaxdd_b200.simss_input import setup_from_texts
     from jaxdd_b200.workloads import SEED_ION_STACKS, drawn_texts
     idx = 2 * k + 1
     t = drawn_texts(idx, np.random.default_rng([SEED_ION_STACKS, idx]), NP)
+    if R_series:
+        t["simulation_setup.txt"] = t["simulation_setup.txt"].replace(
+            "R_series = 0\n", f"R_series = {R_series!r}\n")
     lines = []
     for line in t["L2.txt"].splitlines():
         key, _, val = (part.strip() for part in line.partition("="))
@@ -375,6 +379,49 @@ def test_charge_gradients_with_ion_regions_at_the_contacts(case):
             ref = fd(which, solve)
             assert np.all(np.abs(mine - ref) < 1e-6 * np.abs(ref) + 1e-9 * np.abs(g.Q)), \
                 (which, solve.__name__, mine, ref)
+
+
+@pytest.mark.parametrize("circuit", ["series", "open"])
+def test_charge_gradients_with_the_internal_voltage_an_unknown(circuit):
+    """The tangents with the internal voltage an unknown of every step (its own tangent from the
+    tangent system's voltage row, the current's and the next step's through it): a series
+    resistance of 1e-4 Ohm m² at 0.9 V, and the open circuit from the steady state at 0 V under
+    light, against central differences of whole GPU transients and of the oracle's."""
+    import dataclasses
+    from jaxdd_b200.transient import charge_gradients
+    tvg = transient_steps(40)
+    rs = 1e-4 if circuit == "series" else 0.0
+    if circuit == "open":
+        tvg = dataclasses.replace(tvg, oc=tvg.t > 0)
+    ks = (0, 1)
+    base = [_scaled_device(k, R_series=rs) for k in ks]
+    g = charge_gradients(prepare(base), tvg)
+    assert g.result.converged.all()
+    assert np.ptp(g.result.V_int[0, 1:]) > 1e-3  # the internal voltage moves
+
+    def fd(which, solve):
+        def q(h):
+            return solve([_scaled_device(k, R_series=rs, **{which: h}) for k in ks])
+        d1 = (q(1e-3) - q(-1e-3)) / 2e-3
+        d2 = (q(2e-3) - q(-2e-3)) / 4e-3
+        return (4 * d1 - d2) / 3
+
+    def gpu(devs):
+        r = solve_transient(prepare(devs), tvg)
+        return _charge(r, r.t)
+
+    def oracle(devs):
+        o = transient.solve_transient(dd.prepare(devs[:1]), tvg.t, tvg.Vext, tvg.G_frac,
+                                      oc=tvg.oc)
+        t = np.broadcast_to(tvg.t, o["J"].shape)
+        return _charge(type("R", (), {"J": o["J"], "accepted": o["accepted"]})(), t)
+
+    for which, mine in (("lnN", g.dQ_dlnN_ion), ("lnmu", g.dQ_dlnmu_ion)):
+        ref = fd(which, gpu)
+        assert np.all(np.abs(mine - ref) < 1e-6 * np.abs(ref) + 1e-9 * np.abs(g.Q)), \
+            (which, mine, ref)
+        ref = fd(which, oracle)
+        assert abs(mine[0] - ref[0]) < 1e-6 * abs(ref[0]) + 1e-9 * abs(g.Q[0]), (which, mine, ref)
 
 
 def test_uneven_devices_and_their_own_steps_in_one_launch():
