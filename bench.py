@@ -53,6 +53,10 @@ NP = 400
 CHUNK = 512  # devices per build task (a multiple of 32)
 #: which kernel build profiles/traffic.json must describe for its traffic to be reported
 KERNEL_TAG = "twisted two-thread fused Newton, shared-memory staged record"
+# Kernel launches of one dd_solve / dd_solve_states in batch mode with the exact Bernoulli
+# function: the specialised solve kernel, then the generic one for the lanes with the
+# differential current (it returns at once for the others).
+SOLVE_LAUNCHES = 2
 
 
 def traffic_entry(precision: str, workload: str, devices: int, npts: int) -> dict | None:
@@ -366,7 +370,7 @@ def adjoint_bench(args, rank: int, world: int, local: int) -> None:
                        "grad_norm": float(g.norm()), "forward_ms": ms_fwd,
                        "adjoint_over_forward": ms_grad / ms_fwd,
                        "converged_fraction": float(target[1].float().mean())},
-            "gpu_launches": args.steps * 5,
+            "gpu_launches": args.steps * (4 + SOLVE_LAUNCHES),
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -428,7 +432,7 @@ def impedance_bench(args, rank: int, world: int, local: int) -> None:
                        "build_s": round(build_s, 1),
                        "converged_fraction": float(ok[:batch["n"]].float().mean()),
                        "nonfinite_points": nonfinite},
-            "gpu_launches": args.steps * 4,
+            "gpu_launches": args.steps * (3 + SOLVE_LAUNCHES),
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -666,7 +670,7 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
                          "peak_source": f"{peak_kind} HBM copy",
                          "kernel": "dd::tr::transient_kernel (one thread per device)"},
             "cpu_baseline": cpu,
-            "gpu_launches": args.steps * 2,
+            "gpu_launches": args.steps * (1 + SOLVE_LAUNCHES),
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -971,7 +975,7 @@ def main() -> None:
                           "of jaxdd's FP64 solve_batch (oracle/dd_cpu.cpp; jaxdd needs JAX)"},
             "e2e": {"value": e2e_value, "unit": "curves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * SOLVE_LAUNCHES,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

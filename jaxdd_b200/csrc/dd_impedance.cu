@@ -1383,10 +1383,10 @@ int dd_admittance_ions(const dd_batch* batch, const double* state, const double*
       !tstat || !vint || !laps || n_freq < 1 || !Y || !workspace)
     return DD_ERR_ARGS;
   if (batch->n_lanes < 1 || batch->lane_stride < batch->n_lanes || batch->lane_stride % 32 != 0 ||
-      batch->np_max < 3 || batch->k_anion != 1 || batch->k_cation != 1)
+      batch->np_max < 3)
     return DD_ERR_ARGS;
   if (bernoulli != DD_BERNOULLI_EXACT && bernoulli != DD_BERNOULLI_SIMSS) return DD_ERR_ARGS;
-  size_t need;
+  size_t need;  // (the slots: k_anion, k_cation >= 1, at most DD_MAXK in all)
   if (dd_admittance_ions_workspace_bytes(batch, n_freq, &need) != DD_OK) return DD_ERR_ARGS;
   if (workspace_bytes < need) return DD_ERR_WORKSPACE;
   const size_t nodes = (size_t)batch->np_max + 2, Bp = batch->lane_stride;
