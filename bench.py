@@ -775,6 +775,9 @@ def main() -> None:
     ap.add_argument("--parity-lanes", type=int, default=1024,
                     help="devices of the timed launch checked against the oracle after the "
                          "timed region (0: none)")
+    ap.add_argument("--graph", default="auto", choices=("auto", "on", "off"),
+                    help="replay the solve from a CUDA graph captured once (auto: the uneven "
+                         "workload, whose config asks for it)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -855,10 +858,11 @@ def main() -> None:
     so = _lib.lib()
     stream = torch.cuda.current_stream(dev)
 
-    def launch(d=desc, v=volts):
+    def launch(d=desc, v=volts, on=None):
         _lib.check(so.dd_solve(ctypes.byref(d), ctypes.byref(v), ctypes.byref(opts),
                                J.data_ptr(), ok.data_ptr(), its.data_ptr(), status.data_ptr(),
-                               steps.data_ptr(), ws.data_ptr(), ws.numel(), stream.cuda_stream),
+                               steps.data_ptr(), ws.data_ptr(), ws.numel(),
+                               (on or stream).cuda_stream),
                    "dd_solve")
 
     def barrier():
@@ -878,14 +882,25 @@ def main() -> None:
                               ctypes.byref(form), times), "dd_tune")
         launch_form = dict(_lib.SOLVE_FORMS[form.value], form=form.value,
                            tune_ms=[round(float(t), 1) for t in times])
+    # the solve's launches (the queue's reset, the specialised and the generic kernel) captured
+    # once into a CUDA graph and replayed, where asked
+    graphed = args.graph == "on" or (args.graph == "auto" and uneven)
+    step = launch
+    if graphed:
+        graph = torch.cuda.CUDAGraph()
+        launch()  # the tuned form's attributes set before the capture
+        barrier()
+        with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+            launch(on=torch.cuda.current_stream(dev))
+        step = graph.replay
     for _ in range(args.warmup):
-        launch()
+        step()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
-            launch()
+            step()
         ev1.record(stream)
         barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -959,7 +974,7 @@ def main() -> None:
                        "l2": f"inputs larger than L2 ({batch['stat'].nbytes / 1e9:.2f} GB of "
                              "statics per launch)",
                        "converged_fraction": ok_frac, "build_s": round(build_s, 1),
-                       "launch": launch_form},
+                       "launch": launch_form, "cuda_graph": graphed},
             "parity": parity,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

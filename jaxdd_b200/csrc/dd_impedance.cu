@@ -1175,6 +1175,8 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
       dJD = dJD + (hk * sign * epsk / (L.L * hk)) * (dV(k + 1) - dV(k));
       // the ions over interval k (points k, k+1): `_ion_currents` linearised at the state
       const Slots sa = slots_at(L, k), sb = slots_at(L, k + 1);
+      // the ions' trapezoids take every interval, the last one (to the right contact) too
+      const double dxi = k < NP ? dx : hk * L.L;
 #pragma unroll
       for (int j = 0; j < K; ++j) {
         if (!(L.tot[j] > 0.0)) continue;
@@ -1235,13 +1237,13 @@ __global__ void __launch_bounds__(64) admittance_ions_kernel(Args a, IonArgs b) 
           const double ia = 1.0 / (mua > 0.0 ? mua : 1.0), ib = 1.0 / (mub > 0.0 ? mub : 1.0);
           const cplx dUa = nRa * dRa, dUb = nRb * dRb;  // per unit of dti
           const double Uva = k == 0 ? nRa - 1.0 : 0.0, Uvb = k + 1 == NP + 1 ? nRb - 1.0 : 0.0;
-          const cplx diu_b2 = diu_i[j] + (0.5 * dx) * (dUa + dUb);
-          const double iu_b2 = iu_v[j] + 0.5 * dx * (Uva + Uvb);
-          is_[j] += 0.5 * dx * (eva * ia + evb * ib);
-          dis[j] = dis[j] + (0.5 * dx) * (ia * deva + ib * devb);
-          dbl_v[j] += 0.5 * dx * (eva * ia * iu_v[j] + evb * ib * iu_b2);
-          ddbl_i[j] = ddbl_i[j] + (0.5 * dx * eva * ia) * diu_i[j] + (0.5 * dx * evb * ib) * diu_b2 +
-                      (0.5 * dx * ia * iu_v[j]) * deva + (0.5 * dx * ib * iu_b2) * devb;
+          const cplx diu_b2 = diu_i[j] + (0.5 * dxi) * (dUa + dUb);
+          const double iu_b2 = iu_v[j] + 0.5 * dxi * (Uva + Uvb);
+          is_[j] += 0.5 * dxi * (eva * ia + evb * ib);
+          dis[j] = dis[j] + (0.5 * dxi) * (ia * deva + ib * devb);
+          dbl_v[j] += 0.5 * dxi * (eva * ia * iu_v[j] + evb * ib * iu_b2);
+          ddbl_i[j] = ddbl_i[j] + (0.5 * dxi * eva * ia) * diu_i[j] + (0.5 * dxi * evb * ib) * diu_b2 +
+                      (0.5 * dxi * ia * iu_v[j]) * deva + (0.5 * dxi * ib * iu_b2) * devb;
           diu_i[j] = diu_b2;
           iu_v[j] = iu_b2;
           const cplx dstep = k > first_i[j] ? (sn * Q * L.L * width) * dUa : mk(0.0);

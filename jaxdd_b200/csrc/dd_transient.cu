@@ -308,9 +308,11 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
         const double qa2 = eva / (mua > 0.0 ? mua : 1.0);
         const double qb2 = evb / (mub > 0.0 ? mub : 1.0);
         const double Ua = dti * (da - qa_), Ub = dti * (db - qb_);
-        const double iu_b = iiu[k] + 0.5 * dx * (Ua + Ub);
-        is[k] += 0.5 * dx * (qa2 + qb2);
-        idb[k] += 0.5 * dx * (qa2 * iiu[k] + qb2 * iu_b);
+        // the ions' trapezoids take every interval, the last one (to the right contact) too
+        const double dxi = e < NP ? dx : h * L.L;
+        const double iu_b = iiu[k] + 0.5 * dxi * (Ua + Ub);
+        is[k] += 0.5 * dxi * (qa2 + qb2);
+        idb[k] += 0.5 * dxi * (qa2 * iiu[k] + qb2 * iu_b);
         iiu[k] = iu_b;
         // J_e = qK + the prefix of the steps; at an interface the interval's before it
         const double stp = e > first_k[k] ? sn * QL * width * Ua : 0.0;
