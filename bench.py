@@ -52,7 +52,7 @@ DEVICES_PER_GPU = 16384
 NP = 400
 CHUNK = 512  # devices per build task (a multiple of 32)
 #: which kernel build profiles/traffic.json must describe for its traffic to be reported
-KERNEL_TAG = "twisted two-thread fused Newton, shared-memory staged record"
+KERNEL_TAG = "twisted two-thread fused Newton, shared-memory staged record, specialised batch instantiation"
 # Kernel launches of one dd_solve / dd_solve_states in batch mode with the exact Bernoulli
 # function: the specialised solve kernel, then the generic one for the lanes with the
 # differential current (it returns at once for the others).
