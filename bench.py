@@ -668,7 +668,8 @@ def transient_bench(args, rank: int, world: int, local: int) -> None:
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "peak_source": f"{peak_kind} HBM copy",
-                         "kernel": "dd::tr::transient_kernel (one thread per device)"},
+                         "kernel": "dd::tr::transient_kernel (two threads per device, the "
+                                   "twisted sweep)"},
             "cpu_baseline": cpu,
             "gpu_launches": args.steps * (1 + SOLVE_LAUNCHES),
             "clocks": clocks.summary(),

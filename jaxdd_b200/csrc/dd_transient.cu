@@ -1116,9 +1116,398 @@ __device__ __noinline__ void vint_row(const Args& a, const View& W, int bn, int 
   }
 }
 
-template <int K, bool VINT>
+// ------------------------------------------------------------------------------------ twisted
+//
+// Two threads a device (`transient_kernel<K, false, true>`, neither the internal voltage an
+// unknown nor the gradients): the Newton iteration's sweep is twisted as the steady solve's is.
+// Half 0 eliminates rows 1 .. m - 1 downwards (c'_i = M_i^-1 C_i, M_i = B_i - A_i c'_{i-1}), half
+// 1 rows NP .. m + 1 upwards (a''_i = N_i^-1 A_i, N_i = B_i - C_i a''_{i+1}), each on the same
+// code in its own frame (NODE(p) and EDGE(p) walk from its contact inwards); half 0 solves the
+// meeting row m, B_m - A_m c'_{m-1} - C_m a''_{m+1}, with half 1's carry, and each half
+// substitutes back outwards from x_m. The slots' border and each region's number are summed per
+// half and added in one order on both, so both halves solve the same border system. The
+// current, the step's start and its end run on half 0 alone.
+
+__device__ __forceinline__ TP tsel(bool t, const TP& x, const TP& y) {
+  TP o;
+  o.c.V = t ? x.c.V : y.c.V;
+  o.c.lnn = t ? x.c.lnn : y.c.lnn;
+  o.c.lnp = t ? x.c.lnp : y.c.lnp;
+  o.c.n = t ? x.c.n : y.c.n;
+  o.c.p = t ? x.c.p : y.c.p;
+  o.c.offn = t ? x.c.offn : y.c.offn;
+  o.c.offp = t ? x.c.offp : y.c.offp;
+  o.c.sl.a = t ? x.c.sl.a : y.c.sl.a;
+  o.c.sl.c = t ? x.c.sl.c : y.c.sl.c;
+  o.c.da = t ? x.c.da : y.c.da;
+  o.c.dc = t ? x.c.dc : y.c.dc;
+  o.la = t ? x.la : y.la;
+  o.lc = t ? x.lc : y.lc;
+  o.a = t ? x.a : y.a;
+  o.c2 = t ? x.c2 : y.c2;
+  return o;
+}
+
+__device__ __forceinline__ Flux fsel(bool t, const Flux& x, const Flux& y) {
+  Flux o;
+  o.Fn = t ? x.Fn : y.Fn; o.n0V = t ? x.n0V : y.n0V; o.n0n = t ? x.n0n : y.n0n;
+  o.n1V = t ? x.n1V : y.n1V; o.n1n = t ? x.n1n : y.n1n; o.Fp = t ? x.Fp : y.Fp;
+  o.p0V = t ? x.p0V : y.p0V; o.p0p = t ? x.p0p : y.p0p; o.p1V = t ? x.p1V : y.p1V;
+  o.p1p = t ? x.p1p : y.p1p;
+  return o;
+}
+
+__device__ __forceinline__ IonIv isel(bool t, const IonIv& x, const IonIv& y) {
+  return IonIv{t ? x.F : y.F, t ? x.gx : y.gx, t ? x.da : y.da, t ? x.db : y.db};
+}
+
+// The other half's value, and a pair's sum in one order on both halves (half 0's first).
+__device__ __forceinline__ double pxchg(unsigned mask, double v) {
+  return __shfl_xor_sync(mask, v, 1);
+}
+__device__ __forceinline__ double psum(unsigned mask, bool top, double v) {
+  const double o = pxchg(mask, v);
+  return top ? v + o : o + v;
+}
+
+// Each region's number over edge e (points lo = e, hi = e + 1), as the forward pass sums it.
+template <int K>
+__device__ __forceinline__ void tw_number(const Lane& L, const TP& lo, const TP& hi, int e,
+                                          double (&gnum)[K]) {
+  const double hL = L.st(e, S_H) * L.L;
+  if (hi.c.sl.a >= 0 && hi.c.sl.a == lo.c.sl.a) gnum[hi.c.sl.a] += 0.5 * (lo.a + hi.a) * hL;
+  if (hi.c.sl.c >= 0 && hi.c.sl.c == lo.c.sl.c)
+    gnum[L.ka + hi.c.sl.c] += 0.5 * (lo.c2 + hi.c2) * hL;
+}
+
+// One twisted Newton iteration of a step (no internal voltage): the sweep, the border, the damped
+// update of this half's points and the slots' scales `lg`. Returns the step's size and whether the
+// new iterate is finite, both of the whole device.
+template <int K>
+__device__ __forceinline__ void tw_iteration(const Args& a, const View& W, int bn, double Vi,
+                                             double dti, double (&lg)[K], bool top,
+                                             unsigned mask, double capV, double& size_out,
+                                             bool& finite_out) {
+  const Lane& L = W.L;
+  const int NP = L.NP, Bp = a.Bp, l = L.l;
+  constexpr int NC = 1 + K;
+  const double* FB = a.FB;
+  const double* FI = a.FI;
+  auto cd = [&](int k, int f) -> double* { return a.CD + ((size_t)k * a.ncd + f) * Bp + l; };
+  const int m = NP / 2;  // the meeting row: half 0 rows 1 .. m, half 1 rows m + 1 .. NP
+  const int nown = top ? m : NP - m;
+  auto NODE = [&](int p) { return top ? p : NP + 1 - p; };
+  auto EDGE = [&](int p) { return top ? p : NP - p; };  // between NODE(p) and NODE(p + 1)
+  double cpv[5][5], dpv[5][NC];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) cpv[r][c] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) dpv[r][c] = 0.0;
+  }
+  double gnum[K], elg[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) { gnum[q] = 0.0; elg[q] = exp(lg[q]); }
+  // -------- assembly and elimination from this half's contact inwards
+  TP po, pc, pi;
+  load_point(W, bn, NODE(0), Vi, po);
+  contact_ions(W, bn, NODE(0), dti, po);
+  load_point(W, bn, NODE(1), Vi, pc);
+  Flux fo;
+  IonIv ivo[2];
+  {
+    const TP lo = tsel(top, po, pc), hi = tsel(top, pc, po);
+    const int e = EDGE(0);
+    flux(L, lo.c, hi.c, L.st(e, S_MUN), L.st(e, S_MUP), fo);
+    ion_ivs(W, e, lo, hi, ivo);
+    tw_number<K>(L, lo, hi, e, gnum);
+  }
+  for (int p = 1; p <= nown; ++p) {
+    const int i = NODE(p);
+    load_point(W, bn, NODE(p + 1), Vi, pi);  // the inner neighbour: inside the device
+    const int ei = EDGE(p);
+    Flux fi;
+    IonIv ivi[2];
+    {
+      const TP lo = tsel(top, pc, pi), hi = tsel(top, pi, pc);
+      flux(L, lo.c, hi.c, L.st(ei, S_MUN), L.st(ei, S_MUP), fi);
+      ion_ivs(W, ei, lo, hi, ivi);
+      // this half's edges: each point's outer one, and half 0 the meeting row's inner one too
+      if (p < nown || top) tw_number<K>(L, lo, hi, ei, gnum);
+    }
+    // row i in the grid's order: its left and right neighbours and intervals
+    const TP pl = tsel(top, po, pi), pr = tsel(top, pi, po);
+    const Flux fl = fsel(top, fo, fi), fr = fsel(top, fi, fo);
+    IonIv ivl[2], ivr[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) { ivl[s] = isel(top, ivo[s], ivi[s]); ivr[s] = isel(top, ivi[s], ivo[s]); }
+    const double hm = L.st(i - 1, S_H), hp = L.st(i, S_H);
+    const int ifm = (int)L.st(i - 1, S_IFK), ifi = (int)L.st(i, S_IFK);
+    const double fb = FB[(size_t)i * Bp + l];
+    const double fim = ifm >= 0 ? FI[(size_t)(i - 1) * Bp + l] : 0.0;
+    const double fii = ifi >= 0 ? FI[(size_t)i * Bp + l] : 0.0;
+    const size_t ob = (size_t)i * 4 * Bp + l;
+    const double bnv = a.BD[ob], bpv = a.BD[ob + Bp];
+    const double bav = a.BD[ob + 2 * Bp], bcv = a.BD[ob + 3 * Bp];
+    double A[5][5], Bm[5][5], Cm[5][5], r[5], U[5][K];
+    row5<K>(W, i, pl, pc, pr, fl, fr, hm, hp, ifm, ifi, dti, fb, fim, fii, bnv, bpv, bav, bcv,
+            lg, A, Bm, Cm, r, U, nullptr, nullptr, elg, ivl, ivr);
+    if (top && p == nown) {
+      // the meeting row waits in memory (the free records of point 0 and of m itself)
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          *cd(0, rr * 5 + c) = A[rr][c];
+          *cd(0, 25 + rr * 5 + c) = Cm[rr][c];
+          *cd(m, rr * 5 + c) = Bm[rr][c];
+        }
+        *cd(m, 25 + rr * NC) = r[rr];
+#pragma unroll
+        for (int k = 0; k < K; ++k) *cd(m, 25 + rr * NC + 1 + k) = U[rr][k];
+      }
+    } else {
+      // eliminate towards the inside: the outer coupling (A for half 0, C for half 1) against
+      // the carry, the inner one into the next carry
+      double M[5][5], rhs[5][NC];
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          double s = Bm[rr][c];
+#pragma unroll
+          for (int q = 0; q < 5; ++q) s -= (top ? A[rr][q] : Cm[rr][q]) * cpv[q][c];
+          M[rr][c] = s;
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          double s = c == 0 ? r[rr] : U[rr][c - 1];
+#pragma unroll
+          for (int q = 0; q < 5; ++q) s -= (top ? A[rr][q] : Cm[rr][q]) * dpv[q][c];
+          rhs[rr][c] = s;
+        }
+      }
+      Part f;
+      partition(M, f);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        double v[5];
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) v[rr] = top ? Cm[rr][c] : A[rr][c];
+        apply(f, v);
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) { cpv[rr][c] = v[rr]; *cd(i, rr * 5 + c) = v[rr]; }
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        double v[5] = {rhs[0][c], rhs[1][c], rhs[2][c], rhs[3][c], rhs[4][c]};
+        apply(f, v);
+#pragma unroll
+        for (int rr = 0; rr < 5; ++rr) { dpv[rr][c] = v[rr]; *cd(i, 25 + rr * NC + c) = v[rr]; }
+      }
+    }
+    po = pc;
+    pc = pi;
+    fo = fi;
+    ivo[0] = ivi[0];
+    ivo[1] = ivi[1];
+  }
+  // -------- the meeting row: half 1's carry to half 0, x_m back to half 1
+  double oc[5][5], od[5][NC];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) oc[r][c] = pxchg(mask, cpv[r][c]);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) od[r][c] = pxchg(mask, dpv[r][c]);
+  }
+  double xm[5][NC];
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) xm[r][c] = 0.0;
+  if (top) {
+    // (B_m - A_m c'_{m-1} - C_m a''_{m+1}) x_m = [r | U]_m - A_m d'_{m-1} - C_m e''_{m+1}
+    double G[5][5], R[5][NC];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        double s = *cd(m, rr * 5 + c);
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+          s -= *cd(0, rr * 5 + q) * cpv[q][c] + *cd(0, 25 + rr * 5 + q) * oc[q][c];
+        G[rr][c] = s;
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        double s = *cd(m, 25 + rr * NC + c);
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+          s -= *cd(0, rr * 5 + q) * dpv[q][c] + *cd(0, 25 + rr * 5 + q) * od[q][c];
+        R[rr][c] = s;
+      }
+    }
+    Part f;
+    partition(G, f);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      double v[5] = {R[0][c], R[1][c], R[2][c], R[3][c], R[4][c]};
+      apply(f, v);
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr) { xm[rr][c] = v[rr]; *cd(m, 25 + rr * NC + c) = v[rr]; }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const double v = pxchg(mask, xm[r][c]);
+      if (!top) xm[r][c] = v;
+    }
+  // -------- back substitution outwards, and this half's part of the border's Schur complement
+  // D - W^T X_U and of W^T X_F (each region's number in its points' ion logarithms; where a region
+  // reaches a contact, the contact's share in its neighbour's ln density and potential)
+  double SMp[K][K], srp[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    srp[q] = 0.0;
+#pragma unroll
+    for (int q2 = 0; q2 < K; ++q2) SMp[q][q2] = 0.0;
+  }
+  auto border = [&](int i, const double (&xi)[5][NC]) {
+    const Slots s_prev = slots_at(L, i - 1), s_here = slots_at(L, i), s_next = slots_at(L, i + 1);
+    const double hLm = L.st(i - 1, S_H) * L.L, hLp = L.st(i, S_H) * L.L;
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) {
+      const int sl = sp == 0 ? s_here.a : s_here.c;
+      if (sl < 0) continue;
+      const int q = sp == 0 ? sl : L.ka + sl;
+      if (!(L.tot[q] > 0.0)) continue;
+      const int slm = sp == 0 ? s_prev.a : s_prev.c, sln = sp == 0 ? s_next.a : s_next.c;
+      const double wpt = 0.5 * ((slm == sl ? hLm : 0.0) + (sln == sl ? hLp : 0.0));
+      double w = wpt * exp(*W.y(bn, i, 3 + sp)) / L.tot[q], wv = 0.0;
+      if ((i == 1 && slm == sl) || (i == NP && sln == sl)) {
+        const int kc = i == 1 ? 0 : NP + 1;
+        TP P;
+        load_point(W, bn, kc, Vi, P);
+        double dr;
+        contact_ions(W, bn, kc, dti, P, &dr);
+        const double wc = 0.5 * (i == 1 ? hLm : hLp) * (sp == 0 ? P.a : P.c2) / L.tot[q];
+        w += wc;
+        wv = wc * (sp == 0 ? dr : -dr);
+      }
+      srp[q] += w * xi[3 + sp][0] + wv * xi[0][0];
+#pragma unroll
+      for (int q2 = 0; q2 < K; ++q2) SMp[q][q2] += w * xi[3 + sp][1 + q2] + wv * xi[0][1 + q2];
+    }
+  };
+  if (top) border(m, xm);
+  {
+    double xn[5][NC];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) xn[rr][c] = xm[rr][c];
+    for (int p = top ? nown - 1 : nown; p >= 1; --p) {
+      const int i = NODE(p);
+      double xi[5][NC];
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          double s = *cd(i, 25 + rr * NC + c);
+#pragma unroll
+          for (int q = 0; q < 5; ++q) s -= *cd(i, rr * 5 + q) * xn[q][c];
+          xi[rr][c] = s;
+        }
+#pragma unroll
+      for (int rr = 0; rr < 5; ++rr)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          *cd(i, 25 + rr * NC + c) = xi[rr][c];
+          xn[rr][c] = xi[rr][c];
+        }
+      border(i, xi);
+    }
+  }
+  // both halves' parts, and the numbers, added in one order: the same border system on both
+  double SM[K][K], sr[K], z[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) gnum[q] = psum(mask, top, gnum[q]);
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const bool has = L.tot[q] > 0.0;
+    sr[q] = -(has ? gnum[q] / L.tot[q] - 1.0 : lg[q]) - psum(mask, top, srp[q]);
+#pragma unroll
+    for (int q2 = 0; q2 < K; ++q2)
+      SM[q][q2] = ((q == q2 && !has) ? 1.0 : 0.0) - psum(mask, top, SMp[q][q2]);
+  }
+  small_solve<K>(SM, sr, z);
+  // -------- the damped update (batch.py:759-785) of this half's points
+  double size = 0.0, dl_max = 0.0;
+  bool finite = true;
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const double dlq = clipd(z[q], -ION_LOG_CAP, ION_LOG_CAP);
+    dl_max = nanmax(dl_max, fabs(dlq));
+    lg[q] += dlq;
+  }
+  for (int p = 1; p <= nown; ++p) {
+    const int i = NODE(p);
+    double d5[5];
+#pragma unroll
+    for (int rr = 0; rr < 5; ++rr) {
+      double s = *cd(i, 25 + rr * NC);
+#pragma unroll
+      for (int q = 0; q < K; ++q) s -= *cd(i, 25 + rr * NC + 1 + q) * z[q];
+      d5[rr] = s;
+    }
+    double y5[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) y5[c] = *W.y(bn, i, c);
+    double st5[5];
+    st5[0] = clipd(d5[0], -capV, capV);
+#pragma unroll
+    for (int c = 1; c < 5; ++c) st5[c] = clipd(d5[c], -CAP_LN, CAP_LN);
+#pragma unroll
+    for (int c = 1; c < 3; ++c) {  // a density below the floor steps in the density
+      if (y5[c] < L.lognf) {
+        const double dd = d5[c];
+        const double in_n = dd > -1.0 ? log1p(dd) : -CAP_LN;
+        st5[c] = clipd(in_n, -FLOOR_DROP_CAP, CAP_LN);
+      }
+    }
+    size = nanmax(size, fabs(st5[0]) * L.iVt);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const double nw = y5[c] + st5[c];
+      *W.y(bn, i, c) = nw;
+      finite = finite && isfinite(nw);
+      if (c >= 1) {
+        const double dens = exp(nw);
+        size = nanmax(size, fabs(st5[c]) * (dens / (dens + L.nfloor)));
+      }
+    }
+  }
+  size = nanmax(size, pxchg(mask, size));
+  size = nanmax(size, dl_max);
+  finite = __shfl_xor_sync(mask, finite ? 1 : 0, 1) != 0 && finite;
+#pragma unroll
+  for (int q = 0; q < K; ++q) finite = finite && isfinite(lg[q]);
+  size_out = size;
+  finite_out = finite;
+  __syncwarp(mask);  // both halves' points written before either reads the other's
+}
+
+template <int K, bool VINT, bool TW = false>
 __global__ void __launch_bounds__(32) transient_kernel(Args a) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  // one thread a device, or with TW two (the twisted sweep), half 0 the device's serial parts
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = TW ? t >> 1 : t;
+  const bool top = !TW || (t & 1) == 0;
+  const unsigned mask = TW ? (0x3u << (threadIdx.x & 30u)) : 0xffffffffu;
   if (l >= a.n) return;
   View W;
   Lane& L = W.L;
@@ -1151,7 +1540,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     logs[k] = given ? 0.0 : a.logs0[(size_t)k * Bp + l];
     logs_p[k] = logs[k];
   }
-  for (int i = 1; i <= NP; ++i) {
+  for (int i = 1; i <= NP && top; ++i) {
     const Slots sl = slots_at(L, i);
     double v5[5];
     if (given) {
@@ -1171,7 +1560,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     for (int c = 0; c < 5; ++c) { *W.y(bk, i, c) = v5[c]; *W.y(bp, i, c) = v5[c]; }
     FB[(size_t)i * Bp + l] = given ? a.init_fb[(size_t)i * Bp + l] : 0.0;
   }
-  for (int e = 0; e <= NP; ++e) FI[(size_t)e * Bp + l] = given ? a.init_fi[(size_t)e * Bp + l] : 0.0;
+  for (int e = 0; e <= NP && top; ++e)
+    FI[(size_t)e * Bp + l] = given ? a.init_fi[(size_t)e * Bp + l] : 0.0;
   const int fm = a.fmode[l];
   // the integrated current and its tangents (zero tangents before the first step)
   const bool grad = a.TY != nullptr;
@@ -1225,7 +1615,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     double num[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) num[q] = 0.0;
-    {
+    if (top) {
       double Vprev = L.V0() + 0.5 * L.left() * Vi;
       Slots slp = slots_at(L, 0);
       for (int i = 1; i <= NP + 1; ++i) {
@@ -1261,6 +1651,14 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         Vprev = V;
       }
     }
+    if constexpr (TW) {  // half 0's start to half 1: the numbers, and the points in memory
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        const double o = pxchg(mask, num[q]);
+        if (!top) num[q] = o;
+      }
+      __syncwarp(mask);
+    }
     double lg[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) {
@@ -1279,6 +1677,10 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     bool done = false, finite = true;
     while (!done && it < a.max_iter && !isnan(sh[STALL_STEPS])) {
       finite = true;  // of this iteration's new iterate
+      double size = 0.0;
+      if constexpr (TW) {
+        tw_iteration<K>(a, W, bn, Vi, dti, lg, top, mask, capV, size, finite);
+      } else {
       // -------- assembly and forward elimination
       double cpv[5][5], dpv[5][NC];
 #pragma unroll
@@ -1456,7 +1858,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       double z[KV];
       small_solve<KV>(SM, sr, z);
       // -------- the damped update (batch.py:759-785)
-      double size = 0.0, dl_max = 0.0;
+      double dl_max = 0.0;
 #pragma unroll
       for (int q = 0; q < K; ++q) {
         const double dlq = clipd(z[q], -ION_LOG_CAP, ION_LOG_CAP);
@@ -1507,8 +1909,11 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       size = nanmax(size, dl_max);
 #pragma unroll
       for (int q = 0; q < K; ++q) finite = finite && isfinite(lg[q]);
-      // -------- the current at the new iterate and the stops
-      const double J = current_t<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI);
+      }
+      // -------- the current at the new iterate (half 0's, to both) and the stops
+      double J = 0.0;
+      if (top) J = current_t<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI);
+      if constexpr (TW) J = __shfl_sync(mask, J, threadIdx.x & 30u);
 #pragma unroll
       for (int q = 0; q < STALL_STEPS; ++q) { sh[q] = sh[q + 1]; jh[q] = jh[q + 1]; }
       sh[STALL_STEPS] = size;
@@ -1531,10 +1936,11 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const bool ok = done;
     const double J = jh[STALL_STEPS];
     const double J_ext = J + L.Gshunt() * Vi;
-    if (a.prof_state) write_profile(a, W, bn, k, Vi, dti);
+    if (a.prof_state && top) write_profile(a, W, bn, k, Vi, dti);
     double err_k = 0.0;  // the step's errJ, where its convVar compares currents
-    if (a.COL || cv != 1)
+    if ((a.COL || cv != 1) && top)
       columns_t<K>(a, W, bn, Vi, bk, V_now, dti, dti_now, J, J_ext, k, cv != 1 ? &err_k : nullptr);
+    if constexpr (TW) err_k = __shfl_sync(mask, err_k, threadIdx.x & 30u);
     // ---- ZimT's main loop (transient.py:419-445)
     const bool running = stop == 0;
     const bool failed = running && !ok && (fm == 0 || (fm == 2 && track_curr == 1));
@@ -1551,7 +1957,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       };
       TP pa, pb;
       load_point(W, bn, 0, Vi, pa);
-      for (int e = 0; e <= NP; ++e) {
+      for (int e = 0; e <= NP && top; ++e) {
         load_point(W, bn, e + 1, Vi, pb);
         const int ifk = (int)L.st(e, S_IFK);
         if (ifk >= 0) {
@@ -1619,7 +2025,7 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     const bool becomes_ref = running && !failed &&
                              ((track_curr == 1 && ok) || (track_curr == 3 && (ok || fm == 1)));
     if (becomes_ref && a.REF) {
-      write_ref(a, W, bk, V_now, dti_now);
+      if (top) write_ref(a, W, bk, V_now, dti_now);
       G_ref = G_cur;
       J_ref = J_cur;
       err_ref = err_cur;
@@ -1628,13 +2034,16 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     else if (running && count >= MIN_COUNT_STATIC) stop = STOP_STATIC;
     first = false;
     const size_t o = (size_t)k * Bp + l;
-    a.J[o] = J;
-    a.Jext[o] = J_ext;
-    a.conv[o] = ok ? 1 : 0;
-    a.iters[o] = it;
-    a.acc[o] = keep ? 1 : 0;
-    if (a.Vout) a.Vout[o] = Vi;
+    if (top) {
+      a.J[o] = J;
+      a.Jext[o] = J_ext;
+      a.conv[o] = ok ? 1 : 0;
+      a.iters[o] = it;
+      a.acc[o] = keep ? 1 : 0;
+      if (a.Vout) a.Vout[o] = Vi;
+    }
   }
+  if (!top) return;  // the outputs below are half 0's
   a.stop[l] = stop;
   if (grad) {
     a.Qout[l] = Qint;
@@ -1791,8 +2200,13 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
   if (steps->vint)
     return k2 ? dd::launch(dd::tr::transient_kernel<2, true>, grid, block, 0, s, a)
               : dd::launch(dd::tr::transient_kernel<4, true>, grid, block, 0, s, a);
-  return k2 ? dd::launch(dd::tr::transient_kernel<2, false>, grid, block, 0, s, a)
-            : dd::launch(dd::tr::transient_kernel<4, false>, grid, block, 0, s, a);
+  if (out->Q)  // the gradients: one thread a device
+    return k2 ? dd::launch(dd::tr::transient_kernel<2, false>, grid, block, 0, s, a)
+              : dd::launch(dd::tr::transient_kernel<4, false>, grid, block, 0, s, a);
+  // two threads a device: the twisted sweep
+  const dim3 grid2((2 * batch->n_lanes + 31) / 32);
+  return k2 ? dd::launch(dd::tr::transient_kernel<2, false, true>, grid2, block, 0, s, a)
+            : dd::launch(dd::tr::transient_kernel<4, false, true>, grid2, block, 0, s, a);
 }
 
 }  // extern "C"
