@@ -138,8 +138,8 @@ def test_the_header_compiles_as_c():
 
 def test_the_transient_refuses_inconsistent_arguments_before_any_launch():
     """`dd_transient`'s checks, which return before any CUDA call: a start or a given state
-    half given, profiles half asked, the internal voltage an unknown without its steps' data or
-    with the gradients, columns without layers, and a workspace below its query. The pointers
+    half given, profiles half asked, the internal voltage an unknown without its steps' data,
+    columns without layers, and a workspace below its query. The pointers
     are placeholders the checks never read through."""
     import ctypes
     so = _lib.lib()
@@ -171,8 +171,6 @@ def test_the_transient_refuses_inconsistent_arguments_before_any_launch():
     assert call(init=ctypes.byref(half)) == ARGS
     assert call(o=out(prof_state=1, prof_f_bulk=1)) == ARGS  # profiles half asked
     assert call(st=steps(vint=1)) == ARGS  # the internal voltage without its steps' data
-    vint = dict(vint=1, oc=1, r_series=1, start_j_ext=1)
-    assert call(st=steps(**vint), o=out(Q=1, dQ=1)) == ARGS  # and with the gradients
     assert call(st=steps(stride=7)) == ARGS
     assert call(o=out(columns=1)) == ARGS  # columns without layers
     assert call(st=steps(n_layers=9, layers=1), o=out(columns=1)) == ARGS  # too many layers
