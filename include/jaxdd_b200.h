@@ -372,9 +372,10 @@ int dd_transient_workspace_bytes(const dd_batch* batch, size_t* bytes);
  * `start` [np_max+2][3][lane_stride] and `start_logs` [DD_MAXK][lane_stride] the steady state
  * at the first step (dd_solve_states at steps->v[0] with the generation factor
  * steps->g_frac[0] and no pre-bias), or `initial` (then start and start_logs may be NULL). opts:
- * tol, max_iter (Newton per step), bernoulli. Not
- * supported (the host refuses them): an open circuit, a series resistance, Track 2 or 3, ion
- * regions that reach a contact. */
+ * tol, max_iter (Newton per step), bernoulli. Two threads a device (the twisted sweep and the
+ * current split between them) unless the gradients (`Q`, `dQ`) or the internal voltage are
+ * asked; then one. The host refuses the internal voltage an unknown with an ion region that
+ * reaches a contact. */
 int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* steps,
                  const double* start, const double* start_logs, const dd_transient_init* initial,
                  const dd_opts* opts, const dd_transient_out* out, void* workspace,
