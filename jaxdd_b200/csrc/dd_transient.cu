@@ -163,10 +163,20 @@ struct CurK {
   bool counted[K];
 };
 
-template <int K, bool PERT = false>
+// The other half's value, and a pair's sum in one order on both halves (half 0's first).
+__device__ __forceinline__ double pxchg(unsigned mask, double v) {
+  return __shfl_xor_sync(mask, v, 1);
+}
+__device__ __forceinline__ double psum(unsigned mask, bool top, double v) {
+  const double o = pxchg(mask, v);
+  return top ? v + o : o + v;
+}
+
+template <int K, bool PERT = false, bool SPLIT = false>
 __device__ double current_t(const View& W, int cur, double Vint, int bef, double Vbef, double dti,
                             double dti_bef, const double* FB, const double* FI,
-                            const Pert* pt = nullptr, CurK<K>* ck = nullptr) {
+                            const Pert* pt = nullptr, CurK<K>* ck = nullptr, bool top = true,
+                            unsigned mask = 0u) {
   const Lane& L = W.L;
   const double mus = PERT ? pt->mus : 1.0;
   auto fb_at = [&](int k) {
@@ -207,11 +217,22 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     first_k[k] = -1;
     have[k] = false;
   }
+  // SPLIT (the twisted transient's halves): half 0 the iterations 0 .. E - 1, half 1 E .. NP
+  // after two that only carry (the capture and U, q at point E - 1, the fluxes of interval
+  // E - 1, whether a region is open at E); their sums joined after the loop
+  const int E = (NP + 1) / 2;
+  const int e0 = SPLIT && !top ? E : 0, ew = SPLIT && !top ? E - 2 : 0;
+  const int e1 = SPLIT && top ? E - 1 : NP;
+  bool first_here[K], last_here[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) { first_here[k] = false; last_here[k] = false; }
+  double Hh = 0.0;  // this half's sum of h
   TP pa, pb, qa, qb;  // pa, pb: the iterate at points e, e+1; qa, qb the state before
-  load_c(cur, 0, Vint, pa, true);
-  load_c(bef, 0, Vbef, qa, false);
+  load_c(cur, ew, Vint, pa, true);
+  load_c(bef, ew, Vbef, qa, false);
   double Ri_next[2] = {0, 0};  // interface capture at point e from the interval before it
-  for (int e = 0; e <= NP; ++e) {
+  for (int e = ew; e <= e1; ++e) {
+    const bool acc = !SPLIT || e >= e0;
     const int kb = e + 1;
     load_c(cur, kb, Vint, pb, true);
     load_c(bef, kb, Vbef, qb, false);
@@ -243,7 +264,7 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
       const double sn = s == 0 ? -1.0 : 1.0;
       const double q = exp(sn * (pa.c.V + (s == 0 ? pa.c.offn : pa.c.offp)) * L.iVt) /
                        L.st(e, s == 0 ? S_MUN : S_MUP);
-      if (e >= 1) {
+      if (e >= 1 && acc) {
         // interval e-1 (points e-1, e; e-1 <= NP-1): its trapezoid and the two sums
         const double dxm = L.st(e - 1, S_DX);
         const double iu_e = iu[s] + 0.5 * dxm * (Uprev[s] + Ue[s]);
@@ -252,9 +273,9 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
         iu[s] = iu_e;
         P[s] += sn * QL * width * Ue[s];
       }
-      bH[s] += h * P[s];
+      if (acc) bH[s] += h * P[s];
       const double through = sn * 0.5 * QL * h * (Ri_a[s] + Ri_b[s]);
-      if (ifk >= -1)  // a layer interface: the current before it plus through its traps
+      if (ifk >= -1 && acc)  // a layer interface: the current before it plus through its traps
         corr[s] += h * (through - (e >= 1 ? sn * QL * width * Ue[s] : 0.0));
       if (L.currdiff) {
         const double Vga = pa.c.V + (s == 0 ? pa.c.offn : pa.c.offp);
@@ -263,14 +284,17 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
         bern_pair(sn * (Vgb - Vga) * L.iVt, L.simss, Bf, Bb, t1, t2);
         const double da = s == 0 ? pa.c.n : pa.c.p, db = s == 0 ? pb.c.n : pb.c.p;
         Jd[s] = sn * Q * L.st(e, s == 0 ? S_MUN : S_MUP) * L.Vt * (db * Bb - da * Bf) / (L.L * h);
-        dtot += h * (ifk >= -1 ? Jd_prev[s] + through : Jd[s]);
+        if (acc) dtot += h * (ifk >= -1 ? Jd_prev[s] + through : Jd[s]);
       }
       Uprev[s] = Ue[s];
       qprev[s] = q;
     }
     Jd_prev[0] = Jd[0]; Jd_prev[1] = Jd[1];
     // the displacement current of interval e
-    disp += W.x(e, T_EPS) * ((pb.c.V - pa.c.V) - (qb.c.V - qa.c.V));
+    if (acc) {
+      disp += W.x(e, T_EPS) * ((pb.c.V - pa.c.V) - (qb.c.V - qa.c.V));
+      Hh += h;
+    }
     // the ions, region by region: exp(+-V/V_T) at the interval's two points, once
     double exa = 1.0, exb = 1.0, iexa = 1.0, iexb = 1.0;
     if (L.tot[0] > 0.0 || L.tot[K - 1] > 0.0 || (K > 2 && (L.tot[1] > 0.0 || L.tot[2] > 0.0))) {
@@ -292,17 +316,21 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
         have[k] = true;
         first_k[k] = e;
         first_v[k] = da * eva;
+        first_here[k] = acc;
       }
-      if (inb) last_v[k] = db * evb;
+      if (inb && acc) {
+        last_v[k] = db * evb;
+        last_here[k] = true;
+      }
       if (L.currdiff) {
         // each interval's flux (an interface takes the interval's before it), counted inside
         double Bf, Bb, t1, t2;
         bern_pair(sn * (pb.c.V - pa.c.V) * L.iVt, L.simss, Bf, Bb, t1, t2);
         const double Jf = sn * Q * mus * W.x(e, an ? T_MUA : T_MUC) * L.Vt * (db * Bb - da * Bf) /
                           (L.L * h);
-        if (ina && inb) isum[k] += h * (ifk >= -1 ? Jion_prev[k] : Jf);
+        if (ina && inb && acc) isum[k] += h * (ifk >= -1 ? Jion_prev[k] : Jf);
         Jion_prev[k] = Jf;
-      } else if (ina && inb) {
+      } else if (ina && inb && acc) {
         const double mua = mus * W.x(e, an ? T_MUA : T_MUC);
         const double mub = mus * W.x(kb, an ? T_MUA : T_MUC);
         const double qa2 = eva / (mua > 0.0 ? mua : 1.0);
@@ -323,6 +351,43 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     }
     pa = pb;
     qa = qb;
+  }
+  if constexpr (SPLIT) {
+  // half 1's partial sums to half 0, joined as one pass would have summed them: half 1's
+  // running integrals and prefixes began at 0, so half 0's last values shift its sums
+  const double oHh = pxchg(mask, Hh);
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const double o_single = pxchg(mask, single[s]), o_dbl = pxchg(mask, dbl[s]);
+    const double o_bH = pxchg(mask, bH[s]), o_corr = pxchg(mask, corr[s]);
+    if (top) {
+      dbl[s] = dbl[s] + (o_dbl + iu[s] * o_single);
+      bH[s] = bH[s] + (o_bH + P[s] * oHh);
+      single[s] += o_single;
+      corr[s] += o_corr;
+    }
+  }
+  {
+    const double o_dtot = pxchg(mask, dtot), o_disp = pxchg(mask, disp);
+    if (top) { dtot += o_dtot; disp += o_disp; }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double o_is = pxchg(mask, is[k]), o_idb = pxchg(mask, idb[k]);
+    const double o_iH = pxchg(mask, iH[k]), o_isum = pxchg(mask, isum[k]);
+    const double o_fv = pxchg(mask, first_v[k]), o_lv = pxchg(mask, last_v[k]);
+    const int flags = (have[k] ? 1 : 0) | (first_here[k] ? 2 : 0) | (last_here[k] ? 4 : 0);
+    const int o_flags = __shfl_xor_sync(mask, flags, 1);
+    if (top) {
+      idb[k] = idb[k] + (o_idb + iiu[k] * o_is);
+      isum[k] = isum[k] + (o_isum + iP[k] * o_iH);
+      is[k] += o_is;
+      iH[k] += o_iH;
+      if (!have[k] && (o_flags & 2)) first_v[k] = o_fv;
+      if (o_flags & 4) last_v[k] = o_lv;
+      have[k] = have[k] || (o_flags & 1);
+    }
+  }
   }
   const double H = L.Hsum();
   double tot = 0.0;
@@ -378,7 +443,9 @@ __device__ double current_t(const View& W, int cur, double Vint, int bef, double
     }
   }
   tot += dti * disp / L.L;
-  return -L.left() * tot / H;
+  const double J = -L.left() * tot / H;
+  if constexpr (SPLIT) return __shfl_sync(mask, J, threadIdx.x & 30u);  // half 0's, to both
+  return J;
 }
 
 // ------------------------------------------------------------------------------------ columns
@@ -1161,276 +1228,6 @@ __device__ __forceinline__ IonIv isel(bool t, const IonIv& x, const IonIv& y) {
   return IonIv{t ? x.F : y.F, t ? x.gx : y.gx, t ? x.da : y.da, t ? x.db : y.db};
 }
 
-// The other half's value, and a pair's sum in one order on both halves (half 0's first).
-__device__ __forceinline__ double pxchg(unsigned mask, double v) {
-  return __shfl_xor_sync(mask, v, 1);
-}
-__device__ __forceinline__ double psum(unsigned mask, bool top, double v) {
-  const double o = pxchg(mask, v);
-  return top ? v + o : o + v;
-}
-
-// The current of the iterate split between the halves (`current_t` without perturbation): half
-// 0 takes the intervals' iterations 0 .. E - 1, half 1 the rest, and their sums are joined.
-template <int K>
-__device__ double current_tw(const View& W, int cur, double Vint, int bef, double Vbef, double dti,
-                             double dti_bef, const double* FB, const double* FI, bool top,
-                             unsigned mask) {
-  constexpr bool PERT = false;
-  const Pert* pt = nullptr;
-  const Lane& L = W.L;
-  const double mus = PERT ? pt->mus : 1.0;
-  auto fb_at = [&](int k) {
-    const size_t o = (size_t)k * L.Bp + L.l;
-    return PERT && pt->tfb ? FB[o] + pt->h * pt->tfb[o] : FB[o];
-  };
-  auto fi_at = [&](int k) {
-    const size_t o = (size_t)k * L.Bp + L.l;
-    return PERT && pt->tfi ? FI[o] + pt->h * pt->tfi[o] : FI[o];
-  };
-  auto load_c = [&](int buf, int k, double Vi, TP& P, bool is_cur) {
-    if (PERT) {
-      load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k, Vi, P, is_cur ? pt->tn : 5,
-                is_cur ? pt->tf : 1);
-      if (k == 0 || k == L.NP + 1) {  // a contact's ions follow its neighbour along the tangent
-        TP nbp;
-        load_pert(W, buf, is_cur ? pt->tcur : pt->tbef, pt->h, k == 0 ? 1 : L.NP, Vi, nbp,
-                  is_cur ? pt->tn : 5, is_cur ? pt->tf : 1);
-        contact_ions(W, buf, k, is_cur ? dti : dti_bef, P, nullptr, &nbp);
-        return;
-      }
-    } else if (is_cur) load_point(W, buf, k, Vi, P);
-    else load_before(W, buf, k, Vi, P);
-    contact_ions(W, buf, k, is_cur ? dti : dti_bef, P);
-  };
-  const int NP = L.NP;
-  const double QL = Q * L.L;
-  double single[2] = {0, 0}, dbl[2] = {0, 0}, iu[2] = {0, 0}, P[2] = {0, 0}, bH[2] = {0, 0};
-  double corr[2] = {0, 0}, dtot = 0.0, disp = 0.0;
-  double Uprev[2] = {0, 0}, qprev[2] = {0, 0}, Jd_prev[2] = {0, 0};
-  double is[K], idb[K], iiu[K], iP[K], iH[K], isum[K], first_v[K], last_v[K], Jion_prev[K];
-  int first_k[K];
-  bool have[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    is[k] = idb[k] = iiu[k] = iP[k] = iH[k] = isum[k] = first_v[k] = last_v[k] = 0.0;
-    Jion_prev[k] = 0.0;
-    first_k[k] = -1;
-    have[k] = false;
-  }
-  // half 0 the iterations 0 .. E - 1, half 1 E .. NP after two that only carry (the capture
-  // and U, q at point E - 1, the fluxes of interval E - 1, whether a region is open at E)
-  const int E = (NP + 1) / 2;
-  const int e0 = top ? 0 : E, ew = top ? 0 : E - 2, e1 = top ? E - 1 : NP;
-  bool first_here[K], last_here[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) { first_here[k] = false; last_here[k] = false; }
-  double Hh = 0.0;  // this half's sum of h
-  TP pa, pb, qa, qb;  // pa, pb: the iterate at points e, e+1; qa, qb the state before
-  load_c(cur, ew, Vint, pa, true);
-  load_c(bef, ew, Vbef, qa, false);
-  double Ri_next[2] = {0, 0};  // interface capture at point e from the interval before it
-  for (int e = ew; e <= e1; ++e) {
-    const bool acc = e >= e0;
-    const int kb = e + 1;
-    load_c(cur, kb, Vint, pb, true);
-    load_c(bef, kb, Vbef, qb, false);
-    const double h = L.st(e, S_H), dx = L.st(e, S_DX);
-    const int ifk = (int)L.st(e, S_IFK);
-    double tRL[2] = {0, 0}, tRR[2] = {0, 0};
-    if (ifk >= 0) {
-      Iface t;
-      iface_edge_t(L, ifk, pa.c.n, pb.c.n, pa.c.p, pb.c.p, fi_at(e), dti, t, false, nullptr);
-      tRL[0] = t.v[0]; tRR[0] = t.v[1]; tRL[1] = t.v[2]; tRR[1] = t.v[3];
-    }
-    // interface capture at points e and e+1 (point e+1's share of interval e+1 is 0: no two
-    // trapped interfaces are neighbours)
-    const double Ri_a[2] = {Ri_next[0] + tRL[0], Ri_next[1] + tRL[1]};
-    const double Ri_b[2] = {tRR[0], tRR[1]};
-    double Ue[2] = {0, 0};  // point e's U (0 on the contacts)
-    if (e >= 1) {
-      double Rn, Rp, d0, d1, d2, d3;
-      bulk_rates(L, e, pa.c.n, pa.c.p, fb_at(e), dti, Rn, Rp, d0, d1, d2, d3);
-      const double G = L.st(e, S_G) * L.gfrac;
-      Ue[0] = Rn + Ri_a[0] - G + dti * (pa.c.n - qa.c.n);
-      Ue[1] = Rp + Ri_a[1] - G + dti * (pa.c.p - qa.c.p);
-    }
-    Ri_next[0] = Ri_b[0]; Ri_next[1] = Ri_b[1];
-    const double width = W.zimt ? h : (e == 0 ? h : 0.5 * (L.st(e - 1, S_H) + h));
-    double Jd[2] = {0, 0};
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const double sn = s == 0 ? -1.0 : 1.0;
-      const double q = exp(sn * (pa.c.V + (s == 0 ? pa.c.offn : pa.c.offp)) * L.iVt) /
-                       L.st(e, s == 0 ? S_MUN : S_MUP);
-      if (e >= 1 && acc) {
-        // interval e-1 (points e-1, e; e-1 <= NP-1): its trapezoid and the two sums
-        const double dxm = L.st(e - 1, S_DX);
-        const double iu_e = iu[s] + 0.5 * dxm * (Uprev[s] + Ue[s]);
-        single[s] += 0.5 * dxm * (qprev[s] + q);
-        dbl[s] += 0.5 * dxm * (qprev[s] * iu[s] + q * iu_e);
-        iu[s] = iu_e;
-        P[s] += sn * QL * width * Ue[s];
-      }
-      if (acc) bH[s] += h * P[s];
-      const double through = sn * 0.5 * QL * h * (Ri_a[s] + Ri_b[s]);
-      if (ifk >= -1 && acc)  // a layer interface: the current before it plus through its traps
-        corr[s] += h * (through - (e >= 1 ? sn * QL * width * Ue[s] : 0.0));
-      if (L.currdiff) {
-        const double Vga = pa.c.V + (s == 0 ? pa.c.offn : pa.c.offp);
-        const double Vgb = pb.c.V + (s == 0 ? pb.c.offn : pb.c.offp);
-        double Bf, Bb, t1, t2;
-        bern_pair(sn * (Vgb - Vga) * L.iVt, L.simss, Bf, Bb, t1, t2);
-        const double da = s == 0 ? pa.c.n : pa.c.p, db = s == 0 ? pb.c.n : pb.c.p;
-        Jd[s] = sn * Q * L.st(e, s == 0 ? S_MUN : S_MUP) * L.Vt * (db * Bb - da * Bf) / (L.L * h);
-        if (acc) dtot += h * (ifk >= -1 ? Jd_prev[s] + through : Jd[s]);
-      }
-      Uprev[s] = Ue[s];
-      qprev[s] = q;
-    }
-    Jd_prev[0] = Jd[0]; Jd_prev[1] = Jd[1];
-    // the displacement current of interval e
-    if (acc) {
-      disp += W.x(e, T_EPS) * ((pb.c.V - pa.c.V) - (qb.c.V - qa.c.V));
-      Hh += h;
-    }
-    // the ions, region by region: exp(+-V/V_T) at the interval's two points, once
-    double exa = 1.0, exb = 1.0, iexa = 1.0, iexb = 1.0;
-    if (L.tot[0] > 0.0 || L.tot[K - 1] > 0.0 || (K > 2 && (L.tot[1] > 0.0 || L.tot[2] > 0.0))) {
-      exa = exp(pa.c.V * L.iVt); exb = exp(pb.c.V * L.iVt);
-      iexa = 1.0 / exa; iexb = 1.0 / exb;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if (!(L.tot[k] > 0.0)) continue;
-      const bool an = k < L.ka;
-      const int sk = an ? k : k - L.ka;
-      const double sn = an ? -1.0 : 1.0;
-      const bool ina = (an ? pa.c.sl.a : pa.c.sl.c) == sk;
-      const bool inb = (an ? pb.c.sl.a : pb.c.sl.c) == sk;
-      const double da = an ? pa.a : pa.c2, db = an ? pb.a : pb.c2;
-      const double qa_ = an ? qa.a : qa.c2, qb_ = an ? qb.a : qb.c2;
-      const double eva = an ? iexa : exa, evb = an ? iexb : exb;
-      if (ina && !have[k]) {
-        have[k] = true;
-        first_k[k] = e;
-        first_v[k] = da * eva;
-        first_here[k] = acc;
-      }
-      if (inb && acc) {
-        last_v[k] = db * evb;
-        last_here[k] = true;
-      }
-      if (L.currdiff) {
-        // each interval's flux (an interface takes the interval's before it), counted inside
-        double Bf, Bb, t1, t2;
-        bern_pair(sn * (pb.c.V - pa.c.V) * L.iVt, L.simss, Bf, Bb, t1, t2);
-        const double Jf = sn * Q * mus * W.x(e, an ? T_MUA : T_MUC) * L.Vt * (db * Bb - da * Bf) /
-                          (L.L * h);
-        if (ina && inb && acc) isum[k] += h * (ifk >= -1 ? Jion_prev[k] : Jf);
-        Jion_prev[k] = Jf;
-      } else if (ina && inb && acc) {
-        const double mua = mus * W.x(e, an ? T_MUA : T_MUC);
-        const double mub = mus * W.x(kb, an ? T_MUA : T_MUC);
-        const double qa2 = eva / (mua > 0.0 ? mua : 1.0);
-        const double qb2 = evb / (mub > 0.0 ? mub : 1.0);
-        const double Ua = dti * (da - qa_), Ub = dti * (db - qb_);
-        // the ions' trapezoids take every interval, the last one (to the right contact) too
-        const double dxi = e < NP ? dx : h * L.L;
-        const double iu_b = iiu[k] + 0.5 * dxi * (Ua + Ub);
-        is[k] += 0.5 * dxi * (qa2 + qb2);
-        idb[k] += 0.5 * dxi * (qa2 * iiu[k] + qb2 * iu_b);
-        iiu[k] = iu_b;
-        // J_e = qK + the prefix of the steps; at an interface the interval's before it
-        const double stp = e > first_k[k] ? sn * QL * width * Ua : 0.0;
-        iP[k] += stp;
-        iH[k] += h;
-        isum[k] += h * (iP[k] - (ifk >= -1 ? stp : 0.0));
-      }
-    }
-    pa = pb;
-    qa = qb;
-  }
-  // half 1's partial sums to half 0, joined as one pass would have summed them: half 1's
-  // running integrals and prefixes began at 0, so half 0's last values shift its sums
-  const double oHh = pxchg(mask, Hh);
-#pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    const double o_single = pxchg(mask, single[s]), o_dbl = pxchg(mask, dbl[s]);
-    const double o_bH = pxchg(mask, bH[s]), o_corr = pxchg(mask, corr[s]);
-    if (top) {
-      dbl[s] = dbl[s] + (o_dbl + iu[s] * o_single);
-      bH[s] = bH[s] + (o_bH + P[s] * oHh);
-      single[s] += o_single;
-      corr[s] += o_corr;
-    }
-  }
-  {
-    const double o_dtot = pxchg(mask, dtot), o_disp = pxchg(mask, disp);
-    if (top) { dtot += o_dtot; disp += o_disp; }
-  }
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const double o_is = pxchg(mask, is[k]), o_idb = pxchg(mask, idb[k]);
-    const double o_iH = pxchg(mask, iH[k]), o_isum = pxchg(mask, isum[k]);
-    const double o_fv = pxchg(mask, first_v[k]), o_lv = pxchg(mask, last_v[k]);
-    const int flags = (have[k] ? 1 : 0) | (first_here[k] ? 2 : 0) | (last_here[k] ? 4 : 0);
-    const int o_flags = __shfl_xor_sync(mask, flags, 1);
-    if (top) {
-      idb[k] = idb[k] + (o_idb + iiu[k] * o_is);
-      isum[k] = isum[k] + (o_isum + iP[k] * o_iH);
-      is[k] += o_is;
-      iH[k] += o_iH;
-      if (!have[k] && (o_flags & 2)) first_v[k] = o_fv;
-      if (o_flags & 4) last_v[k] = o_lv;
-      have[k] = have[k] || (o_flags & 1);
-    }
-  }
-  const double H = L.Hsum();
-  double tot = 0.0;
-  // ZimT 5.36's ion currents with several regions: each species' last region's alone
-  int last_a = -1, last_c = -1;
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-    if (L.tot[k] > 0.0) {
-      if (k < L.ka) last_a = k;
-      else last_c = k;
-    }
-  if (!L.currdiff) {
-    Pt c0, cN;
-    contact(L, 0, Vint, c0);
-    contact(L, 1, Vint, cN);
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const double sn = s == 0 ? -1.0 : 1.0;
-      const double off0 = L.st(0, s == 0 ? S_OFFN : S_OFFP);
-      const double offN = L.st(NP + 1, s == 0 ? S_OFFN : S_OFFP);
-      const double d0 = exp(s == 0 ? c0.lnn : c0.lnp), dN = exp(s == 0 ? cN.lnn : cN.lnp);
-      const double Kc = (L.Vt * (sn * dN * exp(sn * (cN.V + offN) * L.iVt) -
-                                 sn * d0 * exp(sn * (c0.V + off0) * L.iVt)) - sn * dbl[s]) /
-                        single[s];
-      tot += Q * Kc * H + bH[s] + corr[s];
-    }
-  } else {
-    tot = dtot;
-  }
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    if (!(L.tot[k] > 0.0) || !have[k]) continue;
-    if (W.ion_last && k != (k < L.ka ? last_a : last_c)) continue;
-    const double sn = k < L.ka ? -1.0 : 1.0;
-    if (!L.currdiff) {
-      const double sgl = is[k] > 0.0 ? is[k] : 1.0;
-      const double Kc = (L.Vt * sn * (last_v[k] - first_v[k]) - sn * idb[k]) / sgl;
-      tot += Q * Kc * iH[k] + isum[k];
-    } else {
-      tot += isum[k];
-    }
-  }
-  tot += dti * disp / L.L;
-  return __shfl_sync(mask, -L.left() * tot / H, threadIdx.x & 30u);  // half 0's, to both
-}
-
 // Each region's number over edge e (points lo = e, hi = e + 1), as the forward pass sums it.
 template <int K>
 __device__ __forceinline__ void tw_number(const Lane& L, const TP& lo, const TP& hi, int e,
@@ -2173,8 +1970,8 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
       }
       // -------- the current at the new iterate (half 0's, to both) and the stops
       double J = 0.0;
-      if constexpr (TW) J = current_tw<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI, top, mask);
-      else J = current_t<K>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI);
+      J = current_t<K, false, TW>(W, bn, Vi, bk, V_now, dti, dti_now, FB, FI, nullptr, nullptr,
+                                  top, mask);
 #pragma unroll
       for (int q = 0; q < STALL_STEPS; ++q) { sh[q] = sh[q + 1]; jh[q] = jh[q + 1]; }
       sh[STALL_STEPS] = size;
