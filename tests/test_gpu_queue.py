@@ -86,3 +86,66 @@ def test_the_autotuner_times_every_form_and_keeps_the_curves():
     after = solve_batch(b, V_SCAN)
     for x, y in zip(ref, after):
         assert np.array_equal(x, y, equal_nan=True)
+
+
+def test_a_solve_captured_in_a_cuda_graph_replays_the_direct_launch():
+    """`dd_solve` (the queue counter's reset, the specialised and the generic kernel) captured
+    once into a CUDA graph, as `bench.py` replays config 3's solve: each replay gives the direct
+    launch's curves, flags and iterations bit for bit, also after the outputs were overwritten
+    between replays, on uneven grids and voltage lists."""
+    from jaxdd_b200.batch import descriptor, _gpu
+    from jaxdd_b200.workloads import ragged_plan, ragged_voltages
+    idx = np.arange(64)
+    _, Nvs = ragged_plan(idx)
+    devs = drawn_devices(64, NP=(60, 160))
+    batch = prepare(devs, ragged=True)
+    lists = [ragged_voltages(nv) for nv in Nvs]
+    g = _gpu(batch)
+    Bp, npmax, lanes = batch["Bp"], batch["np_max"], batch["lane_of"]
+    from jaxdd_b200.batch import initial_state
+    y0 = np.zeros((npmax + 2, 3, Bp))
+    counts = np.zeros(Bp, dtype=np.int32)
+    for k, d in enumerate(devs):
+        first = d.V_pre if d.pre_cond else lists[k][0]
+        y0[:len(d.x), :, lanes[k]] = initial_state(d, first)
+        counts[lanes[k]] = len(lists[k])
+    offsets = np.zeros(Bp, dtype=np.int32)
+    offsets[1:] = np.cumsum(counts)[:-1]
+    flat = np.zeros(int(counts.sum()))
+    for k in range(len(devs)):
+        flat[offsets[lanes[k]]:offsets[lanes[k]] + counts[lanes[k]]] = lists[k]
+    cuda = torch.device("cuda")
+    t_y0 = torch.from_numpy(y0).to(cuda)
+    t_v, t_off, t_cnt = (torch.from_numpy(a).to(cuda) for a in (flat, offsets, counts))
+    J = torch.empty(flat.size, dtype=torch.float64, device=cuda)
+    ok = torch.empty(flat.size, dtype=torch.uint8, device=cuda)
+    its = torch.empty(flat.size, dtype=torch.int32, device=cuda)
+    status = torch.empty(Bp, dtype=torch.int32, device=cuda)
+    steps = torch.zeros((3, Bp), dtype=torch.int32, device=cuda)
+    desc = descriptor(batch, g, t_y0)
+    volts = _lib.DdVoltages(t_v.data_ptr(), t_off.data_ptr(), t_cnt.data_ptr())
+    opts = _lib.DdOpts(1e-10, 60, 60, 0, 0, _lib.DD_MODE_BATCH, 0, 0)
+    ws = g.workspace(desc)
+    so = _lib.lib()
+
+    def launch(stream):
+        _lib.check(so.dd_solve(ctypes.byref(desc), ctypes.byref(volts), ctypes.byref(opts),
+                               J.data_ptr(), ok.data_ptr(), its.data_ptr(), status.data_ptr(),
+                               steps.data_ptr(), ws.data_ptr(), ws.numel(), stream.cuda_stream),
+                   "dd_solve")
+
+    launch(torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    direct = [t.cpu().numpy().copy() for t in (J, ok, its)]
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+        launch(torch.cuda.current_stream())
+    for _ in range(2):
+        J.fill_(float("nan"))
+        ok.zero_()
+        its.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        for a, b in zip(direct, (J, ok, its)):
+            np.testing.assert_array_equal(a, b.cpu().numpy())
+    assert direct[1].all()
