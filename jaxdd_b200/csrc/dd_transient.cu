@@ -1673,10 +1673,18 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
     double num[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) num[q] = 0.0;
-    if (top) {
+    {
+      // with TW half 0 points 1 .. m, half 1 m + 1 .. NP + 1 (the point before its first
+      // extrapolated again for the numbers' trapezoid)
+      const int mh = NP / 2;
+      const int lo = TW && !top ? mh + 1 : 1, hi = TW && top ? mh : NP + 1;
       double Vprev = L.V0() + 0.5 * L.left() * Vi;
-      Slots slp = slots_at(L, 0);
-      for (int i = 1; i <= NP + 1; ++i) {
+      if (lo > 1) {
+        const double y = *W.y(bk, lo - 1, 0), yp = *W.y(bp, lo - 1, 0);
+        Vprev = y + clipd(rt * (y - yp), -capV, capV);
+      }
+      Slots slp = slots_at(L, lo - 1);
+      for (int i = lo; i <= hi; ++i) {
         double V;
         if (i <= NP) {
 #pragma unroll
@@ -1709,12 +1717,9 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         Vprev = V;
       }
     }
-    if constexpr (TW) {  // half 0's start to half 1: the numbers, and the points in memory
+    if constexpr (TW) {  // both halves' numbers, added in one order; the points in memory
 #pragma unroll
-      for (int q = 0; q < K; ++q) {
-        const double o = pxchg(mask, num[q]);
-        if (!top) num[q] = o;
-      }
+      for (int q = 0; q < K; ++q) num[q] = psum(mask, top, num[q]);
       __syncwarp(mask);
     }
     double lg[K];
@@ -2013,9 +2018,14 @@ __global__ void __launch_bounds__(32) transient_kernel(Args a) {
         return (k < 1 || k > NP) ? 0.0
                                  : a.TY[((((size_t)(p * 2 + 1 - tb)) * tnodes + k) * 5 + c) * Bp + l];
       };
+      // the traps' occupations at the step's end: with TW half 0 intervals 0 .. m - 1 (points
+      // 1 .. m), half 1 the rest, after half 0's reads of the old ones (profile, columns)
+      if constexpr (TW) __syncwarp(mask);
+      const int mh = NP / 2;
+      const int e_lo = TW && !top ? mh : 0, e_hi = TW && top ? mh - 1 : NP;
       TP pa, pb;
-      load_point(W, bn, 0, Vi, pa);
-      for (int e = 0; e <= NP && top; ++e) {
+      load_point(W, bn, e_lo, Vi, pa);
+      for (int e = e_lo; e <= e_hi; ++e) {
         load_point(W, bn, e + 1, Vi, pb);
         const int ifk = (int)L.st(e, S_IFK);
         if (ifk >= 0) {
