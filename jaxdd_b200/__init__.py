@@ -13,14 +13,15 @@ from .batch import (Batch, external_voltages, prepare, solve_batch, solve_states
 from .device import Device, build_device, layer_points, make_grid
 from .simss_input import (TVG, Layer, Setup, check_supported, read_setup, read_tvg,
                           setup_from_texts, simss_voltages)
-from .solver import JVResult, solve_jv
+from .solver import JVResult, StateResult, solve_jv, solve_state
 from .transient import TransientResult, TransientState, solve_transient
 
 __version__ = "0.1.0"
 
 __all__ = [
-    "Batch", "Device", "JVResult", "Layer", "Setup", "TVG", "TransientResult", "TransientState",
-    "build_device", "check_supported", "external_voltages", "layer_points", "make_grid",
-    "prepare", "read_setup", "read_tvg", "setup_from_texts", "simss_voltages", "solve_batch",
-    "solve_jv", "solve_states", "solve_transient", "solve_uneven", "tune",
+    "Batch", "Device", "JVResult", "Layer", "Setup", "StateResult", "TVG", "TransientResult",
+    "TransientState", "build_device", "check_supported", "external_voltages", "layer_points",
+    "make_grid", "prepare", "read_setup", "read_tvg", "setup_from_texts", "simss_voltages",
+    "solve_batch", "solve_jv", "solve_state", "solve_states", "solve_transient", "solve_uneven",
+    "tune",
 ]

@@ -38,6 +38,7 @@ class Plan:
     max_iter: int = 60
     bernoulli: str = "exact"
     strict: bool = False
+    mode: int = _lib.DD_MODE_BATCH  # DD_MODE_JV: solve_jv's scan (`solver.solve_state`)
 
 
 def plan(batch: Batch, voltages, tol: float = 1e-10, max_iter: int = 60,
@@ -83,11 +84,12 @@ def _desc(p: Plan, stat, scal, iface):
 
 def _opts(p: Plan):
     return _lib.DdOpts(float(p.tol), int(p.max_iter), int(p.max_iter), int(bool(p.strict)),
-                       _lib.DD_BERNOULLI[p.bernoulli], _lib.DD_MODE_BATCH, 0, 0)
+                       _lib.DD_BERNOULLI[p.bernoulli], p.mode, 0, 0)
 
 
 def solve_states(p: Plan, stat, scal, iface):
-    """The curves and the checkpoints: `(J, ok, its, ckpt)`, J/ok/its flat in lane order."""
+    """The curves and the checkpoints: `(J, ok, its, ckpt)`, J/ok/its flat in lane order;
+    `ckpt["status"]` each lane's status (`DD_LANE_*`)."""
     import torch
     b = p.batch
     cuda = stat.device
@@ -117,6 +119,7 @@ def solve_states(p: Plan, stat, scal, iface):
         its.data_ptr(), status.data_ptr(), None, ckpt["states"].data_ptr(),
         ckpt["logs"].data_ptr(), ckpt["pre"].data_ptr(), ckpt["pre_logs"].data_ptr(), p.nv_max,
         ws.data_ptr(), ws.numel(), stream), "dd_solve_states")
+    ckpt["status"] = status
     return J, ok, its, ckpt
 
 

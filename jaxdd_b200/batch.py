@@ -425,7 +425,6 @@ def solve_states(batch: Batch, voltages=0.0, tol: float = 1e-10, max_iter: int =
     `solve_batch` (one pass at `max_iter`, which gives jaxdd's two passes' results); the
     states are the checkpoints of `dd_solve_states`, the profiles and measures those of
     `dd_observables`. One grid size per batch, as jaxdd's `prepare` has it."""
-    import torch
     from .adjoint import plan as _plan
     from .adjoint import solve_states as _solve_states
     del first_max_iter, devices
@@ -438,10 +437,27 @@ def solve_states(batch: Batch, voltages=0.0, tol: float = 1e-10, max_iter: int =
     p = _plan(batch, vs, tol=tol, max_iter=max_iter, bernoulli_name=bernoulli_name,
               strict=strict)
     g = _gpu(batch)
-    rec = (g.stat, g.scal, g.iface)
-    J, ok, its, ckpt = _solve_states(p, *rec)
+    J, ok, its, ckpt = _solve_states(p, g.stat, g.scal, g.iface)
+    prof, meas = observables(batch, p, ckpt)
+    lanes = batch["lane_of"]
+    offsets = p.offsets.cpu().numpy()
+    Jd, okd, itd = _gather(batch, J, ok, its, offsets, p.nv_max, inv)
+    out = {k: np.transpose(v.cpu().numpy()[:, :, lanes], (2, 0, 1))[:, inv]
+           for k, v in prof.items()}
+    out.update({k: v.cpu().numpy()[:, lanes].T[:, inv] for k, v in meas.items()})
+    out.update({"J": Jd, "converged": okd, "iterations": itd})
+    return out
+
+
+def observables(batch: Batch, p, ckpt) -> tuple[dict, dict]:
+    """`dd_observables` of the checkpoints `ckpt` that `dd_solve_states` wrote for the plan `p`
+    (`adjoint.Plan`): the profiles `V`, `n`, `p`, `qfls`, `anion`, `cation` (voltages x NP + 2 x
+    lanes) and the measures `implied_voc`, `plqy` (voltages x lanes), device tensors in lane
+    order, the stream synchronised."""
+    import torch
+    g = _gpu(batch)
     nv, nodes, Bp = p.nv_max, batch["np_max"] + 2, batch["Bp"]
-    cuda = J.device
+    cuda = p.v.device
     prof = {k: torch.empty((nv, nodes, Bp), dtype=torch.float64, device=cuda)
             for k in ("V", "n", "p", "qfls", "anion", "cation")}
     meas = {k: torch.empty((nv, Bp), dtype=torch.float64, device=cuda)
@@ -455,14 +471,7 @@ def solve_states(batch: Batch, voltages=0.0, tol: float = 1e-10, max_iter: int =
         meas["implied_voc"].data_ptr(), meas["plqy"].data_ptr(),
         torch.cuda.current_stream(cuda).cuda_stream), "dd_observables")
     torch.cuda.synchronize()
-    lanes = batch["lane_of"]
-    offsets = p.offsets.cpu().numpy()
-    Jd, okd, itd = _gather(batch, J, ok, its, offsets, nv, inv)
-    out = {k: np.transpose(v.cpu().numpy()[:, :, lanes], (2, 0, 1))[:, inv]
-           for k, v in prof.items()}
-    out.update({k: v.cpu().numpy()[:, lanes].T[:, inv] for k, v in meas.items()})
-    out.update({"J": Jd, "converged": okd, "iterations": itd})
-    return out
+    return prof, meas
 
 
 def _gather(batch, J, ok, its, offsets, nv, inv):

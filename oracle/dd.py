@@ -977,11 +977,12 @@ def _initial_jv(dev, Vint):
     return np.stack([V, np.log(n), np.log(p)], -1)
 
 
-def solve_jv(dev, voltages, g_frac=None, tol=1e-10, max_iter=200, bernoulli_name="exact"):
-    """solver.solve_jv / _scan (solver.py:2041-2060, 2105-2245): each voltage in the caller's
-    order from the last converged solution. Returns `(J, converged, iterations)`; raises
-    `RuntimeError` where the pre-bias does not converge."""
-    bern = BERNOULLI[bernoulli_name]
+def _scan_jv(dev, voltages, g_frac, tol, max_iter, bern):
+    """solver._scan (solver.py:2105-2245): the start, the pre-bias and its freeze, then each
+    voltage in the caller's order from the last converged solution. Yields per voltage
+    `(Vint, y, logs, converged, iterations, dz)`: the final iterate (even where Newton did not
+    converge) and the tree it was solved in (after any freeze). Raises `RuntimeError` where the
+    pre-bias does not converge."""
     d = prepare([dev])
     if g_frac is not None:
         d["g_frac"] = np.array([float(g_frac)])
@@ -1023,14 +1024,41 @@ def solve_jv(dev, voltages, g_frac=None, tol=1e-10, max_iter=200, bernoulli_name
         if dev.fix_ions:
             s, ion = freeze(d["s"], d["ion"], y, logs, d["Vt"], np.array([True]))
             dz = _with(d, s, ion)
-    J, conv, its = [], [], []
     for Vint in voltages:
         y_new, logs_new, ok, it = _settle(y, logs, dz, float(Vint), bern, tol, max_iter)
         full = full_of(bounds(dz, np.array([float(Vint)])), y_new)
         if ok and np.isfinite(full).all() and np.isfinite(logs_new).all():
             y, logs = y_new, logs_new
-        Jv = float(current(dz, full, bern)[0])
-        J.append(Jv + (float(Vint) / dev.R_shunt if dev.R_shunt > 0 else 0.0))
+        yield float(Vint), y_new, logs_new, ok, it, dz
+
+
+def solve_jv(dev, voltages, g_frac=None, tol=1e-10, max_iter=200, bernoulli_name="exact"):
+    """solver.solve_jv (solver.py:2041-2060) over `_scan_jv`: each voltage in the caller's order
+    from the last converged solution. Returns `(J, converged, iterations)`; raises
+    `RuntimeError` where the pre-bias does not converge."""
+    bern = BERNOULLI[bernoulli_name]
+    J, conv, its = [], [], []
+    for Vint, y, _, ok, it, dz in _scan_jv(dev, voltages, g_frac, tol, max_iter, bern):
+        Jv = float(current(dz, full_of(bounds(dz, np.array([Vint])), y), bern)[0])
+        J.append(Jv + (Vint / dev.R_shunt if dev.R_shunt > 0 else 0.0))
         conv.append(ok)
         its.append(it)
     return np.array(J), np.array(conv), np.array(its)
+
+
+def solve_state(dev, Vint=0.0, g_frac=None, tol=1e-10, max_iter=200, bernoulli_name="exact"):
+    """solver.solve_state (solver.py:2063-2093) in this scope (Boltzmann statistics, contacts of
+    infinite surface recombination, no field-dependent rates): `_scan_jv` at the one voltage
+    `Vint`, its state on all NP + 2 points and what photoluminescence measures of it
+    (`observed`). A dict of `x, V, n, p, qfls, anion, cation` (NP + 2), `implied_voc`, `plqy`,
+    `J` (`_current`: without the shunt's current, as jaxdd's `solve_state` has it),
+    `converged`, `iterations`."""
+    bern = BERNOULLI[bernoulli_name]
+    (Vint, y, logs, ok, it, dz), = _scan_jv(dev, [Vint], g_frac, tol, max_iter, bern)
+    full, voc, plqy, ions = observed(dz, y, logs, np.array([Vint]))
+    n, p = np.exp(full[0, :, 1]), np.exp(full[0, :, 2])
+    return {"x": np.asarray(dev.x), "V": full[0, :, 0], "n": n, "p": p,
+            "qfls": dev.Vt * np.log(n * p / dev.ni ** 2), "implied_voc": float(voc[0]),
+            "plqy": float(plqy[0]), "J": float(current(dz, full, bern)[0]),
+            "anion": ions[0, :, 0], "cation": ions[0, :, 1], "converged": bool(ok),
+            "iterations": int(it)}

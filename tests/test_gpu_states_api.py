@@ -35,3 +35,39 @@ def test_states_match_the_oracle():
     ni2 = np.array([d.ni ** 2 for d in devs])[:, None, :]
     Vt = np.array([d.Vt for d in devs])[:, None, None]
     assert np.allclose(got["qfls"], Vt * np.log(got["n"] * got["p"] / ni2), rtol=0, atol=1e-12)
+
+
+def test_one_state_matches_the_oracle():
+    """`solve_state` (jaxdd solver.py:2063-2093) on the GPU, solve_jv's scan at one voltage,
+    against the oracle's restatement: the SimSS cell of `none_light` (NP 400), the p-i-n cell and
+    a frozen and a free-ion drawn device (NP 120), at 0 and 0.8 V and at half the generation:
+    converged as the oracle, J within 1e-6 of the current scale and without the shunt's current,
+    the potential, ions and radiative measures to the bars of the batch test above, the
+    densities and their splitting there where Newton weighs them (above its floor, as the
+    reference compares states: tests/test_free_surface.py:290-310)."""
+    from jaxdd_b200 import StateResult, build_device, read_setup, solve_state
+    from jaxdd_b200.workloads import pin_stack
+    from conftest import GOLDEN
+    cell = build_device(read_setup(GOLDEN / "inputs" / "none_light" / "simulation_setup.txt"))
+    cases = [(d, V, None) for d in [cell, pin_stack(NP=120)] + drawn_devices(2, NP=120)
+             for V in (0.0, 0.8)] + [(cell, 0.0, 0.5)]
+    for d, V, g in cases:
+        got = solve_state(d, V, g_frac=g)
+        ref = dd.solve_state(d, V, g_frac=g)
+        assert isinstance(got, StateResult)
+        assert got.converged and ref["converged"]
+        assert np.array_equal(got.x, ref["x"])
+        scale = float(dd.prepare([d])["J_scale"][0])
+        assert abs(got.J - ref["J"]) < 1e-6 * scale, (got.J, ref["J"])
+        assert np.max(np.abs(got.V - ref["V"])) < 1e-8
+        floor = 1e-12 * np.max(d.N_c)
+        weighed = (ref["n"] > floor) & (ref["p"] > floor)
+        for key in ("n", "p", "anion", "cation"):
+            a, b = getattr(got, key), ref[key]
+            assert a.shape == b.shape == (len(d.x),)
+            w = b > floor if key in ("n", "p") else np.ones(len(b), bool)
+            assert np.max(np.abs(a - b)[w] / np.maximum(np.abs(b[w]), 1e-30)) < 1e-6, key
+        assert np.max(np.abs(got.qfls - ref["qfls"])[weighed]) < 1e-8
+        assert np.allclose(got.qfls, d.Vt * np.log(got.n * got.p / d.ni ** 2), rtol=0, atol=1e-12)
+        assert abs(got.implied_voc - ref["implied_voc"]) < 1e-9
+        assert abs(got.plqy / ref["plqy"] - 1) < 1e-6

@@ -175,3 +175,16 @@ def test_the_transient_refuses_inconsistent_arguments_before_any_launch():
     assert call(o=out(columns=1)) == ARGS  # columns without layers
     assert call(st=steps(n_layers=9, layers=1), o=out(columns=1)) == ARGS  # too many layers
     assert call(bytes_=ws - 1) == WORKSPACE
+
+
+def test_the_solvers_refuse_without_a_gpu():
+    """No CPU fallback: without a CUDA GPU the one-device solvers raise before any solve."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from jaxdd_b200 import solve_jv, solve_state
+    dev = build_device(read_setup(GOLDEN / "inputs" / "thin_l1_light" / "simulation_setup.txt"))
+    with pytest.raises(RuntimeError, match="needs a CUDA GPU"):
+        solve_state(dev, 0.0)
+    with pytest.raises(RuntimeError, match="needs a CUDA GPU"):
+        solve_jv(dev, [0.0, 0.5])

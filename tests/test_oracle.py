@@ -140,3 +140,35 @@ def test_states_restatement_is_consistent_with_the_curves():
     assert np.all(np.isfinite(st["implied_voc"])) and np.all((st["plqy"] > 0) & (st["plqy"] < 1))
     # the ions at the boundary points are their neighbours'
     assert np.array_equal(st["anion"][..., 0], st["anion"][..., 1])
+
+
+def test_state_restatement_is_each_devices_batch_state():
+    """`solve_state` (solver.py:2063-2093) restated: as the reference checks it against
+    `solve_states` (tests/test_free_surface.py:290-310), each device's implied V_oc to 1e-8 V,
+    its PLQY to 1e-7 and its densities to 1e-7 where Newton weighs them (above its floor), for
+    the SimSS cell of `none_light`, the p-i-n cell and a frozen and a free-ion drawn device, at
+    0 and 0.8 V; its current is `solve_jv`'s at the same voltage less the shunt's, which pins it
+    on SimSS's curve through `test_oracle_reproduces_simss`; and a generation factor scales the
+    generation as `solve_jv`'s does."""
+    from jaxdd_b200.workloads import drawn_devices, pin_stack
+    cell = build_device(read_setup(GOLDEN / "inputs" / "none_light" / "simulation_setup.txt"))
+    devs = [cell, pin_stack(NP=120)] + drawn_devices(2, NP=120)
+    for d in devs:
+        for V in (0.0, 0.8):
+            s = dd.solve_state(d, V)
+            b = dd.solve_states(dd.prepare([d]), V)
+            assert s["converged"] and b["converged"][0, 0]
+            assert s["V"].shape == s["n"].shape == s["anion"].shape == (len(d.x),)
+            assert abs(b["implied_voc"][0, 0] - s["implied_voc"]) < 1e-8
+            assert abs(b["plqy"][0, 0] / s["plqy"] - 1) < 1e-7
+            floor = 1e-12 * np.max(d.N_c)
+            for key in ("n", "p"):
+                w = s[key] > floor
+                np.testing.assert_allclose(b[key][0, 0][w], s[key][w], rtol=1e-7)
+            J, ok, _ = dd.solve_jv(d, [V])
+            assert ok[0] and s["J"] == J[0] - (V / d.R_shunt if d.R_shunt > 0 else 0.0)
+            assert np.allclose(s["qfls"], d.Vt * np.log(s["n"] * s["p"] / d.ni ** 2))
+    half = dd.solve_state(cell, 0.0, g_frac=0.5)
+    J, _, _ = dd.solve_jv(cell, [0.0], g_frac=0.5)
+    assert half["J"] == J[0]  # at 0 V the shunt carries nothing
+    assert half["plqy"] != dd.solve_state(cell, 0.0)["plqy"]
