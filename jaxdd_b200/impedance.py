@@ -113,17 +113,22 @@ class Work:
 
 def solve_impedance(batch: Batch, frequencies, voltage: float = 0.0, tol: float = 1e-10,
                     max_iter: int = 60, bernoulli_name: str = "exact",
+                    ion_flux: str = "electrochemical",
                     dt: float | None = None) -> ImpedanceResult:
     """The impedance of a batch at the internal voltage `voltage` (V) at each of `frequencies`
     (Hz), from the steady state there by one complex linear solve per frequency (jaxdd
-    impedance.py:365-409). Free mobile ions move with the voltage as unknowns of their own.
-    Several ion regions of a species each keep their own number; a region that reaches a contact
-    takes the contact's ions from its neighbour's (jaxdd's `_ion_full`). Refused
-    (`NotImplementedError`), as the reference refuses them: ions frozen at a pre-bias. With the differential current (`currDiffInt = 1`) the current's tangent is
-    each interval's Scharfetter–Gummel flux's, the ions' too. `dt` (s): instead of the continuous
-    response, what
-    `solve_transient` sees through implicit Euler at steps of `dt` (its time terms at
-    `(1 − e^(−iω dt))/dt`, the traps' occupations over each step as it solves them)."""
+    impedance.py:371-409, same arguments). Free mobile ions move with the voltage as unknowns of
+    their own. Several ion regions of a species each keep their own number; a region that
+    reaches a contact takes the contact's ions from its neighbour's (jaxdd's `_ion_full`). With
+    the differential current (`currDiffInt = 1`) the current's tangent is each interval's
+    Scharfetter–Gummel flux's, the ions' too. Refused (`NotImplementedError`), as the reference
+    refuses them: ions frozen at a pre-bias. `ion_flux`: one of jaxdd's two ion fluxes
+    (`ValueError` otherwise); without ion sites both are the Scharfetter–Gummel flux, the only
+    case built. `dt` (s): instead of the continuous response, what `solve_transient` sees
+    through implicit Euler at steps of `dt` (its time terms at `(1 − e^(−iω dt))/dt`, the traps'
+    occupations over each step as it solves them)."""
+    if ion_flux not in ("electrochemical", "modified-drift"):
+        raise ValueError(f"ion_flux {ion_flux!r}: one of ('electrochemical', 'modified-drift')")
     devs = batch["devices"]
     if _mobile(batch) and any(d.pre_cond and d.fix_ions for d in devs):
         raise NotImplementedError("impedance with ions frozen at a pre-bias")

@@ -188,3 +188,18 @@ def test_the_solvers_refuse_without_a_gpu():
         solve_state(dev, 0.0)
     with pytest.raises(RuntimeError, match="needs a CUDA GPU"):
         solve_jv(dev, [0.0, 0.5])
+
+
+def test_the_public_names_are_the_references_in_scope():
+    """The names jaxdd exports (src/jaxdd/__init__.py) that lie on the path are exported here
+    under the same names; `solve_impedance` checks `ion_flux` as jaxdd does before any solve."""
+    import jaxdd_b200
+    for name in ("TVG", "Device", "ImpedanceResult", "JVResult", "Layer", "Setup",
+                 "StateResult", "TransientResult", "TransientState", "build_device",
+                 "check_supported", "external_voltages", "prepare", "read_setup", "read_tvg",
+                 "setup_from_texts", "simss_voltages", "solve_batch", "solve_impedance",
+                 "solve_jv", "solve_state", "solve_states", "solve_transient", "tj_columns"):
+        assert name in jaxdd_b200.__all__ and hasattr(jaxdd_b200, name), name
+    dev = build_device(read_setup(GOLDEN / "inputs" / "thin_l1_light" / "simulation_setup.txt"))
+    with pytest.raises(ValueError, match="ion_flux"):
+        jaxdd_b200.solve_impedance(prepare([dev]), [1e3], ion_flux="sites")
