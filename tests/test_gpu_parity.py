@@ -202,3 +202,33 @@ def test_pin_cell_at_its_full_size_through_both_solvers():
     assert np.max(np.abs(J - Jb)) < 1e-6 * js, np.max(np.abs(J - Jb)) / js
     # the two solvers reach the same roots: each curve within the other's tolerance
     assert np.max(np.abs(J[0] - r.J)) < 1e-6 * js
+
+
+def test_voltage_lists_in_any_order_with_repeats_and_alone():
+    """The voltages as a caller may give them (jaxdd batch.py:1043-1045 returns every result in
+    the caller's order): unsorted with a voltage repeated, and a single voltage, through
+    `solve_batch` and `solve_jv`, for the p-i-n cell and a frozen and a free-ion drawn device,
+    against the oracle: J within 1e-6 of the current scale, converged flags equal; a repeated
+    voltage's results agree to the same bar wherever it sits in the list."""
+    from jaxdd_b200.workloads import drawn_devices, pin_stack
+    devs = [pin_stack(NP=120)] + drawn_devices(2, NP=120)
+    od = dd.prepare(devs)
+    scale = od["J_scale"][:, None]
+    V = [0.5, 0.5, -0.1, 1.0, 0.5, 0.2]
+    J, ok, its = solve_batch(prepare(devs), V)
+    Jo, oko, _ = dd.solve_batch(od, V)
+    assert J.shape == ok.shape == its.shape == (3, 6)
+    assert np.array_equal(ok, oko) and ok.all()
+    assert np.all(np.abs(J - Jo) < 1e-6 * scale)
+    assert np.all(np.abs(J[:, [1, 4]] - J[:, [0]]) < 1e-6 * scale)
+    J1, ok1, _ = solve_batch(prepare(devs), [0.3])
+    Jo1, oko1, _ = dd.solve_batch(od, [0.3])
+    assert J1.shape == (3, 1) and np.array_equal(ok1, oko1) and ok1.all()
+    assert np.all(np.abs(J1 - Jo1) < 1e-6 * scale)
+    for k, d in enumerate(devs):
+        for volts in (V, [0.3]):
+            r = solve_jv(d, volts)
+            Jj, okj, _ = dd.solve_jv(d, volts)
+            assert np.array_equal(r.converged, okj) and r.converged.all()
+            assert np.max(np.abs(r.J - Jj)) < 1e-6 * scale[k, 0]
+            assert np.array_equal(r.V, np.asarray(volts, dtype=float))
