@@ -2199,8 +2199,9 @@ int dd_transient(const dd_batch* batch, const double* tstat, const dd_steps* ste
       !steps->failure_mode || (steps->stride != 0 && steps->stride != batch->lane_stride))
     return DD_ERR_ARGS;
   if (steps->vint && (!steps->oc || !steps->r_series || !steps->start_j_ext)) return DD_ERR_ARGS;
-  // the gradients with the internal voltage an unknown: not with an ion region at a contact
-  // (the host refuses that case for the transient itself)
+  // The internal voltage an unknown with an ion region that reaches a contact (the transient
+  // and its gradients) is not built: the host (jaxdd_b200/transient.py) refuses it before any
+  // launch; this entry point does not check it.
   if (!out->J || !out->J_ext || !out->converged || !out->iterations || !out->accepted ||
       !out->stop || !out->state || !out->logs)
     return DD_ERR_ARGS;
