@@ -183,8 +183,9 @@ int dd_admittance_workspace_bytes(const dd_batch* batch, int n_freq, size_t* byt
  * one complex block-tridiagonal solve of (J + i omega M + the traps' occupations' own dynamics)
  * dy = -dF/dV per (lane, frequency) and the linearised current of a time step (control-volume
  * widths, each density's change, the displacement current; `eps` [np_max+2][lane_stride] the
- * permittivity at every point). Y [n_freq][2][lane_stride] (re, im). Lanes with mobile ions are
- * not supported (the host refuses them): k_anion and k_cation must be 1. `dt` 0: the continuous
+ * permittivity at every point). Y [n_freq][2][lane_stride] (re, im). A batch with mobile ions
+ * goes to dd_admittance_ions instead (the host routes it there): here k_anion and k_cation must
+ * be 1 (DD_ERR_ARGS otherwise). `dt` 0: the continuous
  * response; dt > 0: what a transient sees through implicit Euler at steps of dt (jaxdd's
  * `solve_impedance(..., dt=)`, impedance.py:379-383): `laps` then (1 - e^(-i omega dt))/dt and
  * the traps' occupations those of their exact step (its mean in the rates, its end in the
