@@ -4,8 +4,8 @@ The drop-in API of jaxdd (`build_device`, `prepare`, `solve_jv`, `solve_batch`, 
 src/jaxdd/__init__.py:14-29), `solve_state` and `solve_states`, `solve_transient` (ZimT's time
 steps with mobile ions) and its `tj_columns`, `solve_impedance`, plus `solve_uneven` (every
 device its own grid size and voltage list, in one launch), over hand-written sm_100a CUDA
-kernels behind a C ABI (include/jaxdd_b200.h). Device building is host NumPy, as in jaxdd; the solve runs only on the
-GPU (no CPU fallback: without the built library the solvers raise).
+kernels behind a C ABI (include/jaxdd_b200.h). Device building is host NumPy, as in jaxdd; the
+solve runs only on the GPU (no CPU fallback: without the built library the solvers raise).
 """
 
 from .batch import (Batch, external_voltages, prepare, solve_batch, solve_states,
