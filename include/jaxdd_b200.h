@@ -130,7 +130,9 @@ int dd_tune(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts
  * [nv_max][np_max+2][3][lane_stride] (interior nodes written) and its ion normalisations
  * `state_logs` [nv_max][DD_MAXK][lane_stride]; and the solution at the pre-bias (or first)
  * voltage, before any freeze, `prebias` [np_max+2][3][lane_stride], `prebias_logs`
- * [DD_MAXK][lane_stride]. Results otherwise those of dd_solve. */
+ * [DD_MAXK][lane_stride]. Results otherwise those of dd_solve, in either mode: DD_MODE_JV with
+ * one voltage is jaxdd's `solve_state` (solver.py:2063-2093) once dd_observables has read the
+ * checkpoint; dd_adjoint (which reads no mode) is used and tested on DD_MODE_BATCH's. */
 int dd_solve_states(const dd_batch* batch, const dd_voltages* volts, const dd_opts* opts,
                     double* J, uint8_t* converged, int32_t* iterations, int32_t* lane_status,
                     int32_t* lane_steps, double* states, double* state_logs, double* prebias,
