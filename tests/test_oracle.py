@@ -146,13 +146,16 @@ def test_state_restatement_is_each_devices_batch_state():
     """`solve_state` (solver.py:2063-2093) restated: as the reference checks it against
     `solve_states` (tests/test_free_surface.py:290-310), each device's implied V_oc to 1e-8 V,
     its PLQY to 1e-7 and its densities to 1e-7 where Newton weighs them (above its floor), for
-    the SimSS cell of `none_light`, the p-i-n cell and a frozen and a free-ion drawn device, at
-    0 and 0.8 V; its current is `solve_jv`'s at the same voltage less the shunt's, which pins it
-    on SimSS's curve through `test_oracle_reproduces_simss`; and a generation factor scales the
-    generation as `solve_jv`'s does."""
+    the SimSS cell of `none_light` and that of `resist_light` (a shunt of 0.3 Ohm m^2), the
+    p-i-n cell and a frozen and a free-ion drawn device, at 0 and 0.8 V; its current is
+    `solve_jv`'s at the same voltage less the shunt's (to the bit without a shunt, to 1e-12 of
+    it with one), which pins it on SimSS's curve through `test_oracle_reproduces_simss`; and a
+    generation factor scales the generation as `solve_jv`'s does."""
     from jaxdd_b200.workloads import drawn_devices, pin_stack
     cell = build_device(read_setup(GOLDEN / "inputs" / "none_light" / "simulation_setup.txt"))
-    devs = [cell, pin_stack(NP=120)] + drawn_devices(2, NP=120)
+    shunted = build_device(read_setup(GOLDEN / "inputs" / "resist_light" / "simulation_setup.txt"))
+    assert shunted.R_shunt > 0
+    devs = [cell, shunted, pin_stack(NP=120)] + drawn_devices(2, NP=120)
     for d in devs:
         for V in (0.0, 0.8):
             s = dd.solve_state(d, V)
@@ -166,7 +169,8 @@ def test_state_restatement_is_each_devices_batch_state():
                 w = s[key] > floor
                 np.testing.assert_allclose(b[key][0, 0][w], s[key][w], rtol=1e-7)
             J, ok, _ = dd.solve_jv(d, [V])
-            assert ok[0] and s["J"] == J[0] - (V / d.R_shunt if d.R_shunt > 0 else 0.0)
+            shunt = V / d.R_shunt if d.R_shunt > 0 else 0.0
+            assert ok[0] and abs(s["J"] - (J[0] - shunt)) <= 1e-12 * abs(shunt)
             assert np.allclose(s["qfls"], d.Vt * np.log(s["n"] * s["p"] / d.ni ** 2))
     half = dd.solve_state(cell, 0.0, g_frac=0.5)
     J, _, _ = dd.solve_jv(cell, [0.0], g_frac=0.5)
