@@ -40,7 +40,8 @@ def test_states_match_the_oracle():
 def test_one_state_matches_the_oracle():
     """`solve_state` (jaxdd solver.py:2063-2093) on the GPU, solve_jv's scan at one voltage,
     against the oracle's restatement: the SimSS cell of `none_light` (NP 400), the p-i-n cell and
-    a frozen and a free-ion drawn device (NP 120), at 0 and 0.8 V and at half the generation:
+    a frozen and a free-ion drawn device (NP 120), at 0 and 0.8 V and at half the generation, and
+    the shunted cell of `resist_light` at 0.8 V:
     converged as the oracle, J within 1e-6 of the current scale and without the shunt's current,
     the potential, ions and radiative measures to the bars of the batch test above, the
     densities and their splitting there where Newton weighs them (above its floor, as the
@@ -49,8 +50,9 @@ def test_one_state_matches_the_oracle():
     from jaxdd_b200.workloads import pin_stack
     from conftest import GOLDEN
     cell = build_device(read_setup(GOLDEN / "inputs" / "none_light" / "simulation_setup.txt"))
+    shunted = build_device(read_setup(GOLDEN / "inputs" / "resist_light" / "simulation_setup.txt"))
     cases = [(d, V, None) for d in [cell, pin_stack(NP=120)] + drawn_devices(2, NP=120)
-             for V in (0.0, 0.8)] + [(cell, 0.0, 0.5)]
+             for V in (0.0, 0.8)] + [(cell, 0.0, 0.5), (shunted, 0.8, None)]
     for d, V, g in cases:
         got = solve_state(d, V, g_frac=g)
         ref = dd.solve_state(d, V, g_frac=g)
