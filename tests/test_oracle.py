@@ -176,3 +176,27 @@ def test_state_restatement_is_each_devices_batch_state():
     J, _, _ = dd.solve_jv(cell, [0.0], g_frac=0.5)
     assert half["J"] == J[0]  # at 0 V the shunt carries nothing
     assert half["plqy"] != dd.solve_state(cell, 0.0)["plqy"]
+
+
+def test_two_passes_give_the_one_pass_result():
+    """jaxdd's two passes (`first_max_iter` steps per voltage, then the devices that missed it
+    with `max_iter`) give one pass at `max_iter`'s flags and Newton steps exactly and its curves
+    to round-off (tests/test_solver.py:1495-1513), on the reference's three cases, two of them
+    twice, one of which needs more than six steps at a voltage; so the GPU kernel, which runs
+    the one pass (every lane advancing on its own), returns what the two passes return. Also on
+    the benchmark's drawn devices (frozen and free ions)."""
+    from jaxdd_b200.workloads import drawn_devices
+    cases = ["thin_l1_light", "frozen_1e17_x1_thin_light", "steady_1e17_thin_light"]
+    devices = [build_device(read_setup(GOLDEN / "inputs" / c / "simulation_setup.txt"))
+               for c in cases]
+    V = np.round(np.arange(-0.2, 1.3 + 1e-9, 0.1), 6)
+    for devs in (devices + devices[:2], drawn_devices(4, NP=120)):
+        b = dd.prepare(devs)
+        first = dd.solve_one(b, V, dd.BERNOULLI["exact"], 1e-10, 6, 60)[1]  # the first pass
+        one = dd.solve_batch(b, V, first_max_iter=None)
+        two = dd.solve_batch(b, V, first_max_iter=6)
+        assert one[1].all()
+        assert np.array_equal(one[1], two[1]) and np.array_equal(one[2], two[2])
+        assert np.max(np.abs(one[0] - two[0])) <= 1e-12 * np.max(np.abs(one[0]))
+        if devs[0] is devices[0]:
+            assert 0 < (~first.all(axis=1)).sum() < len(devs)  # a second pass ran
