@@ -48,6 +48,8 @@ CASES = (
     "zimt_track_tpv_light", "zimt_track_tpv3_light",
     # the sweep with each layer's voltage drop written (`specialOutput = spv`)
     "zimt_sweep_spv_light",
+    # SimSS's curve at 0.1 mV steps around its open-circuit voltage
+    "thin_l1_voc_light",
 )
 
 

@@ -176,6 +176,25 @@ def test_the_photovoltage_at_the_open_circuit_reproduces_zimt():
     assert np.max(np.abs(r["J_ext"])) < 1e-10 * np.max(ref["JphotoL2"])
 
 
+def test_the_open_circuit_in_the_steady_state_is_simss_voc():
+    """The open circuit at `t = 0` (the internal voltage the unknown of the steady state): SimSS
+    5.36's V_oc, from its curve at 0.1 mV steps around it (the reference's thin_l1_voc_light, a
+    cubic through its points), to 1e-10 V (test_solver.py:750-765)."""
+    import dataclasses
+    setup, tvg, _ = zimt_case("zimt_tpv_light")
+    first = dataclasses.replace(tvg, **{k: getattr(tvg, k)[:1] for k in
+                                        ("t", "Vext", "oc", "G_frac", "track", "dti")})
+    r = transient.solve_transient(dd.prepare([build_device(setup, grid="simss")]), first.t,
+                                  first.Vext, first.G_frac, first.track, first.failure_mode,
+                                  bernoulli_name="simss", oc=first.oc)
+    jv = np.genfromtxt(INPUTS / "thin_l1_voc_light" / "JV.dat", names=True)
+    roots = np.roots(np.polyfit(jv["Vext"] - jv["Vext"].mean(), jv["Jext"], 3))
+    roots = roots[np.abs(roots.imag) == 0].real + jv["Vext"].mean()
+    voc = roots[(roots > jv["Vext"].min()) & (roots < jv["Vext"].max())]
+    assert first.oc[0] and r["converged"].all() and voc.size == 1
+    assert abs(r["V_int"][0, 0] - voc[0]) < 1e-10
+
+
 def test_a_series_resistance_in_time_reproduces_zimt():
     """`R_series` with a shunt, `Vint` the unknown whose `Vint + Jext R_series` is the given
     `Vext`: ZimT 5.36's `Jext` through a sweep to 1.2 V and back in 2 x 100 ns to 1e-9 of its
