@@ -200,3 +200,19 @@ def test_two_passes_give_the_one_pass_result():
         assert np.max(np.abs(one[0] - two[0])) <= 1e-12 * np.max(np.abs(one[0]))
         if devs[0] is devices[0]:
             assert 0 < (~first.all(axis=1)).sum() < len(devs)  # a second pass ran
+
+
+def test_newton_ends_at_a_step_that_is_not_a_number():
+    """A Newton loop whose iterate is lost ends there, unconverged, after that one step, not at
+    `max_iter` (tests/test_solver.py:2115-2131): no later step is a number either, and the lane
+    would otherwise pay every one of them. The same loop from the intact start converges."""
+    dev, _, _ = _case("steady_1e17_thin_light")
+    d = dd.prepare([dev])
+    full = dd.initial(d, np.zeros(1))
+    y = full[:, 1:-1].copy()
+    logs = dd.ion_logs(full[..., 0], d["ion"], d["Vt"])
+    _, _, _, ok, it = dd.newton_loop(y, logs, d, 0.0, dd.BERNOULLI["exact"], 1e-10, 50)
+    assert ok[0] and 1 < it[0] < 50
+    y[0, 7, 1] = np.nan
+    _, _, _, ok, it = dd.newton_loop(y, logs, d, 0.0, dd.BERNOULLI["exact"], 1e-10, 50)
+    assert not ok[0] and it[0] == 1
