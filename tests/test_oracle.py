@@ -216,3 +216,18 @@ def test_newton_ends_at_a_step_that_is_not_a_number():
     y[0, 7, 1] = np.nan
     _, _, _, ok, it = dd.newton_loop(y, logs, d, 0.0, dd.BERNOULLI["exact"], 1e-10, 50)
     assert not ok[0] and it[0] == 1
+
+
+def test_free_ions_keep_their_number():
+    """The steady state moves the ions, never creates them (tests/test_solver.py:1462-1476):
+    at any potential the normalisations `ion_logs` gives make each region's trapezoidal number
+    its total (the constraints zero to 1e-12), on the steady-ions case and a two-region one."""
+    rng = np.random.default_rng(0)
+    for case in ("steady_1e17_thin_light", "two_regions_light"):
+        dev, _, _ = _case(case)
+        d = dd.prepare([dev])
+        V = rng.normal(0.0, 0.3, (1, len(dev.x)))
+        logs = dd.ion_logs(V, d["ion"], d["Vt"])
+        g, _, _ = dd.ion_constraints(V, logs, d["ion"], d["Vt"])
+        assert np.any(dd._masks(d["ion"])[1] > 0)
+        assert np.allclose(g, 0.0, atol=1e-12)
