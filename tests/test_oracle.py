@@ -231,3 +231,67 @@ def test_free_ions_keep_their_number():
         g, _, _ = dd.ion_constraints(V, logs, d["ion"], d["Vt"])
         assert np.any(dd._masks(d["ion"])[1] > 0)
         assert np.allclose(g, 0.0, atol=1e-12)
+
+
+def _fd_column(f, x, idx, h=1e-6):
+    """Central difference of `f` along one entry `idx` of `x`."""
+    xp, xm = x.copy(), x.copy()
+    xp[idx] += h
+    xm[idx] -= h
+    fp, fm = f(xp), f(xm)
+    return [(a - b) / (2 * h) for a, b in zip(fp, fm)], fp
+
+
+@pytest.mark.parametrize("case", ["iface_charged_light", "two_regions_light", "pin_iface_light",
+                                  "steady_1e17_thin_light"])
+def test_the_blocks_are_the_residuals_derivatives(case):
+    """The hand-written Jacobian (the reference takes it by autodiff: tests/test_solver.py's
+    `the_jacobian_by_edges_is_autodiff_of_the_rows` and `the_interface_traps_jacobian_is_
+    autodiff`) against central differences of the residual at a state off the solution: the
+    blocks A, B, C of every row next to a perturbed point, nothing elsewhere; the slots' columns
+    U; the constraints' W and D. To 1e-7 of each row's largest entry, beside the difference's
+    own rounding (the residual's size over the step)."""
+    dev, _, _ = _case(case)
+    d = dd.prepare([dev])
+    bnd = dd.bounds(d, np.array([0.4]))
+    rng = np.random.default_rng(1)
+    y = dd.initial(d, np.array([0.4]))[:, 1:-1].copy()
+    y[..., 0] += rng.normal(0, 0.02, y.shape[1])
+    y[..., 1:] += rng.normal(0, 0.2, (y.shape[1], 2))
+    logs = dd.ion_logs(dd.full_of(bnd, y)[..., 0], d["ion"], d["Vt"])
+    bern = dd.BERNOULLI["exact"]
+    F0, g0, (A, Bb, C, U, W, D) = dd.system(y, logs, bnd, d, d["s"], d["ion"], bern)
+    NP, h, eps = y.shape[1], 1e-6, np.finfo(float).eps
+    scale = np.maximum(np.maximum(np.abs(A[0]).max(2), np.abs(Bb[0]).max(2)), np.abs(C[0]).max(2))
+
+    def bar(F):  # each row's allowance: 1e-7 of its scale plus the difference's rounding
+        return 1e-7 * scale + 100 * eps * np.maximum(np.abs(F[0]), np.abs(F0[0])) / h
+
+    def by_state(yy):
+        F, g, _ = dd.system(yy, logs, bnd, d, d["s"], d["ion"], bern)
+        return F, g
+
+    interfaces = [i for i in dev.i1[:-1]]
+    nodes = sorted({0, 1, NP // 2, NP - 1} | {j for i in interfaces for j in (i - 2, i - 1, i)
+                                              if 0 <= j < NP})
+    for j in nodes:
+        for c in range(3):
+            (dF, dg), (Fp, _) = _fd_column(by_state, y, (0, j, c), h)
+            an = np.zeros_like(dF[0])
+            an[j] = Bb[0, j, :, c]
+            if j > 0:
+                an[j - 1] = C[0, j - 1, :, c]
+            if j < NP - 1:
+                an[j + 1] = A[0, j + 1, :, c]
+            assert np.all(np.abs(dF[0] - an) <= bar(Fp)), (j, c)
+            if c == 0:
+                assert np.allclose(dg[0], W[0, :, j], rtol=0, atol=1e-7 * np.max(np.abs(W)) + 1e-30)
+            else:
+                assert np.all(dg == 0)
+    held = dd._held(d["ion"])[0]
+    for k in range(logs.shape[1]):
+        (dF, dg), (Fp, _) = _fd_column(
+            lambda ll: dd.system(y, ll, bnd, d, d["s"], d["ion"], bern)[:2], logs, (0, k), h)
+        assert np.all(np.abs(dF[0] - U[0, :, :, k]) <= bar(Fp)), k
+        if not held[k]:
+            assert np.allclose(dg[0], D[0, :, k], rtol=0, atol=1e-7)
