@@ -386,3 +386,77 @@ def test_a_given_state_is_checked_before_any_solve():
         solve_transient(batch, later, initial=dataclasses.replace(good, V_int=np.zeros(2)))
     with pytest.raises(ValueError, match=r"initial\.f_bulk"):
         solve_transient(batch, later, initial=dataclasses.replace(good, f_bulk=np.zeros((1, 4))))
+
+
+@pytest.mark.parametrize("case", ["zimt_ions_fast_light", "zimt_traps_photo_light",
+                                  "zimt_iface_sweep_light", "zimt_region_slow_light",
+                                  "zimt_regions2_light"])
+def test_the_blocks_of_a_step_are_its_residuals_derivatives(case):
+    """The 5x5 Jacobian of a time step (the reference takes it by autodiff:
+    tests/test_solver.py's `the_ions_blocks_in_time_are_autodiff`) against central differences
+    of the step's residual, off the solution, over a 1 us step with the traps' occupations
+    anywhere in (0, 1): the blocks next to every perturbed point (bulk and interface traps, ion
+    regions inside the device and at its contacts, whose densities follow their neighbours), the
+    slots' columns and the constraints' derivatives. To 1e-7 of each row's largest entry beside
+    the difference's own rounding."""
+    setup, tvg, _ = zimt_case(case)
+    dev = build_device(setup, grid="simss")
+    d = dd.prepare([dev])
+    bern = dd.BERNOULLI["simss"]
+    Vint = np.array([0.5])
+    y3, logs, _ = dd.start(d, Vint, bern, 1e-10, 200)
+    s, ion, Vt = d["s"], d["ion"], d["Vt"]
+    la, lc = dd.point_logs(logs, ion)
+    za, zc = la + y3[..., 0] / Vt[:, None], lc - y3[..., 0] / Vt[:, None]
+    y = np.concatenate([y3, np.stack([np.where(s["a_mask"] > 0, za, 0.0),
+                                      np.where(s["c_mask"] > 0, zc, 0.0)], -1)], -1)
+    NP = y.shape[1]
+    rng = np.random.default_rng(2)
+    before = transient.full_of(d, y, Vint)
+    tr = {"dti": np.array([1e6]), "n": np.exp(before[:, 1:-1, 1]),
+          "p": np.exp(before[:, 1:-1, 2]), "a": np.exp(before[:, 1:-1, 3]) * s["a_mask"],
+          "c": np.exp(before[:, 1:-1, 4]) * s["c_mask"], "fb": rng.uniform(0, 1, (1, NP)),
+          "fi": rng.uniform(0, 1, (1, NP + 1))}
+    mobile = np.stack([s["a_mask"][0], s["c_mask"][0]], -1) > 0
+    y[..., 0] += rng.normal(0, 0.01, NP)
+    y[..., 1:3] += rng.normal(0, 0.1, (NP, 2))
+    y[..., 3:] += np.where(mobile, rng.normal(0, 0.1, (NP, 2)), 0.0)
+
+    def system(yy, ll):
+        full, dV = transient.ion_full(d, transient.full_of(d, yy, Vint), bern, tr["dti"])
+        F, A, Bb, C, U = transient.assemble(full, d, tr, ll, bern)
+        g, W, D = transient.constraints(full, ll, ion, dV)
+        return F, g, (A, Bb, C, U, W, D)
+
+    F0, _, (A, Bb, C, U, W, D) = system(y, logs)
+    h, eps = 1e-6, np.finfo(float).eps
+    scale = np.maximum(np.maximum(np.abs(A[0]).max(2), np.abs(Bb[0]).max(2)), np.abs(C[0]).max(2))
+
+    def bar(F):
+        return 1e-7 * scale + 100 * eps * np.maximum(np.abs(F[0]), np.abs(F0[0])) / h
+
+    nodes = sorted({0, 1, NP // 2, NP - 2, NP - 1}
+                   | {j for i in dev.i1[:-1] for j in (i - 2, i - 1, i) if 0 <= j < NP})
+    for j in nodes:
+        for c in range(5):
+            yp, ym = y.copy(), y.copy()
+            yp[0, j, c] += h
+            ym[0, j, c] -= h
+            Fp, gp, _ = system(yp, logs)
+            Fm, gm, _ = system(ym, logs)
+            an = np.zeros_like(F0[0])
+            an[j] = Bb[0, j, :, c]
+            if j > 0:
+                an[j - 1] = C[0, j - 1, :, c]
+            if j < NP - 1:
+                an[j + 1] = A[0, j + 1, :, c]
+            assert np.all(np.abs((Fp - Fm)[0] / (2 * h) - an) <= bar(Fp)), (j, c)
+            assert np.allclose((gp - gm)[0] / (2 * h), W[0, :, j, c], rtol=0,
+                               atol=1e-7 * np.max(np.abs(W)) + 1e-30), (j, c)
+    for k in range(logs.shape[1]):
+        lp, lm = logs.copy(), logs.copy()
+        lp[0, k] += h
+        lm[0, k] -= h
+        Fp, gp, _ = system(y, lp)
+        Fm, gm, _ = system(y, lm)
+        assert np.all(np.abs((Fp - Fm)[0] / (2 * h) - U[0, :, :, k]) <= bar(Fp)), k
