@@ -295,3 +295,44 @@ def test_the_blocks_are_the_residuals_derivatives(case):
         assert np.all(np.abs(dF[0] - U[0, :, :, k]) <= bar(Fp)), k
         if not held[k]:
             assert np.allclose(dg[0], D[0, :, k], rtol=0, atol=1e-7)
+
+
+def test_the_bordered_system_is_solved():
+    """The bordered solve (batch.py:595-603: the block sweep on 1 + K right-hand sides, then
+    the K x K Schur complement) against a dense solve of the whole system [[T, U], [W, D]]
+    (tests/test_solver.py's `the_bordered_system_and_its_transpose_are_solved`), for the
+    steady form (W on the potential only) and the time step's (W on every unknown), K = 2
+    and 4."""
+    from oracle import transient
+    rng = np.random.default_rng(3)
+    for m, K, solve in ((3, 2, dd.bordered_solve), (3, 4, dd.bordered_solve),
+                        (5, 2, transient.bordered_solve), (5, 4, transient.bordered_solve)):
+        nb, NP = 2, 9
+        A = rng.normal(size=(nb, NP, m, m))
+        C = rng.normal(size=(nb, NP, m, m))
+        Bb = rng.normal(size=(nb, NP, m, m)) + 8 * m * np.eye(m)
+        A[:, 0] = 0
+        C[:, -1] = 0
+        U = rng.normal(size=(nb, NP, m, K))
+        W = rng.normal(size=(nb, K, NP)) if m == 3 else rng.normal(size=(nb, K, NP, m))
+        D = rng.normal(size=(nb, K, K)) + 4 * NP * np.eye(K)
+        r, rg = rng.normal(size=(nb, NP, m)), rng.normal(size=(nb, K))
+        x, z = solve(A, Bb, C, U, W, D, r, rg)
+        for b in range(nb):
+            n = m * NP
+            M = np.zeros((n + K, n + K))
+            for i in range(NP):
+                M[m * i:m * i + m, m * i:m * i + m] = Bb[b, i]
+                if i:
+                    M[m * i:m * i + m, m * i - m:m * i] = A[b, i]
+                if i < NP - 1:
+                    M[m * i:m * i + m, m * i + m:m * i + 2 * m] = C[b, i]
+            M[:n, n:] = U[b].reshape(n, K)
+            if m == 3:
+                M[n:, 0:n:3] = W[b]
+            else:
+                M[n:, :n] = W[b].reshape(K, n)
+            M[n:, n:] = D[b]
+            ref = np.linalg.solve(M, np.concatenate([r[b].reshape(n), rg[b]]))
+            assert np.allclose(np.concatenate([x[b].reshape(n), z[b]]), ref, rtol=1e-10,
+                               atol=1e-12)
