@@ -336,3 +336,12 @@ def test_the_bordered_system_is_solved():
             ref = np.linalg.solve(M, np.concatenate([r[b].reshape(n), rg[b]]))
             assert np.allclose(np.concatenate([x[b].reshape(n), z[b]]), ref, rtol=1e-10,
                                atol=1e-12)
+
+
+def test_bernoulli_is_finite_at_zero_and_simss_is_within_its_own_error():
+    """B(0) = 1 and B'(0) = -1/2, neither seeing 0/0 (tests/test_solver.py:50-53); SIMsalabim's
+    Bernoulli function is the exact one to 1e-3 over [-5, 5] (tests/test_solver.py:62-64)."""
+    B, dB = dd.bern_exact(np.array([0.0]))
+    assert B[0] == 1.0 and dB[0] == pytest.approx(-0.5)
+    x = np.linspace(-5.0, 5.0, 2001)
+    assert np.max(np.abs(dd.bern_simss(x)[0] / dd.bern_exact(x)[0] - 1)) < 1e-3
