@@ -5,7 +5,10 @@ Tolerances and solvers follow the reference's tests (jaxdd tests/test_solver.py)
 (thin_l1_light 1e-5), 254-273 (held 1e-9, both solvers), 275-299 (regions 1e-6 / 2e-5), 302-321
 (two regions 2e-6), 878-888 (ions 2e-5), 890-906 (interface traps), 1318-1345 (resistances),
 1348-1358 (uniform generation), 408-420 (logarithmic scan), 1556-1575 (dark, batch, invariants),
-277-290 of the differential current (1e-9 single, 1e-8 batch)."""
+277-290 of the differential current (1e-9 single, 1e-8 batch). Beside the curves: the hand-written
+Jacobian against differences of the residual, the bordered solve against a dense one, two passes
+against one, Newton's end at a step that is not a number, the ions' numbers, the Bernoulli
+functions, and `solve_state` against `solve_states`."""
 
 import numpy as np
 import pytest
