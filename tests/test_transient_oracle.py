@@ -482,3 +482,23 @@ def test_the_integral_current_in_time_is_the_one_the_equations_balance():
     z = transient.solve_transient(b, *steps, zimt_current=True)
     assert np.max(np.abs(z["J_ext"][0] - r["J_ext"][1])) > 1e-3 * scale
     assert np.array_equal(z["J_ext"][1], r["J_ext"][1])
+
+
+def test_transients_with_and_without_ions_in_one_batch():
+    """Devices with mobile ions (one region of two layers, with the differential current)
+    beside devices with traps and with neither, in one batch of 5x5 blocks (the others' ion rows
+    held), each with its own steps and failure mode: each device's `Jext` is ZimT's to the
+    bar of its own case (tests/test_solver.py:698-712)."""
+    names = ("zimt_ions_slow_light", "zimt_region_diff_light", "zimt_photo_light",
+             "zimt_traps_photo_light")
+    cases = [zimt_case(c) for c in names]
+    tvgs = [tvg for _, tvg, _ in cases]
+    b = dd.prepare([build_device(setup, grid="simss") for setup, _, _ in cases])
+    r = transient.solve_transient(b, *(np.stack([getattr(t, f) for t in tvgs])
+                                       for f in ("t", "Vext", "G_frac", "track")),
+                                  np.array([t.failure_mode for t in tvgs]),
+                                  bernoulli_name="simss", zimt_current=True)
+    assert r["converged"].all()
+    for k, (name, (_, _, ref)) in enumerate(zip(names, cases)):
+        scale = np.max(np.abs(ref["Jext"]))
+        assert np.max(np.abs(r["J_ext"][k] - ref["Jext"])) < ZIMT[name] * scale, name
