@@ -9,7 +9,8 @@ Scope: the product's scope (Boltzmann carriers, neutral SRH bulk traps, interfac
 recombination, mobile ions in slots, pre-bias with frozen or free ions, integral or differential
 current, shunt). Derivatives that the reference takes by autodiff (`jax.jvp` of the Bernoulli
 function and of the interface traps, `jax.jacrev` of the ion constraints) are written out by hand
-here; they are exact, as autodiff is.
+here; they are exact, as autodiff is, and tests/test_oracle.py checks them against central
+differences of the residual.
 
 Pinning: the reference cannot run in this container (no JAX). The oracle is pinned against the
 reference's golden J-V curves (SimSS runs under the reference's tests/data) at the reference's
